@@ -1,0 +1,168 @@
+// The context, error reporting and device scratch of the C ABI, and the field gather
+// (kernels/staggered_field_2d/staggered_field_2d_pyccel.py:13-55).
+#include <mutex>
+
+#include "common.cuh"
+
+namespace bt {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string &message) { g_last_error = message; }
+
+void *Buffer::get(size_t need) {
+    if (need == 0) need = 1;
+    if (need <= bytes) return ptr;
+    release();
+    size_t grown = need + need / 4;
+    cudaError_t e = cudaMalloc(&ptr, grown);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        bytes = 0;
+        (void)cudaGetLastError();
+        throw Error{BT_ERR_ALLOC, std::string("cudaMalloc of ") + std::to_string(grown) +
+                                      " bytes: " + cudaGetErrorString(e)};
+    }
+    bytes = grown;
+    return ptr;
+}
+
+void Buffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+void *HostBuffer::get(size_t need) {
+    if (need <= bytes) return ptr;
+    release();
+    cudaError_t e = cudaMallocHost(&ptr, need);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        bytes = 0;
+        (void)cudaGetLastError();
+        throw Error{BT_ERR_ALLOC, std::string("cudaMallocHost: ") + cudaGetErrorString(e)};
+    }
+    bytes = need;
+    return ptr;
+}
+
+void HostBuffer::release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+namespace {
+
+__device__ __forceinline__ double clamped_bilinear(const double *__restrict__ f, i64 nj,
+                                                   double s, double t, i64 imax, i64 jmax) {
+    i64 i = (i64)floor(s);
+    if (i < 0) i = 0;
+    if (i > imax) i = imax;
+    i64 j = (i64)floor(t);
+    if (j < 0) j = 0;
+    if (j > jmax) j = jmax;
+    const double u = s - (double)i;
+    const double w = t - (double)j;
+    const double *p = f + i * nj + j;
+    const double f00 = __ldg(p), f01 = __ldg(p + 1), f10 = __ldg(p + nj), f11 = __ldg(p + nj + 1);
+    const double low = f00 + w * (f01 - f00);
+    const double high = f10 + w * (f11 - f10);
+    return low + u * (high - low);
+}
+
+__global__ void staggered_field(const double *__restrict__ px, const double *__restrict__ py,
+                                i64 n, const double *__restrict__ fx,
+                                const double *__restrict__ fy, i64 nx, i64 ny, double origin_x,
+                                double origin_y, double h, double *__restrict__ ex,
+                                double *__restrict__ ey) {
+    const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double sx = (px[k] - origin_x) / h;
+    const double sy = (py[k] - origin_y) / h;
+    ex[k] = clamped_bilinear(fx, ny, sx + 0.5, sy, nx - 1, ny - 2);
+    ey[k] = clamped_bilinear(fy, ny + 1, sx, sy + 0.5, nx - 2, ny - 1);
+}
+
+}  // namespace
+
+}  // namespace bt
+
+extern "C" {
+
+size_t bt_last_error(char *buf, size_t len) {
+    const std::string &m = bt::g_last_error;
+    if (buf && len) {
+        size_t c = m.size() < len - 1 ? m.size() : len - 1;
+        memcpy(buf, m.data(), c);
+        buf[c] = '\0';
+    }
+    return m.size();
+}
+
+const char *bt_version(void) { return "beamtracer-b200 0.1.0 (sm_100a)"; }
+
+int bt_ctx_create(int device, bt_ctx **out) {
+    return bt::guarded([&] {
+        BT_REQUIRE(out, "ctx: null out");
+        *out = nullptr;
+        int count = 0;
+        BT_CUDA(cudaGetDeviceCount(&count));
+        BT_REQUIRE(device >= 0 && device < count, "ctx: no such CUDA device");
+        BT_CUDA(cudaSetDevice(device));
+        bt_ctx *ctx = new bt_ctx;
+        ctx->device = device;
+        cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete ctx;
+            throw bt::Error{BT_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)};
+        }
+        ctx->stream = ctx->own_stream;
+        cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+        *out = ctx;
+    });
+}
+
+int bt_ctx_destroy(bt_ctx *ctx) {
+    return bt::guarded([&] {
+        if (!ctx) return;
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        delete ctx;
+    });
+}
+
+int bt_ctx_set_stream(bt_ctx *ctx, void *stream) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx, "ctx: null context");
+        ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    });
+}
+
+int bt_ctx_synchronize(bt_ctx *ctx) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx, "ctx: null context");
+        BT_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int bt_staggered_field_2d(bt_ctx *ctx, const double *px, const double *py, int64_t n,
+                          const double *fx, const double *fy, int64_t nx, int64_t ny,
+                          double origin_x, double origin_y, double h, double *ex, double *ey) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx, "gather: null context");
+        BT_REQUIRE(n >= 0, "gather: negative point count");
+        BT_REQUIRE(nx >= 2 && ny >= 2, "gather: the mesh needs at least 2 x 2 nodes");
+        if (n == 0) return;
+        BT_REQUIRE(px && py && fx && fy && ex && ey, "gather: null array");
+        bt::staggered_field<<<bt::blocks_for(n, 256), 256, 0, ctx->stream>>>(
+            px, py, n, fx, fy, nx, ny, origin_x, origin_y, h, ex, ey);
+        BT_CHECK_LAUNCH();
+    });
+}
+
+}  // extern "C"

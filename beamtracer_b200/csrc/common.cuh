@@ -1,0 +1,145 @@
+// Shared declarations of the beamtracer-b200 CUDA library: the context, device scratch,
+// error reporting and the small device helpers every kernel file uses.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/bt200.h"
+
+typedef int64_t i64;
+
+namespace bt {
+
+// -- errors --------------------------------------------------------------------------------
+
+void set_error(const std::string &message);
+
+struct Error {
+    int code;
+    std::string message;
+};
+
+#define BT_CUDA(call)                                                                     \
+    do {                                                                                  \
+        cudaError_t bt_e_ = (call);                                                       \
+        if (bt_e_ != cudaSuccess)                                                         \
+            throw ::bt::Error{BT_ERR_CUDA, std::string(#call) + ": " +                    \
+                                               cudaGetErrorString(bt_e_)};                \
+    } while (0)
+
+#define BT_CHECK_LAUNCH() BT_CUDA(cudaGetLastError())
+
+#define BT_REQUIRE(cond, msg)                                                             \
+    do {                                                                                  \
+        if (!(cond)) throw ::bt::Error{BT_ERR_ARG, (msg)};                                \
+    } while (0)
+
+// -- device scratch ------------------------------------------------------------------------
+
+// A growable device buffer owned by a context (grown with cudaMalloc, never shrunk).
+struct Buffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    void *get(size_t need);
+    template <class T>
+    T *as(size_t count) {
+        return static_cast<T *>(get(count * sizeof(T)));
+    }
+    void release();
+    ~Buffer() { release(); }
+};
+
+// Pinned host memory for small read-backs.
+struct HostBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    void *get(size_t need);
+    void release();
+    ~HostBuffer() { release(); }
+};
+
+// The scratch of the deterministic deposit (records, their radix sort, per-cell sums).
+struct DepositScratch {
+    Buffer keys, keys_alt, vals, vals_alt, u, w, q;
+    Buffer hist, row_offsets, digit_base;
+    Buffer cell_sums, warp_first, warp_last, warp_flags;
+};
+
+// The tracer's live-trajectory lists and its deposit records.
+struct TraceScratch {
+    Buffer active_a, active_b, block_counts, n_alive;
+    Buffer rec_keys, rec_u, rec_w, rec_q;
+};
+
+}  // namespace bt
+
+struct bt_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int num_sms = 148;
+    bt::DepositScratch deposit;
+    bt::TraceScratch trace;
+    bt::HostBuffer host;
+    i64 last_windows = 0, last_records = 0, last_flushes = 0;
+};
+
+namespace bt {
+
+// Run `body` and map exceptions to an error code and message.
+template <class F>
+int guarded(F &&body) {
+    try {
+        body();
+        return BT_OK;
+    } catch (const Error &e) {
+        set_error(e.message);
+        return e.code;
+    } catch (const std::exception &e) {
+        set_error(e.what());
+        return BT_ERR_ALLOC;
+    }
+}
+
+inline unsigned blocks_for(i64 n, int threads) {
+    return (unsigned)((n + threads - 1) / threads);
+}
+
+// -- device helpers --------------------------------------------------------------------------
+
+// The radius sqrt(y^2 + z^2), formed by that expression (the oracle forms it the same way).
+__device__ __forceinline__ double radius(double y, double z) { return sqrt(y * y + z * z); }
+
+// The Lorentz factor sqrt(1 + |u|^2 / c^2) of a proper velocity u (1 for inv_c2 = 0).
+__device__ __forceinline__ double lorentz(double u0, double u1, double u2, double inv_c2) {
+    return sqrt(1.0 + (u0 * u0 + u1 * u1 + u2 * u2) * inv_c2);
+}
+
+// -- the deterministic deposit (deposit.cu) ---------------------------------------------------
+
+// Records: key[r] = the lower-left node of the cell the contribution goes to (or
+// `sentinel` for none), with its area weights (u along x, w along y) and charge q.
+// Sort by key (stable) and add every cell's contributions in record order into its
+// four nodes of `charge`; `node_patch` describes how keys map to nodes.
+struct NodeLayout {
+    const i64 *patch_int;  // (n_patches, 6) as the trace kernel's, device; NULL: one patch
+    i64 n_patches;
+    i64 nx, ny;            // the single patch's shape when patch_int is NULL
+    i64 n_nodes;
+};
+
+void deposit_records(bt_ctx *ctx, const uint32_t *keys, const double *u, const double *w,
+                     const double *q, i64 n_records, uint32_t sentinel, double *charge,
+                     const NodeLayout &layout);
+
+// Stable LSD radix sort of (key, index) pairs: sorted keys and the permutation.
+// Returns the device pointers of the sorted keys and values (inside the scratch).
+void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, int key_bits,
+                      uint32_t **keys_out, uint32_t **vals_out);
+
+}  // namespace bt

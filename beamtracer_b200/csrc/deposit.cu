@@ -1,0 +1,390 @@
+// The deterministic space-charge deposit: contributions (records) sorted by cell with a
+// stable LSD radix sort, summed per cell by warp segmented reductions in record order, and
+// added to the nodes by a gather in a fixed order.  No floating-point atomics: every call
+// on the same records gives the same node charges bit for bit.
+//
+// The per-record shape is the reference's area weighting
+// (kernels/deposit_trajectories_2d/deposit_trajectories_2d_pyccel.py:28-59,
+//  kernels/trace_trajectories_2d/trace_trajectories_2d_pyccel.py:397-423): a record
+// (cell c, u, w, q) adds (1-u)(1-w)q, (1-u)w q, u(1-w)q and u w q to the nodes c, c+1,
+// c+ny, c+ny+1.
+#include "common.cuh"
+
+namespace bt {
+
+namespace {
+
+constexpr int kThreads = 256;  // = the radix (one thread per digit in the scans)
+constexpr int kItems = 16;
+constexpr int kTile = kThreads * kItems;
+constexpr int kRadix = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+__global__ void radix_hist(const uint32_t *__restrict__ keys, i64 n, int shift,
+                           uint32_t *__restrict__ hist, int nblocks) {
+    __shared__ uint32_t h[kRadix];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const i64 base = (i64)blockIdx.x * kTile;
+#pragma unroll 4
+    for (int i = 0; i < kItems; ++i) {
+        const i64 r = base + (i64)i * kThreads + threadIdx.x;
+        if (r < n) atomicAdd(&h[(keys[r] >> shift) & (kRadix - 1)], 1u);
+    }
+    __syncthreads();
+    hist[(i64)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Inclusive scan of one value per thread over a block of kThreads threads.
+__device__ uint32_t block_inclusive_scan(uint32_t v, uint32_t *warp_sums) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        uint32_t y = __shfl_up_sync(kFull, v, off);
+        if (lane >= off) v += y;
+    }
+    if (lane == 31) warp_sums[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = lane < kWarps ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < kWarps; off <<= 1) {
+            uint32_t y = __shfl_up_sync(kFull, s, off);
+            if (lane >= off) s += y;
+        }
+        if (lane < kWarps) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    uint32_t out = v + (warp > 0 ? warp_sums[warp - 1] : 0);
+    __syncthreads();
+    return out;
+}
+
+// Row d of hist (one digit over all blocks) to its exclusive prefix; the row total.
+__global__ void radix_row_scan(const uint32_t *__restrict__ hist, uint32_t *__restrict__ offs,
+                               uint32_t *__restrict__ totals, int nblocks) {
+    __shared__ uint32_t warp_sums[kWarps];
+    __shared__ uint32_t carry;
+    const i64 row = (i64)blockIdx.x * nblocks;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int start = 0; start < nblocks; start += kThreads) {
+        const int b = start + threadIdx.x;
+        const uint32_t v = b < nblocks ? hist[row + b] : 0;
+        const uint32_t incl = block_inclusive_scan(v, warp_sums);
+        const uint32_t c = carry;
+        if (b < nblocks) offs[row + b] = c + incl - v;
+        __syncthreads();
+        if (threadIdx.x == kThreads - 1) carry = c + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
+}
+
+__global__ void radix_digit_base(const uint32_t *__restrict__ totals, uint32_t *__restrict__ base) {
+    __shared__ uint32_t warp_sums[kWarps];
+    const uint32_t v = totals[threadIdx.x];
+    const uint32_t incl = block_inclusive_scan(v, warp_sums);
+    base[threadIdx.x] = incl - v;
+}
+
+// Stable scatter of one tile: items in the order i * kThreads + t keep their order among
+// equal digits (warp ranks by __match_any_sync, warps in order by a per-digit prefix).
+__global__ void radix_scatter(const uint32_t *__restrict__ keys_in,
+                              const uint32_t *__restrict__ vals_in, i64 n, int shift,
+                              const uint32_t *__restrict__ offs,
+                              const uint32_t *__restrict__ base, int nblocks,
+                              uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out) {
+    __shared__ uint32_t wcount[kWarps][kRadix];
+    __shared__ uint32_t woff[kWarps][kRadix];
+    __shared__ uint32_t run[kRadix];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) wcount[w][t] = 0;
+    run[t] = base[t] + offs[(i64)t * nblocks + blockIdx.x];
+    __syncthreads();
+    const i64 tile = (i64)blockIdx.x * kTile;
+    const unsigned below = (1u << lane) - 1u;
+    for (int i = 0; i < kItems; ++i) {
+        const i64 r = tile + (i64)i * kThreads + t;
+        const bool valid = r < n;
+        const uint32_t key = valid ? keys_in[r] : 0u;
+        const uint32_t d = (key >> shift) & (kRadix - 1);
+        const uint32_t val = valid ? (vals_in ? vals_in[r] : (uint32_t)r) : 0u;
+        const unsigned peers = __match_any_sync(kFull, valid ? d : 0xffffffffu);
+        const int rank = __popc(peers & below);
+        if (valid && rank == 0) wcount[warp][d] = __popc(peers);
+        __syncthreads();
+        uint32_t acc = run[t];
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = wcount[w][t];
+            woff[w][t] = acc;
+            acc += c;
+            wcount[w][t] = 0;
+        }
+        run[t] = acc;
+        __syncthreads();
+        if (valid) {
+            const uint32_t pos = woff[warp][d] + (uint32_t)rank;
+            keys_out[pos] = key;
+            vals_out[pos] = val;
+        }
+        __syncthreads();
+    }
+}
+
+// Warp segmented reduction of the sorted records.  A segment (one cell) wholly inside a
+// warp is written to its cell; pieces of segments crossing warp boundaries are left for
+// `seg_reduce_chains`: `first` is a warp's leading piece of a segment begun earlier
+// (`tail` set when that segment ends in the warp), `last` its trailing piece of a segment
+// that begins in the warp and continues (`owner` set).
+__global__ void seg_reduce_warps(const uint32_t *__restrict__ K, const uint32_t *__restrict__ I,
+                                 const double *__restrict__ U, const double *__restrict__ W,
+                                 const double *__restrict__ Q, i64 R, uint32_t sentinel,
+                                 double4 *__restrict__ cells, double4 *__restrict__ first,
+                                 double4 *__restrict__ last, uint8_t *__restrict__ tail_flag,
+                                 uint8_t *__restrict__ owner_flag) {
+    const i64 gw = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw * 32 >= R) return;  // whole warps only
+    const i64 r = gw * 32 + lane;
+    const uint32_t key = r < R ? K[r] : sentinel;
+    const bool valid = key < sentinel;
+    double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
+    if (valid) {
+        const uint32_t idx = I[r];
+        const double u = U[idx], w = W[idx], q = Q[idx];
+        c00 = (1.0 - u) * (1.0 - w) * q;
+        c01 = (1.0 - u) * w * q;
+        c10 = u * (1.0 - w) * q;
+        c11 = u * w * q;
+    }
+    const uint32_t prev = (r > 0 && r - 1 < R) ? K[r - 1] : 0xffffffffu;
+    const uint32_t next = (r + 1 < R) ? K[r + 1] : 0xffffffffu;
+    const bool head = valid && (r == 0 || prev != key);
+    const bool tail = valid && (r + 1 >= R || next != key);
+    bool f = head;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double y0 = __shfl_up_sync(kFull, c00, off);
+        const double y1 = __shfl_up_sync(kFull, c01, off);
+        const double y2 = __shfl_up_sync(kFull, c10, off);
+        const double y3 = __shfl_up_sync(kFull, c11, off);
+        const bool g = __shfl_up_sync(kFull, f, off);
+        if (lane >= off) {
+            if (!f) {
+                c00 = y0 + c00;
+                c01 = y1 + c01;
+                c10 = y2 + c10;
+                c11 = y3 + c11;
+            }
+            f = f || g;
+        }
+    }
+    const double4 sum = make_double4(c00, c01, c10, c11);
+    if (tail) {
+        if (f) {
+            cells[key] = sum;
+        } else {
+            first[gw] = sum;
+            tail_flag[gw] = 1;
+        }
+    }
+    if (lane == 31) {
+        const bool open = valid && !tail;
+        owner_flag[gw] = (open && f) ? 1 : 0;
+        if (open && f) last[gw] = sum;
+        if (open && !f) {
+            first[gw] = sum;
+            tail_flag[gw] = 0;
+        }
+    }
+}
+
+// The segments that cross warps: the owning warp's trailing piece plus the following
+// warps' leading pieces, added in warp order until the segment ends.
+__global__ void seg_reduce_chains(const uint32_t *__restrict__ K, i64 n_warps,
+                                  double4 *__restrict__ cells, const double4 *__restrict__ first,
+                                  const double4 *__restrict__ last,
+                                  const uint8_t *__restrict__ tail_flag,
+                                  const uint8_t *__restrict__ owner_flag) {
+    const i64 gw = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gw >= n_warps || !owner_flag[gw]) return;
+    double4 s = last[gw];
+    for (i64 w = gw + 1; w < n_warps; ++w) {
+        const double4 p = first[w];
+        s.x = s.x + p.x;
+        s.y = s.y + p.y;
+        s.z = s.z + p.z;
+        s.w = s.w + p.w;
+        if (tail_flag[w]) break;
+    }
+    cells[K[gw * 32 + 31]] = s;
+}
+
+// charge[node] += the four cells around it, in the fixed order (i, j), (i, j-1), (i-1, j),
+// (i-1, j-1): the corners (0,0), (0,1), (1,0), (1,1) of those cells.
+__global__ void node_accumulate(const double4 *__restrict__ cells, double *__restrict__ charge,
+                                const i64 *__restrict__ patch_int, i64 n_patches, i64 nx0,
+                                i64 ny0, i64 n_nodes) {
+    const i64 node = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= n_nodes) return;
+    i64 ny = ny0, offset = 0;
+    if (patch_int) {
+        for (i64 p = 0; p < n_patches; ++p) {
+            const i64 off = patch_int[p * 6 + 5];
+            if (node >= off && node < off + patch_int[p * 6 + 4]) {
+                ny = patch_int[p * 6 + 1];
+                offset = off;
+                break;
+            }
+        }
+    }
+    (void)nx0;
+    const i64 local = node - offset;
+    const i64 i = local / ny, j = local - i * ny;
+    double s = cells[node].x;
+    if (j >= 1) s = s + cells[node - 1].y;
+    if (i >= 1) s = s + cells[node - ny].z;
+    if (i >= 1 && j >= 1) s = s + cells[node - ny - 1].w;
+    charge[node] += s;
+}
+
+// Records of point charges (deposit_trajectories_2d_pyccel.py:28-59).
+__global__ void point_records(const double *__restrict__ px, const double *__restrict__ py,
+                              const double *__restrict__ q, i64 n, double origin_x,
+                              double origin_y, double h, i64 cylindrical, i64 nx, i64 ny,
+                              uint32_t *__restrict__ keys, double *__restrict__ U,
+                              double *__restrict__ W, double *__restrict__ Q) {
+    const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double x = px[k], y = py[k];
+    i64 i = (i64)floor((x - origin_x) / h);
+    i64 j = (i64)floor((y - origin_y) / h);
+    double t = (x - (origin_x + h * (double)i)) / h;
+    double u;
+    if (cylindrical != 0) {
+        const double r1 = origin_y + h * (double)j;
+        const double r2 = r1 + h;
+        u = (y * y - r1 * r1) / (r2 * r2 - r1 * r1);
+    } else {
+        u = (y - (origin_y + h * (double)j)) / h;
+    }
+    if (i < 0) {
+        t = 0.0;
+        i = 0;
+    } else if (i >= nx - 1) {
+        t = 1.0;
+        i = nx - 2;
+    }
+    if (j < 0) {
+        u = 0.0;
+        j = 0;
+    } else if (j >= ny - 1) {
+        u = 1.0;
+        j = ny - 2;
+    }
+    keys[k] = (uint32_t)(i * ny + j);
+    U[k] = t;
+    W[k] = u;
+    Q[k] = q[k];
+}
+
+int bits_for(uint64_t max_key) {
+    int b = 0;
+    while (b < 32 && (max_key >> b) != 0) ++b;
+    return b;
+}
+
+}  // namespace
+
+void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, int key_bits,
+                      uint32_t **keys_out, uint32_t **vals_out) {
+    BT_REQUIRE(n < (i64)0xffffffffLL, "radix sort: too many records for 32-bit indices");
+    DepositScratch &s = ctx->deposit;
+    cudaStream_t st = ctx->stream;
+    const int nblocks = (int)((n + kTile - 1) / kTile);
+    uint32_t *ka = s.keys_alt.as<uint32_t>(n), *va = s.vals.as<uint32_t>(n);
+    uint32_t *kb = s.keys.as<uint32_t>(n), *vb = s.vals_alt.as<uint32_t>(n);
+    uint32_t *hist = s.hist.as<uint32_t>((size_t)kRadix * nblocks);
+    uint32_t *offs = s.row_offsets.as<uint32_t>((size_t)kRadix * nblocks);
+    uint32_t *digit = s.digit_base.as<uint32_t>(2 * kRadix);
+    uint32_t *totals = digit + kRadix;
+    const uint32_t *src_k = keys_in;
+    const uint32_t *src_v = nullptr;
+    uint32_t *dst_k = ka, *dst_v = va;
+    BT_REQUIRE(n > 0 && key_bits > 0, "radix sort: nothing to sort");
+    const int passes = (key_bits + 7) / 8;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        radix_hist<<<nblocks, kThreads, 0, st>>>(src_k, n, shift, hist, nblocks);
+        radix_row_scan<<<kRadix, kThreads, 0, st>>>(hist, offs, totals, nblocks);
+        radix_digit_base<<<1, kThreads, 0, st>>>(totals, digit);
+        radix_scatter<<<nblocks, kThreads, 0, st>>>(src_k, src_v, n, shift, offs, digit,
+                                                    nblocks, dst_k, dst_v);
+        BT_CHECK_LAUNCH();
+        src_k = dst_k;
+        src_v = dst_v;
+        if (dst_k == ka) {
+            dst_k = kb;
+            dst_v = vb;
+        } else {
+            dst_k = ka;
+            dst_v = va;
+        }
+    }
+    *keys_out = const_cast<uint32_t *>(src_k);
+    *vals_out = const_cast<uint32_t *>(src_v);
+}
+
+void deposit_records(bt_ctx *ctx, const uint32_t *keys, const double *u, const double *w,
+                     const double *q, i64 n_records, uint32_t sentinel, double *charge,
+                     const NodeLayout &layout) {
+    if (n_records == 0) return;
+    DepositScratch &s = ctx->deposit;
+    cudaStream_t st = ctx->stream;
+    uint32_t *sk = nullptr, *sv = nullptr;
+    radix_sort_pairs(ctx, keys, n_records, bits_for(sentinel), &sk, &sv);
+    const i64 n_warps = (n_records + 31) / 32;
+    double4 *cells = s.cell_sums.as<double4>((size_t)layout.n_nodes);
+    double4 *first = s.warp_first.as<double4>((size_t)n_warps);
+    double4 *last = s.warp_last.as<double4>((size_t)n_warps);
+    uint8_t *flags = s.warp_flags.as<uint8_t>((size_t)2 * n_warps);
+    BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * layout.n_nodes, st));
+    const int threads = 256;
+    seg_reduce_warps<<<blocks_for(n_warps * 32, threads), threads, 0, st>>>(
+        sk, sv, u, w, q, n_records, sentinel, cells, first, last, flags, flags + n_warps);
+    seg_reduce_chains<<<blocks_for(n_warps, threads), threads, 0, st>>>(
+        sk, n_warps, cells, first, last, flags, flags + n_warps);
+    node_accumulate<<<blocks_for(layout.n_nodes, threads), threads, 0, st>>>(
+        cells, charge, layout.patch_int, layout.n_patches, layout.nx, layout.ny,
+        layout.n_nodes);
+    BT_CHECK_LAUNCH();
+}
+
+}  // namespace bt
+
+extern "C" int bt_deposit_trajectories_2d(bt_ctx *ctx, const double *px, const double *py,
+                                          const double *q, int64_t n, double origin_x,
+                                          double origin_y, double h, int64_t cylindrical,
+                                          double *charge, int64_t nx, int64_t ny) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx, "deposit: null context");
+        BT_REQUIRE(n >= 0, "deposit: negative point count");
+        BT_REQUIRE(nx >= 2 && ny >= 2, "deposit: the mesh needs at least 2 x 2 nodes");
+        BT_REQUIRE(nx * ny < (int64_t)0xffffffffLL, "deposit: mesh too large for 32-bit keys");
+        if (n == 0) return;
+        BT_REQUIRE(px && py && q && charge, "deposit: null array");
+        bt::DepositScratch &s = ctx->deposit;
+        uint32_t *keys = s.keys.as<uint32_t>(n);
+        double *U = s.u.as<double>(n), *W = s.w.as<double>(n), *Q = s.q.as<double>(n);
+        bt::point_records<<<bt::blocks_for(n, 256), 256, 0, ctx->stream>>>(
+            px, py, q, n, origin_x, origin_y, h, cylindrical, nx, ny, keys, U, W, Q);
+        BT_CHECK_LAUNCH();
+        // the records' keys live in `keys`; the sort reads them and writes elsewhere
+        bt::NodeLayout layout{nullptr, 1, nx, ny, nx * ny};
+        bt::deposit_records(ctx, keys, U, W, Q, n, (uint32_t)(nx * ny), charge, layout);
+    });
+}

@@ -1,0 +1,574 @@
+// The trajectory tracer: kernels/trace_trajectories_2d/trace_trajectories_2d_pyccel.py:42-507
+// re-designed for the B200.
+//
+// One thread per live trajectory advances it by at most `window` steps per launch (RK4 or
+// Boris's kick-drift-kick through the staggered edge fields of the patches, plane
+// crossings, kept paths, exit and electrode sub-cell tests: the reference's step, term by
+// term, in FP64 with no fused multiply-add, so a trajectory ends bit for bit where the
+// reference's CPU kernel ends it).  Instead of adding its charge to the mesh with atomics,
+// every step writes one deposit record (cell, u, w, dq dt) to a slot fixed by (window,
+// step, trajectory); between windows the live trajectories are compacted in order, and the
+// records are sorted by cell and reduced per cell in record order (deposit.cu), so the
+// node charges are deterministic.  Short windows bound the tail of a warp (its threads
+// wait only for the longest trajectory of the window, not of the whole trace).
+#include "common.cuh"
+
+namespace bt {
+
+namespace {
+
+struct Trace {
+    bt_trace_args a;
+    i64 nx, ny;  // the last patch's node counts
+};
+
+__device__ __forceinline__ i64 node_cell(double x, const double *__restrict__ nodes, i64 n) {
+    i64 lo = 0, hi = n - 1;
+    if (x >= nodes[n - 1]) {
+        lo = n - 2;
+    } else if (x > nodes[0]) {
+        while (hi - lo > 1) {
+            const i64 mid = (lo + hi) / 2;
+            if (nodes[mid] <= x)
+                lo = mid;
+            else
+                hi = mid;
+        }
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double uniform_x(double x, const double *__restrict__ nodes, i64 n,
+                                            double x0, double h) {
+    const i64 c = node_cell(x, nodes, n);
+    return x0 + h * ((double)c + (x - nodes[c]) / (nodes[c + 1] - nodes[c]));
+}
+
+__device__ __forceinline__ i64 finest_patch(const bt_trace_args &a, double px, double py) {
+    const i64 P = a.n_patches;
+    for (i64 qq = 0; qq < P - 1; ++qq) {
+        const double *pr = a.patch_real + qq * 7;
+        if (px >= __ldg(pr + 3) && px <= __ldg(pr + 5) && py >= __ldg(pr + 4) &&
+            py <= __ldg(pr + 6))
+            return qq;
+    }
+    return P - 1;
+}
+
+// E at (lq, qy), the uniform x and the mesh y, from the finest patch holding the point
+// (trace_trajectories_2d_pyccel.py:212-269).
+__device__ __forceinline__ void edge_field(const bt_trace_args &a, double lq, double qy,
+                                           double &ex, double &ey) {
+    const i64 pp = finest_patch(a, lq, qy);
+    const i64 *pi = a.patch_int + pp * 6;
+    const double *pr = a.patch_real + pp * 7;
+    const i64 pnx = __ldg(pi + 0), pny = __ldg(pi + 1), ofx = __ldg(pi + 2), ofy = __ldg(pi + 3);
+    const double pox = __ldg(pr + 0), poy = __ldg(pr + 1), phh = __ldg(pr + 2);
+    const double sx = (lq - pox) / phh;
+    const double sy = (qy - poy) / phh;
+    double s = sx + 0.5;
+    i64 i = (i64)floor(s);
+    if (i < 0)
+        i = 0;
+    else if (i > pnx - 1)
+        i = pnx - 1;
+    i64 j = (i64)floor(sy);
+    if (j < 0)
+        j = 0;
+    else if (j > pny - 2)
+        j = pny - 2;
+    double u = s - (double)i;
+    double w = sy - (double)j;
+    const double *fx = a.fxs + ofx + i * pny + j;
+    double f00 = __ldg(fx), f01 = __ldg(fx + 1), f10 = __ldg(fx + pny), f11 = __ldg(fx + pny + 1);
+    double low = f00 + w * (f01 - f00);
+    double high = f10 + w * (f11 - f10);
+    ex = low + u * (high - low);
+    s = sy + 0.5;
+    i = (i64)floor(sx);
+    if (i < 0)
+        i = 0;
+    else if (i > pnx - 2)
+        i = pnx - 2;
+    j = (i64)floor(s);
+    if (j < 0)
+        j = 0;
+    else if (j > pny - 1)
+        j = pny - 1;
+    u = sx - (double)i;
+    w = s - (double)j;
+    const double *fy = a.fys + ofy + i * (pny + 1) + j;
+    f00 = __ldg(fy);
+    f01 = __ldg(fy + 1);
+    f10 = __ldg(fy + pny + 1);
+    f11 = __ldg(fy + pny + 2);
+    low = f00 + w * (f01 - f00);
+    high = f10 + w * (f11 - f10);
+    ey = low + u * (high - low);
+}
+
+__global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restrict__ act,
+                                                   i64 n_act, int S,
+                                                   uint32_t *__restrict__ keys,
+                                                   double *__restrict__ RU,
+                                                   double *__restrict__ RW,
+                                                   double *__restrict__ RQ, uint32_t sentinel) {
+    const i64 m = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_act) return;
+    const bt_trace_args &a = tr.a;
+    const i64 k = act[m];
+    const i64 P = a.n_patches;
+    const i64 nx = tr.nx, ny = tr.ny;
+    const double origin_x = a.origin_x, origin_y = a.origin_y, h = a.h;
+    const i64 cyl = a.cylindrical;
+    const double inv_c2 = a.inv_c2;
+    const i64 n = a.n;
+    const bool graded = a.graded != 0;
+    double x0 = a.x[k], x1 = a.x[n + k], x2 = a.x[2 * n + k];
+    double v0 = a.v[k], v1 = a.v[n + k], v2 = a.v[2 * n + k];
+    const double qmk = a.qm[k];
+    const double dqk = a.dq[k];
+    const i64 slot = a.path_slot[k];
+    i64 ns = a.steps[k];
+    i64 st = -1;
+    const int nstage = a.integrator == 0 ? 4 : 2;
+    int have = 0;
+    double ca0 = 0.0, ca1 = 0.0, ca2 = 0.0;
+    int s = 0;
+    for (; s < S; ++s) {
+        if (ns >= a.max_steps) break;
+        double rr = x1;
+        if (cyl == 1)
+            rr = radius(x1, x2);
+        else if (cyl == 2)
+            rr = origin_y + fabs(x1 - origin_y);
+        double lx = x0;
+        if (graded) lx = uniform_x(x0, a.x_nodes, a.n_x_nodes, origin_x, h);
+        double hloc = h;
+        for (i64 qq = 0; qq < P - 1; ++qq) {
+            const double *pr = a.patch_real + qq * 7;
+            if (lx >= __ldg(pr + 3) && lx <= __ldg(pr + 5) && rr >= __ldg(pr + 4) &&
+                rr <= __ldg(pr + 6)) {
+                hloc = __ldg(pr + 2);
+                break;
+            }
+        }
+        if (graded) {
+            const i64 cg = node_cell(x0, a.x_nodes, a.n_x_nodes);
+            const double d2 = (a.x_nodes[cg + 1] - a.x_nodes[cg]) / h;
+            if (d2 < 1.0) hloc = hloc * d2;
+        }
+        const double gv = 1.0 / lorentz(v0, v1, v2, inv_c2);
+        double q0 = x0, q1 = x1, q2 = x2;
+        double kx0 = v0, kx1 = v1, kx2 = v2;
+        double sx0 = 0, sx1 = 0, sx2 = 0, sv0 = 0, sv1 = 0, sv2 = 0;
+        double w0 = 0, w1 = 0, w2 = 0, y0, y1, y2;
+        double dt = 0.0, hdt = 0.0, dt6 = 0.0;
+        for (int stage = 0; stage < nstage; ++stage) {
+            double gk = 1.0 / lorentz(kx0, kx1, kx2, inv_c2);
+            double g0, g1, g2;
+            if (stage == 0 && have != 0) {
+                g0 = ca0;
+                g1 = ca1;
+                g2 = ca2;
+            } else {
+                double qy = q1, cy = 0.0, cz = 0.0;
+                if (cyl == 1) {
+                    const double r = radius(q1, q2);
+                    if (r > 0.0) {
+                        cy = q1 / r;
+                        cz = q2 / r;
+                    }
+                    qy = r;
+                } else if (cyl == 2) {
+                    cy = 1.0;
+                    if (q1 < origin_y) cy = -1.0;
+                    qy = origin_y + fabs(q1 - origin_y);
+                }
+                double lq = q0;
+                if (graded) lq = uniform_x(q0, a.x_nodes, a.n_x_nodes, origin_x, h);
+                double ex, ey;
+                edge_field(a, lq, qy, ex, ey);
+                if (cyl != 0) {
+                    g0 = qmk * ex;
+                    g1 = qmk * (ey * cy);
+                    g2 = qmk * (ey * cz);
+                } else {
+                    g0 = qmk * ex;
+                    g1 = qmk * ey;
+                    g2 = qmk * 0.0;
+                }
+            }
+            if (stage == 0) {
+                const double a0 = g0, a1 = g1, a2 = g2;
+                const double speed = gv * sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+                const double accel = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+                dt = -1.0;
+                if (speed > 0.0) dt = hloc / speed;
+                if (accel > 0.0) {
+                    const double d2 = sqrt(2.0 * hloc / accel);
+                    if (dt < 0.0 || d2 < dt) dt = d2;
+                }
+                if (dt < 0.0) dt = hloc;
+                dt = a.step_fraction * dt;
+                hdt = 0.5 * dt;
+                dt6 = dt / 6.0;
+                if (a.integrator != 0) {
+                    kx0 = v0 + hdt * a0;
+                    kx1 = v1 + hdt * a1;
+                    kx2 = v2 + hdt * a2;
+                    gk = 1.0 / lorentz(kx0, kx1, kx2, inv_c2);
+                    q0 = x0 + dt * gk * kx0;
+                    q1 = x1 + dt * gk * kx1;
+                    q2 = x2 + dt * gk * kx2;
+                    continue;
+                }
+                sx0 = gv * v0;
+                sx1 = gv * v1;
+                sx2 = gv * v2;
+                sv0 = a0;
+                sv1 = a1;
+                sv2 = a2;
+                q0 = x0 + hdt * gv * v0;
+                q1 = x1 + hdt * gv * v1;
+                q2 = x2 + hdt * gv * v2;
+                kx0 = v0 + hdt * a0;
+                kx1 = v1 + hdt * a1;
+                kx2 = v2 + hdt * a2;
+            } else if (a.integrator != 0) {
+                w0 = kx0 + hdt * g0;
+                w1 = kx1 + hdt * g1;
+                w2 = kx2 + hdt * g2;
+                ca0 = g0;
+                ca1 = g1;
+                ca2 = g2;
+                have = 1;
+            } else if (stage == 1 || stage == 2) {
+                sx0 = sx0 + 2.0 * gk * kx0;
+                sx1 = sx1 + 2.0 * gk * kx1;
+                sx2 = sx2 + 2.0 * gk * kx2;
+                sv0 = sv0 + 2.0 * g0;
+                sv1 = sv1 + 2.0 * g1;
+                sv2 = sv2 + 2.0 * g2;
+                const double f = stage == 1 ? hdt : dt;
+                q0 = x0 + f * gk * kx0;
+                q1 = x1 + f * gk * kx1;
+                q2 = x2 + f * gk * kx2;
+                kx0 = v0 + f * g0;
+                kx1 = v1 + f * g1;
+                kx2 = v2 + f * g2;
+            } else {
+                sx0 = sx0 + gk * kx0;
+                sx1 = sx1 + gk * kx1;
+                sx2 = sx2 + gk * kx2;
+                sv0 = sv0 + g0;
+                sv1 = sv1 + g1;
+                sv2 = sv2 + g2;
+            }
+        }
+        if (a.integrator == 0) {
+            y0 = x0 + dt6 * sx0;
+            y1 = x1 + dt6 * sx1;
+            y2 = x2 + dt6 * sx2;
+            w0 = v0 + dt6 * sv0;
+            w1 = v1 + dt6 * sv1;
+            w2 = v2 + dt6 * sv2;
+        } else {
+            y0 = q0;
+            y1 = q1;
+            y2 = q2;
+        }
+
+        // the deposit record of the step's Hermite midpoint (:372-423)
+        const double gw = 1.0 / lorentz(w0, w1, w2, inv_c2);
+        double m0 = 0.5 * (x0 + y0) + dt * (gv * v0 - gw * w0) / 8.0;
+        double m1 = 0.5 * (x1 + y1) + dt * (gv * v1 - gw * w1) / 8.0;
+        const double m2 = 0.5 * (x2 + y2) + dt * (gv * v2 - gw * w2) / 8.0;
+        if (cyl == 1)
+            m1 = radius(m1, m2);
+        else if (cyl == 2)
+            m1 = origin_y + fabs(m1 - origin_y);
+        if (graded) m0 = uniform_x(m0, a.x_nodes, a.n_x_nodes, origin_x, h);
+        {
+            const i64 pp = finest_patch(a, m0, m1);
+            const i64 *pi = a.patch_int + pp * 6;
+            const double *pr = a.patch_real + pp * 7;
+            const i64 pnx = __ldg(pi + 0), pny = __ldg(pi + 1), ofn = __ldg(pi + 5);
+            const double pox = __ldg(pr + 0), poy = __ldg(pr + 1), phh = __ldg(pr + 2);
+            i64 i = (i64)floor((m0 - pox) / phh);
+            i64 j = (i64)floor((m1 - poy) / phh);
+            double u = (m0 - (pox + phh * (double)i)) / phh;
+            double w;
+            if (cyl == 1) {
+                const double low = poy + phh * (double)j;
+                const double high = low + phh;
+                w = (m1 * m1 - low * low) / (high * high - low * low);
+            } else {
+                w = (m1 - (poy + phh * (double)j)) / phh;
+            }
+            if (i < 0) {
+                u = 0.0;
+                i = 0;
+            } else if (i >= pnx - 1) {
+                u = 1.0;
+                i = pnx - 2;
+            }
+            if (j < 0) {
+                w = 0.0;
+                j = 0;
+            } else if (j >= pny - 1) {
+                w = 1.0;
+                j = pny - 2;
+            }
+            const i64 r = (i64)s * n_act + m;
+            keys[r] = (uint32_t)(ofn + i * pny + j);
+            RU[r] = u;
+            RW[r] = w;
+            RQ[r] = dqk * dt;
+        }
+        ns = ns + 1;
+
+        for (i64 p = 0; p < a.n_planes; ++p) {
+            const double xp = a.planes[p];
+            const double before = x0 - xp;
+            const double after = y0 - xp;
+            if ((before < 0.0) != (after < 0.0)) {
+                const double sc = before / (before - after);
+                i64 *cnt = a.counts + k * a.n_planes + p;
+                const i64 c = *cnt;
+                if (c < a.capacity) {
+                    double *hit = a.hits + ((k * a.n_planes + p) * a.capacity + c) * 8;
+                    hit[0] = xp;
+                    hit[1] = x1 + sc * (y1 - x1);
+                    hit[2] = x2 + sc * (y2 - x2);
+                    hit[3] = gv * v0 + sc * (gw * w0 - gv * v0);
+                    hit[4] = gv * v1 + sc * (gw * w1 - gv * v1);
+                    hit[5] = gv * v2 + sc * (gw * w2 - gv * v2);
+                    hit[6] = after >= 0.0 ? 1.0 : -1.0;
+                    hit[7] = 1.0 * (double)ns;
+                }
+                *cnt = c + 1;
+            }
+        }
+        x0 = y0;
+        x1 = y1;
+        x2 = y2;
+        v0 = w0;
+        v1 = w1;
+        v2 = w2;
+
+        double px = x0, py = x1;
+        if (cyl == 1)
+            py = radius(x1, x2);
+        else if (cyl == 2)
+            py = origin_y + fabs(x1 - origin_y);
+        if (slot >= 0) {
+            const i64 c = a.path_count[slot];
+            if (c < a.path_capacity) {
+                a.paths[(slot * a.path_capacity + c) * 2 + 0] = px;
+                a.paths[(slot * a.path_capacity + c) * 2 + 1] = py;
+            }
+            a.path_count[slot] = c + 1;
+        }
+        if (graded) px = uniform_x(px, a.x_nodes, a.n_x_nodes, origin_x, h);
+        if (px >= a.upper_x) {
+            st = 0;
+        } else if (px < origin_x) {
+            st = 1;
+        } else if (py > a.upper_y || (cyl == 0 && py < origin_y)) {
+            st = 2;
+        } else {
+            i64 i = (i64)((px - origin_x) / h);
+            if (i > nx - 2) i = nx - 2;
+            i64 j = (i64)((py - origin_y) / h);
+            if (j > ny - 2) j = ny - 2;
+            // a point below the mesh (only a malformed geometry puts one there) takes
+            // its first cell, where the reference indexes outside the table
+            if (i < 0) i = 0;
+            if (j < 0) j = 0;
+            const i64 cell = __ldg(a.cells + i * (ny - 1) + j);
+            if (cell >= 0) {
+                const i64 R = a.refine;
+                i64 si = (i64)(((px - origin_x) / h - (double)i) * (double)R);
+                if (si < 0)
+                    si = 0;
+                else if (si > R - 1)
+                    si = R - 1;
+                i64 sj = (i64)(((py - origin_y) / h - (double)j) * (double)R);
+                if (sj < 0)
+                    sj = 0;
+                else if (sj > R - 1)
+                    sj = R - 1;
+                const i64 e = __ldg(a.subcells + (cell * R + si) * R + sj);
+                if (e >= 0) {
+                    st = 3;
+                    a.electrode[k] = e;
+                } else if (e == -2) {
+                    st = -2;
+                }
+            }
+        }
+        if (st != -1) {
+            ++s;
+            break;
+        }
+    }
+    // the slots of the steps not taken hold no record
+    for (; s < S; ++s) keys[(i64)s * n_act + m] = sentinel;
+    if (st == -1 && ns >= a.max_steps) st = 4;
+    a.x[k] = x0;
+    a.x[n + k] = x1;
+    a.x[2 * n + k] = x2;
+    a.v[k] = v0;
+    a.v[n + k] = v1;
+    a.v[2 * n + k] = v2;
+    a.steps[k] = ns;
+    a.status[k] = st;
+}
+
+// -- order-preserving compaction of the live trajectories ----------------------------------
+
+constexpr int kCompact = 1024;
+
+__global__ void count_alive(const i64 *__restrict__ act, i64 n, const i64 *__restrict__ status,
+                            uint32_t *__restrict__ block_counts) {
+    __shared__ uint32_t warp_counts[kCompact / 32];
+    const i64 m = (i64)blockIdx.x * kCompact + threadIdx.x;
+    const bool alive = m < n && status[act[m]] == -1;
+    const unsigned ballot = __ballot_sync(0xffffffffu, alive);
+    if ((threadIdx.x & 31) == 0) warp_counts[threadIdx.x >> 5] = __popc(ballot);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t total = 0;
+        for (int w = 0; w < kCompact / 32; ++w) total += warp_counts[w];
+        block_counts[blockIdx.x] = total;
+    }
+}
+
+// One block: exclusive prefix of the block counts (in place) and the total.
+__global__ void scan_counts(uint32_t *__restrict__ block_counts, int nblocks,
+                            i64 *__restrict__ total) {
+    if (threadIdx.x != 0) return;
+    uint32_t run = 0;
+    for (int b = 0; b < nblocks; ++b) {
+        const uint32_t c = block_counts[b];
+        block_counts[b] = run;
+        run += c;
+    }
+    *total = run;
+}
+
+__global__ void scatter_alive(const i64 *__restrict__ act, i64 n, const i64 *__restrict__ status,
+                              const uint32_t *__restrict__ block_offsets, i64 *__restrict__ out) {
+    __shared__ uint32_t warp_counts[kCompact / 32];
+    const i64 m = (i64)blockIdx.x * kCompact + threadIdx.x;
+    const bool alive = m < n && status[act[m]] == -1;
+    const unsigned ballot = __ballot_sync(0xffffffffu, alive);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) warp_counts[warp] = __popc(ballot);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < kCompact / 32; ++w) {
+            const uint32_t c = warp_counts[w];
+            warp_counts[w] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    if (alive) {
+        const uint32_t rank = warp_counts[warp] + __popc(ballot & ((1u << lane) - 1u));
+        out[block_offsets[blockIdx.x] + rank] = act[m];
+    }
+}
+
+}  // namespace
+
+}  // namespace bt
+
+extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, int64_t window) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx && args, "trace: null argument");
+        const bt_trace_args &a = *args;
+        BT_REQUIRE(a.n_patches >= 1 && a.patch_int && a.patch_real, "trace: no patches");
+        BT_REQUIRE(a.n_active >= 0 && a.n >= 0, "trace: negative sizes");
+        BT_REQUIRE(a.capacity >= 0 && a.path_capacity >= 0 && a.n_planes >= 0,
+                   "trace: negative buffer sizes");
+        BT_REQUIRE(a.refine >= 1, "trace: refine must be positive");
+        BT_REQUIRE(!a.graded || a.n_x_nodes >= 2, "trace: a graded axis needs its nodes");
+        BT_REQUIRE(a.n_nodes < (int64_t)0xffffffffLL, "trace: too many nodes for 32-bit keys");
+        bt::Trace tr;
+        tr.a = a;
+        // the last patch's shape, for the exit and electrode tests
+        int64_t last[6];
+        BT_CUDA(cudaMemcpyAsync(last, a.patch_int + (a.n_patches - 1) * 6, sizeof(last),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+        BT_CUDA(cudaStreamSynchronize(ctx->stream));
+        tr.nx = last[0];
+        tr.ny = last[1];
+        BT_REQUIRE(tr.nx >= 2 && tr.ny >= 2, "trace: the mesh needs at least 2 x 2 nodes");
+        const int S = window > 0 ? (int)window : 64;
+        ctx->last_windows = ctx->last_records = ctx->last_flushes = 0;
+        if (a.n_active == 0) return;
+        bt::TraceScratch &ts = ctx->trace;
+        cudaStream_t st = ctx->stream;
+        const uint32_t sentinel = (uint32_t)a.n_nodes;
+        // the record buffer: flushed (sorted and reduced into charge[0]) when the next
+        // window would not fit
+        const int64_t per_window = a.n_active * (int64_t)S;
+        int64_t capacity = (int64_t)1 << 25;
+        if (capacity < per_window) capacity = per_window;
+        uint32_t *keys = ts.rec_keys.as<uint32_t>(capacity);
+        double *RU = ts.rec_u.as<double>(capacity);
+        double *RW = ts.rec_w.as<double>(capacity);
+        double *RQ = ts.rec_q.as<double>(capacity);
+        int64_t *act_a = ts.active_a.as<int64_t>(a.n_active);
+        int64_t *act_b = ts.active_b.as<int64_t>(a.n_active);
+        const int nb_max = (int)bt::blocks_for(a.n_active, bt::kCompact);
+        uint32_t *block_counts = ts.block_counts.as<uint32_t>(nb_max);
+        int64_t *n_alive_dev = ts.n_alive.as<int64_t>(1);
+        int64_t *n_alive_host = static_cast<int64_t *>(ctx->host.get(sizeof(int64_t)));
+        BT_CUDA(cudaMemcpyAsync(act_a, a.active, sizeof(int64_t) * a.n_active,
+                                cudaMemcpyDeviceToDevice, st));
+        bt::NodeLayout layout{a.patch_int, a.n_patches, tr.nx, tr.ny, a.n_nodes};
+        int64_t n_act = a.n_active, used = 0;
+        auto flush = [&] {
+            if (used == 0) return;
+            bt::deposit_records(ctx, keys, RU, RW, RQ, used, sentinel, a.charge, layout);
+            ctx->last_records += used;
+            ctx->last_flushes += 1;
+            used = 0;
+        };
+        while (n_act > 0) {
+            const int64_t need = n_act * (int64_t)S;
+            if (used + need > capacity) flush();
+            bt::trace_window<<<bt::blocks_for(n_act, 128), 128, 0, st>>>(
+                tr, act_a, n_act, S, keys + used, RU + used, RW + used, RQ + used, sentinel);
+            BT_CHECK_LAUNCH();
+            used += need;
+            ctx->last_windows += 1;
+            const int nb = (int)bt::blocks_for(n_act, bt::kCompact);
+            bt::count_alive<<<nb, bt::kCompact, 0, st>>>(act_a, n_act, a.status, block_counts);
+            bt::scan_counts<<<1, 32, 0, st>>>(block_counts, nb, n_alive_dev);
+            bt::scatter_alive<<<nb, bt::kCompact, 0, st>>>(act_a, n_act, a.status, block_counts,
+                                                           act_b);
+            BT_CHECK_LAUNCH();
+            BT_CUDA(cudaMemcpyAsync(n_alive_host, n_alive_dev, sizeof(int64_t),
+                                    cudaMemcpyDeviceToHost, st));
+            BT_CUDA(cudaStreamSynchronize(st));
+            n_act = *n_alive_host;
+            std::swap(act_a, act_b);
+        }
+        flush();
+    });
+}
+
+extern "C" int bt_trace_last_stats(bt_ctx *ctx, int64_t *windows, int64_t *records,
+                                   int64_t *deposit_flushes) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx, "trace stats: null context");
+        if (windows) *windows = ctx->last_windows;
+        if (records) *records = ctx->last_records;
+        if (deposit_flushes) *deposit_flushes = ctx->last_flushes;
+    });
+}

@@ -1,0 +1,136 @@
+/*
+ * beamtracer-b200: the C ABI of the B200 (sm_100a) Vlasov-iteration path.
+ *
+ * Every entry point returns 0 on success or a negative BT_ERR_* code; bt_last_error()
+ * gives the message of the calling thread's last failure.  Array arguments are plain
+ * pointers: DEVICE pointers for the kernel-level entry points (the cunumpy kernel
+ * interface of the reference, which runs its CUDA kernels on CuPy device arrays) and the
+ * solver entry points that say so, HOST pointers where an entry point says "host".
+ * Layouts are C order, the reference's: a (3, n) array is three rows of n values, an
+ * (nx, ny) mesh array has y contiguous.  Integers are int64 where the reference passes
+ * "int[:]" arrays (long long in its CUDA kernels).
+ *
+ * Work is queued on the context's CUDA stream; an entry point that must read a result
+ * back (a count, a norm) synchronises that stream.  One context per host thread.
+ */
+#ifndef BT200_H
+#define BT200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BT_OK 0
+#define BT_ERR_ARG (-1)      /* an argument is invalid (null, negative size, bad shape) */
+#define BT_ERR_CUDA (-2)     /* a CUDA call failed */
+#define BT_ERR_CAPACITY (-3) /* an output buffer is too small; see bt_last_error */
+#define BT_ERR_NOCONV (-4)   /* an iterative solve did not converge */
+#define BT_ERR_TIMEOUT (-5)  /* a bounded device wait ran out */
+#define BT_ERR_ALLOC (-6)    /* device memory could not be allocated */
+
+typedef struct bt_ctx bt_ctx;
+
+/* -- context ------------------------------------------------------------------------- */
+
+/* A context on CUDA device `device` with its own non-blocking stream. */
+int bt_ctx_create(int device, bt_ctx **out);
+int bt_ctx_destroy(bt_ctx *ctx);
+/* Queue the context's work on `stream` (a cudaStream_t; NULL: the context's own). */
+int bt_ctx_set_stream(bt_ctx *ctx, void *stream);
+int bt_ctx_synchronize(bt_ctx *ctx);
+/* Copy the calling thread's last error message into buf (NUL-terminated); returns its length. */
+size_t bt_last_error(char *buf, size_t len);
+/* The library's version string. */
+const char *bt_version(void);
+
+/* -- the reference's kernel interface (device pointers) ------------------------------- */
+
+/* kernels/staggered_field_2d/staggered_field_2d_pyccel.py:13-55 (CUDA: *_cuda.cu:18-37).
+ * (E_x, E_y) at the n points (px, py): fx (nx + 1, ny) and fy (nx, ny + 1) interpolated
+ * bilinearly with the cell clamped to the arrays. */
+int bt_staggered_field_2d(bt_ctx *ctx, const double *px, const double *py, int64_t n,
+                          const double *fx, const double *fy, int64_t nx, int64_t ny,
+                          double origin_x, double origin_y, double h, double *ex,
+                          double *ey);
+
+/* kernels/deposit_trajectories_2d/deposit_trajectories_2d_pyccel.py:13-59 (CUDA:
+ * *_cuda.cu:8-55).  Adds the n charges q at (px, py) to charge (nx, ny), area-weighted
+ * (linear in r^2 radially when cylindrical != 0).  Deterministic: the contributions are
+ * sorted by cell and summed per cell by warp segmented reductions in a fixed order, so
+ * the result is the same bit for bit on every call.  Uses context-owned scratch. */
+int bt_deposit_trajectories_2d(bt_ctx *ctx, const double *px, const double *py,
+                               const double *q, int64_t n, double origin_x, double origin_y,
+                               double h, int64_t cylindrical, double *charge, int64_t nx,
+                               int64_t ny);
+
+/* The arguments of kernels/trace_trajectories_2d/trace_trajectories_2d_pyccel.py:42-78,
+ * all arrays on the device, with their shapes. */
+typedef struct bt_trace_args {
+    const int64_t *active; /* (n_active,) trajectory indices */
+    int64_t n_active;
+    double *x, *v; /* (3, n) positions, velocities (proper velocities if inv_c2 > 0) */
+    int64_t n;
+    const double *qm, *dq;                  /* (n,) charge/mass, signed current */
+    int64_t *steps, *status, *electrode;    /* (n,) */
+    const double *fxs, *fys;                /* the patches' edge fields, flattened */
+    const int64_t *patch_int;               /* (n_patches, 6) */
+    const double *patch_real;               /* (n_patches, 7) */
+    int64_t n_patches;
+    double origin_x, origin_y, h, upper_x, upper_y;
+    int64_t cylindrical; /* 0 planar, 1 cylindrical, 2 planar with a symmetry plane */
+    int64_t integrator;  /* 0 RK4, 1 Boris */
+    double step_fraction;
+    int64_t max_steps;
+    const int64_t *cells;    /* (nx - 1, ny - 1) of the last patch */
+    const int64_t *subcells; /* (cells, refine, refine) */
+    int64_t refine;
+    const double *planes; /* (n_planes,) */
+    int64_t n_planes;
+    double *hits; /* (n, n_planes, capacity, 8) */
+    int64_t capacity;
+    int64_t *counts;          /* (n, n_planes) */
+    const int64_t *path_slot; /* (n,) */
+    double *paths;            /* (slots, path_capacity, 2) */
+    int64_t path_capacity;
+    int64_t *path_count; /* (slots,) */
+    int64_t num_threads; /* the reference's host threads: ignored on the GPU */
+    double *charge;      /* (num_threads, n_nodes): the GPU adds into charge[0] */
+    int64_t n_nodes;
+    int64_t graded;
+    const double *x_nodes; /* (n_x_nodes,) */
+    int64_t n_x_nodes;
+    double inv_c2;
+} bt_trace_args;
+
+/* kernels/trace_trajectories_2d/trace_trajectories_2d_pyccel.py:42-507 (CUDA:
+ * *_cuda.cu:165-362).  Traces the active trajectories to their ends (status 0-4) or to a
+ * sub-cell cut by an electrode surface (status -2), depositing dq dt at every step's
+ * Hermite midpoint into charge[0] deterministically, recording plane crossings and kept
+ * paths.  The trajectories advance in windows of `window` steps (0: the default), one
+ * thread per trajectory; after each window the live ones are compacted and every
+ * window's deposit records are sorted by cell and reduced in a fixed order. */
+int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, int64_t window);
+
+/* Counters of the last bt_trace_trajectories_2d call on this context (host out-params). */
+int bt_trace_last_stats(bt_ctx *ctx, int64_t *windows, int64_t *records,
+                        int64_t *deposit_flushes);
+
+/* -- the edge field (device pointers) --------------------------------------------------- */
+
+/* solver/fields.py:18-67 and 116-152: the staggered edge fields of a potential.
+ * phi (nx, ny); solid (nx, ny) int32 electrode index or -1; near (nx, ny) uint8;
+ * distance (4, nx, ny) fractions of the edge towards -x, +x, -y, +y; dx (nx - 1,) the
+ * edge lengths along x (graded) or NULL for a uniform h; extrapolation[4] 0 =
+ * "extrapolate", 1 = "symmetric" for the faces x_min, x_max, y_min, y_max.
+ * Writes fx (nx + 1, ny) and fy (nx, ny + 1). */
+int bt_edge_field(bt_ctx *ctx, const double *phi, const int32_t *solid, const uint8_t *near,
+                  const double *distance, const double *dx, int64_t nx, int64_t ny,
+                  double h, const int32_t extrapolation[4], double *fx, double *fy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BT200_H */

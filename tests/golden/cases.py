@@ -1,0 +1,152 @@
+"""Seeded inputs of the kernel-level parity cases (shared by the fixture script and tests).
+
+The trace cases exercise every branch of ``trace_trajectories_2d``: the three geometries
+(planar, cylindrical, planar with a symmetry plane), both integrators (RK4, Boris), a
+refined patch, a graded x axis, relativistic proper velocities, plane crossings beyond the
+hit buffer, kept paths beyond their buffer, and electrode sub-cells that stop a trajectory
+(status 3) or pause it (status -2).  They are modelled on the case list of the reference's
+kernel tests (``tests/unit/test_compiled_tracer.py:253-347`` and
+``tests/unit/test_kernels.py:26-40``), drawn from this file's own generator.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+#: The scaled 1 / c^2 of the relativistic cases: c = 500 km/s, so trajectories at about
+#: 300 km/s have a Lorentz factor near 1.2.
+INV_C2 = 1.0 / 5.0e5**2
+
+#: Positions of the outputs in the trace kernel's argument list.
+TRACE_OUTPUTS = {
+    "x": 1, "v": 2, "steps": 5, "status": 6, "electrode": 7, "hits": 25,
+    "counts": 26, "paths": 28, "path_count": 29,
+}  # fmt: skip
+TRACE_CHARGE = 31
+TRACE_NAMES = (
+    "active x v qm dq steps status electrode fxs fys patch_int patch_real origin_x "
+    "origin_y h upper_x upper_y cylindrical integrator step_fraction max_steps cells "
+    "subcells refine planes hits counts path_slot paths path_count num_threads charge "
+    "graded x_nodes inv_c2"
+).split()
+
+
+def gather_case(seed: int, n: int = 257, nx: int = 9, ny: int = 7, h: float = 0.1):
+    """Edge fields and points inside, on and beyond a small mesh."""
+    rng = np.random.default_rng(seed)
+    fx = rng.normal(size=(nx + 1, ny))
+    fy = rng.normal(size=(nx, ny + 1))
+    origin = (rng.uniform(-0.05, 0.05), rng.uniform(-0.05, 0.05))
+    px = origin[0] + h * rng.uniform(-3.0, nx + 2.0, n)
+    py = origin[1] + h * rng.uniform(-3.0, ny + 2.0, n)
+    return [px, py, fx, fy, origin[0], origin[1], h, np.zeros(n), np.zeros(n)]
+
+
+def deposit_case(seed: int, cylindrical: int, n: int = 257, nx: int = 9, ny: int = 7):
+    """Charges at points inside and beyond a small mesh (radii >= 0 when cylindrical)."""
+    rng = np.random.default_rng(seed)
+    h = 0.1
+    origin = (rng.uniform(-0.05, 0.05), 0.0 if cylindrical else rng.uniform(-0.05, 0.05))
+    px = origin[0] + h * rng.uniform(-2.0, nx + 1.0, n)
+    low = 0.0 if cylindrical else -2.0
+    py = origin[1] + h * rng.uniform(low, ny + 1.0, n)
+    q = rng.normal(size=n)
+    return [px, py, q, origin[0], origin[1], h, cylindrical, np.zeros((nx, ny))]
+
+
+def trace_case(
+    cylindrical: int,
+    integrator: int,
+    refined: bool = False,
+    graded: bool = False,
+    relativistic: bool = False,
+    seed: int = 11,
+    n: int = 48,
+    max_steps: int = 500,
+) -> list:
+    """The 35 positional arguments of ``trace_trajectories_2d`` for one branch combination."""
+    rng = np.random.default_rng(seed + 100 * cylindrical + 10 * integrator)
+    nx, ny, h = 32, 13, 1.0e-3
+    patches = [(nx, ny, 0.0, 0.0, h)]
+    if refined:
+        # a box of half the spacing, finest first
+        patches.insert(0, (23, 15, 9.0e-3, 0.0, 0.5 * h))
+    fxs, fys, patch_int, patch_real = [], [], [], []
+    fx_off = fy_off = node_off = 0
+    for pnx, pny, ox, oy, ph in patches:
+        fxs.append((3.0e5 + 1.5e4 * rng.normal(size=(pnx + 1, pny))).ravel())
+        fys.append((1.5e4 * rng.normal(size=(pnx, pny + 1))).ravel())
+        patch_int.append((pnx, pny, fx_off, fy_off, pnx * pny, node_off))
+        patch_real.append(
+            (ox, oy, ph, ox, oy, ox + (pnx - 1) * ph, oy + (pny - 1) * ph)
+        )
+        fx_off += fxs[-1].size
+        fy_off += fys[-1].size
+        node_off += pnx * pny
+    if graded:
+        s = np.linspace(0.0, 1.0, nx)
+        x_nodes = (nx - 1) * h * (0.4 * s + 0.6 * s * s)
+    else:
+        x_nodes = np.zeros(2)
+    x = np.stack(
+        [rng.uniform(0.0, 4.0e-3, n), rng.uniform(0.2e-3, 10.0e-3, n), np.zeros(n)]
+    )
+    v = np.stack(
+        [
+            np.full(n, 3.0e5) + 2.0e4 * rng.normal(size=n),
+            3.0e4 * rng.normal(size=n),
+            3.0e4 * rng.normal(size=n) * (cylindrical == 1),
+        ]
+    )
+    if cylindrical == 2:
+        # near the symmetry plane and heading across it
+        x[1] *= 0.3
+        v[1] = -2.5 * np.abs(v[1])
+    x[:, 0] = (-1.0e-3, 1.0e-3, 0.0)  # one starts behind the mesh: backward at once
+    cells = np.full((nx - 1, ny - 1), -1, dtype=np.int64)
+    cells[21, 2:10] = np.arange(8)
+    cells[26, 3:9] = np.arange(8, 14)
+    refine = 8
+    subcells = rng.choice(
+        np.array([-2, -1, -1, -1, -1, -1, -1, 0, 1], dtype=np.int64), size=14 * refine**2
+    )
+    slot = np.full(n, -1, dtype=np.int64)
+    slot[::3] = np.arange(len(slot[::3]))
+    slots = int(slot.max()) + 1
+    threads = 3
+    return [
+        np.arange(n, dtype=np.int64), x, v, np.full(n, 9.58e7), rng.uniform(0.5, 1.5, n),
+        np.zeros(n, dtype=np.int64), np.full(n, -1, dtype=np.int64),
+        np.full(n, -1, dtype=np.int64), np.concatenate(fxs), np.concatenate(fys),
+        np.array(patch_int, dtype=np.int64), np.array(patch_real), 0.0, 0.0, h,
+        (nx - 1) * h, (ny - 1) * h, cylindrical, integrator, 0.5, max_steps, cells, subcells,
+        refine, np.array([6.0e-3, 17.5e-3]), np.zeros((n, 2, 3, 8)),
+        np.zeros((n, 2), dtype=np.int64), slot, np.zeros((slots, 40, 2)),
+        np.zeros(slots, dtype=np.int64), threads, np.zeros((threads, node_off)),
+        int(graded), x_nodes, INV_C2 if relativistic else 0.0,
+    ]  # fmt: skip
+
+
+def trace_case_names() -> list[tuple[str, tuple]]:
+    """Every branch combination, named ``trace_c{geometry}_i{integrator}_r_g_rel``."""
+    out = []
+    for cylindrical in (0, 1, 2):
+        for integrator in (0, 1):
+            for refined in (False, True):
+                for graded in (False, True):
+                    for relativistic in (False, True):
+                        name = (
+                            f"trace_c{cylindrical}_i{integrator}_r{int(refined)}"
+                            f"_g{int(graded)}_rel{int(relativistic)}"
+                        )
+                        out.append(
+                            (name, (cylindrical, integrator, refined, graded, relativistic))
+                        )
+    out.append(("trace_c0_i0_max_steps", (0, 0, False, False, False, 11, 48, 40)))
+    out.append(("trace_c1_i1_max_steps", (1, 1, True, False, False, 12, 48, 55)))
+    return out
+
+
+def copy_args(args: list) -> list:
+    """A deep copy of an argument list (arrays copied, scalars kept)."""
+    return [a.copy() if isinstance(a, np.ndarray) else a for a in args]

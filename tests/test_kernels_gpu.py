@@ -1,0 +1,136 @@
+"""The CUDA kernels against the oracle and the reference's golden outputs (on a B200).
+
+The gather and the tracer's per-trajectory outputs (positions, velocities, steps,
+statuses, electrodes, plane crossings, kept paths) must equal the oracle's bit for bit:
+both evaluate the reference's expressions in the same order in FP64 without fused
+multiply-adds.  The node charges are sums in a different order (sorted per cell on the
+GPU, trajectory by trajectory on the CPU), so they agree to rounding: 1e-12 of the
+largest node charge.  The GPU deposit is deterministic: repeated calls agree bit for bit.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import kernels as oracle
+from tests.golden.cases import TRACE_CHARGE, TRACE_OUTPUTS, copy_args, trace_case_names
+from tests.gpu_util import load_golden, to_device, to_host
+
+pytestmark = pytest.mark.gpu
+
+EXACT = ("steps", "status", "electrode", "counts", "path_count")
+
+
+@pytest.fixture(scope="module")
+def kernels():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("the GPU tests need a CUDA device")
+    from beamtracer_b200.kernels import KERNELS
+
+    return KERNELS
+
+
+@pytest.mark.parametrize("seed", [4, 5, 6])
+def test_gather_matches_the_oracle_bit_for_bit(kernels, seed):
+    args, golden = load_golden(f"gather_s{seed}_pyccel")
+    expected = copy_args(args)
+    oracle.staggered_field_2d(*expected)
+    device = to_device(args)
+    kernels["staggered_field_2d"](*device)
+    result = to_host(device)
+    for i in (7, 8):
+        np.testing.assert_array_equal(result[i], expected[i])
+        np.testing.assert_allclose(result[i], golden[i], rtol=1e-13, atol=1e-13)
+
+
+def test_gather_takes_host_arrays(kernels):
+    args, golden = load_golden("gather_s4_pyccel")
+    kernels["staggered_field_2d"](*args)
+    np.testing.assert_allclose(args[7], golden[7], rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.parametrize("seed", [4, 5, 6])
+@pytest.mark.parametrize("cylindrical", [0, 1])
+def test_deposit_matches_the_oracle(kernels, seed, cylindrical):
+    args, golden = load_golden(f"deposit_s{seed}_c{cylindrical}_pyccel")
+    expected = copy_args(args)
+    oracle.deposit_trajectories_2d(*expected)
+    device = to_device(args)
+    kernels["deposit_trajectories_2d"](*device)
+    result = to_host(device)
+    scale = np.abs(expected[7]).max()
+    np.testing.assert_allclose(result[7], expected[7], rtol=0, atol=1e-13 * scale)
+    np.testing.assert_allclose(result[7], golden[7], rtol=0, atol=1e-13 * scale)
+    assert result[7].sum() == pytest.approx(args[2].sum(), abs=1e-12)
+
+
+def test_deposit_is_deterministic_and_adds(kernels):
+    import torch
+
+    rng = np.random.default_rng(9)
+    n, nx, ny = 200_000, 64, 48
+    px = torch.from_numpy(rng.uniform(-0.1, 6.5, n)).cuda()
+    py = torch.from_numpy(rng.uniform(0.0, 4.9, n)).cuda()
+    # a hot cell: a quarter of the charges in one cell, so segments span many warps
+    px[: n // 4] = 3.05
+    py[: n // 4] = 2.05
+    q = torch.from_numpy(rng.normal(size=n)).cuda()
+    first = torch.full((nx, ny), 0.25, dtype=torch.float64, device="cuda")
+    second = first.clone()
+    kernels["deposit_trajectories_2d"](px, py, q, 0.0, 0.0, 0.1, 1, first)
+    kernels["deposit_trajectories_2d"](px, py, q, 0.0, 0.0, 0.1, 1, second)
+    assert torch.equal(first, second)
+    expected = np.full((nx, ny), 0.25)
+    oracle.deposit_trajectories_2d(
+        px.cpu().numpy(), py.cpu().numpy(), q.cpu().numpy(), 0.0, 0.0, 0.1, 1, expected
+    )
+    np.testing.assert_allclose(first.cpu().numpy(), expected, rtol=0,
+                               atol=1e-11 * np.abs(expected).max())  # fmt: skip
+
+
+@pytest.mark.parametrize("name", [name for name, _ in trace_case_names()])
+def test_trace_matches_the_oracle(kernels, name):
+    args, golden = load_golden(name)
+    expected = copy_args(args)
+    oracle.trace_trajectories_2d(*expected)
+    device = to_device(args)
+    device[TRACE_CHARGE] = device[TRACE_CHARGE][:1].clone()  # one slab on the GPU
+    kernels["trace_trajectories_2d"](*device, window=16)
+    result = to_host(device)
+    for key, i in TRACE_OUTPUTS.items():
+        np.testing.assert_array_equal(result[i], expected[i], err_msg=key)
+        if key in EXACT:
+            np.testing.assert_array_equal(result[i], golden[i], err_msg=key)
+        else:
+            np.testing.assert_allclose(result[i], golden[i], rtol=1e-12, atol=1e-12,
+                                       err_msg=key)  # fmt: skip
+    total = expected[TRACE_CHARGE].sum(0)
+    scale = np.abs(total).max()
+    np.testing.assert_allclose(result[TRACE_CHARGE][0], total, rtol=0, atol=1e-12 * scale)
+
+
+@pytest.mark.parametrize("window", [1, 5, 64, 1000])
+def test_trace_windows_agree(kernels, window):
+    import torch
+
+    args, _ = load_golden("trace_c1_i0_r1_g0_rel0")
+    runs = []
+    for _ in range(2):
+        device = to_device(args)
+        device[TRACE_CHARGE] = device[TRACE_CHARGE][:1].clone()
+        kernels["trace_trajectories_2d"](*device, window=window)
+        runs.append(to_host(device))
+    np.testing.assert_array_equal(runs[0][TRACE_CHARGE], runs[1][TRACE_CHARGE])
+    reference = to_device(args)
+    reference[TRACE_CHARGE] = reference[TRACE_CHARGE][:1].clone()
+    kernels["trace_trajectories_2d"](*reference, window=64)
+    reference = to_host(reference)
+    for key, i in TRACE_OUTPUTS.items():
+        np.testing.assert_array_equal(runs[0][i], reference[i], err_msg=key)
+    scale = np.abs(reference[TRACE_CHARGE]).max()
+    np.testing.assert_allclose(runs[0][TRACE_CHARGE], reference[TRACE_CHARGE], rtol=0,
+                               atol=1e-13 * scale)  # fmt: skip
+    del torch
