@@ -87,6 +87,13 @@ SIGNATURES: dict[str, list] = {
     "bt_trace_trajectories_2d": [P, ctypes.POINTER(TraceArgs), I64],
     "bt_trace_last_stats": [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64)],
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],
+    "bt_poisson_create": [P, ctypes.POINTER(MeshDesc), ctypes.POINTER(P)],
+    "bt_poisson_destroy": [P],
+    "bt_poisson_set_region": [P, P, F64],
+    "bt_poisson_solve": [
+        P, P, P, F64, F64, F64, I32, F64, F64, I32,
+        ctypes.POINTER(I32), ctypes.POINTER(I32),
+    ],  # fmt: skip
 }
 
 

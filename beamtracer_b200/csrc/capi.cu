@@ -36,6 +36,8 @@ void Buffer::release() {
 }
 
 void *HostBuffer::get(size_t need) {
+    // at least 64 KB, so that the small read-backs of one call never move the buffer
+    if (need < 65536) need = 65536;
     if (need <= bytes) return ptr;
     release();
     cudaError_t e = cudaMallocHost(&ptr, need);

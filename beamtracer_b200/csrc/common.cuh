@@ -42,9 +42,27 @@ struct Error {
 // -- device scratch ------------------------------------------------------------------------
 
 // A growable device buffer owned by a context (grown with cudaMalloc, never shrunk).
+// Move-only: a copy would free the same memory twice.
 struct Buffer {
     void *ptr = nullptr;
     size_t bytes = 0;
+    Buffer() = default;
+    Buffer(const Buffer &) = delete;
+    Buffer &operator=(const Buffer &) = delete;
+    Buffer(Buffer &&o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+        o.ptr = nullptr;
+        o.bytes = 0;
+    }
+    Buffer &operator=(Buffer &&o) noexcept {
+        if (this != &o) {
+            release();
+            ptr = o.ptr;
+            bytes = o.bytes;
+            o.ptr = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
     void *get(size_t need);
     template <class T>
     T *as(size_t count) {
@@ -58,6 +76,9 @@ struct Buffer {
 struct HostBuffer {
     void *ptr = nullptr;
     size_t bytes = 0;
+    HostBuffer() = default;
+    HostBuffer(const HostBuffer &) = delete;
+    HostBuffer &operator=(const HostBuffer &) = delete;
     void *get(size_t need);
     void release();
     ~HostBuffer() { release(); }

@@ -1,0 +1,995 @@
+// The field solve on the B200: the finite-volume operator of the reference's field
+// (patchwork's NodalPoisson as solver/poisson.py:1-24, 491-534 documents it), solved by
+// GMRES preconditioned with a geometric multigrid V-cycle, and Newton's method for the
+// Boltzmann plasma species (poisson.py:860-933).
+//
+// The operator, per free node, A phi = rho / eps0 + c (A = -laplacian, FD-scaled rows):
+// Shortley-Weller rows with the bracketed surface distances at nodes with four cells, the
+// cut edge's two-point flux at nodes on a face, (1 -/+ 1/2j) radial weights and 4 (phi_1 -
+// phi_0) on the axis, mirror images on Neumann faces; fixed nodes keep their values.
+//
+// Multigrid: vertex-centred coarsening (coarse node I at fine node 2I, the last coarse
+// node on the last fine node), bilinear prolongation P that is zero at fixed fine nodes,
+// Galerkin coarse operators A_1 = P^T W A_0 P (W the control volumes, which make W A_0
+// nearly symmetric) and A_{l+1} = P^T A_l P: 9-point stencils on every coarse level, built
+// on the device (and rebuilt for every Newton step's Jacobian).  Smoothing: red-black
+// Gauss-Seidel on the 5-point fine level, four-colour Gauss-Seidel on the 9-point levels;
+// the coarsest level (at most 64 nodes) is inverted by Gauss-Jordan in shared memory.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace bt {
+namespace {
+
+constexpr int kCoarsest = 64;
+constexpr double kEps0 = 8.8541878188e-12;  // scipy.constants.epsilon_0 (CODATA 2022)
+
+struct Axis {
+    i64 n = 0, nc = 0;
+    bool coarsened = false;
+    Buffer lo, w, cidx;  // per fine node: coarse index and its weight; per coarse: fine index
+};
+
+struct Level {
+    i64 nx = 0, ny = 0, n = 0;
+    Buffer c4;      // level 0: cw, ce, cs, cn (4 n)
+    Buffer diag;    // level 0: the diagonal (with the reaction)
+    Buffer base;    // level 0: the diagonal without the reaction
+    Buffer weight;  // level 0: the control volumes W
+    Buffer a9;      // coarse levels: 9 coefficients per node, (dI + 1) * 3 + (dJ + 1)
+    Buffer active;  // uint8: free (level 0) or a nonzero row (coarse)
+    Buffer x, b, r;
+    Axis ax, ay;  // the map to the next coarser level
+};
+
+__device__ __forceinline__ double pw(const int32_t *lo, const double *w, i64 k, i64 I) {
+    const i64 l = lo[k];
+    if (l == I) return w[k];
+    if (l + 1 == I) return 1.0 - w[k];
+    return 0.0;
+}
+
+// -- the fine operator (mirrors oracle/poisson.py:coefficients) ---------------------------
+
+__global__ void build_fine(i64 nx, i64 ny, const double *__restrict__ x, double h, int cyl,
+                           const uint8_t *__restrict__ fixed, const double *__restrict__ dist,
+                           double g0, double g1, double g2, double g3,
+                           double *__restrict__ c4, double *__restrict__ base,
+                           double *__restrict__ src, double *__restrict__ weight,
+                           uint8_t *__restrict__ active) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const i64 n = nx * ny;
+    if (t >= n) return;
+    const i64 i = t / ny, j = t - i * ny;
+    const double h_lo = i > 0 ? x[i] - x[i - 1] : 0.0;
+    const double h_hi = i < nx - 1 ? x[i + 1] - x[i] : 0.0;
+    const double ax = dist[t], bx = dist[n + t], ay = dist[2 * n + t], by = dist[3 * n + t];
+    const bool four = i > 0 && i < nx - 1 && j > 0 && j < ny - 1;
+    double cw = 0.0, ce = 0.0, cs = 0.0, cn = 0.0, s = 0.0;
+    // x
+    if (i > 0 && i < nx - 1) {
+        const double dm = ax * h_lo, dp = bx * h_hi;
+        if (four) {
+            cw = 2.0 / ((dm + dp) * dm);
+            ce = 2.0 / ((dm + dp) * dp);
+        } else {
+            const double L = 0.5 * (h_lo + h_hi);
+            cw = 1.0 / (L * dm);
+            ce = 1.0 / (L * dp);
+        }
+    } else if (i == 0) {
+        ce = 2.0 / (h_hi * (bx * h_hi));
+        s += 2.0 * g0 / h_hi;
+    } else {
+        cw = 2.0 / (h_lo * (ax * h_lo));
+        s += 2.0 * g1 / h_lo;
+    }
+    // y
+    const bool mid = j > 0 && j < ny - 1;
+    if (!cyl) {
+        const double dm = ay * h, dp = by * h;
+        if (mid) {
+            if (four) {
+                cs = 2.0 / ((dm + dp) * dm);
+                cn = 2.0 / ((dm + dp) * dp);
+            } else {
+                cs = 1.0 / (h * dm);
+                cn = 1.0 / (h * dp);
+            }
+        } else if (j == 0) {
+            cn = 2.0 / (h * dp);
+            s += 2.0 * g2 / h;
+        } else {
+            cs = 2.0 / (h * dm);
+            s += 2.0 * g3 / h;
+        }
+    } else {
+        const double jj = j > 1 ? (double)j : 1.0;
+        const double h2 = h * h;
+        if (mid) {
+            if (four) {
+                cs = (2.0 / ay - 1.0 / jj) / ((ay + by) * h2);
+                cn = (2.0 / by + 1.0 / jj) / ((ay + by) * h2);
+            } else {
+                cs = (1.0 - 0.5 / jj) / (ay * h2);
+                cn = (1.0 + 0.5 / jj) / (by * h2);
+            }
+        } else if (j == 0) {
+            cn = 4.0 / (by * h2);
+        } else {
+            cs = 2.0 / (ay * h2);
+            s += (1.0 + 0.5 / jj) * 2.0 * g3 / h;
+        }
+    }
+    const bool free = fixed[t] == 0;
+    c4[t] = free ? cw : 0.0;
+    c4[n + t] = free ? ce : 0.0;
+    c4[2 * n + t] = free ? cs : 0.0;
+    c4[3 * n + t] = free ? cn : 0.0;
+    base[t] = free ? cw + ce + cs + cn : 1.0;
+    src[t] = free ? s : 0.0;
+    active[t] = free ? 1 : 0;
+    // the control volume (divided by 2 pi in cylindrical geometry)
+    const double lx = 0.5 * (h_lo + h_hi);  // half an edge at an x face
+    double ly = (j > 0 && j < ny - 1) ? h : 0.5 * h;
+    if (cyl) ly = j == 0 ? 0.125 * h * h : (double)j * h * ly;
+    weight[t] = lx * ly;
+}
+
+__global__ void add_diag(i64 n, const double *__restrict__ base, const double *__restrict__ reaction,
+                         const uint8_t *__restrict__ active, double *__restrict__ diag) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    diag[t] = base[t] + ((reaction && active[t]) ? reaction[t] : 0.0);
+}
+
+// -- Galerkin coarse operator -----------------------------------------------------------
+
+struct Fine {
+    i64 nx, ny;
+    const double *c4, *diag, *a9, *weight;  // c4/diag for the 5-point level, a9 otherwise
+    const uint8_t *active;
+    const int32_t *lox, *loy;
+    const double *wx, *wy;
+    const int32_t *cix, *ciy;  // fine index of each coarse node
+    i64 ncx, ncy;
+};
+
+__device__ __forceinline__ double fine_coef(const Fine &F, i64 f, int di, int dj) {
+    if (F.a9) return F.a9[(i64)((di + 1) * 3 + (dj + 1)) * (F.nx * F.ny) + f];
+    const i64 n = F.nx * F.ny;
+    if (di == 0 && dj == 0) return F.diag[f];
+    if (di == -1 && dj == 0) return -F.c4[f];
+    if (di == 1 && dj == 0) return -F.c4[n + f];
+    if (di == 0 && dj == -1) return -F.c4[2 * n + f];
+    if (di == 0 && dj == 1) return -F.c4[3 * n + f];
+    return 0.0;
+}
+
+__global__ void galerkin(Fine F, double *__restrict__ a9c, uint8_t *__restrict__ active_c) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const i64 nc = F.ncx * F.ncy;
+    if (t >= nc) return;
+    const i64 I = t / F.ncy, J = t - I * F.ncy;
+    double acc[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) acc[q] = 0.0;
+    const i64 k0 = I > 0 ? F.cix[I - 1] : 0, k1 = I < F.ncx - 1 ? F.cix[I + 1] : F.nx - 1;
+    const i64 l0 = J > 0 ? F.ciy[J - 1] : 0, l1 = J < F.ncy - 1 ? F.ciy[J + 1] : F.ny - 1;
+    const int span = F.a9 ? 1 : 0;  // the 9-point fine stencil reaches diagonals
+    for (i64 k = k0; k <= k1; ++k) {
+        const double pk = pw(F.lox, F.wx, k, I);
+        if (pk == 0.0) continue;
+        for (i64 l = l0; l <= l1; ++l) {
+            const double pl = pw(F.loy, F.wy, l, J);
+            if (pl == 0.0) continue;
+            const i64 f = k * F.ny + l;
+            if (!F.active[f]) continue;
+            const double wgt = pk * pl * (F.weight ? F.weight[f] : 1.0);
+            for (int di = -1; di <= 1; ++di) {
+                const i64 k2 = k + di;
+                if (k2 < 0 || k2 >= F.nx) continue;
+                for (int dj = -1; dj <= 1; ++dj) {
+                    if (!span && di != 0 && dj != 0) continue;
+                    const i64 l2 = l + dj;
+                    if (l2 < 0 || l2 >= F.ny) continue;
+                    const i64 f2 = k2 * F.ny + l2;
+                    if (!F.active[f2]) continue;
+                    const double a = fine_coef(F, f, di, dj);
+                    if (a == 0.0) continue;
+                    const i64 ix = F.lox[k2], iy = F.loy[l2];
+                    const double wx = F.wx[k2], wy = F.wy[l2];
+                    for (int sx = 0; sx < 2; ++sx) {
+                        const double px = sx ? 1.0 - wx : wx;
+                        const i64 I2 = ix + sx;
+                        if (px == 0.0 || I2 - I < -1 || I2 - I > 1) continue;
+                        for (int sy = 0; sy < 2; ++sy) {
+                            const double py = sy ? 1.0 - wy : wy;
+                            const i64 J2 = iy + sy;
+                            if (py == 0.0 || J2 - J < -1 || J2 - J > 1) continue;
+                            acc[(I2 - I + 1) * 3 + (J2 - J + 1)] += wgt * a * px * py;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    const bool on = acc[4] != 0.0;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) a9c[(i64)q * nc + t] = on ? acc[q] : (q == 4 ? 1.0 : 0.0);
+    active_c[t] = on ? 1 : 0;
+}
+
+// -- smoothing, residual, transfer ---------------------------------------------------------
+
+__global__ void smooth5(i64 nx, i64 ny, const double *__restrict__ c4,
+                        const double *__restrict__ diag, const uint8_t *__restrict__ active,
+                        const double *__restrict__ b, double *__restrict__ x, int colour) {
+    const i64 n = nx * ny;
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    // thread t handles the t-th node of the colour
+    const i64 half = (ny + 1) / 2;
+    const i64 i = t / half;
+    if (i >= nx) return;
+    const i64 j = 2 * (t - i * half) + ((i + colour) & 1);
+    if (j >= ny) return;
+    const i64 f = i * ny + j;
+    if (!active[f]) return;
+    double s = b[f];
+    if (i > 0) s += c4[f] * x[f - ny];
+    if (i < nx - 1) s += c4[n + f] * x[f + ny];
+    if (j > 0) s += c4[2 * n + f] * x[f - 1];
+    if (j < ny - 1) s += c4[3 * n + f] * x[f + 1];
+    x[f] = s / diag[f];
+}
+
+__global__ void smooth9(i64 nx, i64 ny, const double *__restrict__ a9,
+                        const uint8_t *__restrict__ active, const double *__restrict__ b,
+                        double *__restrict__ x, int colour) {
+    const i64 n = nx * ny;
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const int ci = colour >> 1, cj = colour & 1;
+    const i64 hx = (nx - ci + 1) / 2, hy = (ny - cj + 1) / 2;
+    if (t >= hx * hy) return;
+    const i64 i = 2 * (t / hy) + ci, j = 2 * (t % hy) + cj;
+    const i64 f = i * ny + j;
+    if (!active[f]) return;
+    double s = b[f];
+#pragma unroll
+    for (int di = -1; di <= 1; ++di) {
+#pragma unroll
+        for (int dj = -1; dj <= 1; ++dj) {
+            if (di == 0 && dj == 0) continue;
+            const i64 i2 = i + di, j2 = j + dj;
+            if (i2 < 0 || i2 >= nx || j2 < 0 || j2 >= ny) continue;
+            s -= a9[(i64)((di + 1) * 3 + (dj + 1)) * n + f] * x[i2 * ny + j2];
+        }
+    }
+    x[f] = s / a9[4 * n + f];
+}
+
+// y = A x (level 0, 5-point) on active rows, 0 elsewhere; with b: r = b - A x.
+__global__ void apply5(i64 nx, i64 ny, const double *__restrict__ c4,
+                       const double *__restrict__ diag, const uint8_t *__restrict__ active,
+                       const double *__restrict__ x, const double *__restrict__ b,
+                       double *__restrict__ y) {
+    const i64 n = nx * ny;
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    if (!active[f]) {
+        y[f] = 0.0;
+        return;
+    }
+    const i64 i = f / ny, j = f - i * ny;
+    double s = diag[f] * x[f];
+    if (i > 0) s -= c4[f] * x[f - ny];
+    if (i < nx - 1) s -= c4[n + f] * x[f + ny];
+    if (j > 0) s -= c4[2 * n + f] * x[f - 1];
+    if (j < ny - 1) s -= c4[3 * n + f] * x[f + 1];
+    y[f] = b ? b[f] - s : s;
+}
+
+__global__ void residual9(i64 nx, i64 ny, const double *__restrict__ a9,
+                          const uint8_t *__restrict__ active, const double *__restrict__ x,
+                          const double *__restrict__ b, double *__restrict__ r) {
+    const i64 n = nx * ny;
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    if (!active[f]) {
+        r[f] = 0.0;
+        return;
+    }
+    const i64 i = f / ny, j = f - i * ny;
+    double s = b[f];
+    for (int di = -1; di <= 1; ++di)
+        for (int dj = -1; dj <= 1; ++dj) {
+            const i64 i2 = i + di, j2 = j + dj;
+            if (i2 < 0 || i2 >= nx || j2 < 0 || j2 >= ny) continue;
+            s -= a9[(i64)((di + 1) * 3 + (dj + 1)) * n + f] * x[i2 * ny + j2];
+        }
+    r[f] = s;
+}
+
+__global__ void restrict_residual(Fine F, const double *__restrict__ r, double *__restrict__ bc,
+                                  double *__restrict__ xc) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const i64 nc = F.ncx * F.ncy;
+    if (t >= nc) return;
+    const i64 I = t / F.ncy, J = t - I * F.ncy;
+    const i64 k0 = I > 0 ? F.cix[I - 1] : 0, k1 = I < F.ncx - 1 ? F.cix[I + 1] : F.nx - 1;
+    const i64 l0 = J > 0 ? F.ciy[J - 1] : 0, l1 = J < F.ncy - 1 ? F.ciy[J + 1] : F.ny - 1;
+    double s = 0.0;
+    for (i64 k = k0; k <= k1; ++k) {
+        const double pk = pw(F.lox, F.wx, k, I);
+        if (pk == 0.0) continue;
+        for (i64 l = l0; l <= l1; ++l) {
+            const double pl = pw(F.loy, F.wy, l, J);
+            if (pl == 0.0) continue;
+            const i64 f = k * F.ny + l;
+            if (!F.active[f]) continue;
+            s += pk * pl * (F.weight ? F.weight[f] : 1.0) * r[f];
+        }
+    }
+    bc[t] = s;
+    xc[t] = 0.0;
+}
+
+__global__ void prolong_add(Fine F, const double *__restrict__ xc, double *__restrict__ x) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F.nx * F.ny || !F.active[f]) return;
+    const i64 k = f / F.ny, l = f - k * F.ny;
+    const i64 ix = F.lox[k], iy = F.loy[l];
+    const double wx = F.wx[k], wy = F.wy[l];
+    double s = 0.0;
+    for (int sx = 0; sx < 2; ++sx) {
+        const double px = sx ? 1.0 - wx : wx;
+        if (px == 0.0 || ix + sx >= F.ncx) continue;
+        for (int sy = 0; sy < 2; ++sy) {
+            const double py = sy ? 1.0 - wy : wy;
+            if (py == 0.0 || iy + sy >= F.ncy) continue;
+            s += px * py * xc[(ix + sx) * F.ncy + iy + sy];
+        }
+    }
+    x[f] += s;
+}
+
+// The coarsest level: the dense matrix of its 9-point operator, inverted in place by
+// Gauss-Jordan with partial pivoting in shared memory.  `status` is set to 1 on a zero
+// pivot (a singular operator: no node of the mesh is held).
+__global__ void coarsest_invert(i64 nx, i64 ny, const double *__restrict__ a9,
+                                double *__restrict__ inv, int *__restrict__ status) {
+    __shared__ double M[kCoarsest][kCoarsest + 1];
+    __shared__ int perm[kCoarsest];
+    __shared__ int pivot_row;
+    const int n = (int)(nx * ny);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < n * n; e += nt) {
+        const int row = e / n, col = e % n;
+        const i64 i = row / ny, j = row % ny, i2 = col / ny, j2 = col % ny;
+        const i64 di = i2 - i, dj = j2 - j;
+        double v = 0.0;
+        if (di >= -1 && di <= 1 && dj >= -1 && dj <= 1)
+            v = a9[(i64)((di + 1) * 3 + (dj + 1)) * n + row];
+        M[row][col] = v;
+    }
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        if (tid == 0) {
+            int p = k;
+            double best = fabs(M[k][k]);
+            for (int r = k + 1; r < n; ++r) {
+                const double v = fabs(M[r][k]);
+                if (v > best) {
+                    best = v;
+                    p = r;
+                }
+            }
+            pivot_row = p;
+            perm[k] = p;
+            if (best == 0.0) *status = 1;
+        }
+        __syncthreads();
+        const int p = pivot_row;
+        if (p != k)
+            for (int c = tid; c < n; c += nt) {
+                const double t = M[k][c];
+                M[k][c] = M[p][c];
+                M[p][c] = t;
+            }
+        __syncthreads();
+        const double piv = M[k][k];
+        __syncthreads();
+        for (int c = tid; c < n; c += nt) M[k][c] = (c == k ? 1.0 : M[k][c]) / piv;
+        __syncthreads();
+        for (int e = tid; e < n * n; e += nt) {
+            const int r = e / n, c = e % n;
+            if (r == k) continue;
+            const double f = M[r][k];
+            if (c == k)
+                continue;
+            M[r][c] -= f * M[k][c];
+        }
+        __syncthreads();
+        for (int r = tid; r < n; r += nt)
+            if (r != k) M[r][k] = -M[r][k] * M[k][k];
+        __syncthreads();
+    }
+    for (int k = n - 1; k >= 0; --k) {
+        const int p = perm[k];
+        if (p != k)
+            for (int r = tid; r < n; r += nt) {
+                const double t = M[r][k];
+                M[r][k] = M[r][p];
+                M[r][p] = t;
+            }
+        __syncthreads();
+    }
+    for (int e = tid; e < n * n; e += nt) inv[e] = M[e / n][e % n];
+}
+
+__global__ void coarsest_apply(int n, const double *__restrict__ inv, const double *__restrict__ b,
+                               double *__restrict__ x) {
+    const int r = threadIdx.x;
+    if (r >= n) return;
+    double s = 0.0;
+    for (int c = 0; c < n; ++c) s += inv[r * n + c] * b[c];
+    x[r] = s;
+}
+
+// -- vector kernels of GMRES and Newton ----------------------------------------------------
+
+// out[q] = sum_f V[q * n + f] * w[f], q < m (one block per q, deterministic tree)
+__global__ void multi_dot(const double *__restrict__ V, const double *__restrict__ w, i64 n,
+                          double *__restrict__ out) {
+    __shared__ double part[256];
+    const int q = blockIdx.x;
+    const double *v = V + (i64)q * n;
+    double s = 0.0;
+    for (i64 f = threadIdx.x; f < n; f += blockDim.x) s += v[f] * w[f];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) part[threadIdx.x] += part[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[q] = part[0];
+}
+
+// w -= sum_q h[q] V[q]
+__global__ void orthogonalise(const double *__restrict__ V, const double *__restrict__ hcol, int m,
+                              i64 n, double *__restrict__ w) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    double s = w[f];
+    for (int q = 0; q < m; ++q) s -= hcol[q] * V[(i64)q * n + f];
+    w[f] = s;
+}
+
+__global__ void scale_into(const double *__restrict__ w, double a, i64 n, double *__restrict__ v) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < n) v[f] = a * w[f];
+}
+
+// x += sum_q y[q] Z[q]
+__global__ void combine(const double *__restrict__ Z, const double *__restrict__ y, int m, i64 n,
+                        double *__restrict__ x) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    double s = x[f];
+    for (int q = 0; q < m; ++q) s += y[q] * Z[(i64)q * n + f];
+    x[f] = s;
+}
+
+// max |v| over the array (one block, deterministic)
+__global__ void max_abs(const double *__restrict__ v, i64 n, double *__restrict__ out) {
+    __shared__ double part[256];
+    double s = 0.0;
+    for (i64 f = threadIdx.x; f < n; f += blockDim.x) s = fmax(s, fabs(v[f]));
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) part[threadIdx.x] = fmax(part[threadIdx.x], part[threadIdx.x + off]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = part[0];
+}
+
+// the right-hand side: rho / eps0 + c on free nodes, 0 on fixed ones; phi's fixed values set
+__global__ void prepare(i64 n, const double *__restrict__ rho, const double *__restrict__ src,
+                        const uint8_t *__restrict__ active, const double *__restrict__ value,
+                        double *__restrict__ b, double *__restrict__ phi) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    if (active[f]) {
+        b[f] = (rho ? rho[f] / kEps0 : 0.0) + src[f];
+    } else {
+        b[f] = 0.0;
+        phi[f] = value[f];
+    }
+}
+
+// The Boltzmann species at phi: e = a exp(min(-s (phi - up) / T, 50)); the Newton
+// residual r = b + s e - A phi (the negative of F) and the reaction e / T, on free nodes.
+__global__ void boltzmann(i64 nx, i64 ny, const double *__restrict__ c4,
+                          const double *__restrict__ base, const uint8_t *__restrict__ active,
+                          const double *__restrict__ phi, const double *__restrict__ b,
+                          double amplitude, double temperature, double up, double sign,
+                          double *__restrict__ r, double *__restrict__ reaction) {
+    const i64 n = nx * ny;
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    if (!active[f]) {
+        r[f] = 0.0;
+        reaction[f] = 0.0;
+        return;
+    }
+    const i64 i = f / ny, j = f - i * ny;
+    double s = base[f] * phi[f];
+    if (i > 0) s -= c4[f] * phi[f - ny];
+    if (i < nx - 1) s -= c4[n + f] * phi[f + ny];
+    if (j > 0) s -= c4[2 * n + f] * phi[f - 1];
+    if (j < ny - 1) s -= c4[3 * n + f] * phi[f + 1];
+    const double e = amplitude * exp(fmin(-sign * (phi[f] - up) / temperature, 50.0));
+    r[f] = b[f] + sign * e - s;
+    reaction[f] = e / temperature;
+}
+
+__global__ void add_into(const double *__restrict__ d, i64 n, double *__restrict__ x) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < n) x[f] += d[f];
+}
+
+// w = r - w
+__global__ void subtract_from(const double *__restrict__ r, i64 n, double *__restrict__ w) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < n) w[f] = r[f] - w[f];
+}
+
+void build_axis(Axis &A, i64 n) {
+    A.n = n;
+    A.coarsened = n > 3;
+    A.nc = A.coarsened ? n / 2 + 1 : n;
+    std::vector<int32_t> lo(n), cidx(A.nc);
+    std::vector<double> w(n);
+    for (i64 I = 0; I < A.nc; ++I) cidx[I] = (int32_t)(A.coarsened ? std::min<i64>(2 * I, n - 1) : I);
+    for (i64 k = 0; k < n; ++k) {
+        if (!A.coarsened) {
+            lo[k] = (int32_t)k;
+            w[k] = 1.0;
+            continue;
+        }
+        i64 I = std::min<i64>(k / 2, A.nc - 2);
+        const double c0 = cidx[I], c1 = cidx[I + 1];
+        lo[k] = (int32_t)I;
+        w[k] = (c1 - (double)k) / (c1 - c0);
+    }
+    cudaMemcpy(A.lo.as<int32_t>(n), lo.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice);
+    cudaMemcpy(A.w.as<double>(n), w.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(A.cidx.as<int32_t>(A.nc), cidx.data(), A.nc * sizeof(int32_t),
+               cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+}  // namespace bt
+
+struct bt_poisson {
+    bt_ctx *ctx = nullptr;
+    i64 nx = 0, ny = 0, n = 0;
+    double h = 0.0;
+    int cyl = 0;
+    double neumann[4] = {0, 0, 0, 0};
+    bt::Buffer x, fixed, value, distance, region;  // mesh; region: the extra held nodes
+    bt::Buffer fixed_eff, value_eff, src;
+    double region_value = 0.0;
+    bool has_region = false;
+    std::vector<bt::Level> levels;
+    bt::Buffer inv, status;
+    bool built = false;        // hierarchy matches the current diagonal
+    bool reaction_on = false;  // level-0 diagonal holds a reaction
+    int restart = 30;
+    // GMRES: the Krylov basis V, its preconditioned images Z, two work vectors, the
+    // Hessenberg column and the solution's coefficients; the solve: its right-hand side,
+    // the residual GMRES reduces, the correction, the Newton reaction and scalars.
+    bt::Buffer V, Z, work, work2, hcol, ycoef, rhs, r0, delta, reaction, scalars;
+};
+
+namespace bt {
+namespace {
+
+Fine fine_of(Level &L, Level &C, bool first) {
+    Fine F{};
+    F.nx = L.nx;
+    F.ny = L.ny;
+    if (first) {
+        F.c4 = L.c4.as<double>(4 * L.n);
+        F.diag = L.diag.as<double>(L.n);
+        F.a9 = nullptr;
+        F.weight = L.weight.as<double>(L.n);
+    } else {
+        F.c4 = nullptr;
+        F.diag = nullptr;
+        F.a9 = L.a9.as<double>(9 * L.n);
+        F.weight = nullptr;
+    }
+    F.active = L.active.as<uint8_t>(L.n);
+    F.lox = L.ax.lo.as<int32_t>(L.nx);
+    F.loy = L.ay.lo.as<int32_t>(L.ny);
+    F.wx = L.ax.w.as<double>(L.nx);
+    F.wy = L.ay.w.as<double>(L.ny);
+    F.cix = L.ax.cidx.as<int32_t>(L.ax.nc);
+    F.ciy = L.ay.cidx.as<int32_t>(L.ay.nc);
+    F.ncx = C.nx;
+    F.ncy = C.ny;
+    return F;
+}
+
+void build_operator(bt_poisson *p) {
+    cudaStream_t st = p->ctx->stream;
+    Level &L = p->levels[0];
+    const i64 n = p->n;
+    build_fine<<<blocks_for(n, 256), 256, 0, st>>>(
+        p->nx, p->ny, p->x.as<double>(p->nx), p->h, p->cyl, p->fixed_eff.as<uint8_t>(n),
+        p->distance.as<double>(4 * n), p->neumann[0], p->neumann[1], p->neumann[2],
+        p->neumann[3], L.c4.as<double>(4 * n), L.base.as<double>(n), p->src.as<double>(n),
+        L.weight.as<double>(n), L.active.as<uint8_t>(n));
+    BT_CHECK_LAUNCH();
+    p->built = false;
+    p->reaction_on = true;  // force the diagonal to be set
+}
+
+// Set the level-0 diagonal (with `reaction`, or without) and rebuild the coarse levels.
+void build_hierarchy(bt_poisson *p, const double *reaction) {
+    cudaStream_t st = p->ctx->stream;
+    Level &L0 = p->levels[0];
+    add_diag<<<blocks_for(p->n, 256), 256, 0, st>>>(p->n, L0.base.as<double>(p->n), reaction,
+                                                    L0.active.as<uint8_t>(p->n),
+                                                    L0.diag.as<double>(p->n));
+    for (size_t l = 0; l + 1 < p->levels.size(); ++l) {
+        Level &L = p->levels[l], &C = p->levels[l + 1];
+        Fine F = fine_of(L, C, l == 0);
+        galerkin<<<blocks_for(C.n, 128), 128, 0, st>>>(F, C.a9.as<double>(9 * C.n),
+                                                        C.active.as<uint8_t>(C.n));
+    }
+    Level &Lc = p->levels.back();
+    int *status = p->status.as<int>(1);
+    BT_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+    coarsest_invert<<<1, 256, 0, st>>>(Lc.nx, Lc.ny, Lc.a9.as<double>(9 * Lc.n),
+                                       p->inv.as<double>(Lc.n * Lc.n), status);
+    BT_CHECK_LAUNCH();
+    p->built = true;
+    p->reaction_on = reaction != nullptr;
+}
+
+// x = V-cycle(b) on level l (x starts at zero on entry for l > 0; level 0's x given).
+void vcycle(bt_poisson *p, size_t l) {
+    cudaStream_t st = p->ctx->stream;
+    Level &L = p->levels[l];
+    const int T = 256;
+    if (l + 1 == p->levels.size()) {
+        coarsest_apply<<<1, kCoarsest, 0, st>>>((int)L.n, p->inv.as<double>(L.n * L.n),
+                                               L.b.as<double>(L.n), L.x.as<double>(L.n));
+        return;
+    }
+    Level &C = p->levels[l + 1];
+    double *x = L.x.as<double>(L.n), *b = L.b.as<double>(L.n), *r = L.r.as<double>(L.n);
+    const uint8_t *act = L.active.as<uint8_t>(L.n);
+    const int sweeps = 2;
+    if (l == 0) {
+        const double *c4 = L.c4.as<double>(4 * L.n), *dg = L.diag.as<double>(L.n);
+        const i64 per = L.nx * ((L.ny + 1) / 2);
+        for (int s = 0; s < sweeps; ++s)
+            for (int c = 0; c < 2; ++c)
+                smooth5<<<blocks_for(per, T), T, 0, st>>>(L.nx, L.ny, c4, dg, act, b, x, c);
+        apply5<<<blocks_for(L.n, T), T, 0, st>>>(L.nx, L.ny, c4, dg, act, x, b, r);
+    } else {
+        const double *a9 = L.a9.as<double>(9 * L.n);
+        const i64 per = ((L.nx + 1) / 2) * ((L.ny + 1) / 2);
+        for (int s = 0; s < sweeps; ++s)
+            for (int c = 0; c < 4; ++c)
+                smooth9<<<blocks_for(per, T), T, 0, st>>>(L.nx, L.ny, a9, act, b, x, c);
+        residual9<<<blocks_for(L.n, T), T, 0, st>>>(L.nx, L.ny, a9, act, x, b, r);
+    }
+    Fine F = fine_of(L, C, l == 0);
+    restrict_residual<<<blocks_for(C.n, T), T, 0, st>>>(F, r, C.b.as<double>(C.n),
+                                                          C.x.as<double>(C.n));
+    vcycle(p, l + 1);
+    prolong_add<<<blocks_for(L.n, T), T, 0, st>>>(F, C.x.as<double>(C.n), x);
+    if (l == 0) {
+        const double *c4 = L.c4.as<double>(4 * L.n), *dg = L.diag.as<double>(L.n);
+        const i64 per = L.nx * ((L.ny + 1) / 2);
+        for (int s = 0; s < sweeps; ++s)
+            for (int c = 1; c >= 0; --c)
+                smooth5<<<blocks_for(per, T), T, 0, st>>>(L.nx, L.ny, c4, dg, act, b, x, c);
+    } else {
+        const double *a9 = L.a9.as<double>(9 * L.n);
+        const i64 per = ((L.nx + 1) / 2) * ((L.ny + 1) / 2);
+        for (int s = 0; s < sweeps; ++s)
+            for (int c = 3; c >= 0; --c)
+                smooth9<<<blocks_for(per, T), T, 0, st>>>(L.nx, L.ny, a9, act, b, x, c);
+    }
+    BT_CHECK_LAUNCH();
+}
+
+// z = M v: one V-cycle from zero
+void precondition(bt_poisson *p, const double *v, double *z) {
+    Level &L = p->levels[0];
+    cudaStream_t st = p->ctx->stream;
+    BT_CUDA(cudaMemcpyAsync(L.b.as<double>(L.n), v, sizeof(double) * L.n, cudaMemcpyDeviceToDevice, st));
+    BT_CUDA(cudaMemsetAsync(L.x.as<double>(L.n), 0, sizeof(double) * L.n, st));
+    vcycle(p, 0);
+    BT_CUDA(cudaMemcpyAsync(z, L.x.as<double>(L.n), sizeof(double) * L.n, cudaMemcpyDeviceToDevice, st));
+}
+
+void apply(bt_poisson *p, const double *x, double *y) {
+    Level &L = p->levels[0];
+    apply5<<<blocks_for(L.n, 256), 256, 0, p->ctx->stream>>>(
+        L.nx, L.ny, L.c4.as<double>(4 * L.n), L.diag.as<double>(L.n),
+        L.active.as<uint8_t>(L.n), x, nullptr, y);
+}
+
+double read_scalar(bt_poisson *p, const double *dev) {
+    double *host = static_cast<double *>(p->ctx->host.get(sizeof(double) * 64));
+    BT_CUDA(cudaMemcpyAsync(host, dev, sizeof(double), cudaMemcpyDeviceToHost, p->ctx->stream));
+    BT_CUDA(cudaStreamSynchronize(p->ctx->stream));
+    return host[0];
+}
+
+double norm2(bt_poisson *p, const double *v) {
+    double *s = p->scalars.as<double>(8);
+    multi_dot<<<1, 256, 0, p->ctx->stream>>>(v, v, p->n, s);
+    return std::sqrt(read_scalar(p, s));
+}
+
+// Solve A d = r0 for d (d zero on entry) by restarted right-preconditioned GMRES until
+// ||r0 - A d|| <= abs_tol or max_iter V-cycles; returns the V-cycles and the final
+// residual norm.
+int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_iter,
+          double *final_norm) {
+    const i64 n = p->n;
+    const int m = p->restart;
+    cudaStream_t st = p->ctx->stream;
+    double *V = p->V.as<double>((size_t)(m + 1) * n);
+    double *Z = p->Z.as<double>((size_t)m * n);
+    double *w = p->work.as<double>(n);
+    double *hdev = p->hcol.as<double>(m + 2);
+    double *ydev = p->ycoef.as<double>(m + 2);
+    double *host = static_cast<double *>(p->ctx->host.get(sizeof(double) * (m + 8)));
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    int total = 0;
+    BT_CUDA(cudaMemcpyAsync(w, r0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    double beta = norm2(p, w);
+    double previous = INFINITY;
+    // stop at the tolerance, or where a whole restart cycle no longer halves the true
+    // residual: the rounding floor of the residual itself
+    while (beta > abs_tol && total < max_iter && beta < 0.5 * previous) {
+        previous = beta;
+        if (!std::isfinite(beta)) throw Error{BT_ERR_NOCONV, "field solve: the residual is not finite"};
+        scale_into<<<blocks_for(n, 256), 256, 0, st>>>(w, 1.0 / beta, n, V);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int j = 0;
+        while (j < m && total < max_iter) {
+            double *v = V + (i64)j * n, *z = Z + (i64)j * n;
+            precondition(p, v, z);
+            apply(p, z, w);
+            // classical Gram-Schmidt, applied twice
+            for (int pass = 0; pass < 2; ++pass) {
+                multi_dot<<<j + 1, 256, 0, st>>>(V, w, n, hdev);
+                orthogonalise<<<blocks_for(n, 256), 256, 0, st>>>(V, hdev, j + 1, n, w);
+                BT_CUDA(cudaMemcpyAsync(host, hdev, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, st));
+                BT_CUDA(cudaStreamSynchronize(st));
+                for (int q = 0; q <= j; ++q) H[q * m + j] = (pass ? H[q * m + j] : 0.0) + host[q];
+            }
+            const double hn = norm2(p, w);
+            H[(j + 1) * m + j] = hn;
+            if (hn > 0.0)
+                scale_into<<<blocks_for(n, 256), 256, 0, st>>>(w, 1.0 / hn, n, V + (i64)(j + 1) * n);
+            for (int q = 0; q < j; ++q) {
+                const double a = H[q * m + j], b = H[(q + 1) * m + j];
+                H[q * m + j] = cs[q] * a + sn[q] * b;
+                H[(q + 1) * m + j] = -sn[q] * a + cs[q] * b;
+            }
+            const double a = H[j * m + j], b = H[(j + 1) * m + j];
+            const double rr = std::hypot(a, b);
+            cs[j] = rr > 0.0 ? a / rr : 1.0;
+            sn[j] = rr > 0.0 ? b / rr : 0.0;
+            H[j * m + j] = rr;
+            H[(j + 1) * m + j] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            ++j;
+            ++total;
+            if (std::fabs(g[j]) <= abs_tol || hn == 0.0) break;
+        }
+        // y = H^-1 g on the j x j upper triangle, then d += Z y
+        for (int q = j - 1; q >= 0; --q) {
+            double s = g[q];
+            for (int c = q + 1; c < j; ++c) s -= H[q * m + c] * y[c];
+            y[q] = s / H[q * m + q];
+        }
+        BT_CUDA(cudaMemcpyAsync(ydev, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, st));
+        combine<<<blocks_for(n, 256), 256, 0, st>>>(Z, ydev, j, n, d);
+        // the true residual r0 - A d
+        apply(p, d, w);
+        subtract_from<<<blocks_for(n, 256), 256, 0, st>>>(r0, n, w);
+        BT_CHECK_LAUNCH();
+        beta = norm2(p, w);
+    }
+    if (final_norm) *final_norm = beta;
+    return total;
+}
+
+}  // namespace
+}  // namespace bt
+
+extern "C" int bt_poisson_create(bt_ctx *ctx, const bt_mesh_desc *m, bt_poisson **out) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx && m && out, "poisson: null argument");
+        BT_REQUIRE(m->nx >= 3 && m->ny >= 3, "poisson: the mesh needs at least 3 nodes per axis");
+        BT_REQUIRE(m->x && m->fixed && m->fixed_value && m->distance, "poisson: null mesh array");
+        BT_REQUIRE(m->h > 0.0, "poisson: h must be positive");
+        auto p = new bt_poisson;
+        try {
+            p->ctx = ctx;
+            p->nx = m->nx;
+            p->ny = m->ny;
+            p->n = m->nx * m->ny;
+            p->h = m->h;
+            p->cyl = m->cylindrical;
+            for (int q = 0; q < 4; ++q) p->neumann[q] = m->neumann ? m->neumann[q] : 0.0;
+            const i64 n = p->n;
+            BT_CUDA(cudaMemcpy(p->x.as<double>(p->nx), m->x, sizeof(double) * p->nx, cudaMemcpyHostToDevice));
+            BT_CUDA(cudaMemcpy(p->fixed.as<uint8_t>(n), m->fixed, n, cudaMemcpyHostToDevice));
+            BT_CUDA(cudaMemcpy(p->value.as<double>(n), m->fixed_value, sizeof(double) * n, cudaMemcpyHostToDevice));
+            BT_CUDA(cudaMemcpy(p->distance.as<double>(4 * n), m->distance, sizeof(double) * 4 * n, cudaMemcpyHostToDevice));
+            BT_CUDA(cudaMemcpy(p->fixed_eff.as<uint8_t>(n), m->fixed, n, cudaMemcpyHostToDevice));
+            BT_CUDA(cudaMemcpy(p->value_eff.as<double>(n), m->fixed_value, sizeof(double) * n, cudaMemcpyHostToDevice));
+            // the levels
+            p->levels.reserve(48);
+            i64 nx = p->nx, ny = p->ny;
+            while (true) {
+                p->levels.emplace_back();
+                bt::Level &L = p->levels.back();
+                L.nx = nx;
+                L.ny = ny;
+                L.n = nx * ny;
+                L.x.as<double>(L.n);
+                L.b.as<double>(L.n);
+                L.r.as<double>(L.n);
+                L.active.as<uint8_t>(L.n);
+                if (p->levels.size() == 1) {
+                    L.c4.as<double>(4 * L.n);
+                    L.diag.as<double>(L.n);
+                    L.base.as<double>(L.n);
+                    L.weight.as<double>(L.n);
+                } else {
+                    L.a9.as<double>(9 * L.n);
+                }
+                const bool more = L.n > bt::kCoarsest && (nx > 3 || ny > 3);
+                if (!more) break;
+                bt::build_axis(L.ax, nx);
+                bt::build_axis(L.ay, ny);
+                nx = L.ax.nc;
+                ny = L.ay.nc;
+            }
+            BT_REQUIRE(p->levels.back().n <= bt::kCoarsest, "poisson: coarsest level too large");
+            p->src.as<double>(n);
+            bt::build_operator(p);
+            BT_CUDA(cudaStreamSynchronize(ctx->stream));
+        } catch (...) {
+            delete p;
+            throw;
+        }
+        *out = p;
+    });
+}
+
+extern "C" int bt_poisson_destroy(bt_poisson *p) {
+    return bt::guarded([&] {
+        if (!p) return;
+        cudaStreamSynchronize(p->ctx->stream);
+        delete p;
+    });
+}
+
+extern "C" int bt_poisson_set_region(bt_poisson *p, const uint8_t *mask, double value) {
+    return bt::guarded([&] {
+        BT_REQUIRE(p, "poisson: null solver");
+        const i64 n = p->n;
+        std::vector<uint8_t> fixed(n);
+        std::vector<double> val(n);
+        BT_CUDA(cudaMemcpy(fixed.data(), p->fixed.as<uint8_t>(n), n, cudaMemcpyDeviceToHost));
+        BT_CUDA(cudaMemcpy(val.data(), p->value.as<double>(n), sizeof(double) * n, cudaMemcpyDeviceToHost));
+        if (mask)
+            for (i64 f = 0; f < n; ++f)
+                if (mask[f] && !fixed[f]) {
+                    fixed[f] = 1;
+                    val[f] = value;
+                }
+        BT_CUDA(cudaMemcpy(p->fixed_eff.as<uint8_t>(n), fixed.data(), n, cudaMemcpyHostToDevice));
+        BT_CUDA(cudaMemcpy(p->value_eff.as<double>(n), val.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        p->has_region = mask != nullptr;
+        p->region_value = value;
+        bt::build_operator(p);
+    });
+}
+
+extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, double amplitude,
+                                double temperature, double up, int32_t sign, double tol,
+                                double newton_tol, int32_t max_newton, int32_t *newton_steps,
+                                int32_t *cycles) {
+    return bt::guarded([&] {
+        BT_REQUIRE(p && phi, "poisson: null argument");
+        BT_REQUIRE(tol > 0.0, "poisson: the tolerance must be positive");
+        const i64 n = p->n;
+        cudaStream_t st = p->ctx->stream;
+        bt::Level &L0 = p->levels[0];
+        double *b = p->rhs.as<double>(n);
+        double *r0 = p->r0.as<double>(n);
+        double *d = p->delta.as<double>(n);
+        double *reaction = p->reaction.as<double>(n);
+        double *scal = p->scalars.as<double>(16);
+        const int max_cycles = 4000;
+        bt::prepare<<<bt::blocks_for(n, 256), 256, 0, st>>>(
+            n, rho, p->src.as<double>(n), L0.active.as<uint8_t>(n), p->value_eff.as<double>(n),
+            b, phi);
+        BT_CHECK_LAUNCH();
+        int total_cycles = 0, steps = 0;
+        if (!(amplitude > 0.0)) {
+            if (!p->built || p->reaction_on) bt::build_hierarchy(p, nullptr);
+            // r0 = b - A phi; the tolerance is relative to the larger of |b| and |r0|
+            bt::apply5<<<bt::blocks_for(n, 256), 256, 0, st>>>(
+                p->nx, p->ny, L0.c4.as<double>(4 * n), L0.diag.as<double>(n),
+                L0.active.as<uint8_t>(n), phi, b, r0);
+            BT_CHECK_LAUNCH();
+            const double scale = std::max(bt::norm2(p, b), bt::norm2(p, r0));
+            BT_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n, st));
+            double left = 0.0;
+            const double goal = tol * (scale > 0.0 ? scale : 1.0);
+            total_cycles = bt::gmres(p, r0, d, goal, max_cycles, &left);
+            bt::add_into<<<bt::blocks_for(n, 256), 256, 0, st>>>(d, n, phi);
+            BT_CHECK_LAUNCH();
+            // a residual stalled within 1e4 of the goal is the floor of its own rounding
+            if (!(left <= 1e4 * goal))
+                throw bt::Error{BT_ERR_NOCONV, "field solve: GMRES did not reach the tolerance"};
+        } else {
+            BT_REQUIRE(temperature > 0.0, "poisson: the temperature must be positive");
+            BT_REQUIRE(sign == 1 || sign == -1, "poisson: the species' sign must be +-1");
+            const int limit = max_newton > 0 ? max_newton : 100;
+            bool converged = false;
+            for (steps = 1; steps <= limit; ++steps) {
+                bt::boltzmann<<<bt::blocks_for(n, 256), 256, 0, st>>>(
+                    p->nx, p->ny, L0.c4.as<double>(4 * n), L0.base.as<double>(n),
+                    L0.active.as<uint8_t>(n), phi, b, amplitude, temperature, up, (double)sign,
+                    r0, reaction);
+                BT_CHECK_LAUNCH();
+                bt::build_hierarchy(p, reaction);
+                const double fnorm = bt::norm2(p, r0);
+                BT_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n, st));
+                double left = 0.0;
+                total_cycles += bt::gmres(p, r0, d, tol * (fnorm > 0.0 ? fnorm : 1.0),
+                                          max_cycles, &left);
+                bt::add_into<<<bt::blocks_for(n, 256), 256, 0, st>>>(d, n, phi);
+                bt::max_abs<<<1, 256, 0, st>>>(d, n, scal + 8);
+                BT_CHECK_LAUNCH();
+                const double change = bt::read_scalar(p, scal + 8);
+                if (!std::isfinite(change))
+                    throw bt::Error{BT_ERR_NOCONV, "field solve: Newton's update is not finite"};
+                if (change < newton_tol) {
+                    converged = true;
+                    break;
+                }
+            }
+            if (!converged) steps = limit;
+        }
+        int status = 0;
+        BT_CUDA(cudaMemcpyAsync(&status, p->status.as<int>(1), sizeof(int), cudaMemcpyDeviceToHost, st));
+        BT_CUDA(cudaStreamSynchronize(st));
+        if (status)
+            throw bt::Error{BT_ERR_NOCONV, "field solve: the coarsest operator is singular (is any node held?)"};
+        if (newton_steps) *newton_steps = steps;
+        if (cycles) *cycles = total_cycles;
+    });
+}

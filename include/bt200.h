@@ -130,6 +130,49 @@ int bt_edge_field(bt_ctx *ctx, const double *phi, const int32_t *solid, const ui
                   const double *distance, const double *dx, int64_t nx, int64_t ny,
                   double h, const int32_t extrapolation[4], double *fx, double *fy);
 
+/* -- the field solve ----------------------------------------------------------------- */
+
+typedef struct bt_poisson bt_poisson;
+
+/* The mesh a field solve is built from (HOST pointers, copied on creation). */
+typedef struct bt_mesh_desc {
+    int64_t nx, ny;
+    double h;                  /* the spacing along y (and along x on a uniform mesh) */
+    const double *x;           /* (nx,) node positions along x */
+    double origin_y;
+    int32_t cylindrical;       /* 1: (x, r) with the axis at y = origin_y = 0 */
+    const uint8_t *fixed;      /* (nx, ny) 1 for electrode and Dirichlet-face nodes */
+    const double *fixed_value; /* (nx, ny) their potentials */
+    const double *distance;    /* (4, nx, ny) surface distances towards -x, +x, -y, +y */
+    const double *neumann;     /* (4,) outward normal derivative on x_min, x_max, y_min,
+                                  y_max (ignored where the face's nodes are fixed), or NULL */
+} bt_mesh_desc;
+
+/* solver/poisson.py:536-933 (IonOpticsPoisson): build the finite-volume operator of the
+ * mesh (patchwork's NodalPoisson as poisson.py:1-24, 491-534 documents it) and its
+ * multigrid hierarchy on the device. */
+int bt_poisson_create(bt_ctx *ctx, const bt_mesh_desc *mesh, bt_poisson **out);
+int bt_poisson_destroy(bt_poisson *p);
+
+/* Hold the nodes of `mask` (HOST (nx, ny) uint8, or NULL for none) that the mesh does not
+ * fix at `value`: the initial plasma region of the first Vlasov iteration
+ * (solver/vlasov.py:350-355, poisson.py:279-309). */
+int bt_poisson_set_region(bt_poisson *p, const uint8_t *mask, double value);
+
+/* poisson.py:809-933 (IonOpticsPoisson.solve).  phi (DEVICE (nx, ny), in/out): the first
+ * guess on entry (its fixed nodes are set), the solution on return; rho (DEVICE (nx, ny),
+ * C/m^3, or NULL).  With amplitude = 0 one linear solve: GMRES preconditioned by a
+ * multigrid V-cycle to ||b - A phi|| <= tol max(||b||, ||b - A phi_0||).  With amplitude > 0
+ * the Boltzmann species sign * amplitude exp(min(-sign (phi - up) / temperature, 50))
+ * (amplitude = rho_0 / eps0) joins the source, and Newton's method runs: every step a
+ * GMRES solve of that step's Jacobian (the multigrid rebuilt for it) to the relative
+ * residual tol, until the largest update is below newton_tol or max_newton steps.
+ * Host out-params (may be NULL): Newton steps, V-cycles. */
+int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, double amplitude,
+                     double temperature, double up, int32_t sign, double tol,
+                     double newton_tol, int32_t max_newton, int32_t *newton_steps,
+                     int32_t *cycles);
+
 #ifdef __cplusplus
 }
 #endif

@@ -150,3 +150,52 @@ def trace_case_names() -> list[tuple[str, tuple]]:
 def copy_args(args: list) -> list:
     """A deep copy of an argument list (arrays copied, scalars kept)."""
     return [a.copy() if isinstance(a, np.ndarray) else a for a in args]
+
+
+# -- meshes -------------------------------------------------------------------------------
+
+
+def _ring(x0: float, x1: float, r0: float, r1: float):
+    """An electrode ``x0 <= x <= x1``, ``r0 <= y <= r1`` (a ring plate in (x, r))."""
+
+    def inside(x, y):
+        return (x >= x0) & (x <= x1) & (y >= r0) & (y <= r1)
+
+    return inside
+
+
+def _disc(cx: float, cy: float, radius: float):
+    def inside(x, y):
+        return (x - cx) ** 2 + (y - cy) ** 2 <= radius**2
+
+    return inside
+
+
+def mesh_cases() -> dict[str, dict]:
+    """Mesh settings (IonOpticsMesh keyword arguments, electrodes as (inside, potential)),
+    covering off-node surfaces on every side, overlapping electrodes, Dirichlet and Neumann
+    faces, the axis and a graded x axis."""
+    h = 1.0e-3
+    s = np.linspace(0.0, 1.0, 41)
+    return {
+        "planar_plates": dict(
+            shape=(31, 17), origin=(0.0, 0.0), h=h, geometry="planar",
+            electrodes=[(_ring(10.37e-3, 13.61e-3, 5.23e-3, 16.0e-3), -500.0),
+                        (_disc(22.4e-3, 6.1e-3, 3.33e-3), 250.0)],
+            faces={"x_min": ("dirichlet", 0.0), "x_max": ("dirichlet", -1000.0)},
+        ),
+        "cylindrical_lens": dict(
+            shape=(81, 21), origin=(0.0, 0.0), h=h, geometry="cylindrical",
+            electrodes=[(_ring(19.3e-3, 21.3e-3, 5.05e-3, 20.0e-3), 0.0),
+                        (_ring(39.4e-3, 41.4e-3, 5.55e-3, 20.0e-3), 7000.0),
+                        (_ring(59.15e-3, 61.15e-3, 5.0e-3, 20.0e-3), 0.0),
+                        (_disc(40.4e-3, 12.0e-3, 2.2e-3), 100.0)],
+            faces={},
+        ),
+        "graded_disc": dict(
+            shape=(41, 19), origin=(0.0, -9.0e-3), h=h, geometry="planar",
+            x_nodes=40 * h * (0.3 * s + 0.7 * s * s),
+            electrodes=[(_disc(20.2e-3, 0.3e-3, 4.1e-3), 1000.0)],
+            faces={"x_min": ("dirichlet", 0.0), "y_min": ("dirichlet", 50.0)},
+        ),
+    }

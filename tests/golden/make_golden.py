@@ -33,6 +33,7 @@ from tests.golden.cases import (  # noqa: E402
     copy_args,
     deposit_case,
     gather_case,
+    mesh_cases,
     trace_case,
     trace_case_names,
 )
@@ -45,6 +46,7 @@ def _lorentz_factor(u0, u1, u2, inv_c2):
 def _load(path: Path, name: str) -> types.ModuleType:
     spec = importlib.util.spec_from_file_location(name, path)
     module = importlib.util.module_from_spec(spec)
+    sys.modules[name] = module
     spec.loader.exec_module(module)
     return module
 
@@ -65,6 +67,27 @@ def reference_kernels(root: Path) -> dict:
                 module = _load(path, f"_ref_{name}_{version}")
                 out[(name, version)] = getattr(module, name)
     return out
+
+
+def reference_mesh_module(root: Path) -> types.ModuleType:
+    """The reference's ``solver/mesh.py`` (its one absent import, ``methodcard.method``, a
+    decorator that records documentation, stood in for by the identity)."""
+    card = types.ModuleType("methodcard")
+    card.method = lambda *a, **k: (lambda obj: obj)
+    sys.modules["methodcard"] = card
+    return _load(root / "src" / "beamtracer" / "solver" / "mesh.py", "_ref_mesh")
+
+
+def reference_edge_field(root: Path):
+    """The reference's ``_edge_field`` (``solver/fields.py:18-67``), taken out of its module."""
+    import ast
+
+    source = (root / "src" / "beamtracer" / "solver" / "fields.py").read_text()
+    tree = ast.parse(source)
+    node = next(n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name == "_edge_field")
+    namespace = {"np": np}
+    exec(compile(ast.Module(body=[node], type_ignores=[]), "fields.py", "exec"), namespace)
+    return namespace["_edge_field"]
 
 
 def _save(name: str, args: list, result: list, extra: dict | None = None) -> None:
@@ -95,6 +118,32 @@ def main() -> None:
                 result = copy_args(args)
                 ref[("deposit_trajectories_2d", version)](*result)
                 _save(f"deposit_s{seed}_c{cylindrical}_{version}", args, result)
+
+    mesh_module = reference_mesh_module(root)
+    edge_field = reference_edge_field(root)
+    for name, settings in mesh_cases().items():
+        settings = dict(settings)
+        electrodes = [mesh_module.Electrode(f, v) for f, v in settings.pop("electrodes")]
+        faces = {k: mesh_module.FaceCondition(*v) for k, v in settings.pop("faces").items()}
+        mesh = mesh_module.IonOpticsMesh(electrodes=electrodes, faces=faces, **settings)
+        rng = np.random.default_rng(21)
+        phi = np.where(mesh.fixed, mesh.fixed_value, rng.normal(size=mesh.shape) * 100.0)
+        extrapolation = ["extrapolate"] * 4
+        if mesh.cylindrical or mesh.symmetry_plane:
+            extrapolation[2] = "symmetric"
+        solid, near = mesh.solid >= 0, mesh.near_solid
+        fx = edge_field(phi, solid, near, mesh.distance[0], mesh.distance[1], mesh.dx,
+                        extrapolation[0:2])
+        fy = np.ascontiguousarray(
+            edge_field(phi.T, solid.T, near.T, mesh.distance[2].T, mesh.distance[3].T,
+                       mesh.h, extrapolation[2:4]).T
+        )  # fmt: skip
+        np.savez_compressed(
+            HERE / f"mesh_{name}.npz", solid=mesh.solid, fixed=mesh.fixed,
+            fixed_value=mesh.fixed_value, distance=mesh.distance,
+            near_solid=mesh.near_solid, phi=phi, fx=fx, fy=fy,
+        )  # fmt: skip
+        print("mesh", name, "near", int(near.sum()), "solid", int(solid.sum()))
 
     kernel = ref[("trace_trajectories_2d", "pyccel")]
     for name, combo in trace_case_names():
