@@ -87,6 +87,8 @@ SIGNATURES: dict[str, list] = {
     "bt_trace_trajectories_2d": [P, ctypes.POINTER(TraceArgs), I64],
     "bt_trace_last_stats": [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64)],
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],
+    "bt_vlasov_mix": [P, P, P, P, I64, I64, F64, I32, P, P],
+    "bt_max_abs_diff": [P, P, P, I64, P],
     "bt_poisson_create": [P, ctypes.POINTER(MeshDesc), ctypes.POINTER(P)],
     "bt_poisson_destroy": [P],
     "bt_poisson_set_region": [P, P, F64],

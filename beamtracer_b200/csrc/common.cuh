@@ -107,6 +107,7 @@ struct bt_ctx {
     bt::DepositScratch deposit;
     bt::TraceScratch trace;
     bt::HostBuffer host;
+    bt::Buffer reduce_partial;  // per-block partial results of the device reductions
     i64 last_windows = 0, last_records = 0, last_flushes = 0;
 };
 

@@ -1,0 +1,560 @@
+"""Beams, the trajectory trace and its results, on the B200.
+
+The interface of the reference's ``solver/tracer.py``: ``BeamParticles``,
+``beam_with_energy``, ``PlaneHits``, ``TraceResult`` and ``BeamTracer``
+(``tracer.py:87-327, 384-1366``).  The trace is the device kernel of
+``trace_trajectories_2d`` (``libbt200.so``); around it, as the reference's
+``_trace_compiled`` (``tracer.py:1186-1304``) does on the host:
+
+- trajectories starting inside an electrode end at once (status 3);
+- trajectories stopped in a sub-cell that an electrode surface cuts (status -2) are
+  decided by the electrodes' own ``inside`` tests and the others resumed;
+- a trace that records more plane crossings or path points than its buffers hold is
+  repeated with larger buffers, which the tracer keeps;
+- the node charges are divided by the node volumes (``tracer.py:678-705``).
+
+`TraceEngine` keeps everything of a trace on the device, so the Vlasov iteration can
+trace the same beam again and again without copying it back and forth.
+"""
+
+from __future__ import annotations
+
+from collections.abc import Sequence
+from dataclasses import dataclass, field
+from typing import Any
+
+import numpy as np
+from scipy import constants
+
+from beamtracer_b200.mesh import IonOpticsMesh
+
+#: Status of a finished trajectory.
+TRANSMITTED, BACKWARD, WALL, ELECTRODE, MAX_STEPS = 0, 1, 2, 3, 4
+STATUS_NAMES = ("transmitted", "backward", "wall", "electrode", "max_steps")
+_ALIVE, _PAUSED = -1, -2
+#: Sub-cells per cell side of the electrode lookup.
+SUBCELLS = 8
+INTEGRATORS = ("rk4", "boris")
+
+
+def lorentz_factor(u: np.ndarray, c: float) -> np.ndarray:
+    """``sqrt(1 + |u|^2 / c^2)`` of proper velocities ``u`` (3, N)."""
+    return np.sqrt(1.0 + np.sum(u * u, axis=0) / (c * c))
+
+
+def proper_velocity(v: np.ndarray, c: float) -> np.ndarray:
+    """``v / sqrt(1 - |v|^2 / c^2)`` of velocities ``v`` (3, N)."""
+    return v / np.sqrt(1.0 - np.sum(v * v, axis=0) / (c * c))
+
+
+@dataclass
+class BeamParticles:
+    """Particle starting states (``tracer.py:87-126``): positions and velocities (3, N),
+    charge [C], mass [kg], current [A] and species index per particle."""
+
+    position: np.ndarray
+    velocity: np.ndarray
+    charge: np.ndarray
+    mass: np.ndarray
+    current: np.ndarray
+    species: np.ndarray
+
+    @staticmethod
+    def concatenate(parts: Sequence[BeamParticles]) -> BeamParticles:
+        return BeamParticles(
+            np.concatenate([p.position for p in parts], axis=1),
+            np.concatenate([p.velocity for p in parts], axis=1),
+            *(np.concatenate([getattr(p, name) for p in parts])
+              for name in ("charge", "mass", "current", "species")),
+        )  # fmt: skip
+
+    def subset(self, index) -> BeamParticles:
+        return BeamParticles(
+            self.position[:, index], self.velocity[:, index], self.charge[index],
+            self.mass[index], self.current[index], self.species[index],
+        )  # fmt: skip
+
+    def __len__(self) -> int:
+        return int(self.position.shape[1])
+
+
+def _gaussian_samples(num: int, sampling) -> np.ndarray:
+    """(num, 3) standard normal samples: an unscrambled Sobol sequence without its origin
+    through the inverse normal, or a NumPy generator's draws."""
+    if isinstance(sampling, np.random.Generator):
+        return sampling.standard_normal((num, 3))
+    if sampling != "sobol":
+        raise ValueError(f"sampling must be 'sobol' or a numpy Generator, got {sampling!r}")
+    from scipy.stats import norm, qmc
+
+    sobol = qmc.Sobol(d=3, scramble=False)
+    sobol.fast_forward(1)
+    return norm.ppf(sobol.random(num))
+
+
+def beam_with_energy(
+    num_particles: int,
+    current_density: float,
+    charge: float,
+    mass: float,
+    energy: float,
+    parallel_temperature: float,
+    transverse_temperature: float,
+    start: tuple[float, float],
+    end: tuple[float, float],
+    *,
+    cylindrical: bool,
+    species: int = 0,
+    sampling="sobol",
+    relativistic: bool = False,
+) -> tuple[BeamParticles, float]:
+    """A beam emitted from the line ``start``-``end`` with ``energy`` [eV]; and ``J / v``.
+
+    ``tracer.py:221-291``: trajectories evenly spaced at ``(k + 1/2) / N`` of the line,
+    moving perpendicular to it (to its right) with Gaussian spreads of the temperatures
+    [eV]; a ring current ``2 pi J s r / N`` (cylindrical) or ``J s / N`` per unit depth.
+    ``charge`` [e], ``mass`` [u], ``current_density`` [A/m^2].
+    """
+    q = charge * constants.e
+    m = mass * constants.atomic_mass
+    if relativistic:
+        c = constants.c
+        gamma = 1.0 + energy * constants.e / (m * c * c)
+        v = float(c * np.sqrt(gamma * gamma - 1.0))
+    else:
+        v = float(np.sqrt(2.0 * energy * constants.e / m))
+    dvp = float(np.sqrt(parallel_temperature * constants.e / m))
+    dvt = float(np.sqrt(transverse_temperature * constants.e / m))
+    (x1, y1), (x2, y2) = start, end
+    s = float(np.hypot(x2 - x1, y2 - y1))
+    if s == 0.0:
+        raise ValueError("the beam start line has zero length")
+    tangent = np.array([x2 - x1, y2 - y1]) / s
+    normal = np.array([tangent[1], -tangent[0]])
+    frac = (np.arange(num_particles) + 0.5) / num_particles
+    px = x1 + (x2 - x1) * frac
+    py = y1 + (y2 - y1) * frac
+    g = _gaussian_samples(num_particles, sampling)
+    vx = normal[0] * v + tangent[0] * dvt * g[:, 0] + normal[0] * dvp * g[:, 1]
+    vy = normal[1] * v + tangent[1] * dvt * g[:, 0] + normal[1] * dvp * g[:, 1]
+    vz = dvt * g[:, 2] if cylindrical else np.zeros(num_particles)
+    if cylindrical:
+        current = 2.0 * np.pi * current_density * s * py / num_particles
+    else:
+        current = np.full(num_particles, current_density * s / num_particles)
+    velocity = np.stack([vx, vy, vz], axis=0)
+    if relativistic:
+        velocity = velocity / lorentz_factor(velocity, constants.c)
+        v = v / float(np.sqrt(1.0 + (v / constants.c) ** 2))
+    particles = BeamParticles(
+        position=np.stack([px, py, np.zeros(num_particles)], axis=0),
+        velocity=velocity,
+        charge=np.full(num_particles, q),
+        mass=np.full(num_particles, m),
+        current=current,
+        species=np.full(num_particles, species, dtype=np.int32),
+    )
+    return particles, current_density / v
+
+
+@dataclass
+class PlaneHits:
+    """Crossings of the plane ``x = position_x`` (``tracer.py:295-325``)."""
+
+    position_x: float
+    point: np.ndarray = field(default_factory=lambda: np.zeros((3, 0)))
+    velocity: np.ndarray = field(default_factory=lambda: np.zeros((3, 0)))
+    current: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    species: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int32))
+    direction: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int8))
+    fractions: np.ndarray | None = None
+
+    def append(self, point, velocity, current, species, direction, fractions=None) -> None:
+        self.point = np.concatenate([self.point, point], axis=1)
+        self.velocity = np.concatenate([self.velocity, velocity], axis=1)
+        self.current = np.concatenate([self.current, current])
+        self.species = np.concatenate([self.species, species.astype(np.int32)])
+        self.direction = np.concatenate([self.direction, direction.astype(np.int8)])
+
+
+@dataclass
+class TraceResult:
+    """The outcome of a trace (``tracer.py:327-347``)."""
+
+    charge_density: Any
+    status: np.ndarray
+    electrode: np.ndarray
+    planes: list[PlaneHits]
+    trajectories: list[np.ndarray]
+    trajectory_species: np.ndarray
+    steps: int
+    fractions: np.ndarray | None = None
+    tallies: Any = None
+    current_density: np.ndarray | None = None
+
+
+def node_volumes(mesh: IonOpticsMesh) -> np.ndarray:
+    """The node volumes the deposit divides by: a quarter of every adjacent cell, a cell
+    ``dx h`` (planar, per unit depth) or ``2 pi r_c dx h`` (cylindrical, ``r_c`` its centre's
+    radius) -- the volumes the area-weighted deposit is consistent with
+    (``solver/refinement.py:274-296`` on an unrefined mesh)."""
+    nx, ny = mesh.shape
+    cell = mesh.dx[:, None] * np.full(ny - 1, mesh.h)[None, :]
+    if mesh.cylindrical:
+        centres = mesh.origin[1] + mesh.h * (np.arange(ny - 1) + 0.5)
+        cell = 2.0 * np.pi * centres[None, :] * cell
+    volumes = np.zeros((nx, ny))
+    quarter = 0.25 * cell
+    volumes[:-1, :-1] += quarter
+    volumes[1:, :-1] += quarter
+    volumes[:-1, 1:] += quarter
+    volumes[1:, 1:] += quarter
+    return volumes
+
+
+def electrode_cells(mesh: IonOpticsMesh) -> np.ndarray:
+    """Cells with an electrode node or a node next to one (``tracer.py:488-493``)."""
+    touch = (mesh.solid >= 0) | mesh.near_solid
+    return touch[:-1, :-1] | touch[1:, :-1] | touch[:-1, 1:] | touch[1:, 1:]
+
+
+def subcell_table(mesh: IonOpticsMesh, ci: np.ndarray, cj: np.ndarray) -> np.ndarray:
+    """The electrode of every sub-cell (len(ci), 8, 8) of cells (ci, cj): the electrode
+    containing its four corners and its centre, -1 for none, -2 where they disagree
+    (``tracer.py:1095-1114``)."""
+
+    def sample(fraction: np.ndarray) -> np.ndarray:
+        px = mesh.position_x(ci[:, None, None] + fraction[None, :, None])
+        py = mesh.origin[1] + mesh.h * (cj[:, None, None] + fraction[None, None, :])
+        px, py = np.broadcast_arrays(px, py)
+        return mesh.inside_solid(px.ravel(), py.ravel()).reshape(px.shape)
+
+    corner = sample(np.arange(SUBCELLS + 1) / SUBCELLS)
+    centre = sample((np.arange(SUBCELLS) + 0.5) / SUBCELLS)
+    same = ((corner[:, :-1, :-1] == centre) & (corner[:, 1:, :-1] == centre)
+            & (corner[:, :-1, 1:] == centre) & (corner[:, 1:, 1:] == centre))  # fmt: skip
+    return np.where(same, centre, -2).astype(np.int64)
+
+
+def electrode_lookup(mesh: IonOpticsMesh) -> tuple[np.ndarray, np.ndarray]:
+    """``cells`` (nx - 1, ny - 1): the number of every cell touching an electrode (-1 for
+    the others); ``subcells``: their sub-cell tables, flattened (``tracer.py:1116-1139``)."""
+    touching = electrode_cells(mesh)
+    cells = np.full(touching.shape, -1, dtype=np.int64)
+    ci, cj = np.nonzero(touching)
+    if not mesh.electrodes or not ci.size:
+        return cells, np.full(1, -1, dtype=np.int64)
+    cells[ci, cj] = np.arange(ci.size, dtype=np.int64)
+    return cells, subcell_table(mesh, ci, cj).ravel()
+
+
+def _project(mesh: IonOpticsMesh, x: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The mesh coordinates (x, y) or (x, r) of Cartesian points (3, N)."""
+    if mesh.cylindrical:
+        return x[0], np.hypot(x[1], x[2])
+    if mesh.symmetry_plane:
+        y0 = mesh.origin[1]
+        return x[0], y0 + np.abs(x[1] - y0)
+    return x[0], x[1]
+
+
+def geometry_code(mesh: IonOpticsMesh) -> int:
+    """0 planar, 1 cylindrical, 2 planar with a symmetry plane."""
+    if mesh.symmetry_plane:
+        return 2
+    return int(mesh.cylindrical)
+
+
+class TraceEngine:
+    """A trace setup held on the device: the mesh's tables, a beam, the result buffers.
+
+    ``load`` copies a beam to the device once; every ``run`` traces it from its start
+    through edge fields ``fx``, ``fy`` (device arrays) and leaves the node charges in
+    ``charge`` and the trajectories' ends in the state arrays.
+    """
+
+    def __init__(
+        self,
+        mesh: IonOpticsMesh,
+        *,
+        planes: Sequence[float] = (),
+        integrator: str = "rk4",
+        step_fraction: float = 0.5,
+        max_steps: int = 100_000,
+        inv_c2: float = 0.0,
+        save_trajectories: int = 0,
+        capacity: tuple[int, int] = (4, 1024),
+        window: int = 64,
+    ) -> None:
+        import torch
+
+        from beamtracer_b200 import _lib
+
+        self.torch = torch
+        self.mesh = mesh
+        self.planes = tuple(float(p) for p in planes)
+        self.integrator = integrator
+        self.step_fraction = float(step_fraction)
+        self.max_steps = int(max_steps)
+        self.inv_c2 = float(inv_c2)
+        self.save_trajectories = int(save_trajectories)
+        self.capacity = tuple(capacity)
+        self.window = int(window)
+        self.ctx = _lib.context()
+        dev = "cuda"
+        nx, ny = mesh.shape
+        cells, subcells = electrode_lookup(mesh)
+        self.cells = torch.from_numpy(cells).to(dev)
+        self.subcells = torch.from_numpy(subcells).to(dev)
+        lo_x, lo_y = mesh.logical_origin
+        up_x, up_y = mesh.logical_upper
+        self.patch_int = torch.tensor([[nx, ny, 0, 0, nx * ny, 0]], dtype=torch.int64, device=dev)
+        self.patch_real = torch.tensor([[lo_x, lo_y, mesh.h, lo_x, lo_y, up_x, up_y]],
+                                       dtype=torch.float64, device=dev)  # fmt: skip
+        self.x_nodes = torch.from_numpy(
+            np.ascontiguousarray(mesh.x if mesh.graded else np.zeros(2))
+        ).to(dev)
+        self.planes_dev = torch.tensor(self.planes or (np.nan,), dtype=torch.float64, device=dev)
+        self.volumes = torch.from_numpy(node_volumes(mesh)).to(dev)
+        self.n_nodes = nx * ny
+        self.charge = torch.zeros((1, self.n_nodes), dtype=torch.float64, device=dev)
+        self.particles: BeamParticles | None = None
+
+    # -- the beam -------------------------------------------------------------------------
+
+    def load(self, particles: BeamParticles) -> None:
+        """Copy a beam to the device (its start states are kept for every run)."""
+        torch = self.torch
+        mesh = self.mesh
+        n = len(particles)
+        dev = "cuda"
+        self.particles = particles
+        self.n = n
+        x = np.ascontiguousarray(particles.position, dtype=np.float64)
+        v = np.array(particles.velocity, dtype=np.float64, order="C")
+        if self.inv_c2 > 0.0:
+            v = np.ascontiguousarray(proper_velocity(v, 1.0 / np.sqrt(self.inv_c2)))
+        status = np.full(n, _ALIVE, dtype=np.int64)
+        electrode = np.full(n, -1, dtype=np.int64)
+        if mesh.electrodes and n:
+            hit = mesh.inside_solid(*_project(mesh, x))
+            dead = hit >= 0
+            status[dead] = ELECTRODE
+            electrode[dead] = hit[dead]
+        self.start_active = torch.from_numpy(np.flatnonzero(status == _ALIVE).astype(np.int64)).to(dev)
+        self.x0 = torch.from_numpy(x).to(dev)
+        self.v0 = torch.from_numpy(v).to(dev)
+        self.status0 = torch.from_numpy(status).to(dev)
+        self.electrode0 = torch.from_numpy(electrode).to(dev)
+        self.qm = torch.from_numpy(np.ascontiguousarray(particles.charge / particles.mass,
+                                                        dtype=np.float64)).to(dev)  # fmt: skip
+        current = particles.current.astype(np.float64)
+        self.dq = torch.from_numpy(
+            np.ascontiguousarray(np.sign(particles.charge) * np.abs(current))
+        ).to(dev)
+        save = self.save_trajectories
+        self.saved_ids = np.arange(0, n, save) if save else np.zeros(0, int)
+        slot = np.full(n, -1, dtype=np.int64)
+        slot[self.saved_ids] = np.arange(self.saved_ids.size)
+        self.path_slot = torch.from_numpy(slot).to(dev)
+        px, py = _project(mesh, x[:, self.saved_ids])
+        self.first_points = torch.from_numpy(np.stack([px, py], axis=1).copy()).to(dev)
+        self.x = torch.empty_like(self.x0)
+        self.v = torch.empty_like(self.v0)
+        self.steps = torch.zeros(n, dtype=torch.int64, device=dev)
+        self.status = torch.empty_like(self.status0)
+        self.electrode = torch.empty_like(self.electrode0)
+        self._allocate_buffers()
+
+    def _allocate_buffers(self) -> None:
+        torch = self.torch
+        capacity, path_capacity = self.capacity
+        slots = max(self.saved_ids.size, 1)
+        P = len(self.planes_dev)
+        self.hits = torch.zeros((self.n, P, capacity, 8), dtype=torch.float64, device="cuda")
+        self.counts = torch.zeros((self.n, P), dtype=torch.int64, device="cuda")
+        self.paths = torch.zeros((slots, path_capacity, 2), dtype=torch.float64, device="cuda")
+        self.path_count = torch.ones(slots, dtype=torch.int64, device="cuda")
+
+    # -- one trace ------------------------------------------------------------------------
+
+    def _reset(self) -> None:
+        self.x.copy_(self.x0)
+        self.v.copy_(self.v0)
+        self.status.copy_(self.status0)
+        self.electrode.copy_(self.electrode0)
+        self.steps.zero_()
+        self.charge.zero_()
+        self.counts.zero_()
+        self.path_count.fill_(1)
+        k = self.saved_ids.size
+        if k:
+            self.paths[:k, 0] = self.first_points
+
+    def _kernel(self, active, fx, fy) -> None:
+        from beamtracer_b200.kernels import trace_trajectories_2d
+
+        mesh = self.mesh
+        lo_x, lo_y = mesh.logical_origin
+        up_x, up_y = mesh.logical_upper
+        trace_trajectories_2d(
+            active, self.x, self.v, self.qm, self.dq, self.steps, self.status,
+            self.electrode, fx.reshape(-1), fy.reshape(-1), self.patch_int, self.patch_real,
+            lo_x, lo_y, mesh.h, up_x, up_y, geometry_code(mesh),
+            INTEGRATORS.index(self.integrator), self.step_fraction, self.max_steps,
+            self.cells, self.subcells, SUBCELLS, self.planes_dev, self.hits, self.counts,
+            self.path_slot, self.paths, self.path_count, 1, self.charge, int(mesh.graded),
+            self.x_nodes, self.inv_c2, window=self.window,
+        )  # fmt: skip
+
+    def run(self, fx, fy) -> None:
+        """Trace the loaded beam through the edge fields (device arrays)."""
+        torch = self.torch
+        mesh = self.mesh
+        while True:
+            self._reset()
+            active = self.start_active
+            while active.numel():
+                self._kernel(active, fx, fy)
+                paused_mask = self.status[active] == _PAUSED
+                if not bool(paused_mask.any()):
+                    break
+                paused = active[paused_mask]
+                points = self.x[:, paused].cpu().numpy()
+                hit = mesh.inside_solid(*_project(mesh, points))
+                inside = torch.from_numpy(hit >= 0).to("cuda")
+                hit_dev = torch.from_numpy(hit.astype(np.int64)).to("cuda")
+                stopped = paused[inside]
+                self.status[stopped] = ELECTRODE
+                self.electrode[stopped] = hit_dev[inside]
+                active = paused[~inside]
+                self.status[active] = _ALIVE
+            capacity, path_capacity = self.capacity
+            most = int(self.counts.max()) if self.counts.numel() else 0
+            longest = int(self.path_count.max())
+            if most <= capacity and longest <= path_capacity:
+                return
+            self.capacity = (max(capacity, most), max(path_capacity, longest))
+            self._allocate_buffers()
+
+    # -- results --------------------------------------------------------------------------
+
+    def density(self):
+        """The charge density on the nodes (device (nx, ny)): charges over volumes."""
+        return (self.charge[0] / self.volumes.reshape(-1)).reshape(self.mesh.shape)
+
+    def result(self, density=None) -> TraceResult:
+        """The trace as the reference returns it (host arrays; ``tracer.py:1265-1304``)."""
+        particles = self.particles
+        current = particles.current.astype(float)
+        species = particles.species
+        counts = self.counts.cpu().numpy()
+        hits = self.hits.cpu().numpy()
+        capacity = hits.shape[2]
+        slots = np.arange(capacity)
+        planes = []
+        for p, position in enumerate(self.planes):
+            k, c = np.nonzero(slots[None, :] < counts[:, p, None])
+            record = hits[k, p, c]
+            order = np.lexsort((k, record[:, 7]))
+            k, record = k[order], record[order]
+            plane = PlaneHits(position)
+            plane.append(record[:, 0:3].T.copy(), record[:, 3:6].T.copy(), current[k],
+                         species[k], record[:, 6].astype(np.int8))  # fmt: skip
+            planes.append(plane)
+        paths = self.paths.cpu().numpy()
+        path_count = self.path_count.cpu().numpy()
+        status = self.status.cpu().numpy()
+        steps = self.steps.cpu().numpy()
+        if density is None:
+            density = self.density()
+        return TraceResult(
+            charge_density=density.cpu().numpy() if hasattr(density, "cpu") else density,
+            status=status.astype(np.int8),
+            electrode=self.electrode.cpu().numpy().astype(np.int32),
+            planes=planes,
+            trajectories=[paths[i, : path_count[i]].copy() for i in range(self.saved_ids.size)],
+            trajectory_species=species[self.saved_ids],
+            steps=int(steps.max()) if steps.size else 0,
+        )
+
+
+class BeamTracer:
+    """Trace particles through a static electric field (``tracer.py:384-1366``).
+
+    ``electric`` is a `StaggeredElectricField` of the mesh.  The trace runs on the device;
+    a magnetic field, an imposed electric field and charge changes belong to the
+    reference's NumPy tracer and are not part of this build.
+    """
+
+    def __init__(
+        self,
+        mesh: IonOpticsMesh,
+        electric: Any,
+        magnetic: Any = None,
+        *,
+        imposed_electric: Any = None,
+        step_fraction: float = 0.5,
+        max_steps: int = 100_000,
+        planes: Sequence[float] = (),
+        save_trajectories: int = 0,
+        charge_changing: Any = None,
+        compiled: bool | None = None,
+        integrator: str = "rk4",
+        relativistic: bool = False,
+        speed_of_light: float = constants.c,
+        window: int = 64,
+    ) -> None:
+        if not 0.0 < step_fraction <= 1.0:
+            raise ValueError(f"step_fraction must be in (0, 1], got {step_fraction}")
+        if integrator not in INTEGRATORS:
+            raise ValueError(f"integrator must be one of {INTEGRATORS}, got {integrator!r}")
+        unsupported = {
+            "a magnetic field": magnetic, "an imposed electric field": imposed_electric,
+            "charge changes": charge_changing,
+        }  # fmt: skip
+        given = [name for name, value in unsupported.items() if value is not None]
+        if given:
+            raise NotImplementedError("this build's tracer takes no " + ", ".join(given))
+        self.mesh = mesh
+        self.electric = electric
+        self.magnetic = None
+        self.step_fraction = float(step_fraction)
+        self.max_steps = int(max_steps)
+        self.planes = tuple(float(p) for p in planes)
+        self.save_trajectories = int(save_trajectories)
+        self.integrator = integrator
+        self.relativistic = bool(relativistic)
+        self.speed_of_light = float(speed_of_light)
+        self.compiled = compiled
+        self.window = int(window)
+        self._capacity = (4, 1024)
+        #: Sums the node charges over ranks (set by a distributed run), or None.
+        self.reduce = None
+        self._engine: TraceEngine | None = None
+
+    def _inv_c2(self) -> float:
+        return 1.0 / self.speed_of_light**2 if self.relativistic else 0.0
+
+    def engine(self) -> TraceEngine:
+        if self._engine is None:
+            self._engine = TraceEngine(
+                self.mesh, planes=self.planes, integrator=self.integrator,
+                step_fraction=self.step_fraction, max_steps=self.max_steps,
+                inv_c2=self._inv_c2(), save_trajectories=self.save_trajectories,
+                capacity=self._capacity, window=self.window,
+            )  # fmt: skip
+        return self._engine
+
+    def trace(self, particles: BeamParticles) -> TraceResult:
+        """Trace ``particles`` until they leave the mesh or hit an electrode."""
+        if self.electric is None:
+            raise RuntimeError("the tracer has no electric field yet")
+        engine = self.engine()
+        engine.load(particles)
+        engine.run(self.electric.fx_device, self.electric.fy_device)
+        self._capacity = engine.capacity
+        density = engine.density()
+        if self.reduce is not None:
+            density = self.reduce(density)
+        return engine.result(density)

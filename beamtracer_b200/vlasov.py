@@ -1,0 +1,337 @@
+"""The Vlasov iteration: solve the field, trace the beam, deposit its space charge, repeat.
+
+The interface and the loop of the reference's ``solver/vlasov.py`` (``vlasov_iterate``,
+``PlasmaModel``, ``NegativeIonPlasmaModel``, ``Compensation``, ``AndersonMixer``,
+``VlasovState``, ``thin_particles``; ``vlasov.py:37-429``), with the potential, the edge
+fields, the beam and the charge density resident on the device from iteration to
+iteration: an iteration is the field solve (``IonOpticsPoisson.solve_device``), the edge
+field, the trace of the beam loaded once, and one kernel that turns the node charges into
+the mixed density and reports the largest changes.  Only scalars cross to the host inside
+the loop; the state's arrays are copied back when they are read.
+"""
+
+from __future__ import annotations
+
+from collections.abc import Callable, Sequence
+from dataclasses import dataclass, field
+from typing import Any
+
+import numpy as np
+
+from beamtracer_b200 import _lib
+from beamtracer_b200.fields import MeshArrays, StaggeredElectricField
+from beamtracer_b200.mesh import IonOpticsMesh
+from beamtracer_b200.poisson import BoltzmannElectrons, BoltzmannIons, IonOpticsPoisson
+from beamtracer_b200.tracer import BeamParticles, BeamTracer, TraceResult
+
+
+@dataclass(frozen=True)
+class PlasmaModel:
+    """Boltzmann plasma electrons for positive-ion extraction (``vlasov.py:37-64``)."""
+
+    electron_temperature: float
+    plasma_potential: float
+    initial_plasma_x: float
+    rho_e: float | None = None
+
+    @property
+    def density(self) -> float | None:
+        return self.rho_e
+
+    def boltzmann(self, density: float) -> BoltzmannElectrons:
+        return BoltzmannElectrons(density, self.electron_temperature, self.plasma_potential)
+
+
+@dataclass(frozen=True)
+class NegativeIonPlasmaModel:
+    """Boltzmann plasma ions for negative-ion extraction (``vlasov.py:67-93``)."""
+
+    ion_temperature: float
+    plasma_potential: float
+    initial_plasma_x: float
+    rho_p: float | None = None
+
+    @property
+    def density(self) -> float | None:
+        return self.rho_p
+
+    def boltzmann(self, density: float) -> BoltzmannIons:
+        return BoltzmannIons(density, self.ion_temperature, self.plasma_potential)
+
+
+@dataclass(frozen=True)
+class Compensation:
+    """The beam's charge density times ``1 - fraction`` for ``x_min <= x <= x_max``."""
+
+    x_min: float
+    x_max: float
+    fraction: float
+
+
+def compensation_factors(x: np.ndarray, compensation: Sequence[Compensation]) -> np.ndarray | None:
+    """The factor of every node column (``vlasov.py:176-184``), or None for no regions."""
+    if not compensation:
+        return None
+    factor = np.ones(len(x))
+    for region in compensation:
+        inside = (x >= region.x_min) & (x <= region.x_max)
+        factor[inside] *= 1.0 - region.fraction
+    return factor
+
+
+class AndersonMixer:
+    """Anderson acceleration of ``rho = G(rho)`` (``vlasov.py:127-173``), on device arrays.
+
+    The least-squares problem of the last ``depth`` differences is solved through a QR
+    factorisation of the (n, m) difference matrix and a cut-off of 1e-10 on the singular
+    values of its small triangular factor (those of the difference matrix itself).
+    """
+
+    def __init__(self, depth: int = 5, relaxation: float = 1.0) -> None:
+        if depth < 1:
+            raise ValueError(f"depth must be at least 1, got {depth}")
+        self.depth = int(depth)
+        self.relaxation = float(relaxation)
+        self._x: list = []
+        self._f: list = []
+
+    def reset(self) -> None:
+        self._x, self._f = [], []
+
+    def update(self, rho, deposit):
+        import torch
+
+        x = rho.reshape(-1).clone()
+        f = deposit.reshape(-1) - x
+        self._x.append(x)
+        self._f.append(f)
+        del self._x[: -self.depth - 1], self._f[: -self.depth - 1]
+        omega = self.relaxation
+        new = x + omega * f
+        if len(self._x) > 1:
+            dx = torch.diff(torch.stack(self._x), dim=0).T
+            df = torch.diff(torch.stack(self._f), dim=0).T
+            q, r = torch.linalg.qr(df)
+            u, s, vh = np.linalg.svd(r.cpu().numpy())
+            keep = s > 1e-10 * s.max() if s.size and s.max() > 0 else np.zeros(s.shape, bool)
+            qf = (q.T @ f).cpu().numpy()
+            gamma = vh[keep].T @ ((u[:, keep].T @ qf) / s[keep])
+            g = torch.from_numpy(gamma).to(rho.device)
+            new = new - (dx + omega * df) @ g
+        return new.reshape(rho.shape)
+
+
+def thin_particles(particles: BeamParticles, stride: int) -> BeamParticles:
+    """Every ``stride``-th trajectory of each species, its current scaled to keep the
+    species' total (``vlasov.py:202-215``)."""
+    keep = np.zeros(len(particles), dtype=bool)
+    scale = np.ones(len(particles))
+    for species in np.unique(particles.species):
+        index = np.flatnonzero(particles.species == species)
+        kept = index[::stride]
+        keep[kept] = True
+        total = np.abs(particles.current[index]).sum()
+        part = np.abs(particles.current[kept]).sum()
+        scale[kept] = total / part if part > 0.0 else 1.0
+    thinned = particles.subset(keep)
+    thinned.current = thinned.current * scale[keep]
+    return thinned
+
+
+class VlasovState:
+    """The last iteration: fields, charge density, trace and history (``vlasov.py:103-124``).
+
+    ``potential`` and ``charge_density`` are host arrays, copied from the device when first
+    read; ``potential_device``, ``charge_density_device`` are the device arrays.
+    """
+
+    def __init__(self, potential, rho, electric, trace, history, plasma) -> None:
+        self.potential_device = potential
+        self.charge_density_device = rho
+        self.electric = electric
+        self._trace = trace
+        self.history = history
+        self.plasma = plasma
+        self.layout = None
+        self._host: dict[str, np.ndarray] = {}
+
+    def _host_copy(self, name: str, array) -> np.ndarray:
+        if name not in self._host:
+            self._host[name] = array.cpu().numpy()
+        return self._host[name]
+
+    @property
+    def potential(self) -> np.ndarray:
+        return self._host_copy("potential", self.potential_device)
+
+    @property
+    def charge_density(self) -> np.ndarray:
+        return self._host_copy("charge_density", self.charge_density_device)
+
+    composite_potential = potential
+    composite_charge_density = charge_density
+
+    @property
+    def trace(self) -> TraceResult:
+        if callable(self._trace):
+            self._trace = self._trace()
+        return self._trace
+
+
+@dataclass
+class _Scalars:
+    """Device scalars read back once per iteration."""
+
+    values: Any = field(default=None)
+
+
+def vlasov_iterate(
+    mesh: IonOpticsMesh,
+    make_particles: Callable[[], tuple[BeamParticles, float]],
+    tracer: BeamTracer,
+    *,
+    iterations: int,
+    plasma: PlasmaModel | NegativeIonPlasmaModel | None = None,
+    compensation: Sequence[Compensation] = (),
+    tolerance: float = 0.0,
+    relaxation: float = 1.0,
+    mixing: str = "linear",
+    anderson_depth: int = 5,
+    coarse_particles: float = 1.0,
+    coarse_tolerance: float = 0.0,
+    field_backend: str = "multigrid",
+    comm: Any = None,
+    refinement: Sequence = (),
+    adaptive: Any = None,
+    self_magnetic: bool = False,
+    callback: Callable[[int, VlasovState], None] | None = None,
+    density_tolerance: float | None = None,
+    poisson: IonOpticsPoisson | None = None,
+) -> VlasovState:
+    """Run at most ``iterations`` Vlasov iterations (``vlasov.py:246-429``).
+
+    Stop when the largest potential change is below ``tolerance`` [V] or, with
+    ``density_tolerance``, when the largest change of the charge density relative to its
+    largest value is below it.  ``mixing`` is ``"linear"`` (``relaxation``) or
+    ``"anderson"``; ``coarse_particles < 1`` traces that share of the trajectories until the
+    potential changes by less than ``coarse_tolerance``.  ``make_particles`` returns the beam
+    and its ``sum J / v``; a beam identical to the last one is not copied to the device
+    again.  ``poisson`` reuses a field solver of this mesh.
+    """
+    import torch
+
+    if mixing not in ("linear", "anderson"):
+        raise ValueError(f"mixing must be 'linear' or 'anderson', got {mixing!r}")
+    if not 0.0 < coarse_particles <= 1.0:
+        raise ValueError(f"coarse_particles must be in (0, 1], got {coarse_particles}")
+    if tuple(refinement) or adaptive is not None or self_magnetic:
+        raise NotImplementedError(
+            "refined boxes, adaptive refinement and the self magnetic field are not part "
+            "of this build"
+        )
+    stride = int(np.ceil(1.0 / coarse_particles - 1e-9))
+    coarse = stride > 1
+    if coarse and not coarse_tolerance > 0.0:
+        raise ValueError("coarse_particles < 1 needs a positive coarse_tolerance")
+    mixer = AndersonMixer(anderson_depth, relaxation) if mixing == "anderson" else None
+    if poisson is None:
+        poisson = IonOpticsPoisson(mesh, backend=field_backend, comm=comm)
+    ctx = _lib.context()
+    arrays = MeshArrays(mesh)
+    nx, ny = mesh.shape
+    dev = "cuda"
+    rho = torch.zeros((nx, ny), dtype=torch.float64, device=dev)
+    phi = torch.zeros((nx, ny), dtype=torch.float64, device=dev)
+    previous = torch.zeros_like(phi)
+    fx = torch.empty((nx + 1, ny), dtype=torch.float64, device=dev)
+    fy = torch.empty((nx, ny + 1), dtype=torch.float64, device=dev)
+    factors = compensation_factors(mesh.x, compensation)
+    column = None if factors is None else torch.from_numpy(factors).to(dev)
+    scalars = torch.zeros(4, dtype=torch.float64, device=dev)
+    region_x = None if plasma is None else plasma.initial_plasma_x
+    engine = tracer.engine()
+    loaded: BeamParticles | None = None
+    history: list[dict[str, float]] = []
+    boltzmann = None
+    j_over_v: float | None = None
+    state: VlasovState | None = None
+    have_potential = False
+    for iteration in range(iterations):
+        previous.copy_(phi)
+        if plasma is not None and iteration == 0:
+            region = lambda x, y: x < region_x  # noqa: E731
+            poisson.solve_device(phi, rho, fixed_region=region,
+                                 fixed_potential=plasma.plasma_potential)  # fmt: skip
+        else:
+            if plasma is not None and boltzmann is None:
+                density = plasma.density if plasma.density is not None else j_over_v
+                boltzmann = plasma.boltzmann(density)
+            if not have_potential:
+                poisson.solve_device(phi, rho)
+            if boltzmann is not None:
+                poisson.solve_device(phi, rho, plasma=boltzmann)
+            else:
+                if have_potential:
+                    poisson.solve_device(phi, rho)
+        _lib.check(_lib.lib().bt_max_abs_diff(ctx.handle, _lib.dptr(phi), _lib.dptr(previous),
+                                              nx * ny, _lib.dptr(scalars)))  # fmt: skip
+        efield = StaggeredElectricField(mesh, phi, arrays=arrays, out=(fx, fy))
+        tracer.electric = efield
+        particles, j_over_v = make_particles()
+        if coarse:
+            potential_change = float(scalars[0]) if have_potential else float("inf")
+            if potential_change < coarse_tolerance:
+                coarse = False
+                if mixer is not None:
+                    mixer.reset()
+        if coarse:
+            particles = thin_particles(particles, stride)
+        if particles is not loaded:
+            engine.load(particles)
+            loaded = particles
+        engine.run(fx, fy)
+        tracer._capacity = engine.capacity
+        if mixer is not None and iteration > 0:
+            deposit = engine.density()
+            if column is not None:
+                deposit = deposit * column[:, None]
+            old = rho.clone()
+            rho.copy_(mixer.update(rho, deposit))
+            scalars[1] = (rho - old).abs().max()
+            scalars[2] = rho.abs().max()
+        else:
+            _lib.check(
+                _lib.lib().bt_vlasov_mix(
+                    ctx.handle, _lib.dptr(engine.charge), _lib.dptr(engine.volumes),
+                    _lib.dptr(column), nx, ny, float(relaxation), int(iteration == 0),
+                    _lib.dptr(rho), _lib.dptr(scalars) + 8,
+                )
+            )  # fmt: skip
+        steps = engine.steps.max() if engine.n else torch.zeros((), dtype=torch.int64)
+        host = scalars.cpu().numpy()
+        change = float(host[0]) if have_potential else float("inf")
+        have_potential = True
+        density_change = float(host[1] / host[2]) if host[2] > 0 else 0.0
+        history.append({
+            "iteration": iteration,
+            "max_potential_change": change,
+            "relative_density_change": density_change if iteration > 0 else float("inf"),
+            "newton_iterations": poisson.newton_iterations,
+            "steps": int(steps),
+            "trajectories": len(particles),
+            "boxes": 1,
+            "max_self_magnetic": 0.0,
+        })  # fmt: skip
+        density_now = engine.density()
+        state = VlasovState(phi, rho, efield, lambda d=density_now: engine.result(d), history,
+                            boltzmann)  # fmt: skip
+        if callback is not None:
+            _ = state.trace  # the buffers are reused by the next trace
+            callback(iteration, state)
+        if not coarse:
+            if change < tolerance:
+                break
+            if density_tolerance is not None and iteration > 0 and density_change < density_tolerance:
+                break
+    assert state is not None
+    return state

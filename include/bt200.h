@@ -130,6 +130,20 @@ int bt_edge_field(bt_ctx *ctx, const double *phi, const int32_t *solid, const ui
                   const double *distance, const double *dx, int64_t nx, int64_t ny,
                   double h, const int32_t extrapolation[4], double *fx, double *fy);
 
+/* -- the per-iteration updates (device pointers) -------------------------------------- */
+
+/* tracer.py:700-705, vlasov.py:176-184 and 389-397: the new density of an iteration.
+ * deposit = charge / volumes (both (nx, ny)), times column_factor[i] (nx,) where given
+ * (the space-charge compensation of node column i, NULL for none); then rho <- deposit
+ * (first != 0) or (1 - relaxation) rho + relaxation deposit.  stats (device, 2 values):
+ * max |rho_new - rho_old| and max |rho_new|. */
+int bt_vlasov_mix(bt_ctx *ctx, const double *charge, const double *volumes,
+                  const double *column_factor, int64_t nx, int64_t ny, double relaxation,
+                  int32_t first, double *rho, double *stats);
+
+/* vlasov.py:362-366: out (device, 1 value) = max |a - b| over n values. */
+int bt_max_abs_diff(bt_ctx *ctx, const double *a, const double *b, int64_t n, double *out);
+
 /* -- the field solve ----------------------------------------------------------------- */
 
 typedef struct bt_poisson bt_poisson;

@@ -1,0 +1,87 @@
+"""Configurations of the end-to-end cases and the oracle problem of a model."""
+
+from __future__ import annotations
+
+import numpy as np
+from scipy import constants
+
+from beamtracer_b200.config import (
+    BeamOpticsConfig,
+    BeamSpecies,
+    ExtractionPlasma,
+    FieldBCs,
+    FieldBoundaryCondition,
+    GridParams,
+    ObjectParams,
+)
+from oracle import vlasov as oracle_vlasov
+
+
+def diode(*, current_density: float, num_gridpoints=(41, 21), **settings) -> BeamOpticsConfig:
+    """A planar diode: ions from x = 0 (0 V) to x = 10 mm (-1 kV); Neumann y walls.  The
+    case of the reference's ``tests/unit/test_beam_optics.py:27-58``."""
+    neumann = FieldBoundaryCondition.neumann(0.0)
+    return BeamOpticsConfig(
+        grid=GridParams(ndim=2, num_gridpoints=num_gridpoints, lower_bound=(0.0, 0.0),
+                        upper_bound=(10e-3, 5e-3), coordinates="cartesian"),
+        bcs_field=FieldBCs(FieldBoundaryCondition.dirichlet(0.0),
+                           FieldBoundaryCondition.dirichlet(-1000.0), neumann, neumann),
+        beams=[BeamSpecies("H+", current_density, (0.0, 0.0), (0.0, 5e-3), energy=0.01,
+                           transverse_temperature=0.0, num_particles=40)],
+        diagnostic_planes=[9.9e-3],
+        **settings,
+    )  # fmt: skip
+
+
+def child_langmuir_density(d=10e-3, voltage=1000.0) -> float:
+    mass = 1.007276 * constants.atomic_mass
+    return 4 * constants.epsilon_0 / 9 * np.sqrt(2 * constants.e / mass) * voltage**1.5 / d**2
+
+
+def plate(x0, x1, r0, r1, voltage) -> ObjectParams:
+    """A plate around the axis from radius r0 outwards between x0 and x1."""
+    return ObjectParams(type="aperture2d", axis=0, position=0.0,
+                        vertices=((x0, r0), (x0, r1), (x1, r1), (x1, r0)),
+                        bc_type="dirichlet", bc_value=voltage)  # fmt: skip
+
+
+def extraction(sign: float = 1.0, **settings) -> BeamOpticsConfig:
+    """Ions extracted through a round aperture from a plasma (the reference's
+    ``tests/unit/test_beam_optics.py:211-261``), cylindrical 81 x 31."""
+    plasma_potential, voltage = 5.0 * sign, -2000.0 * sign
+    neumann = FieldBoundaryCondition.neumann(0.0)
+    return BeamOpticsConfig(
+        grid=GridParams(ndim=2, num_gridpoints=(81, 31), lower_bound=(0.0, 0.0),
+                        upper_bound=(8e-3, 3e-3), coordinates="cylindrical"),
+        bcs_field=FieldBCs(FieldBoundaryCondition.dirichlet(plasma_potential),
+                           FieldBoundaryCondition.dirichlet(voltage), neumann, neumann),
+        objects={"pg": plate(0.5e-3, 1.0e-3, 1.0e-3, 3.1e-3, 0.0),
+                 "eg": plate(3.0e-3, 4.0e-3, 1.2e-3, 3.1e-3, voltage)},
+        beams=[BeamSpecies("ion", 50.0, (0.0, 0.0), (0.0, 0.9e-3), charge=sign, mass=1.0,
+                           energy=5.0, transverse_temperature=0.5, num_particles=100)],
+        plasma=ExtractionPlasma(5.0, plasma_potential, 0.6e-3),
+        **{"iterations": 30, "tolerance": 1e-4, "relaxation": 0.8,
+           "diagnostic_planes": [7.5e-3], **settings},
+    )  # fmt: skip
+
+
+def oracle_problem(model) -> oracle_vlasov.Problem:
+    """The oracle's description of a `BeamOptics` model's mesh, electrodes and trace."""
+    from beamtracer_b200.mesh import FACES
+    from beamtracer_b200.tracer import INTEGRATORS, electrode_lookup, geometry_code
+
+    mesh = model.mesh
+    cells, subcells = electrode_lookup(mesh)
+    neumann = tuple(0.0 if mesh.faces[f].kind != "neumann" else float(mesh.faces[f].value)
+                    for f in FACES)  # fmt: skip
+    config = model.config
+    return oracle_vlasov.Problem(
+        shape=mesh.shape, x=np.asarray(mesh.x, float), h=mesh.h, origin=mesh.origin,
+        logical_origin=mesh.logical_origin, logical_upper=mesh.logical_upper,
+        geometry=geometry_code(mesh), graded=mesh.graded, fixed=mesh.fixed,
+        fixed_value=mesh.fixed_value, solid=mesh.solid, near_solid=mesh.near_solid,
+        distance=mesh.distance, neumann=neumann, cells=cells, subcells=subcells,
+        inside_solid=mesh.inside_solid, planes=tuple(config.diagnostic_planes),
+        integrator=INTEGRATORS.index(config.integrator), step_fraction=config.step_fraction,
+        max_steps=config.max_steps,
+    )  # fmt: skip
