@@ -80,6 +80,10 @@ SIGNATURES: dict[str, list] = {
     "bt_ctx_destroy": [P],
     "bt_ctx_set_stream": [P, P],
     "bt_ctx_synchronize": [P],
+    "bt_ctx_set_timing": [P, I32],
+    "bt_ctx_read_timer": [P, ctypes.c_char_p, ctypes.POINTER(F64), ctypes.POINTER(I64)],
+    "bt_ctx_reset_timers": [P],
+    "bt_ctx_launch_count": [P, ctypes.POINTER(I64)],
     "bt_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "bt_version": [],
     "bt_staggered_field_2d": [P, P, P, I64, P, P, I64, I64, F64, F64, F64, P, P],
@@ -148,6 +152,26 @@ class Context:
     def use_stream(self, stream: int | None) -> None:
         """Queue work on ``stream`` (a ``cudaStream_t`` as an int; None: the context's own)."""
         check(lib().bt_ctx_set_stream(self.handle, P(stream) if stream else None))
+
+    def set_timing(self, on: bool) -> None:
+        """Record the launch times of the library's kernels (CUDA events on its stream)."""
+        check(lib().bt_ctx_set_timing(self.handle, int(bool(on))))
+
+    def read_timer(self, name: str) -> tuple[float, int]:
+        """The summed launch time [ms] and the launches of a timed kernel since the reset."""
+        ms, count = F64(), I64()
+        check(lib().bt_ctx_read_timer(self.handle, name.encode(), ctypes.byref(ms),
+                                      ctypes.byref(count)))  # fmt: skip
+        return ms.value, count.value
+
+    def launch_count(self) -> int:
+        """The kernels this context has launched since its creation."""
+        count = I64()
+        check(lib().bt_ctx_launch_count(self.handle, ctypes.byref(count)))
+        return count.value
+
+    def reset_timers(self) -> None:
+        check(lib().bt_ctx_reset_timers(self.handle))
 
     def synchronize(self) -> None:
         check(lib().bt_ctx_synchronize(self.handle))

@@ -57,7 +57,39 @@ void HostBuffer::release() {
     bytes = 0;
 }
 
+Timed::Timed(bt_ctx *c, const char *name) : ctx(c) {
+    if (!ctx || !ctx->timing) return;
+    timer = &ctx->timers[name];
+    if (!timer->spare.empty()) {
+        ev = timer->spare.back();
+        timer->spare.pop_back();
+    } else {
+        cudaEventCreate(&ev.first);
+        cudaEventCreate(&ev.second);
+    }
+    cudaEventRecord(ev.first, ctx->stream);
+}
+
+Timed::~Timed() {
+    if (!timer) return;
+    cudaEventRecord(ev.second, ctx->stream);
+    timer->pending.push_back(ev);
+}
+
 namespace {
+
+void collect(Timer &t) {
+    for (auto &e : t.pending) {
+        cudaEventSynchronize(e.second);
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, e.first, e.second) == cudaSuccess) {
+            t.total_ms += ms;
+            t.launches += 1;
+        }
+        t.spare.push_back(e);
+    }
+    t.pending.clear();
+}
 
 __device__ __forceinline__ double clamped_bilinear(const double *__restrict__ f, i64 nj,
                                                    double s, double t, i64 imax, i64 jmax) {
@@ -128,11 +160,59 @@ int bt_ctx_create(int device, bt_ctx **out) {
     });
 }
 
+int bt_ctx_set_timing(bt_ctx *ctx, int on) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx, "ctx: null context");
+        ctx->timing = on != 0;
+    });
+}
+
+int bt_ctx_read_timer(bt_ctx *ctx, const char *name, double *total_ms, int64_t *launches) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx && name, "ctx: null argument");
+        auto it = ctx->timers.find(name);
+        double ms = 0.0;
+        int64_t count = 0;
+        if (it != ctx->timers.end()) {
+            bt::collect(it->second);
+            ms = it->second.total_ms;
+            count = it->second.launches;
+        }
+        if (total_ms) *total_ms = ms;
+        if (launches) *launches = count;
+    });
+}
+
+int bt_ctx_launch_count(bt_ctx *ctx, int64_t *count) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx && count, "ctx: null argument");
+        *count = ctx->launch_count;
+    });
+}
+
+int bt_ctx_reset_timers(bt_ctx *ctx) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx, "ctx: null context");
+        for (auto &kv : ctx->timers) {
+            bt::collect(kv.second);
+            kv.second.total_ms = 0.0;
+            kv.second.launches = 0;
+        }
+    });
+}
+
 int bt_ctx_destroy(bt_ctx *ctx) {
     return bt::guarded([&] {
         if (!ctx) return;
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
+        for (auto &kv : ctx->timers) {
+            bt::collect(kv.second);
+            for (auto &e : kv.second.spare) {
+                cudaEventDestroy(e.first);
+                cudaEventDestroy(e.second);
+            }
+        }
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         delete ctx;
     });
@@ -161,8 +241,8 @@ int bt_staggered_field_2d(bt_ctx *ctx, const double *px, const double *py, int64
         BT_REQUIRE(nx >= 2 && ny >= 2, "gather: the mesh needs at least 2 x 2 nodes");
         if (n == 0) return;
         BT_REQUIRE(px && py && fx && fy && ex && ey, "gather: null array");
-        bt::staggered_field<<<bt::blocks_for(n, 256), 256, 0, ctx->stream>>>(
-            px, py, n, fx, fy, nx, ny, origin_x, origin_y, h, ex, ey);
+        bt::Timed timed(ctx, "staggered_field_2d");
+        BT_LAUNCH(ctx, bt::staggered_field, bt::blocks_for(n, 256), 256, 0, ctx->stream, px, py, n, fx, fy, nx, ny, origin_x, origin_y, h, ex, ey);
         BT_CHECK_LAUNCH();
     });
 }

@@ -6,7 +6,9 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/bt200.h"
@@ -33,6 +35,13 @@ struct Error {
     } while (0)
 
 #define BT_CHECK_LAUNCH() BT_CUDA(cudaGetLastError())
+
+// Launch a kernel on the context's behalf and count it (one statement).
+#define BT_LAUNCH(ctx, kernel, grid, block, smem, stream, ...)                              \
+    do {                                                                                  \
+        ++(ctx)->launch_count;                                                            \
+        kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                       \
+    } while (0)
 
 #define BT_REQUIRE(cond, msg)                                                             \
     do {                                                                                  \
@@ -99,8 +108,20 @@ struct TraceScratch {
 
 }  // namespace bt
 
+namespace bt {
+// The launch times of one named kernel (or group of launches): CUDA events recorded on
+// the context's stream around each launch, read back and summed on request.
+struct Timer {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending, spare;
+    double total_ms = 0.0;
+    i64 launches = 0;
+};
+}  // namespace bt
+
 struct bt_ctx {
     int device = 0;
+    bool timing = false;
+    std::map<std::string, bt::Timer> timers;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     int num_sms = 148;
@@ -108,10 +129,21 @@ struct bt_ctx {
     bt::TraceScratch trace;
     bt::HostBuffer host;
     bt::Buffer reduce_partial;  // per-block partial results of the device reductions
+    i64 launch_count = 0;       // kernels launched on the context since its creation
     i64 last_windows = 0, last_records = 0, last_flushes = 0;
 };
 
 namespace bt {
+
+// Records the launches between its construction and destruction under `name` when the
+// context's timing is on.
+struct Timed {
+    bt_ctx *ctx;
+    Timer *timer = nullptr;
+    std::pair<cudaEvent_t, cudaEvent_t> ev{};
+    Timed(bt_ctx *c, const char *name);
+    ~Timed();
+};
 
 // Run `body` and map exceptions to an error code and message.
 template <class F>

@@ -319,10 +319,10 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, int key_bits,
     const int passes = (key_bits + 7) / 8;
     for (int p = 0; p < passes; ++p) {
         const int shift = 8 * p;
-        radix_hist<<<nblocks, kThreads, 0, st>>>(src_k, n, shift, hist, nblocks);
-        radix_row_scan<<<kRadix, kThreads, 0, st>>>(hist, offs, totals, nblocks);
-        radix_digit_base<<<1, kThreads, 0, st>>>(totals, digit);
-        radix_scatter<<<nblocks, kThreads, 0, st>>>(src_k, src_v, n, shift, offs, digit,
+        BT_LAUNCH(ctx, radix_hist, nblocks, kThreads, 0, st, src_k, n, shift, hist, nblocks);
+        BT_LAUNCH(ctx, radix_row_scan, kRadix, kThreads, 0, st, hist, offs, totals, nblocks);
+        BT_LAUNCH(ctx, radix_digit_base, 1, kThreads, 0, st, totals, digit);
+        BT_LAUNCH(ctx, radix_scatter, nblocks, kThreads, 0, st, src_k, src_v, n, shift, offs, digit,
                                                     nblocks, dst_k, dst_v);
         BT_CHECK_LAUNCH();
         src_k = dst_k;
@@ -354,12 +354,9 @@ void deposit_records(bt_ctx *ctx, const uint32_t *keys, const double *u, const d
     uint8_t *flags = s.warp_flags.as<uint8_t>((size_t)2 * n_warps);
     BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * layout.n_nodes, st));
     const int threads = 256;
-    seg_reduce_warps<<<blocks_for(n_warps * 32, threads), threads, 0, st>>>(
-        sk, sv, u, w, q, n_records, sentinel, cells, first, last, flags, flags + n_warps);
-    seg_reduce_chains<<<blocks_for(n_warps, threads), threads, 0, st>>>(
-        sk, n_warps, cells, first, last, flags, flags + n_warps);
-    node_accumulate<<<blocks_for(layout.n_nodes, threads), threads, 0, st>>>(
-        cells, charge, layout.patch_int, layout.n_patches, layout.nx, layout.ny,
+    BT_LAUNCH(ctx, seg_reduce_warps, blocks_for(n_warps * 32, threads), threads, 0, st, sk, sv, u, w, q, n_records, sentinel, cells, first, last, flags, flags + n_warps);
+    BT_LAUNCH(ctx, seg_reduce_chains, blocks_for(n_warps, threads), threads, 0, st, sk, n_warps, cells, first, last, flags, flags + n_warps);
+    BT_LAUNCH(ctx, node_accumulate, blocks_for(layout.n_nodes, threads), threads, 0, st, cells, charge, layout.patch_int, layout.n_patches, layout.nx, layout.ny,
         layout.n_nodes);
     BT_CHECK_LAUNCH();
 }
@@ -380,8 +377,7 @@ extern "C" int bt_deposit_trajectories_2d(bt_ctx *ctx, const double *px, const d
         bt::DepositScratch &s = ctx->deposit;
         uint32_t *keys = s.keys.as<uint32_t>(n);
         double *U = s.u.as<double>(n), *W = s.w.as<double>(n), *Q = s.q.as<double>(n);
-        bt::point_records<<<bt::blocks_for(n, 256), 256, 0, ctx->stream>>>(
-            px, py, q, n, origin_x, origin_y, h, cylindrical, nx, ny, keys, U, W, Q);
+        BT_LAUNCH(ctx, bt::point_records, bt::blocks_for(n, 256), 256, 0, ctx->stream, px, py, q, n, origin_x, origin_y, h, cylindrical, nx, ny, keys, U, W, Q);
         BT_CHECK_LAUNCH();
         // the records' keys live in `keys`; the sort reads them and writes elsewhere
         bt::NodeLayout layout{nullptr, 1, nx, ny, nx * ny};

@@ -97,10 +97,9 @@ extern "C" int bt_edge_field(bt_ctx *ctx, const double *phi, const int32_t *soli
         const i64 nn = nx * ny;
         bt::Line lx{phi, solid, near, distance, distance + nn, dx, h, nx, ny};
         bt::Line ly{phi, solid, near, distance + 2 * nn, distance + 3 * nn, nullptr, h, ny, 1};
-        bt::edge_field_x<<<bt::blocks_for((nx + 1) * ny, 256), 256, 0, ctx->stream>>>(
-            lx, ny, extrapolation[0], extrapolation[1], fx);
-        bt::edge_field_y<<<bt::blocks_for(nx * (ny + 1), 256), 256, 0, ctx->stream>>>(
-            ly, nx, extrapolation[2], extrapolation[3], fy);
+        bt::Timed timed(ctx, "edge_field");
+        BT_LAUNCH(ctx, bt::edge_field_x, bt::blocks_for((nx + 1) * ny, 256), 256, 0, ctx->stream, lx, ny, extrapolation[0], extrapolation[1], fx);
+        BT_LAUNCH(ctx, bt::edge_field_y, bt::blocks_for(nx * (ny + 1), 256), 256, 0, ctx->stream, ly, nx, extrapolation[2], extrapolation[3], fy);
         BT_CHECK_LAUNCH();
     });
 }

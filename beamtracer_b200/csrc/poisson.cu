@@ -629,8 +629,7 @@ void build_operator(bt_poisson *p) {
     cudaStream_t st = p->ctx->stream;
     Level &L = p->levels[0];
     const i64 n = p->n;
-    build_fine<<<blocks_for(n, 256), 256, 0, st>>>(
-        p->nx, p->ny, p->x.as<double>(p->nx), p->h, p->cyl, p->fixed_eff.as<uint8_t>(n),
+    BT_LAUNCH(p->ctx, build_fine, blocks_for(n, 256), 256, 0, st, p->nx, p->ny, p->x.as<double>(p->nx), p->h, p->cyl, p->fixed_eff.as<uint8_t>(n),
         p->distance.as<double>(4 * n), p->neumann[0], p->neumann[1], p->neumann[2],
         p->neumann[3], L.c4.as<double>(4 * n), L.base.as<double>(n), p->src.as<double>(n),
         L.weight.as<double>(n), L.active.as<uint8_t>(n));
@@ -643,19 +642,19 @@ void build_operator(bt_poisson *p) {
 void build_hierarchy(bt_poisson *p, const double *reaction) {
     cudaStream_t st = p->ctx->stream;
     Level &L0 = p->levels[0];
-    add_diag<<<blocks_for(p->n, 256), 256, 0, st>>>(p->n, L0.base.as<double>(p->n), reaction,
+    BT_LAUNCH(p->ctx, add_diag, blocks_for(p->n, 256), 256, 0, st, p->n, L0.base.as<double>(p->n), reaction,
                                                     L0.active.as<uint8_t>(p->n),
                                                     L0.diag.as<double>(p->n));
     for (size_t l = 0; l + 1 < p->levels.size(); ++l) {
         Level &L = p->levels[l], &C = p->levels[l + 1];
         Fine F = fine_of(L, C, l == 0);
-        galerkin<<<blocks_for(C.n, 128), 128, 0, st>>>(F, C.a9.as<double>(9 * C.n),
+        BT_LAUNCH(p->ctx, galerkin, blocks_for(C.n, 128), 128, 0, st, F, C.a9.as<double>(9 * C.n),
                                                         C.active.as<uint8_t>(C.n));
     }
     Level &Lc = p->levels.back();
     int *status = p->status.as<int>(1);
     BT_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-    coarsest_invert<<<1, 256, 0, st>>>(Lc.nx, Lc.ny, Lc.a9.as<double>(9 * Lc.n),
+    BT_LAUNCH(p->ctx, coarsest_invert, 1, 256, 0, st, Lc.nx, Lc.ny, Lc.a9.as<double>(9 * Lc.n),
                                        p->inv.as<double>(Lc.n * Lc.n), status);
     BT_CHECK_LAUNCH();
     p->built = true;
@@ -668,7 +667,7 @@ void vcycle(bt_poisson *p, size_t l) {
     Level &L = p->levels[l];
     const int T = 256;
     if (l + 1 == p->levels.size()) {
-        coarsest_apply<<<1, kCoarsest, 0, st>>>((int)L.n, p->inv.as<double>(L.n * L.n),
+        BT_LAUNCH(p->ctx, coarsest_apply, 1, kCoarsest, 0, st, (int)L.n, p->inv.as<double>(L.n * L.n),
                                                L.b.as<double>(L.n), L.x.as<double>(L.n));
         return;
     }
@@ -681,33 +680,33 @@ void vcycle(bt_poisson *p, size_t l) {
         const i64 per = L.nx * ((L.ny + 1) / 2);
         for (int s = 0; s < sweeps; ++s)
             for (int c = 0; c < 2; ++c)
-                smooth5<<<blocks_for(per, T), T, 0, st>>>(L.nx, L.ny, c4, dg, act, b, x, c);
-        apply5<<<blocks_for(L.n, T), T, 0, st>>>(L.nx, L.ny, c4, dg, act, x, b, r);
+                BT_LAUNCH(p->ctx, smooth5, blocks_for(per, T), T, 0, st, L.nx, L.ny, c4, dg, act, b, x, c);
+        BT_LAUNCH(p->ctx, apply5, blocks_for(L.n, T), T, 0, st, L.nx, L.ny, c4, dg, act, x, b, r);
     } else {
         const double *a9 = L.a9.as<double>(9 * L.n);
         const i64 per = ((L.nx + 1) / 2) * ((L.ny + 1) / 2);
         for (int s = 0; s < sweeps; ++s)
             for (int c = 0; c < 4; ++c)
-                smooth9<<<blocks_for(per, T), T, 0, st>>>(L.nx, L.ny, a9, act, b, x, c);
-        residual9<<<blocks_for(L.n, T), T, 0, st>>>(L.nx, L.ny, a9, act, x, b, r);
+                BT_LAUNCH(p->ctx, smooth9, blocks_for(per, T), T, 0, st, L.nx, L.ny, a9, act, b, x, c);
+        BT_LAUNCH(p->ctx, residual9, blocks_for(L.n, T), T, 0, st, L.nx, L.ny, a9, act, x, b, r);
     }
     Fine F = fine_of(L, C, l == 0);
-    restrict_residual<<<blocks_for(C.n, T), T, 0, st>>>(F, r, C.b.as<double>(C.n),
+    BT_LAUNCH(p->ctx, restrict_residual, blocks_for(C.n, T), T, 0, st, F, r, C.b.as<double>(C.n),
                                                           C.x.as<double>(C.n));
     vcycle(p, l + 1);
-    prolong_add<<<blocks_for(L.n, T), T, 0, st>>>(F, C.x.as<double>(C.n), x);
+    BT_LAUNCH(p->ctx, prolong_add, blocks_for(L.n, T), T, 0, st, F, C.x.as<double>(C.n), x);
     if (l == 0) {
         const double *c4 = L.c4.as<double>(4 * L.n), *dg = L.diag.as<double>(L.n);
         const i64 per = L.nx * ((L.ny + 1) / 2);
         for (int s = 0; s < sweeps; ++s)
             for (int c = 1; c >= 0; --c)
-                smooth5<<<blocks_for(per, T), T, 0, st>>>(L.nx, L.ny, c4, dg, act, b, x, c);
+                BT_LAUNCH(p->ctx, smooth5, blocks_for(per, T), T, 0, st, L.nx, L.ny, c4, dg, act, b, x, c);
     } else {
         const double *a9 = L.a9.as<double>(9 * L.n);
         const i64 per = ((L.nx + 1) / 2) * ((L.ny + 1) / 2);
         for (int s = 0; s < sweeps; ++s)
             for (int c = 3; c >= 0; --c)
-                smooth9<<<blocks_for(per, T), T, 0, st>>>(L.nx, L.ny, a9, act, b, x, c);
+                BT_LAUNCH(p->ctx, smooth9, blocks_for(per, T), T, 0, st, L.nx, L.ny, a9, act, b, x, c);
     }
     BT_CHECK_LAUNCH();
 }
@@ -724,8 +723,7 @@ void precondition(bt_poisson *p, const double *v, double *z) {
 
 void apply(bt_poisson *p, const double *x, double *y) {
     Level &L = p->levels[0];
-    apply5<<<blocks_for(L.n, 256), 256, 0, p->ctx->stream>>>(
-        L.nx, L.ny, L.c4.as<double>(4 * L.n), L.diag.as<double>(L.n),
+    BT_LAUNCH(p->ctx, apply5, blocks_for(L.n, 256), 256, 0, p->ctx->stream, L.nx, L.ny, L.c4.as<double>(4 * L.n), L.diag.as<double>(L.n),
         L.active.as<uint8_t>(L.n), x, nullptr, y);
 }
 
@@ -738,7 +736,7 @@ double read_scalar(bt_poisson *p, const double *dev) {
 
 double norm2(bt_poisson *p, const double *v) {
     double *s = p->scalars.as<double>(8);
-    multi_dot<<<1, 256, 0, p->ctx->stream>>>(v, v, p->n, s);
+    BT_LAUNCH(p->ctx, multi_dot, 1, 256, 0, p->ctx->stream, v, v, p->n, s);
     return std::sqrt(read_scalar(p, s));
 }
 
@@ -766,7 +764,7 @@ int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_it
     while (beta > abs_tol && total < max_iter && beta < 0.5 * previous) {
         previous = beta;
         if (!std::isfinite(beta)) throw Error{BT_ERR_NOCONV, "field solve: the residual is not finite"};
-        scale_into<<<blocks_for(n, 256), 256, 0, st>>>(w, 1.0 / beta, n, V);
+        BT_LAUNCH(p->ctx, scale_into, blocks_for(n, 256), 256, 0, st, w, 1.0 / beta, n, V);
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
         int j = 0;
@@ -776,8 +774,8 @@ int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_it
             apply(p, z, w);
             // classical Gram-Schmidt, applied twice
             for (int pass = 0; pass < 2; ++pass) {
-                multi_dot<<<j + 1, 256, 0, st>>>(V, w, n, hdev);
-                orthogonalise<<<blocks_for(n, 256), 256, 0, st>>>(V, hdev, j + 1, n, w);
+                BT_LAUNCH(p->ctx, multi_dot, j + 1, 256, 0, st, V, w, n, hdev);
+                BT_LAUNCH(p->ctx, orthogonalise, blocks_for(n, 256), 256, 0, st, V, hdev, j + 1, n, w);
                 BT_CUDA(cudaMemcpyAsync(host, hdev, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, st));
                 BT_CUDA(cudaStreamSynchronize(st));
                 for (int q = 0; q <= j; ++q) H[q * m + j] = (pass ? H[q * m + j] : 0.0) + host[q];
@@ -785,7 +783,7 @@ int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_it
             const double hn = norm2(p, w);
             H[(j + 1) * m + j] = hn;
             if (hn > 0.0)
-                scale_into<<<blocks_for(n, 256), 256, 0, st>>>(w, 1.0 / hn, n, V + (i64)(j + 1) * n);
+                BT_LAUNCH(p->ctx, scale_into, blocks_for(n, 256), 256, 0, st, w, 1.0 / hn, n, V + (i64)(j + 1) * n);
             for (int q = 0; q < j; ++q) {
                 const double a = H[q * m + j], b = H[(q + 1) * m + j];
                 H[q * m + j] = cs[q] * a + sn[q] * b;
@@ -810,10 +808,10 @@ int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_it
             y[q] = s / H[q * m + q];
         }
         BT_CUDA(cudaMemcpyAsync(ydev, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, st));
-        combine<<<blocks_for(n, 256), 256, 0, st>>>(Z, ydev, j, n, d);
+        BT_LAUNCH(p->ctx, combine, blocks_for(n, 256), 256, 0, st, Z, ydev, j, n, d);
         // the true residual r0 - A d
         apply(p, d, w);
-        subtract_from<<<blocks_for(n, 256), 256, 0, st>>>(r0, n, w);
+        BT_LAUNCH(p->ctx, subtract_from, blocks_for(n, 256), 256, 0, st, r0, n, w);
         BT_CHECK_LAUNCH();
         beta = norm2(p, w);
     }
@@ -932,16 +930,15 @@ extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, d
         double *reaction = p->reaction.as<double>(n);
         double *scal = p->scalars.as<double>(16);
         const int max_cycles = 4000;
-        bt::prepare<<<bt::blocks_for(n, 256), 256, 0, st>>>(
-            n, rho, p->src.as<double>(n), L0.active.as<uint8_t>(n), p->value_eff.as<double>(n),
+        bt::Timed timed(p->ctx, "field_solve");
+        BT_LAUNCH(p->ctx, bt::prepare, bt::blocks_for(n, 256), 256, 0, st, n, rho, p->src.as<double>(n), L0.active.as<uint8_t>(n), p->value_eff.as<double>(n),
             b, phi);
         BT_CHECK_LAUNCH();
         int total_cycles = 0, steps = 0;
         if (!(amplitude > 0.0)) {
             if (!p->built || p->reaction_on) bt::build_hierarchy(p, nullptr);
             // r0 = b - A phi; the tolerance is relative to the larger of |b| and |r0|
-            bt::apply5<<<bt::blocks_for(n, 256), 256, 0, st>>>(
-                p->nx, p->ny, L0.c4.as<double>(4 * n), L0.diag.as<double>(n),
+            BT_LAUNCH(p->ctx, bt::apply5, bt::blocks_for(n, 256), 256, 0, st, p->nx, p->ny, L0.c4.as<double>(4 * n), L0.diag.as<double>(n),
                 L0.active.as<uint8_t>(n), phi, b, r0);
             BT_CHECK_LAUNCH();
             const double scale = std::max(bt::norm2(p, b), bt::norm2(p, r0));
@@ -949,7 +946,7 @@ extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, d
             double left = 0.0;
             const double goal = tol * (scale > 0.0 ? scale : 1.0);
             total_cycles = bt::gmres(p, r0, d, goal, max_cycles, &left);
-            bt::add_into<<<bt::blocks_for(n, 256), 256, 0, st>>>(d, n, phi);
+            BT_LAUNCH(p->ctx, bt::add_into, bt::blocks_for(n, 256), 256, 0, st, d, n, phi);
             BT_CHECK_LAUNCH();
             // a residual stalled within 1e4 of the goal is the floor of its own rounding
             if (!(left <= 1e4 * goal))
@@ -960,8 +957,7 @@ extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, d
             const int limit = max_newton > 0 ? max_newton : 100;
             bool converged = false;
             for (steps = 1; steps <= limit; ++steps) {
-                bt::boltzmann<<<bt::blocks_for(n, 256), 256, 0, st>>>(
-                    p->nx, p->ny, L0.c4.as<double>(4 * n), L0.base.as<double>(n),
+                BT_LAUNCH(p->ctx, bt::boltzmann, bt::blocks_for(n, 256), 256, 0, st, p->nx, p->ny, L0.c4.as<double>(4 * n), L0.base.as<double>(n),
                     L0.active.as<uint8_t>(n), phi, b, amplitude, temperature, up, (double)sign,
                     r0, reaction);
                 BT_CHECK_LAUNCH();
@@ -971,8 +967,8 @@ extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, d
                 double left = 0.0;
                 total_cycles += bt::gmres(p, r0, d, tol * (fnorm > 0.0 ? fnorm : 1.0),
                                           max_cycles, &left);
-                bt::add_into<<<bt::blocks_for(n, 256), 256, 0, st>>>(d, n, phi);
-                bt::max_abs<<<1, 256, 0, st>>>(d, n, scal + 8);
+                BT_LAUNCH(p->ctx, bt::add_into, bt::blocks_for(n, 256), 256, 0, st, d, n, phi);
+                BT_LAUNCH(p->ctx, bt::max_abs, 1, 256, 0, st, d, n, scal + 8);
                 BT_CHECK_LAUNCH();
                 const double change = bt::read_scalar(p, scal + 8);
                 if (!std::isfinite(change))

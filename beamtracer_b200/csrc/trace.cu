@@ -534,6 +534,7 @@ extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, 
         int64_t n_act = a.n_active, used = 0;
         auto flush = [&] {
             if (used == 0) return;
+            bt::Timed timed(ctx, "deposit");
             bt::deposit_records(ctx, keys, RU, RW, RQ, used, sentinel, a.charge, layout);
             ctx->last_records += used;
             ctx->last_flushes += 1;
@@ -542,15 +543,17 @@ extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, 
         while (n_act > 0) {
             const int64_t need = n_act * (int64_t)S;
             if (used + need > capacity) flush();
-            bt::trace_window<<<bt::blocks_for(n_act, 128), 128, 0, st>>>(
-                tr, act_a, n_act, S, keys + used, RU + used, RW + used, RQ + used, sentinel);
+            {
+                bt::Timed timed(ctx, "trace_window");
+                BT_LAUNCH(ctx, bt::trace_window, bt::blocks_for(n_act, 128), 128, 0, st, tr, act_a, n_act, S, keys + used, RU + used, RW + used, RQ + used, sentinel);
+            }
             BT_CHECK_LAUNCH();
             used += need;
             ctx->last_windows += 1;
             const int nb = (int)bt::blocks_for(n_act, bt::kCompact);
-            bt::count_alive<<<nb, bt::kCompact, 0, st>>>(act_a, n_act, a.status, block_counts);
-            bt::scan_counts<<<1, 32, 0, st>>>(block_counts, nb, n_alive_dev);
-            bt::scatter_alive<<<nb, bt::kCompact, 0, st>>>(act_a, n_act, a.status, block_counts,
+            BT_LAUNCH(ctx, bt::count_alive, nb, bt::kCompact, 0, st, act_a, n_act, a.status, block_counts);
+            BT_LAUNCH(ctx, bt::scan_counts, 1, 32, 0, st, block_counts, nb, n_alive_dev);
+            BT_LAUNCH(ctx, bt::scatter_alive, nb, bt::kCompact, 0, st, act_a, n_act, a.status, block_counts,
                                                            act_b);
             BT_CHECK_LAUNCH();
             BT_CUDA(cudaMemcpyAsync(n_alive_host, n_alive_dev, sizeof(int64_t),

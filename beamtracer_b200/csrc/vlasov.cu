@@ -80,9 +80,9 @@ extern "C" int bt_vlasov_mix(bt_ctx *ctx, const double *charge, const double *vo
         BT_REQUIRE(ctx && charge && volumes && rho && stats, "vlasov mix: null argument");
         BT_REQUIRE(nx > 0 && ny > 0, "vlasov mix: empty mesh");
         double *partial = ctx->reduce_partial.as<double>(2 * bt::kReduceBlocks);
-        bt::mix<<<bt::kReduceBlocks, bt::kReduceThreads, 0, ctx->stream>>>(
-            charge, volumes, column_factor, nx, ny, relaxation, first, rho, partial);
-        bt::finish_max<<<1, bt::kReduceThreads, 0, ctx->stream>>>(partial, bt::kReduceBlocks, 2, stats);
+        bt::Timed timed(ctx, "vlasov_mix");
+        BT_LAUNCH(ctx, bt::mix, bt::kReduceBlocks, bt::kReduceThreads, 0, ctx->stream, charge, volumes, column_factor, nx, ny, relaxation, first, rho, partial);
+        BT_LAUNCH(ctx, bt::finish_max, 1, bt::kReduceThreads, 0, ctx->stream, partial, bt::kReduceBlocks, 2, stats);
         BT_CHECK_LAUNCH();
     });
 }
@@ -92,8 +92,8 @@ extern "C" int bt_max_abs_diff(bt_ctx *ctx, const double *a, const double *b, in
     return bt::guarded([&] {
         BT_REQUIRE(ctx && a && b && out, "max abs diff: null argument");
         double *partial = ctx->reduce_partial.as<double>(2 * bt::kReduceBlocks);
-        bt::diff_max<<<bt::kReduceBlocks, bt::kReduceThreads, 0, ctx->stream>>>(a, b, n, partial);
-        bt::finish_max<<<1, bt::kReduceThreads, 0, ctx->stream>>>(partial, bt::kReduceBlocks, 1, out);
+        BT_LAUNCH(ctx, bt::diff_max, bt::kReduceBlocks, bt::kReduceThreads, 0, ctx->stream, a, b, n, partial);
+        BT_LAUNCH(ctx, bt::finish_max, 1, bt::kReduceThreads, 0, ctx->stream, partial, bt::kReduceBlocks, 1, out);
         BT_CHECK_LAUNCH();
     });
 }

@@ -286,9 +286,9 @@ def vlasov_iterate(
                     mixer.reset()
         if coarse:
             particles = thin_particles(particles, stride)
-        if particles is not loaded:
+        if particles is not loaded and particles is not engine.particles:
             engine.load(particles)
-            loaded = particles
+        loaded = particles
         engine.run(fx, fy)
         tracer._capacity = engine.capacity
         if mixer is not None and iteration > 0:
@@ -307,8 +307,11 @@ def vlasov_iterate(
                     _lib.dptr(rho), _lib.dptr(scalars) + 8,
                 )
             )  # fmt: skip
-        steps = engine.steps.max() if engine.n else torch.zeros((), dtype=torch.int64)
+        if engine.n:
+            scalars[3] = engine.steps.max().to(torch.float64)
+            steps_sum = engine.steps.sum()
         host = scalars.cpu().numpy()
+        total_steps = int(steps_sum) if engine.n else 0
         change = float(host[0]) if have_potential else float("inf")
         have_potential = True
         density_change = float(host[1] / host[2]) if host[2] > 0 else 0.0
@@ -317,7 +320,8 @@ def vlasov_iterate(
             "max_potential_change": change,
             "relative_density_change": density_change if iteration > 0 else float("inf"),
             "newton_iterations": poisson.newton_iterations,
-            "steps": int(steps),
+            "steps": int(host[3]) if engine.n else 0,
+            "total_steps": total_steps,
             "trajectories": len(particles),
             "boxes": 1,
             "max_self_magnetic": 0.0,

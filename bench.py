@@ -1,0 +1,327 @@
+"""Benchmark: converged Vlasov solves per second of the einzel lens at 801 x 201.
+
+The workload is the einzel lens of the reference's configuration list at scale: a
+cylindrical (x, r) mesh of 801 x 201 nodes on 80 x 20 mm, three plates at 0 / V_mid / 0
+(V_mid seeded uniform in 5-9 kV), Neumann faces, a 10 keV H+ beam of 1 mA in 20,000 rings
+(seeded Gaussian radius, rms 2 mm cut at 4 mm, 5 mrad rms angle, 2 mm mrad emittance),
+planes at 70 and 79 mm; the reference's iteration defaults (at most 20 iterations, linear
+mixing with relaxation 1, until the potential changes by less than 1 mV).  A step is one
+converged solve from a zero charge density.
+
+- ``value``: steps per second with the mesh, operator and beam resident on the device
+  (CUDA events around each step on the launching stream; L2 flushed between steps);
+- ``e2e``: the same through the public call ``BeamOptics(config).run()`` plus
+  ``beam_moments()``, from host inputs to host results;
+- ``roofline``: the dominant kernel's launches timed live (CUDA events) against its
+  algorithmic work;
+- ``cpu_baseline``: the oracle (the reference's kernel restated in C, OpenMP over every
+  host core, and SciPy's sparse LU for the field) on one iteration of the same workload,
+  scaled by the iterations of a converged solve.
+
+``--impl reference`` times that CPU path alone (the reference's Pyccel build cannot be
+made here).  Under torchrun every rank solves its own lens (weak scaling, no collective).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "converged einzel-lens Vlasov solves/s (801x201 cyl., 20k rings)"
+UNIT = "solves/s"
+WORKLOAD = "einzel lens 801x201 cylindrical, 20,000 rings, 3 plates, tol 1 mV"
+#: FP64 operations of one RK4 step of the trace kernel, counted from its source
+#: (trace.cu): four field gathers (2 x 3 bilinear lerps of 3 ops + cell arithmetic),
+#: the stage updates, the step size, the Hermite midpoint and the deposit weights.
+FLOPS_PER_RK4_STEP = 370
+#: Deposit bytes per record (key 4 B + u, w, q 24 B written by the trace, read by the
+#: reduction) and per node (charge read and written).
+DEPOSIT_BYTES_PER_RECORD = 28 * 2
+NOMINAL_FP64_TFLOPS = 37.0
+
+
+def _env_int(name: str, default: int) -> int:
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def _peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return {"hbm_gbs": float(data["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")  # fmt: skip
+
+    def __init__(self, device: int) -> None:
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )  # fmt: skip
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc) -> None:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [line for line in out.splitlines() if line.strip()]
+        else:
+            self.lines = []
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in getattr(self, "lines", []):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8], strict=False):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}  # fmt: skip
+
+
+def build_workload(seed: int):
+    from beamtracer_b200.einzel import EinzelDesign, einzel_config
+
+    return einzel_config(EinzelDesign(seed=seed))
+
+
+def cpu_baseline(config, iterations: int) -> dict:
+    """The oracle on one Vlasov iteration of the workload, on every host core."""
+    from beamtracer_b200.model import BeamOptics
+    from oracle import kernels as oracle_kernels
+    from oracle import vlasov as oracle_vlasov
+    from tests.vlasov_cases import oracle_problem
+
+    model = BeamOptics(config)
+    problem = oracle_problem(model)
+    particles, j_over_v = model._particles()
+    start = time.perf_counter()
+    oracle_vlasov.vlasov(problem, particles, j_over_v, iterations=1, tolerance=0.0,
+                         relaxation=config.relaxation)  # fmt: skip
+    seconds = time.perf_counter() - start
+    cores = oracle_kernels.host_cores()
+    per_solve = seconds * max(iterations, 1)
+    return {"value": 1.0 / per_solve, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"1 Vlasov iteration (field LU solve + 20k-ring trace + deposit) in "
+                      f"{seconds:.2f} s, times {iterations} iterations per converged solve"}  # fmt: skip
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    config = build_workload(2)
+    iterations = 6
+    samples = []
+    base = None
+    for _ in range(max(args.warmup, 0) and 1):
+        base = cpu_baseline(config, iterations)  # warm the oracle's build and caches
+    for _ in range(args.steps):
+        base = cpu_baseline(config, iterations)
+        samples.append(1.0 / base["value"])
+    seconds = float(np.mean(samples))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": 1.0 / seconds, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "l2": "inputs larger than L2 (trace records)"},
+        "cpu_baseline": base,
+        "e2e": {"value": 1.0 / seconds, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--window", type=int, default=64)
+    args = parser.parse_args()
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    distributed = world > 1
+    if distributed:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))  # fmt: skip
+    from beamtracer_b200 import _lib
+    from beamtracer_b200.model import BeamOptics
+    from beamtracer_b200.vlasov import vlasov_iterate
+
+    config = build_workload(2 + rank)
+    model = BeamOptics(config)
+    model.tracer.window = args.window
+    from beamtracer_b200.poisson import IonOpticsPoisson
+
+    poisson = IonOpticsPoisson(model.mesh, backend=config.field_backend)
+    ctx = _lib.context()
+    stream = torch.cuda.current_stream()
+
+    def solve_once():
+        return vlasov_iterate(model.mesh, model._particles, model.tracer,
+                              iterations=config.iterations, tolerance=config.tolerance,
+                              relaxation=config.relaxation, poisson=poisson)  # fmt: skip
+
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        state = solve_once()
+    torch.cuda.synchronize()
+    iterations = len(state.history)
+    ctx.set_timing(True)
+    ctx.reset_timers()
+    launches_before = ctx.launch_count()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]  # fmt: skip
+    steps_total = 0
+    if distributed:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            events[k][0].record(stream)
+            state = solve_once()
+            events[k][1].record(stream)
+            steps_total += sum(h["total_steps"] for h in state.history)
+        torch.cuda.synchronize()
+    if distributed:
+        dist.barrier()
+    launches = ctx.launch_count() - launches_before
+    step_ms = [a.elapsed_time(b) for a, b in events]
+    total_ms = float(sum(step_ms))
+    if distributed:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms / 1e3)
+    timers = {name: ctx.read_timer(name) for name in
+              ("trace_window", "deposit", "field_solve", "edge_field", "vlasov_mix")}  # fmt: skip
+    ctx.set_timing(False)
+    history = state.history
+
+    # the dominant kernel and its roofline
+    kernels = {name: {"ms": ms, "launches": n, "share": ms / total_ms if total_ms else 0.0}
+               for name, (ms, n) in timers.items()}  # fmt: skip
+    trace_ms, trace_launches = timers["trace_window"]
+    flops = FLOPS_PER_RK4_STEP * steps_total
+    fp64 = {"bound": "fp64", "achieved": flops / (trace_ms / 1e3) / 1e12 if trace_ms else None,
+            "peak": NOMINAL_FP64_TFLOPS, "unit": "TFLOP/s",
+            "frac": (flops / (trace_ms / 1e3) / 1e12) / NOMINAL_FP64_TFLOPS if trace_ms else None,
+            "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)",
+            "kernel": "trace_window", "flops_per_step": FLOPS_PER_RK4_STEP,
+            "steps_per_launch": steps_total / max(trace_launches, 1)}  # fmt: skip
+    peaks = _peaks()
+    dep_ms, dep_launches = timers["deposit"]
+    records = steps_total
+    dep_bytes = records * DEPOSIT_BYTES_PER_RECORD
+    hbm = {"bound": "hbm", "kernel": "deposit",
+           "achieved": dep_bytes / (dep_ms / 1e3) / 1e9 if dep_ms else None,
+           "peak": peaks["hbm_gbs"], "unit": "GB/s",
+           "frac": (dep_bytes / (dep_ms / 1e3) / 1e9) / peaks["hbm_gbs"] if dep_ms else None,
+           "peak_source": peaks["source"], "traffic": None}  # fmt: skip
+
+    # end to end: the public call from host inputs to host results
+    e2e_ms = []
+    h2d = d2h = 0
+    for k in range(max(1, min(args.steps, 3))):
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record(stream)
+        m = BeamOptics(config)
+        m.run()
+        moments = m.beam_moments(79e-3)
+        stop.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(start.elapsed_time(stop))
+        engine = m.tracer.engine()
+        n = engine.n
+        nn = m.mesh.shape[0] * m.mesh.shape[1]
+        h2d = (nn * (1 + 8 + 32 + 4 + 1 + 8) + engine.cells.numel() * 8
+               + engine.subcells.numel() * 8 + n * (48 + 16 + 24 + 8))  # fmt: skip
+        d2h = (engine.counts.numel() * 8 + engine.hits.numel() * 8 + n * 24
+               + engine.paths.numel() * 8 + 2 * nn * 8)  # fmt: skip
+    e2e_value = world * 1e3 / float(np.mean(e2e_ms))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(config, len(history))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "iterations_per_solve": len(history),
+                   "trajectories": 20000, "mesh": [801, 201], "window": args.window,
+                   "l2": "256 MiB written between timed steps"},
+        "roofline": hbm, "roofline_fp64": fp64, "kernels": kernels,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms": float(np.mean(e2e_ms))},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+        "moments_79mm": {"current": moments.current, "rms_size": moments.rms_size,
+                         "rms_angle": moments.rms_angle, "emittance": moments.emittance},
+    }  # fmt: skip
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if distributed:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

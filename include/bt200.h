@@ -41,6 +41,16 @@ int bt_ctx_destroy(bt_ctx *ctx);
 /* Queue the context's work on `stream` (a cudaStream_t; NULL: the context's own). */
 int bt_ctx_set_stream(bt_ctx *ctx, void *stream);
 int bt_ctx_synchronize(bt_ctx *ctx);
+/* Time the context's launches with CUDA events on its stream (off by default): the
+ * kernels "trace_window", "deposit" (the sort and reduction of a flush of records),
+ * "field_solve" (a whole bt_poisson_solve), "edge_field", "vlasov_mix",
+ * "staggered_field_2d".  bt_ctx_read_timer waits for the recorded launches and returns
+ * their summed time [ms] and count since the last reset. */
+int bt_ctx_set_timing(bt_ctx *ctx, int on);
+int bt_ctx_read_timer(bt_ctx *ctx, const char *name, double *total_ms, int64_t *launches);
+int bt_ctx_reset_timers(bt_ctx *ctx);
+/* The number of kernels the context has launched since its creation (host out-param). */
+int bt_ctx_launch_count(bt_ctx *ctx, int64_t *count);
 /* Copy the calling thread's last error message into buf (NUL-terminated); returns its length. */
 size_t bt_last_error(char *buf, size_t len);
 /* The library's version string. */
