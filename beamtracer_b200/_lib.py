@@ -88,6 +88,7 @@ SIGNATURES: dict[str, list] = {
     "bt_version": [],
     "bt_staggered_field_2d": [P, P, P, I64, P, P, I64, I64, F64, F64, F64, P, P],
     "bt_deposit_trajectories_2d": [P, P, P, P, I64, F64, F64, F64, I64, P, I64, I64],
+    "bt_deposit_trajectories_2d_noalloc": [P, P, P, P, I64, F64, F64, F64, I64, P, I64, I64],
     "bt_trace_trajectories_2d": [P, ctypes.POINTER(TraceArgs), I64],
     "bt_trace_last_stats": [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64)],
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],

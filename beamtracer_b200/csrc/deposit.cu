@@ -8,6 +8,8 @@
 //  kernels/trace_trajectories_2d/trace_trajectories_2d_pyccel.py:397-423): a record
 // (cell c, u, w, q) adds (1-u)(1-w)q, (1-u)w q, u(1-w)q and u w q to the nodes c, c+1,
 // c+ny, c+ny+1.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace bt {
@@ -382,5 +384,132 @@ extern "C" int bt_deposit_trajectories_2d(bt_ctx *ctx, const double *px, const d
         // the records' keys live in `keys`; the sort reads them and writes elsewhere
         bt::NodeLayout layout{nullptr, 1, nx, ny, nx * ny};
         bt::deposit_records(ctx, keys, U, W, Q, n, (uint32_t)(nx * ny), charge, layout);
+    });
+}
+
+// -- the deposit without allocation ---------------------------------------------------------
+//
+// bt_deposit_trajectories_2d_noalloc: the same deterministic deposit for callers that may
+// not allocate device memory (their memory is budgeted up front by another allocator, or
+// cudaMalloc's implicit device synchronisation is not acceptable where they call).  Its
+// scratch is the file-scope array below, of a fixed size; every GPU that loads the library
+// holds it until the process exits.  Every call shares it and leaves its last contents
+// there: calls that overlap on the GPU (on different streams, or from different host
+// threads without ordering) race on it.
+
+namespace bt {
+namespace {
+
+constexpr i64 kNoallocPoints = 65536;  // at most this many charges per call
+constexpr i64 kNoallocNodes = 65536;   // and a mesh of at most this many nodes
+constexpr i64 kNoallocBlocks = (kNoallocPoints + kTile - 1) / kTile;
+constexpr i64 kNoallocWarps = (kNoallocPoints + 31) / 32;
+
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+// the carving of the static array, in bytes
+constexpr size_t kOffKeys = 0;  // keys, keys_alt, vals, vals_alt (u32)
+constexpr size_t kOffPayload = kOffKeys + align256(4 * 4 * kNoallocPoints);  // u, w, q
+constexpr size_t kOffHist = kOffPayload + align256(3 * 8 * kNoallocPoints);  // hist, offs
+constexpr size_t kOffDigits = kOffHist + align256(2 * 4 * kRadix * kNoallocBlocks);
+constexpr size_t kOffCells = kOffDigits + align256(2 * 4 * kRadix);
+constexpr size_t kOffWarps = kOffCells + align256(32 * kNoallocNodes);  // first, last
+constexpr size_t kOffFlags = kOffWarps + align256(2 * 32 * kNoallocWarps);
+constexpr size_t kNoallocBytes = kOffFlags + align256(2 * kNoallocWarps);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+// The device address of the array on each device, looked up on the first call there
+// (with that device current); the name itself is only a host-side stand-in.
+std::mutex g_noalloc_mutex;
+void *g_noalloc_address[64] = {};
+
+unsigned char *noalloc_scratch(int device) {
+    BT_REQUIRE(device >= 0 && device < 64, "deposit (no allocation): device index too large");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_address[device]) {
+        void *address = nullptr;
+        BT_CUDA(cudaGetSymbolAddress(&address, g_noalloc_scratch));
+        g_noalloc_address[device] = address;
+    }
+    return static_cast<unsigned char *>(g_noalloc_address[device]);
+}
+
+}  // namespace
+}  // namespace bt
+
+extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px,
+                                                  const double *py, const double *q,
+                                                  int64_t n, double origin_x, double origin_y,
+                                                  double h, int64_t cylindrical, double *charge,
+                                                  int64_t nx, int64_t ny) {
+    using namespace bt;
+    return guarded([&] {
+        BT_REQUIRE(n >= 0, "deposit (no allocation): negative point count");
+        BT_REQUIRE(nx >= 2 && ny >= 2, "deposit (no allocation): the mesh needs 2 x 2 nodes");
+        BT_REQUIRE(n <= kNoallocPoints,
+                   "deposit (no allocation): more than 65536 charges in one call exceed its "
+                   "static scratch; split the call or use bt_deposit_trajectories_2d");
+        BT_REQUIRE(nx * ny <= kNoallocNodes,
+                   "deposit (no allocation): a mesh of more than 65536 nodes exceeds its "
+                   "static scratch; use bt_deposit_trajectories_2d");
+        if (n == 0) return;
+        BT_REQUIRE(px && py && q && charge, "deposit (no allocation): null array");
+        int device = 0;
+        BT_CUDA(cudaGetDevice(&device));
+        unsigned char *base = noalloc_scratch(device);
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        uint32_t *keys = reinterpret_cast<uint32_t *>(base + kOffKeys);
+        uint32_t *keys_alt = keys + kNoallocPoints;
+        uint32_t *vals = keys_alt + kNoallocPoints;
+        uint32_t *vals_alt = vals + kNoallocPoints;
+        double *U = reinterpret_cast<double *>(base + kOffPayload);
+        double *W = U + kNoallocPoints;
+        double *Q = W + kNoallocPoints;
+        uint32_t *hist = reinterpret_cast<uint32_t *>(base + kOffHist);
+        uint32_t *offs = hist + kRadix * kNoallocBlocks;
+        uint32_t *digit = reinterpret_cast<uint32_t *>(base + kOffDigits);
+        uint32_t *totals = digit + kRadix;
+        double4 *cells = reinterpret_cast<double4 *>(base + kOffCells);
+        double4 *first = reinterpret_cast<double4 *>(base + kOffWarps);
+        double4 *last = first + kNoallocWarps;
+        uint8_t *flags = base + kOffFlags;
+        const uint32_t sentinel = (uint32_t)(nx * ny);
+
+        point_records<<<blocks_for(n, 256), 256, 0, st>>>(px, py, q, n, origin_x, origin_y, h,
+                                                          cylindrical, nx, ny, keys, U, W, Q);
+        // the stable radix sort, ping-ponging between the key and value arrays
+        const int nblocks = (int)((n + kTile - 1) / kTile);
+        const int passes = (bits_for(sentinel) + 7) / 8;
+        const uint32_t *src_k = keys, *src_v = nullptr;
+        uint32_t *dst_k = keys_alt, *dst_v = vals;
+        for (int pass = 0; pass < passes; ++pass) {
+            const int shift = 8 * pass;
+            radix_hist<<<nblocks, kThreads, 0, st>>>(src_k, n, shift, hist, nblocks);
+            radix_row_scan<<<kRadix, kThreads, 0, st>>>(hist, offs, totals, nblocks);
+            radix_digit_base<<<1, kThreads, 0, st>>>(totals, digit);
+            radix_scatter<<<nblocks, kThreads, 0, st>>>(src_k, src_v, n, shift, offs, digit,
+                                                        nblocks, dst_k, dst_v);
+            src_k = dst_k;
+            src_v = dst_v;
+            if (dst_k == keys_alt) {
+                dst_k = keys;
+                dst_v = vals_alt;
+            } else {
+                dst_k = keys_alt;
+                dst_v = vals;
+            }
+        }
+        // the per-cell sums start at zero; the warp pieces are all written before read
+        const i64 n_nodes = nx * ny;
+        const i64 n_warps = (n + 31) / 32;
+        BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * n_nodes, st));
+        seg_reduce_warps<<<blocks_for(n_warps * 32, 256), 256, 0, st>>>(
+            src_k, src_v, U, W, Q, n, sentinel, cells, first, last, flags, flags + n_warps);
+        seg_reduce_chains<<<blocks_for(n_warps, 256), 256, 0, st>>>(src_k, n_warps, cells, first,
+                                                                   last, flags, flags + n_warps);
+        node_accumulate<<<blocks_for(n_nodes, 256), 256, 0, st>>>(cells, charge, nullptr, 1, nx,
+                                                                 ny, n_nodes);
+        BT_CHECK_LAUNCH();
     });
 }

@@ -76,6 +76,22 @@ int bt_deposit_trajectories_2d(bt_ctx *ctx, const double *px, const double *py,
                                double h, int64_t cylindrical, double *charge, int64_t nx,
                                int64_t ny);
 
+/* No counterpart in the reference.  The deposit of bt_deposit_trajectories_2d for callers
+ * that may not allocate device memory -- whose device memory is budgeted up front by
+ * another allocator, or that cannot take cudaMalloc's implicit synchronisation of the
+ * device at the point where they deposit.  It allocates nothing: its scratch is a
+ * file-scope __device__ array of about 4.7 MB that every GPU loading the library holds
+ * until the process exits, sized for at most 65536 charges per call and a mesh of at most
+ * 65536 nodes; larger calls fail with BT_ERR_ARG.  `stream` is a cudaStream_t (NULL: the
+ * legacy default stream) on the calling thread's current device.  The first call on a
+ * device looks up the array's device address there (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  All calls share the array and leave their scratch in
+ * it: calls that overlap on the GPU race, so order them (one stream, or events). */
+int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px, const double *py,
+                                       const double *q, int64_t n, double origin_x,
+                                       double origin_y, double h, int64_t cylindrical,
+                                       double *charge, int64_t nx, int64_t ny);
+
 /* The arguments of kernels/trace_trajectories_2d/trace_trajectories_2d_pyccel.py:42-78,
  * all arrays on the device, with their shapes. */
 typedef struct bt_trace_args {
