@@ -245,18 +245,30 @@ __global__ void smooth5(i64 nx, i64 ny, const double *__restrict__ c4,
     x[f] = s / diag[f];
 }
 
-__global__ void smooth9(i64 nx, i64 ny, const double *__restrict__ a9,
-                        const uint8_t *__restrict__ active, const double *__restrict__ b,
-                        double *__restrict__ x, int colour) {
-    const i64 n = nx * ny;
-    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+// How the item functions load the vectors they read (plain loads; a kernel whose blocks
+// shared vectors through global memory within one launch would bypass L1 here).
+struct PlainLoad {
+    __device__ __forceinline__ double operator()(const double *p) const { return *p; }
+};
+
+// The nodes of one of four colours (i % 2, j % 2) of a 9-point level: item t of `count`.
+__device__ __forceinline__ i64 colour_count(i64 nx, i64 ny, int colour) {
     const int ci = colour >> 1, cj = colour & 1;
-    const i64 hx = (nx - ci + 1) / 2, hy = (ny - cj + 1) / 2;
-    if (t >= hx * hy) return;
+    return ((nx - ci + 1) / 2) * ((ny - cj + 1) / 2);
+}
+
+template <class Load>
+__device__ __forceinline__ void smooth9_item(i64 t, i64 nx, i64 ny, const double *__restrict__ a9,
+                                             const uint8_t *__restrict__ active,
+                                             const double *__restrict__ b, double *x, int colour,
+                                             Load load) {
+    const i64 n = nx * ny;
+    const int ci = colour >> 1, cj = colour & 1;
+    const i64 hy = (ny - cj + 1) / 2;
     const i64 i = 2 * (t / hy) + ci, j = 2 * (t % hy) + cj;
     const i64 f = i * ny + j;
     if (!active[f]) return;
-    double s = b[f];
+    double s = load(b + f);
 #pragma unroll
     for (int di = -1; di <= 1; ++di) {
 #pragma unroll
@@ -264,10 +276,18 @@ __global__ void smooth9(i64 nx, i64 ny, const double *__restrict__ a9,
             if (di == 0 && dj == 0) continue;
             const i64 i2 = i + di, j2 = j + dj;
             if (i2 < 0 || i2 >= nx || j2 < 0 || j2 >= ny) continue;
-            s -= a9[(i64)((di + 1) * 3 + (dj + 1)) * n + f] * x[i2 * ny + j2];
+            s -= a9[(i64)((di + 1) * 3 + (dj + 1)) * n + f] * load(x + i2 * ny + j2);
         }
     }
     x[f] = s / a9[4 * n + f];
+}
+
+__global__ void smooth9(i64 nx, i64 ny, const double *__restrict__ a9,
+                        const uint8_t *__restrict__ active, const double *__restrict__ b,
+                        double *__restrict__ x, int colour) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= colour_count(nx, ny, colour)) return;
+    smooth9_item(t, nx, ny, a9, active, b, x, colour, PlainLoad{});
 }
 
 // y = A x (level 0, 5-point) on active rows, 0 elsewhere; with b: r = b - A x.
@@ -291,32 +311,38 @@ __global__ void apply5(i64 nx, i64 ny, const double *__restrict__ c4,
     y[f] = b ? b[f] - s : s;
 }
 
-__global__ void residual9(i64 nx, i64 ny, const double *__restrict__ a9,
-                          const uint8_t *__restrict__ active, const double *__restrict__ x,
-                          const double *__restrict__ b, double *__restrict__ r) {
+template <class Load>
+__device__ __forceinline__ void residual9_item(i64 f, i64 nx, i64 ny, const double *__restrict__ a9,
+                                               const uint8_t *__restrict__ active,
+                                               const double *x, const double *b, double *r,
+                                               Load load) {
     const i64 n = nx * ny;
-    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= n) return;
     if (!active[f]) {
         r[f] = 0.0;
         return;
     }
     const i64 i = f / ny, j = f - i * ny;
-    double s = b[f];
+    double s = load(b + f);
     for (int di = -1; di <= 1; ++di)
         for (int dj = -1; dj <= 1; ++dj) {
             const i64 i2 = i + di, j2 = j + dj;
             if (i2 < 0 || i2 >= nx || j2 < 0 || j2 >= ny) continue;
-            s -= a9[(i64)((di + 1) * 3 + (dj + 1)) * n + f] * x[i2 * ny + j2];
+            s -= a9[(i64)((di + 1) * 3 + (dj + 1)) * n + f] * load(x + i2 * ny + j2);
         }
     r[f] = s;
 }
 
-__global__ void restrict_residual(Fine F, const double *__restrict__ r, double *__restrict__ bc,
-                                  double *__restrict__ xc) {
-    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    const i64 nc = F.ncx * F.ncy;
-    if (t >= nc) return;
+__global__ void residual9(i64 nx, i64 ny, const double *__restrict__ a9,
+                          const uint8_t *__restrict__ active, const double *__restrict__ x,
+                          const double *__restrict__ b, double *__restrict__ r) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nx * ny) return;
+    residual9_item(f, nx, ny, a9, active, x, b, r, PlainLoad{});
+}
+
+template <class Load>
+__device__ __forceinline__ void restrict_item(i64 t, const Fine &F, const double *r, double *bc,
+                                              double *xc, Load load) {
     const i64 I = t / F.ncy, J = t - I * F.ncy;
     const i64 k0 = I > 0 ? F.cix[I - 1] : 0, k1 = I < F.ncx - 1 ? F.cix[I + 1] : F.nx - 1;
     const i64 l0 = J > 0 ? F.ciy[J - 1] : 0, l1 = J < F.ncy - 1 ? F.ciy[J + 1] : F.ny - 1;
@@ -329,16 +355,24 @@ __global__ void restrict_residual(Fine F, const double *__restrict__ r, double *
             if (pl == 0.0) continue;
             const i64 f = k * F.ny + l;
             if (!F.active[f]) continue;
-            s += pk * pl * (F.weight ? F.weight[f] : 1.0) * r[f];
+            s += pk * pl * (F.weight ? F.weight[f] : 1.0) * load(r + f);
         }
     }
     bc[t] = s;
     xc[t] = 0.0;
 }
 
-__global__ void prolong_add(Fine F, const double *__restrict__ xc, double *__restrict__ x) {
-    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= F.nx * F.ny || !F.active[f]) return;
+__global__ void restrict_residual(Fine F, const double *__restrict__ r, double *__restrict__ bc,
+                                  double *__restrict__ xc) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= F.ncx * F.ncy) return;
+    restrict_item(t, F, r, bc, xc, PlainLoad{});
+}
+
+template <class Load>
+__device__ __forceinline__ void prolong_item(i64 f, const Fine &F, const double *xc, double *x,
+                                             Load load) {
+    if (!F.active[f]) return;
     const i64 k = f / F.ny, l = f - k * F.ny;
     const i64 ix = F.lox[k], iy = F.loy[l];
     const double wx = F.wx[k], wy = F.wy[l];
@@ -349,10 +383,16 @@ __global__ void prolong_add(Fine F, const double *__restrict__ xc, double *__res
         for (int sy = 0; sy < 2; ++sy) {
             const double py = sy ? 1.0 - wy : wy;
             if (py == 0.0 || iy + sy >= F.ncy) continue;
-            s += px * py * xc[(ix + sx) * F.ncy + iy + sy];
+            s += px * py * load(xc + (ix + sx) * F.ncy + iy + sy);
         }
     }
-    x[f] += s;
+    x[f] = load(x + f) + s;
+}
+
+__global__ void prolong_add(Fine F, const double *__restrict__ xc, double *__restrict__ x) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F.nx * F.ny) return;
+    prolong_item(f, F, xc, x, PlainLoad{});
 }
 
 // The coarsest level: the dense matrix of its 9-point operator, inverted in place by
@@ -438,24 +478,164 @@ __global__ void coarsest_apply(int n, const double *__restrict__ inv, const doub
     x[r] = s;
 }
 
-// -- vector kernels of GMRES and Newton ----------------------------------------------------
+// The 9-point form of the 5-point level-0 operator, for a mesh whose first level is
+// already the coarsest (the dense inverse reads 9-point rows).
+__global__ void five_to_nine(i64 n, const double *__restrict__ c4, const double *__restrict__ diag,
+                             const uint8_t *__restrict__ active, double *__restrict__ a9) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    for (int q = 0; q < 9; ++q) a9[(i64)q * n + f] = 0.0;
+    if (!active[f]) {
+        a9[4 * n + f] = 1.0;
+        return;
+    }
+    a9[4 * n + f] = diag[f];
+    a9[1 * n + f] = -c4[2 * n + f];  // (0, -1)
+    a9[7 * n + f] = -c4[3 * n + f];  // (0, +1)
+    a9[3 * n + f] = -c4[f];          // (-1, 0)
+    a9[5 * n + f] = -c4[n + f];      // (+1, 0)
+}
 
-// out[q] = sum_f V[q * n + f] * w[f], q < m (one block per q, deterministic tree)
-__global__ void multi_dot(const double *__restrict__ V, const double *__restrict__ w, i64 n,
-                          double *__restrict__ out) {
-    __shared__ double part[256];
-    const int q = blockIdx.x;
-    const double *v = V + (i64)q * n;
-    double s = 0.0;
-    for (i64 f = threadIdx.x; f < n; f += blockDim.x) s += v[f] * w[f];
-    part[threadIdx.x] = s;
-    __syncthreads();
-    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-        if (threadIdx.x < off) part[threadIdx.x] += part[threadIdx.x + off];
+// -- the small levels in one launch, in shared memory ---------------------------------------
+
+constexpr int kTailThreads = 1024;
+constexpr i64 kTailLevelNodes = 4096;  // levels at most this large go to the tail
+
+struct TailLevel {
+    i64 nx, ny, n;
+    const double *a9;
+    const uint8_t *active;
+    double *x, *b;  // the level's global vectors (read: b of the first, written: x of the first)
+    Fine next;      // the map to the next coarser level (unused on the coarsest)
+};
+
+// The V-cycle of the small levels in one block: the x, b and r of every tail level staged
+// in shared memory (levels[0].b read from global memory, levels[0].x written back), the
+// coefficients read through the L1 cache; four-colour Gauss-Seidel, residual and
+// restriction down, the coarsest level's inverse, prolongation and smoothing up, with a
+// block barrier between steps.
+__global__ void __launch_bounds__(kTailThreads, 1)
+vcycle_tail(const TailLevel *__restrict__ levels, int count, const double *__restrict__ inv,
+            int sweeps) {
+    extern __shared__ double sm[];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const PlainLoad load{};
+    // level l's x, b, r in shared memory
+    auto X = [&](int l) {
+        i64 off = 0;
+        for (int k = 0; k < l; ++k) off += 3 * levels[k].n;
+        return sm + off;
+    };
+    {
+        const TailLevel &L = levels[0];
+        double *x = X(0);
+        for (i64 f = tid; f < L.n; f += nt) {
+            x[f] = 0.0;
+            x[L.n + f] = L.b[f];
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[q] = part[0];
+    for (int l = 0; l + 1 < count; ++l) {
+        const TailLevel &L = levels[l];
+        double *x = X(l), *b = x + L.n, *r = b + L.n;
+        for (int s = 0; s < sweeps; ++s)
+            for (int c = 0; c < 4; ++c) {
+                const i64 m = colour_count(L.nx, L.ny, c);
+                for (i64 t = tid; t < m; t += nt) smooth9_item(t, L.nx, L.ny, L.a9, L.active, b, x, c, load);
+                __syncthreads();
+            }
+        for (i64 f = tid; f < L.n; f += nt) residual9_item(f, L.nx, L.ny, L.a9, L.active, x, b, r, load);
+        __syncthreads();
+        const TailLevel &C = levels[l + 1];
+        double *xc = X(l + 1), *bc = xc + C.n;
+        for (i64 t = tid; t < C.n; t += nt) restrict_item(t, L.next, r, bc, xc, load);
+        __syncthreads();
+    }
+    {
+        const TailLevel &C = levels[count - 1];
+        double *x = X(count - 1), *b = x + C.n;
+        const int n = (int)C.n;
+        for (int row = tid; row < n; row += nt) {
+            double s = 0.0;
+            for (int c = 0; c < n; ++c) s += __ldg(inv + row * n + c) * b[c];
+            x[row] = s;
+        }
+        __syncthreads();
+    }
+    for (int l = count - 2; l >= 0; --l) {
+        const TailLevel &L = levels[l];
+        double *x = X(l), *b = x + L.n;
+        const double *xc = X(l + 1);
+        for (i64 f = tid; f < L.n; f += nt) prolong_item(f, L.next, xc, x, load);
+        __syncthreads();
+        for (int s = 0; s < sweeps; ++s)
+            for (int c = 3; c >= 0; --c) {
+                const i64 m = colour_count(L.nx, L.ny, c);
+                for (i64 t = tid; t < m; t += nt) smooth9_item(t, L.nx, L.ny, L.a9, L.active, b, x, c, load);
+                __syncthreads();
+            }
+    }
+    {
+        const TailLevel &L = levels[0];
+        const double *x = X(0);
+        for (i64 f = tid; f < L.n; f += nt) L.x[f] = x[f];
+    }
 }
+
+// -- dot products: partial sums per block, then an ordered sum (deterministic) -----------
+
+constexpr int kDotMax = 32;     // at most this many vectors against one
+constexpr int kDotBlocks = 296;  // two per SM
+constexpr int kDotThreads = 256;
+
+// partial[block * kDotMax + q] = the block's share of sum_f V[q n + f] w[f], q < m
+__global__ void __launch_bounds__(kDotThreads) multi_dot_partial(
+    const double *__restrict__ V, const double *__restrict__ w, i64 n, int m,
+    double *__restrict__ partial) {
+    __shared__ double warp_part[kDotThreads / 32][kDotMax];
+    double acc[kDotMax];
+#pragma unroll
+    for (int q = 0; q < kDotMax; ++q) acc[q] = 0.0;
+    for (i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
+        const double wf = w[f];
+#pragma unroll
+        for (int q = 0; q < kDotMax; ++q)
+            if (q < m) acc[q] += V[(i64)q * n + f] * wf;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kDotMax; ++q) {
+        double v = acc[q];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) warp_part[warp][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kDotMax) {
+        double v = 0.0;
+        for (int wi = 0; wi < kDotThreads / 32; ++wi) v += warp_part[wi][threadIdx.x];
+        partial[(i64)blockIdx.x * kDotMax + threadIdx.x] = v;
+    }
+}
+
+// out[q] = the blocks' partials of q summed in a fixed order: each of 8 warps sums a
+// strided eighth of the blocks for every q, then the eight sums are added in order.
+__global__ void multi_dot_final(const double *__restrict__ partial, int blocks, int m,
+                                double *__restrict__ out) {
+    __shared__ double part[8][kDotMax];
+    const int q = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double v = 0.0;
+    if (q < m)
+        for (int bi = warp; bi < blocks; bi += 8) v += partial[(i64)bi * kDotMax + q];
+    part[warp][q] = v;
+    __syncthreads();
+    if (warp == 0 && q < m) {
+        double s = 0.0;
+        for (int w = 0; w < 8; ++w) s += part[w][q];
+        out[q] = s;
+    }
+}
+
+// -- vector kernels of GMRES and Newton ----------------------------------------------------
 
 // w -= sum_q h[q] V[q]
 __global__ void orthogonalise(const double *__restrict__ V, const double *__restrict__ hcol, int m,
@@ -465,6 +645,15 @@ __global__ void orthogonalise(const double *__restrict__ V, const double *__rest
     double s = w[f];
     for (int q = 0; q < m; ++q) s -= hcol[q] * V[(i64)q * n + f];
     w[f] = s;
+}
+
+// v = w / sqrt(norm2[0]) (zero for a zero norm: GMRES stops there)
+__global__ void scale_by_norm(const double *__restrict__ w, const double *__restrict__ norm2, i64 n,
+                              double *__restrict__ v) {
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    const double s = norm2[0];
+    v[f] = s > 0.0 ? w[f] / sqrt(s) : 0.0;
 }
 
 __global__ void scale_into(const double *__restrict__ w, double a, i64 n, double *__restrict__ v) {
@@ -589,6 +778,18 @@ struct bt_poisson {
     bool built = false;        // hierarchy matches the current diagonal
     bool reaction_on = false;  // level-0 diagonal holds a reaction
     int restart = 30;
+    int tail_start = -1;    // the first level of the V-cycle's one-block tail
+    size_t tail_smem = 0;    // its shared memory: x, b, r of every tail level
+    bt::Buffer tail_levels;  // its TailLevel descriptors
+    bt::Buffer dot_partial;  // per-block partial dot products
+    // the V-cycle from a zero guess on level 0's b into its x, captured once as a graph
+    cudaGraph_t vgraph = nullptr;
+    cudaGraphExec_t vexec = nullptr;
+    i64 vgraph_kernels = 0;
+    ~bt_poisson() {
+        if (vexec) cudaGraphExecDestroy(vexec);
+        if (vgraph) cudaGraphDestroy(vgraph);
+    }
     // GMRES: the Krylov basis V, its preconditioned images Z, two work vectors, the
     // Hessenberg column and the solution's coefficients; the solve: its right-hand side,
     // the residual GMRES reduces, the correction, the Newton reaction and scalars.
@@ -652,6 +853,10 @@ void build_hierarchy(bt_poisson *p, const double *reaction) {
                                                         C.active.as<uint8_t>(C.n));
     }
     Level &Lc = p->levels.back();
+    if (p->levels.size() == 1)
+        BT_LAUNCH(p->ctx, five_to_nine, blocks_for(Lc.n, 256), 256, 0, st, Lc.n,
+                  Lc.c4.as<double>(4 * Lc.n), Lc.diag.as<double>(Lc.n), Lc.active.as<uint8_t>(Lc.n),
+                  Lc.a9.as<double>(9 * Lc.n));
     int *status = p->status.as<int>(1);
     BT_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
     BT_LAUNCH(p->ctx, coarsest_invert, 1, 256, 0, st, Lc.nx, Lc.ny, Lc.a9.as<double>(9 * Lc.n),
@@ -666,6 +871,13 @@ void vcycle(bt_poisson *p, size_t l) {
     cudaStream_t st = p->ctx->stream;
     Level &L = p->levels[l];
     const int T = 256;
+    if ((int)l == p->tail_start) {
+        const int count = (int)(p->levels.size() - l);
+        const Level &Lc = p->levels.back();
+        BT_LAUNCH(p->ctx, vcycle_tail, 1, kTailThreads, p->tail_smem, st,
+                  p->tail_levels.as<TailLevel>(count), count, p->inv.as<double>(Lc.n * Lc.n), 2);
+        return;
+    }
     if (l + 1 == p->levels.size()) {
         BT_LAUNCH(p->ctx, coarsest_apply, 1, kCoarsest, 0, st, (int)L.n, p->inv.as<double>(L.n * L.n),
                                                L.b.as<double>(L.n), L.x.as<double>(L.n));
@@ -712,12 +924,40 @@ void vcycle(bt_poisson *p, size_t l) {
 }
 
 // z = M v: one V-cycle from zero
+// Capture the V-cycle (level 0's x zeroed, then the cycle on its b) as a graph: every
+// buffer it touches keeps its address for the solver's life, so one capture serves every
+// solve and every Newton Jacobian (whose coefficients change in place).
+void capture_vcycle(bt_poisson *p) {
+    cudaStream_t st = p->ctx->stream;
+    Level &L = p->levels[0];
+    const i64 before = p->ctx->launch_count;
+    BT_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+        BT_CUDA(cudaMemsetAsync(L.x.as<double>(L.n), 0, sizeof(double) * L.n, st));
+        vcycle(p, 0);
+    } catch (...) {
+        cudaGraph_t broken = nullptr;
+        cudaStreamEndCapture(st, &broken);
+        if (broken) cudaGraphDestroy(broken);
+        throw;
+    }
+    BT_CUDA(cudaStreamEndCapture(st, &p->vgraph));
+    BT_CUDA(cudaGraphInstantiate(&p->vexec, p->vgraph, 0));
+    p->vgraph_kernels = p->ctx->launch_count - before;
+    p->ctx->launch_count = before;  // counted when the graph runs
+}
+
+// z = M v: one V-cycle from zero
 void precondition(bt_poisson *p, const double *v, double *z) {
     Level &L = p->levels[0];
     cudaStream_t st = p->ctx->stream;
+    if (!p->vexec) capture_vcycle(p);
     BT_CUDA(cudaMemcpyAsync(L.b.as<double>(L.n), v, sizeof(double) * L.n, cudaMemcpyDeviceToDevice, st));
-    BT_CUDA(cudaMemsetAsync(L.x.as<double>(L.n), 0, sizeof(double) * L.n, st));
-    vcycle(p, 0);
+    {
+        Timed timed(p->ctx, "vcycle");
+        BT_CUDA(cudaGraphLaunch(p->vexec, st));
+    }
+    p->ctx->launch_count += p->vgraph_kernels;
     BT_CUDA(cudaMemcpyAsync(z, L.x.as<double>(L.n), sizeof(double) * L.n, cudaMemcpyDeviceToDevice, st));
 }
 
@@ -734,9 +974,17 @@ double read_scalar(bt_poisson *p, const double *dev) {
     return host[0];
 }
 
+// out[q] = <V_q, w> for q < m (V's rows of n values), deterministic
+void dots(bt_poisson *p, const double *V, const double *w, int m, double *out) {
+    double *partial = p->dot_partial.as<double>((size_t)kDotBlocks * kDotMax);
+    BT_LAUNCH(p->ctx, multi_dot_partial, kDotBlocks, kDotThreads, 0, p->ctx->stream, V, w, p->n, m,
+              partial);
+    BT_LAUNCH(p->ctx, multi_dot_final, 1, 256, 0, p->ctx->stream, partial, kDotBlocks, m, out);
+}
+
 double norm2(bt_poisson *p, const double *v) {
     double *s = p->scalars.as<double>(8);
-    BT_LAUNCH(p->ctx, multi_dot, 1, 256, 0, p->ctx->stream, v, v, p->n, s);
+    dots(p, v, v, 1, s);
     return std::sqrt(read_scalar(p, s));
 }
 
@@ -746,14 +994,16 @@ double norm2(bt_poisson *p, const double *v) {
 int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_iter,
           double *final_norm) {
     const i64 n = p->n;
-    const int m = p->restart;
+    const int m = p->restart;  // at most kDotMax - 1: a basis of m + 1 vectors
     cudaStream_t st = p->ctx->stream;
     double *V = p->V.as<double>((size_t)(m + 1) * n);
     double *Z = p->Z.as<double>((size_t)m * n);
     double *w = p->work.as<double>(n);
-    double *hdev = p->hcol.as<double>(m + 2);
+    // the Hessenberg column's two Gram-Schmidt passes and the new vector's squared norm
+    double *hdev = p->hcol.as<double>(2 * (m + 2) + 2);
+    double *hdev2 = hdev + (m + 2), *hnorm = hdev + 2 * (m + 2);
     double *ydev = p->ycoef.as<double>(m + 2);
-    double *host = static_cast<double *>(p->ctx->host.get(sizeof(double) * (m + 8)));
+    double *host = static_cast<double *>(p->ctx->host.get(sizeof(double) * (2 * (m + 2) + 2)));
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
     int total = 0;
     BT_CUDA(cudaMemcpyAsync(w, r0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
@@ -772,18 +1022,21 @@ int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_it
             double *v = V + (i64)j * n, *z = Z + (i64)j * n;
             precondition(p, v, z);
             apply(p, z, w);
-            // classical Gram-Schmidt, applied twice
-            for (int pass = 0; pass < 2; ++pass) {
-                BT_LAUNCH(p->ctx, multi_dot, j + 1, 256, 0, st, V, w, n, hdev);
-                BT_LAUNCH(p->ctx, orthogonalise, blocks_for(n, 256), 256, 0, st, V, hdev, j + 1, n, w);
-                BT_CUDA(cudaMemcpyAsync(host, hdev, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, st));
-                BT_CUDA(cudaStreamSynchronize(st));
-                for (int q = 0; q <= j; ++q) H[q * m + j] = (pass ? H[q * m + j] : 0.0) + host[q];
-            }
-            const double hn = norm2(p, w);
+            // classical Gram-Schmidt applied twice, the new basis vector normalised on the
+            // device; one read-back of the column and the norm
+            dots(p, V, w, j + 1, hdev);
+            BT_LAUNCH(p->ctx, orthogonalise, blocks_for(n, 256), 256, 0, st, V, hdev, j + 1, n, w);
+            dots(p, V, w, j + 1, hdev2);
+            BT_LAUNCH(p->ctx, orthogonalise, blocks_for(n, 256), 256, 0, st, V, hdev2, j + 1, n, w);
+            dots(p, w, w, 1, hnorm);
+            BT_LAUNCH(p->ctx, scale_by_norm, blocks_for(n, 256), 256, 0, st, w, hnorm, n,
+                      V + (i64)(j + 1) * n);
+            BT_CUDA(cudaMemcpyAsync(host, hdev, sizeof(double) * (2 * (m + 2) + 1),
+                                    cudaMemcpyDeviceToHost, st));
+            BT_CUDA(cudaStreamSynchronize(st));
+            for (int q = 0; q <= j; ++q) H[q * m + j] = host[q] + host[(m + 2) + q];
+            const double hn = std::sqrt(host[2 * (m + 2)]);
             H[(j + 1) * m + j] = hn;
-            if (hn > 0.0)
-                BT_LAUNCH(p->ctx, scale_into, blocks_for(n, 256), 256, 0, st, w, 1.0 / hn, n, V + (i64)(j + 1) * n);
             for (int q = 0; q < j; ++q) {
                 const double a = H[q * m + j], b = H[(q + 1) * m + j];
                 H[q * m + j] = cs[q] * a + sn[q] * b;
@@ -873,6 +1126,36 @@ extern "C" int bt_poisson_create(bt_ctx *ctx, const bt_mesh_desc *m, bt_poisson 
                 ny = L.ay.nc;
             }
             BT_REQUIRE(p->levels.back().n <= bt::kCoarsest, "poisson: coarsest level too large");
+            // the tail: every level from the first small one (never level 0, whose
+            // operator is 5-point) down to the coarsest, in one cluster launch
+            for (size_t l = 1; l < p->levels.size(); ++l)
+                if (p->levels[l].n <= bt::kTailLevelNodes) {
+                    p->tail_start = (int)l;
+                    break;
+                }
+            if (p->tail_start > 0) {
+                std::vector<bt::TailLevel> tail;
+                for (size_t l = p->tail_start; l < p->levels.size(); ++l) {
+                    bt::Level &L = p->levels[l];
+                    bt::TailLevel t{};
+                    t.nx = L.nx;
+                    t.ny = L.ny;
+                    t.n = L.n;
+                    t.a9 = L.a9.as<double>(9 * L.n);
+                    t.active = L.active.as<uint8_t>(L.n);
+                    t.x = L.x.as<double>(L.n);
+                    t.b = L.b.as<double>(L.n);
+                    if (l + 1 < p->levels.size()) t.next = bt::fine_of(L, p->levels[l + 1], false);
+                    tail.push_back(t);
+                    p->tail_smem += 3 * sizeof(double) * L.n;
+                }
+                BT_REQUIRE(p->tail_smem <= 200 * 1024, "poisson: the tail levels exceed shared memory");
+                BT_CUDA(cudaFuncSetAttribute(bt::vcycle_tail,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)p->tail_smem));
+                BT_CUDA(cudaMemcpy(p->tail_levels.as<bt::TailLevel>(tail.size()), tail.data(),
+                                   sizeof(bt::TailLevel) * tail.size(), cudaMemcpyHostToDevice));
+            }
             p->src.as<double>(n);
             bt::build_operator(p);
             BT_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -11,6 +11,8 @@
 // records are sorted by cell and reduced per cell in record order (deposit.cu), so the
 // node charges are deterministic.  Short windows bound the tail of a warp (its threads
 // wait only for the longest trajectory of the window, not of the whole trace).
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace bt {
@@ -515,8 +517,10 @@ extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, 
         const uint32_t sentinel = (uint32_t)a.n_nodes;
         // the record buffer: flushed (sorted and reduced into charge[0]) when the next
         // window would not fit
+        // room for 16 windows of the starting trajectories, at most 2^25 records (0.9 GB),
+        // at least one window
         const int64_t per_window = a.n_active * (int64_t)S;
-        int64_t capacity = (int64_t)1 << 25;
+        int64_t capacity = std::min<int64_t>(per_window * 16, (int64_t)1 << 25);
         if (capacity < per_window) capacity = per_window;
         uint32_t *keys = ts.rec_keys.as<uint32_t>(capacity);
         double *RU = ts.rec_u.as<double>(capacity);

@@ -320,6 +320,7 @@ def vlasov_iterate(
             "max_potential_change": change,
             "relative_density_change": density_change if iteration > 0 else float("inf"),
             "newton_iterations": poisson.newton_iterations,
+            "krylov_steps": poisson.krylov_steps,
             "steps": int(host[3]) if engine.n else 0,
             "total_steps": total_steps,
             "trajectories": len(particles),

@@ -121,10 +121,43 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}  # fmt: skip
 
 
-def build_workload(seed: int):
+def build_workload(seed: int, small: bool = False):
     from beamtracer_b200.einzel import EinzelDesign, einzel_config
 
+    if small:
+        return einzel_config(EinzelDesign(seed=seed, shape=(401, 101), trajectories=2000))
     return einzel_config(EinzelDesign(seed=seed))
+
+
+def run_profile(args) -> None:
+    """One converged solve to warm up, then one inside the NVTX range "profiled_solve"
+    (the range a profiler's capture selects)."""
+    import torch
+
+    from beamtracer_b200.model import BeamOptics
+    from beamtracer_b200.poisson import IonOpticsPoisson
+    from beamtracer_b200.vlasov import vlasov_iterate
+
+    torch.cuda.set_device(0)
+    config = build_workload(2, small=args.small)
+    model = BeamOptics(config)
+    model.tracer.window = args.window
+    poisson = IonOpticsPoisson(model.mesh, backend=config.field_backend)
+
+    def solve():
+        return vlasov_iterate(model.mesh, model._particles, model.tracer,
+                              iterations=config.iterations, tolerance=config.tolerance,
+                              relaxation=config.relaxation, poisson=poisson)  # fmt: skip
+
+    solve()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("profiled_solve")
+    state = solve()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile": "ok", "small": args.small,
+                      "iterations": len(state.history),
+                      "total_steps": sum(h["total_steps"] for h in state.history)}))  # fmt: skip
 
 
 def cpu_baseline(config, iterations: int) -> dict:
@@ -182,7 +215,14 @@ def main() -> None:
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--window", type=int, default=64)
+    parser.add_argument("--profile", action="store_true",
+                        help="one warm solve, then one in the NVTX range 'profiled_solve'")
+    parser.add_argument("--small", action="store_true",
+                        help="with --profile: the lens at 401 x 101 with 2,000 rings")
     args = parser.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
     local = _env_int("LOCAL_RANK", 0)
@@ -251,7 +291,8 @@ def main() -> None:
         total_ms = float(t.item())
     value = world * args.steps / (total_ms / 1e3)
     timers = {name: ctx.read_timer(name) for name in
-              ("trace_window", "deposit", "field_solve", "edge_field", "vlasov_mix")}  # fmt: skip
+              ("trace_window", "deposit", "field_solve", "vcycle", "edge_field",
+               "vlasov_mix")}  # fmt: skip
     ctx.set_timing(False)
     history = state.history
 
@@ -306,6 +347,7 @@ def main() -> None:
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "iterations_per_solve": len(history),
+                   "vcycles_per_solve": sum(h["krylov_steps"] for h in history),
                    "trajectories": 20000, "mesh": [801, 201], "window": args.window,
                    "l2": "256 MiB written between timed steps"},
         "roofline": hbm, "roofline_fp64": fp64, "kernels": kernels,
