@@ -46,8 +46,7 @@ __device__ __forceinline__ double uniform_x(double x, const double *__restrict__
     return x0 + h * ((double)c + (x - nodes[c]) / (nodes[c + 1] - nodes[c]));
 }
 
-__device__ __forceinline__ i64 finest_patch(const bt_trace_args &a, double px, double py) {
-    const i64 P = a.n_patches;
+__device__ __forceinline__ i64 finest_patch(const bt_trace_args &a, i64 P, double px, double py) {
     for (i64 qq = 0; qq < P - 1; ++qq) {
         const double *pr = a.patch_real + qq * 7;
         if (px >= __ldg(pr + 3) && px <= __ldg(pr + 5) && py >= __ldg(pr + 4) &&
@@ -57,15 +56,26 @@ __device__ __forceinline__ i64 finest_patch(const bt_trace_args &a, double px, d
     return P - 1;
 }
 
-// E at (lq, qy), the uniform x and the mesh y, from the finest patch holding the point
-// (trace_trajectories_2d_pyccel.py:212-269).
-__device__ __forceinline__ void edge_field(const bt_trace_args &a, double lq, double qy,
-                                           double &ex, double &ey) {
-    const i64 pp = finest_patch(a, lq, qy);
+// A patch's shape: node counts, its offsets into the edge-field and node arrays, origin and
+// spacing (one row of patch_int / patch_real).
+struct PatchGeom {
+    i64 pnx, pny, ofx, ofy, ofn;
+    double pox, poy, phh;
+};
+
+__device__ __forceinline__ PatchGeom patch_geom(const bt_trace_args &a, i64 pp) {
     const i64 *pi = a.patch_int + pp * 6;
     const double *pr = a.patch_real + pp * 7;
-    const i64 pnx = __ldg(pi + 0), pny = __ldg(pi + 1), ofx = __ldg(pi + 2), ofy = __ldg(pi + 3);
-    const double pox = __ldg(pr + 0), poy = __ldg(pr + 1), phh = __ldg(pr + 2);
+    return {__ldg(pi + 0), __ldg(pi + 1), __ldg(pi + 2), __ldg(pi + 3), __ldg(pi + 5),
+            __ldg(pr + 0), __ldg(pr + 1), __ldg(pr + 2)};
+}
+
+// E at (lq, qy), the uniform x and the mesh y, on patch g (the finest patch holding the
+// point; trace_trajectories_2d_pyccel.py:212-269).
+__device__ __forceinline__ void edge_field(const bt_trace_args &a, const PatchGeom &g, double lq,
+                                           double qy, double &ex, double &ey) {
+    const i64 pnx = g.pnx, pny = g.pny, ofx = g.ofx, ofy = g.ofy;
+    const double pox = g.pox, poy = g.poy, phh = g.phh;
     const double sx = (lq - pox) / phh;
     const double sy = (qy - poy) / phh;
     double s = sx + 0.5;
@@ -109,6 +119,18 @@ __device__ __forceinline__ void edge_field(const bt_trace_args &a, double lq, do
     ey = low + u * (high - low);
 }
 
+// 1 / gamma of a proper velocity: exactly 1 without relativity (inv_c2 = 0), which the
+// non-general kernels fold away.
+template <bool GENERAL>
+__device__ __forceinline__ double inv_gamma(double u0, double u1, double u2, double inv_c2) {
+    return GENERAL ? 1.0 / lorentz(u0, u1, u2, inv_c2) : 1.0;
+}
+
+// The kernel is specialised on the geometry (0 planar, 1 cylindrical, 2 symmetry plane),
+// the integrator (0 RK4, 1 Boris) and GENERAL: refined patches, a graded x axis or
+// relativity.  Without them the mesh is one patch, whose shape is read once, and gamma is
+// exactly 1; the operations on every value are the general kernel's, so the results are.
+template <int CYL, int INTEG, bool GENERAL>
 __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restrict__ act,
                                                    i64 n_act, int S,
                                                    uint32_t *__restrict__ keys,
@@ -119,13 +141,14 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
     if (m >= n_act) return;
     const bt_trace_args &a = tr.a;
     const i64 k = act[m];
-    const i64 P = a.n_patches;
+    const i64 P = GENERAL ? a.n_patches : 1;
+    const PatchGeom base = patch_geom(a, 0);  // the one patch of a non-general mesh
     const i64 nx = tr.nx, ny = tr.ny;
     const double origin_x = a.origin_x, origin_y = a.origin_y, h = a.h;
-    const i64 cyl = a.cylindrical;
+    constexpr int cyl = CYL;
     const double inv_c2 = a.inv_c2;
     const i64 n = a.n;
-    const bool graded = a.graded != 0;
+    const bool graded = GENERAL && a.graded != 0;
     double x0 = a.x[k], x1 = a.x[n + k], x2 = a.x[2 * n + k];
     double v0 = a.v[k], v1 = a.v[n + k], v2 = a.v[2 * n + k];
     const double qmk = a.qm[k];
@@ -133,7 +156,7 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
     const i64 slot = a.path_slot[k];
     i64 ns = a.steps[k];
     i64 st = -1;
-    const int nstage = a.integrator == 0 ? 4 : 2;
+    constexpr int nstage = INTEG == 0 ? 4 : 2;
     int have = 0;
     double ca0 = 0.0, ca1 = 0.0, ca2 = 0.0;
     int s = 0;
@@ -160,14 +183,14 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
             const double d2 = (a.x_nodes[cg + 1] - a.x_nodes[cg]) / h;
             if (d2 < 1.0) hloc = hloc * d2;
         }
-        const double gv = 1.0 / lorentz(v0, v1, v2, inv_c2);
+        const double gv = inv_gamma<GENERAL>(v0, v1, v2, inv_c2);
         double q0 = x0, q1 = x1, q2 = x2;
         double kx0 = v0, kx1 = v1, kx2 = v2;
         double sx0 = 0, sx1 = 0, sx2 = 0, sv0 = 0, sv1 = 0, sv2 = 0;
         double w0 = 0, w1 = 0, w2 = 0, y0, y1, y2;
         double dt = 0.0, hdt = 0.0, dt6 = 0.0;
         for (int stage = 0; stage < nstage; ++stage) {
-            double gk = 1.0 / lorentz(kx0, kx1, kx2, inv_c2);
+            double gk = inv_gamma<GENERAL>(kx0, kx1, kx2, inv_c2);
             double g0, g1, g2;
             if (stage == 0 && have != 0) {
                 g0 = ca0;
@@ -190,7 +213,8 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
                 double lq = q0;
                 if (graded) lq = uniform_x(q0, a.x_nodes, a.n_x_nodes, origin_x, h);
                 double ex, ey;
-                edge_field(a, lq, qy, ex, ey);
+                const PatchGeom g = GENERAL ? patch_geom(a, finest_patch(a, P, lq, qy)) : base;
+                edge_field(a, g, lq, qy, ex, ey);
                 if (cyl != 0) {
                     g0 = qmk * ex;
                     g1 = qmk * (ey * cy);
@@ -215,11 +239,11 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
                 dt = a.step_fraction * dt;
                 hdt = 0.5 * dt;
                 dt6 = dt / 6.0;
-                if (a.integrator != 0) {
+                if (INTEG != 0) {
                     kx0 = v0 + hdt * a0;
                     kx1 = v1 + hdt * a1;
                     kx2 = v2 + hdt * a2;
-                    gk = 1.0 / lorentz(kx0, kx1, kx2, inv_c2);
+                    gk = inv_gamma<GENERAL>(kx0, kx1, kx2, inv_c2);
                     q0 = x0 + dt * gk * kx0;
                     q1 = x1 + dt * gk * kx1;
                     q2 = x2 + dt * gk * kx2;
@@ -237,7 +261,7 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
                 kx0 = v0 + hdt * a0;
                 kx1 = v1 + hdt * a1;
                 kx2 = v2 + hdt * a2;
-            } else if (a.integrator != 0) {
+            } else if (INTEG != 0) {
                 w0 = kx0 + hdt * g0;
                 w1 = kx1 + hdt * g1;
                 w2 = kx2 + hdt * g2;
@@ -268,7 +292,7 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
                 sv2 = sv2 + g2;
             }
         }
-        if (a.integrator == 0) {
+        if (INTEG == 0) {
             y0 = x0 + dt6 * sx0;
             y1 = x1 + dt6 * sx1;
             y2 = x2 + dt6 * sx2;
@@ -282,7 +306,7 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
         }
 
         // the deposit record of the step's Hermite midpoint (:372-423)
-        const double gw = 1.0 / lorentz(w0, w1, w2, inv_c2);
+        const double gw = inv_gamma<GENERAL>(w0, w1, w2, inv_c2);
         double m0 = 0.5 * (x0 + y0) + dt * (gv * v0 - gw * w0) / 8.0;
         double m1 = 0.5 * (x1 + y1) + dt * (gv * v1 - gw * w1) / 8.0;
         const double m2 = 0.5 * (x2 + y2) + dt * (gv * v2 - gw * w2) / 8.0;
@@ -292,11 +316,9 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
             m1 = origin_y + fabs(m1 - origin_y);
         if (graded) m0 = uniform_x(m0, a.x_nodes, a.n_x_nodes, origin_x, h);
         {
-            const i64 pp = finest_patch(a, m0, m1);
-            const i64 *pi = a.patch_int + pp * 6;
-            const double *pr = a.patch_real + pp * 7;
-            const i64 pnx = __ldg(pi + 0), pny = __ldg(pi + 1), ofn = __ldg(pi + 5);
-            const double pox = __ldg(pr + 0), poy = __ldg(pr + 1), phh = __ldg(pr + 2);
+            const PatchGeom g = GENERAL ? patch_geom(a, finest_patch(a, P, m0, m1)) : base;
+            const i64 pnx = g.pnx, pny = g.pny, ofn = g.ofn;
+            const double pox = g.pox, poy = g.poy, phh = g.phh;
             i64 i = (i64)floor((m0 - pox) / phh);
             i64 j = (i64)floor((m1 - poy) / phh);
             double u = (m0 - (pox + phh * (double)i)) / phh;
@@ -509,7 +531,9 @@ extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, 
         tr.nx = last[0];
         tr.ny = last[1];
         BT_REQUIRE(tr.nx >= 2 && tr.ny >= 2, "trace: the mesh needs at least 2 x 2 nodes");
+        BT_REQUIRE(a.cylindrical >= 0 && a.cylindrical <= 2, "trace: geometry must be 0, 1 or 2");
         const int S = window > 0 ? (int)window : 64;
+        const bool general = a.n_patches > 1 || a.graded != 0 || a.inv_c2 != 0.0;
         ctx->last_windows = ctx->last_records = ctx->last_flushes = 0;
         if (a.n_active == 0) return;
         bt::TraceScratch &ts = ctx->trace;
@@ -549,7 +573,16 @@ extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, 
             if (used + need > capacity) flush();
             {
                 bt::Timed timed(ctx, "trace_window");
-                BT_LAUNCH(ctx, bt::trace_window, bt::blocks_for(n_act, 128), 128, 0, st, tr, act_a, n_act, S, keys + used, RU + used, RW + used, RQ + used, sentinel);
+                const unsigned grid = (unsigned)bt::blocks_for(n_act, 128);
+#define BT_TRACE_CASE(C, I, G)                                                                  \
+    if (a.cylindrical == C && (a.integrator != 0) == (I != 0) && general == G)                  \
+        BT_LAUNCH(ctx, (bt::trace_window<C, I, G>), grid, 128, 0, st, tr, act_a, n_act, S,       \
+                  keys + used, RU + used, RW + used, RQ + used, sentinel);
+                BT_TRACE_CASE(0, 0, false) BT_TRACE_CASE(0, 0, true) BT_TRACE_CASE(0, 1, false)
+                BT_TRACE_CASE(0, 1, true) BT_TRACE_CASE(1, 0, false) BT_TRACE_CASE(1, 0, true)
+                BT_TRACE_CASE(1, 1, false) BT_TRACE_CASE(1, 1, true) BT_TRACE_CASE(2, 0, false)
+                BT_TRACE_CASE(2, 0, true) BT_TRACE_CASE(2, 1, false) BT_TRACE_CASE(2, 1, true)
+#undef BT_TRACE_CASE
             }
             BT_CHECK_LAUNCH();
             used += need;
