@@ -97,6 +97,7 @@ SIGNATURES: dict[str, list] = {
     "bt_poisson_create": [P, ctypes.POINTER(MeshDesc), ctypes.POINTER(P)],
     "bt_poisson_destroy": [P],
     "bt_poisson_set_region": [P, P, F64],
+    "bt_poisson_set_options": [P, I32, I32, I32, I64],
     "bt_poisson_solve": [
         P, P, P, F64, F64, F64, I32, F64, F64, I32,
         ctypes.POINTER(I32), ctypes.POINTER(I32),

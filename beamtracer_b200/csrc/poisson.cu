@@ -30,7 +30,10 @@ struct Axis {
     i64 n = 0, nc = 0;
     bool coarsened = false;
     Buffer lo, w, cidx;  // per fine node: coarse index and its weight; per coarse: fine index
+    Buffer r0, rw;       // per coarse node: its first fine node and kRestrict weights from there
 };
+
+constexpr int kRestrict = 4;  // fine nodes per axis that one coarse node restricts from
 
 struct Level {
     i64 nx = 0, ny = 0, n = 0;
@@ -41,7 +44,9 @@ struct Level {
     Buffer a9;      // coarse levels: 9 coefficients per node, (dI + 1) * 3 + (dJ + 1)
     Buffer active;  // uint8: free (level 0) or a nonzero row (coarse)
     Buffer x, b, r;
-    Axis ax, ay;  // the map to the next coarser level
+    Buffer x2;              // the second x of staged smoothing (it writes the other buffer)
+    double *cur = nullptr;  // which of x, x2 holds the level's x while a V-cycle is recorded
+    Axis ax, ay;            // the map to the next coarser level
 };
 
 __device__ __forceinline__ double pw(const int32_t *lo, const double *w, i64 k, i64 I) {
@@ -154,6 +159,8 @@ struct Fine {
     const int32_t *lox, *loy;
     const double *wx, *wy;
     const int32_t *cix, *ciy;  // fine index of each coarse node
+    const int32_t *rx0, *ry0;  // restriction: first fine node of each coarse node
+    const double *rxw, *ryw;   //   and kRestrict weights from it (zero: not a neighbour)
     i64 ncx, ncy;
 };
 
@@ -252,7 +259,7 @@ struct PlainLoad {
 };
 
 // The nodes of one of four colours (i % 2, j % 2) of a 9-point level: item t of `count`.
-__device__ __forceinline__ i64 colour_count(i64 nx, i64 ny, int colour) {
+__host__ __device__ __forceinline__ i64 colour_count(i64 nx, i64 ny, int colour) {
     const int ci = colour >> 1, cj = colour & 1;
     return ((nx - ci + 1) / 2) * ((ny - cj + 1) / 2);
 }
@@ -288,6 +295,149 @@ __global__ void smooth9(i64 nx, i64 ny, const double *__restrict__ a9,
     const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= colour_count(nx, ny, colour)) return;
     smooth9_item(t, nx, ny, a9, active, b, x, colour, PlainLoad{});
+}
+
+// -- smoothing staged through shared memory -------------------------------------------------
+//
+// One launch runs up to kMaxPhases colour phases of Gauss-Seidel on a tile of interior
+// nodes plus a halo as wide as the phases (phase k is exact on the halo's rings k + 1 and
+// inward, so after the last phase the interior is exactly what per-colour launches give).
+// The tile's coefficients, right-hand side, active flags and x are read from global memory
+// once, each phase then runs from shared memory, and the interior is written to a second x
+// buffer: no block reads what another block of the same launch writes.  Coefficients and b
+// are stored compacted by colour, so the threads of a phase read consecutive words; x keeps
+// the tile's natural layout.
+constexpr int kMaxPhases = 8;
+constexpr int kStageThreads = 512;
+constexpr int kStage5X = 32, kStage5Y = 32;  // 5-point level: interior rows x columns
+constexpr int kStage9X = 16, kStage9Y = 32;  // 9-point levels
+
+struct Phases {
+    int count;
+    int colour[kMaxPhases];
+};
+
+// The halo of `count` phases: rounded up to even, so the tile's origin has even (i, j)
+// and a node's colour follows from its place in the tile.
+__host__ __device__ inline int stage_halo(int count) { return (count + 1) & ~1; }
+
+__host__ __device__ inline size_t stage_smem(bool nine, int tx, int ty, int halo) {
+    const size_t m = (size_t)(tx + 2 * halo) * (ty + 2 * halo);
+    return m * sizeof(double) * (nine ? 11 : 7) + m;
+}
+
+template <bool NINE, int R>
+__global__ void __launch_bounds__(kStageThreads) smooth_staged(
+    i64 nx, i64 ny, const double *__restrict__ c4, const double *__restrict__ diag,
+    const double *__restrict__ a9, const uint8_t *__restrict__ active,
+    const double *__restrict__ b, const double *__restrict__ xin, double *__restrict__ xout,
+    int tx, int ty, Phases ph) {
+    extern __shared__ double sm[];
+    constexpr int Q = NINE ? 9 : 5;  // coefficients per node (5-point: w, e, s, n, diagonal)
+    constexpr int K = NINE ? 4 : 2;  // colours
+    const int halo = stage_halo(ph.count);
+    const int wx = tx + 2 * halo, wy = ty + 2 * halo, m = wx * wy, per = m / K, hy = wy / 2;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    double *coef = sm;          // [Q][m], position slot(a, c)
+    double *bs = coef + Q * m;  // [m], position slot(a, c)
+    double *xs = bs + m;        // [m], natural a * wy + c
+    uint8_t *act = reinterpret_cast<uint8_t *>(xs + m);
+    // the compacted position of tile node (a, c): its colour's block, then its index there
+    auto slot = [&](int a, int c) -> int {
+        if (NINE) return (((a & 1) << 1) | (c & 1)) * per + (a >> 1) * hy + (c >> 1);
+        return ((a + c) & 1) * per + ((a * wy + c) >> 1);
+    };
+    const i64 i0 = (i64)blockIdx.x * tx - halo, j0 = (i64)blockIdx.y * ty - halo;
+    const i64 n = nx * ny;
+#pragma unroll 4
+    for (int e = tid; e < m; e += nt) {
+        const int a = e / wy, c = e - a * wy;
+        const i64 i = i0 + a, j = j0 + c;
+        const int pos = slot(a, c);
+        double xv = 0.0, bv = 0.0;
+        uint8_t av = 0;
+        if (i >= 0 && i < nx && j >= 0 && j < ny) {
+            const i64 f = i * ny + j;
+            xv = xin[f];
+            av = active[f];
+            if (av) {
+                bv = b[f];
+                if (NINE) {
+#pragma unroll
+                    for (int q = 0; q < 9; ++q) coef[q * m + pos] = a9[(i64)q * n + f];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) coef[q * m + pos] = c4[(i64)q * n + f];
+                    coef[4 * m + pos] = diag[f];
+                }
+            }
+        }
+        xs[e] = xv;
+        bs[pos] = bv;
+        act[pos] = av;
+    }
+    __syncthreads();
+    // The nodes this thread updates: node u = tid + r nt of each colour's compacted list,
+    // with its place in x's layout and its ring (its distance from the tile's edge; -1 for
+    // a node it never updates: past the list, outside the mesh, or held).  A neighbour
+    // outside the mesh holds x = 0 in the tile and adds nothing: no bounds tests.
+    int xi[K][R], ring[K][R];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int u = tid + r * nt;
+            int a = 0, c = 0;
+            if (NINE) {
+                const int ua = u / hy;
+                a = 2 * ua + (k >> 1);
+                c = 2 * (u - ua * hy) + (k & 1);
+            } else {
+                a = u / hy;
+                c = 2 * (u - a * hy) + ((a + k) & 1);
+            }
+            const i64 i = i0 + a, j = j0 + c;
+            const bool mine = u < per && i >= 0 && i < nx && j >= 0 && j < ny && act[k * per + u];
+            xi[k][r] = a * wy + c;
+            ring[k][r] = mine ? min(min(a, wx - 1 - a), min(c, wy - 1 - c)) : -1;
+        }
+    }
+    for (int kk = 0; kk < ph.count; ++kk) {
+        const int colour = ph.colour[kk];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (k != colour) continue;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (ring[k][r] <= kk) continue;  // phase kk is exact from ring kk + 1 inward
+                const int pos = k * per + tid + r * nt, q = xi[k][r];
+                double s = bs[pos];
+                if (NINE) {
+                    s -= coef[pos] * xs[q - wy - 1];
+                    s -= coef[m + pos] * xs[q - wy];
+                    s -= coef[2 * m + pos] * xs[q - wy + 1];
+                    s -= coef[3 * m + pos] * xs[q - 1];
+                    s -= coef[5 * m + pos] * xs[q + 1];
+                    s -= coef[6 * m + pos] * xs[q + wy - 1];
+                    s -= coef[7 * m + pos] * xs[q + wy];
+                    s -= coef[8 * m + pos] * xs[q + wy + 1];
+                } else {
+                    s += coef[pos] * xs[q - wy];
+                    s += coef[m + pos] * xs[q + wy];
+                    s += coef[2 * m + pos] * xs[q - 1];
+                    s += coef[3 * m + pos] * xs[q + 1];
+                }
+                xs[q] = s / coef[4 * m + pos];
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < tx * ty; e += nt) {
+        const int ea = e / ty;
+        const int a = halo + ea, c = halo + (e - ea * ty);
+        const i64 i = i0 + a, j = j0 + c;
+        if (i < nx && j < ny) xout[i * ny + j] = xs[a * wy + c];
+    }
 }
 
 // y = A x (level 0, 5-point) on active rows, 0 elsewhere; with b: r = b - A x.
@@ -340,22 +490,30 @@ __global__ void residual9(i64 nx, i64 ny, const double *__restrict__ a9,
     residual9_item(f, nx, ny, a9, active, x, b, r, PlainLoad{});
 }
 
+// bc[t] = (R r)[t] over the active fine nodes (weighted by the control volumes on level 0),
+// xc[t] = 0.  The terms are those of the fine nodes with a nonzero prolongation weight, in
+// ascending (k, l) order; the weights and the fine values are independent loads.
 template <class Load>
 __device__ __forceinline__ void restrict_item(i64 t, const Fine &F, const double *r, double *bc,
                                               double *xc, Load load) {
     const i64 I = t / F.ncy, J = t - I * F.ncy;
-    const i64 k0 = I > 0 ? F.cix[I - 1] : 0, k1 = I < F.ncx - 1 ? F.cix[I + 1] : F.nx - 1;
-    const i64 l0 = J > 0 ? F.ciy[J - 1] : 0, l1 = J < F.ncy - 1 ? F.ciy[J + 1] : F.ny - 1;
+    const i64 k0 = F.rx0[I], l0 = F.ry0[J];
+    double px[kRestrict], py[kRestrict];
+#pragma unroll
+    for (int a = 0; a < kRestrict; ++a) {
+        px[a] = F.rxw[kRestrict * I + a];
+        py[a] = F.ryw[kRestrict * J + a];
+    }
     double s = 0.0;
-    for (i64 k = k0; k <= k1; ++k) {
-        const double pk = pw(F.lox, F.wx, k, I);
-        if (pk == 0.0) continue;
-        for (i64 l = l0; l <= l1; ++l) {
-            const double pl = pw(F.loy, F.wy, l, J);
-            if (pl == 0.0) continue;
-            const i64 f = k * F.ny + l;
+#pragma unroll
+    for (int a = 0; a < kRestrict; ++a) {
+        if (px[a] == 0.0) continue;
+#pragma unroll
+        for (int c = 0; c < kRestrict; ++c) {
+            if (py[c] == 0.0) continue;
+            const i64 f = (k0 + a) * F.ny + l0 + c;
             if (!F.active[f]) continue;
-            s += pk * pl * (F.weight ? F.weight[f] : 1.0) * load(r + f);
+            s += px[a] * py[c] * (F.weight ? F.weight[f] : 1.0) * load(r + f);
         }
     }
     bc[t] = s;
@@ -499,7 +657,8 @@ __global__ void five_to_nine(i64 n, const double *__restrict__ c4, const double 
 // -- the small levels in one launch, in shared memory ---------------------------------------
 
 constexpr int kTailThreads = 1024;
-constexpr i64 kTailLevelNodes = 4096;  // levels at most this large go to the tail
+constexpr int kTailMaxLevels = 16;
+constexpr size_t kTailSmemMax = 200 * 1024;
 
 struct TailLevel {
     i64 nx, ny, n;
@@ -509,77 +668,275 @@ struct TailLevel {
     Fine next;      // the map to the next coarser level (unused on the coarsest)
 };
 
-// The V-cycle of the small levels in one block: the x, b and r of every tail level staged
-// in shared memory (levels[0].b read from global memory, levels[0].x written back), the
-// coefficients read through the L1 cache; four-colour Gauss-Seidel, residual and
-// restriction down, the coarsest level's inverse, prolongation and smoothing up, with a
-// block barrier between steps.
-__global__ void __launch_bounds__(kTailThreads, 1)
-vcycle_tail(const TailLevel *__restrict__ levels, int count, const double *__restrict__ inv,
-            int sweeps) {
-    extern __shared__ double sm[];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const PlainLoad load{};
-    // level l's x, b, r in shared memory
-    auto X = [&](int l) {
-        i64 off = 0;
-        for (int k = 0; k < l; ++k) off += 3 * levels[k].n;
-        return sm + off;
-    };
-    {
-        const TailLevel &L = levels[0];
-        double *x = X(0);
-        for (i64 f = tid; f < L.n; f += nt) {
-            x[f] = 0.0;
-            x[L.n + f] = L.b[f];
-        }
-        __syncthreads();
+// Where a tail level lives in shared memory: offsets in doubles from the start, in int32s
+// from the int block, in bytes from the byte block.
+struct TailPlan {
+    int nx, ny, n, ncx, ncy;
+    int x, b, r, a9;         // x: (nx + 2) (ny + 2) with a ring of zeros; b, r: n; a9: 9 n
+    int wx, wy, rxw, ryw;    // transfer weights to the next level
+    int lox, loy, rx0, ry0;  // transfer indices (ints)
+    int act;                 // active flags (bytes)
+};
+
+struct TailLayout {
+    std::vector<TailPlan> plan;
+    int doubles = 0, ints = 0, bytes = 0, inv = 0;
+    size_t total() const {
+        return sizeof(double) * (size_t)doubles + sizeof(int32_t) * (size_t)ints + (size_t)bytes;
     }
-    for (int l = 0; l + 1 < count; ++l) {
+};
+
+// The V-cycle of the small levels in one block, entirely in shared memory: every tail
+// level's x (with a ring of zeros around the mesh, so stencils need no bounds tests), b, r,
+// coefficients, active flags and transfer tables and the coarsest level's inverse are
+// staged once (levels[0].b read from global memory, levels[0].x written back at the end);
+// four-colour Gauss-Seidel, residual and restriction down, the coarsest level's inverse,
+// prolongation and smoothing up, with a block barrier between steps.  A zero neighbour
+// outside the mesh changes no sum, so the values are those of the launched kernels.
+__device__ __forceinline__ void tail_smooth(const TailPlan &P, double *sm, const uint8_t *act,
+                                            int colour, int tid, int nt) {
+    const int nx = P.nx, ny = P.ny, n = P.n, W = ny + 2;
+    const int ci = colour >> 1, cj = colour & 1;
+    const int hx = (nx - ci + 1) >> 1, hy = (ny - cj + 1) >> 1;
+    double *x = sm + P.x;
+    const double *b = sm + P.b, *a9 = sm + P.a9;
+    for (int t = tid; t < hx * hy; t += nt) {
+        const int ti = t / hy;
+        const int i = 2 * ti + ci, j = 2 * (t - ti * hy) + cj;
+        const int f = i * ny + j;
+        if (!act[f]) continue;
+        const int q = (i + 1) * W + j + 1;
+        double s = b[f];
+        s -= a9[f] * x[q - W - 1];
+        s -= a9[n + f] * x[q - W];
+        s -= a9[2 * n + f] * x[q - W + 1];
+        s -= a9[3 * n + f] * x[q - 1];
+        s -= a9[5 * n + f] * x[q + 1];
+        s -= a9[6 * n + f] * x[q + W - 1];
+        s -= a9[7 * n + f] * x[q + W];
+        s -= a9[8 * n + f] * x[q + W + 1];
+        x[q] = s / a9[4 * n + f];
+    }
+}
+
+__device__ __forceinline__ void tail_residual(const TailPlan &P, double *sm, const uint8_t *act,
+                                              int tid, int nt) {
+    const int ny = P.ny, n = P.n, W = ny + 2;
+    const double *x = sm + P.x, *b = sm + P.b, *a9 = sm + P.a9;
+    double *r = sm + P.r;
+    for (int f = tid; f < n; f += nt) {
+        if (!act[f]) {
+            r[f] = 0.0;
+            continue;
+        }
+        const int i = f / ny;
+        const int q = f + 2 * i + W + 1;
+        double s = b[f];
+        s -= a9[f] * x[q - W - 1];
+        s -= a9[n + f] * x[q - W];
+        s -= a9[2 * n + f] * x[q - W + 1];
+        s -= a9[3 * n + f] * x[q - 1];
+        s -= a9[4 * n + f] * x[q];
+        s -= a9[5 * n + f] * x[q + 1];
+        s -= a9[6 * n + f] * x[q + W - 1];
+        s -= a9[7 * n + f] * x[q + W];
+        s -= a9[8 * n + f] * x[q + W + 1];
+        r[f] = s;
+    }
+}
+
+// b of the next level = R r of this one (the next level's x is zero already).
+__device__ __forceinline__ void tail_restrict(const TailPlan &P, const TailPlan &C, double *sm,
+                                              const int32_t *smi, const uint8_t *act, int tid,
+                                              int nt) {
+    const int ny = P.ny, ncy = P.ncy;
+    const double *r = sm + P.r, *rxw = sm + P.rxw, *ryw = sm + P.ryw;
+    const int32_t *rx0 = smi + P.rx0, *ry0 = smi + P.ry0;
+    double *bc = sm + C.b;
+    for (int t = tid; t < C.n; t += nt) {
+        const int I = t / ncy, J = t - I * ncy;
+        const int k0 = rx0[I], l0 = ry0[J];
+        double s = 0.0;
+#pragma unroll
+        for (int a = 0; a < kRestrict; ++a) {
+            const double px = rxw[kRestrict * I + a];
+            if (px == 0.0) continue;
+#pragma unroll
+            for (int c = 0; c < kRestrict; ++c) {
+                const double py = ryw[kRestrict * J + c];
+                if (py == 0.0) continue;
+                const int f = (k0 + a) * ny + l0 + c;
+                if (!act[f]) continue;
+                s += px * py * 1.0 * r[f];
+            }
+        }
+        bc[t] = s;
+    }
+}
+
+// x of this level += P x of the next level.
+__device__ __forceinline__ void tail_prolong(const TailPlan &P, const TailPlan &C, double *sm,
+                                             const int32_t *smi, const uint8_t *act, int tid,
+                                             int nt) {
+    const int ny = P.ny, n = P.n, W = ny + 2, ncx = P.ncx, ncy = P.ncy, Wc = ncy + 2;
+    double *x = sm + P.x;
+    const double *xc = sm + C.x, *wxs = sm + P.wx, *wys = sm + P.wy;
+    const int32_t *lox = smi + P.lox, *loy = smi + P.loy;
+    for (int f = tid; f < n; f += nt) {
+        if (!act[f]) continue;
+        const int k = f / ny, l = f - k * ny;
+        const int ix = lox[k], iy = loy[l];
+        const double wx = wxs[k], wy = wys[l];
+        double s = 0.0;
+        for (int sx = 0; sx < 2; ++sx) {
+            const double px = sx ? 1.0 - wx : wx;
+            if (px == 0.0 || ix + sx >= ncx) continue;
+            for (int sy = 0; sy < 2; ++sy) {
+                const double py = sy ? 1.0 - wy : wy;
+                if (py == 0.0 || iy + sy >= ncy) continue;
+                s += px * py * xc[(ix + sx + 1) * Wc + iy + sy + 1];
+            }
+        }
+        const int q = f + 2 * k + W + 1;
+        x[q] = x[q] + s;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void stage(T *dst, const T *src, int count, int tid, int nt) {
+#pragma unroll 4
+    for (int e = tid; e < count; e += nt) dst[e] = src[e];
+}
+
+__global__ void __launch_bounds__(kTailThreads, 1)
+vcycle_tail(const TailLevel *__restrict__ levels, const TailPlan *__restrict__ plans, int count,
+            const double *__restrict__ inv, int inv_at, int doubles, int ints, int sweeps) {
+    extern __shared__ double sm[];
+    __shared__ TailPlan plan[kTailMaxLevels];
+    int32_t *smi = reinterpret_cast<int32_t *>(sm + doubles);
+    uint8_t *smb = reinterpret_cast<uint8_t *>(smi + ints);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    {
+        const int *src = reinterpret_cast<const int *>(plans);
+        int *dst = reinterpret_cast<int *>(plan);
+        const int words = count * (int)(sizeof(TailPlan) / sizeof(int));
+        for (int e = tid; e < words; e += nt) dst[e] = src[e];
+    }
+    for (int l = 0; l < count; ++l) {
         const TailLevel &L = levels[l];
-        double *x = X(l), *b = x + L.n, *r = b + L.n;
+        const TailPlan &P = plans[l];
+        stage(sm + P.a9, L.a9, 9 * P.n, tid, nt);
+        stage(smb + P.act, L.active, P.n, tid, nt);
+        for (int e = tid; e < (P.nx + 2) * (P.ny + 2); e += nt) sm[P.x + e] = 0.0;
+        if (l + 1 < count) {
+            const Fine &G = L.next;
+            stage(sm + P.wx, G.wx, P.nx, tid, nt);
+            stage(sm + P.wy, G.wy, P.ny, tid, nt);
+            stage(sm + P.rxw, G.rxw, kRestrict * P.ncx, tid, nt);
+            stage(sm + P.ryw, G.ryw, kRestrict * P.ncy, tid, nt);
+            stage(smi + P.lox, G.lox, P.nx, tid, nt);
+            stage(smi + P.loy, G.loy, P.ny, tid, nt);
+            stage(smi + P.rx0, G.rx0, P.ncx, tid, nt);
+            stage(smi + P.ry0, G.ry0, P.ncy, tid, nt);
+        }
+    }
+    {
+        const int nc = plans[count - 1].n;
+        stage(sm + inv_at, inv, nc * nc, tid, nt);
+        stage(sm + plans[0].b, levels[0].b, plans[0].n, tid, nt);
+    }
+    __syncthreads();
+    for (int l = 0; l + 1 < count; ++l) {
+        const TailPlan &P = plan[l];
+        const uint8_t *act = smb + P.act;
         for (int s = 0; s < sweeps; ++s)
             for (int c = 0; c < 4; ++c) {
-                const i64 m = colour_count(L.nx, L.ny, c);
-                for (i64 t = tid; t < m; t += nt) smooth9_item(t, L.nx, L.ny, L.a9, L.active, b, x, c, load);
+                tail_smooth(P, sm, act, c, tid, nt);
                 __syncthreads();
             }
-        for (i64 f = tid; f < L.n; f += nt) residual9_item(f, L.nx, L.ny, L.a9, L.active, x, b, r, load);
+        tail_residual(P, sm, act, tid, nt);
         __syncthreads();
-        const TailLevel &C = levels[l + 1];
-        double *xc = X(l + 1), *bc = xc + C.n;
-        for (i64 t = tid; t < C.n; t += nt) restrict_item(t, L.next, r, bc, xc, load);
+        tail_restrict(P, plan[l + 1], sm, smi, act, tid, nt);
         __syncthreads();
     }
     {
-        const TailLevel &C = levels[count - 1];
-        double *x = X(count - 1), *b = x + C.n;
-        const int n = (int)C.n;
+        const TailPlan &C = plan[count - 1];
+        const int n = C.n, W = C.ny + 2;
+        const double *b = sm + C.b, *iv = sm + inv_at;
         for (int row = tid; row < n; row += nt) {
             double s = 0.0;
-            for (int c = 0; c < n; ++c) s += __ldg(inv + row * n + c) * b[c];
-            x[row] = s;
+            for (int c = 0; c < n; ++c) s += iv[row * n + c] * b[c];
+            const int i = row / C.ny;
+            sm[C.x + row + 2 * i + W + 1] = s;
         }
         __syncthreads();
     }
     for (int l = count - 2; l >= 0; --l) {
-        const TailLevel &L = levels[l];
-        double *x = X(l), *b = x + L.n;
-        const double *xc = X(l + 1);
-        for (i64 f = tid; f < L.n; f += nt) prolong_item(f, L.next, xc, x, load);
+        const TailPlan &P = plan[l];
+        const uint8_t *act = smb + P.act;
+        tail_prolong(P, plan[l + 1], sm, smi, act, tid, nt);
         __syncthreads();
         for (int s = 0; s < sweeps; ++s)
             for (int c = 3; c >= 0; --c) {
-                const i64 m = colour_count(L.nx, L.ny, c);
-                for (i64 t = tid; t < m; t += nt) smooth9_item(t, L.nx, L.ny, L.a9, L.active, b, x, c, load);
+                tail_smooth(P, sm, act, c, tid, nt);
                 __syncthreads();
             }
     }
     {
-        const TailLevel &L = levels[0];
-        const double *x = X(0);
-        for (i64 f = tid; f < L.n; f += nt) L.x[f] = x[f];
+        const TailPlan &P = plan[0];
+        const int W = P.ny + 2;
+        for (int f = tid; f < P.n; f += nt) {
+            const int i = f / P.ny;
+            levels[0].x[f] = sm[P.x + f + 2 * i + W + 1];
+        }
     }
+}
+
+// The shared-memory layout of tail levels first .. (the coarsest).
+TailLayout tail_layout(const std::vector<Level> &levels, int first) {
+    TailLayout T;
+    const int last = (int)levels.size() - 1;
+    for (int l = first; l <= last; ++l) {
+        const Level &L = levels[l];
+        TailPlan P{};
+        P.nx = (int)L.nx;
+        P.ny = (int)L.ny;
+        P.n = (int)L.n;
+        P.x = T.doubles;
+        T.doubles += (P.nx + 2) * (P.ny + 2);
+        P.b = T.doubles;
+        T.doubles += P.n;
+        P.r = T.doubles;
+        T.doubles += P.n;
+        P.a9 = T.doubles;
+        T.doubles += 9 * P.n;
+        if (l < last) {
+            P.ncx = (int)levels[l + 1].nx;
+            P.ncy = (int)levels[l + 1].ny;
+            P.wx = T.doubles;
+            T.doubles += P.nx;
+            P.wy = T.doubles;
+            T.doubles += P.ny;
+            P.rxw = T.doubles;
+            T.doubles += kRestrict * P.ncx;
+            P.ryw = T.doubles;
+            T.doubles += kRestrict * P.ncy;
+            P.lox = T.ints;
+            T.ints += P.nx;
+            P.loy = T.ints;
+            T.ints += P.ny;
+            P.rx0 = T.ints;
+            T.ints += P.ncx;
+            P.ry0 = T.ints;
+            T.ints += P.ncy;
+        }
+        P.act = T.bytes;
+        T.bytes += P.n;
+        T.plan.push_back(P);
+    }
+    T.inv = T.doubles;
+    T.doubles += (int)(levels[last].n * levels[last].n);
+    return T;
 }
 
 // -- dot products: partial sums per block, then an ordered sum (deterministic) -----------
@@ -754,6 +1111,23 @@ void build_axis(Axis &A, i64 n) {
         lo[k] = (int32_t)I;
         w[k] = (c1 - (double)k) / (c1 - c0);
     }
+    // the restriction tables: the prolongation weights read by coarse node
+    std::vector<int32_t> r0(A.nc, 0);
+    std::vector<double> rw((size_t)kRestrict * A.nc, 0.0);
+    for (i64 I = 0; I < A.nc; ++I) {
+        i64 first = -1;
+        for (i64 k = 0; k < n; ++k) {
+            const double p = lo[k] == I ? w[k] : (lo[k] + 1 == I ? 1.0 - w[k] : 0.0);
+            if (p == 0.0) continue;
+            if (first < 0) first = k;
+            BT_REQUIRE(k - first < kRestrict, "poisson: a coarse node restricts from too many nodes");
+            rw[(size_t)kRestrict * I + (k - first)] = p;
+        }
+        r0[I] = (int32_t)std::max<i64>(first, 0);
+    }
+    cudaMemcpy(A.r0.as<int32_t>(A.nc), r0.data(), A.nc * sizeof(int32_t), cudaMemcpyHostToDevice);
+    cudaMemcpy(A.rw.as<double>(kRestrict * A.nc), rw.data(), rw.size() * sizeof(double),
+               cudaMemcpyHostToDevice);
     cudaMemcpy(A.lo.as<int32_t>(n), lo.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice);
     cudaMemcpy(A.w.as<double>(n), w.data(), n * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(A.cidx.as<int32_t>(A.nc), cidx.data(), A.nc * sizeof(int32_t),
@@ -778,9 +1152,16 @@ struct bt_poisson {
     bool built = false;        // hierarchy matches the current diagonal
     bool reaction_on = false;  // level-0 diagonal holds a reaction
     int restart = 30;
+    // the V-cycle's settings (bt_poisson_set_options)
+    int fine_sweeps = 2;    // red-black sweeps on level 0, before and after
+    int coarse_sweeps = 2;  // four-colour sweeps on the 9-point levels
+    int staged = 1;         // smoothing staged through shared memory (else a launch per colour)
+    i64 tail_nodes = 4096;  // levels at most this large may go to the one-block tail
     int tail_start = -1;    // the first level of the V-cycle's one-block tail
-    size_t tail_smem = 0;    // its shared memory: x, b, r of every tail level
+    size_t tail_smem = 0;   // its shared memory
+    int tail_doubles = 0, tail_ints = 0, tail_inv = 0;  // its layout (bt::TailLayout)
     bt::Buffer tail_levels;  // its TailLevel descriptors
+    bt::Buffer tail_plans;   // and TailPlan layouts
     bt::Buffer dot_partial;  // per-block partial dot products
     // the V-cycle from a zero guess on level 0's b into its x, captured once as a graph
     cudaGraph_t vgraph = nullptr;
@@ -821,6 +1202,10 @@ Fine fine_of(Level &L, Level &C, bool first) {
     F.wy = L.ay.w.as<double>(L.ny);
     F.cix = L.ax.cidx.as<int32_t>(L.ax.nc);
     F.ciy = L.ay.cidx.as<int32_t>(L.ay.nc);
+    F.rx0 = L.ax.r0.as<int32_t>(L.ax.nc);
+    F.ry0 = L.ay.r0.as<int32_t>(L.ay.nc);
+    F.rxw = L.ax.rw.as<double>(kRestrict * L.ax.nc);
+    F.ryw = L.ay.rw.as<double>(kRestrict * L.ay.nc);
     F.ncx = C.nx;
     F.ncy = C.ny;
     return F;
@@ -866,7 +1251,122 @@ void build_hierarchy(bt_poisson *p, const double *reaction) {
     p->reaction_on = reaction != nullptr;
 }
 
-// x = V-cycle(b) on level l (x starts at zero on entry for l > 0; level 0's x given).
+// The tail: the longest run of coarsest levels (never level 0, whose operator is 5-point),
+// each at most tail_nodes large, whose shared-memory image fits one block; its descriptors
+// and layout, and the shared memory of the staged smoother.
+void setup_tail(bt_poisson *p) {
+    const int levels = (int)p->levels.size();
+    p->tail_start = -1;
+    p->tail_smem = 0;
+    for (int l = levels - 1; l >= 1 && levels - l <= kTailMaxLevels; --l) {
+        if (p->levels[l].n > p->tail_nodes || tail_layout(p->levels, l).total() > kTailSmemMax)
+            break;
+        p->tail_start = l;
+    }
+    const int big5 = (int)stage_smem(false, kStage5X, kStage5Y, kMaxPhases);
+    const int big9 = (int)stage_smem(true, kStage9X, kStage9Y, kMaxPhases);
+    BT_CUDA(cudaFuncSetAttribute(smooth_staged<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big5));
+    BT_CUDA(cudaFuncSetAttribute(smooth_staged<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big5));
+    BT_CUDA(cudaFuncSetAttribute(smooth_staged<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big9));
+    if (p->tail_start <= 0) return;
+    const TailLayout T = tail_layout(p->levels, p->tail_start);
+    p->tail_smem = T.total();
+    p->tail_doubles = T.doubles;
+    p->tail_ints = T.ints;
+    p->tail_inv = T.inv;
+    std::vector<TailLevel> tail;
+    for (int l = p->tail_start; l < levels; ++l) {
+        Level &L = p->levels[l];
+        TailLevel t{};
+        t.nx = L.nx;
+        t.ny = L.ny;
+        t.n = L.n;
+        t.a9 = L.a9.as<double>(9 * L.n);
+        t.active = L.active.as<uint8_t>(L.n);
+        t.x = L.x.as<double>(L.n);
+        t.b = L.b.as<double>(L.n);
+        if (l + 1 < levels) t.next = fine_of(L, p->levels[l + 1], false);
+        tail.push_back(t);
+    }
+    BT_CUDA(cudaFuncSetAttribute(vcycle_tail, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)p->tail_smem));
+    BT_CUDA(cudaMemcpy(p->tail_levels.as<TailLevel>(tail.size()), tail.data(),
+                       sizeof(TailLevel) * tail.size(), cudaMemcpyHostToDevice));
+    BT_CUDA(cudaMemcpy(p->tail_plans.as<TailPlan>(T.plan.size()), T.plan.data(),
+                       sizeof(TailPlan) * T.plan.size(), cudaMemcpyHostToDevice));
+}
+
+void drop_graphs(bt_poisson *p) {
+    if (p->vexec) cudaGraphExecDestroy(p->vexec);
+    if (p->vgraph) cudaGraphDestroy(p->vgraph);
+    p->vexec = nullptr;
+    p->vgraph = nullptr;
+}
+
+// The smoothing of level l before (pre) or after the coarse correction: red-black sweeps
+// on level 0, four-colour sweeps on 9-point levels, the colours reversed afterwards; the
+// phases in shared-memory staged launches (up to kMaxPhases each) that move x between the
+// level's two buffers, or one in-place launch per colour.
+void smooth(bt_poisson *p, size_t l, bool pre) {
+    cudaStream_t st = p->ctx->stream;
+    Level &L = p->levels[l];
+    const int T = 256;
+    const double *b = L.b.as<double>(L.n);
+    const uint8_t *act = L.active.as<uint8_t>(L.n);
+    const bool five = l == 0;
+    const int colours = five ? 2 : 4;
+    const int sweeps = five ? p->fine_sweeps : p->coarse_sweeps;
+    std::vector<int> order;
+    for (int sw = 0; sw < sweeps; ++sw)
+        for (int c = 0; c < colours; ++c) order.push_back(pre ? c : colours - 1 - c);
+    if (p->staged) {
+        const int tx = five ? kStage5X : kStage9X, ty = five ? kStage5Y : kStage9Y;
+        const dim3 tiles((unsigned)((L.nx + tx - 1) / tx), (unsigned)((L.ny + ty - 1) / ty));
+        for (size_t start = 0; start < order.size(); start += kMaxPhases) {
+            Phases ph{};
+            ph.count = (int)std::min<size_t>(kMaxPhases, order.size() - start);
+            for (int k = 0; k < ph.count; ++k) ph.colour[k] = order[start + k];
+            const int halo = stage_halo(ph.count);
+            const size_t smem = stage_smem(!five, tx, ty, halo);
+            const int per = (tx + 2 * halo) * (ty + 2 * halo) / colours;
+            const int own = (per + kStageThreads - 1) / kStageThreads;
+            double *x = L.x.as<double>(L.n);
+            double *in = L.cur, *out = L.cur == x ? L.x2.as<double>(L.n) : x;
+            if (five && own <= 2)
+                BT_LAUNCH(p->ctx, (smooth_staged<false, 2>), tiles, kStageThreads, smem, st, L.nx,
+                          L.ny, L.c4.as<double>(4 * L.n), L.diag.as<double>(L.n),
+                          (const double *)nullptr, act, b, in, out, tx, ty, ph);
+            else if (five && own == 3)
+                BT_LAUNCH(p->ctx, (smooth_staged<false, 3>), tiles, kStageThreads, smem, st, L.nx,
+                          L.ny, L.c4.as<double>(4 * L.n), L.diag.as<double>(L.n),
+                          (const double *)nullptr, act, b, in, out, tx, ty, ph);
+            else if (!five && own == 1)
+                BT_LAUNCH(p->ctx, (smooth_staged<true, 1>), tiles, kStageThreads, smem, st, L.nx,
+                          L.ny, (const double *)nullptr, (const double *)nullptr,
+                          L.a9.as<double>(9 * L.n), act, b, in, out, tx, ty, ph);
+            else
+                BT_REQUIRE(false, "poisson: staged smoothing tile too large for its block");
+            L.cur = out;
+        }
+        return;
+    }
+    double *x = L.cur;
+    for (int c : order) {
+        if (five) {
+            const i64 per = L.nx * ((L.ny + 1) / 2);
+            BT_LAUNCH(p->ctx, smooth5, blocks_for(per, T), T, 0, st, L.nx, L.ny,
+                      L.c4.as<double>(4 * L.n), L.diag.as<double>(L.n), act, b, x, c);
+        } else {
+            const i64 per = colour_count(L.nx, L.ny, c);
+            BT_LAUNCH(p->ctx, smooth9, blocks_for(per, T), T, 0, st, L.nx, L.ny,
+                      L.a9.as<double>(9 * L.n), act, b, x, c);
+        }
+    }
+}
+
+// x = V-cycle(b) on level l (x starts at zero on entry for l > 0; level 0's x given).  The
+// staged smoother moves a level's x between its two buffers; the cycle leaves it in the
+// first.
 void vcycle(bt_poisson *p, size_t l) {
     cudaStream_t st = p->ctx->stream;
     Level &L = p->levels[l];
@@ -875,7 +1375,9 @@ void vcycle(bt_poisson *p, size_t l) {
         const int count = (int)(p->levels.size() - l);
         const Level &Lc = p->levels.back();
         BT_LAUNCH(p->ctx, vcycle_tail, 1, kTailThreads, p->tail_smem, st,
-                  p->tail_levels.as<TailLevel>(count), count, p->inv.as<double>(Lc.n * Lc.n), 2);
+                  p->tail_levels.as<TailLevel>(count), p->tail_plans.as<TailPlan>(count), count,
+                  p->inv.as<double>(Lc.n * Lc.n), p->tail_inv, p->tail_doubles, p->tail_ints,
+                  p->coarse_sweeps);
         return;
     }
     if (l + 1 == p->levels.size()) {
@@ -884,46 +1386,29 @@ void vcycle(bt_poisson *p, size_t l) {
         return;
     }
     Level &C = p->levels[l + 1];
-    double *x = L.x.as<double>(L.n), *b = L.b.as<double>(L.n), *r = L.r.as<double>(L.n);
+    double *b = L.b.as<double>(L.n), *r = L.r.as<double>(L.n);
     const uint8_t *act = L.active.as<uint8_t>(L.n);
-    const int sweeps = 2;
-    if (l == 0) {
-        const double *c4 = L.c4.as<double>(4 * L.n), *dg = L.diag.as<double>(L.n);
-        const i64 per = L.nx * ((L.ny + 1) / 2);
-        for (int s = 0; s < sweeps; ++s)
-            for (int c = 0; c < 2; ++c)
-                BT_LAUNCH(p->ctx, smooth5, blocks_for(per, T), T, 0, st, L.nx, L.ny, c4, dg, act, b, x, c);
-        BT_LAUNCH(p->ctx, apply5, blocks_for(L.n, T), T, 0, st, L.nx, L.ny, c4, dg, act, x, b, r);
-    } else {
-        const double *a9 = L.a9.as<double>(9 * L.n);
-        const i64 per = ((L.nx + 1) / 2) * ((L.ny + 1) / 2);
-        for (int s = 0; s < sweeps; ++s)
-            for (int c = 0; c < 4; ++c)
-                BT_LAUNCH(p->ctx, smooth9, blocks_for(per, T), T, 0, st, L.nx, L.ny, a9, act, b, x, c);
-        BT_LAUNCH(p->ctx, residual9, blocks_for(L.n, T), T, 0, st, L.nx, L.ny, a9, act, x, b, r);
-    }
+    L.cur = L.x.as<double>(L.n);
+    smooth(p, l, true);
+    if (l == 0)
+        BT_LAUNCH(p->ctx, apply5, blocks_for(L.n, T), T, 0, st, L.nx, L.ny, L.c4.as<double>(4 * L.n),
+                  L.diag.as<double>(L.n), act, L.cur, b, r);
+    else
+        BT_LAUNCH(p->ctx, residual9, blocks_for(L.n, T), T, 0, st, L.nx, L.ny,
+                  L.a9.as<double>(9 * L.n), act, L.cur, b, r);
     Fine F = fine_of(L, C, l == 0);
     BT_LAUNCH(p->ctx, restrict_residual, blocks_for(C.n, T), T, 0, st, F, r, C.b.as<double>(C.n),
                                                           C.x.as<double>(C.n));
     vcycle(p, l + 1);
-    BT_LAUNCH(p->ctx, prolong_add, blocks_for(L.n, T), T, 0, st, F, C.x.as<double>(C.n), x);
-    if (l == 0) {
-        const double *c4 = L.c4.as<double>(4 * L.n), *dg = L.diag.as<double>(L.n);
-        const i64 per = L.nx * ((L.ny + 1) / 2);
-        for (int s = 0; s < sweeps; ++s)
-            for (int c = 1; c >= 0; --c)
-                BT_LAUNCH(p->ctx, smooth5, blocks_for(per, T), T, 0, st, L.nx, L.ny, c4, dg, act, b, x, c);
-    } else {
-        const double *a9 = L.a9.as<double>(9 * L.n);
-        const i64 per = ((L.nx + 1) / 2) * ((L.ny + 1) / 2);
-        for (int s = 0; s < sweeps; ++s)
-            for (int c = 3; c >= 0; --c)
-                BT_LAUNCH(p->ctx, smooth9, blocks_for(per, T), T, 0, st, L.nx, L.ny, a9, act, b, x, c);
-    }
+    BT_LAUNCH(p->ctx, prolong_add, blocks_for(L.n, T), T, 0, st, F, C.x.as<double>(C.n), L.cur);
+    smooth(p, l, false);
+    if (L.cur != L.x.as<double>(L.n))
+        BT_CUDA(cudaMemcpyAsync(L.x.as<double>(L.n), L.cur, sizeof(double) * L.n,
+                                cudaMemcpyDeviceToDevice, st));
+    L.cur = L.x.as<double>(L.n);
     BT_CHECK_LAUNCH();
 }
 
-// z = M v: one V-cycle from zero
 // Capture the V-cycle (level 0's x zeroed, then the cycle on its b) as a graph: every
 // buffer it touches keeps its address for the solver's life, so one capture serves every
 // solve and every Newton Jacobian (whose coefficients change in place).
@@ -1107,6 +1592,7 @@ extern "C" int bt_poisson_create(bt_ctx *ctx, const bt_mesh_desc *m, bt_poisson 
                 L.ny = ny;
                 L.n = nx * ny;
                 L.x.as<double>(L.n);
+                L.x2.as<double>(L.n);
                 L.b.as<double>(L.n);
                 L.r.as<double>(L.n);
                 L.active.as<uint8_t>(L.n);
@@ -1126,36 +1612,7 @@ extern "C" int bt_poisson_create(bt_ctx *ctx, const bt_mesh_desc *m, bt_poisson 
                 ny = L.ay.nc;
             }
             BT_REQUIRE(p->levels.back().n <= bt::kCoarsest, "poisson: coarsest level too large");
-            // the tail: every level from the first small one (never level 0, whose
-            // operator is 5-point) down to the coarsest, in one cluster launch
-            for (size_t l = 1; l < p->levels.size(); ++l)
-                if (p->levels[l].n <= bt::kTailLevelNodes) {
-                    p->tail_start = (int)l;
-                    break;
-                }
-            if (p->tail_start > 0) {
-                std::vector<bt::TailLevel> tail;
-                for (size_t l = p->tail_start; l < p->levels.size(); ++l) {
-                    bt::Level &L = p->levels[l];
-                    bt::TailLevel t{};
-                    t.nx = L.nx;
-                    t.ny = L.ny;
-                    t.n = L.n;
-                    t.a9 = L.a9.as<double>(9 * L.n);
-                    t.active = L.active.as<uint8_t>(L.n);
-                    t.x = L.x.as<double>(L.n);
-                    t.b = L.b.as<double>(L.n);
-                    if (l + 1 < p->levels.size()) t.next = bt::fine_of(L, p->levels[l + 1], false);
-                    tail.push_back(t);
-                    p->tail_smem += 3 * sizeof(double) * L.n;
-                }
-                BT_REQUIRE(p->tail_smem <= 200 * 1024, "poisson: the tail levels exceed shared memory");
-                BT_CUDA(cudaFuncSetAttribute(bt::vcycle_tail,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)p->tail_smem));
-                BT_CUDA(cudaMemcpy(p->tail_levels.as<bt::TailLevel>(tail.size()), tail.data(),
-                                   sizeof(bt::TailLevel) * tail.size(), cudaMemcpyHostToDevice));
-            }
+            bt::setup_tail(p);
             p->src.as<double>(n);
             bt::build_operator(p);
             BT_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1270,5 +1727,23 @@ extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, d
             throw bt::Error{BT_ERR_NOCONV, "field solve: the coarsest operator is singular (is any node held?)"};
         if (newton_steps) *newton_steps = steps;
         if (cycles) *cycles = total_cycles;
+    });
+}
+
+extern "C" int bt_poisson_set_options(bt_poisson *p, int32_t fine_sweeps, int32_t coarse_sweeps,
+                                      int32_t staged, int64_t tail_nodes) {
+    return bt::guarded([&] {
+        BT_REQUIRE(p, "poisson: null solver");
+        BT_REQUIRE(fine_sweeps >= 1 && fine_sweeps <= 4, "poisson: fine_sweeps must be 1 to 4");
+        BT_REQUIRE(coarse_sweeps >= 1 && coarse_sweeps <= 4,
+                   "poisson: coarse_sweeps must be 1 to 4");
+        BT_REQUIRE(tail_nodes >= 1, "poisson: tail_nodes must be positive");
+        BT_CUDA(cudaStreamSynchronize(p->ctx->stream));
+        p->fine_sweeps = fine_sweeps;
+        p->coarse_sweeps = coarse_sweeps;
+        p->staged = staged != 0;
+        p->tail_nodes = tail_nodes;
+        bt::drop_graphs(p);
+        bt::setup_tail(p);
     });
 }

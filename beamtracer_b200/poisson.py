@@ -135,6 +135,15 @@ class IonOpticsPoisson:
         except Exception:
             pass
 
+    def set_options(self, fine_sweeps: int = 2, coarse_sweeps: int = 2, staged: bool = True,
+                    tail_nodes: int = 4096) -> None:
+        """The V-cycle's settings: red-black sweeps on the finest level, four-colour sweeps
+        on the coarse levels, smoothing staged through shared memory or one launch per
+        colour (the same values), and the largest level the one-block tail may take."""
+        _lib.check(_lib.lib().bt_poisson_set_options(self._handle, int(fine_sweeps),
+                                                     int(coarse_sweeps), int(bool(staged)),
+                                                     int(tail_nodes)))  # fmt: skip
+
     # -- the device path --------------------------------------------------------------
 
     def _set_region(self, region: Any, potential: float) -> None:

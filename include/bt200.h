@@ -200,6 +200,14 @@ int bt_poisson_destroy(bt_poisson *p);
  * (solver/vlasov.py:350-355, poisson.py:279-309). */
 int bt_poisson_set_region(bt_poisson *p, const uint8_t *mask, double value);
 
+/* The V-cycle's settings, the solver's tuning knobs (no counterpart in the reference, which
+ * factorises with LU; defaults 2, 2, 1, 4096): red-black sweeps on the finest level and
+ * four-colour sweeps on the coarse levels before and after each coarse correction (1-4),
+ * smoothing staged through shared memory (1) or one launch per colour (0; the same values),
+ * and the size above which a level is never part of the one-block tail. */
+int bt_poisson_set_options(bt_poisson *p, int32_t fine_sweeps, int32_t coarse_sweeps,
+                           int32_t staged, int64_t tail_nodes);
+
 /* poisson.py:809-933 (IonOpticsPoisson.solve).  phi (DEVICE (nx, ny), in/out): the first
  * guess on entry (its fixed nodes are set), the solution on return; rho (DEVICE (nx, ny),
  * C/m^3, or NULL).  With amplitude = 0 one linear solve: GMRES preconditioned by a

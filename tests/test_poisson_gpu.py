@@ -133,3 +133,52 @@ def test_large_mesh_converges(solver):
     print("V-cycles", p.krylov_steps)
     np.testing.assert_allclose(phi, expected, rtol=0, atol=1e-9 * 7e3)
     assert p.krylov_steps < 200
+
+
+def _three_plates(shape, h):
+    def plate(xc):
+        return lambda x, r: (np.abs(x - xc) <= 4 * h) & (r >= shape[1] * h / 3)
+
+    n = shape[0] * h
+    return IonOpticsMesh(shape=shape, origin=(0.0, 0.0), h=h,
+                         electrodes=[Electrode(plate(n / 4), 0.0), Electrode(plate(n / 2), 5e3),
+                                     Electrode(plate(3 * n / 4), 0.0)])  # fmt: skip
+
+
+@pytest.mark.parametrize("sweeps", [(2, 2), (1, 1), (3, 3), (4, 2)])
+def test_staged_smoothing_is_exact(solver, sweeps):
+    """Smoothing staged through shared memory (several phases per launch, two x buffers)
+    gives the values of one launch per colour, and so the same solve."""
+    mesh = _three_plates((331, 97), 0.2e-3)
+    rho = np.zeros(mesh.shape)
+    rho[:, :20] = 2e-5
+    out = []
+    for staged in (False, True):
+        p = solver(mesh)
+        p.set_options(fine_sweeps=sweeps[0], coarse_sweeps=sweeps[1], staged=staged)
+        out.append((p.solve(rho), p.krylov_steps))
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])
+
+
+@pytest.mark.parametrize("tail_nodes", [1, 64, 300, 1 << 20])
+def test_tail_split_converges(solver, tail_nodes):
+    """Any split between launched levels and the one-block tail gives the oracle's field."""
+    mesh = _three_plates((257, 65), 0.2e-3)
+    rho = np.zeros(mesh.shape)
+    rho[:, :10] = 1e-5
+    p = solver(mesh)
+    p.set_options(tail_nodes=tail_nodes)
+    phi = p.solve(rho)
+    expected = oracle.solve(oracle.operator_of_mesh(mesh), rho)
+    np.testing.assert_allclose(phi, expected, rtol=0, atol=1e-9 * 5e3)
+
+
+def test_options_are_checked(solver):
+    p = solver(_plates())
+    with pytest.raises(ValueError):
+        p.set_options(fine_sweeps=0)
+    with pytest.raises(ValueError):
+        p.set_options(coarse_sweeps=5)
+    with pytest.raises(ValueError):
+        p.set_options(tail_nodes=0)
