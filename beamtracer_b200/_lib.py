@@ -64,6 +64,15 @@ class TraceArgs(ctypes.Structure):
     ]  # fmt: skip
 
 
+class MagneticDesc(ctypes.Structure):
+    """``bt_magnetic`` of ``include/bt200.h``."""
+
+    _fields_ = [
+        ("mode", I32), ("order", I32), ("n", I64), ("z0", F64), ("hz", F64),
+        ("axis_y", F64), ("samples", P),
+    ]  # fmt: skip
+
+
 class MeshDesc(ctypes.Structure):
     """``bt_mesh_desc`` of ``include/bt200.h``."""
 
@@ -89,6 +98,8 @@ SIGNATURES: dict[str, list] = {
     "bt_staggered_field_2d": [P, P, P, I64, P, P, I64, I64, F64, F64, F64, P, P],
     "bt_deposit_trajectories_2d": [P, P, P, P, I64, F64, F64, F64, I64, P, I64, I64],
     "bt_deposit_trajectories_2d_noalloc": [P, P, P, P, I64, F64, F64, F64, I64, P, I64, I64],
+    "bt_trace_trajectories_2d_magnetic": [P, ctypes.POINTER(TraceArgs),
+                                          ctypes.POINTER(MagneticDesc), I64],
     "bt_trace_trajectories_2d": [P, ctypes.POINTER(TraceArgs), I64],
     "bt_trace_last_stats": [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64)],
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],

@@ -340,6 +340,20 @@ class NegativeExtractionPlasma:
             raise ValueError(f"ion_temperature must be positive, got {self.ion_temperature}")
 
 
+@dataclass
+class AxialField:
+    """A measured on-axis field ``bz`` [T] sampled at ``z0 + dz k`` [m]
+    (``config.py:370-382``; SI numbers)."""
+
+    z0: float
+    dz: float
+    bz: tuple
+
+    def __post_init__(self) -> None:
+        self.z0, self.dz = float(self.z0), float(self.dz)
+        self.bz = tuple(float(b) for b in self.bz)
+
+
 @dataclass(frozen=True)
 class Solenoid:
     """A thin-walled solenoid on the axis: centre, length, radius [m], peak [T]."""
@@ -446,6 +460,10 @@ class BeamOpticsConfig:
         self.beams = [beam_from_value(beam) for beam in self.beams]
         self.plasma = plasma_from_value(self.plasma)
         self.solenoids = [_coerce(Solenoid, s) for s in self.solenoids]
+        if self.axial_field is not None:
+            self.axial_field = _coerce(AxialField, self.axial_field)
+        if not 0 <= int(self.field_order) <= 6:
+            raise ValueError(f"field_order must be 0 to 6, got {self.field_order}")
         self.compensation = [_coerce(SpaceChargeCompensation, c) for c in self.compensation]
         self.diagnostic_planes = [float(p) for p in self.diagnostic_planes]
         if (self.solenoids or self.axial_field) and self.grid.coordinates != "cylindrical":
@@ -474,8 +492,7 @@ class BeamOpticsConfig:
         unsupported = {
             "field_map": self.field_map, "charge_changing": self.charge_changing,
             "refinement": self.refinement, "adaptive_refinement": self.adaptive_refinement,
-            "self_magnetic_field": self.self_magnetic_field, "solenoids": self.solenoids,
-            "axial_field": self.axial_field,
+            "self_magnetic_field": self.self_magnetic_field,
         }  # fmt: skip
         given = sorted(name for name, value in unsupported.items() if value)
         if given:
@@ -504,6 +521,8 @@ class BeamOpticsConfig:
             entry["type"] = "negative" if isinstance(self.plasma, NegativeExtractionPlasma) else "positive"
             params["plasma"] = entry
         params["solenoids"] = [asdict(s) for s in self.solenoids]
+        if self.axial_field is not None:
+            params["axial_field"] = asdict(self.axial_field)
         params["compensation"] = [asdict(c) for c in self.compensation]
         return params
 

@@ -21,7 +21,8 @@ namespace {
 
 struct Trace {
     bt_trace_args a;
-    i64 nx, ny;  // the last patch's node counts
+    i64 nx, ny;       // the last patch's node counts
+    bt_magnetic mag;  // the magnetic field of the MAG kernels
 };
 
 __device__ __forceinline__ i64 node_cell(double x, const double *__restrict__ nodes, i64 n) {
@@ -119,6 +120,88 @@ __device__ __forceinline__ void edge_field(const bt_trace_args &a, const PatchGe
     ey = low + u * (high - low);
 }
 
+// (B_z, B_r) of an on-axis profile at axial position z and radius r (fields.py:250-279,
+// term by term: the derivatives interpolated between samples, then the series in r).
+__device__ __forceinline__ void axial_field(const bt_magnetic &m, double z, double r,
+                                            double &bz_out, double &br_out) {
+    const i64 n = m.n;
+    const int K = m.order + 1;
+    const double s = (z - m.z0) / m.hz;
+    i64 i = (i64)floor(s);
+    if (i < 3)
+        i = 3;
+    else if (i > n - 5)
+        i = n - 5;
+    const double t = s - (double)i;
+    const double *lo = m.samples + i * K, *hi = lo + K;
+    double d[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+        if (k < K) {
+            const double a = __ldg(lo + k);
+            d[k] = a + t * (__ldg(hi + k) - a);
+        }
+    const double r2 = r * r;
+    const double bz_c[4] = {1.0, -1.0 / 4.0, 1.0 / 64.0, -1.0 / 2304.0};
+    const double br_c[3] = {-1.0 / 2.0, 1.0 / 16.0, -1.0 / 384.0};
+    double bz = d[0], br = 0.0, power = 1.0;
+#pragma unroll
+    for (int k = 1; k <= 3; ++k)
+        if (k <= m.order / 2) {
+            power = power * r2;
+            bz = bz + bz_c[k] * power * d[2 * k];
+        }
+    power = r;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (k < (m.order + 1) / 2) {
+            br = br + br_c[k] * power * d[2 * k + 1];
+            power = power * r2;
+        }
+    bz_out = bz;
+    br_out = br;
+}
+
+// The Cartesian B at (q0, q1, q2): mode 1 on a cylindrical mesh ((cy, cz) the radial unit
+// vector, r the radius), mode 2 a planar mesh with the solenoid axis on y = axis_y.
+__device__ __forceinline__ void magnetic_at(const bt_magnetic &m, double q0, double q1, double r,
+                                            double cy, double cz, double *b) {
+    double bz, br;
+    if (m.mode == 1) {
+        axial_field(m, q0, r, bz, br);
+        b[0] = bz;
+        b[1] = br * cy;
+        b[2] = br * cz;
+    } else {
+        const double yr = q1 - m.axis_y;
+        axial_field(m, q0, fabs(yr), bz, br);
+        b[0] = bz;
+        b[1] = yr < 0.0 ? -br : br;
+        b[2] = 0.0;
+    }
+}
+
+// v <- Boris's kick over tau in the fields e, b (non-relativistic; tracer.py:605-621):
+// v- = v + (tau/2) q/m E, t = (tau/2) q/m B, v+ = v- + (v- + v- x t) x 2t / (1 + t^2),
+// then + (tau/2) q/m E; the operations in the oracle's order.
+__device__ __forceinline__ void kick(double *v, const double *e, const double *b, double tau,
+                                     double qm) {
+    const double f = 0.5 * tau * qm;
+    const double m0 = v[0] + f * e[0], m1 = v[1] + f * e[1], m2 = v[2] + f * e[2];
+    const double t0 = f * b[0], t1 = f * b[1], t2 = f * b[2];
+    const double d = 2.0 / (1.0 + (t0 * t0 + t1 * t1 + t2 * t2));
+    const double s0 = d * t0, s1 = d * t1, s2 = d * t2;
+    const double p0 = m0 + (m1 * t2 - m2 * t1);
+    const double p1 = m1 + (m2 * t0 - m0 * t2);
+    const double p2 = m2 + (m0 * t1 - m1 * t0);
+    const double w0 = m0 + (p1 * s2 - p2 * s1);
+    const double w1 = m1 + (p2 * s0 - p0 * s2);
+    const double w2 = m2 + (p0 * s1 - p1 * s0);
+    v[0] = w0 + f * e[0];
+    v[1] = w1 + f * e[1];
+    v[2] = w2 + f * e[2];
+}
+
 // 1 / gamma of a proper velocity: exactly 1 without relativity (inv_c2 = 0), which the
 // non-general kernels fold away.
 template <bool GENERAL>
@@ -130,7 +213,10 @@ __device__ __forceinline__ double inv_gamma(double u0, double u1, double u2, dou
 // the integrator (0 RK4, 1 Boris) and GENERAL: refined patches, a graded x axis or
 // relativity.  Without them the mesh is one patch, whose shape is read once, and gamma is
 // exactly 1; the operations on every value are the general kernel's, so the results are.
-template <int CYL, int INTEG, bool GENERAL>
+// MAG: the reference's NumPy tracer's step in a magnetic field instead (tracer.py:851-1054):
+// q/m (E + v x B) at every stage, Boris with the rotation, and every step that ends in a
+// cell touching an electrode pauses (status -2) for the caller's exact inside test.
+template <int CYL, int INTEG, bool GENERAL, bool MAG>
 __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restrict__ act,
                                                    i64 n_act, int S,
                                                    uint32_t *__restrict__ keys,
@@ -159,6 +245,7 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
     constexpr int nstage = INTEG == 0 ? 4 : 2;
     int have = 0;
     double ca0 = 0.0, ca1 = 0.0, ca2 = 0.0;
+    double cE[3] = {0, 0, 0}, cB[3] = {0, 0, 0};  // with B: the fields at the step's end
     int s = 0;
     for (; s < S; ++s) {
         if (ns >= a.max_steps) break;
@@ -180,8 +267,14 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
         }
         if (graded) {
             const i64 cg = node_cell(x0, a.x_nodes, a.n_x_nodes);
-            const double d2 = (a.x_nodes[cg + 1] - a.x_nodes[cg]) / h;
-            if (d2 < 1.0) hloc = hloc * d2;
+            if (MAG) {
+                // the NumPy tracer's spacing: the smaller of the cell's edge and h
+                const double dxc = a.x_nodes[cg + 1] - a.x_nodes[cg];
+                if (dxc < hloc) hloc = dxc;
+            } else {
+                const double d2 = (a.x_nodes[cg + 1] - a.x_nodes[cg]) / h;
+                if (d2 < 1.0) hloc = hloc * d2;
+            }
         }
         const double gv = inv_gamma<GENERAL>(v0, v1, v2, inv_c2);
         double q0 = x0, q1 = x1, q2 = x2;
@@ -192,7 +285,49 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
         for (int stage = 0; stage < nstage; ++stage) {
             double gk = inv_gamma<GENERAL>(kx0, kx1, kx2, inv_c2);
             double g0, g1, g2;
-            if (stage == 0 && have != 0) {
+            double E[3], B[3];
+            if (MAG && stage == 0 && have != 0) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    E[c] = cE[c];
+                    B[c] = cB[c];
+                }
+            }
+            if (MAG && !(stage == 0 && have != 0)) {
+                double qy = q1, cy = 0.0, cz = 0.0;
+                if (cyl == 1) {
+                    const double r = radius(q1, q2);
+                    if (r > 0.0) {
+                        cy = q1 / r;
+                        cz = q2 / r;
+                    }
+                    qy = r;
+                }
+                double lq = q0;
+                if (graded) lq = uniform_x(q0, a.x_nodes, a.n_x_nodes, origin_x, h);
+                double ex, ey;
+                const PatchGeom g = GENERAL ? patch_geom(a, finest_patch(a, P, lq, qy)) : base;
+                edge_field(a, g, lq, qy, ex, ey);
+                if (cyl != 0) {
+                    E[0] = ex;
+                    E[1] = ey * cy;
+                    E[2] = ey * cz;
+                } else {
+                    E[0] = ex;
+                    E[1] = ey;
+                    E[2] = 0.0;
+                }
+                magnetic_at(tr.mag, q0, q1, qy, cy, cz, B);
+            }
+            if (MAG) {
+                // q/m (E + v x B) at the stage velocity (tracer.py:519-529)
+                const double c0 = kx1 * B[2] - kx2 * B[1];
+                const double c1 = kx2 * B[0] - kx0 * B[2];
+                const double c2 = kx0 * B[1] - kx1 * B[0];
+                g0 = qmk * (E[0] + c0);
+                g1 = qmk * (E[1] + c1);
+                g2 = qmk * (E[2] + c2);
+            } else if (stage == 0 && have != 0) {
                 g0 = ca0;
                 g1 = ca1;
                 g2 = ca2;
@@ -239,6 +374,18 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
                 dt = a.step_fraction * dt;
                 hdt = 0.5 * dt;
                 dt6 = dt / 6.0;
+                if (INTEG != 0 && MAG) {
+                    // Boris with B: the kick over half the step, then the drift
+                    double u[3] = {v0, v1, v2};
+                    kick(u, E, B, hdt, qmk);
+                    kx0 = u[0];
+                    kx1 = u[1];
+                    kx2 = u[2];
+                    q0 = x0 + dt * kx0;
+                    q1 = x1 + dt * kx1;
+                    q2 = x2 + dt * kx2;
+                    continue;
+                }
                 if (INTEG != 0) {
                     kx0 = v0 + hdt * a0;
                     kx1 = v1 + hdt * a1;
@@ -261,6 +408,19 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
                 kx0 = v0 + hdt * a0;
                 kx1 = v1 + hdt * a1;
                 kx2 = v2 + hdt * a2;
+            } else if (INTEG != 0 && MAG) {
+                // Boris with B: the second kick in the fields at the end of the step
+                double u[3] = {kx0, kx1, kx2};
+                kick(u, E, B, hdt, qmk);
+                w0 = u[0];
+                w1 = u[1];
+                w2 = u[2];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    cE[c] = E[c];
+                    cB[c] = B[c];
+                }
+                have = 1;
             } else if (INTEG != 0) {
                 w0 = kx0 + hdt * g0;
                 w1 = kx1 + hdt * g1;
@@ -411,7 +571,9 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
             if (i < 0) i = 0;
             if (j < 0) j = 0;
             const i64 cell = __ldg(a.cells + i * (ny - 1) + j);
-            if (cell >= 0) {
+            if (MAG && cell >= 0) {
+                st = -2;  // the caller tests the electrodes' shapes
+            } else if (cell >= 0) {
                 const i64 R = a.refine;
                 i64 si = (i64)(((px - origin_x) / h - (double)i) * (double)R);
                 if (si < 0)
@@ -510,8 +672,11 @@ __global__ void scatter_alive(const i64 *__restrict__ act, i64 n, const i64 *__r
 
 }  // namespace bt
 
-extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, int64_t window) {
-    return bt::guarded([&] {
+namespace bt {
+namespace {
+
+void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, int64_t window) {
+    {
         BT_REQUIRE(ctx && args, "trace: null argument");
         const bt_trace_args &a = *args;
         BT_REQUIRE(a.n_patches >= 1 && a.patch_int && a.patch_real, "trace: no patches");
@@ -523,6 +688,18 @@ extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, 
         BT_REQUIRE(a.n_nodes < (int64_t)0xffffffffLL, "trace: too many nodes for 32-bit keys");
         bt::Trace tr;
         tr.a = a;
+        tr.mag = mag ? *mag : bt_magnetic{};
+        if (mag) {
+            BT_REQUIRE(mag->mode == 1 || mag->mode == 2, "trace: magnetic mode must be 1 or 2");
+            BT_REQUIRE(mag->order >= 0 && mag->order <= 6, "trace: magnetic order must be 0 to 6");
+            BT_REQUIRE(mag->n >= 8 && mag->samples, "trace: the profile needs 8 samples");
+            BT_REQUIRE(mag->hz > 0.0, "trace: the profile spacing must be positive");
+            BT_REQUIRE((mag->mode == 1) == (a.cylindrical == 1),
+                       "trace: mode 1 needs a cylindrical mesh, mode 2 a planar one");
+            BT_REQUIRE(a.inv_c2 == 0.0 && a.n_patches == 1,
+                       "trace: the magnetic trace is non-relativistic on one patch");
+            BT_REQUIRE(a.cylindrical != 2, "trace: no magnetic field with a symmetry plane");
+        }
         // the last patch's shape, for the exit and electrode tests
         int64_t last[6];
         BT_CUDA(cudaMemcpyAsync(last, a.patch_int + (a.n_patches - 1) * 6, sizeof(last),
@@ -574,15 +751,24 @@ extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, 
             {
                 bt::Timed timed(ctx, "trace_window");
                 const unsigned grid = (unsigned)bt::blocks_for(n_act, 128);
-#define BT_TRACE_CASE(C, I, G)                                                                  \
-    if (a.cylindrical == C && (a.integrator != 0) == (I != 0) && general == G)                  \
-        BT_LAUNCH(ctx, (bt::trace_window<C, I, G>), grid, 128, 0, st, tr, act_a, n_act, S,       \
+                const int64_t launched = ctx->launch_count;
+#define BT_TRACE_CASE(C, I, G, M)                                                               \
+    if (a.cylindrical == C && (a.integrator != 0) == (I != 0) && general == G &&                 \
+        (mag != nullptr) == M)                                                                   \
+        BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M>), grid, 128, 0, st, tr, act_a, n_act, S,    \
                   keys + used, RU + used, RW + used, RQ + used, sentinel);
-                BT_TRACE_CASE(0, 0, false) BT_TRACE_CASE(0, 0, true) BT_TRACE_CASE(0, 1, false)
-                BT_TRACE_CASE(0, 1, true) BT_TRACE_CASE(1, 0, false) BT_TRACE_CASE(1, 0, true)
-                BT_TRACE_CASE(1, 1, false) BT_TRACE_CASE(1, 1, true) BT_TRACE_CASE(2, 0, false)
-                BT_TRACE_CASE(2, 0, true) BT_TRACE_CASE(2, 1, false) BT_TRACE_CASE(2, 1, true)
+                BT_TRACE_CASE(0, 0, false, false) BT_TRACE_CASE(0, 0, true, false)
+                BT_TRACE_CASE(0, 1, false, false) BT_TRACE_CASE(0, 1, true, false)
+                BT_TRACE_CASE(1, 0, false, false) BT_TRACE_CASE(1, 0, true, false)
+                BT_TRACE_CASE(1, 1, false, false) BT_TRACE_CASE(1, 1, true, false)
+                BT_TRACE_CASE(2, 0, false, false) BT_TRACE_CASE(2, 0, true, false)
+                BT_TRACE_CASE(2, 1, false, false) BT_TRACE_CASE(2, 1, true, false)
+                BT_TRACE_CASE(0, 0, false, true) BT_TRACE_CASE(0, 0, true, true)
+                BT_TRACE_CASE(0, 1, false, true) BT_TRACE_CASE(0, 1, true, true)
+                BT_TRACE_CASE(1, 0, false, true) BT_TRACE_CASE(1, 0, true, true)
+                BT_TRACE_CASE(1, 1, false, true) BT_TRACE_CASE(1, 1, true, true)
 #undef BT_TRACE_CASE
+                BT_REQUIRE(ctx->launch_count > launched, "trace: no kernel for these settings");
             }
             BT_CHECK_LAUNCH();
             used += need;
@@ -600,6 +786,21 @@ extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, 
             std::swap(act_a, act_b);
         }
         flush();
+    }
+}
+
+}  // namespace
+}  // namespace bt
+
+extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, int64_t window) {
+    return bt::guarded([&] { bt::trace_all(ctx, args, nullptr, window); });
+}
+
+extern "C" int bt_trace_trajectories_2d_magnetic(bt_ctx *ctx, const bt_trace_args *args,
+                                                 const bt_magnetic *magnetic, int64_t window) {
+    return bt::guarded([&] {
+        BT_REQUIRE(magnetic, "trace: null magnetic field");
+        bt::trace_all(ctx, args, magnetic, window);
     });
 }
 

@@ -175,6 +175,57 @@ class AxisymmetricMagneticField:
             power = power * r2
         return bz, br
 
+    def profile(self) -> MagneticProfile:
+        """The field on the device for a cylindrical mesh (``B_z`` along x, ``B_r``)."""
+        return MagneticProfile(1, self, 0.0)
+
+    @property
+    def samples(self) -> np.ndarray:
+        """The derivative table ``(n, order + 1)``: ``d^k B_z / dz^k`` at every sample."""
+        return self._samples
+
+
+class PlanarSolenoidField:
+    """A solenoid's axisymmetric field laid on a planar mesh, its axis the line
+    ``y = axis_y``: ``(B_x, B_y, B_z) = (B_z, sign(y - axis_y) B_r, 0)`` at
+    ``r = |y - axis_y|`` -- the magnetic callable ``BeamTracer`` takes on a planar mesh
+    (``tracer.py:401-404, 567-572``), built from `AxisymmetricMagneticField`."""
+
+    def __init__(self, field: AxisymmetricMagneticField, axis_y: float = 0.0) -> None:
+        self.field = field
+        self.axis_y = float(axis_y)
+
+    def __call__(self, x, y) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        y = np.asarray(y, dtype=float)
+        yr = y - self.axis_y
+        bz, br = self.field(x, np.abs(yr))
+        return bz, np.where(yr < 0.0, -br, br), np.zeros_like(bz)
+
+    def profile(self) -> MagneticProfile:
+        return MagneticProfile(2, self.field, self.axis_y)
+
+
+class MagneticProfile:
+    """An on-axis profile's derivative table on the device, for the magnetic trace
+    (``bt_magnetic``): mode 1 on a cylindrical mesh, 2 on a planar one."""
+
+    def __init__(self, mode: int, field: AxisymmetricMagneticField, axis_y: float) -> None:
+        import torch
+
+        self.mode = int(mode)
+        self.order = field.order
+        self.z0, self.hz, self.axis_y = field.z0, field.hz, float(axis_y)
+        self.samples = torch.from_numpy(np.ascontiguousarray(field.samples)).to("cuda")
+
+    def descriptor(self) -> _lib.MagneticDesc:
+        return _lib.MagneticDesc(self.mode, self.order, int(self.samples.shape[0]), self.z0,
+                                 self.hz, self.axis_y, _lib.dptr(self.samples))  # fmt: skip
+
+    def oracle_tuple(self) -> tuple:
+        """``(mode, order, z0, hz, axis_y, samples)`` for the oracle."""
+        return (self.mode, self.order, self.z0, self.hz, self.axis_y,
+                self.samples.cpu().numpy())  # fmt: skip
+
 
 def solenoid_on_axis(z, centre: float, length: float, radius: float, peak: float) -> np.ndarray:
     """The on-axis B_z [T] of a thin-walled solenoid scaled to ``peak`` at its centre

@@ -151,12 +151,14 @@ _TRACE_ARRAYS = {
 }  # fmt: skip
 
 
-def trace_trajectories_2d(*args, window: int = 0) -> None:
+def trace_trajectories_2d(*args, window: int = 0, magnetic=None) -> None:
     """Trace the ``active`` trajectories until they end, or reach a cut electrode sub-cell.
 
     The 35 arguments of the reference kernel, in its order (see the module docstring);
     ``window`` is the number of steps a launch advances every trajectory (0: the library's
-    default).
+    default).  ``magnetic``, a `MagneticProfile` on the device, selects the reference's
+    NumPy tracer's step in that field (``tracer.py:851-1054``): every step ending in a cell
+    that touches an electrode then pauses (status -2) for the caller's inside test.
     """
     if len(args) != 35:
         raise TypeError(f"trace_trajectories_2d takes 35 arguments, got {len(args)}")
@@ -190,7 +192,12 @@ def trace_trajectories_2d(*args, window: int = 0) -> None:
         int(graded), _lib.dptr(x_nodes), _size(x_nodes), float(inv_c2),
     )  # fmt: skip
     ctx = _lib.context()
-    _lib.check(_lib.lib().bt_trace_trajectories_2d(ctx.handle, ctypes.byref(a), int(window)))
+    if magnetic is None:
+        _lib.check(_lib.lib().bt_trace_trajectories_2d(ctx.handle, ctypes.byref(a), int(window)))
+    else:
+        m = magnetic.descriptor()
+        _lib.check(_lib.lib().bt_trace_trajectories_2d_magnetic(
+            ctx.handle, ctypes.byref(a), ctypes.byref(m), int(window)))  # fmt: skip
     s.finish()
 
 

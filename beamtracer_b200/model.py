@@ -23,6 +23,7 @@ from beamtracer_b200.config import (
     ObjectParams,
 )
 from beamtracer_b200.diagnostics import BeamMoments, plane_moments
+from beamtracer_b200.fields import AxisymmetricMagneticField, solenoid_on_axis
 from beamtracer_b200.mesh import Electrode, FaceCondition, IonOpticsMesh
 from beamtracer_b200.tracer import (
     STATUS_NAMES,
@@ -83,13 +84,36 @@ class BeamOptics:
             faces=self._faces(),
             symmetry_plane=config.symmetry_plane,
         )
-        self.axial_magnetic_field = None
+        self.axial_magnetic_field = self._magnetic_field()
         self.field_map = None
         self.tracer = BeamTracer(
-            self.mesh, None, step_fraction=config.step_fraction, integrator=config.integrator,
+            self.mesh, None, self.axial_magnetic_field, step_fraction=config.step_fraction,
+            integrator=config.integrator,
             relativistic=config.relativistic, max_steps=config.max_steps,
             planes=config.diagnostic_planes, save_trajectories=config.save_trajectories,
         )  # fmt: skip
+
+    def _magnetic_field(self) -> AxisymmetricMagneticField | None:
+        """The axisymmetric field of the solenoids and the measured axial field
+        (``model.py:169-188``): the solenoids sampled at ``h / 2`` from ``x_min - 8 dz`` to
+        ``x_max + 8 dz``, or added to the axial field's samples."""
+        config = self.config
+        if not config.solenoids and config.axial_field is None:
+            return None
+        if config.axial_field is not None:
+            z0, dz = config.axial_field.z0, config.axial_field.dz
+            bz = np.asarray(config.axial_field.bz, dtype=float)
+            z = z0 + dz * np.arange(bz.size)
+        else:
+            dz = 0.5 * self.mesh.h
+            lo, hi = self.mesh.origin[0], self.mesh.upper[0]
+            z = np.arange(lo - 8 * dz, hi + 8.5 * dz, dz)
+            z0 = float(z[0])
+            bz = np.zeros(z.size)
+        for solenoid in config.solenoids:
+            bz = bz + solenoid_on_axis(z, solenoid.centre, solenoid.length, solenoid.radius,
+                                       solenoid.peak)  # fmt: skip
+        return AxisymmetricMagneticField(z0, dz, bz, order=config.field_order)
 
     def _faces(self) -> dict[str, FaceCondition]:
         faces = {}

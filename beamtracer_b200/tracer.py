@@ -285,6 +285,7 @@ class TraceEngine:
         save_trajectories: int = 0,
         capacity: tuple[int, int] = (4, 1024),
         window: int = 64,
+        magnetic: Any = None,
     ) -> None:
         import torch
 
@@ -300,6 +301,8 @@ class TraceEngine:
         self.save_trajectories = int(save_trajectories)
         self.capacity = tuple(capacity)
         self.window = int(window)
+        #: a `MagneticProfile` on the device: the NumPy tracer's step in that field
+        self.magnetic = magnetic
         self.ctx = _lib.context()
         dev = "cuda"
         nx, ny = mesh.shape
@@ -404,7 +407,7 @@ class TraceEngine:
             INTEGRATORS.index(self.integrator), self.step_fraction, self.max_steps,
             self.cells, self.subcells, SUBCELLS, self.planes_dev, self.hits, self.counts,
             self.path_slot, self.paths, self.path_count, 1, self.charge, int(mesh.graded),
-            self.x_nodes, self.inv_c2, window=self.window,
+            self.x_nodes, self.inv_c2, window=self.window, magnetic=self.magnetic,
         )  # fmt: skip
 
     def run(self, fx, fy) -> None:
@@ -482,9 +485,11 @@ class TraceEngine:
 class BeamTracer:
     """Trace particles through a static electric field (``tracer.py:384-1366``).
 
-    ``electric`` is a `StaggeredElectricField` of the mesh.  The trace runs on the device;
-    a magnetic field, an imposed electric field and charge changes belong to the
-    reference's NumPy tracer and are not part of this build.
+    ``electric`` is a `StaggeredElectricField` of the mesh.  The trace runs on the device.
+    ``magnetic`` -- an `AxisymmetricMagneticField` on a cylindrical mesh, or a
+    `PlanarSolenoidField` on a planar one -- selects the reference's NumPy tracer's step
+    in that field (``tracer.py:851-1054``; non-relativistic, no symmetry plane).  An
+    imposed electric field and charge changes are not part of this build.
     """
 
     def __init__(
@@ -510,15 +515,25 @@ class BeamTracer:
         if integrator not in INTEGRATORS:
             raise ValueError(f"integrator must be one of {INTEGRATORS}, got {integrator!r}")
         unsupported = {
-            "a magnetic field": magnetic, "an imposed electric field": imposed_electric,
-            "charge changes": charge_changing,
+            "an imposed electric field": imposed_electric, "charge changes": charge_changing,
         }  # fmt: skip
         given = [name for name, value in unsupported.items() if value is not None]
         if given:
             raise NotImplementedError("this build's tracer takes no " + ", ".join(given))
         self.mesh = mesh
         self.electric = electric
-        self.magnetic = None
+        if magnetic is not None:
+            from beamtracer_b200.fields import AxisymmetricMagneticField, PlanarSolenoidField
+
+            if mesh.cylindrical and not isinstance(magnetic, AxisymmetricMagneticField):
+                raise NotImplementedError("a cylindrical mesh takes an AxisymmetricMagneticField")
+            if not mesh.cylindrical and not isinstance(magnetic, PlanarSolenoidField):
+                raise NotImplementedError("a planar mesh takes a PlanarSolenoidField")
+            if mesh.symmetry_plane:
+                raise NotImplementedError("a magnetic field with a symmetry plane")
+            if relativistic:
+                raise NotImplementedError("a relativistic trace in a magnetic field")
+        self.magnetic = magnetic
         self.step_fraction = float(step_fraction)
         self.max_steps = int(max_steps)
         self.planes = tuple(float(p) for p in planes)
@@ -543,6 +558,7 @@ class BeamTracer:
                 step_fraction=self.step_fraction, max_steps=self.max_steps,
                 inv_c2=self._inv_c2(), save_trajectories=self.save_trajectories,
                 capacity=self._capacity, window=self.window,
+                magnetic=None if self.magnetic is None else self.magnetic.profile(),
             )  # fmt: skip
         return self._engine
 

@@ -141,6 +141,30 @@ typedef struct bt_trace_args {
  * window's deposit records are sorted by cell and reduced in a fixed order. */
 int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, int64_t window);
 
+/* An axisymmetric magnetic field from its on-axis profile (solver/fields.py:192-279,
+ * AxisymmetricMagneticField): samples (DEVICE, n rows of order + 1) hold d^k B_z / dz^k,
+ * k = 0..order, at z0 + hz i (fields.py:236-243); between samples they are interpolated
+ * linearly and summed in the power series in r (fields.py:250-279).
+ * mode 1: a cylindrical mesh, B = B_z x^ + B_r r^ at (x, r);
+ * mode 2: a planar mesh with the solenoid's axis on y = axis_y: B = (B_z, sign(y - axis_y)
+ * B_r, 0) at r = |y - axis_y|. */
+typedef struct bt_magnetic {
+    int32_t mode;
+    int32_t order; /* 0..6 */
+    int64_t n;     /* samples, at least 8 */
+    double z0, hz, axis_y;
+    const double *samples;
+} bt_magnetic;
+
+/* solver/tracer.py:851-1054 (BeamTracer._trace_numpy, the reference's only path with a
+ * magnetic field) with _rk4 (:586-603) and _boris / _kick (:605-660): the arguments and
+ * outputs of bt_trace_trajectories_2d, each step's acceleration q/m (E + v x B), Boris's
+ * kick with the magnetic rotation, the spacing of mesh.py:197-202; every step ending in a
+ * cell that touches an electrode pauses (status -2) for the caller's exact inside test
+ * (tracer.py:1019-1024).  Non-relativistic (inv_c2 = 0), one patch, no symmetry plane. */
+int bt_trace_trajectories_2d_magnetic(bt_ctx *ctx, const bt_trace_args *args,
+                                      const bt_magnetic *magnetic, int64_t window);
+
 /* Counters of the last bt_trace_trajectories_2d call on this context (host out-params). */
 int bt_trace_last_stats(bt_ctx *ctx, int64_t *windows, int64_t *records,
                         int64_t *deposit_flushes);

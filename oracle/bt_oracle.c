@@ -177,6 +177,89 @@ typedef struct {
     double inv_c2;
 } bto_trace_args;
 
+/* An axisymmetric magnetic field from its on-axis profile (solver/fields.py:192-279): the
+ * derivatives d^k B_z / dz^k, k = 0..order, at the samples z0 + hz i (n rows of order + 1).
+ * mode 1: a cylindrical mesh, B = B_z x + B_r r^; mode 2: a planar mesh with the solenoid's
+ * axis on the line y = axis_y, B = (B_z, sign(y - axis_y) B_r, 0) at r = |y - axis_y|. */
+typedef struct bto_magnetic {
+    int32_t mode, order;
+    i64 n;
+    double z0, hz, axis_y;
+    const double *samples;
+} bto_magnetic;
+
+/* (B_z, B_r) at axial position z and radius r (fields.py:250-279, term by term). */
+static void bto_axial_field(const bto_magnetic *m, double z, double r, double *bz_out,
+                            double *br_out) {
+    static const double bz_c[4] = {1.0, -1.0 / 4.0, 1.0 / 64.0, -1.0 / 2304.0};
+    static const double br_c[3] = {-1.0 / 2.0, 1.0 / 16.0, -1.0 / 384.0};
+    const i64 n = m->n;
+    const int K = m->order + 1;
+    double s = (z - m->z0) / m->hz;
+    i64 i = bto_floor(s);
+    if (i < 3)
+        i = 3;
+    else if (i > n - 5)
+        i = n - 5;
+    double t = s - (double)i;
+    const double *lo = m->samples + i * K, *hi = lo + K;
+    double d[7];
+    for (int k = 0; k < K; ++k) d[k] = lo[k] + t * (hi[k] - lo[k]);
+    double r2 = r * r;
+    double bz = d[0], br = 0.0, power = 1.0;
+    for (int k = 1; k <= m->order / 2; ++k) {
+        power = power * r2;
+        bz = bz + bz_c[k] * power * d[2 * k];
+    }
+    power = r;
+    for (int k = 0; k < (m->order + 1) / 2; ++k) {
+        br = br + br_c[k] * power * d[2 * k + 1];
+        power = power * r2;
+    }
+    *bz_out = bz;
+    *br_out = br;
+}
+
+/* The Cartesian B at a point (q0, q1, q2); (cy, cz) its radial unit vector on a
+ * cylindrical mesh, r its radius. */
+static void bto_magnetic_at(const bto_magnetic *m, double q0, double q1, double r, double cy,
+                            double cz, double *b) {
+    double bz, br;
+    if (m->mode == 1) {
+        bto_axial_field(m, q0, r, &bz, &br);
+        b[0] = bz;
+        b[1] = br * cy;
+        b[2] = br * cz;
+    } else {
+        double yr = q1 - m->axis_y;
+        bto_axial_field(m, q0, fabs(yr), &bz, &br);
+        b[0] = bz;
+        b[1] = yr < 0.0 ? -br : br;
+        b[2] = 0.0;
+    }
+}
+
+/* v <- Boris's kick over tau in the fields e, b (non-relativistic; tracer.py:605-616 with
+ * its equations :620-621): v- = v + (tau/2) q/m E, t = (tau/2) q/m B,
+ * v+ = v- + (v- + v- x t) x 2t / (1 + t^2), then + (tau/2) q/m E.  The association of the
+ * operations is this restatement's own (mpiparticles' source is not available). */
+static void bto_kick(double *v, const double *e, const double *b, double tau, double qm) {
+    double f = 0.5 * tau * qm;
+    double m0 = v[0] + f * e[0], m1 = v[1] + f * e[1], m2 = v[2] + f * e[2];
+    double t0 = f * b[0], t1 = f * b[1], t2 = f * b[2];
+    double d = 2.0 / (1.0 + (t0 * t0 + t1 * t1 + t2 * t2));
+    double s0 = d * t0, s1 = d * t1, s2 = d * t2;
+    double p0 = m0 + (m1 * t2 - m2 * t1);
+    double p1 = m1 + (m2 * t0 - m0 * t2);
+    double p2 = m2 + (m0 * t1 - m1 * t0);
+    double w0 = m0 + (p1 * s2 - p2 * s1);
+    double w1 = m1 + (p2 * s0 - p0 * s2);
+    double w2 = m2 + (p0 * s1 - p1 * s0);
+    v[0] = w0 + f * e[0];
+    v[1] = w1 + f * e[1];
+    v[2] = w2 + f * e[2];
+}
+
 /* The field E at (lq, qy) [uniform x, mesh y] from the finest patch holding it
  * (trace_trajectories_2d_pyccel.py:212-269). */
 static void bto_edge_field(const bto_trace_args *a, double lq, double qy, double *ex_out,
@@ -235,7 +318,8 @@ static void bto_edge_field(const bto_trace_args *a, double lq, double qy, double
 }
 
 /* One trajectory from its state to its end (trace_trajectories_2d_pyccel.py:134-507). */
-static void bto_trace_one(const bto_trace_args *a, i64 k, double *charge) {
+static void bto_trace_one(const bto_trace_args *a, const bto_magnetic *mag, i64 k,
+                          double *charge) {
     const i64 P = a->n_patches;
     const i64 nx = a->patch_int[(P - 1) * 6 + 0];
     const i64 ny = a->patch_int[(P - 1) * 6 + 1];
@@ -253,6 +337,7 @@ static void bto_trace_one(const bto_trace_args *a, i64 k, double *charge) {
     const int nstage = a->integrator == 0 ? 4 : 2;
     int have = 0;
     double ca0 = 0.0, ca1 = 0.0, ca2 = 0.0;
+    double cE[3] = {0, 0, 0}, cB[3] = {0, 0, 0};  /* with B: the fields at the step's end */
     while (ns < a->max_steps) {
         /* the spacing of the finest patch at the step's start */
         double rr = x1;
@@ -272,8 +357,15 @@ static void bto_trace_one(const bto_trace_args *a, i64 k, double *charge) {
         }
         if (a->graded) {
             i64 cg = bto_node_cell(x0, a->x_nodes, a->n_x_nodes);
-            double d2 = (a->x_nodes[cg + 1] - a->x_nodes[cg]) / h;
-            if (d2 < 1.0) hloc = hloc * d2;
+            if (mag) {
+                /* the NumPy tracer's spacing: the smaller of the cell's edge and h
+                   (mesh.py:197-202) */
+                double dxc = a->x_nodes[cg + 1] - a->x_nodes[cg];
+                if (dxc < hloc) hloc = dxc;
+            } else {
+                double d2 = (a->x_nodes[cg + 1] - a->x_nodes[cg]) / h;
+                if (d2 < 1.0) hloc = hloc * d2;
+            }
         }
         double gv = 1.0 / bto_lorentz(v0, v1, v2, inv_c2);
         double q0 = x0, q1 = x1, q2 = x2;
@@ -283,7 +375,48 @@ static void bto_trace_one(const bto_trace_args *a, i64 k, double *charge) {
         for (int stage = 0; stage < nstage; ++stage) {
             double gk = 1.0 / bto_lorentz(kx0, kx1, kx2, inv_c2);
             double g0, g1, g2;
-            if (stage == 0 && have != 0) {
+            double E[3], B[3];
+            if (mag && stage == 0 && have != 0) {
+                for (int c = 0; c < 3; ++c) {
+                    E[c] = cE[c];
+                    B[c] = cB[c];
+                }
+            }
+            if (mag && !(stage == 0 && have != 0)) {
+                /* E and B at the stage point (tracer.py:547-583) */
+                double qy = q1, cy = 0.0, cz = 0.0;
+                if (cyl == 1) {
+                    double r = bto_radius(q1, q2);
+                    if (r > 0.0) {
+                        cy = q1 / r;
+                        cz = q2 / r;
+                    }
+                    qy = r;
+                }
+                double lq = q0;
+                if (a->graded) lq = bto_uniform_x(q0, a->x_nodes, a->n_x_nodes, origin_x, h);
+                double ex, ey;
+                bto_edge_field(a, lq, qy, &ex, &ey);
+                if (cyl != 0) {
+                    E[0] = ex;
+                    E[1] = ey * cy;
+                    E[2] = ey * cz;
+                } else {
+                    E[0] = ex;
+                    E[1] = ey;
+                    E[2] = 0.0;
+                }
+                bto_magnetic_at(mag, q0, q1, qy, cy, cz, B);
+            }
+            if (mag) {
+                /* q/m (E + v x B) at the stage velocity (tracer.py:519-529) */
+                double c0 = kx1 * B[2] - kx2 * B[1];
+                double c1 = kx2 * B[0] - kx0 * B[2];
+                double c2 = kx0 * B[1] - kx1 * B[0];
+                g0 = qmk * (E[0] + c0);
+                g1 = qmk * (E[1] + c1);
+                g2 = qmk * (E[2] + c2);
+            } else if (stage == 0 && have != 0) {
                 g0 = ca0;
                 g1 = ca1;
                 g2 = ca2;
@@ -329,6 +462,18 @@ static void bto_trace_one(const bto_trace_args *a, i64 k, double *charge) {
                 dt = a->step_fraction * dt;
                 hdt = 0.5 * dt;
                 dt6 = dt / 6.0;
+                if (a->integrator != 0 && mag) {
+                    /* Boris with B: the kick over half the step, the drift (tracer.py:652-660) */
+                    double u[3] = {v0, v1, v2};
+                    bto_kick(u, E, B, hdt, qmk);
+                    kx0 = u[0];
+                    kx1 = u[1];
+                    kx2 = u[2];
+                    q0 = x0 + dt * kx0;
+                    q1 = x1 + dt * kx1;
+                    q2 = x2 + dt * kx2;
+                    continue;
+                }
                 if (a->integrator != 0) {
                     /* Boris: the half kick, then the drift to the end of the step */
                     kx0 = v0 + hdt * a0;
@@ -352,6 +497,18 @@ static void bto_trace_one(const bto_trace_args *a, i64 k, double *charge) {
                 kx0 = v0 + hdt * a0;
                 kx1 = v1 + hdt * a1;
                 kx2 = v2 + hdt * a2;
+            } else if (a->integrator != 0 && mag) {
+                /* Boris with B: the second kick in the fields at the end of the step */
+                double u[3] = {kx0, kx1, kx2};
+                bto_kick(u, E, B, hdt, qmk);
+                w0 = u[0];
+                w1 = u[1];
+                w2 = u[2];
+                for (int c = 0; c < 3; ++c) {
+                    cE[c] = E[c];
+                    cB[c] = B[c];
+                }
+                have = 1;
             } else if (a->integrator != 0) {
                 /* Boris: the second half kick at the end of the step */
                 w0 = kx0 + hdt * g0;
@@ -515,7 +672,11 @@ static void bto_trace_one(const bto_trace_args *a, i64 k, double *charge) {
             if (i < 0) i = 0;
             if (j < 0) j = 0;
             i64 cell = a->cells[i * (ny - 1) + j];
-            if (cell >= 0) {
+            if (cell >= 0 && mag) {
+                /* the NumPy tracer tests the exact electrode shapes in every cell touching
+                   one (tracer.py:1019-1024): the caller decides */
+                st = -2;
+            } else if (cell >= 0) {
                 i64 R = a->refine;
                 i64 si = (i64)(((px - origin_x) / h - (double)i) * (double)R);
                 if (si < 0)
@@ -556,7 +717,20 @@ void bto_trace_trajectories_2d(const bto_trace_args *a) {
 #pragma omp parallel for schedule(static, 1) num_threads(T)
     for (i64 t = 0; t < T; ++t) {
         double *slab = a->charge + t * a->n_nodes;
-        for (i64 m = t; m < a->n_active; m += T) bto_trace_one(a, a->active[m], slab);
+        for (i64 m = t; m < a->n_active; m += T) bto_trace_one(a, NULL, a->active[m], slab);
+    }
+}
+
+/* The NumPy tracer's step in a magnetic field (tracer.py:851-1054 with _rk4 / _boris and
+ * AxisymmetricMagneticField), each trajectory to its end or to a cell touching an
+ * electrode (status -2, where the caller tests the electrodes' shapes).  Needs inv_c2 = 0
+ * and one patch. */
+void bto_trace_magnetic_2d(const bto_trace_args *a, const bto_magnetic *m) {
+    const i64 T = a->num_threads;
+#pragma omp parallel for schedule(static, 1) num_threads(T)
+    for (i64 t = 0; t < T; ++t) {
+        double *slab = a->charge + t * a->n_nodes;
+        for (i64 q = t; q < a->n_active; q += T) bto_trace_one(a, m, a->active[q], slab);
     }
 }
 

@@ -45,6 +45,13 @@ class _TraceArgs(ctypes.Structure):
     ]  # fmt: skip
 
 
+class _Magnetic(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int32), ("order", ctypes.c_int32), ("n", _I64), ("z0", _F64),
+        ("hz", _F64), ("axis_y", _F64), ("samples", _D),
+    ]  # fmt: skip
+
+
 @functools.cache
 def library() -> ctypes.CDLL:
     """The compiled oracle (built on first use)."""
@@ -56,6 +63,7 @@ def library() -> ctypes.CDLL:
         _D, _D, _D, _I64, _F64, _F64, _F64, _I64, _D, _I64, _I64,
     ]
     lib.bto_trace_trajectories_2d.argtypes = [ctypes.POINTER(_TraceArgs)]
+    lib.bto_trace_magnetic_2d.argtypes = [ctypes.POINTER(_TraceArgs), ctypes.POINTER(_Magnetic)]
     lib.bto_num_procs.restype = ctypes.c_int
     return lib
 
@@ -102,9 +110,15 @@ def trace_trajectories_2d(
     active, x, v, qm, dq, steps, status, electrode, fxs, fys, patch_int, patch_real,
     origin_x, origin_y, h, upper_x, upper_y, cylindrical, integrator, step_fraction,
     max_steps, cells, subcells, refine, planes, hits, counts, path_slot, paths,
-    path_count, num_threads, charge, graded, x_nodes, inv_c2,
+    path_count, num_threads, charge, graded, x_nodes, inv_c2, magnetic=None,
 ) -> None:  # fmt: skip
-    """Trace the ``active`` trajectories to their ends (restated Pyccel kernel)."""
+    """Trace the ``active`` trajectories to their ends (restated Pyccel kernel).
+
+    With ``magnetic = (mode, order, z0, hz, axis_y, samples)`` the step is the reference's
+    NumPy tracer's in that field instead (``tracer.py:851-1054``): acceleration
+    ``q/m (E + v x B)``, Boris with the magnetic rotation, and every step ending in a cell
+    that touches an electrode pauses (status -2) for the caller's exact inside test.
+    """
     for a, n in ((active, "active"), (steps, "steps"), (status, "status"),
                  (electrode, "electrode"), (patch_int, "patch_int"), (cells, "cells"),
                  (subcells, "subcells"), (counts, "counts"), (path_slot, "path_slot"),
@@ -126,7 +140,18 @@ def trace_trajectories_2d(
     )  # fmt: skip
     if charge.shape[0] < int(num_threads):
         raise ValueError("charge needs one slab per thread")
-    library().bto_trace_trajectories_2d(ctypes.byref(args))
+    if magnetic is None:
+        library().bto_trace_trajectories_2d(ctypes.byref(args))
+        return
+    mode, order, z0, hz, axis_y, samples = magnetic
+    samples = _f64(np.ascontiguousarray(samples, dtype=np.float64), "samples")
+    if samples.ndim != 2 or samples.shape[1] != int(order) + 1 or samples.shape[0] < 8:
+        raise ValueError("samples must be (n >= 8, order + 1)")
+    if float(inv_c2) != 0.0 or patch_int.shape[0] != 1:
+        raise ValueError("the magnetic trace is non-relativistic on one patch")
+    mag = _Magnetic(int(mode), int(order), samples.shape[0], float(z0), float(hz),
+                    float(axis_y), _p(samples))  # fmt: skip
+    library().bto_trace_magnetic_2d(ctypes.byref(args), ctypes.byref(mag))
 
 
 def host_cores() -> int:

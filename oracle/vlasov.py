@@ -53,6 +53,8 @@ class Problem:
     inv_c2: float = 0.0
     threads: int = 0  # 0: every host core
     capacity: tuple[int, int] = (4, 1024)
+    #: a magnetic field (mode, order, z0, hz, axis_y, samples) for the NumPy tracer's step
+    magnetic: Any = None
     extra: dict = field(default_factory=dict)
 
 
@@ -136,7 +138,7 @@ def trace(p: Problem, fx, fy, particles) -> Trace:
                 patch_real, *p.logical_origin, p.h, *p.logical_upper, p.geometry,
                 p.integrator, p.step_fraction, p.max_steps, p.cells, p.subcells, 8, planes,
                 hits, counts, slot, paths, path_count, threads, charge, int(p.graded),
-                x_nodes, p.inv_c2,
+                x_nodes, p.inv_c2, magnetic=p.magnetic,
             )  # fmt: skip
             paused = active[status[active] == -2]
             if not paused.size:

@@ -97,3 +97,21 @@ def test_negative_extraction_mirrors_positive(beam_optics):
     a, b = positive.beam_moments(7.5e-3), negative.beam_moments(7.5e-3)
     assert a.current == pytest.approx(b.current)
     assert a.emittance == pytest.approx(b.emittance, rel=1e-6)
+
+
+@pytest.mark.parametrize("integrator", ["rk4", "boris"])
+def test_extraction_through_a_solenoid_matches_the_oracle(beam_optics, integrator):
+    """The plasma extraction case inside a solenoid: the trace takes the reference's
+    NumPy tracer's magnetic step, every electrode cell decided by the exact inside test."""
+    from beamtracer_b200.config import Solenoid
+
+    config = extraction(1.0, iterations=4, tolerance=0.0, integrator=integrator,
+                        solenoids=[Solenoid(5e-3, 4e-3, 3e-3, 0.5)])  # fmt: skip
+    model = beam_optics(config)
+    assert model.tracer.magnetic is not None
+    gpu, ora = _run_both(model, 4, plasma=oracle_vlasov.Plasma(5.0, 5.0, 0.6e-3, -1))
+    for k, ((phi_g, rho_g), (phi_o, rho_o)) in enumerate(zip(gpu, ora)):
+        np.testing.assert_allclose(phi_g, phi_o, rtol=0, atol=1e-7 * 2000.0, err_msg=f"{k}")
+        np.testing.assert_allclose(rho_g, rho_o, rtol=0, atol=1e-7 * np.abs(rho_o).max(),
+                                   err_msg=f"{k}")  # fmt: skip
+    assert model.stats["transmitted"] > 0

@@ -65,23 +65,40 @@ def extraction(sign: float = 1.0, **settings) -> BeamOpticsConfig:
     )  # fmt: skip
 
 
-def oracle_problem(model) -> oracle_vlasov.Problem:
-    """The oracle's description of a `BeamOptics` model's mesh, electrodes and trace."""
+def mesh_problem(mesh, *, planes=(), integrator: int = 0, step_fraction: float = 0.5,
+                 max_steps: int = 100_000, magnetic=None) -> oracle_vlasov.Problem:
+    """The oracle's description of a mesh, its electrodes and a trace; ``magnetic`` an
+    `AxisymmetricMagneticField` (cylindrical mesh) or `PlanarSolenoidField` (planar)."""
+    from beamtracer_b200.fields import PlanarSolenoidField
     from beamtracer_b200.mesh import FACES
-    from beamtracer_b200.tracer import INTEGRATORS, electrode_lookup, geometry_code
+    from beamtracer_b200.tracer import electrode_lookup, geometry_code
 
-    mesh = model.mesh
     cells, subcells = electrode_lookup(mesh)
     neumann = tuple(0.0 if mesh.faces[f].kind != "neumann" else float(mesh.faces[f].value)
                     for f in FACES)  # fmt: skip
-    config = model.config
+    mag = None
+    if isinstance(magnetic, PlanarSolenoidField):
+        f = magnetic.field
+        mag = (2, f.order, f.z0, f.hz, magnetic.axis_y, f.samples)
+    elif magnetic is not None:
+        mag = (1, magnetic.order, magnetic.z0, magnetic.hz, 0.0, magnetic.samples)
     return oracle_vlasov.Problem(
         shape=mesh.shape, x=np.asarray(mesh.x, float), h=mesh.h, origin=mesh.origin,
         logical_origin=mesh.logical_origin, logical_upper=mesh.logical_upper,
         geometry=geometry_code(mesh), graded=mesh.graded, fixed=mesh.fixed,
         fixed_value=mesh.fixed_value, solid=mesh.solid, near_solid=mesh.near_solid,
         distance=mesh.distance, neumann=neumann, cells=cells, subcells=subcells,
-        inside_solid=mesh.inside_solid, planes=tuple(config.diagnostic_planes),
-        integrator=INTEGRATORS.index(config.integrator), step_fraction=config.step_fraction,
-        max_steps=config.max_steps,
+        inside_solid=mesh.inside_solid, planes=tuple(planes), integrator=integrator,
+        step_fraction=step_fraction, max_steps=max_steps, magnetic=mag,
     )  # fmt: skip
+
+
+def oracle_problem(model) -> oracle_vlasov.Problem:
+    """The oracle's description of a `BeamOptics` model's mesh, electrodes and trace."""
+    from beamtracer_b200.tracer import INTEGRATORS
+
+    config = model.config
+    return mesh_problem(model.mesh, planes=config.diagnostic_planes,
+                        integrator=INTEGRATORS.index(config.integrator),
+                        step_fraction=config.step_fraction, max_steps=config.max_steps,
+                        magnetic=model.tracer.magnetic)  # fmt: skip
