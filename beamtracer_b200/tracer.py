@@ -315,7 +315,7 @@ class TraceEngine:
         self.patch_real = torch.tensor([[lo_x, lo_y, mesh.h, lo_x, lo_y, up_x, up_y]],
                                        dtype=torch.float64, device=dev)  # fmt: skip
         self.x_nodes = torch.from_numpy(
-            np.ascontiguousarray(mesh.x if mesh.graded else np.zeros(2))
+            np.array(mesh.x if mesh.graded else np.zeros(2), dtype=np.float64, order="C")
         ).to(dev)
         self.planes_dev = torch.tensor(self.planes or (np.nan,), dtype=torch.float64, device=dev)
         self.volumes = torch.from_numpy(node_volumes(mesh)).to(dev)

@@ -210,6 +210,79 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_plasma(args) -> None:
+    """The planar plasma + solenoid extraction (1025 x 513, x graded, 100,000 H+, Newton
+    field solve, Boris step in the solenoid's field): converged solves per second, device
+    resident and through ``solenoid_extraction(design).run()`` from host inputs."""
+    import torch
+
+    from beamtracer_b200 import _lib
+    from beamtracer_b200.poisson import IonOpticsPoisson
+    from beamtracer_b200.solenoid_extraction import SolenoidExtractionDesign, solenoid_extraction
+
+    torch.cuda.set_device(0)
+    design = SolenoidExtractionDesign()
+    case = solenoid_extraction(design, window=args.window)
+    poisson = IonOpticsPoisson(case.mesh)
+    ctx = _lib.context()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        state = case.run(poisson=poisson)
+    torch.cuda.synchronize()
+    ctx.set_timing(True)
+    ctx.reset_timers()
+    launches_before = ctx.launch_count()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]  # fmt: skip
+    steps_total = 0
+    with ClockSampler(0) as clocks:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            events[k][0].record(stream)
+            state = case.run(poisson=poisson)
+            events[k][1].record(stream)
+            steps_total += sum(h["total_steps"] for h in state.history)
+        torch.cuda.synchronize()
+    total_ms = float(sum(a.elapsed_time(b) for a, b in events))
+    timers = {name: ctx.read_timer(name) for name in
+              ("trace_window", "deposit", "field_solve", "vcycle", "edge_field")}  # fmt: skip
+    ctx.set_timing(False)
+    launches = ctx.launch_count() - launches_before
+    e2e_ms = []
+    for k in range(3):
+        gc.collect()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record(stream)
+        solenoid_extraction(design, window=args.window).run()
+        stop.record(stream)
+        torch.cuda.synchronize()
+        if k:
+            e2e_ms.append(start.elapsed_time(stop))
+    nx, ny = design.shape
+    line = {
+        "metric": "converged plasma+solenoid extraction solves/s (1025x513 planar graded, "
+                  "100k H+)", "value": args.steps / (total_ms / 1e3), "unit": UNIT,
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "solenoid extraction 1025x513 planar, x graded, 100,000 H+, "
+                               "Boltzmann electrons, Boris in a 0.2 T solenoid",
+                   "mesh": [nx, ny], "trajectories": design.trajectories,
+                   "iterations_per_solve": len(state.history),
+                   "newton_steps_per_solve": sum(h["newton_iterations"] for h in state.history),
+                   "l2": "256 MiB written between timed steps"},
+        "kernels": {name: {"ms": ms, "launches": n, "share": ms / total_ms}
+                    for name, (ms, n) in timers.items()},
+        "steps_per_solve": steps_total / args.steps,
+        "e2e": {"value": 1e3 / float(np.median(e2e_ms)), "unit": UNIT,
+                "runs_ms": [round(v, 2) for v in e2e_ms]},
+        "gpu_launches": launches, "clocks": clocks.summary(),
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -222,9 +295,14 @@ def main() -> None:
                         help="one warm solve, then one in the NVTX range 'profiled_solve'")
     parser.add_argument("--small", action="store_true",
                         help="with --profile: the lens at 401 x 101 with 2,000 rings")
+    parser.add_argument("--workload", default="einzel", choices=["einzel", "plasma"],
+                        help="plasma: the planar plasma + solenoid extraction (one GPU)")
     args = parser.parse_args()
     if args.profile:
         run_profile(args)
+        return
+    if args.workload == "plasma" and args.impl == "b200":
+        run_plasma(args)
         return
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)

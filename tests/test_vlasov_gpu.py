@@ -115,3 +115,29 @@ def test_extraction_through_a_solenoid_matches_the_oracle(beam_optics, integrato
         np.testing.assert_allclose(rho_g, rho_o, rtol=0, atol=1e-7 * np.abs(rho_o).max(),
                                    err_msg=f"{k}")  # fmt: skip
     assert model.stats["transmitted"] > 0
+
+
+def test_solenoid_extraction_matches_the_oracle():
+    """The planar plasma + solenoid workload (x-graded mesh, Newton solve, Boris step in
+    the solenoid's field) on a coarse mesh: every iteration against the oracle."""
+    from beamtracer_b200.solenoid_extraction import SolenoidExtractionDesign, solenoid_extraction
+    from tests.vlasov_cases import mesh_problem
+
+    case = solenoid_extraction(SolenoidExtractionDesign().small())
+    gpu = []
+    case.run(lambda it, state: gpu.append((state.potential.copy(), state.charge_density.copy())),
+             iterations=3, tolerance=0.0)  # fmt: skip
+    problem = mesh_problem(case.mesh, integrator=1, magnetic=case.magnetic)
+    d = case.design
+    ora = []
+    oracle_vlasov.vlasov(problem, case.particles, case.j_over_v, iterations=3,
+                         relaxation=d.relaxation,
+                         plasma=oracle_vlasov.Plasma(d.electron_temperature, d.plasma_potential,
+                                                     d.plasma_x, -1, density=case.plasma.rho_e),
+                         callback=lambda it, out: ora.append(
+                             (out["potential"].copy(), out["charge_density"].copy())))  # fmt: skip
+    assert len(gpu) == len(ora) == 3
+    for k, ((phi_g, rho_g), (phi_o, rho_o)) in enumerate(zip(gpu, ora)):
+        np.testing.assert_allclose(phi_g, phi_o, rtol=0, atol=1e-7 * 1e4, err_msg=f"{k}")
+        np.testing.assert_allclose(rho_g, rho_o, rtol=0, atol=1e-7 * np.abs(rho_o).max(),
+                                   err_msg=f"{k}")  # fmt: skip
