@@ -73,6 +73,12 @@ class MagneticDesc(ctypes.Structure):
     ]  # fmt: skip
 
 
+class ShapesDesc(ctypes.Structure):
+    """``bt_shapes`` of ``include/bt200.h``."""
+
+    _fields_ = [("count", I64), ("kind", P), ("offset", P), ("params", P)]
+
+
 class MeshDesc(ctypes.Structure):
     """``bt_mesh_desc`` of ``include/bt200.h``."""
 
@@ -98,6 +104,8 @@ SIGNATURES: dict[str, list] = {
     "bt_staggered_field_2d": [P, P, P, I64, P, P, I64, I64, F64, F64, F64, P, P],
     "bt_deposit_trajectories_2d": [P, P, P, P, I64, F64, F64, F64, I64, P, I64, I64],
     "bt_deposit_trajectories_2d_noalloc": [P, P, P, P, I64, F64, F64, F64, I64, P, I64, I64],
+    "bt_subcell_table": [P, ctypes.POINTER(ShapesDesc), P, P, I64, F64, F64, F64, P, I64, I64,
+                         P],
     "bt_trace_trajectories_2d_magnetic": [P, ctypes.POINTER(TraceArgs),
                                           ctypes.POINTER(MagneticDesc), I64],
     "bt_trace_trajectories_2d": [P, ctypes.POINTER(TraceArgs), I64],

@@ -1,0 +1,116 @@
+// Electrode shapes on the device: the inside tests of the configuration's objects
+// (config.py's rectangles, lines, circles, polygons, triangles and mirrored apertures; the
+// reference's simgeometry tests, restated with closed boundaries) and the sub-cell table
+// the tracer's electrode test reads (solver/tracer.py:1092-1114): for every sub-cell of the
+// cells touching an electrode, the electrode holding its four corners and its centre, -1
+// for none, -2 where they disagree.  The tests evaluate the same expressions in the same
+// order as the host's NumPy ones, with the per-edge thresholds computed on the host, so the
+// table is the host's bit for bit.
+#include "common.cuh"
+
+namespace bt {
+namespace {
+
+constexpr int kShapeRect = 0, kShapeCircle = 1, kShapePolygon = 2, kShapeAperture = 3;
+constexpr int kEdgeWords = 9;  // x1, y1, x2, y2, threshold, x_lo, x_hi, y_lo, y_hi
+
+// Inside the polygon at p (p[0] its edge count, then its edges) or on its boundary.
+__device__ bool polygon_inside(const double *__restrict__ p, double x, double y) {
+    const i64 n = (i64)p[0];
+    const double *e = p + 1;
+    bool inside = false, boundary = false;
+    for (i64 k = 0; k < n; ++k, e += kEdgeWords) {
+        const double x1 = e[0], y1 = e[1], x2 = e[2], y2 = e[3];
+        if ((y1 > y) != (y2 > y)) {
+            const double at = x1 + (y - y1) * (x2 - x1) / (y2 - y1);
+            if (x < at) inside = !inside;
+        }
+        const double cross = (x2 - x1) * (y - y1) - (y2 - y1) * (x - x1);
+        if (fabs(cross) <= e[4] && x >= e[5] && x <= e[6] && y >= e[7] && y <= e[8])
+            boundary = true;
+    }
+    return inside || boundary;
+}
+
+__device__ bool shape_inside(int kind, const double *__restrict__ p, double x, double y) {
+    if (kind == kShapeRect) return fabs(x - p[0]) <= p[2] && fabs(y - p[1]) <= p[3];
+    if (kind == kShapeCircle) {
+        const double dx = x - p[0], dy = y - p[1];
+        return dx * dx + dy * dy <= p[2];
+    }
+    if (kind == kShapePolygon) return polygon_inside(p, x, y);
+    // an aperture: the polygon and its mirror image, one after the other
+    const bool first = polygon_inside(p, x, y);
+    const double *q = p + 1 + (i64)p[0] * kEdgeWords;
+    return first || polygon_inside(q, x, y);
+}
+
+struct Shapes {
+    i64 count;
+    const int32_t *kind;
+    const i64 *offset;
+    const double *params;
+};
+
+// The first electrode holding (x, y), or -1 (mesh.inside_solid).
+__device__ i64 inside_solid(const Shapes &S, double x, double y) {
+    for (i64 s = 0; s < S.count; ++s)
+        if (shape_inside(S.kind[s], S.params + S.offset[s], x, y)) return s;
+    return -1;
+}
+
+// The position along x of the fractional node index `index` (mesh.position_x).
+__device__ double position_x(double index, double origin_x, double h, const double *nodes,
+                             i64 n_nodes) {
+    if (!nodes) return origin_x + h * index;
+    i64 i = (i64)floor(index);
+    if (i < 0) i = 0;
+    if (i > n_nodes - 2) i = n_nodes - 2;
+    return nodes[i] + (index - (double)i) * (nodes[i + 1] - nodes[i]);
+}
+
+__global__ void subcell_kernel(Shapes S, const i64 *__restrict__ ci, const i64 *__restrict__ cj,
+                               i64 n_cells, double origin_x, double origin_y, double h,
+                               const double *__restrict__ nodes, i64 n_nodes, int R,
+                               i64 *__restrict__ out) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_cells * R * R) return;
+    const i64 k = t / (R * R);
+    const int a = (int)(t / R % R), b = (int)(t % R);
+    const double fi = (double)ci[k], fj = (double)cj[k];
+    auto at = [&](double fa, double fb) {
+        const double px = position_x(fi + fa, origin_x, h, nodes, n_nodes);
+        const double py = origin_y + h * (fj + fb);
+        return inside_solid(S, px, py);
+    };
+    const double r = (double)R;
+    const i64 centre = at(((double)a + 0.5) / r, ((double)b + 0.5) / r);
+    const bool same = at((double)a / r, (double)b / r) == centre &&
+                      at((double)(a + 1) / r, (double)b / r) == centre &&
+                      at((double)a / r, (double)(b + 1) / r) == centre &&
+                      at((double)(a + 1) / r, (double)(b + 1) / r) == centre;
+    out[t] = same ? centre : -2;
+}
+
+}  // namespace
+}  // namespace bt
+
+extern "C" int bt_subcell_table(bt_ctx *ctx, const bt_shapes *shapes, const int64_t *ci,
+                                const int64_t *cj, int64_t n_cells, double origin_x,
+                                double origin_y, double h, const double *x_nodes,
+                                int64_t n_x_nodes, int64_t refine, int64_t *out) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx && shapes && out, "subcells: null argument");
+        BT_REQUIRE(n_cells >= 0 && refine >= 1 && refine <= 64, "subcells: bad sizes");
+        BT_REQUIRE(shapes->count >= 0 && (shapes->count == 0 || (shapes->kind && shapes->offset &&
+                                                                 shapes->params)),
+                   "subcells: null shape arrays");
+        BT_REQUIRE(!x_nodes || n_x_nodes >= 2, "subcells: a graded axis needs its nodes");
+        if (n_cells == 0) return;
+        const bt::Shapes S{shapes->count, shapes->kind, shapes->offset, shapes->params};
+        const int64_t total = n_cells * refine * refine;
+        BT_LAUNCH(ctx, bt::subcell_kernel, bt::blocks_for(total, 256), 256, 0, ctx->stream, S, ci,
+                  cj, n_cells, origin_x, origin_y, h, x_nodes, n_x_nodes, (int)refine, out);
+        BT_CHECK_LAUNCH();
+    });
+}

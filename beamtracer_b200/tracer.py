@@ -19,6 +19,7 @@ trace the same beam again and again without copying it back and forth.
 
 from __future__ import annotations
 
+import ctypes
 from collections.abc import Sequence
 from dataclasses import dataclass, field
 from typing import Any
@@ -248,6 +249,86 @@ def electrode_lookup(mesh: IonOpticsMesh) -> tuple[np.ndarray, np.ndarray]:
     return cells, subcell_table(mesh, ci, cj).ravel()
 
 
+def _polygon_words(vertices: np.ndarray) -> list[float]:
+    """A polygon for the device's inside test: its edge count, then per edge its ends, the
+    boundary threshold and the extent the host's test uses (``config._polygon_inside``)."""
+    vx, vy = vertices[:, 0], vertices[:, 1]
+    n = len(vx)
+    words = [float(n)]
+    for k in range(n):
+        x1, y1, x2, y2 = vx[k], vy[k], vx[(k + 1) % n], vy[(k + 1) % n]
+        length = np.hypot(x2 - x1, y2 - y1)
+        threshold = 1e-12 * max(length, 1e-300) * max(length, 1.0)
+        words += [x1, y1, x2, y2, threshold, min(x1, x2) - 1e-15, max(x1, x2) + 1e-15,
+                  min(y1, y2) - 1e-15, max(y1, y2) + 1e-15]  # fmt: skip
+    return [float(w) for w in words]
+
+
+def shape_table(mesh: IonOpticsMesh):
+    """The electrodes as device shapes ``(kind, offset, params)`` arrays, or None when one
+    is not a configuration shape (an arbitrary inside function: tested on the host)."""
+    from beamtracer_b200.config import ObjectParams
+
+    kinds, offsets, params = [], [], []
+    for electrode in mesh.electrodes:
+        obj = getattr(electrode.inside, "__self__", None)
+        if not isinstance(obj, ObjectParams):
+            return None
+        offsets.append(len(params))
+        if obj.type in ("rectangle", "line"):
+            (mx, my), (lx, ly) = obj.midpoint, obj.side_lengths
+            kinds.append(0)
+            params += [float(mx), float(my), 0.5 * lx, 0.5 * ly]
+        elif obj.type == "circle":
+            mx, my = obj.midpoint
+            kinds.append(1)
+            params += [float(mx), float(my), float(obj.radius) ** 2]
+        else:
+            vertices = np.asarray(obj.vertices, dtype=float)
+            if obj.type in ("polygon", "triangle"):
+                kinds.append(2)
+                params += _polygon_words(vertices)
+            else:
+                axis = int(obj.axis) if obj.axis is not None else 0
+                position = float(obj.position or 0.0)
+                mirrored = vertices.copy()
+                mirrored[:, 1 - axis] = 2.0 * position - mirrored[:, 1 - axis]
+                kinds.append(3)
+                params += _polygon_words(vertices) + _polygon_words(mirrored)
+    return (np.array(kinds, dtype=np.int32), np.array(offsets, dtype=np.int64),
+            np.array(params or [0.0], dtype=np.float64))  # fmt: skip
+
+
+def electrode_lookup_device(mesh: IonOpticsMesh):
+    """`electrode_lookup` as device tensors, its sub-cell table sampled on the device when
+    every electrode is a configuration shape (else on the host)."""
+    import torch
+
+    from beamtracer_b200 import _lib
+
+    table = shape_table(mesh) if mesh.electrodes else None
+    touching = electrode_cells(mesh)
+    if table is None or not touching.any():
+        cells, subcells = electrode_lookup(mesh)
+        return torch.from_numpy(cells).cuda(), torch.from_numpy(subcells).cuda()
+    cells = np.full(touching.shape, -1, dtype=np.int64)
+    ci, cj = np.nonzero(touching)
+    cells[ci, cj] = np.arange(ci.size, dtype=np.int64)
+    kinds, offsets, params = (torch.from_numpy(a).cuda() for a in table)
+    ci_d = torch.from_numpy(ci.astype(np.int64)).cuda()
+    cj_d = torch.from_numpy(cj.astype(np.int64)).cuda()
+    nodes = torch.from_numpy(np.array(mesh.x, dtype=np.float64)).cuda() if mesh.graded else None
+    out = torch.empty(ci.size * SUBCELLS * SUBCELLS, dtype=torch.int64, device="cuda")
+    shapes = _lib.ShapesDesc(len(kinds), _lib.dptr(kinds), _lib.dptr(offsets), _lib.dptr(params))
+    ctx = _lib.context()
+    _lib.check(_lib.lib().bt_subcell_table(
+        ctx.handle, ctypes.byref(shapes), _lib.dptr(ci_d), _lib.dptr(cj_d), ci.size,
+        float(mesh.origin[0]), float(mesh.origin[1]), float(mesh.h),
+        _lib.dptr(nodes) if nodes is not None else None, mesh.shape[0] if nodes is not None else 0,
+        SUBCELLS, _lib.dptr(out)))  # fmt: skip
+    return torch.from_numpy(cells).cuda(), out
+
+
 def _project(mesh: IonOpticsMesh, x: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     """The mesh coordinates (x, y) or (x, r) of Cartesian points (3, N)."""
     if mesh.cylindrical:
@@ -306,9 +387,7 @@ class TraceEngine:
         self.ctx = _lib.context()
         dev = "cuda"
         nx, ny = mesh.shape
-        cells, subcells = electrode_lookup(mesh)
-        self.cells = torch.from_numpy(cells).to(dev)
-        self.subcells = torch.from_numpy(subcells).to(dev)
+        self.cells, self.subcells = electrode_lookup_device(mesh)
         lo_x, lo_y = mesh.logical_origin
         up_x, up_y = mesh.logical_upper
         self.patch_int = torch.tensor([[nx, ny, 0, 0, nx * ny, 0]], dtype=torch.int64, device=dev)

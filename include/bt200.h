@@ -169,6 +169,30 @@ int bt_trace_trajectories_2d_magnetic(bt_ctx *ctx, const bt_trace_args *args,
 int bt_trace_last_stats(bt_ctx *ctx, int64_t *windows, int64_t *records,
                         int64_t *deposit_flushes);
 
+/* -- electrode shapes (device pointers) ------------------------------------------------ */
+
+/* The configuration's electrode shapes (config.py ObjectParams.inside, the reference's
+ * sections.py:636-784 objects): count shapes, shape s of kind[s] with its parameters at
+ * params + offset[s]: 0 rectangle or line (mx, my, lx/2, ly/2), 1 circle (mx, my, r^2),
+ * 2 polygon (n, then per edge x1, y1, x2, y2, boundary threshold, x_lo, x_hi, y_lo, y_hi),
+ * 3 aperture (two such polygons: the shape and its mirror image).  The first holding a
+ * point is its electrode. */
+typedef struct bt_shapes {
+    int64_t count;
+    const int32_t *kind;
+    const int64_t *offset;
+    const double *params;
+} bt_shapes;
+
+/* solver/tracer.py:1092-1114 (BeamTracer._subcells): out (n_cells, refine, refine) int64,
+ * the electrode of every sub-cell of the cells (ci, cj) holding its four corners and its
+ * centre, -1 for none, -2 where they disagree.  x_nodes (n_x_nodes,) for a graded x axis,
+ * else NULL. */
+int bt_subcell_table(bt_ctx *ctx, const bt_shapes *shapes, const int64_t *ci,
+                     const int64_t *cj, int64_t n_cells, double origin_x, double origin_y,
+                     double h, const double *x_nodes, int64_t n_x_nodes, int64_t refine,
+                     int64_t *out);
+
 /* -- the edge field (device pointers) --------------------------------------------------- */
 
 /* solver/fields.py:18-67 and 116-152: the staggered edge fields of a potential.
