@@ -12,7 +12,7 @@ the angles.
 
 from __future__ import annotations
 
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 from scipy import constants
@@ -86,12 +86,20 @@ def _plate(centre: float, design: EinzelDesign, voltage: float) -> ObjectParams:
                         bc_type="dirichlet", bc_value=float(voltage))  # fmt: skip
 
 
+def resolved_voltages(design: EinzelDesign) -> tuple[float, float, float]:
+    """The plates' voltages: the design's, or (0, V_mid, 0) with ``V_mid`` the seed's first
+    draw (every design draws it, so the beam does not depend on whether it is used)."""
+    if design.voltages is not None:
+        return tuple(float(v) for v in design.voltages)  # type: ignore[return-value]
+    rng = np.random.default_rng(design.seed)
+    return (0.0, float(rng.uniform(*design.v_mid_range)), 0.0)
+
+
 def einzel_config(design: EinzelDesign = EinzelDesign(), **settings) -> BeamOpticsConfig:
     """The `BeamOpticsConfig` of a lens design (``settings`` override the iteration's)."""
+    voltages = resolved_voltages(design)
     rng = np.random.default_rng(design.seed)
-    voltages = design.voltages
-    if voltages is None:
-        voltages = (0.0, float(rng.uniform(*design.v_mid_range)), 0.0)
+    rng.uniform(*design.v_mid_range)  # V_mid's draw, made whether or not it is used
     beam = einzel_beam(design, rng)
     neumann = FieldBoundaryCondition.neumann(0.0)
     params = {"iterations": 20, "tolerance": 1e-3, "relaxation": 1.0, **settings}
@@ -105,3 +113,101 @@ def einzel_config(design: EinzelDesign = EinzelDesign(), **settings) -> BeamOpti
         diagnostic_planes=list(design.planes),
         **params,
     )  # fmt: skip
+
+
+# -- the batched design sweep -----------------------------------------------------------------
+
+#: The meshes of the sweep's candidates (nodes along x, r) on 80 x 20 mm.
+SWEEP_MESHES = ((257, 65), (513, 129), (1025, 257))
+
+
+def sweep_designs(count: int = 256, seed: int = 5) -> list[EinzelDesign]:
+    """Candidate lenses drawn from ``numpy.random.default_rng(seed)``: per candidate
+    ``V_mid`` in U(3, 12) kV, aperture in U(3, 7) mm, plate gap in U(10, 25) mm about the
+    middle plate at 40 mm, beam current in U(0.1, 2) mA, one of `SWEEP_MESHES`, and
+    U{2000..20000} trajectories."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        v_mid = float(rng.uniform(3e3, 12e3))
+        aperture = float(rng.uniform(3e-3, 7e-3))
+        gap = float(rng.uniform(10e-3, 25e-3))
+        current = float(rng.uniform(0.1e-3, 2e-3))
+        shape = SWEEP_MESHES[int(rng.integers(len(SWEEP_MESHES)))]
+        trajectories = int(rng.integers(2000, 20001))
+        out.append(EinzelDesign(shape=shape, centres=(40e-3 - gap, 40e-3, 40e-3 + gap),
+                                aperture=aperture, voltages=(0.0, v_mid, 0.0),
+                                current=current, trajectories=trajectories, seed=seed + 1 + k))
+    return out
+
+
+def design_cost(design: EinzelDesign) -> float:
+    """The relative cost of solving a candidate: its nodes times its trajectories."""
+    return float(design.shape[0] * design.shape[1]) * float(design.trajectories)
+
+
+def share_of_designs(designs: list[EinzelDesign], rank: int, world: int) -> list[int]:
+    """The candidates one of ``world`` ranks solves: the longest first, each to the rank
+    with the least work so far (ties to the lower rank) -- every candidate exactly once,
+    no collective needed to agree on it."""
+    load = [0.0] * world
+    mine = []
+    for k in sorted(range(len(designs)), key=lambda i: (-design_cost(designs[i]), i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += design_cost(designs[k])
+        if r == rank:
+            mine.append(k)
+    return sorted(mine)
+
+
+def evaluate_design(design: EinzelDesign, plane: float = 79e-3, **settings) -> dict:
+    """Solve a candidate to convergence; its beam moments at ``plane`` and its stats."""
+    from beamtracer_b200.model import BeamOptics
+
+    model = BeamOptics(einzel_config(design, **settings)).run()
+    moments = model.beam_moments(plane)
+    return {"current": moments.current, "rms_size": moments.rms_size,
+            "rms_angle": moments.rms_angle, "emittance": moments.emittance,
+            "iterations": len(model.state.history), "converged": model.stats["converged"]}  # fmt: skip
+
+
+def sweep(designs: list[EinzelDesign], rank: int = 0, world: int = 1, **settings) -> dict[int, dict]:
+    """This rank's share of the candidates (`share_of_designs`), each solved in turn:
+    ``{candidate index: evaluate_design(...)}``.  Ranks need no collective; a caller that
+    wants every result gathers the dictionaries."""
+    return {k: evaluate_design(designs[k], **settings) for k in share_of_designs(designs, rank, world)}
+
+
+# -- design gradients (central differences through the solver) --------------------------------
+
+#: The design parameters of a gradient: the three plate voltages and the beam current.
+GRADIENT_PARAMETERS = ("v1", "v2", "v3", "current")
+
+
+def _perturbed(design: EinzelDesign, parameter: str, delta: float) -> EinzelDesign:
+    voltages = list(resolved_voltages(design))
+    if parameter == "current":
+        return replace(design, voltages=tuple(voltages), current=design.current + delta)
+    voltages[GRADIENT_PARAMETERS.index(parameter)] += delta
+    return replace(design, voltages=tuple(voltages))
+
+
+def design_gradient(design: EinzelDesign, plane: float = 79e-3, rel_step: float = 1e-4,
+                    tolerance: float = 1e-7, iterations: int = 60) -> dict:  # fmt: skip
+    """The gradients of the rms angle and the current at ``plane`` with respect to
+    `GRADIENT_PARAMETERS`, by central differences of converged solves: voltage steps of
+    ``rel_step`` times the largest plate voltage, a current step of ``rel_step`` times the
+    current; every solve converged to ``tolerance`` [V] (tighter than the steps' effect)."""
+    scale = max(abs(v) for v in resolved_voltages(design))
+    out = {"rms_angle": np.zeros(len(GRADIENT_PARAMETERS)),
+           "current": np.zeros(len(GRADIENT_PARAMETERS)), "solves": 0}  # fmt: skip
+    for k, name in enumerate(GRADIENT_PARAMETERS):
+        step = rel_step * (design.current if name == "current" else scale)
+        plus = evaluate_design(_perturbed(design, name, step), plane, tolerance=tolerance,
+                               iterations=iterations)  # fmt: skip
+        minus = evaluate_design(_perturbed(design, name, -step), plane, tolerance=tolerance,
+                                iterations=iterations)  # fmt: skip
+        out["rms_angle"][k] = (plus["rms_angle"] - minus["rms_angle"]) / (2.0 * step)
+        out["current"][k] = (plus["current"] - minus["current"]) / (2.0 * step)
+        out["solves"] += 2
+    return out

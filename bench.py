@@ -283,6 +283,81 @@ def run_plasma(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_design(args, rank: int, world: int, local: int) -> None:
+    """Design workloads: ``gradient`` -- the gradient of the rms angle and the current at
+    79 mm with respect to the three plate voltages and the beam current of the einzel lens
+    at 401 x 101 with 8,000 rings, by central differences of converged solves (8 solves an
+    evaluation); ``sweep`` -- the seeded candidates of the batched design sweep (meshes of
+    257 x 65 to 1025 x 257, 2,000-20,000 rings), every rank solving its cost-balanced share
+    with no collective.  Device time with CUDA events, the max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    from beamtracer_b200.einzel import EinzelDesign, design_gradient, share_of_designs, sweep, sweep_designs
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))  # fmt: skip
+    stream = torch.cuda.current_stream()
+    if args.workload == "gradient":
+        design = EinzelDesign(shape=(401, 101), trajectories=8000, seed=2 + rank)
+
+        def step():
+            return design_gradient(design)
+
+        units_per_step, unit = world, "gradient evals/s"
+        metric = "einzel design-gradient evals/s (401x101 cyl., 8k rings, 4 parameters)"
+        workload = "einzel lens 401x101, 8,000 rings: d(rms angle, current)/d(V1, V2, V3, J)"
+    else:
+        designs = sweep_designs(args.sweep_count)
+
+        def step():
+            return sweep(designs, rank, world)
+
+        units_per_step, unit = args.sweep_count, "candidates/s"
+        metric = "einzel design-sweep candidates/s (257x65..1025x257, 2k-20k rings)"
+        workload = f"{args.sweep_count} seeded einzel candidates (seed 5), cost-balanced shares"
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]  # fmt: skip
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            events[k][0].record(stream)
+            result = step()
+            events[k][1].record(stream)
+        torch.cuda.synchronize()
+    total_ms = float(sum(a.elapsed_time(b) for a, b in events))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": metric, "value": units_per_step * args.steps / (total_ms / 1e3), "unit": unit,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak" if args.workload == "gradient" else "strong", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload,
+                   "share_of_rank0": len(share_of_designs(designs, 0, world))
+                   if args.workload == "sweep" else None},
+        "clocks": clocks.summary(),
+    }  # fmt: skip
+    if args.workload == "gradient":
+        line["gradient"] = {k: [float(v) for v in result[k]] for k in ("rms_angle", "current")}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -295,8 +370,12 @@ def main() -> None:
                         help="one warm solve, then one in the NVTX range 'profiled_solve'")
     parser.add_argument("--small", action="store_true",
                         help="with --profile: the lens at 401 x 101 with 2,000 rings")
-    parser.add_argument("--workload", default="einzel", choices=["einzel", "plasma"],
-                        help="plasma: the planar plasma + solenoid extraction (one GPU)")
+    parser.add_argument("--workload", default="einzel",
+                        choices=["einzel", "plasma", "gradient", "sweep"],
+                        help="plasma: the planar plasma + solenoid extraction (one GPU); "
+                             "gradient: einzel design gradients; sweep: the design sweep")
+    parser.add_argument("--sweep-count", type=int, default=32,
+                        help="with --workload sweep: the candidates of one step")
     args = parser.parse_args()
     if args.profile:
         run_profile(args)
@@ -309,6 +388,9 @@ def main() -> None:
     local = _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload in ("gradient", "sweep"):
+        run_design(args, rank, world, local)
         return
 
     import torch
