@@ -23,7 +23,7 @@
 namespace bt {
 namespace {
 
-constexpr int kCoarsest = 64;
+constexpr int kCoarsest = 256;  // the coarsest level is inverted densely (at most this size)
 constexpr double kEps0 = 8.8541878188e-12;  // scipy.constants.epsilon_0 (CODATA 2022)
 
 struct Axis {
@@ -553,16 +553,20 @@ __global__ void prolong_add(Fine F, const double *__restrict__ xc, double *__res
     prolong_item(f, F, xc, x, PlainLoad{});
 }
 
-// The coarsest level: the dense matrix of its 9-point operator, inverted in place by
-// Gauss-Jordan with partial pivoting in shared memory.  `status` is set to 1 on a zero
-// pivot (a singular operator: no node of the mesh is held).
-__global__ void coarsest_invert(i64 nx, i64 ny, const double *__restrict__ a9,
-                                double *__restrict__ inv, int *__restrict__ status) {
-    __shared__ double M[kCoarsest][kCoarsest + 1];
+// The coarsest level: the dense matrix of its 9-point operator, inverted in place in `M`
+// (global memory, n x n) by Gauss-Jordan with partial pivoting, one block.  The pivot is the
+// largest |M[r][k]| (the first such row).  `status` is set to 1 on a zero pivot (a singular
+// operator: no node of the mesh is held).
+constexpr int kInvertThreads = 1024;
+
+__global__ void __launch_bounds__(kInvertThreads) coarsest_invert(
+    i64 nx, i64 ny, const double *__restrict__ a9, double *M, int *__restrict__ status) {
     __shared__ int perm[kCoarsest];
+    __shared__ double best_v[kInvertThreads / 32];
+    __shared__ int best_r[kInvertThreads / 32];
     __shared__ int pivot_row;
     const int n = (int)(nx * ny);
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int e = tid; e < n * n; e += nt) {
         const int row = e / n, col = e % n;
         const i64 i = row / ny, j = row % ny, i2 = col / ny, j2 = col % ny;
@@ -570,70 +574,90 @@ __global__ void coarsest_invert(i64 nx, i64 ny, const double *__restrict__ a9,
         double v = 0.0;
         if (di >= -1 && di <= 1 && dj >= -1 && dj <= 1)
             v = a9[(i64)((di + 1) * 3 + (dj + 1)) * n + row];
-        M[row][col] = v;
+        M[e] = v;
     }
     __syncthreads();
     for (int k = 0; k < n; ++k) {
-        if (tid == 0) {
-            int p = k;
-            double best = fabs(M[k][k]);
-            for (int r = k + 1; r < n; ++r) {
-                const double v = fabs(M[r][k]);
-                if (v > best) {
-                    best = v;
-                    p = r;
-                }
+        // the pivot: a block-wide arg-max of |M[r][k]|, r >= k, the lowest r on ties
+        double v = -1.0;
+        int r = n;
+        for (int q = k + tid; q < n; q += nt) {
+            const double a = fabs(M[(i64)q * n + k]);
+            if (a > v) {
+                v = a;
+                r = q;
             }
-            pivot_row = p;
-            perm[k] = p;
-            if (best == 0.0) *status = 1;
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const double v2 = __shfl_down_sync(0xffffffffu, v, off);
+            const int r2 = __shfl_down_sync(0xffffffffu, r, off);
+            if (v2 > v || (v2 == v && r2 < r)) {
+                v = v2;
+                r = r2;
+            }
+        }
+        if (lane == 0) {
+            best_v[warp] = v;
+            best_r[warp] = r;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double bv = best_v[0];
+            int br = best_r[0];
+            for (int w = 1; w < nt / 32; ++w)
+                if (best_v[w] > bv || (best_v[w] == bv && best_r[w] < br)) {
+                    bv = best_v[w];
+                    br = best_r[w];
+                }
+            if (br >= n) br = k;
+            pivot_row = br;
+            perm[k] = br;
+            if (!(bv > 0.0)) *status = 1;
         }
         __syncthreads();
         const int p = pivot_row;
         if (p != k)
             for (int c = tid; c < n; c += nt) {
-                const double t = M[k][c];
-                M[k][c] = M[p][c];
-                M[p][c] = t;
+                const double t = M[(i64)k * n + c];
+                M[(i64)k * n + c] = M[(i64)p * n + c];
+                M[(i64)p * n + c] = t;
             }
         __syncthreads();
-        const double piv = M[k][k];
+        const double piv = M[(i64)k * n + k];
         __syncthreads();
-        for (int c = tid; c < n; c += nt) M[k][c] = (c == k ? 1.0 : M[k][c]) / piv;
+        for (int c = tid; c < n; c += nt) M[(i64)k * n + c] = (c == k ? 1.0 : M[(i64)k * n + c]) / piv;
         __syncthreads();
         for (int e = tid; e < n * n; e += nt) {
-            const int r = e / n, c = e % n;
-            if (r == k) continue;
-            const double f = M[r][k];
-            if (c == k)
-                continue;
-            M[r][c] -= f * M[k][c];
+            const int rr = e / n, c = e % n;
+            if (rr == k || c == k) continue;
+            M[e] -= M[(i64)rr * n + k] * M[(i64)k * n + c];
         }
         __syncthreads();
-        for (int r = tid; r < n; r += nt)
-            if (r != k) M[r][k] = -M[r][k] * M[k][k];
+        for (int rr = tid; rr < n; rr += nt)
+            if (rr != k) M[(i64)rr * n + k] = -M[(i64)rr * n + k] * M[(i64)k * n + k];
         __syncthreads();
     }
     for (int k = n - 1; k >= 0; --k) {
         const int p = perm[k];
         if (p != k)
-            for (int r = tid; r < n; r += nt) {
-                const double t = M[r][k];
-                M[r][k] = M[r][p];
-                M[r][p] = t;
+            for (int rr = tid; rr < n; rr += nt) {
+                const double t = M[(i64)rr * n + k];
+                M[(i64)rr * n + k] = M[(i64)rr * n + p];
+                M[(i64)rr * n + p] = t;
             }
         __syncthreads();
     }
-    for (int e = tid; e < n * n; e += nt) inv[e] = M[e / n][e % n];
 }
 
-__global__ void coarsest_apply(int n, const double *__restrict__ inv, const double *__restrict__ b,
-                               double *__restrict__ x) {
+// x = inv b on the active rows, 0 on held ones (the inverse's held rows are unit rows up to
+// the rounding that pivoting mixes into them; a correction never moves a held node).
+__global__ void coarsest_apply(int n, const double *__restrict__ inv, const uint8_t *__restrict__ active,
+                               const double *__restrict__ b, double *__restrict__ x) {
     const int r = threadIdx.x;
     if (r >= n) return;
     double s = 0.0;
     for (int c = 0; c < n; ++c) s += inv[r * n + c] * b[c];
-    x[r] = s;
+    x[r] = active[r] ? s : 0.0;
 }
 
 // The 9-point form of the 5-point level-0 operator, for a mesh whose first level is
@@ -668,8 +692,12 @@ struct TailLevel {
     Fine next;      // the map to the next coarser level (unused on the coarsest)
 };
 
-// Where a tail level lives in shared memory: offsets in doubles from the start, in int32s
-// from the int block, in bytes from the byte block.
+// Where a tail level lives in shared memory.  The block's shared memory is a static image
+// -- the levels' coefficients and transfer weights (doubles), transfer indices (int32s) and
+// active flags (bytes), copied in one piece from a device buffer kept in step with the
+// hierarchy -- then the levels' x (with a ring of zeros), b and r (doubles).  a9, wx, wy,
+// rxw, ryw count doubles from the start; lox, loy, rx0, ry0 int32s from the int block; act
+// bytes from the byte block; x, b, r doubles from the dynamic block.
 struct TailPlan {
     int nx, ny, n, ncx, ncy;
     int x, b, r, a9;         // x: (nx + 2) (ny + 2) with a ring of zeros; b, r: n; a9: 9 n
@@ -680,26 +708,23 @@ struct TailPlan {
 
 struct TailLayout {
     std::vector<TailPlan> plan;
-    int doubles = 0, ints = 0, bytes = 0, inv = 0;
-    size_t total() const {
-        return sizeof(double) * (size_t)doubles + sizeof(int32_t) * (size_t)ints + (size_t)bytes;
+    int doubles = 0, ints = 0, bytes = 0, dynamic = 0;
+    // the static image's bytes, rounded up to whole 16-byte words, and where the dynamic
+    // doubles start
+    size_t image() const {
+        const size_t b = sizeof(double) * (size_t)doubles + sizeof(int32_t) * (size_t)ints + bytes;
+        return (b + 15) & ~(size_t)15;
     }
+    size_t total() const { return image() + sizeof(double) * (size_t)dynamic; }
 };
 
-// The V-cycle of the small levels in one block, entirely in shared memory: every tail
-// level's x (with a ring of zeros around the mesh, so stencils need no bounds tests), b, r,
-// coefficients, active flags and transfer tables and the coarsest level's inverse are
-// staged once (levels[0].b read from global memory, levels[0].x written back at the end);
-// four-colour Gauss-Seidel, residual and restriction down, the coarsest level's inverse,
-// prolongation and smoothing up, with a block barrier between steps.  A zero neighbour
-// outside the mesh changes no sum, so the values are those of the launched kernels.
-__device__ __forceinline__ void tail_smooth(const TailPlan &P, double *sm, const uint8_t *act,
-                                            int colour, int tid, int nt) {
+__device__ __forceinline__ void tail_smooth(const TailPlan &P, const double *sm, double *smd,
+                                            const uint8_t *act, int colour, int tid, int nt) {
     const int nx = P.nx, ny = P.ny, n = P.n, W = ny + 2;
     const int ci = colour >> 1, cj = colour & 1;
     const int hx = (nx - ci + 1) >> 1, hy = (ny - cj + 1) >> 1;
-    double *x = sm + P.x;
-    const double *b = sm + P.b, *a9 = sm + P.a9;
+    double *x = smd + P.x;
+    const double *b = smd + P.b, *a9 = sm + P.a9;
     for (int t = tid; t < hx * hy; t += nt) {
         const int ti = t / hy;
         const int i = 2 * ti + ci, j = 2 * (t - ti * hy) + cj;
@@ -719,11 +744,11 @@ __device__ __forceinline__ void tail_smooth(const TailPlan &P, double *sm, const
     }
 }
 
-__device__ __forceinline__ void tail_residual(const TailPlan &P, double *sm, const uint8_t *act,
-                                              int tid, int nt) {
+__device__ __forceinline__ void tail_residual(const TailPlan &P, const double *sm, double *smd,
+                                              const uint8_t *act, int tid, int nt) {
     const int ny = P.ny, n = P.n, W = ny + 2;
-    const double *x = sm + P.x, *b = sm + P.b, *a9 = sm + P.a9;
-    double *r = sm + P.r;
+    const double *x = smd + P.x, *b = smd + P.b, *a9 = sm + P.a9;
+    double *r = smd + P.r;
     for (int f = tid; f < n; f += nt) {
         if (!act[f]) {
             r[f] = 0.0;
@@ -746,13 +771,13 @@ __device__ __forceinline__ void tail_residual(const TailPlan &P, double *sm, con
 }
 
 // b of the next level = R r of this one (the next level's x is zero already).
-__device__ __forceinline__ void tail_restrict(const TailPlan &P, const TailPlan &C, double *sm,
-                                              const int32_t *smi, const uint8_t *act, int tid,
-                                              int nt) {
+__device__ __forceinline__ void tail_restrict(const TailPlan &P, const TailPlan &C,
+                                              const double *sm, double *smd, const int32_t *smi,
+                                              const uint8_t *act, int tid, int nt) {
     const int ny = P.ny, ncy = P.ncy;
-    const double *r = sm + P.r, *rxw = sm + P.rxw, *ryw = sm + P.ryw;
+    const double *r = smd + P.r, *rxw = sm + P.rxw, *ryw = sm + P.ryw;
     const int32_t *rx0 = smi + P.rx0, *ry0 = smi + P.ry0;
-    double *bc = sm + C.b;
+    double *bc = smd + C.b;
     for (int t = tid; t < C.n; t += nt) {
         const int I = t / ncy, J = t - I * ncy;
         const int k0 = rx0[I], l0 = ry0[J];
@@ -775,12 +800,12 @@ __device__ __forceinline__ void tail_restrict(const TailPlan &P, const TailPlan 
 }
 
 // x of this level += P x of the next level.
-__device__ __forceinline__ void tail_prolong(const TailPlan &P, const TailPlan &C, double *sm,
-                                             const int32_t *smi, const uint8_t *act, int tid,
-                                             int nt) {
+__device__ __forceinline__ void tail_prolong(const TailPlan &P, const TailPlan &C,
+                                             const double *sm, double *smd, const int32_t *smi,
+                                             const uint8_t *act, int tid, int nt) {
     const int ny = P.ny, n = P.n, W = ny + 2, ncx = P.ncx, ncy = P.ncy, Wc = ncy + 2;
-    double *x = sm + P.x;
-    const double *xc = sm + C.x, *wxs = sm + P.wx, *wys = sm + P.wy;
+    double *x = smd + P.x;
+    const double *xc = smd + C.x, *wxs = sm + P.wx, *wys = sm + P.wy;
     const int32_t *lox = smi + P.lox, *loy = smi + P.loy;
     for (int f = tid; f < n; f += nt) {
         if (!act[f]) continue;
@@ -802,48 +827,37 @@ __device__ __forceinline__ void tail_prolong(const TailPlan &P, const TailPlan &
     }
 }
 
-template <class T>
-__device__ __forceinline__ void stage(T *dst, const T *src, int count, int tid, int nt) {
-#pragma unroll 4
-    for (int e = tid; e < count; e += nt) dst[e] = src[e];
-}
-
+// levels[0] reads b from, and writes x to, global memory; `image` holds the static part
+// of the shared memory (image_words 16-byte words); inv is the coarsest level's inverse.
 __global__ void __launch_bounds__(kTailThreads, 1)
 vcycle_tail(const TailLevel *__restrict__ levels, const TailPlan *__restrict__ plans, int count,
-            const double *__restrict__ inv, int inv_at, int doubles, int ints, int sweeps) {
-    extern __shared__ double sm[];
+            const uint4 *__restrict__ image, int image_words, int doubles, int ints,
+            const double *__restrict__ inv, int sweeps) {
+    extern __shared__ __align__(16) double sm[];
     __shared__ TailPlan plan[kTailMaxLevels];
     int32_t *smi = reinterpret_cast<int32_t *>(sm + doubles);
     uint8_t *smb = reinterpret_cast<uint8_t *>(smi + ints);
+    double *smd = sm + 2 * image_words;  // the dynamic doubles follow the image
     const int tid = threadIdx.x, nt = blockDim.x;
+    const PlainLoad load{};
     {
         const int *src = reinterpret_cast<const int *>(plans);
         int *dst = reinterpret_cast<int *>(plan);
         const int words = count * (int)(sizeof(TailPlan) / sizeof(int));
         for (int e = tid; e < words; e += nt) dst[e] = src[e];
     }
+    // the static image in one piece, x zero, level 0's b
+    uint4 *dst = reinterpret_cast<uint4 *>(sm);
+#pragma unroll 4
+    for (int e = tid; e < image_words; e += nt) dst[e] = image[e];
     for (int l = 0; l < count; ++l) {
-        const TailLevel &L = levels[l];
         const TailPlan &P = plans[l];
-        stage(sm + P.a9, L.a9, 9 * P.n, tid, nt);
-        stage(smb + P.act, L.active, P.n, tid, nt);
-        for (int e = tid; e < (P.nx + 2) * (P.ny + 2); e += nt) sm[P.x + e] = 0.0;
-        if (l + 1 < count) {
-            const Fine &G = L.next;
-            stage(sm + P.wx, G.wx, P.nx, tid, nt);
-            stage(sm + P.wy, G.wy, P.ny, tid, nt);
-            stage(sm + P.rxw, G.rxw, kRestrict * P.ncx, tid, nt);
-            stage(sm + P.ryw, G.ryw, kRestrict * P.ncy, tid, nt);
-            stage(smi + P.lox, G.lox, P.nx, tid, nt);
-            stage(smi + P.loy, G.loy, P.ny, tid, nt);
-            stage(smi + P.rx0, G.rx0, P.ncx, tid, nt);
-            stage(smi + P.ry0, G.ry0, P.ncy, tid, nt);
-        }
+        for (int e = tid; e < (P.nx + 2) * (P.ny + 2); e += nt) smd[P.x + e] = 0.0;
     }
     {
-        const int nc = plans[count - 1].n;
-        stage(sm + inv_at, inv, nc * nc, tid, nt);
-        stage(sm + plans[0].b, levels[0].b, plans[0].n, tid, nt);
+        const TailPlan &P = plans[0];
+        const double *b0 = levels[0].b;
+        for (int f = tid; f < P.n; f += nt) smd[P.b + f] = b0[f];
     }
     __syncthreads();
     for (int l = 0; l + 1 < count; ++l) {
@@ -851,48 +865,50 @@ vcycle_tail(const TailLevel *__restrict__ levels, const TailPlan *__restrict__ p
         const uint8_t *act = smb + P.act;
         for (int s = 0; s < sweeps; ++s)
             for (int c = 0; c < 4; ++c) {
-                tail_smooth(P, sm, act, c, tid, nt);
+                tail_smooth(P, sm, smd, act, c, tid, nt);
                 __syncthreads();
             }
-        tail_residual(P, sm, act, tid, nt);
+        tail_residual(P, sm, smd, act, tid, nt);
         __syncthreads();
-        tail_restrict(P, plan[l + 1], sm, smi, act, tid, nt);
+        tail_restrict(P, plan[l + 1], sm, smd, smi, act, tid, nt);
         __syncthreads();
     }
     {
+        // the coarsest level: x = inv b, a warp per row, its lanes over the columns
         const TailPlan &C = plan[count - 1];
-        const int n = C.n, W = C.ny + 2;
-        const double *b = sm + C.b, *iv = sm + inv_at;
-        for (int row = tid; row < n; row += nt) {
+        const int n = C.n, W = C.ny + 2, lane = tid & 31;
+        const double *b = smd + C.b;
+        const uint8_t *act = smb + C.act;
+        for (int row = tid >> 5; row < n; row += nt >> 5) {
             double s = 0.0;
-            for (int c = 0; c < n; ++c) s += iv[row * n + c] * b[c];
-            const int i = row / C.ny;
-            sm[C.x + row + 2 * i + W + 1] = s;
+            for (int c = lane; c < n; c += 32) s += __ldg(inv + (i64)row * n + c) * b[c];
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+            if (lane == 0) smd[C.x + row + 2 * (row / C.ny) + W + 1] = act[row] ? s : 0.0;
         }
         __syncthreads();
     }
     for (int l = count - 2; l >= 0; --l) {
         const TailPlan &P = plan[l];
         const uint8_t *act = smb + P.act;
-        tail_prolong(P, plan[l + 1], sm, smi, act, tid, nt);
+        tail_prolong(P, plan[l + 1], sm, smd, smi, act, tid, nt);
         __syncthreads();
         for (int s = 0; s < sweeps; ++s)
             for (int c = 3; c >= 0; --c) {
-                tail_smooth(P, sm, act, c, tid, nt);
+                tail_smooth(P, sm, smd, act, c, tid, nt);
                 __syncthreads();
             }
     }
     {
         const TailPlan &P = plan[0];
         const int W = P.ny + 2;
-        for (int f = tid; f < P.n; f += nt) {
-            const int i = f / P.ny;
-            levels[0].x[f] = sm[P.x + f + 2 * i + W + 1];
-        }
+        double *x0 = levels[0].x;
+        for (int f = tid; f < P.n; f += nt) x0[f] = smd[P.x + f + 2 * (f / P.ny) + W + 1];
     }
 }
 
-// The shared-memory layout of tail levels first .. (the coarsest).
+// The shared-memory layout of tail levels first .. (the coarsest): the static image
+// (coefficients of every level but the coarsest, transfer tables, active flags), then the
+// dynamic x, b, r of every level.
 TailLayout tail_layout(const std::vector<Level> &levels, int first) {
     TailLayout T;
     const int last = (int)levels.size() - 1;
@@ -902,17 +918,11 @@ TailLayout tail_layout(const std::vector<Level> &levels, int first) {
         P.nx = (int)L.nx;
         P.ny = (int)L.ny;
         P.n = (int)L.n;
-        P.x = T.doubles;
-        T.doubles += (P.nx + 2) * (P.ny + 2);
-        P.b = T.doubles;
-        T.doubles += P.n;
-        P.r = T.doubles;
-        T.doubles += P.n;
-        P.a9 = T.doubles;
-        T.doubles += 9 * P.n;
         if (l < last) {
             P.ncx = (int)levels[l + 1].nx;
             P.ncy = (int)levels[l + 1].ny;
+            P.a9 = T.doubles;
+            T.doubles += 9 * P.n;
             P.wx = T.doubles;
             T.doubles += P.nx;
             P.wy = T.doubles;
@@ -932,10 +942,14 @@ TailLayout tail_layout(const std::vector<Level> &levels, int first) {
         }
         P.act = T.bytes;
         T.bytes += P.n;
+        P.x = T.dynamic;
+        T.dynamic += (P.nx + 2) * (P.ny + 2);
+        P.b = T.dynamic;
+        T.dynamic += P.n;
+        P.r = T.dynamic;
+        T.dynamic += P.n;
         T.plan.push_back(P);
     }
-    T.inv = T.doubles;
-    T.doubles += (int)(levels[last].n * levels[last].n);
     return T;
 }
 
@@ -1159,9 +1173,10 @@ struct bt_poisson {
     i64 tail_nodes = 4096;  // levels at most this large may go to the one-block tail
     int tail_start = -1;    // the first level of the V-cycle's one-block tail
     size_t tail_smem = 0;   // its shared memory
-    int tail_doubles = 0, tail_ints = 0, tail_inv = 0;  // its layout (bt::TailLayout)
+    int tail_doubles = 0, tail_ints = 0, tail_words = 0;  // its layout (bt::TailLayout)
     bt::Buffer tail_levels;  // its TailLevel descriptors
     bt::Buffer tail_plans;   // and TailPlan layouts
+    bt::Buffer tail_image;   // the static part of its shared memory (tail_words 16-byte words)
     bt::Buffer dot_partial;  // per-block partial dot products
     // the V-cycle from a zero guess on level 0's b into its x, captured once as a graph
     cudaGraph_t vgraph = nullptr;
@@ -1179,6 +1194,8 @@ struct bt_poisson {
 
 namespace bt {
 namespace {
+
+void refresh_tail_image(bt_poisson *p);
 
 Fine fine_of(Level &L, Level &C, bool first) {
     Fine F{};
@@ -1244,9 +1261,10 @@ void build_hierarchy(bt_poisson *p, const double *reaction) {
                   Lc.a9.as<double>(9 * Lc.n));
     int *status = p->status.as<int>(1);
     BT_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-    BT_LAUNCH(p->ctx, coarsest_invert, 1, 256, 0, st, Lc.nx, Lc.ny, Lc.a9.as<double>(9 * Lc.n),
-                                       p->inv.as<double>(Lc.n * Lc.n), status);
+    BT_LAUNCH(p->ctx, coarsest_invert, 1, kInvertThreads, 0, st, Lc.nx, Lc.ny,
+              Lc.a9.as<double>(9 * Lc.n), p->inv.as<double>(Lc.n * Lc.n), status);
     BT_CHECK_LAUNCH();
+    refresh_tail_image(p);
     p->built = true;
     p->reaction_on = reaction != nullptr;
 }
@@ -1273,7 +1291,7 @@ void setup_tail(bt_poisson *p) {
     p->tail_smem = T.total();
     p->tail_doubles = T.doubles;
     p->tail_ints = T.ints;
-    p->tail_inv = T.inv;
+    p->tail_words = (int)(T.image() / 16);
     std::vector<TailLevel> tail;
     for (int l = p->tail_start; l < levels; ++l) {
         Level &L = p->levels[l];
@@ -1294,6 +1312,40 @@ void setup_tail(bt_poisson *p) {
                        sizeof(TailLevel) * tail.size(), cudaMemcpyHostToDevice));
     BT_CUDA(cudaMemcpy(p->tail_plans.as<TailPlan>(T.plan.size()), T.plan.data(),
                        sizeof(TailPlan) * T.plan.size(), cudaMemcpyHostToDevice));
+    p->tail_image.get(T.image());
+    refresh_tail_image(p);
+}
+
+// Copy the tail levels' coefficients, transfer tables and active flags into the tail's
+// static image (after the hierarchy's coefficients change).
+void refresh_tail_image(bt_poisson *p) {
+    if (p->tail_start <= 0) return;
+    cudaStream_t st = p->ctx->stream;
+    const TailLayout T = tail_layout(p->levels, p->tail_start);
+    char *image = static_cast<char *>(p->tail_image.get(T.image()));
+    double *d = reinterpret_cast<double *>(image);
+    int32_t *ints = reinterpret_cast<int32_t *>(d + T.doubles);
+    uint8_t *bytes = reinterpret_cast<uint8_t *>(ints + T.ints);
+    auto copy = [&](void *dst, const void *src, size_t n) {
+        if (n) BT_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToDevice, st));
+    };
+    const int levels = (int)p->levels.size();
+    for (int l = p->tail_start; l < levels; ++l) {
+        Level &L = p->levels[l];
+        const TailPlan &P = T.plan[l - p->tail_start];
+        copy(bytes + P.act, L.active.as<uint8_t>(L.n), L.n);
+        if (l + 1 == levels) continue;
+        const Fine F = fine_of(L, p->levels[l + 1], false);
+        copy(d + P.a9, L.a9.as<double>(9 * L.n), sizeof(double) * 9 * L.n);
+        copy(d + P.wx, F.wx, sizeof(double) * P.nx);
+        copy(d + P.wy, F.wy, sizeof(double) * P.ny);
+        copy(d + P.rxw, F.rxw, sizeof(double) * kRestrict * P.ncx);
+        copy(d + P.ryw, F.ryw, sizeof(double) * kRestrict * P.ncy);
+        copy(ints + P.lox, F.lox, sizeof(int32_t) * P.nx);
+        copy(ints + P.loy, F.loy, sizeof(int32_t) * P.ny);
+        copy(ints + P.rx0, F.rx0, sizeof(int32_t) * P.ncx);
+        copy(ints + P.ry0, F.ry0, sizeof(int32_t) * P.ncy);
+    }
 }
 
 void drop_graphs(bt_poisson *p) {
@@ -1376,13 +1428,14 @@ void vcycle(bt_poisson *p, size_t l) {
         const Level &Lc = p->levels.back();
         BT_LAUNCH(p->ctx, vcycle_tail, 1, kTailThreads, p->tail_smem, st,
                   p->tail_levels.as<TailLevel>(count), p->tail_plans.as<TailPlan>(count), count,
-                  p->inv.as<double>(Lc.n * Lc.n), p->tail_inv, p->tail_doubles, p->tail_ints,
+                  static_cast<const uint4 *>(p->tail_image.get(16 * (size_t)p->tail_words)),
+                  p->tail_words, p->tail_doubles, p->tail_ints, p->inv.as<double>(Lc.n * Lc.n),
                   p->coarse_sweeps);
         return;
     }
     if (l + 1 == p->levels.size()) {
         BT_LAUNCH(p->ctx, coarsest_apply, 1, kCoarsest, 0, st, (int)L.n, p->inv.as<double>(L.n * L.n),
-                                               L.b.as<double>(L.n), L.x.as<double>(L.n));
+                  L.active.as<uint8_t>(L.n), L.b.as<double>(L.n), L.x.as<double>(L.n));
         return;
     }
     Level &C = p->levels[l + 1];
