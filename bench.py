@@ -50,6 +50,13 @@ FLOPS_PER_RK4_STEP = 370
 #: reduction) and per node (charge read and written).
 DEPOSIT_BYTES_PER_RECORD = 28 * 2
 NOMINAL_FP64_TFLOPS = 37.0
+#: The trace's algorithmic bytes per step: its deposit record (u32 key, u, w, q f64).
+TRACE_BYTES_PER_STEP = 28
+#: DRAM bytes read + written per trace_window launch at this workload: ncu's
+#: dram__bytes_read.sum + dram__bytes_write.sum averaged over the 175 launches of one
+#: converged solve (1.864 MB read, 0.026 MB written; the records it writes stay in L2 and
+#: drain during the deposit).
+TRACE_DRAM_BYTES_PER_LAUNCH = 1.890e6
 #: Timed end-to-end calls (after one untimed call); their median is reported.
 E2E_RUNS = 5
 
@@ -474,11 +481,22 @@ def main() -> None:
     dep_ms, dep_launches = timers["deposit"]
     records = steps_total
     dep_bytes = records * DEPOSIT_BYTES_PER_RECORD
-    hbm = {"bound": "hbm", "kernel": "deposit",
-           "achieved": dep_bytes / (dep_ms / 1e3) / 1e9 if dep_ms else None,
+    deposit = {"bound": "hbm", "kernel": "deposit",
+               "achieved": dep_bytes / (dep_ms / 1e3) / 1e9 if dep_ms else None,
+               "peak": peaks["hbm_gbs"], "unit": "GB/s",
+               "frac": (dep_bytes / (dep_ms / 1e3) / 1e9) / peaks["hbm_gbs"] if dep_ms else None,
+               "peak_source": peaks["source"], "traffic": None}  # fmt: skip
+    # the dominant kernel, the trace: its algorithmic bytes are the deposit records it
+    # writes (the edge fields it reads stay in L1/L2); its limit is the latency of its
+    # dependent FP64 chain at one warp per scheduler (roofline_fp64)
+    per_launch = TRACE_BYTES_PER_STEP * steps_total / max(trace_launches, 1)
+    trace_gbs = per_launch / (trace_ms / max(trace_launches, 1) / 1e3) / 1e9 if trace_ms else None
+    hbm = {"bound": "hbm", "kernel": "trace_window", "achieved": trace_gbs,
            "peak": peaks["hbm_gbs"], "unit": "GB/s",
-           "frac": (dep_bytes / (dep_ms / 1e3) / 1e9) / peaks["hbm_gbs"] if dep_ms else None,
-           "peak_source": peaks["source"], "traffic": None}  # fmt: skip
+           "frac": trace_gbs / peaks["hbm_gbs"] if trace_gbs else None,
+           "peak_source": peaks["source"], "traffic": TRACE_DRAM_BYTES_PER_LAUNCH,
+           "algorithmic_bytes_per_launch": per_launch,
+           "limiter": "FP64 dependency latency at one warp per scheduler"}  # fmt: skip
 
     # end to end: the public call from host inputs to host results; one untimed call first
     # (its first-use allocations), then the median of E2E_RUNS calls (the host is shared,
@@ -518,7 +536,8 @@ def main() -> None:
                    "vcycles_per_solve": sum(h["krylov_steps"] for h in history),
                    "trajectories": 20000, "mesh": [801, 201], "window": args.window,
                    "l2": "256 MiB written between timed steps"},
-        "roofline": hbm, "roofline_fp64": fp64, "kernels": kernels,
+        "roofline": hbm, "roofline_fp64": fp64, "roofline_deposit": deposit,
+        "kernels": kernels,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms": float(np.median(e2e_ms)),
                 "runs_ms": [round(v, 2) for v in e2e_ms]},
