@@ -67,7 +67,8 @@ class BeamOptics:
                 config = config.replace(**settings)
         self.config = config
         self.comm = comm
-        self.rank = 0
+        self.rank = comm.Get_rank() if comm is not None else 0
+        self.size = comm.Get_size() if comm is not None else 1
         self.verbose = verbose
         grid = config.grid
         self.species_names = [beam.name for beam in config.beams]
@@ -162,7 +163,13 @@ class BeamOptics:
             parts.append(particles)
         if not parts:
             raise ValueError("BeamOptics needs at least one beam")
-        self._beam = (BeamParticles.concatenate(parts), j_over_v)
+        particles = BeamParticles.concatenate(parts)
+        if self.size > 1:
+            # every rank traces its share; the node charges are summed over the ranks
+            from beamtracer_b200.distributed import share
+
+            particles = particles.subset(share(len(particles), self.rank, self.size))
+        self._beam = (particles, j_over_v)
         return self._beam
 
     def run(self, callback: Callable[[int, VlasovState], None] | None = None, *,
@@ -183,6 +190,8 @@ class BeamOptics:
             plasma = PlasmaModel(config.plasma.electron_temperature, config.plasma.plasma_potential,
                                  config.plasma.initial_plasma_x, config.plasma.rho_e)  # fmt: skip
         compensation = [Compensation(c.x_min, c.x_max, c.fraction) for c in config.compensation]
+        if self.size > 1:
+            self.tracer.reduce = self.comm.allreduce_tensor
         self._state = vlasov_iterate(
             self.mesh, self._particles, self.tracer, iterations=config.iterations,
             plasma=plasma, compensation=compensation, tolerance=config.tolerance,
@@ -191,6 +200,10 @@ class BeamOptics:
             coarse_tolerance=config.coarse_tolerance, field_backend=config.field_backend,
             callback=callback, density_tolerance=density_tolerance,
         )  # fmt: skip
+        if self.size > 1:
+            from beamtracer_b200.distributed import gather_trace
+
+            gather_trace(self.comm, self._state.trace)
         self._is_finished = True
         return self
 

@@ -290,6 +290,8 @@ def vlasov_iterate(
             engine.load(particles)
         loaded = particles
         engine.run(fx, fy)
+        if tracer.reduce is not None:
+            tracer.reduce(engine.charge)  # the node charges of every rank's share, summed
         tracer._capacity = engine.capacity
         if mixer is not None and iteration > 0:
             deposit = engine.density()
