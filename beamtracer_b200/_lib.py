@@ -170,8 +170,9 @@ class Context:
         check(lib().bt_ctx_create(self.device, ctypes.byref(handle)))
         self.handle = handle
 
-    def use_stream(self, stream: int | None) -> None:
-        """Queue work on ``stream`` (a ``cudaStream_t`` as an int; None: the context's own)."""
+    def use_stream(self, stream: int) -> None:
+        """Queue work on ``stream`` (a ``cudaStream_t`` as an int; 0: CUDA's default stream,
+        which is torch's default stream)."""
         check(lib().bt_ctx_set_stream(self.handle, P(stream) if stream else None))
 
     def set_timing(self, on: bool) -> None:

@@ -221,7 +221,7 @@ int bt_ctx_destroy(bt_ctx *ctx) {
 int bt_ctx_set_stream(bt_ctx *ctx, void *stream) {
     return bt::guarded([&] {
         BT_REQUIRE(ctx, "ctx: null context");
-        ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+        ctx->stream = static_cast<cudaStream_t>(stream);  // NULL: CUDA's default stream
     });
 }
 

@@ -1466,9 +1466,13 @@ void vcycle(bt_poisson *p, size_t l) {
 // buffer it touches keeps its address for the solver's life, so one capture serves every
 // solve and every Newton Jacobian (whose coefficients change in place).
 void capture_vcycle(bt_poisson *p) {
-    cudaStream_t st = p->ctx->stream;
+    // captured on the context's own stream (the default stream cannot capture); the
+    // graph then runs on whichever stream the context queues on
+    cudaStream_t st = p->ctx->own_stream;
+    cudaStream_t queue = p->ctx->stream;
     Level &L = p->levels[0];
     const i64 before = p->ctx->launch_count;
+    p->ctx->stream = st;
     BT_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     try {
         BT_CUDA(cudaMemsetAsync(L.x.as<double>(L.n), 0, sizeof(double) * L.n, st));
@@ -1477,8 +1481,10 @@ void capture_vcycle(bt_poisson *p) {
         cudaGraph_t broken = nullptr;
         cudaStreamEndCapture(st, &broken);
         if (broken) cudaGraphDestroy(broken);
+        p->ctx->stream = queue;
         throw;
     }
+    p->ctx->stream = queue;
     BT_CUDA(cudaStreamEndCapture(st, &p->vgraph));
     BT_CUDA(cudaGraphInstantiate(&p->vexec, p->vgraph, 0));
     p->vgraph_kernels = p->ctx->launch_count - before;

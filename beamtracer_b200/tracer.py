@@ -474,32 +474,51 @@ class TraceEngine:
             self.paths[:k, 0] = self.first_points
 
     def _kernel(self, active, fx, fy) -> None:
-        from beamtracer_b200.kernels import trace_trajectories_2d
+        """One call of the trace entry point: its arguments built straight from the
+        engine's device tensors (the plugin's staging and checks are for outside callers)."""
+        from beamtracer_b200 import _lib
 
         mesh = self.mesh
         lo_x, lo_y = mesh.logical_origin
         up_x, up_y = mesh.logical_upper
-        trace_trajectories_2d(
-            active, self.x, self.v, self.qm, self.dq, self.steps, self.status,
-            self.electrode, fx.reshape(-1), fy.reshape(-1), self.patch_int, self.patch_real,
-            lo_x, lo_y, mesh.h, up_x, up_y, geometry_code(mesh),
-            INTEGRATORS.index(self.integrator), self.step_fraction, self.max_steps,
-            self.cells, self.subcells, SUBCELLS, self.planes_dev, self.hits, self.counts,
-            self.path_slot, self.paths, self.path_count, 1, self.charge, int(mesh.graded),
-            self.x_nodes, self.inv_c2, window=self.window, magnetic=self.magnetic,
+        d = _lib.dptr
+        a = _lib.TraceArgs(
+            d(active), int(active.numel()), d(self.x), d(self.v), self.n, d(self.qm),
+            d(self.dq), d(self.steps), d(self.status), d(self.electrode), d(fx), d(fy),
+            d(self.patch_int), d(self.patch_real), 1, float(lo_x), float(lo_y), float(mesh.h),
+            float(up_x), float(up_y), geometry_code(mesh), INTEGRATORS.index(self.integrator),
+            self.step_fraction, self.max_steps, d(self.cells), d(self.subcells), SUBCELLS,
+            d(self.planes_dev), int(self.planes_dev.numel()), d(self.hits),
+            int(self.hits.shape[2]), d(self.counts), d(self.path_slot), d(self.paths),
+            int(self.paths.shape[1]), d(self.path_count), 1, d(self.charge), self.n_nodes,
+            int(mesh.graded), d(self.x_nodes), int(self.x_nodes.numel()), self.inv_c2,
         )  # fmt: skip
+        lib, ctx = _lib.lib(), _lib.context()
+        if self.magnetic is None:
+            _lib.check(lib.bt_trace_trajectories_2d(ctx.handle, ctypes.byref(a), self.window))
+        else:
+            m = self.magnetic.descriptor()
+            _lib.check(lib.bt_trace_trajectories_2d_magnetic(ctx.handle, ctypes.byref(a),
+                                                             ctypes.byref(m), self.window))  # fmt: skip
 
     def run(self, fx, fy) -> None:
         """Trace the loaded beam through the edge fields (device arrays)."""
         torch = self.torch
         mesh = self.mesh
+        fx, fy = fx.reshape(-1), fy.reshape(-1)
+        zero = torch.zeros(1, dtype=torch.int64, device="cuda")
         while True:
             self._reset()
             active = self.start_active
             while active.numel():
                 self._kernel(active, fx, fy)
+                # one read-back: the paused trajectories, the fullest hit and path buffers
                 paused_mask = self.status[active] == _PAUSED
-                if not bool(paused_mask.any()):
+                flags = torch.stack([paused_mask.sum(),
+                                     self.counts.max() if self.counts.numel() else zero[0],
+                                     self.path_count.max()]).cpu().tolist()  # fmt: skip
+                most, longest = flags[1], flags[2]
+                if flags[0] == 0:
                     break
                 paused = active[paused_mask]
                 points = self.x[:, paused].cpu().numpy()
@@ -511,9 +530,10 @@ class TraceEngine:
                 self.electrode[stopped] = hit_dev[inside]
                 active = paused[~inside]
                 self.status[active] = _ALIVE
+            else:
+                most = int(self.counts.max()) if self.counts.numel() else 0
+                longest = int(self.path_count.max())
             capacity, path_capacity = self.capacity
-            most = int(self.counts.max()) if self.counts.numel() else 0
-            longest = int(self.path_count.max())
             if most <= capacity and longest <= path_capacity:
                 return
             self.capacity = (max(capacity, most), max(path_capacity, longest))

@@ -38,7 +38,11 @@ typedef struct bt_ctx bt_ctx;
 /* A context on CUDA device `device` with its own non-blocking stream. */
 int bt_ctx_create(int device, bt_ctx **out);
 int bt_ctx_destroy(bt_ctx *ctx);
-/* Queue the context's work on `stream` (a cudaStream_t; NULL: the context's own). */
+/* Queue the context's work on `stream` (a cudaStream_t; NULL is CUDA's default stream, as
+ * for CuPy's and PyTorch's default streams).  A new context queues on its own non-blocking
+ * stream until this is called; work on another stream is ordered with the context's only
+ * by that stream's own rules (the default stream waits for blocking streams, not for
+ * non-blocking ones). */
 int bt_ctx_set_stream(bt_ctx *ctx, void *stream);
 int bt_ctx_synchronize(bt_ctx *ctx);
 /* Time the context's launches with CUDA events on its stream (off by default): the
