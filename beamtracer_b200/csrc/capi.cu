@@ -1,5 +1,6 @@
 // The context, error reporting and device scratch of the C ABI, and the field gather
 // (kernels/staggered_field_2d/staggered_field_2d_pyccel.py:13-55).
+#include <map>
 #include <mutex>
 
 #include "common.cuh"
@@ -12,25 +13,86 @@ thread_local std::string g_last_error;
 
 void set_error(const std::string &message) { g_last_error = message; }
 
+namespace {
+
+constexpr size_t kPoolMaxBytes = (size_t)8 << 30;
+
+struct Pool {
+    std::mutex mu;
+    std::multimap<std::pair<int, size_t>, void *> blocks;  // (device, bytes) -> block
+    size_t cached = 0;
+};
+
+Pool &pool() {
+    static Pool p;
+    return p;
+}
+
+}  // namespace
+
+// A cached block on the current device of at least `need` bytes and at most twice that
+// (plus 1 MB), else a new one.
+void *pool_take(size_t need, size_t *got, int *device_out) {
+    int device = 0;
+    cudaGetDevice(&device);
+    *device_out = device;
+    {
+        Pool &p = pool();
+        std::lock_guard<std::mutex> lock(p.mu);
+        auto it = p.blocks.lower_bound({device, need});
+        if (it != p.blocks.end() && it->first.first == device &&
+            it->first.second <= 2 * need + ((size_t)1 << 20)) {
+            void *ptr = it->second;
+            *got = it->first.second;
+            p.cached -= it->first.second;
+            p.blocks.erase(it);
+            return ptr;
+        }
+    }
+    void *ptr = nullptr;
+    cudaError_t e = cudaMalloc(&ptr, need);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw Error{BT_ERR_ALLOC, std::string("cudaMalloc of ") + std::to_string(need) +
+                                      " bytes: " + cudaGetErrorString(e)};
+    }
+    *got = need;
+    return ptr;
+}
+
+void pool_give(void *ptr, size_t bytes, int device) {
+    if (!ptr) return;
+    {
+        Pool &p = pool();
+        std::lock_guard<std::mutex> lock(p.mu);
+        if (p.cached + bytes <= kPoolMaxBytes) {
+            p.blocks.insert({{device, bytes}, ptr});
+            p.cached += bytes;
+            return;
+        }
+    }
+    int current = 0;
+    cudaGetDevice(&current);
+    cudaSetDevice(device);
+    cudaFree(ptr);
+    cudaSetDevice(current);
+}
+
 void *Buffer::get(size_t need) {
     if (need == 0) need = 1;
     if (need <= bytes) return ptr;
-    release();
-    size_t grown = need + need / 4;
-    cudaError_t e = cudaMalloc(&ptr, grown);
-    if (e != cudaSuccess) {
-        ptr = nullptr;
-        bytes = 0;
-        (void)cudaGetLastError();
-        throw Error{BT_ERR_ALLOC, std::string("cudaMalloc of ") + std::to_string(grown) +
-                                      " bytes: " + cudaGetErrorString(e)};
-    }
-    bytes = grown;
+    // the old block may still be read by queued work: free it the waiting way
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    size_t got = 0;
+    ptr = pool_take(need + need / 4, &got, &device);
+    bytes = got;
     return ptr;
 }
 
 void Buffer::release() {
-    if (ptr) cudaFree(ptr);
+    pool_give(ptr, bytes, device);
     ptr = nullptr;
     bytes = 0;
 }

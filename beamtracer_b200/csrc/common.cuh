@@ -52,13 +52,23 @@ struct Error {
 
 // A growable device buffer owned by a context (grown with cudaMalloc, never shrunk).
 // Move-only: a copy would free the same memory twice.
+// Device memory of a context or solver.  Growing a buffer frees its old block at once
+// (cudaFree waits for the work that may still use it); a destroyed buffer's block goes to a
+// per-device cache that later buffers draw from, since its owners (a solver, a context)
+// synchronise their stream before they destroy their buffers.  The cache keeps at most
+// kPoolMaxBytes; cudaMalloc and cudaFree stay off the path of a solver made and dropped
+// per call.
+void *pool_take(size_t need, size_t *got, int *device);
+void pool_give(void *ptr, size_t bytes, int device);
+
 struct Buffer {
     void *ptr = nullptr;
     size_t bytes = 0;
+    int device = 0;  // where the block lives
     Buffer() = default;
     Buffer(const Buffer &) = delete;
     Buffer &operator=(const Buffer &) = delete;
-    Buffer(Buffer &&o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+    Buffer(Buffer &&o) noexcept : ptr(o.ptr), bytes(o.bytes), device(o.device) {
         o.ptr = nullptr;
         o.bytes = 0;
     }
@@ -67,6 +77,7 @@ struct Buffer {
             release();
             ptr = o.ptr;
             bytes = o.bytes;
+            device = o.device;
             o.ptr = nullptr;
             o.bytes = 0;
         }
