@@ -1306,8 +1306,9 @@ void setup_tail(bt_poisson *p) {
         if (l + 1 < levels) t.next = fine_of(L, p->levels[l + 1], false);
         tail.push_back(t);
     }
+    // the largest any solver asks for: solvers of other meshes may launch concurrently
     BT_CUDA(cudaFuncSetAttribute(vcycle_tail, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)p->tail_smem));
+                                 (int)kTailSmemMax));
     BT_CUDA(cudaMemcpy(p->tail_levels.as<TailLevel>(tail.size()), tail.data(),
                        sizeof(TailLevel) * tail.size(), cudaMemcpyHostToDevice));
     BT_CUDA(cudaMemcpy(p->tail_plans.as<TailPlan>(T.plan.size()), T.plan.data(),

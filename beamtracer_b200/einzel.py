@@ -171,11 +171,38 @@ def evaluate_design(design: EinzelDesign, plane: float = 79e-3, **settings) -> d
             "iterations": len(model.state.history), "converged": model.stats["converged"]}  # fmt: skip
 
 
-def sweep(designs: list[EinzelDesign], rank: int = 0, world: int = 1, **settings) -> dict[int, dict]:
-    """This rank's share of the candidates (`share_of_designs`), each solved in turn:
-    ``{candidate index: evaluate_design(...)}``.  Ranks need no collective; a caller that
-    wants every result gathers the dictionaries."""
-    return {k: evaluate_design(designs[k], **settings) for k in share_of_designs(designs, rank, world)}
+def sweep(designs: list[EinzelDesign], rank: int = 0, world: int = 1, concurrency: int = 1,
+          **settings) -> dict[int, dict]:  # fmt: skip
+    """This rank's share of the candidates (`share_of_designs`):
+    ``{candidate index: evaluate_design(...)}``.  With ``concurrency`` > 1 that many host
+    threads solve candidates at once, each on its own CUDA stream and library context, so
+    one candidate's trace overlaps another's field solve on the same GPU; every solve is
+    deterministic, so the results do not depend on it.  Ranks need no collective; a caller
+    that wants every result gathers the dictionaries."""
+    mine = share_of_designs(designs, rank, world)
+    if concurrency <= 1:
+        return {k: evaluate_design(designs[k], **settings) for k in mine}
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    device = torch.cuda.current_device()
+    local = threading.local()
+
+    def solve(k: int) -> tuple[int, dict]:
+        torch.cuda.set_device(device)
+        if getattr(local, "stream", None) is None:
+            local.stream = torch.cuda.Stream()
+        with torch.cuda.stream(local.stream):
+            result = evaluate_design(designs[k], **settings)
+        local.stream.synchronize()
+        return k, result
+
+    # the costliest first, so the threads finish together
+    order = sorted(mine, key=lambda k: -design_cost(designs[k]))
+    with ThreadPoolExecutor(max_workers=concurrency) as pool:
+        return dict(sorted(pool.map(solve, order)))
 
 
 # -- design gradients (central differences through the solver) --------------------------------

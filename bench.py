@@ -322,11 +322,12 @@ def run_design(args, rank: int, world: int, local: int) -> None:
         designs = sweep_designs(args.sweep_count)
 
         def step():
-            return sweep(designs, rank, world)
+            return sweep(designs, rank, world, concurrency=args.concurrency)
 
         units_per_step, unit = args.sweep_count, "candidates/s"
         metric = "einzel design-sweep candidates/s (257x65..1025x257, 2k-20k rings)"
-        workload = f"{args.sweep_count} seeded einzel candidates (seed 5), cost-balanced shares"
+        workload = (f"{args.sweep_count} seeded einzel candidates (seed 5), cost-balanced "
+                    f"shares, {args.concurrency} solved at once per GPU on their own streams")
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -383,6 +384,8 @@ def main() -> None:
                              "gradient: einzel design gradients; sweep: the design sweep")
     parser.add_argument("--sweep-count", type=int, default=32,
                         help="with --workload sweep: the candidates of one step")
+    parser.add_argument("--concurrency", type=int, default=8,
+                        help="with --workload sweep: candidates solved at once per GPU")
     args = parser.parse_args()
     if args.profile:
         run_profile(args)

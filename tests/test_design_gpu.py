@@ -78,3 +78,13 @@ def test_sweep_candidates_solve():
     small = EinzelDesign(**{**design.__dict__, "shape": (129, 33), "trajectories": 300})
     result = evaluate_design(small)
     assert np.isfinite(result["rms_angle"])
+
+
+def test_concurrent_sweep_equals_the_sequential_one():
+    """Three candidates solved at once on three streams give the sequential results bit
+    for bit (every solve is deterministic and keeps to its own stream)."""
+    designs = [EinzelDesign(shape=((129, 33), (257, 65))[k % 2], trajectories=300 + 100 * k,
+                            seed=20 + k, voltages=(0.0, 3e3 + 1e3 * k, 0.0)) for k in range(5)]  # fmt: skip
+    sequential = sweep(designs)
+    concurrent = sweep(designs, concurrency=3)
+    assert concurrent == sequential
