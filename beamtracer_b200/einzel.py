@@ -219,22 +219,53 @@ def _perturbed(design: EinzelDesign, parameter: str, delta: float) -> EinzelDesi
     return replace(design, voltages=tuple(voltages))
 
 
+def _evaluate_all(designs: list[EinzelDesign], plane: float, concurrency: int,
+                  **settings) -> list[dict]:  # fmt: skip
+    """`evaluate_design` of every design, ``concurrency`` at once on their own streams."""
+    if concurrency <= 1:
+        return [evaluate_design(d, plane, **settings) for d in designs]
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    device = torch.cuda.current_device()
+    local = threading.local()
+
+    def solve(design: EinzelDesign) -> dict:
+        torch.cuda.set_device(device)
+        if getattr(local, "stream", None) is None:
+            local.stream = torch.cuda.Stream()
+        with torch.cuda.stream(local.stream):
+            result = evaluate_design(design, plane, **settings)
+        local.stream.synchronize()
+        return result
+
+    with ThreadPoolExecutor(max_workers=concurrency) as pool:
+        return list(pool.map(solve, designs))
+
+
 def design_gradient(design: EinzelDesign, plane: float = 79e-3, rel_step: float = 1e-4,
-                    tolerance: float = 1e-7, iterations: int = 60) -> dict:  # fmt: skip
+                    tolerance: float = 1e-7, iterations: int = 60,
+                    concurrency: int = 1) -> dict:  # fmt: skip
     """The gradients of the rms angle and the current at ``plane`` with respect to
     `GRADIENT_PARAMETERS`, by central differences of converged solves: voltage steps of
     ``rel_step`` times the largest plate voltage, a current step of ``rel_step`` times the
-    current; every solve converged to ``tolerance`` [V] (tighter than the steps' effect)."""
+    current; every solve converged to ``tolerance`` [V] (tighter than the steps' effect).
+    The 2 x 4 solves are independent: ``concurrency`` of them run at once, each on its own
+    stream (the results do not depend on it)."""
     scale = max(abs(v) for v in resolved_voltages(design))
+    steps = [rel_step * (design.current if name == "current" else scale)
+             for name in GRADIENT_PARAMETERS]  # fmt: skip
+    designs = []
+    for name, step in zip(GRADIENT_PARAMETERS, steps, strict=True):
+        designs += [_perturbed(design, name, step), _perturbed(design, name, -step)]
+    results = _evaluate_all(designs, plane, concurrency, tolerance=tolerance,
+                            iterations=iterations)  # fmt: skip
     out = {"rms_angle": np.zeros(len(GRADIENT_PARAMETERS)),
-           "current": np.zeros(len(GRADIENT_PARAMETERS)), "solves": 0}  # fmt: skip
-    for k, name in enumerate(GRADIENT_PARAMETERS):
-        step = rel_step * (design.current if name == "current" else scale)
-        plus = evaluate_design(_perturbed(design, name, step), plane, tolerance=tolerance,
-                               iterations=iterations)  # fmt: skip
-        minus = evaluate_design(_perturbed(design, name, -step), plane, tolerance=tolerance,
-                                iterations=iterations)  # fmt: skip
+           "current": np.zeros(len(GRADIENT_PARAMETERS)), "solves": len(designs)}  # fmt: skip
+    for k, step in enumerate(steps):
+        plus, minus = results[2 * k], results[2 * k + 1]
         out["rms_angle"][k] = (plus["rms_angle"] - minus["rms_angle"]) / (2.0 * step)
         out["current"][k] = (plus["current"] - minus["current"]) / (2.0 * step)
-        out["solves"] += 2
     return out

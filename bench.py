@@ -313,11 +313,12 @@ def run_design(args, rank: int, world: int, local: int) -> None:
         design = EinzelDesign(shape=(401, 101), trajectories=8000, seed=2 + rank)
 
         def step():
-            return design_gradient(design)
+            return design_gradient(design, concurrency=args.concurrency)
 
         units_per_step, unit = world, "gradient evals/s"
         metric = "einzel design-gradient evals/s (401x101 cyl., 8k rings, 4 parameters)"
-        workload = "einzel lens 401x101, 8,000 rings: d(rms angle, current)/d(V1, V2, V3, J)"
+        workload = ("einzel lens 401x101, 8,000 rings: d(rms angle, current)/d(V1, V2, V3, J), "
+                    f"central differences, {args.concurrency} solves at once on their own streams")
     else:
         designs = sweep_designs(args.sweep_count)
 
@@ -385,7 +386,7 @@ def main() -> None:
     parser.add_argument("--sweep-count", type=int, default=32,
                         help="with --workload sweep: the candidates of one step")
     parser.add_argument("--concurrency", type=int, default=8,
-                        help="with --workload sweep: candidates solved at once per GPU")
+                        help="with --workload sweep or gradient: solves at once per GPU")
     args = parser.parse_args()
     if args.profile:
         run_profile(args)

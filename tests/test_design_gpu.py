@@ -61,6 +61,10 @@ def test_gradient_matches_the_oracle_central_differences():
         assert gpu["rms_angle"][k] == pytest.approx(angle, rel=1e-5, abs=1e-12), name
         assert gpu["current"][k] == pytest.approx(current, rel=1e-5, abs=1e-12), name
     assert np.all(np.isfinite(gpu["rms_angle"])) and gpu["rms_angle"][1] != 0.0
+    concurrent = design_gradient(SMALL, plane, rel_step=rel, tolerance=tol, iterations=its,
+                                 concurrency=8)  # fmt: skip
+    np.testing.assert_array_equal(concurrent["rms_angle"], gpu["rms_angle"])
+    np.testing.assert_array_equal(concurrent["current"], gpu["current"])
 
 
 def test_sweep_solves_this_ranks_share():
