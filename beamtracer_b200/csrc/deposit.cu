@@ -19,23 +19,25 @@ namespace {
 constexpr int kThreads = 256;  // = the radix (one thread per digit in the scans)
 constexpr int kItems = 16;
 constexpr int kTile = kThreads * kItems;
-constexpr int kRadix = 256;
+constexpr int kRadix = 256;     // 8-bit digits
+constexpr int kRadixMax = 512;  // 9-bit digits, when they save a pass
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned kFull = 0xffffffffu;
 
+template <int R>
 __global__ void radix_hist(const uint32_t *__restrict__ keys, i64 n, int shift,
                            uint32_t *__restrict__ hist, int nblocks) {
-    __shared__ uint32_t h[kRadix];
-    h[threadIdx.x] = 0;
+    __shared__ uint32_t h[R];
+    for (int d = threadIdx.x; d < R; d += kThreads) h[d] = 0;
     __syncthreads();
     const i64 base = (i64)blockIdx.x * kTile;
 #pragma unroll 4
     for (int i = 0; i < kItems; ++i) {
         const i64 r = base + (i64)i * kThreads + threadIdx.x;
-        if (r < n) atomicAdd(&h[(keys[r] >> shift) & (kRadix - 1)], 1u);
+        if (r < n) atomicAdd(&h[(keys[r] >> shift) & (R - 1)], 1u);
     }
     __syncthreads();
-    hist[(i64)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+    for (int d = threadIdx.x; d < R; d += kThreads) hist[(i64)d * nblocks + blockIdx.x] = h[d];
 }
 
 // Inclusive scan of one value per thread over a block of kThreads threads.
@@ -84,27 +86,43 @@ __global__ void radix_row_scan(const uint32_t *__restrict__ hist, uint32_t *__re
     if (threadIdx.x == 0) totals[blockIdx.x] = carry;
 }
 
+// Exclusive prefix of the R digit totals; thread t scans digits t * R / kThreads onwards.
+template <int R>
 __global__ void radix_digit_base(const uint32_t *__restrict__ totals, uint32_t *__restrict__ base) {
     __shared__ uint32_t warp_sums[kWarps];
-    const uint32_t v = totals[threadIdx.x];
-    const uint32_t incl = block_inclusive_scan(v, warp_sums);
-    base[threadIdx.x] = incl - v;
+    constexpr int D = R / kThreads;
+    uint32_t mine[D];
+    uint32_t v = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        mine[k] = totals[threadIdx.x * D + k];
+        v += mine[k];
+    }
+    uint32_t run = block_inclusive_scan(v, warp_sums) - v;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        base[threadIdx.x * D + k] = run;
+        run += mine[k];
+    }
 }
 
 // Stable scatter of one tile: items in the order i * kThreads + t keep their order among
 // equal digits (warp ranks by __match_any_sync, warps in order by a per-digit prefix).
+template <int R>
 __global__ void radix_scatter(const uint32_t *__restrict__ keys_in,
                               const uint32_t *__restrict__ vals_in, i64 n, int shift,
                               const uint32_t *__restrict__ offs,
                               const uint32_t *__restrict__ base, int nblocks,
                               uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out) {
-    __shared__ uint32_t wcount[kWarps][kRadix];
-    __shared__ uint32_t woff[kWarps][kRadix];
-    __shared__ uint32_t run[kRadix];
+    __shared__ uint32_t wcount[kWarps][R];
+    __shared__ uint32_t woff[kWarps][R];
+    __shared__ uint32_t run[R];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (int d = t; d < R; d += kThreads) {
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) wcount[w][t] = 0;
-    run[t] = base[t] + offs[(i64)t * nblocks + blockIdx.x];
+        for (int w = 0; w < kWarps; ++w) wcount[w][d] = 0;
+        run[d] = base[d] + offs[(i64)d * nblocks + blockIdx.x];
+    }
     __syncthreads();
     const i64 tile = (i64)blockIdx.x * kTile;
     const unsigned below = (1u << lane) - 1u;
@@ -112,21 +130,23 @@ __global__ void radix_scatter(const uint32_t *__restrict__ keys_in,
         const i64 r = tile + (i64)i * kThreads + t;
         const bool valid = r < n;
         const uint32_t key = valid ? keys_in[r] : 0u;
-        const uint32_t d = (key >> shift) & (kRadix - 1);
+        const uint32_t d = (key >> shift) & (R - 1);
         const uint32_t val = valid ? (vals_in ? vals_in[r] : (uint32_t)r) : 0u;
         const unsigned peers = __match_any_sync(kFull, valid ? d : 0xffffffffu);
         const int rank = __popc(peers & below);
         if (valid && rank == 0) wcount[warp][d] = __popc(peers);
         __syncthreads();
-        uint32_t acc = run[t];
+        for (int dd = t; dd < R; dd += kThreads) {
+            uint32_t acc = run[dd];
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const uint32_t c = wcount[w][t];
-            woff[w][t] = acc;
-            acc += c;
-            wcount[w][t] = 0;
+            for (int w = 0; w < kWarps; ++w) {
+                const uint32_t c = wcount[w][dd];
+                woff[w][dd] = acc;
+                acc += c;
+                wcount[w][dd] = 0;
+            }
+            run[dd] = acc;
         }
-        run[t] = acc;
         __syncthreads();
         if (valid) {
             const uint32_t pos = woff[warp][d] + (uint32_t)rank;
@@ -310,22 +330,34 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, int key_bits,
     const int nblocks = (int)((n + kTile - 1) / kTile);
     uint32_t *ka = s.keys_alt.as<uint32_t>(n), *va = s.vals.as<uint32_t>(n);
     uint32_t *kb = s.keys.as<uint32_t>(n), *vb = s.vals_alt.as<uint32_t>(n);
-    uint32_t *hist = s.hist.as<uint32_t>((size_t)kRadix * nblocks);
-    uint32_t *offs = s.row_offsets.as<uint32_t>((size_t)kRadix * nblocks);
-    uint32_t *digit = s.digit_base.as<uint32_t>(2 * kRadix);
-    uint32_t *totals = digit + kRadix;
+    uint32_t *hist = s.hist.as<uint32_t>((size_t)kRadixMax * nblocks);
+    uint32_t *offs = s.row_offsets.as<uint32_t>((size_t)kRadixMax * nblocks);
+    uint32_t *digit = s.digit_base.as<uint32_t>(2 * kRadixMax);
+    uint32_t *totals = digit + kRadixMax;
     const uint32_t *src_k = keys_in;
     const uint32_t *src_v = nullptr;
     uint32_t *dst_k = ka, *dst_v = va;
     BT_REQUIRE(n > 0 && key_bits > 0, "radix sort: nothing to sort");
-    const int passes = (key_bits + 7) / 8;
+    // 9-bit digits where they need fewer passes than 8-bit ones (17-18, 25-27 bits)
+    const int bits = (key_bits + 8) / 9 < (key_bits + 7) / 8 ? 9 : 8;
+    const int passes = (key_bits + bits - 1) / bits;
     for (int p = 0; p < passes; ++p) {
-        const int shift = 8 * p;
-        BT_LAUNCH(ctx, radix_hist, nblocks, kThreads, 0, st, src_k, n, shift, hist, nblocks);
-        BT_LAUNCH(ctx, radix_row_scan, kRadix, kThreads, 0, st, hist, offs, totals, nblocks);
-        BT_LAUNCH(ctx, radix_digit_base, 1, kThreads, 0, st, totals, digit);
-        BT_LAUNCH(ctx, radix_scatter, nblocks, kThreads, 0, st, src_k, src_v, n, shift, offs, digit,
-                                                    nblocks, dst_k, dst_v);
+        const int shift = bits * p;
+        if (bits == 9) {
+            BT_LAUNCH(ctx, radix_hist<kRadixMax>, nblocks, kThreads, 0, st, src_k, n, shift, hist,
+                      nblocks);
+            BT_LAUNCH(ctx, radix_row_scan, kRadixMax, kThreads, 0, st, hist, offs, totals, nblocks);
+            BT_LAUNCH(ctx, radix_digit_base<kRadixMax>, 1, kThreads, 0, st, totals, digit);
+            BT_LAUNCH(ctx, radix_scatter<kRadixMax>, nblocks, kThreads, 0, st, src_k, src_v, n,
+                      shift, offs, digit, nblocks, dst_k, dst_v);
+        } else {
+            BT_LAUNCH(ctx, radix_hist<kRadix>, nblocks, kThreads, 0, st, src_k, n, shift, hist,
+                      nblocks);
+            BT_LAUNCH(ctx, radix_row_scan, kRadix, kThreads, 0, st, hist, offs, totals, nblocks);
+            BT_LAUNCH(ctx, radix_digit_base<kRadix>, 1, kThreads, 0, st, totals, digit);
+            BT_LAUNCH(ctx, radix_scatter<kRadix>, nblocks, kThreads, 0, st, src_k, src_v, n, shift,
+                      offs, digit, nblocks, dst_k, dst_v);
+        }
         BT_CHECK_LAUNCH();
         src_k = dst_k;
         src_v = dst_v;
@@ -485,10 +517,10 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
         uint32_t *dst_k = keys_alt, *dst_v = vals;
         for (int pass = 0; pass < passes; ++pass) {
             const int shift = 8 * pass;
-            radix_hist<<<nblocks, kThreads, 0, st>>>(src_k, n, shift, hist, nblocks);
+            radix_hist<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, n, shift, hist, nblocks);
             radix_row_scan<<<kRadix, kThreads, 0, st>>>(hist, offs, totals, nblocks);
-            radix_digit_base<<<1, kThreads, 0, st>>>(totals, digit);
-            radix_scatter<<<nblocks, kThreads, 0, st>>>(src_k, src_v, n, shift, offs, digit,
+            radix_digit_base<kRadix><<<1, kThreads, 0, st>>>(totals, digit);
+            radix_scatter<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, src_v, n, shift, offs, digit,
                                                         nblocks, dst_k, dst_v);
             src_k = dst_k;
             src_v = dst_v;
