@@ -311,6 +311,17 @@ class ParticleBeam:
         object.__setattr__(self, "position", tuple(map(tuple, position)))
         object.__setattr__(self, "velocity", tuple(map(tuple, velocity)))
         object.__setattr__(self, "current", tuple(current))
+        # the arrays the tuples were made from, so a model reads them without rebuilding
+        object.__setattr__(self, "_arrays", (position, velocity, current))
+
+    def arrays(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Positions and velocities (N, 3) and currents (N,) as float arrays."""
+        arrays = getattr(self, "_arrays", None)
+        if arrays is None or len(arrays[2]) != len(self.current):
+            arrays = (np.asarray(self.position, dtype=float).reshape(-1, 3),
+                      np.asarray(self.velocity, dtype=float).reshape(-1, 3),
+                      np.asarray(self.current, dtype=float).ravel())  # fmt: skip
+        return arrays
 
     def __len__(self) -> int:
         return len(self.current)

@@ -152,12 +152,13 @@ class BeamOptics:
                 j_over_v += jv
             else:
                 n = len(beam)
+                position, velocity, current = beam.arrays()
                 particles = BeamParticles(
-                    position=np.ascontiguousarray(np.asarray(beam.position, float).reshape(n, 3).T),
-                    velocity=np.ascontiguousarray(np.asarray(beam.velocity, float).reshape(n, 3).T),
+                    position=np.ascontiguousarray(position.T),
+                    velocity=np.ascontiguousarray(velocity.T),
                     charge=np.full(n, beam.charge * constants.e),
                     mass=np.full(n, beam.mass * constants.atomic_mass),
-                    current=np.asarray(beam.current, dtype=float),
+                    current=np.array(current, dtype=float),
                     species=np.full(n, number, dtype=np.int32),
                 )
             parts.append(particles)
