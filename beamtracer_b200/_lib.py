@@ -104,6 +104,7 @@ SIGNATURES: dict[str, list] = {
     "bt_staggered_field_2d": [P, P, P, I64, P, P, I64, I64, F64, F64, F64, P, P],
     "bt_deposit_trajectories_2d": [P, P, P, P, I64, F64, F64, F64, I64, P, I64, I64],
     "bt_deposit_trajectories_2d_noalloc": [P, P, P, P, I64, F64, F64, F64, I64, P, I64, I64],
+    "bt_classify_mesh": [P, ctypes.POINTER(ShapesDesc), I64, I64, P, P, F64, F64, P, P, P],
     "bt_subcell_table": [P, ctypes.POINTER(ShapesDesc), P, P, I64, F64, F64, F64, P, I64, I64,
                          P],
     "bt_trace_trajectories_2d_magnetic": [P, ctypes.POINTER(TraceArgs),

@@ -262,11 +262,48 @@ class IonOpticsMesh:
         code = np.where(code == 0, 1, code)
         return code / 255.0
 
+    def _classify_on_device(self):
+        """``(solid, near, distance)`` sampled on the device (``bt_classify_mesh``) when a
+        CUDA device is present and every electrode is a configuration shape; else None."""
+        if not self.electrodes:
+            return None
+        try:
+            import torch
+        except ImportError:  # pragma: no cover
+            return None
+        if not torch.cuda.is_available():
+            return None
+        from beamtracer_b200.shapes import shape_table
+
+        table = shape_table(self)
+        if table is None:
+            return None
+        import ctypes
+
+        from beamtracer_b200 import _lib
+
+        nx, ny = self.shape
+        kinds, offsets, params = (torch.from_numpy(a).cuda() for a in table)
+        x = torch.from_numpy(np.array(self.x, dtype=np.float64)).cuda()
+        dx = torch.from_numpy(np.array(self.dx, dtype=np.float64)).cuda()
+        solid = torch.empty((nx, ny), dtype=torch.int32, device="cuda")
+        near = torch.empty((nx, ny), dtype=torch.uint8, device="cuda")
+        distance = torch.empty((4, nx, ny), dtype=torch.float64, device="cuda")
+        shapes = _lib.ShapesDesc(len(table[0]), _lib.dptr(kinds), _lib.dptr(offsets),
+                                 _lib.dptr(params))  # fmt: skip
+        ctx = _lib.context()
+        _lib.check(_lib.lib().bt_classify_mesh(
+            ctx.handle, ctypes.byref(shapes), nx, ny, _lib.dptr(x), _lib.dptr(dx),
+            float(self.origin[1]), float(self.h), _lib.dptr(solid), _lib.dptr(near),
+            _lib.dptr(distance)))  # fmt: skip
+        return solid.cpu().numpy(), near.cpu().numpy().astype(bool), distance.cpu().numpy()
+
     def _classify(self) -> None:
         nx, ny = self.shape
         xn, yn = self.nodes()
+        device = self._classify_on_device()
         #: The electrode index of every node (-1: none).
-        self.solid = self.inside_solid(xn, yn)
+        self.solid = self.inside_solid(xn, yn) if device is None else device[0]
         solid = self.solid >= 0
         potentials = np.array([e.potential for e in self.electrodes] + [0.0])
         fixed = solid.copy()
@@ -289,6 +326,9 @@ class IonOpticsMesh:
         self.fixed = fixed
         #: Their potential (0 elsewhere).
         self.fixed_value = value
+        if device is not None:
+            self.near_solid, self.distance = device[1], device[2]
+            return
         #: The fraction of the edge to the surface along -x, +x, -y, +y (1: no surface).
         self.distance = np.ones((4, nx, ny))
         #: Free nodes with an electrode neighbour.

@@ -197,6 +197,16 @@ int bt_subcell_table(bt_ctx *ctx, const bt_shapes *shapes, const int64_t *ci,
                      double h, const double *x_nodes, int64_t n_x_nodes, int64_t refine,
                      int64_t *out);
 
+/* solver/mesh.py:127-201 (IonOpticsMesh._classify, _bracket): solid (nx, ny) int32, the
+ * first electrode holding each node or -1; near (nx, ny) uint8, a free node with an
+ * electrode neighbour; distance (4, nx, ny), towards -x, +x, -y, +y, the surface's place on
+ * the edge to an electrode neighbour by eight bisections of that electrode's inside test
+ * in 1/255 (1 without one).  x (nx,) the node positions, dx (nx - 1,) the edge lengths, the
+ * nodes' y = origin_y + h j. */
+int bt_classify_mesh(bt_ctx *ctx, const bt_shapes *shapes, int64_t nx, int64_t ny,
+                     const double *x, const double *dx, double origin_y, double h,
+                     int32_t *solid, uint8_t *near, double *distance);
+
 /* -- the edge field (device pointers) --------------------------------------------------- */
 
 /* solver/fields.py:18-67 and 116-152: the staggered edge fields of a potential.

@@ -59,3 +59,26 @@ def test_arbitrary_inside_functions_stay_on_the_host():
     cells, subcells = electrode_lookup(mesh)
     cells_d, subcells_d = electrode_lookup_device(mesh)
     np.testing.assert_array_equal(subcells_d.cpu().numpy(), subcells)
+
+
+@pytest.mark.parametrize("geometry", ["planar", "cylindrical"])
+@pytest.mark.parametrize("graded", [False, True])
+def test_device_classification_equals_the_host(geometry, graded):
+    """The mesh's solid, near-solid, bracketed distances, held nodes and values sampled on
+    the device equal the host's (the same electrodes given as plain inside functions,
+    which only the host can call)."""
+    shape, h = (81, 21), 0.25e-3
+    nodes = None
+    if graded:
+        s = np.linspace(0.0, 1.0, shape[0])
+        nodes = 20e-3 * (0.3 * s + 0.7 * s * s)
+    objs = _objects()
+    device = IonOpticsMesh(shape=shape, origin=(0.0, 0.0), h=h, geometry=geometry, x_nodes=nodes,
+                           electrodes=[Electrode(o.inside, o.bc_value) for o in objs])  # fmt: skip
+    host = IonOpticsMesh(shape=shape, origin=(0.0, 0.0), h=h, geometry=geometry, x_nodes=nodes,
+                         electrodes=[Electrode(lambda x, y, o=o: o.inside(x, y), o.bc_value)
+                                     for o in objs])  # fmt: skip
+    assert shape_table(device) is not None and shape_table(host) is None
+    for name in ("solid", "near_solid", "distance", "fixed", "fixed_value"):
+        np.testing.assert_array_equal(getattr(device, name), getattr(host, name), err_msg=name)
+    assert host.near_solid.any() and (host.distance < 1).any()
