@@ -275,6 +275,13 @@ int bt_ctx_destroy(bt_ctx *ctx) {
                 cudaEventDestroy(e.second);
             }
         }
+        bt::TraceScratch &ts = ctx->trace;
+        if (ts.side) cudaStreamSynchronize(ts.side);
+        for (int b = 0; b < 2; ++b) {
+            if (ts.filled[b]) cudaEventDestroy(ts.filled[b]);
+            if (ts.drained[b]) cudaEventDestroy(ts.drained[b]);
+        }
+        if (ts.side) cudaStreamDestroy(ts.side);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         delete ctx;
     });

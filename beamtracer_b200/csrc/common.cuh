@@ -112,9 +112,14 @@ struct DepositScratch {
 };
 
 // The tracer's live-trajectory lists and its deposit records.
+// The tracer's scratch: the live lists and two record buffers, one filled by the trace
+// windows while the other's records are deposited on the side stream.
 struct TraceScratch {
     Buffer active_a, active_b, block_counts, n_alive;
-    Buffer rec_keys, rec_u, rec_w, rec_q;
+    Buffer rec_keys[2], rec_u[2], rec_w[2], rec_q[2];
+    cudaStream_t side = nullptr;                 // the deposits' stream
+    cudaEvent_t filled[2] = {nullptr, nullptr};  // a buffer's windows are traced
+    cudaEvent_t drained[2] = {nullptr, nullptr}; // a buffer's records are deposited
 };
 
 }  // namespace bt
@@ -179,6 +184,31 @@ inline unsigned blocks_for(i64 n, int threads) {
 
 // The radius sqrt(y^2 + z^2), formed by that expression (the oracle forms it the same way).
 __device__ __forceinline__ double radius(double y, double z) { return sqrt(y * y + z * z); }
+
+// The reciprocal that `div_known` divides by b with: 1 / b rounded to nearest, or 0 (plain
+// division) for a b outside [2^-60, 2^60] or not a number.
+__host__ __device__ __forceinline__ double known_reciprocal(double b) {
+    return (b >= 0x1p-60 && b <= 0x1p60) ? 1.0 / b : 0.0;
+}
+
+// a / b rounded to nearest, as the IEEE division, for a divisor whose reciprocal
+// rb = known_reciprocal(b) is known in advance: the quotient a rb and two corrections by the
+// exact remainder.  Markstein's theorem (P. W. Markstein, IBM J. Res. Develop. 34(1), 1990):
+// if rb is within half an ulp of 1/b and q within one ulp of a/b, the remainder a - b q is
+// exact and q + (a - b q) rb rounds to a/b rounded to nearest.  a rb is within 1.5 ulp of
+// a/b, its correction within one, the second correction the rounded quotient.  The
+// remainders stay normal and the quotients finite for 2^-900 <= |a| <= 2^900 and
+// 2^-60 <= b <= 2^60; any other a (zero, subnormal, huge, infinite, NaN) or b takes the
+// IEEE division, so the result is a / b for every a and b.
+__device__ __forceinline__ double div_known(double a, double b, double rb) {
+    const double m = fabs(a);
+    if (rb == 0.0 || !(m >= 0x1p-900 && m <= 0x1p900)) return a / b;
+    double q = a * rb;
+    double r = fma(-q, b, a);
+    q = fma(r, rb, q);
+    r = fma(-q, b, a);
+    return fma(r, rb, q);
+}
 
 // The Lorentz factor sqrt(1 + |u|^2 / c^2) of a proper velocity u (1 for inv_c2 = 0).
 __device__ __forceinline__ double lorentz(double u0, double u1, double u2, double inv_c2) {

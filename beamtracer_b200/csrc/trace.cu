@@ -4,13 +4,16 @@
 // One thread per live trajectory advances it by at most `window` steps per launch (RK4 or
 // Boris's kick-drift-kick through the staggered edge fields of the patches, plane
 // crossings, kept paths, exit and electrode sub-cell tests: the reference's step, term by
-// term, in FP64 with no fused multiply-add, so a trajectory ends bit for bit where the
-// reference's CPU kernel ends it).  Instead of adding its charge to the mesh with atomics,
-// every step writes one deposit record (cell, u, w, dq dt) to a slot fixed by (window,
-// step, trajectory); between windows the live trajectories are compacted in order, and the
-// records are sorted by cell and reduced per cell in record order (deposit.cu), so the
-// node charges are deterministic.  Short windows bound the tail of a warp (its threads
-// wait only for the longest trajectory of the window, not of the whole trace).
+// term, in FP64 with no contracted multiply-add, so a trajectory ends bit for bit where the
+// reference's CPU kernel ends it; the only fused multiply-adds are those of `div_known`,
+// whose quotients are the IEEE division's).  Instead of adding its charge to the mesh with
+// atomics, every step writes one deposit record (cell, u, w, dq dt) to a slot fixed by
+// (window, step, trajectory); between windows the live trajectories are compacted in order,
+// and the records are sorted by cell and reduced per cell in record order (deposit.cu), so
+// the node charges are deterministic.  The deposits run on a side stream under the next
+// windows, in the order the record buffers were filled.  Short windows bound the tail of a
+// warp (its threads wait only for the longest trajectory of the window, not of the whole
+// trace).
 #include <algorithm>
 
 #include "common.cuh"
@@ -58,59 +61,49 @@ __device__ __forceinline__ i64 finest_patch(const bt_trace_args &a, i64 P, doubl
 }
 
 // A patch's shape: node counts, its offsets into the edge-field and node arrays, origin and
-// spacing (one row of patch_int / patch_real).
+// spacing (one row of patch_int / patch_real), and the spacing's reciprocal for `div_known`
+// (0: divide plainly).
 struct PatchGeom {
     i64 pnx, pny, ofx, ofy, ofn;
-    double pox, poy, phh;
+    double pox, poy, phh, rphh;
 };
 
 __device__ __forceinline__ PatchGeom patch_geom(const bt_trace_args &a, i64 pp) {
     const i64 *pi = a.patch_int + pp * 6;
     const double *pr = a.patch_real + pp * 7;
     return {__ldg(pi + 0), __ldg(pi + 1), __ldg(pi + 2), __ldg(pi + 3), __ldg(pi + 5),
-            __ldg(pr + 0), __ldg(pr + 1), __ldg(pr + 2)};
+            __ldg(pr + 0), __ldg(pr + 1), __ldg(pr + 2), 0.0};
 }
+
+// Cell indices are 32-bit: a patch has fewer than 2^31 nodes along an axis (the deposit keys
+// are 32-bit).  floor and truncation saturate outside that range, where the clamps that
+// follow them give what the 64-bit conversions give.
+__device__ __forceinline__ int clamp_index(int i, int lo, int hi) { return min(max(i, lo), hi); }
 
 // E at (lq, qy), the uniform x and the mesh y, on patch g (the finest patch holding the
 // point; trace_trajectories_2d_pyccel.py:212-269).
 __device__ __forceinline__ void edge_field(const bt_trace_args &a, const PatchGeom &g, double lq,
                                            double qy, double &ex, double &ey) {
-    const i64 pnx = g.pnx, pny = g.pny, ofx = g.ofx, ofy = g.ofy;
+    const int pnx = (int)g.pnx, pny = (int)g.pny;
     const double pox = g.pox, poy = g.poy, phh = g.phh;
-    const double sx = (lq - pox) / phh;
-    const double sy = (qy - poy) / phh;
+    const double sx = div_known(lq - pox, phh, g.rphh);
+    const double sy = div_known(qy - poy, phh, g.rphh);
     double s = sx + 0.5;
-    i64 i = (i64)floor(s);
-    if (i < 0)
-        i = 0;
-    else if (i > pnx - 1)
-        i = pnx - 1;
-    i64 j = (i64)floor(sy);
-    if (j < 0)
-        j = 0;
-    else if (j > pny - 2)
-        j = pny - 2;
+    int i = clamp_index(__double2int_rd(s), 0, pnx - 1);
+    int j = clamp_index(__double2int_rd(sy), 0, pny - 2);
     double u = s - (double)i;
     double w = sy - (double)j;
-    const double *fx = a.fxs + ofx + i * pny + j;
+    const double *fx = a.fxs + g.ofx + (i64)i * pny + j;
     double f00 = __ldg(fx), f01 = __ldg(fx + 1), f10 = __ldg(fx + pny), f11 = __ldg(fx + pny + 1);
     double low = f00 + w * (f01 - f00);
     double high = f10 + w * (f11 - f10);
     ex = low + u * (high - low);
     s = sy + 0.5;
-    i = (i64)floor(sx);
-    if (i < 0)
-        i = 0;
-    else if (i > pnx - 2)
-        i = pnx - 2;
-    j = (i64)floor(s);
-    if (j < 0)
-        j = 0;
-    else if (j > pny - 1)
-        j = pny - 1;
+    i = clamp_index(__double2int_rd(sx), 0, pnx - 2);
+    j = clamp_index(__double2int_rd(s), 0, pny - 1);
     u = sx - (double)i;
     w = s - (double)j;
-    const double *fy = a.fys + ofy + i * (pny + 1) + j;
+    const double *fy = a.fys + g.ofy + (i64)i * (pny + 1) + j;
     f00 = __ldg(fy);
     f01 = __ldg(fy + 1);
     f10 = __ldg(fy + pny + 1);
@@ -217,7 +210,7 @@ __device__ __forceinline__ double inv_gamma(double u0, double u1, double u2, dou
 // q/m (E + v x B) at every stage, Boris with the rotation, and every step that ends in a
 // cell touching an electrode pauses (status -2) for the caller's exact inside test.
 template <int CYL, int INTEG, bool GENERAL, bool MAG>
-__global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restrict__ act,
+__global__ void __launch_bounds__(128, 1) trace_window(Trace tr, const i64 *__restrict__ act,
                                                    i64 n_act, int S,
                                                    uint32_t *__restrict__ keys,
                                                    double *__restrict__ RU,
@@ -228,7 +221,9 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
     const bt_trace_args &a = tr.a;
     const i64 k = act[m];
     const i64 P = GENERAL ? a.n_patches : 1;
-    const PatchGeom base = patch_geom(a, 0);  // the one patch of a non-general mesh
+    PatchGeom base = patch_geom(a, 0);  // the one patch of a non-general mesh
+    base.rphh = known_reciprocal(base.phh);
+    const double rh = known_reciprocal(a.h);
     const i64 nx = tr.nx, ny = tr.ny;
     const double origin_x = a.origin_x, origin_y = a.origin_y, h = a.h;
     constexpr int cyl = CYL;
@@ -373,7 +368,7 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
                 if (dt < 0.0) dt = hloc;
                 dt = a.step_fraction * dt;
                 hdt = 0.5 * dt;
-                dt6 = dt / 6.0;
+                dt6 = div_known(dt, 6.0, 1.0 / 6.0);
                 if (INTEG != 0 && MAG) {
                     // Boris with B: the kick over half the step, then the drift
                     double u[3] = {v0, v1, v2};
@@ -467,9 +462,10 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
 
         // the deposit record of the step's Hermite midpoint (:372-423)
         const double gw = inv_gamma<GENERAL>(w0, w1, w2, inv_c2);
-        double m0 = 0.5 * (x0 + y0) + dt * (gv * v0 - gw * w0) / 8.0;
-        double m1 = 0.5 * (x1 + y1) + dt * (gv * v1 - gw * w1) / 8.0;
-        const double m2 = 0.5 * (x2 + y2) + dt * (gv * v2 - gw * w2) / 8.0;
+        // (a / 8 is a * 0.125 exactly)
+        double m0 = 0.5 * (x0 + y0) + dt * (gv * v0 - gw * w0) * 0.125;
+        double m1 = 0.5 * (x1 + y1) + dt * (gv * v1 - gw * w1) * 0.125;
+        const double m2 = 0.5 * (x2 + y2) + dt * (gv * v2 - gw * w2) * 0.125;
         if (cyl == 1)
             m1 = radius(m1, m2);
         else if (cyl == 2)
@@ -477,18 +473,18 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
         if (graded) m0 = uniform_x(m0, a.x_nodes, a.n_x_nodes, origin_x, h);
         {
             const PatchGeom g = GENERAL ? patch_geom(a, finest_patch(a, P, m0, m1)) : base;
-            const i64 pnx = g.pnx, pny = g.pny, ofn = g.ofn;
-            const double pox = g.pox, poy = g.poy, phh = g.phh;
-            i64 i = (i64)floor((m0 - pox) / phh);
-            i64 j = (i64)floor((m1 - poy) / phh);
-            double u = (m0 - (pox + phh * (double)i)) / phh;
+            const int pnx = (int)g.pnx, pny = (int)g.pny;
+            const double pox = g.pox, poy = g.poy, phh = g.phh, rphh = g.rphh;
+            int i = __double2int_rd(div_known(m0 - pox, phh, rphh));
+            int j = __double2int_rd(div_known(m1 - poy, phh, rphh));
+            double u = div_known(m0 - (pox + phh * (double)i), phh, rphh);
             double w;
             if (cyl == 1) {
                 const double low = poy + phh * (double)j;
                 const double high = low + phh;
                 w = (m1 * m1 - low * low) / (high * high - low * low);
             } else {
-                w = (m1 - (poy + phh * (double)j)) / phh;
+                w = div_known(m1 - (poy + phh * (double)j), phh, rphh);
             }
             if (i < 0) {
                 u = 0.0;
@@ -505,7 +501,7 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
                 j = pny - 2;
             }
             const i64 r = (i64)s * n_act + m;
-            keys[r] = (uint32_t)(ofn + i * pny + j);
+            keys[r] = (uint32_t)(g.ofn + (i64)i * pny + j);
             RU[r] = u;
             RW[r] = w;
             RQ[r] = dqk * dt;
@@ -562,25 +558,23 @@ __global__ void __launch_bounds__(128) trace_window(Trace tr, const i64 *__restr
         } else if (py > a.upper_y || (cyl == 0 && py < origin_y)) {
             st = 2;
         } else {
-            i64 i = (i64)((px - origin_x) / h);
-            if (i > nx - 2) i = nx - 2;
-            i64 j = (i64)((py - origin_y) / h);
-            if (j > ny - 2) j = ny - 2;
+            const double ux = div_known(px - origin_x, h, rh);
+            const double uy = div_known(py - origin_y, h, rh);
             // a point below the mesh (only a malformed geometry puts one there) takes
             // its first cell, where the reference indexes outside the table
-            if (i < 0) i = 0;
-            if (j < 0) j = 0;
-            const i64 cell = __ldg(a.cells + i * (ny - 1) + j);
+            const int i = max(min(__double2int_rz(ux), (int)nx - 2), 0);
+            const int j = max(min(__double2int_rz(uy), (int)ny - 2), 0);
+            const i64 cell = __ldg(a.cells + (i64)i * (ny - 1) + j);
             if (MAG && cell >= 0) {
                 st = -2;  // the caller tests the electrodes' shapes
             } else if (cell >= 0) {
                 const i64 R = a.refine;
-                i64 si = (i64)(((px - origin_x) / h - (double)i) * (double)R);
+                i64 si = (i64)((ux - (double)i) * (double)R);
                 if (si < 0)
                     si = 0;
                 else if (si > R - 1)
                     si = R - 1;
-                i64 sj = (i64)(((py - origin_y) / h - (double)j) * (double)R);
+                i64 sj = (i64)((uy - (double)j) * (double)R);
                 if (sj < 0)
                     sj = 0;
                 else if (sj > R - 1)
@@ -675,6 +669,18 @@ __global__ void scatter_alive(const i64 *__restrict__ act, i64 n, const i64 *__r
 namespace bt {
 namespace {
 
+// Records per deposit batch (at most; 16 windows of the starting trajectories when fewer):
+// large batches keep the deposits, which compete with the windows for the SMs' L1, rare.
+constexpr int64_t kBatchRecords = (int64_t)1 << 24;
+
+// Points the context's launches at `side` for its lifetime.
+struct SideStream {
+    bt_ctx *ctx;
+    cudaStream_t saved;
+    SideStream(bt_ctx *c, cudaStream_t side) : ctx(c), saved(c->stream) { ctx->stream = side; }
+    ~SideStream() { ctx->stream = saved; }
+};
+
 void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, int64_t window) {
     {
         BT_REQUIRE(ctx && args, "trace: null argument");
@@ -716,17 +722,28 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         bt::TraceScratch &ts = ctx->trace;
         cudaStream_t st = ctx->stream;
         const uint32_t sentinel = (uint32_t)a.n_nodes;
-        // the record buffer: flushed (sorted and reduced into charge[0]) when the next
-        // window would not fit
-        // room for 16 windows of the starting trajectories, at most 2^25 records (0.9 GB),
-        // at least one window
+        // Two record buffers: the windows fill one while the records of the other are sorted
+        // and reduced into charge[0] on the side stream, in the order the buffers were
+        // filled, so the deposit runs under the next windows and the sums are the same
+        // whatever the timing.  A buffer is deposited once it holds `batch` records.
         const int64_t per_window = a.n_active * (int64_t)S;
-        int64_t capacity = std::min<int64_t>(per_window * 16, (int64_t)1 << 25);
-        if (capacity < per_window) capacity = per_window;
-        uint32_t *keys = ts.rec_keys.as<uint32_t>(capacity);
-        double *RU = ts.rec_u.as<double>(capacity);
-        double *RW = ts.rec_w.as<double>(capacity);
-        double *RQ = ts.rec_q.as<double>(capacity);
+        const int64_t batch = std::min<int64_t>(kBatchRecords, 16 * per_window);
+        const int64_t capacity = per_window + batch;
+        uint32_t *keys[2];
+        double *RU[2], *RW[2], *RQ[2];
+        for (int b = 0; b < 2; ++b) {
+            keys[b] = ts.rec_keys[b].as<uint32_t>(capacity);
+            RU[b] = ts.rec_u[b].as<double>(capacity);
+            RW[b] = ts.rec_w[b].as<double>(capacity);
+            RQ[b] = ts.rec_q[b].as<double>(capacity);
+        }
+        if (!ts.side) {
+            BT_CUDA(cudaStreamCreateWithFlags(&ts.side, cudaStreamNonBlocking));
+            for (int b = 0; b < 2; ++b) {
+                BT_CUDA(cudaEventCreateWithFlags(&ts.filled[b], cudaEventDisableTiming));
+                BT_CUDA(cudaEventCreateWithFlags(&ts.drained[b], cudaEventDisableTiming));
+            }
+        }
         int64_t *act_a = ts.active_a.as<int64_t>(a.n_active);
         int64_t *act_b = ts.active_b.as<int64_t>(a.n_active);
         const int nb_max = (int)bt::blocks_for(a.n_active, bt::kCompact);
@@ -737,13 +754,26 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                                 cudaMemcpyDeviceToDevice, st));
         bt::NodeLayout layout{a.patch_int, a.n_patches, tr.nx, tr.ny, a.n_nodes};
         int64_t n_act = a.n_active, used = 0;
+        int cur = 0;
+        bool pending[2] = {false, false};
+        // deposit buffer `cur` on the side stream and switch the windows to the other one
         auto flush = [&] {
             if (used == 0) return;
-            bt::Timed timed(ctx, "deposit");
-            bt::deposit_records(ctx, keys, RU, RW, RQ, used, sentinel, a.charge, layout);
+            BT_CUDA(cudaEventRecord(ts.filled[cur], st));
+            BT_CUDA(cudaStreamWaitEvent(ts.side, ts.filled[cur], 0));
+            {
+                SideStream on_side(ctx, ts.side);
+                bt::Timed timed(ctx, "deposit");
+                bt::deposit_records(ctx, keys[cur], RU[cur], RW[cur], RQ[cur], used, sentinel,
+                                    a.charge, layout);
+            }
+            BT_CUDA(cudaEventRecord(ts.drained[cur], ts.side));
+            pending[cur] = true;
             ctx->last_records += used;
             ctx->last_flushes += 1;
             used = 0;
+            cur ^= 1;
+            if (pending[cur]) BT_CUDA(cudaStreamWaitEvent(st, ts.drained[cur], 0));
         };
         while (n_act > 0) {
             const int64_t need = n_act * (int64_t)S;
@@ -756,7 +786,8 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
     if (a.cylindrical == C && (a.integrator != 0) == (I != 0) && general == G &&                 \
         (mag != nullptr) == M)                                                                   \
         BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M>), grid, 128, 0, st, tr, act_a, n_act, S,    \
-                  keys + used, RU + used, RW + used, RQ + used, sentinel);
+                  keys[cur] + used, RU[cur] + used, RW[cur] + used, RQ[cur] + used,  \
+                  sentinel);
                 BT_TRACE_CASE(0, 0, false, false) BT_TRACE_CASE(0, 0, true, false)
                 BT_TRACE_CASE(0, 1, false, false) BT_TRACE_CASE(0, 1, true, false)
                 BT_TRACE_CASE(1, 0, false, false) BT_TRACE_CASE(1, 0, true, false)
@@ -784,8 +815,12 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
             BT_CUDA(cudaStreamSynchronize(st));
             n_act = *n_alive_host;
             std::swap(act_a, act_b);
+            if (used >= batch) flush();
         }
         flush();
+        // the caller's stream continues once every deposit is in charge[0]
+        for (int b = 0; b < 2; ++b)
+            if (pending[b]) BT_CUDA(cudaStreamWaitEvent(st, ts.drained[b], 0));
     }
 }
 
