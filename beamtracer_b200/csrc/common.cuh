@@ -228,13 +228,16 @@ struct NodeLayout {
     i64 n_nodes;
 };
 
+// n_records sizes the launches; n_dev, when not NULL, is the device-held count of the
+// records to deposit (at most n_records): the first ones, the rest ignored.
 void deposit_records(bt_ctx *ctx, const uint32_t *keys, const double *u, const double *w,
-                     const double *q, i64 n_records, uint32_t sentinel, double *charge,
-                     const NodeLayout &layout);
+                     const double *q, i64 n_records, const i64 *n_dev, uint32_t sentinel,
+                     double *charge, const NodeLayout &layout);
 
 // Stable LSD radix sort of (key, index) pairs: sorted keys and the permutation.
-// Returns the device pointers of the sorted keys and values (inside the scratch).
-void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, int key_bits,
-                      uint32_t **keys_out, uint32_t **vals_out);
+// Returns the device pointers of the sorted keys and values (inside the scratch).  n sizes
+// the launches; n_dev, when not NULL, is the device-held count of keys to sort (at most n).
+void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_dev,
+                      int key_bits, uint32_t **keys_out, uint32_t **vals_out);
 
 }  // namespace bt

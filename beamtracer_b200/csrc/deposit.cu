@@ -24,10 +24,16 @@ constexpr int kRadixMax = 512;  // 9-bit digits, when they save a pass
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned kFull = 0xffffffffu;
 
+// The record count of a sort or reduction: `n` from the host, or, where the caller gives
+// one, the count the device holds (at most n; the grids are sized for n).
+__device__ __forceinline__ i64 record_count(i64 n, const i64 *n_dev) { return n_dev ? *n_dev : n; }
+
 template <int R>
-__global__ void radix_hist(const uint32_t *__restrict__ keys, i64 n, int shift,
-                           uint32_t *__restrict__ hist, int nblocks) {
+__global__ void radix_hist(const uint32_t *__restrict__ keys, i64 n_host,
+                           const i64 *__restrict__ n_dev, int shift, uint32_t *__restrict__ hist,
+                           int nblocks) {
     __shared__ uint32_t h[R];
+    const i64 n = record_count(n_host, n_dev);
     for (int d = threadIdx.x; d < R; d += kThreads) h[d] = 0;
     __syncthreads();
     const i64 base = (i64)blockIdx.x * kTile;
@@ -110,13 +116,15 @@ __global__ void radix_digit_base(const uint32_t *__restrict__ totals, uint32_t *
 // equal digits (warp ranks by __match_any_sync, warps in order by a per-digit prefix).
 template <int R>
 __global__ void radix_scatter(const uint32_t *__restrict__ keys_in,
-                              const uint32_t *__restrict__ vals_in, i64 n, int shift,
+                              const uint32_t *__restrict__ vals_in, i64 n_host,
+                              const i64 *__restrict__ n_dev, int shift,
                               const uint32_t *__restrict__ offs,
                               const uint32_t *__restrict__ base, int nblocks,
                               uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out) {
     __shared__ uint32_t wcount[kWarps][R];
     __shared__ uint32_t woff[kWarps][R];
     __shared__ uint32_t run[R];
+    const i64 n = record_count(n_host, n_dev);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     for (int d = t; d < R; d += kThreads) {
 #pragma unroll
@@ -164,10 +172,12 @@ __global__ void radix_scatter(const uint32_t *__restrict__ keys_in,
 // that begins in the warp and continues (`owner` set).
 __global__ void seg_reduce_warps(const uint32_t *__restrict__ K, const uint32_t *__restrict__ I,
                                  const double *__restrict__ U, const double *__restrict__ W,
-                                 const double *__restrict__ Q, i64 R, uint32_t sentinel,
+                                 const double *__restrict__ Q, i64 R_host,
+                                 const i64 *__restrict__ R_dev, uint32_t sentinel,
                                  double4 *__restrict__ cells, double4 *__restrict__ first,
                                  double4 *__restrict__ last, uint8_t *__restrict__ tail_flag,
                                  uint8_t *__restrict__ owner_flag) {
+    const i64 R = record_count(R_host, R_dev);
     const i64 gw = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (gw * 32 >= R) return;  // whole warps only
@@ -227,11 +237,13 @@ __global__ void seg_reduce_warps(const uint32_t *__restrict__ K, const uint32_t 
 
 // The segments that cross warps: the owning warp's trailing piece plus the following
 // warps' leading pieces, added in warp order until the segment ends.
-__global__ void seg_reduce_chains(const uint32_t *__restrict__ K, i64 n_warps,
-                                  double4 *__restrict__ cells, const double4 *__restrict__ first,
+__global__ void seg_reduce_chains(const uint32_t *__restrict__ K, i64 R_host,
+                                  const i64 *__restrict__ R_dev, double4 *__restrict__ cells,
+                                  const double4 *__restrict__ first,
                                   const double4 *__restrict__ last,
                                   const uint8_t *__restrict__ tail_flag,
                                   const uint8_t *__restrict__ owner_flag) {
+    const i64 n_warps = (record_count(R_host, R_dev) + 31) / 32;
     const i64 gw = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (gw >= n_warps || !owner_flag[gw]) return;
     double4 s = last[gw];
@@ -322,8 +334,8 @@ int bits_for(uint64_t max_key) {
 
 }  // namespace
 
-void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, int key_bits,
-                      uint32_t **keys_out, uint32_t **vals_out) {
+void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_dev,
+                      int key_bits, uint32_t **keys_out, uint32_t **vals_out) {
     BT_REQUIRE(n < (i64)0xffffffffLL, "radix sort: too many records for 32-bit indices");
     DepositScratch &s = ctx->deposit;
     cudaStream_t st = ctx->stream;
@@ -344,19 +356,19 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, int key_bits,
     for (int p = 0; p < passes; ++p) {
         const int shift = bits * p;
         if (bits == 9) {
-            BT_LAUNCH(ctx, radix_hist<kRadixMax>, nblocks, kThreads, 0, st, src_k, n, shift, hist,
-                      nblocks);
+            BT_LAUNCH(ctx, radix_hist<kRadixMax>, nblocks, kThreads, 0, st, src_k, n, n_dev, shift,
+                      hist, nblocks);
             BT_LAUNCH(ctx, radix_row_scan, kRadixMax, kThreads, 0, st, hist, offs, totals, nblocks);
             BT_LAUNCH(ctx, radix_digit_base<kRadixMax>, 1, kThreads, 0, st, totals, digit);
             BT_LAUNCH(ctx, radix_scatter<kRadixMax>, nblocks, kThreads, 0, st, src_k, src_v, n,
-                      shift, offs, digit, nblocks, dst_k, dst_v);
+                      n_dev, shift, offs, digit, nblocks, dst_k, dst_v);
         } else {
-            BT_LAUNCH(ctx, radix_hist<kRadix>, nblocks, kThreads, 0, st, src_k, n, shift, hist,
-                      nblocks);
+            BT_LAUNCH(ctx, radix_hist<kRadix>, nblocks, kThreads, 0, st, src_k, n, n_dev, shift,
+                      hist, nblocks);
             BT_LAUNCH(ctx, radix_row_scan, kRadix, kThreads, 0, st, hist, offs, totals, nblocks);
             BT_LAUNCH(ctx, radix_digit_base<kRadix>, 1, kThreads, 0, st, totals, digit);
-            BT_LAUNCH(ctx, radix_scatter<kRadix>, nblocks, kThreads, 0, st, src_k, src_v, n, shift,
-                      offs, digit, nblocks, dst_k, dst_v);
+            BT_LAUNCH(ctx, radix_scatter<kRadix>, nblocks, kThreads, 0, st, src_k, src_v, n, n_dev,
+                      shift, offs, digit, nblocks, dst_k, dst_v);
         }
         BT_CHECK_LAUNCH();
         src_k = dst_k;
@@ -374,13 +386,13 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, int key_bits,
 }
 
 void deposit_records(bt_ctx *ctx, const uint32_t *keys, const double *u, const double *w,
-                     const double *q, i64 n_records, uint32_t sentinel, double *charge,
-                     const NodeLayout &layout) {
+                     const double *q, i64 n_records, const i64 *n_dev, uint32_t sentinel,
+                     double *charge, const NodeLayout &layout) {
     if (n_records == 0) return;
     DepositScratch &s = ctx->deposit;
     cudaStream_t st = ctx->stream;
     uint32_t *sk = nullptr, *sv = nullptr;
-    radix_sort_pairs(ctx, keys, n_records, bits_for(sentinel), &sk, &sv);
+    radix_sort_pairs(ctx, keys, n_records, n_dev, bits_for(sentinel), &sk, &sv);
     const i64 n_warps = (n_records + 31) / 32;
     double4 *cells = s.cell_sums.as<double4>((size_t)layout.n_nodes);
     double4 *first = s.warp_first.as<double4>((size_t)n_warps);
@@ -388,8 +400,10 @@ void deposit_records(bt_ctx *ctx, const uint32_t *keys, const double *u, const d
     uint8_t *flags = s.warp_flags.as<uint8_t>((size_t)2 * n_warps);
     BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * layout.n_nodes, st));
     const int threads = 256;
-    BT_LAUNCH(ctx, seg_reduce_warps, blocks_for(n_warps * 32, threads), threads, 0, st, sk, sv, u, w, q, n_records, sentinel, cells, first, last, flags, flags + n_warps);
-    BT_LAUNCH(ctx, seg_reduce_chains, blocks_for(n_warps, threads), threads, 0, st, sk, n_warps, cells, first, last, flags, flags + n_warps);
+    BT_LAUNCH(ctx, seg_reduce_warps, blocks_for(n_warps * 32, threads), threads, 0, st, sk, sv,
+              u, w, q, n_records, n_dev, sentinel, cells, first, last, flags, flags + n_warps);
+    BT_LAUNCH(ctx, seg_reduce_chains, blocks_for(n_warps, threads), threads, 0, st, sk, n_records,
+              n_dev, cells, first, last, flags, flags + n_warps);
     BT_LAUNCH(ctx, node_accumulate, blocks_for(layout.n_nodes, threads), threads, 0, st, cells, charge, layout.patch_int, layout.n_patches, layout.nx, layout.ny,
         layout.n_nodes);
     BT_CHECK_LAUNCH();
@@ -415,7 +429,7 @@ extern "C" int bt_deposit_trajectories_2d(bt_ctx *ctx, const double *px, const d
         BT_CHECK_LAUNCH();
         // the records' keys live in `keys`; the sort reads them and writes elsewhere
         bt::NodeLayout layout{nullptr, 1, nx, ny, nx * ny};
-        bt::deposit_records(ctx, keys, U, W, Q, n, (uint32_t)(nx * ny), charge, layout);
+        bt::deposit_records(ctx, keys, U, W, Q, n, nullptr, (uint32_t)(nx * ny), charge, layout);
     });
 }
 
@@ -517,11 +531,13 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
         uint32_t *dst_k = keys_alt, *dst_v = vals;
         for (int pass = 0; pass < passes; ++pass) {
             const int shift = 8 * pass;
-            radix_hist<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, n, shift, hist, nblocks);
+            radix_hist<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, n, nullptr, shift, hist,
+                                                             nblocks);
             radix_row_scan<<<kRadix, kThreads, 0, st>>>(hist, offs, totals, nblocks);
             radix_digit_base<kRadix><<<1, kThreads, 0, st>>>(totals, digit);
-            radix_scatter<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, src_v, n, shift, offs, digit,
-                                                        nblocks, dst_k, dst_v);
+            radix_scatter<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, src_v, n, nullptr, shift,
+                                                                offs, digit, nblocks, dst_k,
+                                                                dst_v);
             src_k = dst_k;
             src_v = dst_v;
             if (dst_k == keys_alt) {
@@ -537,9 +553,10 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
         const i64 n_warps = (n + 31) / 32;
         BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * n_nodes, st));
         seg_reduce_warps<<<blocks_for(n_warps * 32, 256), 256, 0, st>>>(
-            src_k, src_v, U, W, Q, n, sentinel, cells, first, last, flags, flags + n_warps);
-        seg_reduce_chains<<<blocks_for(n_warps, 256), 256, 0, st>>>(src_k, n_warps, cells, first,
-                                                                   last, flags, flags + n_warps);
+            src_k, src_v, U, W, Q, n, nullptr, sentinel, cells, first, last, flags,
+            flags + n_warps);
+        seg_reduce_chains<<<blocks_for(n_warps, 256), 256, 0, st>>>(
+            src_k, n, nullptr, cells, first, last, flags, flags + n_warps);
         node_accumulate<<<blocks_for(n_nodes, 256), 256, 0, st>>>(cells, charge, nullptr, 1, nx,
                                                                  ny, n_nodes);
         BT_CHECK_LAUNCH();

@@ -80,14 +80,11 @@ __device__ __forceinline__ PatchGeom patch_geom(const bt_trace_args &a, i64 pp) 
 // follow them give what the 64-bit conversions give.
 __device__ __forceinline__ int clamp_index(int i, int lo, int hi) { return min(max(i, lo), hi); }
 
-// E at (lq, qy), the uniform x and the mesh y, on patch g (the finest patch holding the
+// E at the point (sx, sy) in cells of patch g from its origin (the finest patch holding the
 // point; trace_trajectories_2d_pyccel.py:212-269).
-__device__ __forceinline__ void edge_field(const bt_trace_args &a, const PatchGeom &g, double lq,
-                                           double qy, double &ex, double &ey) {
+__device__ __forceinline__ void edge_field_cells(const bt_trace_args &a, const PatchGeom &g,
+                                                 double sx, double sy, double &ex, double &ey) {
     const int pnx = (int)g.pnx, pny = (int)g.pny;
-    const double pox = g.pox, poy = g.poy, phh = g.phh;
-    const double sx = div_known(lq - pox, phh, g.rphh);
-    const double sy = div_known(qy - poy, phh, g.rphh);
     double s = sx + 0.5;
     int i = clamp_index(__double2int_rd(s), 0, pnx - 1);
     int j = clamp_index(__double2int_rd(sy), 0, pny - 2);
@@ -111,6 +108,13 @@ __device__ __forceinline__ void edge_field(const bt_trace_args &a, const PatchGe
     low = f00 + w * (f01 - f00);
     high = f10 + w * (f11 - f10);
     ey = low + u * (high - low);
+}
+
+// E at (lq, qy), the uniform x and the mesh y, on patch g.
+__device__ __forceinline__ void edge_field(const bt_trace_args &a, const PatchGeom &g, double lq,
+                                           double qy, double &ex, double &ey) {
+    edge_field_cells(a, g, div_known(lq - g.pox, g.phh, g.rphh),
+                     div_known(qy - g.poy, g.phh, g.rphh), ex, ey);
 }
 
 // (B_z, B_r) of an on-axis profile at axial position z and radius r (fields.py:250-279,
@@ -209,15 +213,26 @@ __device__ __forceinline__ double inv_gamma(double u0, double u1, double u2, dou
 // MAG: the reference's NumPy tracer's step in a magnetic field instead (tracer.py:851-1054):
 // q/m (E + v x B) at every stage, Boris with the rotation, and every step that ends in a
 // cell touching an electrode pauses (status -2) for the caller's exact inside test.
+//
+// The live trajectories are act[0, *live); the grid covers `stride` >= *live threads, the
+// live count when the host last read it, and the records of step s of thread m go to slot
+// s * stride + m.  Threads past the live count fill their slots with the sentinel.  A
+// window with live trajectories sets *records_end to `end`, the end of its slots, so the
+// deposit sorts no window that had none.
 template <int CYL, int INTEG, bool GENERAL, bool MAG>
-__global__ void __launch_bounds__(128, 1) trace_window(Trace tr, const i64 *__restrict__ act,
-                                                   i64 n_act, int S,
-                                                   uint32_t *__restrict__ keys,
-                                                   double *__restrict__ RU,
-                                                   double *__restrict__ RW,
-                                                   double *__restrict__ RQ, uint32_t sentinel) {
+__global__ void __launch_bounds__(128, 1)
+    trace_window(Trace tr, const i64 *__restrict__ act, const i64 *__restrict__ live, i64 stride,
+                 int S, uint32_t *__restrict__ keys, double *__restrict__ RU,
+                 double *__restrict__ RW, double *__restrict__ RQ, uint32_t sentinel,
+                 i64 *__restrict__ records_end, i64 end) {
     const i64 m = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= n_act) return;
+    const i64 n_act = *live;
+    if (m == 0 && n_act > 0) *records_end = end;
+    if (m >= stride) return;
+    if (m >= n_act) {
+        for (int s = 0; s < S; ++s) keys[(i64)s * stride + m] = sentinel;
+        return;
+    }
     const bt_trace_args &a = tr.a;
     const i64 k = act[m];
     const i64 P = GENERAL ? a.n_patches : 1;
@@ -241,6 +256,21 @@ __global__ void __launch_bounds__(128, 1) trace_window(Trace tr, const i64 *__re
     int have = 0;
     double ca0 = 0.0, ca1 = 0.0, ca2 = 0.0;
     double cE[3] = {0, 0, 0}, cB[3] = {0, 0, 0};  // with B: the fields at the step's end
+    // A one-patch mesh whose patch is the mesh: the first gather of a step is at the point
+    // where the exit test of the step before found the radius and the cell coordinates;
+    // they are kept (the same expressions on the same values).
+    const bool reuse = !GENERAL && !MAG && base.pox == origin_x && base.poy == origin_y &&
+                       base.phh == h;
+    double start_r = 0.0, start_sx = 0.0, start_sy = 0.0;
+    if (reuse) {
+        start_r = x1;
+        if (cyl == 1)
+            start_r = radius(x1, x2);
+        else if (cyl == 2)
+            start_r = origin_y + fabs(x1 - origin_y);
+        start_sx = div_known(x0 - origin_x, h, rh);
+        start_sy = div_known(start_r - origin_y, h, rh);
+    }
     int s = 0;
     for (; s < S; ++s) {
         if (ns >= a.max_steps) break;
@@ -327,9 +357,10 @@ __global__ void __launch_bounds__(128, 1) trace_window(Trace tr, const i64 *__re
                 g1 = ca1;
                 g2 = ca2;
             } else {
+                const bool kept = reuse && stage == 0;
                 double qy = q1, cy = 0.0, cz = 0.0;
                 if (cyl == 1) {
-                    const double r = radius(q1, q2);
+                    const double r = kept ? start_r : radius(q1, q2);
                     if (r > 0.0) {
                         cy = q1 / r;
                         cz = q2 / r;
@@ -344,7 +375,10 @@ __global__ void __launch_bounds__(128, 1) trace_window(Trace tr, const i64 *__re
                 if (graded) lq = uniform_x(q0, a.x_nodes, a.n_x_nodes, origin_x, h);
                 double ex, ey;
                 const PatchGeom g = GENERAL ? patch_geom(a, finest_patch(a, P, lq, qy)) : base;
-                edge_field(a, g, lq, qy, ex, ey);
+                if (kept)
+                    edge_field_cells(a, g, start_sx, start_sy, ex, ey);
+                else
+                    edge_field(a, g, lq, qy, ex, ey);
                 if (cyl != 0) {
                     g0 = qmk * ex;
                     g1 = qmk * (ey * cy);
@@ -500,7 +534,7 @@ __global__ void __launch_bounds__(128, 1) trace_window(Trace tr, const i64 *__re
                 w = 1.0;
                 j = pny - 2;
             }
-            const i64 r = (i64)s * n_act + m;
+            const i64 r = (i64)s * stride + m;
             keys[r] = (uint32_t)(g.ofn + (i64)i * pny + j);
             RU[r] = u;
             RW[r] = w;
@@ -560,6 +594,9 @@ __global__ void __launch_bounds__(128, 1) trace_window(Trace tr, const i64 *__re
         } else {
             const double ux = div_known(px - origin_x, h, rh);
             const double uy = div_known(py - origin_y, h, rh);
+            start_r = py;
+            start_sx = ux;
+            start_sy = uy;
             // a point below the mesh (only a malformed geometry puts one there) takes
             // its first cell, where the reference indexes outside the table
             const int i = max(min(__double2int_rz(ux), (int)nx - 2), 0);
@@ -594,7 +631,7 @@ __global__ void __launch_bounds__(128, 1) trace_window(Trace tr, const i64 *__re
         }
     }
     // the slots of the steps not taken hold no record
-    for (; s < S; ++s) keys[(i64)s * n_act + m] = sentinel;
+    for (; s < S; ++s) keys[(i64)s * stride + m] = sentinel;
     if (st == -1 && ns >= a.max_steps) st = 4;
     a.x[k] = x0;
     a.x[n + k] = x1;
@@ -610,9 +647,11 @@ __global__ void __launch_bounds__(128, 1) trace_window(Trace tr, const i64 *__re
 
 constexpr int kCompact = 1024;
 
-__global__ void count_alive(const i64 *__restrict__ act, i64 n, const i64 *__restrict__ status,
-                            uint32_t *__restrict__ block_counts) {
+// act[0, *live) are the trajectories of the last window; the grid covers at least *live.
+__global__ void count_alive(const i64 *__restrict__ act, const i64 *__restrict__ live,
+                            const i64 *__restrict__ status, uint32_t *__restrict__ block_counts) {
     __shared__ uint32_t warp_counts[kCompact / 32];
+    const i64 n = *live;
     const i64 m = (i64)blockIdx.x * kCompact + threadIdx.x;
     const bool alive = m < n && status[act[m]] == -1;
     const unsigned ballot = __ballot_sync(0xffffffffu, alive);
@@ -626,6 +665,8 @@ __global__ void count_alive(const i64 *__restrict__ act, i64 n, const i64 *__res
 }
 
 // One block: exclusive prefix of the block counts (in place) and the total.
+__global__ void set_count(i64 *__restrict__ count, i64 value) { *count = value; }
+
 __global__ void scan_counts(uint32_t *__restrict__ block_counts, int nblocks,
                             i64 *__restrict__ total) {
     if (threadIdx.x != 0) return;
@@ -638,9 +679,11 @@ __global__ void scan_counts(uint32_t *__restrict__ block_counts, int nblocks,
     *total = run;
 }
 
-__global__ void scatter_alive(const i64 *__restrict__ act, i64 n, const i64 *__restrict__ status,
+__global__ void scatter_alive(const i64 *__restrict__ act, const i64 *__restrict__ live,
+                              const i64 *__restrict__ status,
                               const uint32_t *__restrict__ block_offsets, i64 *__restrict__ out) {
     __shared__ uint32_t warp_counts[kCompact / 32];
+    const i64 n = *live;
     const i64 m = (i64)blockIdx.x * kCompact + threadIdx.x;
     const bool alive = m < n && status[act[m]] == -1;
     const unsigned ballot = __ballot_sync(0xffffffffu, alive);
@@ -668,6 +711,9 @@ __global__ void scatter_alive(const i64 *__restrict__ act, i64 n, const i64 *__r
 
 namespace bt {
 namespace {
+
+// Windows launched between two reads of the live count.
+constexpr int kGroup = 8;
 
 // Records per deposit batch (at most; 16 windows of the starting trajectories when fewer):
 // large batches keep the deposits, which compete with the windows for the SMs' L1, rare.
@@ -748,12 +794,18 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         int64_t *act_b = ts.active_b.as<int64_t>(a.n_active);
         const int nb_max = (int)bt::blocks_for(a.n_active, bt::kCompact);
         uint32_t *block_counts = ts.block_counts.as<uint32_t>(nb_max);
-        int64_t *n_alive_dev = ts.n_alive.as<int64_t>(1);
+        // live[2]: the live count before and after a window's compaction; records_end[2]:
+        // where the slots of each buffer's last window with live trajectories end
+        int64_t *live = ts.n_alive.as<int64_t>(4);
+        int64_t *records_end = live + 2;
         int64_t *n_alive_host = static_cast<int64_t *>(ctx->host.get(sizeof(int64_t)));
         BT_CUDA(cudaMemcpyAsync(act_a, a.active, sizeof(int64_t) * a.n_active,
                                 cudaMemcpyDeviceToDevice, st));
+        BT_CUDA(cudaMemsetAsync(records_end, 0, 2 * sizeof(int64_t), st));
+        BT_LAUNCH(ctx, bt::set_count, 1, 1, 0, st, live, a.n_active);
         bt::NodeLayout layout{a.patch_int, a.n_patches, tr.nx, tr.ny, a.n_nodes};
-        int64_t n_act = a.n_active, used = 0;
+        int64_t bound = a.n_active, used = 0;
+        int lv = 0;
         int cur = 0;
         bool pending[2] = {false, false};
         // deposit buffer `cur` on the side stream and switch the windows to the other one
@@ -764,9 +816,10 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
             {
                 SideStream on_side(ctx, ts.side);
                 bt::Timed timed(ctx, "deposit");
-                bt::deposit_records(ctx, keys[cur], RU[cur], RW[cur], RQ[cur], used, sentinel,
-                                    a.charge, layout);
+                bt::deposit_records(ctx, keys[cur], RU[cur], RW[cur], RQ[cur], used,
+                                    records_end + cur, sentinel, a.charge, layout);
             }
+            BT_CUDA(cudaMemsetAsync(records_end + cur, 0, sizeof(int64_t), ts.side));
             BT_CUDA(cudaEventRecord(ts.drained[cur], ts.side));
             pending[cur] = true;
             ctx->last_records += used;
@@ -775,46 +828,53 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
             cur ^= 1;
             if (pending[cur]) BT_CUDA(cudaStreamWaitEvent(st, ts.drained[cur], 0));
         };
-        while (n_act > 0) {
-            const int64_t need = n_act * (int64_t)S;
-            if (used + need > capacity) flush();
-            {
-                bt::Timed timed(ctx, "trace_window");
-                const unsigned grid = (unsigned)bt::blocks_for(n_act, 128);
-                const int64_t launched = ctx->launch_count;
+        // The windows go in groups of kGroup between reads of the live count: each reads
+        // the count on the device, and a window after the last trajectory ended does no work.
+        while (bound > 0) {
+            for (int g = 0; g < kGroup; ++g) {
+                const int64_t need = bound * (int64_t)S;
+                if (used + need > capacity) flush();
+                {
+                    bt::Timed timed(ctx, "trace_window");
+                    const unsigned grid = (unsigned)bt::blocks_for(bound, 128);
+                    const int64_t launched = ctx->launch_count;
 #define BT_TRACE_CASE(C, I, G, M)                                                               \
     if (a.cylindrical == C && (a.integrator != 0) == (I != 0) && general == G &&                 \
         (mag != nullptr) == M)                                                                   \
-        BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M>), grid, 128, 0, st, tr, act_a, n_act, S,    \
-                  keys[cur] + used, RU[cur] + used, RW[cur] + used, RQ[cur] + used,  \
-                  sentinel);
-                BT_TRACE_CASE(0, 0, false, false) BT_TRACE_CASE(0, 0, true, false)
-                BT_TRACE_CASE(0, 1, false, false) BT_TRACE_CASE(0, 1, true, false)
-                BT_TRACE_CASE(1, 0, false, false) BT_TRACE_CASE(1, 0, true, false)
-                BT_TRACE_CASE(1, 1, false, false) BT_TRACE_CASE(1, 1, true, false)
-                BT_TRACE_CASE(2, 0, false, false) BT_TRACE_CASE(2, 0, true, false)
-                BT_TRACE_CASE(2, 1, false, false) BT_TRACE_CASE(2, 1, true, false)
-                BT_TRACE_CASE(0, 0, false, true) BT_TRACE_CASE(0, 0, true, true)
-                BT_TRACE_CASE(0, 1, false, true) BT_TRACE_CASE(0, 1, true, true)
-                BT_TRACE_CASE(1, 0, false, true) BT_TRACE_CASE(1, 0, true, true)
-                BT_TRACE_CASE(1, 1, false, true) BT_TRACE_CASE(1, 1, true, true)
+        BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M>), grid, 128, 0, st, tr, act_a, live + lv,   \
+                  bound, S, keys[cur] + used, RU[cur] + used, RW[cur] + used, RQ[cur] + used,    \
+                  sentinel, records_end + cur, used + need);
+                    BT_TRACE_CASE(0, 0, false, false) BT_TRACE_CASE(0, 0, true, false)
+                    BT_TRACE_CASE(0, 1, false, false) BT_TRACE_CASE(0, 1, true, false)
+                    BT_TRACE_CASE(1, 0, false, false) BT_TRACE_CASE(1, 0, true, false)
+                    BT_TRACE_CASE(1, 1, false, false) BT_TRACE_CASE(1, 1, true, false)
+                    BT_TRACE_CASE(2, 0, false, false) BT_TRACE_CASE(2, 0, true, false)
+                    BT_TRACE_CASE(2, 1, false, false) BT_TRACE_CASE(2, 1, true, false)
+                    BT_TRACE_CASE(0, 0, false, true) BT_TRACE_CASE(0, 0, true, true)
+                    BT_TRACE_CASE(0, 1, false, true) BT_TRACE_CASE(0, 1, true, true)
+                    BT_TRACE_CASE(1, 0, false, true) BT_TRACE_CASE(1, 0, true, true)
+                    BT_TRACE_CASE(1, 1, false, true) BT_TRACE_CASE(1, 1, true, true)
 #undef BT_TRACE_CASE
-                BT_REQUIRE(ctx->launch_count > launched, "trace: no kernel for these settings");
+                    BT_REQUIRE(ctx->launch_count > launched,
+                               "trace: no kernel for these settings");
+                }
+                BT_CHECK_LAUNCH();
+                used += need;
+                ctx->last_windows += 1;
+                const int nb = (int)bt::blocks_for(bound, bt::kCompact);
+                BT_LAUNCH(ctx, bt::count_alive, nb, bt::kCompact, 0, st, act_a, live + lv,
+                          a.status, block_counts);
+                BT_LAUNCH(ctx, bt::scan_counts, 1, 32, 0, st, block_counts, nb, live + (lv ^ 1));
+                BT_LAUNCH(ctx, bt::scatter_alive, nb, bt::kCompact, 0, st, act_a, live + lv,
+                          a.status, block_counts, act_b);
+                BT_CHECK_LAUNCH();
+                std::swap(act_a, act_b);
+                lv ^= 1;
             }
-            BT_CHECK_LAUNCH();
-            used += need;
-            ctx->last_windows += 1;
-            const int nb = (int)bt::blocks_for(n_act, bt::kCompact);
-            BT_LAUNCH(ctx, bt::count_alive, nb, bt::kCompact, 0, st, act_a, n_act, a.status, block_counts);
-            BT_LAUNCH(ctx, bt::scan_counts, 1, 32, 0, st, block_counts, nb, n_alive_dev);
-            BT_LAUNCH(ctx, bt::scatter_alive, nb, bt::kCompact, 0, st, act_a, n_act, a.status, block_counts,
-                                                           act_b);
-            BT_CHECK_LAUNCH();
-            BT_CUDA(cudaMemcpyAsync(n_alive_host, n_alive_dev, sizeof(int64_t),
+            BT_CUDA(cudaMemcpyAsync(n_alive_host, live + lv, sizeof(int64_t),
                                     cudaMemcpyDeviceToHost, st));
             BT_CUDA(cudaStreamSynchronize(st));
-            n_act = *n_alive_host;
-            std::swap(act_a, act_b);
+            bound = *n_alive_host;
             if (used >= batch) flush();
         }
         flush();

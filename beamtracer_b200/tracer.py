@@ -497,36 +497,52 @@ class TraceEngine:
         return (self.charge[0] / self.volumes.reshape(-1)).reshape(self.mesh.shape)
 
     def result(self, density=None) -> TraceResult:
-        """The trace as the reference returns it (host arrays; ``tracer.py:1265-1304``)."""
+        """The trace as the reference returns it (host arrays; ``tracer.py:1265-1304``).
+
+        The crossings are picked from the hit buffers and ordered (by step, then trajectory,
+        as ``tracer.py:1279-1290``) on the device, so only the crossings that exist come to
+        the host, in one copy with the trajectory of each.
+        """
+        import torch
+
         particles = self.particles
         current = particles.current.astype(float)
         species = particles.species
-        counts = self.counts.cpu().numpy()
-        hits = self.hits.cpu().numpy()
-        capacity = hits.shape[2]
-        slots = np.arange(capacity)
-        planes = []
-        for p, position in enumerate(self.planes):
-            k, c = np.nonzero(slots[None, :] < counts[:, p, None])
-            record = hits[k, p, c]
-            order = np.lexsort((k, record[:, 7]))
-            k, record = k[order], record[order]
+        n_planes = len(self.planes)
+        slots = torch.arange(self.hits.shape[2], device=self.hits.device)
+        pieces, sizes = [], []
+        for p in range(n_planes):
+            k, c = (slots[None, :] < self.counts[:, p, None]).nonzero(as_tuple=True)
+            record = self.hits[k, p, c]
+            order = torch.sort(record[:, 7], stable=True).indices
+            pieces.append(torch.cat([record[order], k[order, None].to(torch.float64)], dim=1))
+            sizes.append(int(k.numel()))
+        crossings = (torch.cat(pieces).cpu().numpy() if pieces else np.zeros((0, 9)))
+        ints = torch.stack([self.status, self.electrode, self.steps]).cpu().numpy()
+        status, electrode, steps = ints
+        planes, start = [], 0
+        for position, size in zip(self.planes, sizes):
+            record = crossings[start : start + size]
+            start += size
+            k = record[:, 8].astype(np.int64)
             plane = PlaneHits(position)
             plane.append(record[:, 0:3].T.copy(), record[:, 3:6].T.copy(), current[k],
                          species[k], record[:, 6].astype(np.int8))  # fmt: skip
             planes.append(plane)
-        paths = self.paths.cpu().numpy()
-        path_count = self.path_count.cpu().numpy()
-        status = self.status.cpu().numpy()
-        steps = self.steps.cpu().numpy()
+        if self.saved_ids.size:
+            paths = self.paths.cpu().numpy()
+            path_count = self.path_count.cpu().numpy()
+            trajectories = [paths[i, : path_count[i]].copy() for i in range(self.saved_ids.size)]
+        else:
+            trajectories = []
         if density is None:
             density = self.density()
         return TraceResult(
             charge_density=density.cpu().numpy() if hasattr(density, "cpu") else density,
             status=status.astype(np.int8),
-            electrode=self.electrode.cpu().numpy().astype(np.int32),
+            electrode=electrode.astype(np.int32),
             planes=planes,
-            trajectories=[paths[i, : path_count[i]].copy() for i in range(self.saved_ids.size)],
+            trajectories=trajectories,
             trajectory_species=species[self.saved_ids],
             steps=int(steps.max()) if steps.size else 0,
         )
