@@ -106,17 +106,16 @@ struct HostBuffer {
 
 // The scratch of the deterministic deposit (records, their radix sort, per-cell sums).
 struct DepositScratch {
-    Buffer keys, keys_alt, vals, vals_alt, u, w, q;
+    Buffer keys, keys_alt, vals, vals_alt, rec;
     Buffer hist, row_offsets, digit_base;
     Buffer cell_sums, warp_first, warp_last, warp_flags;
 };
 
-// The tracer's live-trajectory lists and its deposit records.
 // The tracer's scratch: the live lists and two record buffers, one filled by the trace
 // windows while the other's records are deposited on the side stream.
 struct TraceScratch {
     Buffer active_a, active_b, block_counts, n_alive;
-    Buffer rec_keys[2], rec_u[2], rec_w[2], rec_q[2];
+    Buffer rec_keys[2], rec[2];
     cudaStream_t side = nullptr;                 // the deposits' stream
     cudaEvent_t filled[2] = {nullptr, nullptr};  // a buffer's windows are traced
     cudaEvent_t drained[2] = {nullptr, nullptr}; // a buffer's records are deposited
@@ -228,11 +227,17 @@ struct NodeLayout {
     i64 n_nodes;
 };
 
+// A record's payload: the area weights and the charge, in one 32-byte sector so that the
+// reduction's gather through the sort permutation reads one sector per record.
+struct __align__(32) DepositRec {
+    double u, w, q, unused;
+};
+
 // n_records sizes the launches; n_dev, when not NULL, is the device-held count of the
 // records to deposit (at most n_records): the first ones, the rest ignored.
-void deposit_records(bt_ctx *ctx, const uint32_t *keys, const double *u, const double *w,
-                     const double *q, i64 n_records, const i64 *n_dev, uint32_t sentinel,
-                     double *charge, const NodeLayout &layout);
+void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i64 n_records,
+                     const i64 *n_dev, uint32_t sentinel, double *charge,
+                     const NodeLayout &layout);
 
 // Stable LSD radix sort of (key, index) pairs: sorted keys and the permutation.
 // Returns the device pointers of the sorted keys and values (inside the scratch).  n sizes

@@ -171,8 +171,7 @@ __global__ void radix_scatter(const uint32_t *__restrict__ keys_in,
 // (`tail` set when that segment ends in the warp), `last` its trailing piece of a segment
 // that begins in the warp and continues (`owner` set).
 __global__ void seg_reduce_warps(const uint32_t *__restrict__ K, const uint32_t *__restrict__ I,
-                                 const double *__restrict__ U, const double *__restrict__ W,
-                                 const double *__restrict__ Q, i64 R_host,
+                                 const DepositRec *__restrict__ rec, i64 R_host,
                                  const i64 *__restrict__ R_dev, uint32_t sentinel,
                                  double4 *__restrict__ cells, double4 *__restrict__ first,
                                  double4 *__restrict__ last, uint8_t *__restrict__ tail_flag,
@@ -186,8 +185,8 @@ __global__ void seg_reduce_warps(const uint32_t *__restrict__ K, const uint32_t 
     const bool valid = key < sentinel;
     double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
     if (valid) {
-        const uint32_t idx = I[r];
-        const double u = U[idx], w = W[idx], q = Q[idx];
+        const DepositRec p = rec[I[r]];
+        const double u = p.u, w = p.w, q = p.q;
         c00 = (1.0 - u) * (1.0 - w) * q;
         c01 = (1.0 - u) * w * q;
         c10 = u * (1.0 - w) * q;
@@ -290,8 +289,7 @@ __global__ void node_accumulate(const double4 *__restrict__ cells, double *__res
 __global__ void point_records(const double *__restrict__ px, const double *__restrict__ py,
                               const double *__restrict__ q, i64 n, double origin_x,
                               double origin_y, double h, i64 cylindrical, i64 nx, i64 ny,
-                              uint32_t *__restrict__ keys, double *__restrict__ U,
-                              double *__restrict__ W, double *__restrict__ Q) {
+                              uint32_t *__restrict__ keys, DepositRec *__restrict__ rec) {
     const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const double x = px[k], y = py[k];
@@ -321,9 +319,7 @@ __global__ void point_records(const double *__restrict__ px, const double *__res
         j = ny - 2;
     }
     keys[k] = (uint32_t)(i * ny + j);
-    U[k] = t;
-    W[k] = u;
-    Q[k] = q[k];
+    rec[k] = DepositRec{t, u, q[k], 0.0};
 }
 
 int bits_for(uint64_t max_key) {
@@ -385,9 +381,9 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_
     *vals_out = const_cast<uint32_t *>(src_v);
 }
 
-void deposit_records(bt_ctx *ctx, const uint32_t *keys, const double *u, const double *w,
-                     const double *q, i64 n_records, const i64 *n_dev, uint32_t sentinel,
-                     double *charge, const NodeLayout &layout) {
+void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i64 n_records,
+                     const i64 *n_dev, uint32_t sentinel, double *charge,
+                     const NodeLayout &layout) {
     if (n_records == 0) return;
     DepositScratch &s = ctx->deposit;
     cudaStream_t st = ctx->stream;
@@ -401,7 +397,7 @@ void deposit_records(bt_ctx *ctx, const uint32_t *keys, const double *u, const d
     BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * layout.n_nodes, st));
     const int threads = 256;
     BT_LAUNCH(ctx, seg_reduce_warps, blocks_for(n_warps * 32, threads), threads, 0, st, sk, sv,
-              u, w, q, n_records, n_dev, sentinel, cells, first, last, flags, flags + n_warps);
+              rec, n_records, n_dev, sentinel, cells, first, last, flags, flags + n_warps);
     BT_LAUNCH(ctx, seg_reduce_chains, blocks_for(n_warps, threads), threads, 0, st, sk, n_records,
               n_dev, cells, first, last, flags, flags + n_warps);
     BT_LAUNCH(ctx, node_accumulate, blocks_for(layout.n_nodes, threads), threads, 0, st, cells, charge, layout.patch_int, layout.n_patches, layout.nx, layout.ny,
@@ -424,12 +420,13 @@ extern "C" int bt_deposit_trajectories_2d(bt_ctx *ctx, const double *px, const d
         BT_REQUIRE(px && py && q && charge, "deposit: null array");
         bt::DepositScratch &s = ctx->deposit;
         uint32_t *keys = s.keys.as<uint32_t>(n);
-        double *U = s.u.as<double>(n), *W = s.w.as<double>(n), *Q = s.q.as<double>(n);
-        BT_LAUNCH(ctx, bt::point_records, bt::blocks_for(n, 256), 256, 0, ctx->stream, px, py, q, n, origin_x, origin_y, h, cylindrical, nx, ny, keys, U, W, Q);
+        bt::DepositRec *rec = s.rec.as<bt::DepositRec>(n);
+        BT_LAUNCH(ctx, bt::point_records, bt::blocks_for(n, 256), 256, 0, ctx->stream, px, py,
+                  q, n, origin_x, origin_y, h, cylindrical, nx, ny, keys, rec);
         BT_CHECK_LAUNCH();
         // the records' keys live in `keys`; the sort reads them and writes elsewhere
         bt::NodeLayout layout{nullptr, 1, nx, ny, nx * ny};
-        bt::deposit_records(ctx, keys, U, W, Q, n, nullptr, (uint32_t)(nx * ny), charge, layout);
+        bt::deposit_records(ctx, keys, rec, n, nullptr, (uint32_t)(nx * ny), charge, layout);
     });
 }
 
@@ -455,8 +452,8 @@ constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
 // the carving of the static array, in bytes
 constexpr size_t kOffKeys = 0;  // keys, keys_alt, vals, vals_alt (u32)
-constexpr size_t kOffPayload = kOffKeys + align256(4 * 4 * kNoallocPoints);  // u, w, q
-constexpr size_t kOffHist = kOffPayload + align256(3 * 8 * kNoallocPoints);  // hist, offs
+constexpr size_t kOffPayload = kOffKeys + align256(4 * 4 * kNoallocPoints);  // records
+constexpr size_t kOffHist = kOffPayload + align256(32 * kNoallocPoints);  // hist, offs
 constexpr size_t kOffDigits = kOffHist + align256(2 * 4 * kRadix * kNoallocBlocks);
 constexpr size_t kOffCells = kOffDigits + align256(2 * 4 * kRadix);
 constexpr size_t kOffWarps = kOffCells + align256(32 * kNoallocNodes);  // first, last
@@ -509,9 +506,7 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
         uint32_t *keys_alt = keys + kNoallocPoints;
         uint32_t *vals = keys_alt + kNoallocPoints;
         uint32_t *vals_alt = vals + kNoallocPoints;
-        double *U = reinterpret_cast<double *>(base + kOffPayload);
-        double *W = U + kNoallocPoints;
-        double *Q = W + kNoallocPoints;
+        DepositRec *rec = reinterpret_cast<DepositRec *>(base + kOffPayload);
         uint32_t *hist = reinterpret_cast<uint32_t *>(base + kOffHist);
         uint32_t *offs = hist + kRadix * kNoallocBlocks;
         uint32_t *digit = reinterpret_cast<uint32_t *>(base + kOffDigits);
@@ -523,7 +518,7 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
         const uint32_t sentinel = (uint32_t)(nx * ny);
 
         point_records<<<blocks_for(n, 256), 256, 0, st>>>(px, py, q, n, origin_x, origin_y, h,
-                                                          cylindrical, nx, ny, keys, U, W, Q);
+                                                          cylindrical, nx, ny, keys, rec);
         // the stable radix sort, ping-ponging between the key and value arrays
         const int nblocks = (int)((n + kTile - 1) / kTile);
         const int passes = (bits_for(sentinel) + 7) / 8;
@@ -553,7 +548,7 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
         const i64 n_warps = (n + 31) / 32;
         BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * n_nodes, st));
         seg_reduce_warps<<<blocks_for(n_warps * 32, 256), 256, 0, st>>>(
-            src_k, src_v, U, W, Q, n, nullptr, sentinel, cells, first, last, flags,
+            src_k, src_v, rec, n, nullptr, sentinel, cells, first, last, flags,
             flags + n_warps);
         seg_reduce_chains<<<blocks_for(n_warps, 256), 256, 0, st>>>(
             src_k, n, nullptr, cells, first, last, flags, flags + n_warps);

@@ -953,69 +953,151 @@ TailLayout tail_layout(const std::vector<Level> &levels, int first) {
     return T;
 }
 
-// -- dot products: partial sums per block, then an ordered sum (deterministic) -----------
+// -- dot products: partial sums per block, the last block adds them in block order --------
 
-constexpr int kDotMax = 32;     // at most this many vectors against one
+constexpr int kDotMax = 32;      // at most this many vectors against one
 constexpr int kDotBlocks = 296;  // two per SM
 constexpr int kDotThreads = 256;
 
-// partial[block * kDotMax + q] = the block's share of sum_f V[q n + f] w[f], q < m
-__global__ void __launch_bounds__(kDotThreads) multi_dot_partial(
-    const double *__restrict__ V, const double *__restrict__ w, i64 n, int m,
-    double *__restrict__ partial) {
-    __shared__ double warp_part[kDotThreads / 32][kDotMax];
-    double acc[kDotMax];
+// What a dot pass does: the sums out[q] = <V_q, w> (kPlain), or first w -= sum_q h[q] V_q
+// (classical Gram-Schmidt's orthogonalisation, written back to w) and then the sums
+// <V_q, w> (kOrthDots) or <w, w> (kOrthNorm) of the new w, q < m.  Every thread adds its
+// grid-stride elements in order, the warps and blocks are added in a fixed order, and the
+// block that finishes last (a ticket counter, reset by it) adds the blocks' partials in
+// block order: the same bits on every run, in one launch.
+enum DotMode { kPlain = 0, kOrthDots = 1, kOrthNorm = 2 };
+
+template <int MQ, int MODE>
+__global__ void __launch_bounds__(kDotThreads) dot_pass(
+    const double *__restrict__ V, const double *__restrict__ h, double *w, i64 n, int m,
+    double *__restrict__ partial, unsigned *__restrict__ ticket, double *__restrict__ out) {
+    constexpr int NACC = MODE == kOrthNorm ? 1 : MQ;
+    __shared__ double warp_part[kDotThreads / 32][NACC];
+    __shared__ bool is_last;
+    const int sums = MODE == kOrthNorm ? 1 : m;
+    double acc[NACC];
 #pragma unroll
-    for (int q = 0; q < kDotMax; ++q) acc[q] = 0.0;
-    for (i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x; f < n; f += (i64)gridDim.x * blockDim.x) {
-        const double wf = w[f];
+    for (int q = 0; q < NACC; ++q) acc[q] = 0.0;
+    for (i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x; f < n;
+         f += (i64)gridDim.x * blockDim.x) {
+        double s = w[f];
+        if (MODE == kPlain) {
 #pragma unroll
-        for (int q = 0; q < kDotMax; ++q)
-            if (q < m) acc[q] += V[(i64)q * n + f] * wf;
+            for (int q = 0; q < MQ; ++q)
+                if (q < m) acc[q] += V[(i64)q * n + f] * s;
+        } else {
+            double vq[MQ];
+#pragma unroll
+            for (int q = 0; q < MQ; ++q)
+                if (q < m) {
+                    vq[q] = V[(i64)q * n + f];
+                    s -= h[q] * vq[q];
+                }
+            w[f] = s;
+            if (MODE == kOrthDots) {
+#pragma unroll
+                for (int q = 0; q < MQ; ++q)
+                    if (q < m) acc[q] += vq[q] * s;
+            } else {
+                acc[0] += s * s;
+            }
+        }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int q = 0; q < kDotMax; ++q) {
+    for (int q = 0; q < NACC; ++q) {
+        if (q >= sums) break;
         double v = acc[q];
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
         if (lane == 0) warp_part[warp][q] = v;
     }
     __syncthreads();
-    if (threadIdx.x < kDotMax) {
+    if (threadIdx.x < sums) {
         double v = 0.0;
         for (int wi = 0; wi < kDotThreads / 32; ++wi) v += warp_part[wi][threadIdx.x];
         partial[(i64)blockIdx.x * kDotMax + threadIdx.x] = v;
     }
-}
-
-// out[q] = the blocks' partials of q summed in a fixed order: each of 8 warps sums a
-// strided eighth of the blocks for every q, then the eight sums are added in order.
-__global__ void multi_dot_final(const double *__restrict__ partial, int blocks, int m,
-                                double *__restrict__ out) {
-    __shared__ double part[8][kDotMax];
-    const int q = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double v = 0.0;
-    if (q < m)
-        for (int bi = warp; bi < blocks; bi += 8) v += partial[(i64)bi * kDotMax + q];
-    part[warp][q] = v;
+    __threadfence();
     __syncthreads();
-    if (warp == 0 && q < m) {
-        double s = 0.0;
-        for (int w = 0; w < 8; ++w) s += part[w][q];
-        out[q] = s;
+    if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    // the last block: warp w adds the blocks' partials of q = w, w + 8, ... (lanes stride
+    // the blocks, then a fixed tree)
+    for (int q = warp; q < sums; q += kDotThreads / 32) {
+        double v = 0.0;
+        for (int b = lane; b < (int)gridDim.x; b += 32) v += __ldcg(partial + (i64)b * kDotMax + q);
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) out[q] = v;
     }
+    if (threadIdx.x == 0) *ticket = 0u;
 }
 
 // -- vector kernels of GMRES and Newton ----------------------------------------------------
 
-// w -= sum_q h[q] V[q]
-__global__ void orthogonalise(const double *__restrict__ V, const double *__restrict__ hcol, int m,
-                              i64 n, double *__restrict__ w) {
-    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= n) return;
-    double s = w[f];
-    for (int q = 0; q < m; ++q) s -= hcol[q] * V[(i64)q * n + f];
-    w[f] = s;
+// The Arnoldi process of one GMRES restart cycle, on the device: the Hessenberg matrix H
+// ((m + 1) x m, row-major), the Givens rotations (cs, sn) and the rotated right-hand side
+// g.  `j` counts the steps taken; once `done` (the residual estimate |g[j]| at the
+// tolerance, or a breakdown) later steps change nothing, so the host may queue steps past
+// the end and the cycle's solution is the same.
+struct Arnoldi {
+    int j, done;
+    double tol;
+    double resid[kDotMax + 1];  // |g[j]| after step j
+};
+
+__global__ void arnoldi_begin(Arnoldi *__restrict__ a, double *__restrict__ g, int m,
+                              double beta, double tol) {
+    if (threadIdx.x != 0) return;
+    a->j = 0;
+    a->done = 0;
+    a->tol = tol;
+    a->resid[0] = beta;
+    g[0] = beta;
+    for (int q = 1; q <= m; ++q) g[q] = 0.0;
+}
+
+// Step j: the new Hessenberg column from the two Gram-Schmidt passes' coefficients h1, h2
+// and the new vector's squared norm, rotated by the earlier rotations; the new rotation and
+// g, whose last entry is the residual norm up to its sign.
+__global__ void arnoldi_step(Arnoldi *__restrict__ a, double *__restrict__ H,
+                             double *__restrict__ cs, double *__restrict__ sn,
+                             double *__restrict__ g, const double *__restrict__ h1,
+                             const double *__restrict__ h2, const double *__restrict__ norm2,
+                             int j, int m) {
+    if (threadIdx.x != 0 || a->done || a->j != j) return;
+    for (int q = 0; q <= j; ++q) H[q * m + j] = h1[q] + h2[q];
+    const double hn = sqrt(norm2[0]);
+    H[(j + 1) * m + j] = hn;
+    for (int q = 0; q < j; ++q) {
+        const double x = H[q * m + j], y = H[(q + 1) * m + j];
+        H[q * m + j] = cs[q] * x + sn[q] * y;
+        H[(q + 1) * m + j] = -sn[q] * x + cs[q] * y;
+    }
+    const double x = H[j * m + j], y = H[(j + 1) * m + j];
+    const double rr = hypot(x, y);
+    cs[j] = rr > 0.0 ? x / rr : 1.0;
+    sn[j] = rr > 0.0 ? y / rr : 0.0;
+    H[j * m + j] = rr;
+    H[(j + 1) * m + j] = 0.0;
+    g[j + 1] = -sn[j] * g[j];
+    g[j] = cs[j] * g[j];
+    a->j = j + 1;
+    a->resid[j + 1] = fabs(g[j + 1]);
+    if (fabs(g[j + 1]) <= a->tol || hn == 0.0) a->done = 1;
+}
+
+// y = H^-1 g on the leading j x j upper triangle (j the steps taken)
+__global__ void arnoldi_solve(const Arnoldi *__restrict__ a, const double *__restrict__ H,
+                              const double *__restrict__ g, double *__restrict__ y, int m) {
+    if (threadIdx.x != 0) return;
+    const int j = a->j;
+    for (int q = j - 1; q >= 0; --q) {
+        double s = g[q];
+        for (int c = q + 1; c < j; ++c) s -= H[q * m + c] * y[c];
+        y[q] = s / H[q * m + q];
+    }
 }
 
 // v = w / sqrt(norm2[0]) (zero for a zero norm: GMRES stops there)
@@ -1032,11 +1114,12 @@ __global__ void scale_into(const double *__restrict__ w, double a, i64 n, double
     if (f < n) v[f] = a * w[f];
 }
 
-// x += sum_q y[q] Z[q]
-__global__ void combine(const double *__restrict__ Z, const double *__restrict__ y, int m, i64 n,
-                        double *__restrict__ x) {
+// x += sum_q y[q] Z[q], q below the cycle's steps
+__global__ void combine(const double *__restrict__ Z, const double *__restrict__ y,
+                        const Arnoldi *__restrict__ a, i64 n, double *__restrict__ x) {
     const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= n) return;
+    const int m = a->j;
     double s = x[f];
     for (int q = 0; q < m; ++q) s += y[q] * Z[(i64)q * n + f];
     x[f] = s;
@@ -1178,6 +1261,9 @@ struct bt_poisson {
     bt::Buffer tail_plans;   // and TailPlan layouts
     bt::Buffer tail_image;   // the static part of its shared memory (tail_words 16-byte words)
     bt::Buffer dot_partial;  // per-block partial dot products
+    bt::Buffer dot_ticket;   // the dot passes' finishing-block counter (zero between passes)
+    bool ticket_ready = false;
+    bt::Buffer arnoldi;      // the device Arnoldi state of GMRES (bt::Arnoldi, H, rotations)
     // the V-cycle from a zero guess on level 0's b into its x, captured once as a graph
     cudaGraph_t vgraph = nullptr;
     cudaGraphExec_t vexec = nullptr;
@@ -1186,10 +1272,10 @@ struct bt_poisson {
         if (vexec) cudaGraphExecDestroy(vexec);
         if (vgraph) cudaGraphDestroy(vgraph);
     }
-    // GMRES: the Krylov basis V, its preconditioned images Z, two work vectors, the
-    // Hessenberg column and the solution's coefficients; the solve: its right-hand side,
-    // the residual GMRES reduces, the correction, the Newton reaction and scalars.
-    bt::Buffer V, Z, work, work2, hcol, ycoef, rhs, r0, delta, reaction, scalars;
+    // GMRES: the Krylov basis V, its preconditioned images Z, two work vectors; the solve:
+    // its right-hand side, the residual GMRES reduces, the correction, the Newton reaction
+    // and scalars.
+    bt::Buffer V, Z, work, work2, rhs, r0, delta, reaction, scalars;
 };
 
 namespace bt {
@@ -1519,12 +1605,34 @@ double read_scalar(bt_poisson *p, const double *dev) {
     return host[0];
 }
 
+// One dot pass (dot_pass) over the n-vectors w and V's rows q < m; out gets its sums.
+template <int MODE>
+void dot_launch(bt_poisson *p, const double *V, const double *h, double *w, int m, double *out) {
+    double *partial = p->dot_partial.as<double>((size_t)kDotBlocks * kDotMax);
+    unsigned *ticket = p->dot_ticket.as<unsigned>(1);
+    cudaStream_t st = p->ctx->stream;
+    if (!p->ticket_ready) {
+        BT_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st));
+        p->ticket_ready = true;
+    }
+    BT_REQUIRE(m >= 1 && m <= kDotMax, "poisson: a dot pass takes 1 to 32 vectors");
+#define BT_DOT(MQ)                                                                              \
+    BT_LAUNCH(p->ctx, (dot_pass<MQ, MODE>), kDotBlocks, kDotThreads, 0, st, V, h, w, p->n, m,  \
+              partial, ticket, out)
+    if (m <= 1)
+        BT_DOT(1);
+    else if (m <= 8)
+        BT_DOT(8);
+    else if (m <= 16)
+        BT_DOT(16);
+    else
+        BT_DOT(32);
+#undef BT_DOT
+}
+
 // out[q] = <V_q, w> for q < m (V's rows of n values), deterministic
 void dots(bt_poisson *p, const double *V, const double *w, int m, double *out) {
-    double *partial = p->dot_partial.as<double>((size_t)kDotBlocks * kDotMax);
-    BT_LAUNCH(p->ctx, multi_dot_partial, kDotBlocks, kDotThreads, 0, p->ctx->stream, V, w, p->n, m,
-              partial);
-    BT_LAUNCH(p->ctx, multi_dot_final, 1, 256, 0, p->ctx->stream, partial, kDotBlocks, m, out);
+    dot_launch<kPlain>(p, V, nullptr, const_cast<double *>(w), m, out);
 }
 
 double norm2(bt_poisson *p, const double *v) {
@@ -1533,9 +1641,26 @@ double norm2(bt_poisson *p, const double *v) {
     return std::sqrt(read_scalar(p, s));
 }
 
+// The steps a cycle still needs by the rate of its last (up to three) steps, one fewer so
+// that a queued step rarely runs past the end: at least 1.
+int steps_to_queue(const Arnoldi &a) {
+    const int j = a.j;
+    const int k = std::min(j, 3);
+    const double r = a.resid[j];
+    if (k == 0 || !(r > 0.0) || !(a.resid[j - k] > 0.0)) return 1;
+    const double rate = std::pow(r / a.resid[j - k], 1.0 / k);
+    if (!(rate < 0.95)) return 1;
+    const double left = std::log(a.tol / r) / std::log(rate);
+    if (!(left < 1e6)) return 1;
+    return std::max(1, (int)std::ceil(left) - 1);
+}
+
 // Solve A d = r0 for d (d zero on entry) by restarted right-preconditioned GMRES until
-// ||r0 - A d|| <= abs_tol or max_iter V-cycles; returns the V-cycles and the final
-// residual norm.
+// ||r0 - A d|| <= abs_tol or max_iter V-cycles; returns the V-cycles run and the final
+// residual norm.  The Arnoldi process runs on the device (Gram-Schmidt twice, the Givens
+// rotations in arnoldi_step); the host queues steps in batches sized by the residual's
+// rate and reads the state between them, and the cycle's solution is the same as if it
+// read it after every step.
 int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_iter,
           double *final_norm) {
     const i64 n = p->n;
@@ -1544,12 +1669,15 @@ int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_it
     double *V = p->V.as<double>((size_t)(m + 1) * n);
     double *Z = p->Z.as<double>((size_t)m * n);
     double *w = p->work.as<double>(n);
-    // the Hessenberg column's two Gram-Schmidt passes and the new vector's squared norm
-    double *hdev = p->hcol.as<double>(2 * (m + 2) + 2);
-    double *hdev2 = hdev + (m + 2), *hnorm = hdev + 2 * (m + 2);
-    double *ydev = p->ycoef.as<double>(m + 2);
-    double *host = static_cast<double *>(p->ctx->host.get(sizeof(double) * (2 * (m + 2) + 2)));
-    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    // the device state: Arnoldi, H, cs, sn, g, y and the passes' coefficients and norm
+    const size_t head = (sizeof(Arnoldi) + 255) / 256 * 256;
+    const size_t doubles = (size_t)(m + 1) * m + 3 * m + 1 + 2 * (m + 2) + 1;
+    unsigned char *state = p->arnoldi.as<unsigned char>(head + sizeof(double) * doubles);
+    Arnoldi *a = reinterpret_cast<Arnoldi *>(state);
+    double *H = reinterpret_cast<double *>(state + head);
+    double *cs = H + (size_t)(m + 1) * m, *sn = cs + m, *g = sn + m, *y = g + m + 1;
+    double *h1 = y + m, *h2 = h1 + (m + 2), *hn = h2 + (m + 2);
+    Arnoldi *host = static_cast<Arnoldi *>(p->ctx->host.get(sizeof(Arnoldi)));
     int total = 0;
     BT_CUDA(cudaMemcpyAsync(w, r0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     double beta = norm2(p, w);
@@ -1560,53 +1688,30 @@ int gmres(bt_poisson *p, const double *r0, double *d, double abs_tol, int max_it
         previous = beta;
         if (!std::isfinite(beta)) throw Error{BT_ERR_NOCONV, "field solve: the residual is not finite"};
         BT_LAUNCH(p->ctx, scale_into, blocks_for(n, 256), 256, 0, st, w, 1.0 / beta, n, V);
-        std::fill(g.begin(), g.end(), 0.0);
-        g[0] = beta;
-        int j = 0;
-        while (j < m && total < max_iter) {
-            double *v = V + (i64)j * n, *z = Z + (i64)j * n;
-            precondition(p, v, z);
-            apply(p, z, w);
-            // classical Gram-Schmidt applied twice, the new basis vector normalised on the
-            // device; one read-back of the column and the norm
-            dots(p, V, w, j + 1, hdev);
-            BT_LAUNCH(p->ctx, orthogonalise, blocks_for(n, 256), 256, 0, st, V, hdev, j + 1, n, w);
-            dots(p, V, w, j + 1, hdev2);
-            BT_LAUNCH(p->ctx, orthogonalise, blocks_for(n, 256), 256, 0, st, V, hdev2, j + 1, n, w);
-            dots(p, w, w, 1, hnorm);
-            BT_LAUNCH(p->ctx, scale_by_norm, blocks_for(n, 256), 256, 0, st, w, hnorm, n,
-                      V + (i64)(j + 1) * n);
-            BT_CUDA(cudaMemcpyAsync(host, hdev, sizeof(double) * (2 * (m + 2) + 1),
-                                    cudaMemcpyDeviceToHost, st));
-            BT_CUDA(cudaStreamSynchronize(st));
-            for (int q = 0; q <= j; ++q) H[q * m + j] = host[q] + host[(m + 2) + q];
-            const double hn = std::sqrt(host[2 * (m + 2)]);
-            H[(j + 1) * m + j] = hn;
-            for (int q = 0; q < j; ++q) {
-                const double a = H[q * m + j], b = H[(q + 1) * m + j];
-                H[q * m + j] = cs[q] * a + sn[q] * b;
-                H[(q + 1) * m + j] = -sn[q] * a + cs[q] * b;
+        BT_LAUNCH(p->ctx, arnoldi_begin, 1, 32, 0, st, a, g, m, beta, abs_tol);
+        int j = 0, batch = 2;
+        for (;;) {
+            const int count = std::min(batch, std::min(m - j, max_iter - total));
+            for (int b = 0; b < count; ++b, ++j, ++total) {
+                double *v = V + (i64)j * n, *z = Z + (i64)j * n;
+                precondition(p, v, z);
+                apply(p, z, w);
+                dot_launch<kPlain>(p, V, nullptr, w, j + 1, h1);
+                dot_launch<kOrthDots>(p, V, h1, w, j + 1, h2);
+                dot_launch<kOrthNorm>(p, V, h2, w, j + 1, hn);
+                BT_LAUNCH(p->ctx, scale_by_norm, blocks_for(n, 256), 256, 0, st, w, hn, n,
+                          V + (i64)(j + 1) * n);
+                BT_LAUNCH(p->ctx, arnoldi_step, 1, 32, 0, st, a, H, cs, sn, g, h1, h2, hn, j, m);
             }
-            const double a = H[j * m + j], b = H[(j + 1) * m + j];
-            const double rr = std::hypot(a, b);
-            cs[j] = rr > 0.0 ? a / rr : 1.0;
-            sn[j] = rr > 0.0 ? b / rr : 0.0;
-            H[j * m + j] = rr;
-            H[(j + 1) * m + j] = 0.0;
-            g[j + 1] = -sn[j] * g[j];
-            g[j] = cs[j] * g[j];
-            ++j;
-            ++total;
-            if (std::fabs(g[j]) <= abs_tol || hn == 0.0) break;
+            BT_CHECK_LAUNCH();
+            BT_CUDA(cudaMemcpyAsync(host, a, sizeof(Arnoldi), cudaMemcpyDeviceToHost, st));
+            BT_CUDA(cudaStreamSynchronize(st));
+            if (host->done || j >= m || total >= max_iter) break;
+            batch = steps_to_queue(*host);
         }
-        // y = H^-1 g on the j x j upper triangle, then d += Z y
-        for (int q = j - 1; q >= 0; --q) {
-            double s = g[q];
-            for (int c = q + 1; c < j; ++c) s -= H[q * m + c] * y[c];
-            y[q] = s / H[q * m + q];
-        }
-        BT_CUDA(cudaMemcpyAsync(ydev, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, st));
-        BT_LAUNCH(p->ctx, combine, blocks_for(n, 256), 256, 0, st, Z, ydev, j, n, d);
+        // d += Z y, y = H^-1 g over the steps taken
+        BT_LAUNCH(p->ctx, arnoldi_solve, 1, 32, 0, st, a, H, g, y, m);
+        BT_LAUNCH(p->ctx, combine, blocks_for(n, 256), 256, 0, st, Z, y, a, n, d);
         // the true residual r0 - A d
         apply(p, d, w);
         BT_LAUNCH(p->ctx, subtract_from, blocks_for(n, 256), 256, 0, st, r0, n, w);

@@ -222,8 +222,8 @@ __device__ __forceinline__ double inv_gamma(double u0, double u1, double u2, dou
 template <int CYL, int INTEG, bool GENERAL, bool MAG>
 __global__ void __launch_bounds__(128, 1)
     trace_window(Trace tr, const i64 *__restrict__ act, const i64 *__restrict__ live, i64 stride,
-                 int S, uint32_t *__restrict__ keys, double *__restrict__ RU,
-                 double *__restrict__ RW, double *__restrict__ RQ, uint32_t sentinel,
+                 int S, uint32_t *__restrict__ keys, DepositRec *__restrict__ rec,
+                 uint32_t sentinel,
                  i64 *__restrict__ records_end, i64 end) {
     const i64 m = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     const i64 n_act = *live;
@@ -536,9 +536,7 @@ __global__ void __launch_bounds__(128, 1)
             }
             const i64 r = (i64)s * stride + m;
             keys[r] = (uint32_t)(g.ofn + (i64)i * pny + j);
-            RU[r] = u;
-            RW[r] = w;
-            RQ[r] = dqk * dt;
+            rec[r] = DepositRec{u, w, dqk * dt, 0.0};
         }
         ns = ns + 1;
 
@@ -776,12 +774,10 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         const int64_t batch = std::min<int64_t>(kBatchRecords, 16 * per_window);
         const int64_t capacity = per_window + batch;
         uint32_t *keys[2];
-        double *RU[2], *RW[2], *RQ[2];
+        bt::DepositRec *rec[2];
         for (int b = 0; b < 2; ++b) {
             keys[b] = ts.rec_keys[b].as<uint32_t>(capacity);
-            RU[b] = ts.rec_u[b].as<double>(capacity);
-            RW[b] = ts.rec_w[b].as<double>(capacity);
-            RQ[b] = ts.rec_q[b].as<double>(capacity);
+            rec[b] = ts.rec[b].as<bt::DepositRec>(capacity);
         }
         if (!ts.side) {
             BT_CUDA(cudaStreamCreateWithFlags(&ts.side, cudaStreamNonBlocking));
@@ -816,8 +812,8 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
             {
                 SideStream on_side(ctx, ts.side);
                 bt::Timed timed(ctx, "deposit");
-                bt::deposit_records(ctx, keys[cur], RU[cur], RW[cur], RQ[cur], used,
-                                    records_end + cur, sentinel, a.charge, layout);
+                bt::deposit_records(ctx, keys[cur], rec[cur], used, records_end + cur, sentinel,
+                                    a.charge, layout);
             }
             BT_CUDA(cudaMemsetAsync(records_end + cur, 0, sizeof(int64_t), ts.side));
             BT_CUDA(cudaEventRecord(ts.drained[cur], ts.side));
@@ -842,8 +838,8 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
     if (a.cylindrical == C && (a.integrator != 0) == (I != 0) && general == G &&                 \
         (mag != nullptr) == M)                                                                   \
         BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M>), grid, 128, 0, st, tr, act_a, live + lv,   \
-                  bound, S, keys[cur] + used, RU[cur] + used, RW[cur] + used, RQ[cur] + used,    \
-                  sentinel, records_end + cur, used + need);
+                  bound, S, keys[cur] + used, rec[cur] + used, sentinel, records_end + cur,       \
+                  used + need);
                     BT_TRACE_CASE(0, 0, false, false) BT_TRACE_CASE(0, 0, true, false)
                     BT_TRACE_CASE(0, 1, false, false) BT_TRACE_CASE(0, 1, true, false)
                     BT_TRACE_CASE(1, 0, false, false) BT_TRACE_CASE(1, 0, true, false)
