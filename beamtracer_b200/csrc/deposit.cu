@@ -112,56 +112,102 @@ __global__ void radix_digit_base(const uint32_t *__restrict__ totals, uint32_t *
     }
 }
 
-// Stable scatter of one tile: items in the order i * kThreads + t keep their order among
-// equal digits (warp ranks by __match_any_sync, warps in order by a per-digit prefix).
+// Stable scatter of one tile of kTile records.  Warp w ranks the tile's items
+// [w * kTile / kWarps, (w + 1) * kTile / kWarps) in order, 32 at a time (peers of a digit
+// by __match_any_sync, a running count per warp and digit in shared memory: no block
+// barrier in the loop); the counts are then turned into per-warp offsets in warp order and
+// the tile's digit starts, the tile is sorted by digit in shared memory, and written out in
+// order, so that the records of one digit go to consecutive addresses (coalesced runs).
+// The shared array first holds the counts, then the sorted tile.
 template <int R>
-__global__ void radix_scatter(const uint32_t *__restrict__ keys_in,
-                              const uint32_t *__restrict__ vals_in, i64 n_host,
-                              const i64 *__restrict__ n_dev, int shift,
-                              const uint32_t *__restrict__ offs,
-                              const uint32_t *__restrict__ base, int nblocks,
-                              uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out) {
-    __shared__ uint32_t wcount[kWarps][R];
-    __shared__ uint32_t woff[kWarps][R];
-    __shared__ uint32_t run[R];
+__global__ void __launch_bounds__(kThreads) radix_scatter(
+    const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, i64 n_host,
+    const i64 *__restrict__ n_dev, int shift, const uint32_t *__restrict__ offs,
+    const uint32_t *__restrict__ base, int nblocks, uint32_t *__restrict__ keys_out,
+    uint32_t *__restrict__ vals_out) {
+    static_assert(kWarps * R * 4 <= kTile * 8, "the counts must fit the tile's space");
+    constexpr int D = R / kThreads;             // digits a thread scans
+    constexpr int kPerWarp = kTile / kWarps;    // items a warp ranks
+    __shared__ __align__(16) uint32_t space[2 * kTile];  // counts [kWarps][R], then the tile
+    __shared__ uint32_t start[R];               // the tile's first slot of each digit
+    __shared__ uint32_t run[R];                 // the digit's first global slot for this tile
+    __shared__ uint32_t warp_sums[kWarps];
+    uint32_t *count = space;
     const i64 n = record_count(n_host, n_dev);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    for (int d = t; d < R; d += kThreads) {
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) wcount[w][d] = 0;
-        run[d] = base[d] + offs[(i64)d * nblocks + blockIdx.x];
-    }
+    for (int d = t; d < kWarps * R; d += kThreads) count[d] = 0;
     __syncthreads();
     const i64 tile = (i64)blockIdx.x * kTile;
     const unsigned below = (1u << lane) - 1u;
-    for (int i = 0; i < kItems; ++i) {
-        const i64 r = tile + (i64)i * kThreads + t;
-        const bool valid = r < n;
-        const uint32_t key = valid ? keys_in[r] : 0u;
-        const uint32_t d = (key >> shift) & (R - 1);
-        const uint32_t val = valid ? (vals_in ? vals_in[r] : (uint32_t)r) : 0u;
-        const unsigned peers = __match_any_sync(kFull, valid ? d : 0xffffffffu);
-        const int rank = __popc(peers & below);
-        if (valid && rank == 0) wcount[warp][d] = __popc(peers);
-        __syncthreads();
-        for (int dd = t; dd < R; dd += kThreads) {
-            uint32_t acc = run[dd];
+    uint32_t key[kItems], val[kItems], pos[kItems];
 #pragma unroll
-            for (int w = 0; w < kWarps; ++w) {
-                const uint32_t c = wcount[w][dd];
-                woff[w][dd] = acc;
-                acc += c;
-                wcount[w][dd] = 0;
-            }
-            run[dd] = acc;
+    for (int i = 0; i < kItems; ++i) {
+        const i64 r = tile + (i64)warp * kPerWarp + (i64)i * 32 + lane;
+        const bool valid = r < n;
+        key[i] = valid ? keys_in[r] : 0xffffffffu;
+        val[i] = valid ? (vals_in ? vals_in[r] : (uint32_t)r) : 0u;
+        const uint32_t d = (key[i] >> shift) & (R - 1);
+        const unsigned peers = __match_any_sync(kFull, valid ? d : 0xffffffffu);
+        uint32_t *c = count + warp * R + d;
+        const uint32_t before = valid ? *c : 0u;
+        pos[i] = before + __popc(peers & below);
+        __syncwarp();
+        if (valid && (peers & below) == 0) *c = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: the warps' counts to offsets in warp order, the digit's total
+    uint32_t total[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int d = t * D + k;
+        uint32_t acc = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = count[w * R + d];
+            count[w * R + d] = acc;
+            acc += c;
         }
-        __syncthreads();
-        if (valid) {
-            const uint32_t pos = woff[warp][d] + (uint32_t)rank;
-            keys_out[pos] = key;
-            vals_out[pos] = val;
+        total[k] = acc;
+    }
+    uint32_t v = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) v += total[k];
+    uint32_t first = block_inclusive_scan(v, warp_sums) - v;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int d = t * D + k;
+        start[d] = first;
+        run[d] = base[d] + offs[(i64)d * nblocks + blockIdx.x];
+        first += total[k];
+    }
+    __syncthreads();
+    const int valid_items = (int)(n - tile < kTile ? n - tile : kTile);
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        const int local = warp * kPerWarp + i * 32 + lane;
+        if (local < valid_items) {
+            const uint32_t d = (key[i] >> shift) & (R - 1);
+            pos[i] += start[d] + count[warp * R + d];
         }
-        __syncthreads();
+    }
+    __syncthreads();  // the counts are read: the space takes the sorted tile
+    uint32_t *skey = space, *sval = space + kTile;
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        const int local = warp * kPerWarp + i * 32 + lane;
+        if (local < valid_items) {
+            skey[pos[i]] = key[i];
+            sval[pos[i]] = val[i];
+        }
+    }
+    __syncthreads();
+    for (int k = t; k < valid_items; k += kThreads) {
+        const uint32_t kk = skey[k];
+        const uint32_t d = (kk >> shift) & (R - 1);
+        const uint32_t at = run[d] + ((uint32_t)k - start[d]);
+        keys_out[at] = kk;
+        vals_out[at] = sval[k];
     }
 }
 
