@@ -19,8 +19,8 @@ namespace {
 constexpr int kThreads = 256;  // = the radix (one thread per digit in the scans)
 constexpr int kItems = 16;
 constexpr int kTile = kThreads * kItems;
-constexpr int kRadix = 256;     // 8-bit digits
-constexpr int kRadixMax = 512;  // 9-bit digits, when they save a pass
+constexpr int kRadix = 256;      // 8-bit digits
+constexpr int kRadixMax = 1024;  // up to 10-bit digits, when they save a pass
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -376,11 +376,24 @@ int bits_for(uint64_t max_key) {
 
 }  // namespace
 
+// One stable pass on the digit of R values at `shift`.
+template <int R>
+void sort_pass(bt_ctx *ctx, const uint32_t *src_k, const uint32_t *src_v, i64 n,
+               const i64 *n_dev, int shift, uint32_t *hist, uint32_t *offs, uint32_t *totals,
+               uint32_t *digit, int nblocks, uint32_t *dst_k, uint32_t *dst_v) {
+    cudaStream_t st = ctx->stream;
+    BT_LAUNCH(ctx, radix_hist<R>, nblocks, kThreads, 0, st, src_k, n, n_dev, shift, hist,
+              nblocks);
+    BT_LAUNCH(ctx, radix_row_scan, R, kThreads, 0, st, hist, offs, totals, nblocks);
+    BT_LAUNCH(ctx, radix_digit_base<R>, 1, kThreads, 0, st, totals, digit);
+    BT_LAUNCH(ctx, radix_scatter<R>, nblocks, kThreads, 0, st, src_k, src_v, n, n_dev, shift,
+              offs, digit, nblocks, dst_k, dst_v);
+}
+
 void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_dev,
                       int key_bits, uint32_t **keys_out, uint32_t **vals_out) {
     BT_REQUIRE(n < (i64)0xffffffffLL, "radix sort: too many records for 32-bit indices");
     DepositScratch &s = ctx->deposit;
-    cudaStream_t st = ctx->stream;
     const int nblocks = (int)((n + kTile - 1) / kTile);
     uint32_t *ka = s.keys_alt.as<uint32_t>(n), *va = s.vals.as<uint32_t>(n);
     uint32_t *kb = s.keys.as<uint32_t>(n), *vb = s.vals_alt.as<uint32_t>(n);
@@ -392,26 +405,23 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_
     const uint32_t *src_v = nullptr;
     uint32_t *dst_k = ka, *dst_v = va;
     BT_REQUIRE(n > 0 && key_bits > 0, "radix sort: nothing to sort");
-    // 9-bit digits where they need fewer passes than 8-bit ones (17-18, 25-27 bits)
-    const int bits = (key_bits + 8) / 9 < (key_bits + 7) / 8 ? 9 : 8;
+    // the narrowest of 8-, 9- and 10-bit digits that needs the fewest passes (9 bits for
+    // 17-18-bit keys, 10 bits for 19-20; 8 bits otherwise up to 24)
+    int bits = 8;
+    for (int b = 9; b <= 10; ++b)
+        if ((key_bits + b - 1) / b < (key_bits + bits - 1) / bits) bits = b;
     const int passes = (key_bits + bits - 1) / bits;
     for (int p = 0; p < passes; ++p) {
         const int shift = bits * p;
-        if (bits == 9) {
-            BT_LAUNCH(ctx, radix_hist<kRadixMax>, nblocks, kThreads, 0, st, src_k, n, n_dev, shift,
-                      hist, nblocks);
-            BT_LAUNCH(ctx, radix_row_scan, kRadixMax, kThreads, 0, st, hist, offs, totals, nblocks);
-            BT_LAUNCH(ctx, radix_digit_base<kRadixMax>, 1, kThreads, 0, st, totals, digit);
-            BT_LAUNCH(ctx, radix_scatter<kRadixMax>, nblocks, kThreads, 0, st, src_k, src_v, n,
-                      n_dev, shift, offs, digit, nblocks, dst_k, dst_v);
-        } else {
-            BT_LAUNCH(ctx, radix_hist<kRadix>, nblocks, kThreads, 0, st, src_k, n, n_dev, shift,
-                      hist, nblocks);
-            BT_LAUNCH(ctx, radix_row_scan, kRadix, kThreads, 0, st, hist, offs, totals, nblocks);
-            BT_LAUNCH(ctx, radix_digit_base<kRadix>, 1, kThreads, 0, st, totals, digit);
-            BT_LAUNCH(ctx, radix_scatter<kRadix>, nblocks, kThreads, 0, st, src_k, src_v, n, n_dev,
-                      shift, offs, digit, nblocks, dst_k, dst_v);
-        }
+        if (bits == 10)
+            sort_pass<1024>(ctx, src_k, src_v, n, n_dev, shift, hist, offs, totals, digit,
+                            nblocks, dst_k, dst_v);
+        else if (bits == 9)
+            sort_pass<512>(ctx, src_k, src_v, n, n_dev, shift, hist, offs, totals, digit,
+                           nblocks, dst_k, dst_v);
+        else
+            sort_pass<256>(ctx, src_k, src_v, n, n_dev, shift, hist, offs, totals, digit,
+                           nblocks, dst_k, dst_v);
         BT_CHECK_LAUNCH();
         src_k = dst_k;
         src_v = dst_v;

@@ -134,3 +134,25 @@ def test_trace_windows_agree(kernels, window):
     np.testing.assert_allclose(runs[0][TRACE_CHARGE], reference[TRACE_CHARGE], rtol=0,
                                atol=1e-13 * scale)  # fmt: skip
     del torch
+
+
+@pytest.mark.parametrize("shape", [(200, 300), (500, 400), (1025, 600)])
+def test_deposit_sorts_keys_of_every_width(kernels, shape):
+    """Meshes of 60,000, 200,000 and 615,000 nodes: 16-, 18- and 20-bit cell keys, sorted
+    with two passes of 8-, 9- and 10-bit digits."""
+    import torch
+
+    rng = np.random.default_rng(sum(shape))
+    nx, ny = shape
+    n = 300_000
+    px = torch.from_numpy(rng.uniform(-0.05, 0.1 * nx, n)).cuda()
+    py = torch.from_numpy(rng.uniform(0.0, 0.1 * ny, n)).cuda()
+    q = torch.from_numpy(rng.normal(size=n)).cuda()
+    charge = torch.zeros((nx, ny), dtype=torch.float64, device="cuda")
+    kernels["deposit_trajectories_2d"](px, py, q, 0.0, 0.0, 0.1, 0, charge)
+    expected = np.zeros((nx, ny))
+    oracle.deposit_trajectories_2d(
+        px.cpu().numpy(), py.cpu().numpy(), q.cpu().numpy(), 0.0, 0.0, 0.1, 0, expected
+    )
+    np.testing.assert_allclose(charge.cpu().numpy(), expected, rtol=0,
+                               atol=1e-12 * np.abs(expected).max())  # fmt: skip
