@@ -107,7 +107,7 @@ struct HostBuffer {
 // The scratch of the deterministic deposit (records, their radix sort, per-cell sums).
 struct DepositScratch {
     Buffer keys, keys_alt, vals, vals_alt, rec;
-    Buffer hist, row_offsets, digit_base;
+    Buffer hist, row_offsets, digit_base, sorted;
     Buffer cell_sums, warp_first, warp_last, warp_flags;
 };
 
@@ -227,10 +227,11 @@ struct NodeLayout {
     i64 n_nodes;
 };
 
-// A record's payload: the area weights and the charge, in one 32-byte sector so that the
-// reduction's gather through the sort permutation reads one sector per record.
+// A record's payload: the charge it adds to the four nodes of its cell, (i, j), (i, j+1),
+// (i+1, j) and (i+1, j+1), in one 32-byte sector so that the reduction's gather through the
+// sort permutation reads one sector per record.
 struct __align__(32) DepositRec {
-    double u, w, q, unused;
+    double c00, c01, c10, c11;
 };
 
 // n_records sizes the launches; n_dev, when not NULL, is the device-held count of the
@@ -239,10 +240,12 @@ void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i
                      const i64 *n_dev, uint32_t sentinel, double *charge,
                      const NodeLayout &layout);
 
-// Stable LSD radix sort of (key, index) pairs: sorted keys and the permutation.
-// Returns the device pointers of the sorted keys and values (inside the scratch).  n sizes
-// the launches; n_dev, when not NULL, is the device-held count of keys to sort (at most n).
+// Stable LSD radix sort of (key, index) pairs: sorted keys and the permutation, leaving
+// out the keys equal to `skip`.  Returns the device pointers of the sorted keys and values
+// (inside the scratch) and of the device-held count of sorted pairs.  n sizes the
+// launches; n_dev, when not NULL, is the device-held count of keys to sort (at most n).
 void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_dev,
-                      int key_bits, uint32_t **keys_out, uint32_t **vals_out);
+                      int key_bits, uint32_t skip, uint32_t **keys_out, uint32_t **vals_out,
+                      const i64 **count_out);
 
 }  // namespace bt

@@ -28,10 +28,14 @@ constexpr unsigned kFull = 0xffffffffu;
 // one, the count the device holds (at most n; the grids are sized for n).
 __device__ __forceinline__ i64 record_count(i64 n, const i64 *n_dev) { return n_dev ? *n_dev : n; }
 
+// Keys equal to `skip` (a sort's first pass: the records with no charge) are left out of
+// the counts and the output; kNoSkip leaves none out.
+constexpr uint32_t kNoSkip = 0xffffffffu;
+
 template <int R>
 __global__ void radix_hist(const uint32_t *__restrict__ keys, i64 n_host,
-                           const i64 *__restrict__ n_dev, int shift, uint32_t *__restrict__ hist,
-                           int nblocks) {
+                           const i64 *__restrict__ n_dev, uint32_t skip, int shift,
+                           uint32_t *__restrict__ hist, int nblocks) {
     __shared__ uint32_t h[R];
     const i64 n = record_count(n_host, n_dev);
     for (int d = threadIdx.x; d < R; d += kThreads) h[d] = 0;
@@ -40,7 +44,10 @@ __global__ void radix_hist(const uint32_t *__restrict__ keys, i64 n_host,
 #pragma unroll 4
     for (int i = 0; i < kItems; ++i) {
         const i64 r = base + (i64)i * kThreads + threadIdx.x;
-        if (r < n) atomicAdd(&h[(keys[r] >> shift) & (R - 1)], 1u);
+        if (r < n) {
+            const uint32_t key = keys[r];
+            if (key != skip) atomicAdd(&h[(key >> shift) & (R - 1)], 1u);
+        }
     }
     __syncthreads();
     for (int d = threadIdx.x; d < R; d += kThreads) hist[(i64)d * nblocks + blockIdx.x] = h[d];
@@ -93,8 +100,10 @@ __global__ void radix_row_scan(const uint32_t *__restrict__ hist, uint32_t *__re
 }
 
 // Exclusive prefix of the R digit totals; thread t scans digits t * R / kThreads onwards.
+// `count`, when not NULL, gets the number of records the pass sorts.
 template <int R>
-__global__ void radix_digit_base(const uint32_t *__restrict__ totals, uint32_t *__restrict__ base) {
+__global__ void radix_digit_base(const uint32_t *__restrict__ totals, uint32_t *__restrict__ base,
+                                 i64 *__restrict__ count) {
     __shared__ uint32_t warp_sums[kWarps];
     constexpr int D = R / kThreads;
     uint32_t mine[D];
@@ -104,12 +113,14 @@ __global__ void radix_digit_base(const uint32_t *__restrict__ totals, uint32_t *
         mine[k] = totals[threadIdx.x * D + k];
         v += mine[k];
     }
-    uint32_t run = block_inclusive_scan(v, warp_sums) - v;
+    const uint32_t inclusive = block_inclusive_scan(v, warp_sums);
+    uint32_t run = inclusive - v;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
         base[threadIdx.x * D + k] = run;
         run += mine[k];
     }
+    if (count && threadIdx.x == kThreads - 1) *count = inclusive;
 }
 
 // Stable scatter of one tile of kTile records.  Warp w ranks the tile's items
@@ -122,7 +133,7 @@ __global__ void radix_digit_base(const uint32_t *__restrict__ totals, uint32_t *
 template <int R>
 __global__ void __launch_bounds__(kThreads) radix_scatter(
     const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, i64 n_host,
-    const i64 *__restrict__ n_dev, int shift, const uint32_t *__restrict__ offs,
+    const i64 *__restrict__ n_dev, uint32_t skip, int shift, const uint32_t *__restrict__ offs,
     const uint32_t *__restrict__ base, int nblocks, uint32_t *__restrict__ keys_out,
     uint32_t *__restrict__ vals_out) {
     static_assert(kWarps * R * 4 <= kTile * 8, "the counts must fit the tile's space");
@@ -132,6 +143,7 @@ __global__ void __launch_bounds__(kThreads) radix_scatter(
     __shared__ uint32_t start[R];               // the tile's first slot of each digit
     __shared__ uint32_t run[R];                 // the digit's first global slot for this tile
     __shared__ uint32_t warp_sums[kWarps];
+    __shared__ uint32_t tile_count;             // the tile's records that are sorted
     uint32_t *count = space;
     const i64 n = record_count(n_host, n_dev);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -140,11 +152,13 @@ __global__ void __launch_bounds__(kThreads) radix_scatter(
     const i64 tile = (i64)blockIdx.x * kTile;
     const unsigned below = (1u << lane) - 1u;
     uint32_t key[kItems], val[kItems], pos[kItems];
+    unsigned valid_mask = 0;  // bit i: item i is sorted
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
         const i64 r = tile + (i64)warp * kPerWarp + (i64)i * 32 + lane;
-        const bool valid = r < n;
-        key[i] = valid ? keys_in[r] : 0xffffffffu;
+        key[i] = r < n ? keys_in[r] : skip;
+        const bool valid = r < n && key[i] != skip;
+        if (valid) valid_mask |= 1u << i;
         val[i] = valid ? (vals_in ? vals_in[r] : (uint32_t)r) : 0u;
         const uint32_t d = (key[i] >> shift) & (R - 1);
         const unsigned peers = __match_any_sync(kFull, valid ? d : 0xffffffffu);
@@ -173,7 +187,9 @@ __global__ void __launch_bounds__(kThreads) radix_scatter(
     uint32_t v = 0;
 #pragma unroll
     for (int k = 0; k < D; ++k) v += total[k];
-    uint32_t first = block_inclusive_scan(v, warp_sums) - v;
+    const uint32_t inclusive = block_inclusive_scan(v, warp_sums);
+    uint32_t first = inclusive - v;
+    if (t == kThreads - 1) tile_count = inclusive;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
         const int d = t * D + k;
@@ -182,11 +198,9 @@ __global__ void __launch_bounds__(kThreads) radix_scatter(
         first += total[k];
     }
     __syncthreads();
-    const int valid_items = (int)(n - tile < kTile ? n - tile : kTile);
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
-        const int local = warp * kPerWarp + i * 32 + lane;
-        if (local < valid_items) {
+        if (valid_mask & (1u << i)) {
             const uint32_t d = (key[i] >> shift) & (R - 1);
             pos[i] += start[d] + count[warp * R + d];
         }
@@ -195,14 +209,14 @@ __global__ void __launch_bounds__(kThreads) radix_scatter(
     uint32_t *skey = space, *sval = space + kTile;
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
-        const int local = warp * kPerWarp + i * 32 + lane;
-        if (local < valid_items) {
+        if (valid_mask & (1u << i)) {
             skey[pos[i]] = key[i];
             sval[pos[i]] = val[i];
         }
     }
     __syncthreads();
-    for (int k = t; k < valid_items; k += kThreads) {
+    const int sorted = (int)tile_count;
+    for (int k = t; k < sorted; k += kThreads) {
         const uint32_t kk = skey[k];
         const uint32_t d = (kk >> shift) & (R - 1);
         const uint32_t at = run[d] + ((uint32_t)k - start[d]);
@@ -232,11 +246,10 @@ __global__ void seg_reduce_warps(const uint32_t *__restrict__ K, const uint32_t 
     double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
     if (valid) {
         const DepositRec p = rec[I[r]];
-        const double u = p.u, w = p.w, q = p.q;
-        c00 = (1.0 - u) * (1.0 - w) * q;
-        c01 = (1.0 - u) * w * q;
-        c10 = u * (1.0 - w) * q;
-        c11 = u * w * q;
+        c00 = p.c00;
+        c01 = p.c01;
+        c10 = p.c10;
+        c11 = p.c11;
     }
     const uint32_t prev = (r > 0 && r - 1 < R) ? K[r - 1] : 0xffffffffu;
     const uint32_t next = (r + 1 < R) ? K[r + 1] : 0xffffffffu;
@@ -365,7 +378,9 @@ __global__ void point_records(const double *__restrict__ px, const double *__res
         j = ny - 2;
     }
     keys[k] = (uint32_t)(i * ny + j);
-    rec[k] = DepositRec{t, u, q[k], 0.0};
+    const double c = q[k];
+    rec[k] = DepositRec{(1.0 - t) * (1.0 - u) * c, (1.0 - t) * u * c, t * (1.0 - u) * c,
+                        t * u * c};
 }
 
 int bits_for(uint64_t max_key) {
@@ -377,21 +392,24 @@ int bits_for(uint64_t max_key) {
 }  // namespace
 
 // One stable pass on the digit of R values at `shift`.
+// `skip`: the key the pass leaves out; `count`, when not NULL, gets the records it sorted.
 template <int R>
 void sort_pass(bt_ctx *ctx, const uint32_t *src_k, const uint32_t *src_v, i64 n,
-               const i64 *n_dev, int shift, uint32_t *hist, uint32_t *offs, uint32_t *totals,
-               uint32_t *digit, int nblocks, uint32_t *dst_k, uint32_t *dst_v) {
+               const i64 *n_dev, uint32_t skip, int shift, uint32_t *hist, uint32_t *offs,
+               uint32_t *totals, uint32_t *digit, i64 *count, int nblocks, uint32_t *dst_k,
+               uint32_t *dst_v) {
     cudaStream_t st = ctx->stream;
-    BT_LAUNCH(ctx, radix_hist<R>, nblocks, kThreads, 0, st, src_k, n, n_dev, shift, hist,
+    BT_LAUNCH(ctx, radix_hist<R>, nblocks, kThreads, 0, st, src_k, n, n_dev, skip, shift, hist,
               nblocks);
     BT_LAUNCH(ctx, radix_row_scan, R, kThreads, 0, st, hist, offs, totals, nblocks);
-    BT_LAUNCH(ctx, radix_digit_base<R>, 1, kThreads, 0, st, totals, digit);
-    BT_LAUNCH(ctx, radix_scatter<R>, nblocks, kThreads, 0, st, src_k, src_v, n, n_dev, shift,
-              offs, digit, nblocks, dst_k, dst_v);
+    BT_LAUNCH(ctx, radix_digit_base<R>, 1, kThreads, 0, st, totals, digit, count);
+    BT_LAUNCH(ctx, radix_scatter<R>, nblocks, kThreads, 0, st, src_k, src_v, n, n_dev, skip,
+              shift, offs, digit, nblocks, dst_k, dst_v);
 }
 
 void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_dev,
-                      int key_bits, uint32_t **keys_out, uint32_t **vals_out) {
+                      int key_bits, uint32_t skip, uint32_t **keys_out, uint32_t **vals_out,
+                      const i64 **count_out) {
     BT_REQUIRE(n < (i64)0xffffffffLL, "radix sort: too many records for 32-bit indices");
     DepositScratch &s = ctx->deposit;
     const int nblocks = (int)((n + kTile - 1) / kTile);
@@ -401,6 +419,7 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_
     uint32_t *offs = s.row_offsets.as<uint32_t>((size_t)kRadixMax * nblocks);
     uint32_t *digit = s.digit_base.as<uint32_t>(2 * kRadixMax);
     uint32_t *totals = digit + kRadixMax;
+    i64 *sorted = s.sorted.as<i64>(1);  // the records left after the first pass
     const uint32_t *src_k = keys_in;
     const uint32_t *src_v = nullptr;
     uint32_t *dst_k = ka, *dst_v = va;
@@ -411,17 +430,22 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_
     for (int b = 9; b <= 10; ++b)
         if ((key_bits + b - 1) / b < (key_bits + bits - 1) / bits) bits = b;
     const int passes = (key_bits + bits - 1) / bits;
+    // the first pass leaves out the `skip` keys and counts the rest; the later passes sort
+    // that many
     for (int p = 0; p < passes; ++p) {
         const int shift = bits * p;
+        const i64 *count = p == 0 ? n_dev : sorted;
+        const uint32_t leave = p == 0 ? skip : kNoSkip;
+        i64 *out = p == 0 ? sorted : nullptr;
         if (bits == 10)
-            sort_pass<1024>(ctx, src_k, src_v, n, n_dev, shift, hist, offs, totals, digit,
-                            nblocks, dst_k, dst_v);
+            sort_pass<1024>(ctx, src_k, src_v, n, count, leave, shift, hist, offs, totals,
+                            digit, out, nblocks, dst_k, dst_v);
         else if (bits == 9)
-            sort_pass<512>(ctx, src_k, src_v, n, n_dev, shift, hist, offs, totals, digit,
-                           nblocks, dst_k, dst_v);
+            sort_pass<512>(ctx, src_k, src_v, n, count, leave, shift, hist, offs, totals, digit,
+                           out, nblocks, dst_k, dst_v);
         else
-            sort_pass<256>(ctx, src_k, src_v, n, n_dev, shift, hist, offs, totals, digit,
-                           nblocks, dst_k, dst_v);
+            sort_pass<256>(ctx, src_k, src_v, n, count, leave, shift, hist, offs, totals, digit,
+                           out, nblocks, dst_k, dst_v);
         BT_CHECK_LAUNCH();
         src_k = dst_k;
         src_v = dst_v;
@@ -435,6 +459,7 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_
     }
     *keys_out = const_cast<uint32_t *>(src_k);
     *vals_out = const_cast<uint32_t *>(src_v);
+    *count_out = sorted;
 }
 
 void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i64 n_records,
@@ -444,7 +469,9 @@ void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i
     DepositScratch &s = ctx->deposit;
     cudaStream_t st = ctx->stream;
     uint32_t *sk = nullptr, *sv = nullptr;
-    radix_sort_pairs(ctx, keys, n_records, n_dev, bits_for(sentinel), &sk, &sv);
+    const i64 *n_sorted = nullptr;  // the records with a charge, on the device
+    radix_sort_pairs(ctx, keys, n_records, n_dev, bits_for(sentinel), sentinel, &sk, &sv,
+                     &n_sorted);
     const i64 n_warps = (n_records + 31) / 32;
     double4 *cells = s.cell_sums.as<double4>((size_t)layout.n_nodes);
     double4 *first = s.warp_first.as<double4>((size_t)n_warps);
@@ -453,9 +480,9 @@ void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i
     BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * layout.n_nodes, st));
     const int threads = 256;
     BT_LAUNCH(ctx, seg_reduce_warps, blocks_for(n_warps * 32, threads), threads, 0, st, sk, sv,
-              rec, n_records, n_dev, sentinel, cells, first, last, flags, flags + n_warps);
+              rec, n_records, n_sorted, sentinel, cells, first, last, flags, flags + n_warps);
     BT_LAUNCH(ctx, seg_reduce_chains, blocks_for(n_warps, threads), threads, 0, st, sk, n_records,
-              n_dev, cells, first, last, flags, flags + n_warps);
+              n_sorted, cells, first, last, flags, flags + n_warps);
     BT_LAUNCH(ctx, node_accumulate, blocks_for(layout.n_nodes, threads), threads, 0, st, cells, charge, layout.patch_int, layout.n_patches, layout.nx, layout.ny,
         layout.n_nodes);
     BT_CHECK_LAUNCH();
@@ -582,11 +609,12 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
         uint32_t *dst_k = keys_alt, *dst_v = vals;
         for (int pass = 0; pass < passes; ++pass) {
             const int shift = 8 * pass;
-            radix_hist<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, n, nullptr, shift, hist,
-                                                             nblocks);
+            radix_hist<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, n, nullptr, kNoSkip, shift,
+                                                             hist, nblocks);
             radix_row_scan<<<kRadix, kThreads, 0, st>>>(hist, offs, totals, nblocks);
-            radix_digit_base<kRadix><<<1, kThreads, 0, st>>>(totals, digit);
-            radix_scatter<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, src_v, n, nullptr, shift,
+            radix_digit_base<kRadix><<<1, kThreads, 0, st>>>(totals, digit, nullptr);
+            radix_scatter<kRadix><<<nblocks, kThreads, 0, st>>>(src_k, src_v, n, nullptr, kNoSkip,
+                                                                shift,
                                                                 offs, digit, nblocks, dst_k,
                                                                 dst_v);
             src_k = dst_k;

@@ -219,8 +219,12 @@ __device__ __forceinline__ double inv_gamma(double u0, double u1, double u2, dou
 // s * stride + m.  Threads past the live count fill their slots with the sentinel.  A
 // window with live trajectories sets *records_end to `end`, the end of its slots, so the
 // deposit sorts no window that had none.
-template <int CYL, int INTEG, bool GENERAL, bool MAG>
-__global__ void __launch_bounds__(128, 1)
+//
+// MINB, the blocks an SM must hold: 1 (the registers the compiler wants) for a window of at
+// most about two blocks per SM, where one warp per scheduler is all there is; 3 (at most
+// 168 registers) for larger windows, whose warps hide each other's latency.
+template <int CYL, int INTEG, bool GENERAL, bool MAG, int MINB>
+__global__ void __launch_bounds__(128, MINB)
     trace_window(Trace tr, const i64 *__restrict__ act, const i64 *__restrict__ live, i64 stride,
                  int S, uint32_t *__restrict__ keys, DepositRec *__restrict__ rec,
                  uint32_t sentinel,
@@ -271,6 +275,11 @@ __global__ void __launch_bounds__(128, 1)
         start_sx = div_known(x0 - origin_x, h, rh);
         start_sy = div_known(start_r - origin_y, h, rh);
     }
+    // The records of consecutive steps in one cell are summed into one (the run's): it goes
+    // to the slot of the run's last step, the slots of its other steps hold the sentinel.
+    i64 run_slot = -1;
+    uint32_t run_key = sentinel;
+    double r00 = 0.0, r01 = 0.0, r10 = 0.0, r11 = 0.0;
     int s = 0;
     for (; s < S; ++s) {
         if (ns >= a.max_steps) break;
@@ -534,9 +543,29 @@ __global__ void __launch_bounds__(128, 1)
                 w = 1.0;
                 j = pny - 2;
             }
-            const i64 r = (i64)s * stride + m;
-            keys[r] = (uint32_t)(g.ofn + (i64)i * pny + j);
-            rec[r] = DepositRec{u, w, dqk * dt, 0.0};
+            const uint32_t key = (uint32_t)(g.ofn + (i64)i * pny + j);
+            const double q = dqk * dt;
+            const double c00 = (1.0 - u) * (1.0 - w) * q, c01 = (1.0 - u) * w * q;
+            const double c10 = u * (1.0 - w) * q, c11 = u * w * q;
+            if (run_slot >= 0 && key == run_key) {
+                // the step stays in the run's cell: its charge joins the run's record
+                keys[run_slot] = sentinel;
+                r00 = r00 + c00;
+                r01 = r01 + c01;
+                r10 = r10 + c10;
+                r11 = r11 + c11;
+            } else {
+                if (run_slot >= 0) {
+                    keys[run_slot] = run_key;
+                    rec[run_slot] = DepositRec{r00, r01, r10, r11};
+                }
+                run_key = key;
+                r00 = c00;
+                r01 = c01;
+                r10 = c10;
+                r11 = c11;
+            }
+            run_slot = (i64)s * stride + m;
         }
         ns = ns + 1;
 
@@ -627,6 +656,10 @@ __global__ void __launch_bounds__(128, 1)
             ++s;
             break;
         }
+    }
+    if (run_slot >= 0) {
+        keys[run_slot] = run_key;
+        rec[run_slot] = DepositRec{r00, r01, r10, r11};
     }
     // the slots of the steps not taken hold no record
     for (; s < S; ++s) keys[(i64)s * stride + m] = sentinel;
@@ -833,13 +866,21 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                 {
                     bt::Timed timed(ctx, "trace_window");
                     const unsigned grid = (unsigned)bt::blocks_for(bound, 128);
+                    const bool busy = grid > 2u * (unsigned)ctx->num_sms;
                     const int64_t launched = ctx->launch_count;
 #define BT_TRACE_CASE(C, I, G, M)                                                               \
     if (a.cylindrical == C && (a.integrator != 0) == (I != 0) && general == G &&                 \
         (mag != nullptr) == M)                                                                   \
-        BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M>), grid, 128, 0, st, tr, act_a, live + lv,   \
-                  bound, S, keys[cur] + used, rec[cur] + used, sentinel, records_end + cur,       \
-                  used + need);
+    {                                                                                            \
+        if (busy)                                                                                \
+            BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M, 3>), grid, 128, 0, st, tr, act_a,       \
+                      live + lv, bound, S, keys[cur] + used, rec[cur] + used, sentinel,          \
+                      records_end + cur, used + need);                                           \
+        else                                                                                     \
+            BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M, 1>), grid, 128, 0, st, tr, act_a,       \
+                      live + lv, bound, S, keys[cur] + used, rec[cur] + used, sentinel,          \
+                      records_end + cur, used + need);                                           \
+    }
                     BT_TRACE_CASE(0, 0, false, false) BT_TRACE_CASE(0, 0, true, false)
                     BT_TRACE_CASE(0, 1, false, false) BT_TRACE_CASE(0, 1, true, false)
                     BT_TRACE_CASE(1, 0, false, false) BT_TRACE_CASE(1, 0, true, false)
