@@ -114,7 +114,7 @@ struct DepositScratch {
 // The tracer's scratch: the live lists and two record buffers, one filled by the trace
 // windows while the other's records are deposited on the side stream.
 struct TraceScratch {
-    Buffer active_a, active_b, block_counts, n_alive;
+    Buffer active_a, active_b, block_counts, n_alive, alive;
     Buffer rec_keys[2], rec[2];
     cudaStream_t side = nullptr;                 // the deposits' stream
     cudaEvent_t filled[2] = {nullptr, nullptr};  // a buffer's windows are traced

@@ -223,19 +223,16 @@ __device__ __forceinline__ double inv_gamma(double u0, double u1, double u2, dou
 // MINB, the blocks an SM must hold: 1 (the registers the compiler wants) for a window of at
 // most about two blocks per SM, where one warp per scheduler is all there is; 3 (at most
 // 168 registers) for larger windows, whose warps hide each other's latency.
-template <int CYL, int INTEG, bool GENERAL, bool MAG, int MINB>
-__global__ void __launch_bounds__(128, MINB)
-    trace_window(Trace tr, const i64 *__restrict__ act, const i64 *__restrict__ live, i64 stride,
-                 int S, uint32_t *__restrict__ keys, DepositRec *__restrict__ rec,
-                 uint32_t sentinel,
-                 i64 *__restrict__ records_end, i64 end) {
-    const i64 m = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    const i64 n_act = *live;
-    if (m == 0 && n_act > 0) *records_end = end;
-    if (m >= stride) return;
+//
+// One thread's window (m < stride): whether its trajectory is still live afterwards.
+template <int CYL, int INTEG, bool GENERAL, bool MAG>
+__device__ __forceinline__ bool trace_thread(const Trace &tr, const i64 *__restrict__ act,
+                                             i64 m, i64 n_act, i64 stride, int S,
+                                             uint32_t *__restrict__ keys,
+                                             DepositRec *__restrict__ rec, uint32_t sentinel) {
     if (m >= n_act) {
         for (int s = 0; s < S; ++s) keys[(i64)s * stride + m] = sentinel;
-        return;
+        return false;
     }
     const bt_trace_args &a = tr.a;
     const i64 k = act[m];
@@ -672,69 +669,58 @@ __global__ void __launch_bounds__(128, MINB)
     a.v[2 * n + k] = v2;
     a.steps[k] = ns;
     a.status[k] = st;
+    return st == -1;
+}
+
+// The window: every thread's trajectory, then each block's count of live trajectories and
+// every thread's flag, for compact_live.
+template <int CYL, int INTEG, bool GENERAL, bool MAG, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+    trace_window(Trace tr, const i64 *__restrict__ act, const i64 *__restrict__ live, i64 stride,
+                 int S, uint32_t *__restrict__ keys, DepositRec *__restrict__ rec,
+                 uint32_t sentinel, i64 *__restrict__ records_end, i64 end,
+                 uint32_t *__restrict__ block_live, uint8_t *__restrict__ alive) {
+    const i64 m = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const i64 n_act = *live;
+    if (m == 0 && n_act > 0) *records_end = end;
+    bool still = false;
+    if (m < stride)
+        still = trace_thread<CYL, INTEG, GENERAL, MAG>(tr, act, m, n_act, stride, S, keys, rec,
+                                                       sentinel);
+    const int count = __syncthreads_count(still);
+    if (m < stride) alive[m] = still ? 1 : 0;
+    if (threadIdx.x == 0) block_live[blockIdx.x] = (uint32_t)count;
 }
 
 // -- order-preserving compaction of the live trajectories ----------------------------------
 
-constexpr int kCompact = 1024;
-
-// act[0, *live) are the trajectories of the last window; the grid covers at least *live.
-__global__ void count_alive(const i64 *__restrict__ act, const i64 *__restrict__ live,
-                            const i64 *__restrict__ status, uint32_t *__restrict__ block_counts) {
-    __shared__ uint32_t warp_counts[kCompact / 32];
-    const i64 n = *live;
-    const i64 m = (i64)blockIdx.x * kCompact + threadIdx.x;
-    const bool alive = m < n && status[act[m]] == -1;
-    const unsigned ballot = __ballot_sync(0xffffffffu, alive);
-    if ((threadIdx.x & 31) == 0) warp_counts[threadIdx.x >> 5] = __popc(ballot);
+// act_out = the live trajectories of act, in order, and *live_out their count, from a
+// window's per-block counts and flags (the window's grid of 128-thread blocks).
+__global__ void __launch_bounds__(128) compact_live(const i64 *__restrict__ act,
+                                                    const uint8_t *__restrict__ alive,
+                                                    const uint32_t *__restrict__ block_live,
+                                                    i64 stride, i64 *__restrict__ act_out,
+                                                    i64 *__restrict__ live_out) {
+    __shared__ uint32_t part[4], warp_first[4];
+    const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    uint32_t before = 0;  // the live trajectories of the blocks before this one
+    for (int q = t; q < b; q += 128) before += block_live[q];
+    for (int off = 16; off > 0; off >>= 1) before += __shfl_down_sync(0xffffffffu, before, off);
+    if (lane == 0) part[warp] = before;
+    const i64 m = (i64)b * 128 + t;
+    const bool a = m < stride && alive[m] != 0;
+    const unsigned ballot = __ballot_sync(0xffffffffu, a);
+    if (lane == 0) warp_first[warp] = __popc(ballot);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t total = 0;
-        for (int w = 0; w < kCompact / 32; ++w) total += warp_counts[w];
-        block_counts[blockIdx.x] = total;
-    }
+    const uint32_t offset = part[0] + part[1] + part[2] + part[3];
+    uint32_t rank = offset;
+    for (int w = 0; w < warp; ++w) rank += warp_first[w];
+    rank += __popc(ballot & ((1u << lane) - 1u));
+    if (a) act_out[rank] = act[m];
+    if (b == (int)gridDim.x - 1 && t == 0) *live_out = offset + block_live[b];
 }
 
-// One block: exclusive prefix of the block counts (in place) and the total.
 __global__ void set_count(i64 *__restrict__ count, i64 value) { *count = value; }
-
-__global__ void scan_counts(uint32_t *__restrict__ block_counts, int nblocks,
-                            i64 *__restrict__ total) {
-    if (threadIdx.x != 0) return;
-    uint32_t run = 0;
-    for (int b = 0; b < nblocks; ++b) {
-        const uint32_t c = block_counts[b];
-        block_counts[b] = run;
-        run += c;
-    }
-    *total = run;
-}
-
-__global__ void scatter_alive(const i64 *__restrict__ act, const i64 *__restrict__ live,
-                              const i64 *__restrict__ status,
-                              const uint32_t *__restrict__ block_offsets, i64 *__restrict__ out) {
-    __shared__ uint32_t warp_counts[kCompact / 32];
-    const i64 n = *live;
-    const i64 m = (i64)blockIdx.x * kCompact + threadIdx.x;
-    const bool alive = m < n && status[act[m]] == -1;
-    const unsigned ballot = __ballot_sync(0xffffffffu, alive);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) warp_counts[warp] = __popc(ballot);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int w = 0; w < kCompact / 32; ++w) {
-            const uint32_t c = warp_counts[w];
-            warp_counts[w] = run;
-            run += c;
-        }
-    }
-    __syncthreads();
-    if (alive) {
-        const uint32_t rank = warp_counts[warp] + __popc(ballot & ((1u << lane) - 1u));
-        out[block_offsets[blockIdx.x] + rank] = act[m];
-    }
-}
 
 }  // namespace
 
@@ -821,8 +807,8 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         }
         int64_t *act_a = ts.active_a.as<int64_t>(a.n_active);
         int64_t *act_b = ts.active_b.as<int64_t>(a.n_active);
-        const int nb_max = (int)bt::blocks_for(a.n_active, bt::kCompact);
-        uint32_t *block_counts = ts.block_counts.as<uint32_t>(nb_max);
+        uint32_t *block_live = ts.block_counts.as<uint32_t>(bt::blocks_for(a.n_active, 128));
+        uint8_t *alive = ts.alive.as<uint8_t>(a.n_active);
         // live[2]: the live count before and after a window's compaction; records_end[2]:
         // where the slots of each buffer's last window with live trajectories end
         int64_t *live = ts.n_alive.as<int64_t>(4);
@@ -863,9 +849,10 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
             for (int g = 0; g < kGroup; ++g) {
                 const int64_t need = bound * (int64_t)S;
                 if (used + need > capacity) flush();
+                unsigned grid = 0;
                 {
                     bt::Timed timed(ctx, "trace_window");
-                    const unsigned grid = (unsigned)bt::blocks_for(bound, 128);
+                    grid = (unsigned)bt::blocks_for(bound, 128);
                     const bool busy = grid > 2u * (unsigned)ctx->num_sms;
                     const int64_t launched = ctx->launch_count;
 #define BT_TRACE_CASE(C, I, G, M)                                                               \
@@ -875,11 +862,11 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         if (busy)                                                                                \
             BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M, 3>), grid, 128, 0, st, tr, act_a,       \
                       live + lv, bound, S, keys[cur] + used, rec[cur] + used, sentinel,          \
-                      records_end + cur, used + need);                                           \
+                      records_end + cur, used + need, block_live, alive);                        \
         else                                                                                     \
             BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M, 1>), grid, 128, 0, st, tr, act_a,       \
                       live + lv, bound, S, keys[cur] + used, rec[cur] + used, sentinel,          \
-                      records_end + cur, used + need);                                           \
+                      records_end + cur, used + need, block_live, alive);                        \
     }
                     BT_TRACE_CASE(0, 0, false, false) BT_TRACE_CASE(0, 0, true, false)
                     BT_TRACE_CASE(0, 1, false, false) BT_TRACE_CASE(0, 1, true, false)
@@ -898,12 +885,8 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                 BT_CHECK_LAUNCH();
                 used += need;
                 ctx->last_windows += 1;
-                const int nb = (int)bt::blocks_for(bound, bt::kCompact);
-                BT_LAUNCH(ctx, bt::count_alive, nb, bt::kCompact, 0, st, act_a, live + lv,
-                          a.status, block_counts);
-                BT_LAUNCH(ctx, bt::scan_counts, 1, 32, 0, st, block_counts, nb, live + (lv ^ 1));
-                BT_LAUNCH(ctx, bt::scatter_alive, nb, bt::kCompact, 0, st, act_a, live + lv,
-                          a.status, block_counts, act_b);
+                BT_LAUNCH(ctx, bt::compact_live, grid, 128, 0, st, act_a, alive, block_live, bound,
+                          act_b, live + (lv ^ 1));
                 BT_CHECK_LAUNCH();
                 std::swap(act_a, act_b);
                 lv ^= 1;
