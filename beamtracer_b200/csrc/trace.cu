@@ -730,10 +730,11 @@ namespace bt {
 namespace {
 
 // Windows launched between two reads of the live count.
-constexpr int kGroup = 8;
+constexpr int kGroup = 4;
 
-// Records per deposit batch (at most; 16 windows of the starting trajectories when fewer):
-// large batches keep the deposits, which compete with the windows for the SMs' L1, rare.
+// Record slots per deposit batch, at most: a batch is a group's windows when they hold
+// fewer.  A batch is deposited at the end of its group, under the next group's windows,
+// so only the last group's deposit is left when the trace ends.
 constexpr int64_t kBatchRecords = (int64_t)1 << 24;
 
 // Points the context's launches at `side` for its lifetime.
@@ -788,10 +789,11 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         // Two record buffers: the windows fill one while the records of the other are sorted
         // and reduced into charge[0] on the side stream, in the order the buffers were
         // filled, so the deposit runs under the next windows and the sums are the same
-        // whatever the timing.  A buffer is deposited once it holds `batch` records.
+        // whatever the timing.  A buffer is deposited at the end of the group that brought
+        // it to `batch` records (or on filling up within a group).
         const int64_t per_window = a.n_active * (int64_t)S;
-        const int64_t batch = std::min<int64_t>(kBatchRecords, 16 * per_window);
-        const int64_t capacity = per_window + batch;
+        const int64_t batch = std::min<int64_t>(kBatchRecords, kGroup * per_window);
+        const int64_t capacity = batch + kGroup * per_window;
         uint32_t *keys[2];
         bt::DepositRec *rec[2];
         for (int b = 0; b < 2; ++b) {

@@ -247,7 +247,7 @@ def vlasov_iterate(
     fy = torch.empty((nx, ny + 1), dtype=torch.float64, device=dev)
     factors = compensation_factors(mesh.x, compensation)
     column = None if factors is None else torch.from_numpy(factors).to(dev)
-    scalars = torch.zeros(4, dtype=torch.float64, device=dev)
+    scalars = torch.zeros(5, dtype=torch.float64, device=dev)
     region_x = None if plasma is None else plasma.initial_plasma_x
     engine = tracer.engine()
     loaded: BeamParticles | None = None
@@ -311,9 +311,9 @@ def vlasov_iterate(
             )  # fmt: skip
         if engine.n:
             scalars[3] = engine.steps.max().to(torch.float64)
-            steps_sum = engine.steps.sum()
+            scalars[4] = engine.steps.sum().to(torch.float64)  # exact below 2^53 steps
         host = scalars.cpu().numpy()
-        total_steps = int(steps_sum) if engine.n else 0
+        total_steps = int(host[4]) if engine.n else 0
         change = float(host[0]) if have_potential else float("inf")
         have_potential = True
         density_change = float(host[1] / host[2]) if host[2] > 0 else 0.0
