@@ -193,18 +193,36 @@ def cpu_baseline(config, iterations: int) -> dict:
 
 
 def run_reference(args, rank: int) -> None:
+    """The reference arm: the oracle's converged solve of the same lens on every host core
+    (the field by SciPy's LU, the trace and deposit by the C port), each step one solve run
+    until the potential changes by less than the tolerance, as the device solve is."""
     if rank != 0:
         return
+    from beamtracer_b200.model import BeamOptics
+    from oracle import kernels as oracle_kernels
+    from oracle import vlasov as oracle_vlasov
+    from tests.vlasov_cases import oracle_problem
+
     config = build_workload(2)
-    iterations = 6
-    samples = []
-    base = None
-    for _ in range(max(args.warmup, 0) and 1):
-        base = cpu_baseline(config, iterations)  # warm the oracle's build and caches
-    for _ in range(args.steps):
-        base = cpu_baseline(config, iterations)
-        samples.append(1.0 / base["value"])
-    seconds = float(np.mean(samples))
+    model = BeamOptics(config)
+    problem = oracle_problem(model)
+    particles, j_over_v = model._particles()
+
+    def solve() -> tuple[float, int]:
+        start = time.perf_counter()
+        out = oracle_vlasov.vlasov(problem, particles, j_over_v, iterations=config.iterations,
+                                   tolerance=config.tolerance, relaxation=config.relaxation)
+        return time.perf_counter() - start, len(out["history"])
+
+    if args.warmup > 0:
+        solve()  # the oracle's build and caches
+    runs = [solve() for _ in range(max(args.steps, 1))]
+    seconds = float(np.mean([t for t, _ in runs]))
+    iterations = runs[-1][1]
+    base = {"value": 1.0 / seconds, "unit": UNIT, "cores": oracle_kernels.host_cores(),
+            "kind": "port",
+            "sample": f"converged solves of the oracle ({iterations} iterations: SciPy LU "
+                      f"field, C trace and deposit), {seconds:.2f} s each"}  # fmt: skip
     line = {
         "impl": "reference", "metric": METRIC, "value": 1.0 / seconds, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
