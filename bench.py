@@ -50,8 +50,9 @@ FLOPS_PER_RK4_STEP = 370
 #: reduction) and per node (charge read and written).
 DEPOSIT_BYTES_PER_RECORD = 28 * 2
 NOMINAL_FP64_TFLOPS = 37.0
-#: The trace's algorithmic bytes per step: its deposit record (u32 key, u, w, q f64; the
-#: kernel writes 36 B, the payload padded to one 32-byte sector).
+#: The trace's algorithmic bytes per step: its deposit record (u32 key, u, w, q f64).  The
+#: kernel writes a 4-byte key per step and a 32-byte record (the four node charges) per run
+#: of steps in one cell.
 TRACE_BYTES_PER_STEP = 28
 #: DRAM bytes read + written per trace_window launch at this workload: ncu's
 #: dram__bytes_read.sum + dram__bytes_write.sum averaged over the 175 launches of one

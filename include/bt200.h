@@ -85,7 +85,7 @@ int bt_deposit_trajectories_2d(bt_ctx *ctx, const double *px, const double *py,
  * that may not allocate device memory -- whose device memory is budgeted up front by
  * another allocator, or that cannot take cudaMalloc's implicit synchronisation of the
  * device at the point where they deposit.  It allocates nothing: its scratch is a
- * file-scope __device__ array of about 4.7 MB that every GPU loading the library holds
+ * file-scope __device__ array of about 5.4 MB that every GPU loading the library holds
  * until the process exits, sized for at most 65536 charges per call and a mesh of at most
  * 65536 nodes; larger calls fail with BT_ERR_ARG.  `stream` is a cudaStream_t (NULL: the
  * legacy default stream) on the calling thread's current device.  The first call on a
