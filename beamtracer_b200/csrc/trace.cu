@@ -694,17 +694,62 @@ __global__ void __launch_bounds__(128, MINB)
 
 // -- order-preserving compaction of the live trajectories ----------------------------------
 
+// Windows of more blocks than this have their blocks' offsets scanned by block_offsets
+// (each compact_live block would otherwise add up all the counts before its own).
+constexpr int kSumBlocks = 2048;
+
+// offsets[b] = the live trajectories of the window's blocks before b (one block, in chunks
+// of 1024).
+__global__ void __launch_bounds__(1024) block_offsets(const uint32_t *__restrict__ block_live,
+                                                      int nblocks, uint32_t *__restrict__ offsets) {
+    __shared__ uint32_t warp_sums[32];
+    __shared__ uint32_t carry;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) carry = 0;
+    __syncthreads();
+    for (int start = 0; start < nblocks; start += 1024) {
+        const int b = start + t;
+        const uint32_t v = b < nblocks ? block_live[b] : 0u;
+        uint32_t x = v;
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        if (lane == 31) warp_sums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = warp_sums[lane];
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, w, off);
+                if (lane >= off) w += y;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        const uint32_t inclusive = x + (warp > 0 ? warp_sums[warp - 1] : 0u) + carry;
+        if (b < nblocks) offsets[b] = inclusive - v;
+        __syncthreads();
+        if (t == 1023) carry = inclusive;
+        __syncthreads();
+    }
+}
+
 // act_out = the live trajectories of act, in order, and *live_out their count, from a
-// window's per-block counts and flags (the window's grid of 128-thread blocks).
+// window's per-block counts and flags (the window's grid of 128-thread blocks); `offsets`,
+// when not NULL, holds each block's count of the live trajectories before it.
 __global__ void __launch_bounds__(128) compact_live(const i64 *__restrict__ act,
                                                     const uint8_t *__restrict__ alive,
                                                     const uint32_t *__restrict__ block_live,
+                                                    const uint32_t *__restrict__ offsets,
                                                     i64 stride, i64 *__restrict__ act_out,
                                                     i64 *__restrict__ live_out) {
     __shared__ uint32_t part[4], warp_first[4];
     const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
     uint32_t before = 0;  // the live trajectories of the blocks before this one
-    for (int q = t; q < b; q += 128) before += block_live[q];
+    if (offsets)
+        before = t == 0 ? offsets[b] : 0u;
+    else
+        for (int q = t; q < b; q += 128) before += block_live[q];
     for (int off = 16; off > 0; off >>= 1) before += __shfl_down_sync(0xffffffffu, before, off);
     if (lane == 0) part[warp] = before;
     const i64 m = (i64)b * 128 + t;
@@ -809,7 +854,9 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         }
         int64_t *act_a = ts.active_a.as<int64_t>(a.n_active);
         int64_t *act_b = ts.active_b.as<int64_t>(a.n_active);
-        uint32_t *block_live = ts.block_counts.as<uint32_t>(bt::blocks_for(a.n_active, 128));
+        // the window's per-block live counts, and room after them for their offsets
+        uint32_t *block_live =
+            ts.block_counts.as<uint32_t>(2 * (size_t)bt::blocks_for(a.n_active, 128));
         uint8_t *alive = ts.alive.as<uint8_t>(a.n_active);
         // live[2]: the live count before and after a window's compaction; records_end[2]:
         // where the slots of each buffer's last window with live trajectories end
@@ -887,8 +934,14 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                 BT_CHECK_LAUNCH();
                 used += need;
                 ctx->last_windows += 1;
-                BT_LAUNCH(ctx, bt::compact_live, grid, 128, 0, st, act_a, alive, block_live, bound,
-                          act_b, live + (lv ^ 1));
+                uint32_t *offsets = nullptr;
+                if (grid > (unsigned)bt::kSumBlocks) {
+                    offsets = block_live + grid;
+                    BT_LAUNCH(ctx, bt::block_offsets, 1, 1024, 0, st, block_live, (int)grid,
+                              offsets);
+                }
+                BT_LAUNCH(ctx, bt::compact_live, grid, 128, 0, st, act_a, alive, block_live,
+                          offsets, bound, act_b, live + (lv ^ 1));
                 BT_CHECK_LAUNCH();
                 std::swap(act_a, act_b);
                 lv ^= 1;

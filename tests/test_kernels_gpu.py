@@ -156,3 +156,40 @@ def test_deposit_sorts_keys_of_every_width(kernels, shape):
     )
     np.testing.assert_allclose(charge.cpu().numpy(), expected, rtol=0,
                                atol=1e-12 * np.abs(expected).max())  # fmt: skip
+
+
+def test_trace_of_many_copies_equals_one(kernels):
+    """A golden case tiled 5,625 times (270,000 trajectories, windows of 2,110 blocks: the
+    compaction's scanned block offsets): every copy ends as the single case ends, bit for
+    bit, and the node charges are 5,625 times the single case's."""
+    args, _ = load_golden("trace_c1_i0_r1_g0_rel0")
+    n = args[1].shape[1]
+    copies = 270_000 // n
+    single = to_device(args)
+    single[TRACE_CHARGE] = single[TRACE_CHARGE][:1].clone()
+    kernels["trace_trajectories_2d"](*single, window=64)
+    single = to_host(single)
+    tiled = list(args)
+    tiled[0] = np.concatenate([args[0] + c * n for c in range(copies)])
+    for i in (1, 2):
+        tiled[i] = np.tile(args[i], (1, copies))
+    for i in (3, 4, 5, 6, 7):
+        tiled[i] = np.tile(args[i], copies)
+    tiled[25] = np.tile(args[25], (copies, 1, 1, 1))
+    tiled[26] = np.tile(args[26], (copies, 1))
+    tiled[27] = np.concatenate([args[27], np.full(n * (copies - 1), -1, dtype=np.int64)])
+    device = to_device(tiled)
+    device[TRACE_CHARGE] = device[TRACE_CHARGE][:1].clone() * 0.0
+    kernels["trace_trajectories_2d"](*device, window=64)
+    result = to_host(device)
+    for key, i in TRACE_OUTPUTS.items():
+        if key in ("paths", "path_count"):
+            np.testing.assert_array_equal(result[i], single[i], err_msg=key)
+            continue
+        axis = 1 if key in ("x", "v") else 0
+        for c in (0, copies // 2, copies - 1):
+            part = np.take(result[i], np.arange(c * n, (c + 1) * n), axis=axis)
+            np.testing.assert_array_equal(part, single[i], err_msg=f"{key}, copy {c}")
+    expected = copies * (single[TRACE_CHARGE][0] - args[TRACE_CHARGE][0])
+    scale = np.abs(expected).max()
+    np.testing.assert_allclose(result[TRACE_CHARGE][0], expected, rtol=0, atol=1e-11 * scale)
