@@ -321,6 +321,26 @@ struct Phases {
 // and a node's colour follows from its place in the tile.
 __host__ __device__ inline int stage_halo(int count) { return (count + 1) & ~1; }
 
+// (P xc)[f], the prolongation of the coarse correction xc to the fine node f of an active
+// fine node (the bilinear weights of the fine node's coarse neighbours, in (sx, sy) order).
+template <class Load>
+__device__ __forceinline__ double prolong_sum(const Fine &F, i64 f, const double *xc, Load load) {
+    const i64 k = f / F.ny, l = f - k * F.ny;
+    const i64 ix = F.lox[k], iy = F.loy[l];
+    const double wx = F.wx[k], wy = F.wy[l];
+    double s = 0.0;
+    for (int sx = 0; sx < 2; ++sx) {
+        const double px = sx ? 1.0 - wx : wx;
+        if (px == 0.0 || ix + sx >= F.ncx) continue;
+        for (int sy = 0; sy < 2; ++sy) {
+            const double py = sy ? 1.0 - wy : wy;
+            if (py == 0.0 || iy + sy >= F.ncy) continue;
+            s += px * py * load(xc + (ix + sx) * F.ncy + iy + sy);
+        }
+    }
+    return s;
+}
+
 __host__ __device__ inline size_t stage_smem(bool nine, int tx, int ty, int halo) {
     const size_t m = (size_t)(tx + 2 * halo) * (ty + 2 * halo);
     return m * sizeof(double) * (nine ? 11 : 7) + m;
@@ -331,7 +351,9 @@ __global__ void __launch_bounds__(kStageThreads) smooth_staged(
     i64 nx, i64 ny, const double *__restrict__ c4, const double *__restrict__ diag,
     const double *__restrict__ a9, const uint8_t *__restrict__ active,
     const double *__restrict__ b, const double *__restrict__ xin, double *__restrict__ xout,
-    int tx, int ty, Phases ph) {
+    int tx, int ty, Phases ph, Fine F, const double *__restrict__ xc) {
+    // xc, when not NULL: the coarse correction, prolonged onto x as it is read (the values
+    // prolong_add would leave in xin)
     extern __shared__ double sm[];
     constexpr int Q = NINE ? 9 : 5;  // coefficients per node (5-point: w, e, s, n, diagonal)
     constexpr int K = NINE ? 4 : 2;  // colours
@@ -361,6 +383,7 @@ __global__ void __launch_bounds__(kStageThreads) smooth_staged(
             xv = xin[f];
             av = active[f];
             if (av) {
+                if (xc) xv = xv + prolong_sum(F, f, xc, PlainLoad{});
                 bv = b[f];
                 if (NINE) {
 #pragma unroll
@@ -531,20 +554,7 @@ template <class Load>
 __device__ __forceinline__ void prolong_item(i64 f, const Fine &F, const double *xc, double *x,
                                              Load load) {
     if (!F.active[f]) return;
-    const i64 k = f / F.ny, l = f - k * F.ny;
-    const i64 ix = F.lox[k], iy = F.loy[l];
-    const double wx = F.wx[k], wy = F.wy[l];
-    double s = 0.0;
-    for (int sx = 0; sx < 2; ++sx) {
-        const double px = sx ? 1.0 - wx : wx;
-        if (px == 0.0 || ix + sx >= F.ncx) continue;
-        for (int sy = 0; sy < 2; ++sy) {
-            const double py = sy ? 1.0 - wy : wy;
-            if (py == 0.0 || iy + sy >= F.ncy) continue;
-            s += px * py * load(xc + (ix + sx) * F.ncy + iy + sy);
-        }
-    }
-    x[f] = load(x + f) + s;
+    x[f] = load(x + f) + prolong_sum(F, f, xc, load);
 }
 
 __global__ void prolong_add(Fine F, const double *__restrict__ xc, double *__restrict__ x) {
@@ -1446,7 +1456,11 @@ void drop_graphs(bt_poisson *p) {
 // on level 0, four-colour sweeps on 9-point levels, the colours reversed afterwards; the
 // phases in shared-memory staged launches (up to kMaxPhases each) that move x between the
 // level's two buffers, or one in-place launch per colour.
-void smooth(bt_poisson *p, size_t l, bool pre) {
+// The level's smoothing sweeps; with xc, after adding the prolonged coarse correction
+// (P of the fine-coarse pair `pf`) to x: in the first staged launch's read of x, or by
+// prolong_add.
+void smooth(bt_poisson *p, size_t l, bool pre, const Fine *pf = nullptr,
+            const double *xc = nullptr) {
     cudaStream_t st = p->ctx->stream;
     Level &L = p->levels[l];
     const int T = 256;
@@ -1471,18 +1485,20 @@ void smooth(bt_poisson *p, size_t l, bool pre) {
             const int own = (per + kStageThreads - 1) / kStageThreads;
             double *x = L.x.as<double>(L.n);
             double *in = L.cur, *out = L.cur == x ? L.x2.as<double>(L.n) : x;
+            const Fine F = start == 0 && xc ? *pf : Fine{};
+            const double *add = start == 0 ? xc : nullptr;
             if (five && own <= 2)
                 BT_LAUNCH(p->ctx, (smooth_staged<false, 2>), tiles, kStageThreads, smem, st, L.nx,
                           L.ny, L.c4.as<double>(4 * L.n), L.diag.as<double>(L.n),
-                          (const double *)nullptr, act, b, in, out, tx, ty, ph);
+                          (const double *)nullptr, act, b, in, out, tx, ty, ph, F, add);
             else if (five && own == 3)
                 BT_LAUNCH(p->ctx, (smooth_staged<false, 3>), tiles, kStageThreads, smem, st, L.nx,
                           L.ny, L.c4.as<double>(4 * L.n), L.diag.as<double>(L.n),
-                          (const double *)nullptr, act, b, in, out, tx, ty, ph);
+                          (const double *)nullptr, act, b, in, out, tx, ty, ph, F, add);
             else if (!five && own == 1)
                 BT_LAUNCH(p->ctx, (smooth_staged<true, 1>), tiles, kStageThreads, smem, st, L.nx,
                           L.ny, (const double *)nullptr, (const double *)nullptr,
-                          L.a9.as<double>(9 * L.n), act, b, in, out, tx, ty, ph);
+                          L.a9.as<double>(9 * L.n), act, b, in, out, tx, ty, ph, F, add);
             else
                 BT_REQUIRE(false, "poisson: staged smoothing tile too large for its block");
             L.cur = out;
@@ -1490,6 +1506,7 @@ void smooth(bt_poisson *p, size_t l, bool pre) {
         return;
     }
     double *x = L.cur;
+    if (xc) BT_LAUNCH(p->ctx, prolong_add, blocks_for(L.n, T), T, 0, st, *pf, xc, x);
     for (int c : order) {
         if (five) {
             const i64 per = L.nx * ((L.ny + 1) / 2);
@@ -1540,8 +1557,7 @@ void vcycle(bt_poisson *p, size_t l) {
     BT_LAUNCH(p->ctx, restrict_residual, blocks_for(C.n, T), T, 0, st, F, r, C.b.as<double>(C.n),
                                                           C.x.as<double>(C.n));
     vcycle(p, l + 1);
-    BT_LAUNCH(p->ctx, prolong_add, blocks_for(L.n, T), T, 0, st, F, C.x.as<double>(C.n), L.cur);
-    smooth(p, l, false);
+    smooth(p, l, false, &F, C.x.as<double>(C.n));
     if (L.cur != L.x.as<double>(L.n))
         BT_CUDA(cudaMemcpyAsync(L.x.as<double>(L.n), L.cur, sizeof(double) * L.n,
                                 cudaMemcpyDeviceToDevice, st));
