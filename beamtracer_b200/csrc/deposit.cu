@@ -5,9 +5,10 @@
 //
 // The per-record shape is the reference's area weighting
 // (kernels/deposit_trajectories_2d/deposit_trajectories_2d_pyccel.py:28-59,
-//  kernels/trace_trajectories_2d/trace_trajectories_2d_pyccel.py:397-423): a record
-// (cell c, u, w, q) adds (1-u)(1-w)q, (1-u)w q, u(1-w)q and u w q to the nodes c, c+1,
-// c+ny, c+ny+1.
+//  kernels/trace_trajectories_2d/trace_trajectories_2d_pyccel.py:397-423): a charge q at
+// (u, w) in cell c adds (1-u)(1-w)q, (1-u)w q, u(1-w)q and u w q to the nodes c, c+1,
+// c+ny, c+ny+1; a record holds those four charges (the sums of a run of a trajectory's
+// steps in one cell, from the tracer), and its key the cell, or the sentinel for none.
 #include <mutex>
 
 #include "common.cuh"
