@@ -1035,9 +1035,20 @@ __global__ void __launch_bounds__(kDotThreads) dot_pass(
     __threadfence();
     // the last block: warp w adds the blocks' partials of q = w, w + 8, ... (lanes stride
     // the blocks, then a fixed tree)
+    // the blocks' partials are read together, then added in block order
+    constexpr int kPer = (kDotBlocks + 31) / 32;
+    const int blocks = (int)gridDim.x;
     for (int q = warp; q < sums; q += kDotThreads / 32) {
+        double part[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int b = lane + 32 * k;
+            part[k] = b < blocks ? __ldcg(partial + (i64)b * kDotMax + q) : 0.0;
+        }
         double v = 0.0;
-        for (int b = lane; b < (int)gridDim.x; b += 32) v += __ldcg(partial + (i64)b * kDotMax + q);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k)
+            if (lane + 32 * k < blocks) v += part[k];
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
         if (lane == 0) out[q] = v;
     }
@@ -1076,23 +1087,40 @@ __global__ void arnoldi_step(Arnoldi *__restrict__ a, double *__restrict__ H,
                              double *__restrict__ g, const double *__restrict__ h1,
                              const double *__restrict__ h2, const double *__restrict__ norm2,
                              int j, int m) {
-    if (threadIdx.x != 0 || a->done || a->j != j) return;
-    for (int q = 0; q <= j; ++q) H[q * m + j] = h1[q] + h2[q];
-    const double hn = sqrt(norm2[0]);
-    H[(j + 1) * m + j] = hn;
-    for (int q = 0; q < j; ++q) {
-        const double x = H[q * m + j], y = H[(q + 1) * m + j];
-        H[q * m + j] = cs[q] * x + sn[q] * y;
-        H[(q + 1) * m + j] = -sn[q] * x + cs[q] * y;
+    // the warp reads the column's coefficients and the rotations together; one thread then
+    // rotates the column in shared memory and writes it out
+    __shared__ double col[kDotMax + 2], c[kDotMax], sv[kDotMax];
+    __shared__ int skip;
+    const int t = threadIdx.x;
+    if (t == 0) skip = a->done || a->j != j;
+    __syncthreads();
+    if (skip) return;
+    for (int q = t; q <= j; q += blockDim.x) col[q] = h1[q] + h2[q];
+    for (int q = t; q < j; q += blockDim.x) {
+        c[q] = cs[q];
+        sv[q] = sn[q];
     }
-    const double x = H[j * m + j], y = H[(j + 1) * m + j];
+    __syncthreads();
+    if (t != 0) return;
+    const double hn = sqrt(norm2[0]);
+    col[j + 1] = hn;
+    for (int q = 0; q < j; ++q) {
+        const double x = col[q], y = col[q + 1];
+        col[q] = c[q] * x + sv[q] * y;
+        col[q + 1] = -sv[q] * x + c[q] * y;
+    }
+    const double x = col[j], y = col[j + 1];
     const double rr = hypot(x, y);
-    cs[j] = rr > 0.0 ? x / rr : 1.0;
-    sn[j] = rr > 0.0 ? y / rr : 0.0;
-    H[j * m + j] = rr;
-    H[(j + 1) * m + j] = 0.0;
-    g[j + 1] = -sn[j] * g[j];
-    g[j] = cs[j] * g[j];
+    const double cj = rr > 0.0 ? x / rr : 1.0;
+    const double sj = rr > 0.0 ? y / rr : 0.0;
+    col[j] = rr;
+    col[j + 1] = 0.0;
+    for (int q = 0; q <= j + 1; ++q) H[q * m + j] = col[q];
+    cs[j] = cj;
+    sn[j] = sj;
+    const double gj = g[j];
+    g[j + 1] = -sj * gj;
+    g[j] = cj * gj;
     a->j = j + 1;
     a->resid[j + 1] = fabs(g[j + 1]);
     if (fabs(g[j + 1]) <= a->tol || hn == 0.0) a->done = 1;
