@@ -220,9 +220,9 @@ __device__ __forceinline__ double inv_gamma(double u0, double u1, double u2, dou
 // window with live trajectories sets *records_end to `end`, the end of its slots, so the
 // deposit sorts no window that had none.
 //
-// MINB, the blocks an SM must hold: 1 (the registers the compiler wants) for a window of at
-// most about two blocks per SM, where one warp per scheduler is all there is; 3 (at most
-// 168 registers) for larger windows, whose warps hide each other's latency.
+// At most 168 registers, so that an SM holds three blocks: measured as fast as the
+// registers the compiler wants on a window of one block per SM (the einzel lens) and
+// faster on larger windows and on concurrent solves, whose warps hide each other's latency.
 //
 // One thread's window (m < stride): whether its trajectory is still live afterwards.
 template <int CYL, int INTEG, bool GENERAL, bool MAG>
@@ -674,8 +674,8 @@ __device__ __forceinline__ bool trace_thread(const Trace &tr, const i64 *__restr
 
 // The window: every thread's trajectory, then each block's count of live trajectories and
 // every thread's flag, for compact_live.
-template <int CYL, int INTEG, bool GENERAL, bool MAG, int MINB>
-__global__ void __launch_bounds__(128, MINB)
+template <int CYL, int INTEG, bool GENERAL, bool MAG>
+__global__ void __launch_bounds__(128, 3)
     trace_window(Trace tr, const i64 *__restrict__ act, const i64 *__restrict__ live, i64 stride,
                  int S, uint32_t *__restrict__ keys, DepositRec *__restrict__ rec,
                  uint32_t sentinel, i64 *__restrict__ records_end, i64 end,
@@ -902,21 +902,13 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                 {
                     bt::Timed timed(ctx, "trace_window");
                     grid = (unsigned)bt::blocks_for(bound, 128);
-                    const bool busy = grid > 2u * (unsigned)ctx->num_sms;
                     const int64_t launched = ctx->launch_count;
 #define BT_TRACE_CASE(C, I, G, M)                                                               \
     if (a.cylindrical == C && (a.integrator != 0) == (I != 0) && general == G &&                 \
         (mag != nullptr) == M)                                                                   \
-    {                                                                                            \
-        if (busy)                                                                                \
-            BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M, 3>), grid, 128, 0, st, tr, act_a,       \
-                      live + lv, bound, S, keys[cur] + used, rec[cur] + used, sentinel,          \
-                      records_end + cur, used + need, block_live, alive);                        \
-        else                                                                                     \
-            BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M, 1>), grid, 128, 0, st, tr, act_a,       \
-                      live + lv, bound, S, keys[cur] + used, rec[cur] + used, sentinel,          \
-                      records_end + cur, used + need, block_live, alive);                        \
-    }
+        BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M>), grid, 128, 0, st, tr, act_a, live + lv,   \
+                  bound, S, keys[cur] + used, rec[cur] + used, sentinel, records_end + cur,       \
+                  used + need, block_live, alive);
                     BT_TRACE_CASE(0, 0, false, false) BT_TRACE_CASE(0, 0, true, false)
                     BT_TRACE_CASE(0, 1, false, false) BT_TRACE_CASE(0, 1, true, false)
                     BT_TRACE_CASE(1, 0, false, false) BT_TRACE_CASE(1, 0, true, false)
