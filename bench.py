@@ -55,10 +55,10 @@ NOMINAL_FP64_TFLOPS = 37.0
 #: of steps in one cell.
 TRACE_BYTES_PER_STEP = 28
 #: DRAM bytes read + written per trace_window launch at this workload: ncu's
-#: dram__bytes_read.sum + dram__bytes_write.sum averaged over the 175 launches of one
-#: converged solve (1.864 MB read, 0.026 MB written; the records it writes stay in L2 and
-#: drain during the deposit).
-TRACE_DRAM_BYTES_PER_LAUNCH = 1.890e6
+#: dram__bytes_read.sum + dram__bytes_write.sum over launches 21-25 of one converged solve
+#: (1.957 MB read, 0.124 MB written on average; the records it writes stay in L2 and drain
+#: during the deposit).
+TRACE_DRAM_BYTES_PER_LAUNCH = 2.081e6
 #: Timed end-to-end calls (after one untimed call); their median is reported.
 E2E_RUNS = 5
 
