@@ -11,7 +11,8 @@
 namespace bt {
 namespace {
 
-constexpr int kShapeRect = 0, kShapeCircle = 1, kShapePolygon = 2, kShapeAperture = 3;
+// shape kinds; 3 is an aperture (a polygon and its mirror image)
+constexpr int kShapeRect = 0, kShapeCircle = 1, kShapePolygon = 2;
 constexpr int kEdgeWords = 9;  // x1, y1, x2, y2, threshold, x_lo, x_hi, y_lo, y_hi
 
 // Inside the polygon at p (p[0] its edge count, then its edges) or on its boundary.

@@ -849,7 +849,6 @@ vcycle_tail(const TailLevel *__restrict__ levels, const TailPlan *__restrict__ p
     uint8_t *smb = reinterpret_cast<uint8_t *>(smi + ints);
     double *smd = sm + 2 * image_words;  // the dynamic doubles follow the image
     const int tid = threadIdx.x, nt = blockDim.x;
-    const PlainLoad load{};
     {
         const int *src = reinterpret_cast<const int *>(plans);
         int *dst = reinterpret_cast<int *>(plan);
