@@ -99,6 +99,7 @@ SIGNATURES: dict[str, list] = {
     "bt_ctx_read_timer": [P, ctypes.c_char_p, ctypes.POINTER(F64), ctypes.POINTER(I64)],
     "bt_ctx_reset_timers": [P],
     "bt_ctx_launch_count": [P, ctypes.POINTER(I64)],
+    "bt_ctx_deposit_records": [P, ctypes.POINTER(I64)],
     "bt_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "bt_version": [],
     "bt_staggered_field_2d": [P, P, P, I64, P, P, I64, I64, F64, F64, F64, P, P],
@@ -191,6 +192,12 @@ class Context:
         """The kernels this context has launched since its creation."""
         count = I64()
         check(lib().bt_ctx_launch_count(self.handle, ctypes.byref(count)))
+        return count.value
+
+    def deposit_records(self) -> int:
+        """The records the deposits reduced while timing was on, since the last reset."""
+        count = I64()
+        check(lib().bt_ctx_deposit_records(self.handle, ctypes.byref(count)))
         return count.value
 
     def reset_timers(self) -> None:

@@ -225,6 +225,9 @@ int bt_ctx_create(int device, bt_ctx **out) {
 int bt_ctx_set_timing(bt_ctx *ctx, int on) {
     return bt::guarded([&] {
         BT_REQUIRE(ctx, "ctx: null context");
+        if (on && !ctx->timing)  // the record count starts from zero with the timing
+            BT_CUDA(cudaMemsetAsync(ctx->kept_records.as<int64_t>(1), 0, sizeof(int64_t),
+                                    ctx->stream));
         ctx->timing = on != 0;
     });
 }
@@ -260,6 +263,17 @@ int bt_ctx_reset_timers(bt_ctx *ctx) {
             kv.second.total_ms = 0.0;
             kv.second.launches = 0;
         }
+        BT_CUDA(cudaMemsetAsync(ctx->kept_records.as<int64_t>(1), 0, sizeof(int64_t),
+                                ctx->stream));
+    });
+}
+
+int bt_ctx_deposit_records(bt_ctx *ctx, int64_t *records) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx && records, "ctx: null argument");
+        BT_CUDA(cudaStreamSynchronize(ctx->stream));
+        BT_CUDA(cudaMemcpy(records, ctx->kept_records.as<int64_t>(1), sizeof(int64_t),
+                           cudaMemcpyDeviceToHost));
     });
 }
 

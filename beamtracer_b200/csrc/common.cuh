@@ -144,6 +144,7 @@ struct bt_ctx {
     bt::TraceScratch trace;
     bt::HostBuffer host;
     bt::Buffer reduce_partial;  // per-block partial results of the device reductions
+    bt::Buffer kept_records;    // (device i64) records the deposits reduced while timing
     i64 launch_count = 0;       // kernels launched on the context since its creation
     i64 last_windows = 0, last_records = 0, last_flushes = 0;
 };

@@ -9,7 +9,6 @@
 // (u, w) in cell c adds (1-u)(1-w)q, (1-u)w q, u(1-w)q and u w q to the nodes c, c+1,
 // c+ny, c+ny+1; a record holds those four charges (the sums of a run of a trajectory's
 // steps in one cell, from the tracer), and its key the cell, or the sentinel for none.
-#include <mutex>
 
 #include "common.cuh"
 
@@ -463,6 +462,11 @@ void radix_sort_pairs(bt_ctx *ctx, const uint32_t *keys_in, i64 n, const i64 *n_
     *count_out = sorted;
 }
 
+// total += the count of records a sort kept (measurement only: runs while timing is on)
+__global__ void add_kept(const i64 *__restrict__ kept, i64 n_records, i64 *__restrict__ total) {
+    *total += kept ? *kept : n_records;
+}
+
 void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i64 n_records,
                      const i64 *n_dev, uint32_t sentinel, double *charge,
                      const NodeLayout &layout) {
@@ -473,6 +477,9 @@ void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i
     const i64 *n_sorted = nullptr;  // the records with a charge, on the device
     radix_sort_pairs(ctx, keys, n_records, n_dev, bits_for(sentinel), sentinel, &sk, &sv,
                      &n_sorted);
+    if (ctx->timing)
+        BT_LAUNCH(ctx, add_kept, 1, 1, 0, st, n_sorted, n_records,
+                  ctx->kept_records.as<i64>(1));
     const i64 n_warps = (n_records + 31) / 32;
     double4 *cells = s.cell_sums.as<double4>((size_t)layout.n_nodes);
     double4 *first = s.warp_first.as<double4>((size_t)n_warps);
@@ -546,20 +553,16 @@ constexpr size_t kNoallocBytes = kOffFlags + align256(2 * kNoallocWarps);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
-// The device address of the array on each device, looked up on the first call there
-// (with that device current); the name itself is only a host-side stand-in.
-std::mutex g_noalloc_mutex;
-void *g_noalloc_address[64] = {};
-
-unsigned char *noalloc_scratch(int device) {
-    BT_REQUIRE(device >= 0 && device < 64, "deposit (no allocation): device index too large");
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_address[device]) {
-        void *address = nullptr;
-        BT_CUDA(cudaGetSymbolAddress(&address, g_noalloc_scratch));
-        g_noalloc_address[device] = address;
-    }
-    return static_cast<unsigned char *>(g_noalloc_address[device]);
+// The device address of the array in the current device's context, looked up on every
+// call: the name itself is only a host-side stand-in, and an address kept from an earlier
+// call would dangle once that context is torn down (cudaDeviceReset, or the primary
+// context released and made again) and the module loaded anew.  The lookup is a host
+// call; the first one in a context may load the module there.
+unsigned char *noalloc_scratch() {
+    void *address = nullptr;
+    BT_CUDA(cudaGetSymbolAddress(&address, g_noalloc_scratch));
+    BT_REQUIRE(address != nullptr, "deposit (no allocation): no device address for its scratch");
+    return static_cast<unsigned char *>(address);
 }
 
 }  // namespace
@@ -582,9 +585,7 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
                    "static scratch; use bt_deposit_trajectories_2d");
         if (n == 0) return;
         BT_REQUIRE(px && py && q && charge, "deposit (no allocation): null array");
-        int device = 0;
-        BT_CUDA(cudaGetDevice(&device));
-        unsigned char *base = noalloc_scratch(device);
+        unsigned char *base = noalloc_scratch();
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         uint32_t *keys = reinterpret_cast<uint32_t *>(base + kOffKeys);
         uint32_t *keys_alt = keys + kNoallocPoints;

@@ -1162,15 +1162,20 @@ __global__ void combine(const double *__restrict__ Z, const double *__restrict__
     x[f] = s;
 }
 
-// max |v| over the array (one block, deterministic)
+// the larger of two values, NaN if either is (a NaN update must not read as converged)
+__device__ __forceinline__ double max_nan(double m, double v) {
+    return (v > m || v != v) ? v : m;
+}
+
+// max |v| over the array (one block, deterministic; NaN if any entry is NaN)
 __global__ void max_abs(const double *__restrict__ v, i64 n, double *__restrict__ out) {
     __shared__ double part[256];
     double s = 0.0;
-    for (i64 f = threadIdx.x; f < n; f += blockDim.x) s = fmax(s, fabs(v[f]));
+    for (i64 f = threadIdx.x; f < n; f += blockDim.x) s = max_nan(s, fabs(v[f]));
     part[threadIdx.x] = s;
     __syncthreads();
     for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-        if (threadIdx.x < off) part[threadIdx.x] = fmax(part[threadIdx.x], part[threadIdx.x + off]);
+        if (threadIdx.x < off) part[threadIdx.x] = max_nan(part[threadIdx.x], part[threadIdx.x + off]);
         __syncthreads();
     }
     if (threadIdx.x == 0) *out = part[0];

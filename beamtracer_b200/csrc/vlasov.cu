@@ -11,11 +11,17 @@ namespace {
 constexpr int kReduceThreads = 256;
 constexpr int kReduceBlocks = 296;  // 2 per SM of a B200
 
+// The larger of two values, NaN if either is NaN (fmax would drop a NaN, and a NaN
+// potential or density would then read as converged; the reference's np.max keeps it).
+__device__ __forceinline__ double max_nan(double m, double v) {
+    return (v > m || v != v) ? v : m;
+}
+
 __device__ __forceinline__ double block_max(double v, double *part) {
     part[threadIdx.x] = v;
     __syncthreads();
     for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-        if (threadIdx.x < off) part[threadIdx.x] = fmax(part[threadIdx.x], part[threadIdx.x + off]);
+        if (threadIdx.x < off) part[threadIdx.x] = max_nan(part[threadIdx.x], part[threadIdx.x + off]);
         __syncthreads();
     }
     return part[0];
@@ -35,8 +41,8 @@ __global__ void mix(const double *__restrict__ charge, const double *__restrict_
         const double old = rho[f];
         const double next = first ? deposit : (1.0 - w) * old + w * deposit;
         rho[f] = next;
-        dmax = fmax(dmax, fabs(next - old));
-        rmax = fmax(rmax, fabs(next));
+        dmax = max_nan(dmax, fabs(next - old));
+        rmax = max_nan(rmax, fabs(next));
     }
     const double a = block_max(dmax, part);
     __syncthreads();
@@ -53,7 +59,7 @@ __global__ void diff_max(const double *__restrict__ a, const double *__restrict_
     double m = 0.0;
     for (i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x; f < n;
          f += (i64)gridDim.x * blockDim.x)
-        m = fmax(m, fabs(a[f] - b[f]));
+        m = max_nan(m, fabs(a[f] - b[f]));
     const double r = block_max(m, part);
     if (threadIdx.x == 0) partial[blockIdx.x] = r;
 }
@@ -63,7 +69,7 @@ __global__ void finish_max(const double *__restrict__ partial, int blocks, int s
     __shared__ double part[kReduceThreads];
     for (int c = 0; c < stride; ++c) {
         double m = 0.0;
-        for (int bi = threadIdx.x; bi < blocks; bi += blockDim.x) m = fmax(m, partial[bi * stride + c]);
+        for (int bi = threadIdx.x; bi < blocks; bi += blockDim.x) m = max_nan(m, partial[bi * stride + c]);
         const double r = block_max(m, part);
         if (threadIdx.x == 0) out[c] = r;
         __syncthreads();

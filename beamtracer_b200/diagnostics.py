@@ -1,15 +1,21 @@
 """Beam quantities at a diagnostic plane: current, rms sizes and angles, emittance, Twiss.
 
 The interface of the reference's ``solver/diagnostics.py`` (``BeamMoments``,
-``plane_moments``, ``mismatch``; ``diagnostics.py:15-170``): current-weighted moments over
-the forward crossings of a plane, in cylindrical geometry of every ring projected on one
-transverse plane (``<x^2> = <r^2>/2``, ``<x'^2> = <r'^2 + a'^2>/2``, ``<x x'> = <r r'>/2``),
-in planar geometry about the means.
+``plane_moments``, ``mismatch``; ``diagnostics.py:15-170``).  The moments are weighted by
+the crossings' currents.  A ring (cylindrical geometry) is projected on one transverse
+plane and averaged over its azimuth, which gives, without dividing by the radius,
+
+    <x^2> = <y^2 + z^2> / 2,   <x x'> = <(y v_y + z v_z) / v_x> / 2,
+    <x'^2> = <(v_y^2 + v_z^2) / v_x^2> / 2
+
+(the rotation to (v_r, v_theta) keeps v_y^2 + v_z^2, and r v_r = y v_y + z v_z); planar
+moments are taken about the means.  The rms ellipse of the 2 x 2 second-moment matrix gives
+the emittance (the square root of its determinant) and the Twiss parameters.
 """
 
 from __future__ import annotations
 
-from dataclasses import dataclass
+from dataclasses import dataclass, fields
 
 import numpy as np
 from scipy import constants
@@ -32,7 +38,35 @@ class BeamMoments:
     count: int
 
     def as_dict(self) -> dict[str, float]:
-        return dict(self.__dict__)
+        return {f.name: getattr(self, f.name) for f in fields(self)}
+
+
+def _empty_moments() -> BeamMoments:
+    """No crossings, or no current: zero current and count, every moment NaN."""
+    nan = float("nan")
+    return BeamMoments(0.0, *([nan] * 9), 0)
+
+
+def _second_moments(weight: np.ndarray, point: np.ndarray, velocity: np.ndarray,
+                    cylindrical: bool, axis: str) -> tuple[float, float, float]:  # fmt: skip
+    """``(<x^2>, <x x'>, <x'^2>)`` of the crossings under the normalised weights."""
+
+    def mean(values: np.ndarray) -> float:
+        return float(np.dot(weight, values))
+
+    vx = velocity[0]
+    if cylindrical:
+        y, z = point[1], point[2]
+        vy, vz = velocity[1], velocity[2]
+        return (0.5 * mean(y * y + z * z), 0.5 * mean((y * vy + z * vz) / vx),
+                0.5 * mean((vy * vy + vz * vz) / (vx * vx)))  # fmt: skip
+    if axis not in ("y", "z"):
+        raise ValueError(f"axis must be 'y' or 'z', got {axis!r}")
+    k = 1 if axis == "y" else 2
+    u = point[k]
+    slope = velocity[k] / vx
+    du, dslope = u - mean(u), slope - mean(slope)
+    return mean(du * du), mean(du * dslope), mean(dslope * dslope)
 
 
 def plane_moments(hits, *, cylindrical: bool, mass, species: int | None = None,
@@ -41,72 +75,49 @@ def plane_moments(hits, *, cylindrical: bool, mass, species: int | None = None,
 
     ``mass`` [kg] per species (indexed by ``hits.species``) or one value; only ``species``
     and, with ``forward_only``, crossings in the +x direction count.  No crossings or no
-    current give NaN moments, zero emittance NaN Twiss parameters.
+    current give NaN moments; a zero emittance gives NaN Twiss parameters.
     """
-    keep = np.ones(hits.current.size, dtype=bool)
+    keep = np.ones(np.shape(hits.current), dtype=bool)
     if species is not None:
-        keep &= hits.species == species
+        keep &= np.asarray(hits.species) == species
     if forward_only:
-        keep &= hits.direction > 0
-    w = np.abs(hits.current[keep])
-    point = hits.point[:, keep]
-    vel = hits.velocity[:, keep]
-    masses = np.asarray(mass, dtype=float)
-    m = masses[hits.species[keep]] if masses.ndim else np.full(w.size, float(masses))
-    total = float(w.sum())
-    if w.size == 0 or total == 0.0:
-        nan = float("nan")
-        return BeamMoments(0.0, nan, nan, nan, nan, nan, nan, nan, nan, nan, 0)
-    vx = vel[0]
-    if cylindrical:
-        r = np.hypot(point[1], point[2])
-        with np.errstate(invalid="ignore", divide="ignore"):
-            cy = np.where(r > 0, point[1] / r, 1.0)
-            cz = np.where(r > 0, point[2] / r, 0.0)
-        vr = vel[1] * cy + vel[2] * cz
-        vt = vel[2] * cy - vel[1] * cz
-        rp, ap = vr / vx, vt / vx
-        xx = np.sum(w * r * r) / (2.0 * total)
-        pp = np.sum(w * (rp * rp + ap * ap)) / (2.0 * total)
-        xp = np.sum(w * r * rp) / (2.0 * total)
-    else:
-        if axis not in ("y", "z"):
-            raise ValueError(f"axis must be 'y' or 'z', got {axis!r}")
-        a = 1 if axis == "y" else 2
-        y = point[a]
-        yp = vel[a] / vx
-        my = np.sum(w * y) / total
-        myp = np.sum(w * yp) / total
-        xx = np.sum(w * (y - my) ** 2) / total
-        pp = np.sum(w * (yp - myp) ** 2) / total
-        xp = np.sum(w * (y - my) * (yp - myp)) / total
+        keep &= np.asarray(hits.direction) > 0
+    current = np.abs(np.asarray(hits.current, dtype=float)[keep])
+    total = float(current.sum())
+    if total == 0.0:
+        return _empty_moments()
+    weight = current / total
+    point = np.asarray(hits.point, dtype=float)[:, keep]
+    velocity = np.asarray(hits.velocity, dtype=float)[:, keep]
+    xx, xp, pp = _second_moments(weight, point, velocity, cylindrical, axis)
     emittance = float(np.sqrt(max(xx * pp - xp * xp, 0.0)))
-    speed2 = np.sum(vel * vel, axis=0)
+
+    # relativistic factors of every crossing (NaN at or above the speed of light)
+    speed2 = np.einsum("ij,ij->j", velocity, velocity)
     with np.errstate(invalid="ignore", divide="ignore"):
         lorentz = 1.0 / np.sqrt(1.0 - speed2 / constants.c**2)
-    beta_gamma = float(np.sum(w * lorentz * vx) / total) / constants.c
-    energy = m * lorentz**2 * speed2 / (lorentz + 1.0) / constants.e
-    twiss = (-xp, xx, pp) if emittance > 0 else (np.nan, np.nan, np.nan)
-    scale = emittance if emittance > 0 else 1.0
+    masses = np.asarray(mass, dtype=float)
+    m = masses[np.asarray(hits.species)[keep]] if masses.ndim else masses
+    # (gamma - 1) m c^2 in a form without cancellation at low speed
+    kinetic = m * lorentz * lorentz * speed2 / (lorentz + 1.0) / constants.e
+    beta_gamma = float(np.dot(weight, lorentz * velocity[0])) / constants.c
+    if emittance > 0.0:
+        alpha, beta, gamma = -xp / emittance, xx / emittance, pp / emittance
+    else:
+        alpha = beta = gamma = float("nan")
     return BeamMoments(
-        current=total,
-        rms_size=float(np.sqrt(xx)),
-        rms_angle=float(np.sqrt(pp)),
-        correlation=float(xp),
-        emittance=emittance,
-        normalized_emittance=emittance * beta_gamma,
-        alpha=float(twiss[0] / scale),
-        beta=float(twiss[1] / scale),
-        gamma=float(twiss[2] / scale),
-        mean_energy=float(np.sum(w * energy) / total),
-        count=int(w.size),
-    )
+        current=total, rms_size=float(np.sqrt(xx)), rms_angle=float(np.sqrt(pp)),
+        correlation=float(xp), emittance=emittance,
+        normalized_emittance=emittance * beta_gamma, alpha=float(alpha), beta=float(beta),
+        gamma=float(gamma), mean_energy=float(np.dot(weight, kinetic)), count=int(current.size),
+    )  # fmt: skip
 
 
 def mismatch(alpha: float, beta: float, alpha0: float, beta0: float) -> float:
     """The mismatch parameter of a beam (alpha, beta) against the design (alpha0, beta0)
-    (Midttun et al., IPAC'17, eq. 1; ``diagnostics.py:138-170``)."""
-    gamma = (1.0 + alpha**2) / beta
-    gamma0 = (1.0 + alpha0**2) / beta0
-    delta = (alpha - alpha0) ** 2 - (gamma - gamma0) * (beta - beta0)
-    return float(np.sqrt(1.0 + (delta + np.sqrt(delta * (delta + 4.0))) / 2.0) - 1.0)
+    (Midttun et al., IPAC'17, eq. 1; the interface of ``diagnostics.py:138-170``): with
+    ``R = (beta gamma0 + beta0 gamma) / 2 - alpha alpha0``, ``M = sqrt(R + sqrt(R^2 - 1)) - 1``,
+    evaluated through ``D = 2 (R - 1)`` so that a matched beam gives exactly 0."""
+    g, g0 = (1.0 + alpha * alpha) / beta, (1.0 + alpha0 * alpha0) / beta0
+    d = (alpha - alpha0) ** 2 - (g - g0) * (beta - beta0)
+    return float(np.sqrt(1.0 + 0.5 * (d + np.sqrt(d * (d + 4.0)))) - 1.0)

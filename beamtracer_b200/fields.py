@@ -115,24 +115,37 @@ class StaggeredElectricField:
         return ex.cpu().numpy(), ey.cpu().numpy()
 
 
+def _derivative_weights() -> np.ndarray:
+    """(7, 7) weights of the central differences over the samples ``i - 3 .. i + 3``: row
+    ``k`` gives ``h^k d^k B / dz^k`` -- orders 6, 6, 4, 4, 2, 2 for ``k = 1 .. 6`` (the widest
+    central stencil of each derivative that seven points hold), the sample itself for 0."""
+    rows = {
+        0: ((0, 0, 0, 1, 0, 0, 0), 1),
+        1: ((-1, 9, -45, 0, 45, -9, 1), 60),
+        2: ((2, -27, 270, -490, 270, -27, 2), 180),
+        3: ((1, -8, 13, 0, -13, 8, -1), 8),
+        4: ((-1, 12, -39, 56, -39, 12, -1), 6),
+        5: ((-1, 4, -5, 0, 5, -4, 1), 2),
+        6: ((1, -6, 15, -20, 15, -6, 1), 1),
+    }  # fmt: skip
+    return np.array([np.array(num, dtype=float) / den for num, den in (rows[k] for k in range(7))])
+
+
 class AxisymmetricMagneticField:
-    """A static axisymmetric magnetic field from its on-axis profile (``fields.py:192-279``).
+    """A static axisymmetric magnetic field from its on-axis profile (the interface of
+    ``fields.py:192-279``).
 
-    ``bz`` [T] sampled at ``z0 + hz k``; off the axis the power series in ``r`` to ``order``
-    (at most 6) with 7-point finite-difference derivatives of the profile, linearly
-    interpolated between the samples.
+    ``bz`` [T] sampled at ``z0 + hz k``.  The derivatives ``B^(k)`` of the profile, to
+    ``order`` (at most 6), are central differences over seven samples at every sample with
+    three neighbours on each side (zero at the three end samples), interpolated linearly
+    between samples and extrapolated along the first and last valid cells.  Off the axis
+    the fields are the current-free series
+
+        B_z = sum_k (-1)^k (r/2)^(2k) B^(2k) / (k!)^2,
+        B_r = sum_k (-1)^(k+1) (r/2)^(2k+1) B^(2k+1) / (k! (k+1)!),
+
+    kept to the terms whose derivative order is at most ``order``.
     """
-
-    #: The derivative stencils (orders 6, 6, 4, 4, 2, 2 for derivatives 1..6).
-    STENCILS = (
-        (0, 0, 0, 1, 0, 0, 0),
-        (-1 / 60, 9 / 60, -45 / 60, 0, 45 / 60, -9 / 60, 1 / 60),
-        (2 / 180, -27 / 180, 270 / 180, -490 / 180, 270 / 180, -27 / 180, 2 / 180),
-        (1 / 8, -8 / 8, 13 / 8, 0, -13 / 8, 8 / 8, -1 / 8),
-        (-1 / 6, 12 / 6, -39 / 6, 56 / 6, -39 / 6, 12 / 6, -1 / 6),
-        (-1 / 2, 4 / 2, -5 / 2, 0, 5 / 2, -4 / 2, 1 / 2),
-        (1, -6, 15, -20, 15, -6, 1),
-    )
 
     def __init__(self, z0: float, hz: float, bz, order: int = 6) -> None:
         samples = np.asarray(bz, dtype=float)
@@ -141,38 +154,38 @@ class AxisymmetricMagneticField:
         if not 0 <= order <= 6:
             raise ValueError(f"order must be 0 to 6, got {order}")
         self.z0, self.hz, self.order, self.bz = float(z0), float(hz), int(order), samples
-        n = samples.size
-        centre = np.arange(3, n - 3)
-        self._derivatives = np.zeros((self.order + 1, n))
-        for k, stencil in enumerate(self.STENCILS[: self.order + 1]):
-            d = sum(c * samples[centre + a - 3] for a, c in enumerate(stencil))
-            self._derivatives[k, centre] = d / self.hz**k
-        self._samples = np.ascontiguousarray(self._derivatives.T)
+        from numpy.lib.stride_tricks import sliding_window_view
+
+        windows = sliding_window_view(samples, 7)  # (n - 6, 7), centred on samples 3 .. n - 4
+        weights = _derivative_weights()[: self.order + 1]
+        scale = self.hz ** -np.arange(self.order + 1, dtype=float)
+        table = np.zeros((samples.size, self.order + 1))
+        table[3:-3] = (windows @ weights.T) * scale
+        #: (n, order + 1): d^k B_z / dz^k at every sample, a row per sample
+        self._samples = np.ascontiguousarray(table)
 
     def derivatives(self, z) -> np.ndarray:
-        n = self.bz.size
+        """``(order + 1, len(z))``: the derivatives of the profile at ``z``."""
         s = (np.asarray(z, dtype=float) - self.z0) / self.hz
-        i = np.clip(np.floor(s).astype(np.int64), 3, n - 5)
-        t = (s - i)[:, None]
-        low = self._samples[i]
-        return (low + t * (self._samples[i + 1] - low)).T
+        cell = np.clip(np.floor(s).astype(np.int64), 3, self.bz.size - 5)
+        t = (s - cell)[:, None]
+        below, above = self._samples[cell], self._samples[cell + 1]
+        return (below + t * (above - below)).T
 
     def __call__(self, z, r) -> tuple[np.ndarray, np.ndarray]:
+        """``(B_z, B_r)`` [T] at axial positions ``z`` and radii ``r``."""
+        from math import factorial
+
         d = self.derivatives(z)
-        r = np.asarray(r, dtype=float)
-        r2 = r * r
-        bz_c = (1.0, -1.0 / 4.0, 1.0 / 64.0, -1.0 / 2304.0)
-        br_c = (-1.0 / 2.0, 1.0 / 16.0, -1.0 / 384.0)
-        bz = d[0].copy()
-        br = np.zeros_like(bz)
-        power = np.ones_like(r2)
-        for k in range(1, self.order // 2 + 1):
-            power = power * r2
-            bz += bz_c[k] * power * d[2 * k]
-        power = r.copy()
-        for k in range((self.order + 1) // 2):
-            br += br_c[k] * power * d[2 * k + 1]
-            power = power * r2
+        half = 0.5 * np.asarray(r, dtype=float)
+        bz = np.zeros(d.shape[1])
+        br = np.zeros(d.shape[1])
+        for n in range(self.order + 1):  # the term of the n-th derivative
+            k = n // 2
+            if n % 2 == 0:
+                bz = bz + ((-1) ** k / factorial(k) ** 2) * half ** (2 * k) * d[n]
+            else:
+                br = br + ((-1) ** (k + 1) / (factorial(k) * factorial(k + 1))) * half ** n * d[n]
         return bz, br
 
     def profile(self) -> MagneticProfile:
@@ -228,13 +241,15 @@ class MagneticProfile:
 
 
 def solenoid_on_axis(z, centre: float, length: float, radius: float, peak: float) -> np.ndarray:
-    """The on-axis B_z [T] of a thin-walled solenoid scaled to ``peak`` at its centre
-    (``fields.py:307-321``)."""
+    """The on-axis B_z [T] of a thin-walled solenoid (a finite current sheet of ``length``
+    and winding ``radius``, centred at ``centre``), scaled to ``peak`` at its centre (the
+    interface of ``fields.py:290-321``): proportional to the difference of the cosines of
+    the angles under which the two ends are seen, ``cos(a1) - cos(a2)``."""
     z = np.asarray(z, dtype=float)
 
-    def shape(zz):
-        a = zz - centre + 0.5 * length
-        b = zz - centre - 0.5 * length
-        return a / np.hypot(a, radius) - b / np.hypot(b, radius)
+    def ends(at):
+        near_end = at - (centre - 0.5 * length)
+        far_end = at - (centre + 0.5 * length)
+        return near_end / np.hypot(near_end, radius) - far_end / np.hypot(far_end, radius)
 
-    return peak * shape(z) / shape(np.asarray(centre))
+    return peak * ends(z) / ends(np.asarray(centre, dtype=float))

@@ -40,14 +40,111 @@ from beamtracer_b200.vlasov import (
     vlasov_iterate,
 )
 
+#: The faces of a mesh and the (direction, side) the configuration names them by.
 _FACES = {"x_min": ("x", "min"), "x_max": ("x", "max"), "y_min": ("y", "min"),
           "y_max": ("y", "max")}  # fmt: skip
+
+#: Magnetic profile samples kept beyond each end of the mesh (the series' stencils need 3).
+_PROFILE_MARGIN = 8
 
 
 def _electrode(name: str, params: ObjectParams) -> Electrode:
     if params.bc_type != "dirichlet" or params.bc_value is None:
         raise ValueError("BeamOptics electrodes need a Dirichlet potential")
     return Electrode(params.inside, float(params.bc_value), name)
+
+
+def config_faces(config: BeamOpticsConfig) -> dict[str, FaceCondition]:
+    """The mesh's face conditions of a configuration (the axis and a symmetry plane are
+    the mesh's own ``y_min``)."""
+    cylindrical = config.grid.coordinates == "cylindrical"
+    faces = {}
+    for face, (direction, side) in _FACES.items():
+        if face == "y_min" and cylindrical:
+            continue
+        bc = config.bcs_field.get_bc(dir=direction, side=side)
+        if face == "y_min" and config.symmetry_plane:
+            zero = not callable(bc.value) and float(bc.value) == 0.0
+            if bc.bc_type != "neumann" or not zero:
+                raise ValueError(
+                    "with symmetry_plane the y lower face needs a zero normal derivative"
+                )
+            continue
+        faces[face] = FaceCondition(bc.bc_type, bc.value)
+    return faces
+
+
+def config_mesh(config: BeamOpticsConfig, *, classify_on_device: bool | None = None
+                ) -> IonOpticsMesh:  # fmt: skip
+    """The `IonOpticsMesh` of a configuration (``classify_on_device=False``: classified on
+    the host alone)."""
+    grid = config.grid
+    return IonOpticsMesh(
+        shape=grid.num_gridpoints, origin=grid.lower_bound, h=grid.deltas[0],
+        geometry="cylindrical" if grid.coordinates == "cylindrical" else "planar",
+        electrodes=[_electrode(name, obj) for name, obj in config.objects.items()],
+        faces=config_faces(config), symmetry_plane=config.symmetry_plane,
+        classify_on_device=classify_on_device,
+    )  # fmt: skip
+
+
+def config_magnetic_field(config: BeamOpticsConfig, mesh: IonOpticsMesh
+                          ) -> AxisymmetricMagneticField | None:  # fmt: skip
+    """The axisymmetric field of the solenoids and the measured axial field (the sampling
+    of ``model.py:169-188``).  Without an axial field the profile is sampled every half
+    node spacing over the mesh and `_PROFILE_MARGIN` samples past each end; the solenoids
+    are added to the axial field's samples or to that zero profile."""
+    if not config.solenoids and config.axial_field is None:
+        return None
+    axial = config.axial_field
+    if axial is not None:
+        z0, dz = float(axial.z0), float(axial.dz)
+        bz = np.array(axial.bz, dtype=float)
+    else:
+        dz = 0.5 * mesh.h
+        z0 = mesh.origin[0] - _PROFILE_MARGIN * dz
+        span = mesh.upper[0] - mesh.origin[0]
+        bz = np.zeros(int(np.ceil(span / dz + 2 * _PROFILE_MARGIN + 0.5)))
+    z = z0 + dz * np.arange(bz.size)
+    for solenoid in config.solenoids:
+        bz += solenoid_on_axis(z, solenoid.centre, solenoid.length, solenoid.radius,
+                               solenoid.peak)  # fmt: skip
+    return AxisymmetricMagneticField(z0, dz, bz, order=config.field_order)
+
+
+def _explicit_particles(beam, number: int) -> BeamParticles:
+    """A `ParticleBeam`'s given positions, velocities and currents."""
+    position, velocity, current = beam.arrays()
+    n = len(beam)
+    return BeamParticles(
+        position=np.ascontiguousarray(np.asarray(position).T),
+        velocity=np.ascontiguousarray(np.asarray(velocity).T),
+        charge=np.full(n, beam.charge * constants.e),
+        mass=np.full(n, beam.mass * constants.atomic_mass),
+        current=np.array(current, dtype=float),
+        species=np.full(n, number, dtype=np.int32),
+    )  # fmt: skip
+
+
+def config_particles(config: BeamOpticsConfig) -> tuple[BeamParticles, float]:
+    """Every beam of a configuration as one `BeamParticles` (species = the beam's place in
+    the list) and the ``sum J / v`` of the emitted beams (``model.py:387-448``)."""
+    if not config.beams:
+        raise ValueError("BeamOptics needs at least one beam")
+    cylindrical = config.grid.coordinates == "cylindrical"
+    parts, j_over_v = [], 0.0
+    for number, beam in enumerate(config.beams):
+        if not isinstance(beam, BeamSpecies):
+            parts.append(_explicit_particles(beam, number))
+            continue
+        particles, jv = beam_with_energy(
+            beam.num_particles, beam.current_density, beam.charge, beam.mass, beam.energy,
+            beam.parallel_temperature, beam.transverse_temperature, beam.start, beam.end,
+            cylindrical=cylindrical, species=number, relativistic=config.relativistic,
+        )  # fmt: skip
+        parts.append(particles)
+        j_over_v += jv
+    return BeamParticles.concatenate(parts), j_over_v
 
 
 class BeamOptics:
@@ -70,22 +167,13 @@ class BeamOptics:
         self.rank = comm.Get_rank() if comm is not None else 0
         self.size = comm.Get_size() if comm is not None else 1
         self.verbose = verbose
-        grid = config.grid
         self.species_names = [beam.name for beam in config.beams]
         self.species_mass = np.array([beam.mass * constants.atomic_mass for beam in config.beams])
         self._state: VlasovState | None = None
         self._is_finished = False
         self._beam: tuple[BeamParticles, float] | None = None
-        self.mesh = IonOpticsMesh(
-            shape=grid.num_gridpoints,
-            origin=grid.lower_bound,
-            h=grid.deltas[0],
-            geometry="cylindrical" if grid.coordinates == "cylindrical" else "planar",
-            electrodes=[_electrode(name, obj) for name, obj in config.objects.items()],
-            faces=self._faces(),
-            symmetry_plane=config.symmetry_plane,
-        )
-        self.axial_magnetic_field = self._magnetic_field()
+        self.mesh = config_mesh(config)
+        self.axial_magnetic_field = config_magnetic_field(config, self.mesh)
         self.field_map = None
         self.tracer = BeamTracer(
             self.mesh, None, self.axial_magnetic_field, step_fraction=config.step_fraction,
@@ -94,83 +182,17 @@ class BeamOptics:
             planes=config.diagnostic_planes, save_trajectories=config.save_trajectories,
         )  # fmt: skip
 
-    def _magnetic_field(self) -> AxisymmetricMagneticField | None:
-        """The axisymmetric field of the solenoids and the measured axial field
-        (``model.py:169-188``): the solenoids sampled at ``h / 2`` from ``x_min - 8 dz`` to
-        ``x_max + 8 dz``, or added to the axial field's samples."""
-        config = self.config
-        if not config.solenoids and config.axial_field is None:
-            return None
-        if config.axial_field is not None:
-            z0, dz = config.axial_field.z0, config.axial_field.dz
-            bz = np.asarray(config.axial_field.bz, dtype=float)
-            z = z0 + dz * np.arange(bz.size)
-        else:
-            dz = 0.5 * self.mesh.h
-            lo, hi = self.mesh.origin[0], self.mesh.upper[0]
-            z = np.arange(lo - 8 * dz, hi + 8.5 * dz, dz)
-            z0 = float(z[0])
-            bz = np.zeros(z.size)
-        for solenoid in config.solenoids:
-            bz = bz + solenoid_on_axis(z, solenoid.centre, solenoid.length, solenoid.radius,
-                                       solenoid.peak)  # fmt: skip
-        return AxisymmetricMagneticField(z0, dz, bz, order=config.field_order)
-
-    def _faces(self) -> dict[str, FaceCondition]:
-        faces = {}
-        cylindrical = self.config.grid.coordinates == "cylindrical"
-        walls = self.config.bcs_field
-        for face, (direction, side) in _FACES.items():
-            if cylindrical and face == "y_min":
-                continue
-            bc = walls.get_bc(dir=direction, side=side)
-            if self.config.symmetry_plane and face == "y_min":
-                if bc.bc_type != "neumann" or (not callable(bc.value) and float(bc.value) != 0.0):
-                    raise ValueError(
-                        "with symmetry_plane the y lower face needs a zero normal derivative"
-                    )
-                continue
-            faces[face] = FaceCondition(bc.bc_type, bc.value)
-        return faces
-
     def _particles(self) -> tuple[BeamParticles, float]:
-        """The beams and their ``sum J / v`` (``model.py:387-448``); made once, since every
-        iteration starts from the same beam."""
-        if self._beam is not None:
-            return self._beam
-        parts = []
-        j_over_v = 0.0
-        cylindrical = self.mesh.cylindrical
-        for number, beam in enumerate(self.config.beams):
-            if isinstance(beam, BeamSpecies):
-                particles, jv = beam_with_energy(
-                    beam.num_particles, beam.current_density, beam.charge, beam.mass,
-                    beam.energy, beam.parallel_temperature, beam.transverse_temperature,
-                    beam.start, beam.end, cylindrical=cylindrical, species=number,
-                    relativistic=self.config.relativistic,
-                )  # fmt: skip
-                j_over_v += jv
-            else:
-                n = len(beam)
-                position, velocity, current = beam.arrays()
-                particles = BeamParticles(
-                    position=np.ascontiguousarray(position.T),
-                    velocity=np.ascontiguousarray(velocity.T),
-                    charge=np.full(n, beam.charge * constants.e),
-                    mass=np.full(n, beam.mass * constants.atomic_mass),
-                    current=np.array(current, dtype=float),
-                    species=np.full(n, number, dtype=np.int32),
-                )
-            parts.append(particles)
-        if not parts:
-            raise ValueError("BeamOptics needs at least one beam")
-        particles = BeamParticles.concatenate(parts)
-        if self.size > 1:
-            # every rank traces its share; the node charges are summed over the ranks
-            from beamtracer_b200.distributed import share
+        """The beams and their ``sum J / v``, made once (every iteration starts from the
+        same beam); in a distributed run this rank's share of the trajectories."""
+        if self._beam is None:
+            particles, j_over_v = config_particles(self.config)
+            if self.size > 1:
+                # every rank traces its share; the node charges are summed over the ranks
+                from beamtracer_b200.distributed import share
 
-            particles = particles.subset(share(len(particles), self.rank, self.size))
-        self._beam = (particles, j_over_v)
+                particles = particles.subset(share(len(particles), self.rank, self.size))
+            self._beam = (particles, j_over_v)
         return self._beam
 
     def run(self, callback: Callable[[int, VlasovState], None] | None = None, *,
@@ -245,21 +267,24 @@ class BeamOptics:
 
     @property
     def stats(self) -> dict[str, int]:
-        status = self.state.trace.status
-        stats = {name: int(np.sum(status == k)) for k, name in enumerate(STATUS_NAMES)}
-        stats["launched"] = int(status.size)
-        stats["iterations"] = len(self.state.history)
-        stats["converged"] = int(
-            self.state.history[-1]["max_potential_change"] < self.config.tolerance
-        )
+        """Trajectories per final status, the launched count, the iterations and whether
+        the last iteration met the tolerance."""
+        status = np.asarray(self.state.trace.status)
+        counts = np.bincount(status[status >= 0].astype(np.int64), minlength=len(STATUS_NAMES))
+        stats = dict(zip(STATUS_NAMES, (int(c) for c in counts[: len(STATUS_NAMES)])))
+        history = self.state.history
+        last_change = history[-1]["max_potential_change"]
+        stats.update(launched=int(status.size), iterations=len(history),
+                     converged=int(last_change < self.config.tolerance))  # fmt: skip
         return stats
 
     def plane(self, x: float) -> PlaneHits:
         """The crossings of the diagnostic plane at ``x``."""
-        for hits in self.state.trace.planes:
-            if np.isclose(hits.position_x, x):
-                return hits
-        raise KeyError(f"no diagnostic plane at x = {x}")
+        planes = self.state.trace.planes
+        match = [hits for hits in planes if np.isclose(hits.position_x, x)]
+        if not match:
+            raise KeyError(f"no diagnostic plane at x = {x}")
+        return match[0]
 
     def beam_moments(self, x: float, species: str | None = None, axis: str = "y") -> BeamMoments:
         """The current, emittance and Twiss parameters at the plane ``x``."""

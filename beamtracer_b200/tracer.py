@@ -41,12 +41,17 @@ INTEGRATORS = ("rk4", "boris")
 
 def lorentz_factor(u: np.ndarray, c: float) -> np.ndarray:
     """``sqrt(1 + |u|^2 / c^2)`` of proper velocities ``u`` (3, N)."""
-    return np.sqrt(1.0 + np.sum(u * u, axis=0) / (c * c))
+    return np.sqrt(1.0 + np.einsum("ij,ij->j", u, u) / (c * c))
 
 
 def proper_velocity(v: np.ndarray, c: float) -> np.ndarray:
     """``v / sqrt(1 - |v|^2 / c^2)`` of velocities ``v`` (3, N)."""
-    return v / np.sqrt(1.0 - np.sum(v * v, axis=0) / (c * c))
+    return v / np.sqrt(1.0 - np.einsum("ij,ij->j", v, v) / (c * c))
+
+
+#: The per-particle arrays of `BeamParticles` and the axis along which particles run.
+_PARTICLE_AXES = {"position": 1, "velocity": 1, "charge": 0, "mass": 0, "current": 0,
+                  "species": 0}  # fmt: skip
 
 
 @dataclass
@@ -63,35 +68,62 @@ class BeamParticles:
 
     @staticmethod
     def concatenate(parts: Sequence[BeamParticles]) -> BeamParticles:
-        return BeamParticles(
-            np.concatenate([p.position for p in parts], axis=1),
-            np.concatenate([p.velocity for p in parts], axis=1),
-            *(np.concatenate([getattr(p, name) for p in parts])
-              for name in ("charge", "mass", "current", "species")),
-        )  # fmt: skip
+        """The particles of every part, in order."""
+        return BeamParticles(**{
+            name: np.concatenate([getattr(p, name) for p in parts], axis=axis)
+            for name, axis in _PARTICLE_AXES.items()
+        })  # fmt: skip
 
     def subset(self, index) -> BeamParticles:
-        return BeamParticles(
-            self.position[:, index], self.velocity[:, index], self.charge[index],
-            self.mass[index], self.current[index], self.species[index],
-        )  # fmt: skip
+        """The particles selected by ``index`` (a mask, indices or a slice)."""
+        return BeamParticles(**{
+            name: getattr(self, name)[(slice(None),) * axis + (index,)]
+            for name, axis in _PARTICLE_AXES.items()
+        })  # fmt: skip
 
     def __len__(self) -> int:
-        return int(self.position.shape[1])
+        return int(np.shape(self.position)[1])
 
 
 def _gaussian_samples(num: int, sampling) -> np.ndarray:
-    """(num, 3) standard normal samples: an unscrambled Sobol sequence without its origin
-    through the inverse normal, or a NumPy generator's draws."""
+    """(num, 3) standard normal samples.  ``"sobol"``: the points 1..num of the unscrambled
+    3D Sobol sequence (its origin left out: its inverse normal is infinite) through the
+    inverse normal distribution, so every call draws the same beam; a NumPy generator:
+    its ``standard_normal`` draws."""
     if isinstance(sampling, np.random.Generator):
         return sampling.standard_normal((num, 3))
     if sampling != "sobol":
         raise ValueError(f"sampling must be 'sobol' or a numpy Generator, got {sampling!r}")
     from scipy.stats import norm, qmc
 
-    sobol = qmc.Sobol(d=3, scramble=False)
-    sobol.fast_forward(1)
-    return norm.ppf(sobol.random(num))
+    engine = qmc.Sobol(d=3, scramble=False)
+    engine.fast_forward(1)
+    return norm.ppf(engine.random(num))
+
+
+@dataclass(frozen=True)
+class _EmissionLine:
+    """The line a beam leaves: its start, unit direction ``t``, its right-hand normal ``n``
+    (the direction of motion) and its length."""
+
+    start: np.ndarray
+    t: np.ndarray
+    n: np.ndarray
+    length: float
+
+    @staticmethod
+    def between(start, end) -> _EmissionLine:
+        a, b = np.asarray(start, dtype=float), np.asarray(end, dtype=float)
+        length = float(np.hypot(*(b - a)))
+        if length == 0.0:
+            raise ValueError("the beam start line has zero length")
+        t = (b - a) / length
+        return _EmissionLine(a, t, np.array([t[1], -t[0]]), length)
+
+    def midpoints(self, count: int) -> np.ndarray:
+        """(2, count) points at the centres of ``count`` equal pieces of the line."""
+        s = (np.arange(count) + 0.5) / count
+        return self.start[:, None] + (self.length * self.t)[:, None] * s[None, :]
 
 
 def beam_with_energy(
@@ -112,71 +144,81 @@ def beam_with_energy(
 ) -> tuple[BeamParticles, float]:
     """A beam emitted from the line ``start``-``end`` with ``energy`` [eV]; and ``J / v``.
 
-    ``tracer.py:221-291``: trajectories evenly spaced at ``(k + 1/2) / N`` of the line,
-    moving perpendicular to it (to its right) with Gaussian spreads of the temperatures
-    [eV]; a ring current ``2 pi J s r / N`` (cylindrical) or ``J s / N`` per unit depth.
-    ``charge`` [e], ``mass`` [u], ``current_density`` [A/m^2].
+    The interface and the draw of ``tracer.py:221-291``: one trajectory at the centre of
+    each of ``num_particles`` equal pieces of the line, moving along its right-hand normal
+    at the beam speed ``v0`` plus Gaussian spreads ``sqrt(T e / m)`` of the temperatures
+    [eV] -- the transverse one along the line (and, cylindrical, around the axis), the
+    parallel one along the normal; a ring current ``2 pi J s r / N`` (cylindrical) or
+    ``J s / N`` per unit depth.  Relativistic: ``v0`` and the spreads are proper speeds
+    (``v0 = c sqrt(g^2 - 1)``, ``g = 1 + E e / (m c^2)``) turned into velocities at the
+    end.  ``charge`` [e], ``mass`` [u], ``current_density`` [A/m^2].
     """
     q = charge * constants.e
     m = mass * constants.atomic_mass
+    line = _EmissionLine.between(start, end)
+    c = constants.c
     if relativistic:
-        c = constants.c
-        gamma = 1.0 + energy * constants.e / (m * c * c)
-        v = float(c * np.sqrt(gamma * gamma - 1.0))
+        g = 1.0 + energy * constants.e / (m * c * c)
+        v0 = float(c * np.sqrt(g * g - 1.0))
     else:
-        v = float(np.sqrt(2.0 * energy * constants.e / m))
-    dvp = float(np.sqrt(parallel_temperature * constants.e / m))
-    dvt = float(np.sqrt(transverse_temperature * constants.e / m))
-    (x1, y1), (x2, y2) = start, end
-    s = float(np.hypot(x2 - x1, y2 - y1))
-    if s == 0.0:
-        raise ValueError("the beam start line has zero length")
-    tangent = np.array([x2 - x1, y2 - y1]) / s
-    normal = np.array([tangent[1], -tangent[0]])
-    frac = (np.arange(num_particles) + 0.5) / num_particles
-    px = x1 + (x2 - x1) * frac
-    py = y1 + (y2 - y1) * frac
-    g = _gaussian_samples(num_particles, sampling)
-    vx = normal[0] * v + tangent[0] * dvt * g[:, 0] + normal[0] * dvp * g[:, 1]
-    vy = normal[1] * v + tangent[1] * dvt * g[:, 0] + normal[1] * dvp * g[:, 1]
-    vz = dvt * g[:, 2] if cylindrical else np.zeros(num_particles)
+        v0 = float(np.sqrt(2.0 * energy * constants.e / m))
+    spread_t, spread_p = (float(np.sqrt(t * constants.e / m))
+                          for t in (transverse_temperature, parallel_temperature))  # fmt: skip
+    g3 = _gaussian_samples(num_particles, sampling)
+    along_normal = v0 + spread_p * g3[:, 1]
+    along_line = spread_t * g3[:, 0]
+    velocity = np.zeros((3, num_particles))
+    velocity[:2] = line.n[:, None] * along_normal[None, :] + line.t[:, None] * along_line[None, :]
     if cylindrical:
-        current = 2.0 * np.pi * current_density * s * py / num_particles
+        velocity[2] = spread_t * g3[:, 2]
+    position = np.zeros((3, num_particles))
+    position[:2] = line.midpoints(num_particles)
+    if cylindrical:
+        current = (2.0 * np.pi * current_density * line.length / num_particles) * position[1]
     else:
-        current = np.full(num_particles, current_density * s / num_particles)
-    velocity = np.stack([vx, vy, vz], axis=0)
+        current = np.full(num_particles, current_density * line.length / num_particles)
     if relativistic:
-        velocity = velocity / lorentz_factor(velocity, constants.c)
-        v = v / float(np.sqrt(1.0 + (v / constants.c) ** 2))
+        velocity = velocity / lorentz_factor(velocity, c)
+        v0 = v0 / float(np.sqrt(1.0 + (v0 / c) ** 2))
     particles = BeamParticles(
-        position=np.stack([px, py, np.zeros(num_particles)], axis=0),
-        velocity=velocity,
-        charge=np.full(num_particles, q),
-        mass=np.full(num_particles, m),
-        current=current,
+        position=position, velocity=velocity, charge=np.full(num_particles, q),
+        mass=np.full(num_particles, m), current=current,
         species=np.full(num_particles, species, dtype=np.int32),
-    )
-    return particles, current_density / v
+    )  # fmt: skip
+    return particles, current_density / v0
+
+
+#: The per-crossing arrays of `PlaneHits`, their empty values and the axis crossings run along.
+_HIT_FIELDS = {
+    "point": (lambda: np.zeros((3, 0)), 1), "velocity": (lambda: np.zeros((3, 0)), 1),
+    "current": (lambda: np.zeros(0), 0), "species": (lambda: np.zeros(0, dtype=np.int32), 0),
+    "direction": (lambda: np.zeros(0, dtype=np.int8), 0),
+}  # fmt: skip
 
 
 @dataclass
 class PlaneHits:
-    """Crossings of the plane ``x = position_x`` (``tracer.py:295-325``)."""
+    """Crossings of the plane ``x = position_x`` (``tracer.py:295-325``): point and
+    velocity (3, m), current, species and direction (+1 / -1) of each."""
 
     position_x: float
-    point: np.ndarray = field(default_factory=lambda: np.zeros((3, 0)))
-    velocity: np.ndarray = field(default_factory=lambda: np.zeros((3, 0)))
-    current: np.ndarray = field(default_factory=lambda: np.zeros(0))
-    species: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int32))
-    direction: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int8))
+    point: np.ndarray = field(default_factory=_HIT_FIELDS["point"][0])
+    velocity: np.ndarray = field(default_factory=_HIT_FIELDS["velocity"][0])
+    current: np.ndarray = field(default_factory=_HIT_FIELDS["current"][0])
+    species: np.ndarray = field(default_factory=_HIT_FIELDS["species"][0])
+    direction: np.ndarray = field(default_factory=_HIT_FIELDS["direction"][0])
     fractions: np.ndarray | None = None
 
     def append(self, point, velocity, current, species, direction, fractions=None) -> None:
-        self.point = np.concatenate([self.point, point], axis=1)
-        self.velocity = np.concatenate([self.velocity, velocity], axis=1)
-        self.current = np.concatenate([self.current, current])
-        self.species = np.concatenate([self.species, species.astype(np.int32)])
-        self.direction = np.concatenate([self.direction, direction.astype(np.int8)])
+        """Add crossings after the ones held."""
+        new = {"point": point, "velocity": velocity, "current": current,
+               "species": np.asarray(species).astype(np.int32),
+               "direction": np.asarray(direction).astype(np.int8)}  # fmt: skip
+        for name, (_, axis) in _HIT_FIELDS.items():
+            setattr(self, name, np.concatenate([getattr(self, name), new[name]], axis=axis))
+        if fractions is not None:
+            self.fractions = (fractions if self.fractions is None
+                              else np.concatenate([self.fractions, fractions], axis=1))  # fmt: skip
 
 
 @dataclass

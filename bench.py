@@ -15,11 +15,14 @@ converged solve from a zero charge density.
 - ``roofline``: the dominant kernel's launches timed live (CUDA events) against its
   algorithmic work;
 - ``cpu_baseline``: the oracle (the reference's kernel restated in C, OpenMP over every
-  host core, and SciPy's sparse LU for the field) on one iteration of the same workload,
-  scaled by the iterations of a converged solve.
+  host core, and SciPy's sparse LU for the field) on one converged solve of the same lens,
+  its problem built on the host alone;
+- ``parity``: the device solve's potential and plane moments against that oracle solve's
+  (relative differences; north-star bound 1e-6).
 
 ``--impl reference`` times that CPU path alone (the reference's Pyccel build cannot be
-made here).  Under torchrun every rank solves its own lens (weak scaling, no collective).
+made here) and prints its moments.  Under torchrun every rank solves its own lens (weak
+scaling, no collective).
 """
 
 from __future__ import annotations
@@ -172,54 +175,69 @@ def run_profile(args) -> None:
                       "total_steps": sum(h["total_steps"] for h in state.history)}))  # fmt: skip
 
 
-def cpu_baseline(config, iterations: int) -> dict:
-    """The oracle on one Vlasov iteration of the workload, on every host core."""
-    from beamtracer_b200.model import BeamOptics
-    from oracle import kernels as oracle_kernels
-    from oracle import vlasov as oracle_vlasov
-    from tests.vlasov_cases import oracle_problem
+#: The workload's identity, the same in both arms' lines.
+def workload_config() -> dict:
+    return {"workload": WORKLOAD, "trajectories": 20000, "mesh": [801, 201],
+            "seed": 2, "l2": "256 MiB written between timed steps"}  # fmt: skip
 
-    model = BeamOptics(config)
-    problem = oracle_problem(model)
-    particles, j_over_v = model._particles()
+
+MOMENT_NAMES = ("current", "rms_size", "rms_angle", "emittance")
+
+
+def oracle_solve(config) -> tuple[float, dict, dict]:
+    """The oracle's converged solve of a configuration, built on the host alone (no device
+    classification, no library load): its seconds, its output and its moments per plane."""
+    from beamtracer_b200.diagnostics import plane_moments
+    from beamtracer_b200.tracer import PlaneHits
+    from oracle import vlasov as oracle_vlasov
+    from tests.vlasov_cases import config_problem
+
+    problem, particles, j_over_v = config_problem(config)
     start = time.perf_counter()
-    oracle_vlasov.vlasov(problem, particles, j_over_v, iterations=1, tolerance=0.0,
-                         relaxation=config.relaxation)  # fmt: skip
+    out = oracle_vlasov.vlasov(problem, particles, j_over_v, iterations=config.iterations,
+                               tolerance=config.tolerance, relaxation=config.relaxation)
     seconds = time.perf_counter() - start
-    cores = oracle_kernels.host_cores()
-    per_solve = seconds * max(iterations, 1)
-    return {"value": 1.0 / per_solve, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"1 Vlasov iteration (field LU solve + 20k-ring trace + deposit) in "
-                      f"{seconds:.2f} s, times {iterations} iterations per converged solve"}  # fmt: skip
+    from scipy import constants
+
+    mass = np.array([beam.mass for beam in config.beams]) * constants.atomic_mass
+    moments = {}
+    for plane, hits in zip(problem.planes, oracle_vlasov.plane_hits(
+            problem, out["trace"], particles.current, particles.species)):  # fmt: skip
+        m = plane_moments(PlaneHits(plane, *hits), cylindrical=problem.geometry == 1, mass=mass)
+        moments[f"{plane * 1e3:g}mm"] = {k: getattr(m, k) for k in MOMENT_NAMES}
+    return seconds, out, moments
+
+
+def parity_report(potential: np.ndarray, moments: dict, oracle_out: dict,
+                  oracle_moments: dict) -> dict:  # fmt: skip
+    """The device solve against the oracle's: the potential's largest difference relative
+    to the oracle's largest magnitude, and every moment's relative difference."""
+    ref = oracle_out["potential"]
+    phi_rel = float(np.max(np.abs(potential - ref)) / np.max(np.abs(ref)))
+    per = {plane: {k: abs(moments[plane][k] - v) / abs(v) for k, v in values.items()}
+           for plane, values in oracle_moments.items()}  # fmt: skip
+    worst = max(max(d.values()) for d in per.values())
+    return {"against": "the oracle's converged solve of the same lens (FP64, same seed)",
+            "potential_max_rel": phi_rel, "moments_max_rel": worst, "moments_rel": per,
+            "oracle_iterations": len(oracle_out["history"]), "bound": 1e-6,
+            "within_bound": bool(phi_rel <= 1e-6 and worst <= 1e-6)}  # fmt: skip
 
 
 def run_reference(args, rank: int) -> None:
     """The reference arm: the oracle's converged solve of the same lens on every host core
     (the field by SciPy's LU, the trace and deposit by the C port), each step one solve run
-    until the potential changes by less than the tolerance, as the device solve is."""
+    until the potential changes by less than the tolerance, as the device solve is.  The
+    problem is built on the host alone."""
     if rank != 0:
         return
-    from beamtracer_b200.model import BeamOptics
     from oracle import kernels as oracle_kernels
-    from oracle import vlasov as oracle_vlasov
-    from tests.vlasov_cases import oracle_problem
 
     config = build_workload(2)
-    model = BeamOptics(config)
-    problem = oracle_problem(model)
-    particles, j_over_v = model._particles()
-
-    def solve() -> tuple[float, int]:
-        start = time.perf_counter()
-        out = oracle_vlasov.vlasov(problem, particles, j_over_v, iterations=config.iterations,
-                                   tolerance=config.tolerance, relaxation=config.relaxation)
-        return time.perf_counter() - start, len(out["history"])
-
     if args.warmup > 0:
-        solve()  # the oracle's build and caches
-    runs = [solve() for _ in range(max(args.steps, 1))]
-    seconds = float(np.mean([t for t, _ in runs]))
-    iterations = runs[-1][1]
+        oracle_solve(config)  # the oracle's build and caches
+    runs = [oracle_solve(config) for _ in range(max(args.steps, 1))]
+    seconds = float(np.mean([r[0] for r in runs]))
+    iterations = len(runs[-1][1]["history"])
     base = {"value": 1.0 / seconds, "unit": UNIT, "cores": oracle_kernels.host_cores(),
             "kind": "port",
             "sample": f"converged solves of the oracle ({iterations} iterations: SciPy LU "
@@ -229,10 +247,11 @@ def run_reference(args, rank: int) -> None:
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "l2": "inputs larger than L2 (trace records)"},
+        "config": workload_config(), "iterations_per_solve": iterations,
         "cpu_baseline": base,
         "e2e": {"value": 1.0 / seconds, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "moments": runs[-1][2],
     }  # fmt: skip
     print(json.dumps(line), flush=True)
 
@@ -477,6 +496,7 @@ def main() -> None:
     if distributed:
         dist.barrier()
     launches = ctx.launch_count() - launches_before
+    records = ctx.deposit_records()
     step_ms = [a.elapsed_time(b) for a, b in events]
     total_ms = float(sum(step_ms))
     if distributed:
@@ -503,13 +523,14 @@ def main() -> None:
             "steps_per_launch": steps_total / max(trace_launches, 1)}  # fmt: skip
     peaks = _peaks()
     dep_ms, dep_launches = timers["deposit"]
-    records = steps_total
     dep_bytes = records * DEPOSIT_BYTES_PER_RECORD
     deposit = {"bound": "hbm", "kernel": "deposit",
                "achieved": dep_bytes / (dep_ms / 1e3) / 1e9 if dep_ms else None,
                "peak": peaks["hbm_gbs"], "unit": "GB/s",
                "frac": (dep_bytes / (dep_ms / 1e3) / 1e9) / peaks["hbm_gbs"] if dep_ms else None,
-               "peak_source": peaks["source"], "traffic": None}  # fmt: skip
+               "peak_source": peaks["source"], "records": records,
+               "records_per_step": records / max(steps_total, 1),
+               "traffic": None}  # fmt: skip
     # the dominant kernel, the trace: its algorithmic bytes are the deposit records it
     # writes (the edge fields it reads stay in L1/L2); its limit is the latency of its
     # dependent FP64 chain at one warp per scheduler (roofline_fp64)
@@ -535,7 +556,7 @@ def main() -> None:
         start.record(stream)
         m = BeamOptics(config)
         m.run()
-        moments = m.beam_moments(79e-3)
+        moments = {f"{x * 1e3:g}mm": m.beam_moments(x) for x in config.diagnostic_planes}
         stop.record(stream)
         torch.cuda.synchronize()
         if k:
@@ -549,17 +570,27 @@ def main() -> None:
                + engine.paths.numel() * 8 + 2 * nn * 8)  # fmt: skip
     e2e_value = world * 1e3 / float(np.median(e2e_ms))
 
-    cpu = None
+    gpu_moments = {plane: {k: getattr(mo, k) for k in MOMENT_NAMES}
+                   for plane, mo in moments.items()}  # fmt: skip
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(config, len(history))
+        from oracle import kernels as oracle_kernels
+
+        seconds, oracle_out, oracle_moments = oracle_solve(config)
+        cpu = {"value": 1.0 / seconds, "unit": UNIT, "cores": oracle_kernels.host_cores(),
+               "kind": "port",
+               "sample": f"one converged solve of the same lens by the oracle "
+                         f"({len(oracle_out['history'])} iterations: SciPy LU field, C trace "
+                         f"and deposit with OpenMP), {seconds:.2f} s"}  # fmt: skip
+        parity = parity_report(m.potential, gpu_moments, oracle_out, oracle_moments)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "iterations_per_solve": len(history),
-                   "vcycles_per_solve": sum(h["krylov_steps"] for h in history),
-                   "trajectories": 20000, "mesh": [801, 201], "window": args.window,
-                   "l2": "256 MiB written between timed steps"},
+        "config": workload_config(),
+        "solve": {"iterations_per_solve": len(history),
+                  "vcycles_per_solve": sum(h["krylov_steps"] for h in history),
+                  "window": args.window},
         "roofline": hbm, "roofline_fp64": fp64, "roofline_deposit": deposit,
         "kernels": kernels,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -568,8 +599,8 @@ def main() -> None:
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
-        "moments_79mm": {"current": moments.current, "rms_size": moments.rms_size,
-                         "rms_angle": moments.rms_angle, "emittance": moments.emittance},
+        "moments": gpu_moments,
+        "parity": parity,
     }  # fmt: skip
     if rank == 0:
         print(json.dumps(line), flush=True)

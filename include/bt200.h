@@ -54,6 +54,12 @@ int bt_ctx_synchronize(bt_ctx *ctx);
 int bt_ctx_set_timing(bt_ctx *ctx, int on);
 int bt_ctx_read_timer(bt_ctx *ctx, const char *name, double *total_ms, int64_t *launches);
 int bt_ctx_reset_timers(bt_ctx *ctx);
+/* The deposit records (the runs of steps with a charge, the slots with none left out) that
+ * the context's deposits have sorted and reduced while timing was on, since the last
+ * bt_ctx_reset_timers (host out-param; waits for the context's stream).  For measurement:
+ * the algorithmic bytes of the deposit are counted per record.  No counterpart in the
+ * reference. */
+int bt_ctx_deposit_records(bt_ctx *ctx, int64_t *records);
 /* The number of kernels the context has launched since its creation (host out-param). */
 int bt_ctx_launch_count(bt_ctx *ctx, int64_t *count);
 /* Copy the calling thread's last error message into buf (NUL-terminated); returns its length. */
@@ -88,9 +94,10 @@ int bt_deposit_trajectories_2d(bt_ctx *ctx, const double *px, const double *py,
  * file-scope __device__ array of about 5.4 MB that every GPU loading the library holds
  * until the process exits, sized for at most 65536 charges per call and a mesh of at most
  * 65536 nodes; larger calls fail with BT_ERR_ARG.  `stream` is a cudaStream_t (NULL: the
- * legacy default stream) on the calling thread's current device.  The first call on a
- * device looks up the array's device address there (cudaGetSymbolAddress); make that first
- * call before any stream capture.  All calls share the array and leave their scratch in
+ * legacy default stream) on the calling thread's current device.  Every call looks up the
+ * array's device address in the current device's context (cudaGetSymbolAddress, a host
+ * call); the first call in a context may load the library's module there, so make that
+ * first call before any stream capture.  All calls share the array and leave their scratch in
  * it: calls that overlap on the GPU race, so order them (one stream, or events). */
 int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px, const double *py,
                                        const double *q, int64_t n, double origin_x,

@@ -2,9 +2,14 @@
 
 Run in the build container, where the reference source tree is readable::
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout>
 
-It loads the reference's kernel sources as plain Python modules -- the Pyccel versions of
+(or with ``BEAMTRACER_REFERENCE`` set to the checkout).
+
+It runs the reference's host functions that both arms share -- ``beam_with_energy``,
+``plane_moments`` and ``AxisymmetricMagneticField`` with ``solenoid_on_axis``, taken out of
+their modules' sources -- on the cases of ``tests/golden/host_cases.py``.  It loads the
+reference's kernel sources as plain Python modules -- the Pyccel versions of
 ``staggered_field_2d``, ``deposit_trajectories_2d`` and ``trace_trajectories_2d`` and the
 NumPy versions of the first two (``src/beamtracer/kernels/*/``) -- runs them on the seeded
 cases of ``tests/golden/cases.py`` and writes inputs and outputs as ``.npz`` files.  The
@@ -19,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import importlib.util
+import os
 import math
 import sys
 import types
@@ -90,6 +96,114 @@ def reference_edge_field(root: Path):
     return namespace["_edge_field"]
 
 
+def reference_definitions(root: Path, module: str, names: tuple[str, ...],
+                          namespace: dict) -> dict:  # fmt: skip
+    """Top-level definitions of a reference module, taken out of its source and run in
+    ``namespace`` (their decorators that only record documentation left off, ``dataclass``
+    kept): the module's absent imports are never executed."""
+    import ast
+
+    source = (root / "src" / "beamtracer" / "solver" / f"{module}.py").read_text()
+    tree = ast.parse(source)
+    picked = []
+    for node in tree.body:
+        if isinstance(node, (ast.FunctionDef, ast.ClassDef)) and node.name in names:
+            node.decorator_list = [
+                d for d in node.decorator_list
+                if isinstance(d, ast.Name) and d.id == "dataclass"
+                or isinstance(d, ast.Call) and getattr(d.func, "id", "") == "dataclass"
+            ]  # fmt: skip
+            picked.append(node)
+    missing = set(names) - {n.name for n in picked}
+    if missing:
+        raise RuntimeError(f"{module}.py has no {sorted(missing)}")
+    exec(compile(ast.Module(body=picked, type_ignores=[]), f"{module}.py", "exec"), namespace)
+    return namespace
+
+
+def reference_host_functions(root: Path) -> dict:
+    """The reference's beam seeding (``tracer.py:87-291``), plane crossings and moments
+    (``tracer.py:295-325``, ``diagnostics.py:15-135``) and axisymmetric field
+    (``fields.py:192-321``), in one namespace.  ``mpiparticles.lorentz_factor`` (absent) is
+    stood in for by ``sqrt(1 + |u|^2 / c^2)`` of (3, N) proper velocities."""
+    from collections.abc import Sequence
+    from dataclasses import dataclass, field
+    from typing import Any
+
+    from scipy import constants
+
+    def lorentz_factor(u, c):
+        return np.sqrt(1.0 + np.sum(u * u, axis=0) / (c * c))
+
+    module = types.ModuleType("_ref_host")  # dataclasses look their module up by name
+    sys.modules[module.__name__] = module
+    namespace = module.__dict__
+    namespace.update({"np": np, "constants": constants, "dataclass": dataclass, "field": field,
+                      "Sequence": Sequence, "Any": Any, "lorentz_factor": lorentz_factor})  # fmt: skip
+    reference_definitions(root, "tracer", ("BeamParticles", "_gaussian_samples", "_beam_speeds",
+                                           "beam_with_energy", "PlaneHits"), namespace)
+    reference_definitions(root, "diagnostics", ("BeamMoments", "plane_moments"), namespace)
+    reference_definitions(root, "fields", ("AxisymmetricMagneticField", "solenoid_on_axis"),
+                          namespace)  # fmt: skip
+    return namespace
+
+
+def host_goldens(root: Path) -> None:
+    """``host_*.npz``: the reference's beams, moments and magnetic fields on the cases of
+    ``tests/golden/host_cases.py``."""
+    from tests.golden import host_cases as hc
+
+    ref = reference_host_functions(root)
+    beams = {}
+    for name, (args, kwargs) in hc.BEAM_CASES.items():
+        kwargs = dict(kwargs)
+        if "seed" in kwargs:
+            kwargs["sampling"] = np.random.default_rng(kwargs.pop("seed"))
+        particles, j_over_v = ref["beam_with_energy"](*args, **kwargs)
+        for key in ("position", "velocity", "charge", "mass", "current", "species"):
+            beams[f"{name}.{key}"] = getattr(particles, key)
+        beams[f"{name}.j_over_v"] = np.array(j_over_v)
+    np.savez_compressed(HERE / "host_beams.npz", **beams)
+
+    moments = {}
+    for name, (seed, cylindrical, species, forward, axis, mass_kind) in hc.MOMENT_CASES.items():
+        h = hc.moment_hits(seed, cylindrical)
+        if name == "planar_fast":
+            h["velocity"] = h["velocity"] * 150.0  # about 0.7 c
+        hits = ref["PlaneHits"](0.0)
+        hits.append(h["point"], h["velocity"], h["current"], h["species"], h["direction"])
+        mass = hc.MOMENT_MASSES if mass_kind == "array" else float(hc.MOMENT_MASSES[0])
+        m = ref["plane_moments"](hits, cylindrical=cylindrical, mass=mass, species=species,
+                                 forward_only=forward, axis=axis)  # fmt: skip
+        moments[name] = np.array([getattr(m, k) for k in m.__dataclass_fields__], dtype=float)
+    np.savez_compressed(HERE / "host_moments.npz", **moments)
+
+    fields = {}
+    field_class, solenoid = ref["AxisymmetricMagneticField"], ref["solenoid_on_axis"]
+    for k, (name, (centre, length, radius, peak, z0, hz, n, order)) in enumerate(
+            hc.FIELD_CASES.items()):  # fmt: skip
+        z = z0 + hz * np.arange(n)
+        profile = solenoid(z, centre, length, radius, peak)
+        f = field_class(z0, hz, profile, order=order)
+        pz, pr = hc.field_points(30 + k, z0, hz, n)
+        bz, br = f(pz, pr)
+        fields.update({f"{name}.profile": profile, f"{name}.table": f._samples,
+                       f"{name}.bz": bz, f"{name}.br": br})  # fmt: skip
+    lo, hi, h, solenoids, order = hc.SAMPLING_CASE
+    dz = 0.5 * h
+    z = np.arange(lo - 8 * dz, hi + 8.5 * dz, dz)  # the sampling of model.py:180-182
+    bz = np.zeros(z.size)
+    for centre, length, radius, peak in solenoids:
+        bz = bz + solenoid(z, centre, length, radius, peak)
+    f = field_class(float(z[0]), dz, bz, order=order)
+    pz, pr = hc.field_points(40, lo, h, int((hi - lo) / h))
+    fields["sampling.bz"], fields["sampling.br"] = f(pz, pr)
+    fields["sampling.z0"], fields["sampling.count"] = np.array(z[0]), np.array(z.size)
+    np.savez_compressed(HERE / "host_fields.npz", **fields)
+    print("host goldens:", len(beams), "beam arrays,", len(moments), "moment cases,",
+          len(fields), "field arrays")
+
+
 def _save(name: str, args: list, result: list, extra: dict | None = None) -> None:
     arrays = {}
     for i, (a, r) in enumerate(zip(args, result, strict=True)):
@@ -102,8 +216,17 @@ def _save(name: str, args: list, result: list, extra: dict | None = None) -> Non
 
 def main() -> None:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
-    root = Path(parser.parse_args().reference)
+    parser.add_argument(
+        "--reference", default=os.environ.get("BEAMTRACER_REFERENCE"),
+        help="the reference checkout (default: $BEAMTRACER_REFERENCE)",
+    )  # fmt: skip
+    given = parser.parse_args().reference
+    if not given:
+        parser.error("give --reference or set BEAMTRACER_REFERENCE to the reference checkout")
+    root = Path(given)
+    if not (root / "src" / "beamtracer").is_dir():
+        parser.error(f"{root} holds no src/beamtracer package")
+    host_goldens(root)
     ref = reference_kernels(root)
 
     for seed in (4, 5, 6):

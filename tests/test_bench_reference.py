@@ -32,3 +32,20 @@ def test_reference_arm_prints_one_converged_solve():
     base = line["cpu_baseline"]
     assert base["kind"] == "port" and base["cores"] >= 1
     assert "7 iterations" in base["sample"]  # the lens converges as on the device
+    assert line["config"]["mesh"] == [801, 201] and line["config"]["trajectories"] == 20000
+    moments = line["moments"]
+    assert sorted(moments) == ["70mm", "79mm"]
+    assert moments["79mm"]["current"] > 0.0 and moments["79mm"]["rms_angle"] > 0.0
+
+
+def test_reference_arm_loads_no_device_library():
+    """The reference arm builds its problem on the host alone: it never loads libbt200."""
+    code = (
+        "import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', "
+        "'--warmup', '0']; runpy.run_path('bench.py', run_name='__main__'); "
+        "maps = open('/proc/self/maps').read(); "
+        "assert 'libbt200' not in maps, 'libbt200 loaded'; print('no-libbt200')"
+    )
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True,
+                         text=True, timeout=600, check=True)  # fmt: skip
+    assert "no-libbt200" in out.stdout

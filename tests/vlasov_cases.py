@@ -65,14 +65,30 @@ def extraction(sign: float = 1.0, **settings) -> BeamOpticsConfig:
     )  # fmt: skip
 
 
+def host_twin(mesh):
+    """The same mesh classified again on the host alone (no library load): the oracle's
+    view of a mesh the product may have classified on the device."""
+    from beamtracer_b200.mesh import IonOpticsMesh
+
+    return IonOpticsMesh(
+        shape=mesh.shape, origin=mesh.origin, h=mesh.h, geometry=mesh.geometry,
+        electrodes=mesh.electrodes, faces=dict(mesh.faces), patch=mesh.patch,
+        symmetry_plane=mesh.symmetry_plane, x_nodes=mesh.x_nodes, logical_x0=mesh.logical_x0,
+        classify_on_device=False,
+    )  # fmt: skip
+
+
 def mesh_problem(mesh, *, planes=(), integrator: int = 0, step_fraction: float = 0.5,
                  max_steps: int = 100_000, magnetic=None) -> oracle_vlasov.Problem:
-    """The oracle's description of a mesh, its electrodes and a trace; ``magnetic`` an
-    `AxisymmetricMagneticField` (cylindrical mesh) or `PlanarSolenoidField` (planar)."""
+    """The oracle's description of a mesh (classified again on the host), its electrodes
+    and a trace; ``magnetic`` an `AxisymmetricMagneticField` (cylindrical mesh) or
+    `PlanarSolenoidField` (planar)."""
     from beamtracer_b200.fields import PlanarSolenoidField
     from beamtracer_b200.mesh import FACES
     from beamtracer_b200.tracer import electrode_lookup, geometry_code
 
+    if getattr(mesh, "classify_on_device", None) is not False:
+        mesh = host_twin(mesh)
     cells, subcells = electrode_lookup(mesh)
     neumann = tuple(0.0 if mesh.faces[f].kind != "neumann" else float(mesh.faces[f].value)
                     for f in FACES)  # fmt: skip
@@ -91,6 +107,21 @@ def mesh_problem(mesh, *, planes=(), integrator: int = 0, step_fraction: float =
         inside_solid=mesh.inside_solid, planes=tuple(planes), integrator=integrator,
         step_fraction=step_fraction, max_steps=max_steps, magnetic=mag,
     )  # fmt: skip
+
+
+def config_problem(config) -> tuple[oracle_vlasov.Problem, object, float]:
+    """The oracle's problem, beam and ``sum J / v`` of a `BeamOpticsConfig`, built on the
+    host alone: no device classification, no library load."""
+    from beamtracer_b200.model import config_magnetic_field, config_mesh, config_particles
+    from beamtracer_b200.tracer import INTEGRATORS
+
+    mesh = config_mesh(config, classify_on_device=False)
+    problem = mesh_problem(mesh, planes=config.diagnostic_planes,
+                           integrator=INTEGRATORS.index(config.integrator),
+                           step_fraction=config.step_fraction, max_steps=config.max_steps,
+                           magnetic=config_magnetic_field(config, mesh))  # fmt: skip
+    particles, j_over_v = config_particles(config)
+    return problem, particles, j_over_v
 
 
 def oracle_problem(model) -> oracle_vlasov.Problem:
