@@ -115,6 +115,7 @@ SIGNATURES: dict[str, list] = {
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],
     "bt_vlasov_mix": [P, P, P, P, I64, I64, F64, I32, P, P],
     "bt_max_abs_diff": [P, P, P, I64, P],
+    "bt_anderson_mix": [P, P, P, P, I64, I64, I32, I32, I32, F64, P, P, P, P, P],
     "bt_poisson_create": [P, ctypes.POINTER(MeshDesc), ctypes.POINTER(P)],
     "bt_poisson_destroy": [P],
     "bt_poisson_set_region": [P, P, F64],

@@ -80,61 +80,84 @@ def compensation_factors(x: np.ndarray, compensation: Sequence[Compensation]) ->
 
 
 class AndersonMixer:
-    """Anderson acceleration of ``rho = G(rho)`` (``vlasov.py:127-173``), on device arrays.
+    """Anderson acceleration of ``rho = G(rho)`` (the interface of ``vlasov.py:127-173``),
+    on the device (``bt_anderson_mix``).
 
-    The least-squares problem of the last ``depth`` differences is solved through a QR
-    factorisation of the (n, m) difference matrix and a cut-off of 1e-10 on the singular
-    values of its small triangular factor (those of the difference matrix itself).
+    Type II: from the last ``depth + 1`` iterates x and residuals f = G(x) - x, the
+    differences dX, dF of consecutive ones, ``gamma = argmin |f - dF gamma|`` (singular
+    values below 1e-10 of the largest cut off, as NumPy's ``lstsq(rcond=1e-10)``) and
+    ``x + w f - (dX + w dF) gamma``; with no history ``x + w f``.  The iterates stay in
+    ring buffers on the device; the least-squares problem is solved there too.
     """
 
     def __init__(self, depth: int = 5, relaxation: float = 1.0) -> None:
         if depth < 1:
             raise ValueError(f"depth must be at least 1, got {depth}")
+        if depth > 16:
+            raise ValueError(f"depth must be at most 16 on the device, got {depth}")
         self.depth = int(depth)
         self.relaxation = float(relaxation)
-        self._x: list = []
-        self._f: list = []
+        self._rings = None
+        self._count = 0
+        self._head = -1
 
     def reset(self) -> None:
-        self._x, self._f = [], []
+        """Forget the stored iterates."""
+        self._count = 0
+        self._head = -1
 
-    def update(self, rho, deposit):
+    def _buffers(self, n: int):
         import torch
 
-        x = rho.reshape(-1).clone()
-        f = deposit.reshape(-1) - x
-        self._x.append(x)
-        self._f.append(f)
-        del self._x[: -self.depth - 1], self._f[: -self.depth - 1]
-        omega = self.relaxation
-        new = x + omega * f
-        if len(self._x) > 1:
-            dx = torch.diff(torch.stack(self._x), dim=0).T
-            df = torch.diff(torch.stack(self._f), dim=0).T
-            q, r = torch.linalg.qr(df)
-            u, s, vh = np.linalg.svd(r.cpu().numpy())
-            keep = s > 1e-10 * s.max() if s.size and s.max() > 0 else np.zeros(s.shape, bool)
-            qf = (q.T @ f).cpu().numpy()
-            gamma = vh[keep].T @ ((u[:, keep].T @ qf) / s[keep])
-            g = torch.from_numpy(gamma).to(rho.device)
-            new = new - (dx + omega * df) @ g
+        if self._rings is None or self._rings[0].shape[1] != n:
+            rows = self.depth + 1
+            make = lambda k: torch.empty((k, n), dtype=torch.float64, device="cuda")  # noqa: E731
+            self._rings = (make(rows), make(rows), make(self.depth))
+            self.reset()
+        return self._rings
+
+    def mix(self, rho, charge, volumes=None, column=None, stats=None) -> None:
+        """``rho`` (device, (nx, ny)) <- the mixed density, from the deposit
+        ``charge / volumes`` times the column factors ``column`` (device arrays or None);
+        ``stats`` (device, 2) gets max |new - old| and max |new|."""
+        import torch
+
+        nx, ny = rho.shape
+        xs, fs, q = self._buffers(nx * ny)
+        self._head = (self._head + 1) % (self.depth + 1)
+        self._count = min(self._count + 1, self.depth + 1)
+        if stats is None:
+            stats = torch.empty(2, dtype=torch.float64, device=rho.device)
+        ctx = _lib.context()
+        d = _lib.dptr
+        _lib.check(_lib.lib().bt_anderson_mix(
+            ctx.handle, d(charge), d(volumes), d(column), nx, ny, self.depth, self._count,
+            self._head, self.relaxation, d(xs), d(fs), d(q), d(rho), d(stats)))  # fmt: skip
+
+    def update(self, rho, deposit):
+        """The next density from ``rho`` and its deposit ``G(rho)`` (device arrays), as
+        the reference's ``AndersonMixer.update``."""
+        new = rho.reshape(rho.shape[0], -1).clone() if rho.dim() == 2 else rho.reshape(1, -1).clone()
+        self.mix(new, deposit.reshape(new.shape).contiguous())
         return new.reshape(rho.shape)
 
 
 def thin_particles(particles: BeamParticles, stride: int) -> BeamParticles:
-    """Every ``stride``-th trajectory of each species, its current scaled to keep the
-    species' total (``vlasov.py:202-215``)."""
-    keep = np.zeros(len(particles), dtype=bool)
-    scale = np.ones(len(particles))
-    for species in np.unique(particles.species):
-        index = np.flatnonzero(particles.species == species)
-        kept = index[::stride]
-        keep[kept] = True
-        total = np.abs(particles.current[index]).sum()
-        part = np.abs(particles.current[kept]).sum()
-        scale[kept] = total / part if part > 0.0 else 1.0
+    """The coarse phase's beam (the interface of ``vlasov.py:202-215``): of each species
+    the trajectories at positions 0, stride, 2 stride, ... of its own list, their currents
+    scaled by one factor so that the species keeps its total |current|."""
+    species = np.asarray(particles.species)
+    order = np.argsort(species, kind="stable")  # each species' trajectories, in list order
+    groups = np.split(order, np.flatnonzero(np.diff(species[order])) + 1)
+    magnitude = np.abs(particles.current)
+    factor = np.zeros(len(particles))
+    for members in groups:
+        kept = members[::stride]
+        kept_total = magnitude[kept].sum()
+        factor[kept] = magnitude[members].sum() / kept_total if kept_total > 0.0 else 1.0
+    keep = factor > 0.0
     thinned = particles.subset(keep)
-    thinned.current = thinned.current * scale[keep]
+    thinned.current = thinned.current * factor[keep]
     return thinned
 
 
@@ -294,13 +317,8 @@ def vlasov_iterate(
             tracer.reduce(engine.charge)  # the node charges of every rank's share, summed
         tracer._capacity = engine.capacity
         if mixer is not None and iteration > 0:
-            deposit = engine.density()
-            if column is not None:
-                deposit = deposit * column[:, None]
-            old = rho.clone()
-            rho.copy_(mixer.update(rho, deposit))
-            scalars[1] = (rho - old).abs().max()
-            scalars[2] = rho.abs().max()
+            mixer.mix(rho, engine.charge.reshape(nx, ny), engine.volumes, column,
+                      scalars[1:3])  # fmt: skip
         else:
             _lib.check(
                 _lib.lib().bt_vlasov_mix(

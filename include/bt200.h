@@ -228,6 +228,22 @@ int bt_edge_field(bt_ctx *ctx, const double *phi, const int32_t *solid, const ui
 
 /* -- the per-iteration updates (device pointers) -------------------------------------- */
 
+/* solver/vlasov.py:127-173 (AndersonMixer.update), on the device.  Anderson mixing of type
+ * II of the iterate rho (DEVICE, nx * ny) with its new deposit G(rho) = charge / volumes
+ * times column_factor[i] on node column i (volumes or column_factor NULL: left out):
+ * the iterate and its residual are stored in row `head` of the ring buffers xs and fs
+ * (DEVICE, (depth + 1) * nx * ny each; `count` rows, 1 to depth + 1, hold the last
+ * iterates, the newest at `head`, the older ones before it cyclically) and rho is
+ * overwritten with x + w f - (dX + w dF) gamma, gamma the least-squares solution of
+ * dF gamma = f with singular values below 1e-10 of the largest left out (numpy.linalg.lstsq
+ * with rcond 1e-10), through a QR of dF by Gram-Schmidt applied twice into q (DEVICE,
+ * depth * nx * ny scratch).  depth 1 to 16.  stats (DEVICE, 2): max |new - old| and
+ * max |new| (NaN if any entry is NaN). */
+int bt_anderson_mix(bt_ctx *ctx, const double *charge, const double *volumes,
+                    const double *column_factor, int64_t nx, int64_t ny, int32_t depth,
+                    int32_t count, int32_t head, double relaxation, double *xs, double *fs,
+                    double *q, double *rho, double *stats);
+
 /* tracer.py:700-705, vlasov.py:176-184 and 389-397: the new density of an iteration.
  * deposit = charge / volumes (both (nx, ny)), times column_factor[i] (nx,) where given
  * (the space-charge compensation of node column i, NULL for none); then rho <- deposit

@@ -180,11 +180,84 @@ class Plasma:
     density: float | None = None
 
 
+def edge_faces(p: Problem) -> list[str]:
+    """The edge field's face rules: extrapolated, mirrored on the axis or symmetry plane."""
+    faces = ["extrapolate"] * 4
+    if p.geometry in (1, 2):
+        faces[2] = "symmetric"
+    return faces
+
+
+def density_of(p: Problem, potential: np.ndarray, particles) -> tuple[np.ndarray, Trace]:
+    """G(phi): the beam's charge density (node charges over node volumes) when traced
+    through the edge field of ``potential`` -- one iteration's stage after its field solve
+    (``vlasov.py:368-397`` before compensation and mixing); and the trace."""
+    fx, fy = oracle_field.edge_fields(potential, p.solid, p.near_solid, p.distance,
+                                      np.diff(p.x), p.h, edge_faces(p))  # fmt: skip
+    t = trace(p, fx, fy, particles)
+    return t.charge / volumes(p), t
+
+
+class Anderson:
+    """Anderson mixing of type II (``vlasov.py:127-173``): from the last ``depth + 1``
+    iterates x and residuals f = G(x) - x, gamma = argmin |f - dF gamma| by NumPy's
+    least squares with singular values below 1e-10 of the largest cut off, and
+    x + w f - (dX + w dF) gamma."""
+
+    def __init__(self, depth: int, relaxation: float) -> None:
+        self.depth, self.relaxation = int(depth), float(relaxation)
+        self.xs: list[np.ndarray] = []
+        self.fs: list[np.ndarray] = []
+
+    def reset(self) -> None:
+        self.xs, self.fs = [], []
+
+    def update(self, rho: np.ndarray, deposit: np.ndarray) -> np.ndarray:
+        x = np.asarray(rho, dtype=float).ravel()
+        f = np.asarray(deposit, dtype=float).ravel() - x
+        self.xs = (self.xs + [x])[-(self.depth + 1):]
+        self.fs = (self.fs + [f])[-(self.depth + 1):]
+        w = self.relaxation
+        new = x + w * f
+        if len(self.xs) > 1:
+            dx = np.diff(np.array(self.xs), axis=0).T
+            df = np.diff(np.array(self.fs), axis=0).T
+            gamma = np.linalg.lstsq(df, f, rcond=1e-10)[0]
+            new = new - (dx + w * df) @ gamma
+        return new.reshape(np.shape(rho))
+
+
+def thin(particles, stride: int):
+    """Every ``stride``-th trajectory of each species, the kept currents scaled to keep the
+    species' total (``vlasov.py:202-215``)."""
+    from types import SimpleNamespace
+
+    keep = np.zeros(particles.current.size, dtype=bool)
+    scale = np.ones(particles.current.size)
+    for s in np.unique(particles.species):
+        members = np.flatnonzero(particles.species == s)
+        kept = members[::stride]
+        keep[kept] = True
+        total, part = np.abs(particles.current[members]).sum(), np.abs(particles.current[kept]).sum()
+        scale[kept] = total / part if part > 0.0 else 1.0
+    return SimpleNamespace(position=particles.position[:, keep],
+                           velocity=particles.velocity[:, keep],
+                           charge=particles.charge[keep], mass=particles.mass[keep],
+                           current=particles.current[keep] * scale[keep],
+                           species=particles.species[keep])  # fmt: skip
+
+
 def vlasov(p: Problem, particles, j_over_v: float, *, iterations: int, tolerance: float = 0.0,
            relaxation: float = 1.0, plasma: Plasma | None = None, compensation=(),
-           density_tolerance: float | None = None, callback=None) -> dict[str, Any]:  # fmt: skip
-    """The Vlasov iteration (``vlasov.py:327-427``, linear mixing); the last iteration's
-    potential, density, trace and history."""
+           density_tolerance: float | None = None, callback=None, mixing: str = "linear",
+           anderson_depth: int = 5, coarse_particles: float = 1.0,
+           coarse_tolerance: float = 0.0) -> dict[str, Any]:  # fmt: skip
+    """The Vlasov iteration (``vlasov.py:327-427``: linear or Anderson mixing, the coarse
+    phase of every k-th trajectory until the potential changes by less than
+    ``coarse_tolerance``); the last iteration's potential, density, trace and history."""
+    mixer = Anderson(anderson_depth, relaxation) if mixing == "anderson" else None
+    stride = int(np.ceil(1.0 / coarse_particles - 1e-9))
+    coarse = stride > 1
     nx, ny = p.shape
     op = poisson.assemble(p.x, p.h, p.geometry == 1, p.fixed, p.fixed_value, p.distance,
                           p.neumann)  # fmt: skip
@@ -192,9 +265,7 @@ def vlasov(p: Problem, particles, j_over_v: float, *, iterations: int, tolerance
     factor = np.ones(nx)
     for x_min, x_max, fraction in compensation:
         factor[(p.x >= x_min) & (p.x <= x_max)] *= 1.0 - fraction
-    faces = ["extrapolate"] * 4
-    if p.geometry in (1, 2):
-        faces[2] = "symmetric"
+    faces = edge_faces(p)
     rho = np.zeros((nx, ny))
     potential = None
     history = []
@@ -221,10 +292,19 @@ def vlasov(p: Problem, particles, j_over_v: float, *, iterations: int, tolerance
         potential = new
         fx, fy = oracle_field.edge_fields(potential, p.solid, p.near_solid, p.distance,
                                           np.diff(p.x), p.h, faces)  # fmt: skip
-        t = trace(p, fx, fy, particles)
+        if coarse and change < coarse_tolerance:
+            coarse = False
+            if mixer is not None:
+                mixer.reset()
+        t = trace(p, fx, fy, thin(particles, stride) if coarse else particles)
         deposit = t.charge / vol * factor[:, None]
         old = rho
-        rho = deposit if iteration == 0 else (1.0 - relaxation) * rho + relaxation * deposit
+        if iteration == 0:
+            rho = deposit
+        elif mixer is not None:
+            rho = mixer.update(rho, deposit)
+        else:
+            rho = (1.0 - relaxation) * rho + relaxation * deposit
         scale = np.max(np.abs(rho))
         density_change = float(np.max(np.abs(rho - old)) / scale) if scale > 0 else 0.0
         history.append({"iteration": iteration, "max_potential_change": change,
@@ -234,6 +314,8 @@ def vlasov(p: Problem, particles, j_over_v: float, *, iterations: int, tolerance
                "history": history, "fields": (fx, fy)}  # fmt: skip
         if callback is not None:
             callback(iteration, out)
+        if coarse:
+            continue
         if change < tolerance:
             break
         if density_tolerance is not None and iteration > 0 and density_change < density_tolerance:
