@@ -79,6 +79,17 @@ class ShapesDesc(ctypes.Structure):
     _fields_ = [("count", I64), ("kind", P), ("offset", P), ("params", P)]
 
 
+class AdjointArgs(ctypes.Structure):
+    """``bt_adjoint_args`` of ``include/bt200.h``."""
+
+    _fields_ = [
+        ("x0", P), ("v0", P), ("qm", P), ("dq", P), ("steps", P), ("n", I64), ("fx", P),
+        ("fy", P), ("nx", I64), ("ny", I64), ("origin_x", F64), ("origin_y", F64), ("h", F64),
+        ("cylindrical", I64), ("step_fraction", F64), ("planes", P), ("n_planes", I64),
+        ("counts", P), ("capacity", I64), ("checkpoints", P), ("segments", I64),
+    ]  # fmt: skip
+
+
 class MeshDesc(ctypes.Structure):
     """``bt_mesh_desc`` of ``include/bt200.h``."""
 
@@ -113,6 +124,11 @@ SIGNATURES: dict[str, list] = {
     "bt_trace_trajectories_2d": [P, ctypes.POINTER(TraceArgs), I64],
     "bt_trace_last_stats": [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64)],
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],
+    "bt_edge_field_adjoint": [P, P, P, P, P, P, P, I64, I64, F64, P, P],
+    "bt_adjoint_checkpoints": [P, ctypes.POINTER(AdjointArgs), P],
+    "bt_adjoint_sweep": [P, ctypes.POINTER(AdjointArgs), P, P, P, P],
+    "bt_poisson_set_transposed": [P, I32],
+    "bt_poisson_fixed_adjoint": [P, P, P, P],
     "bt_vlasov_mix": [P, P, P, P, I64, I64, F64, I32, P, P],
     "bt_max_abs_diff": [P, P, P, I64, P],
     "bt_anderson_mix": [P, P, P, P, I64, I64, I32, I32, I32, F64, P, P, P, P, P],

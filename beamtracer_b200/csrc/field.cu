@@ -25,11 +25,25 @@ __device__ __forceinline__ double edge_len(const Line &L, i64 t) {  // edge t ..
     return L.len ? L.len[t] : L.h;
 }
 
+// The potential at a node index: the array itself for the field, or a unit vector at one
+// node for the field's transpose (every edge is linear in the potential and its branches
+// depend on the node classes only, so evaluating it on a unit vector gives that node's
+// coefficient).
+struct PhiArray {
+    const double *phi;
+    __device__ __forceinline__ double operator()(i64 idx) const { return phi[idx]; }
+};
+struct PhiUnit {
+    i64 node;
+    __device__ __forceinline__ double operator()(i64 idx) const { return idx == node ? 1.0 : 0.0; }
+};
+
 // The edge between nodes e - 1 and e (1 <= e <= n - 1) of the line starting at `base`.
-__device__ double interior_edge(const Line &L, i64 base, i64 e) {
+template <class Phi>
+__device__ double interior_edge(const Line &L, const Phi &phi, i64 base, i64 e) {
     const i64 s = L.stride;
     const i64 ia = base + (e - 1) * s, ib = base + e * s;
-    const double a = L.phi[ia], b = L.phi[ib];
+    const double a = phi(ia), b = phi(ib);
     const double h = edge_len(L, e - 1);
     const bool sa = L.solid[ia] >= 0, sb = L.solid[ib] >= 0;
     const bool na = L.near[ia] != 0, nb = L.near[ib] != 0;
@@ -40,8 +54,8 @@ __device__ double interior_edge(const Line &L, i64 base, i64 e) {
         const bool has0 = e >= 2, has3 = e + 1 <= L.n - 1;
         const bool near0 = has0 && L.near[base + (e - 2) * s] != 0;
         const bool near3 = has3 && L.near[base + (e + 1) * s] != 0;
-        const double phi0 = has0 ? L.phi[base + (e - 2) * s] : 0.0;
-        const double phi3 = has3 ? L.phi[base + (e + 1) * s] : 0.0;
+        const double phi0 = has0 ? phi(base + (e - 2) * s) : 0.0;
+        const double phi3 = has3 ? phi(base + (e + 1) * s) : 0.0;
         const double d0 = has0 ? L.dist_hi[base + (e - 2) * s] : 1.0;
         const double d3 = has3 ? L.dist_lo[base + (e + 1) * s] : 1.0;
         const double h_before = e - 1 >= 1 ? edge_len(L, e - 2) : 1.0;
@@ -54,17 +68,49 @@ __device__ double interior_edge(const Line &L, i64 base, i64 e) {
     return field;
 }
 
-__device__ double edge(const Line &L, i64 base, i64 e, int sym_lo, int sym_hi) {
+template <class Phi>
+__device__ double edge(const Line &L, const Phi &phi, i64 base, i64 e, int sym_lo, int sym_hi) {
     const i64 n = L.n;
     if (e == 0) {
-        const double first = interior_edge(L, base, 1);
-        return sym_lo ? -first : 2.0 * first - interior_edge(L, base, 2);
+        const double first = interior_edge(L, phi, base, 1);
+        return sym_lo ? -first : 2.0 * first - interior_edge(L, phi, base, 2);
     }
     if (e == n) {
-        const double first = interior_edge(L, base, n - 1);
-        return sym_hi ? -first : 2.0 * first - interior_edge(L, base, n - 2);
+        const double first = interior_edge(L, phi, base, n - 1);
+        return sym_hi ? -first : 2.0 * first - interior_edge(L, phi, base, n - 2);
     }
-    return interior_edge(L, base, e);
+    return interior_edge(L, phi, base, e);
+}
+
+// The transpose of the field along one line at node k of the line (its index `node`):
+// sum over the edges that read the node -- interior edges k - 1 .. k + 2, and the face
+// edges, which read the first or last four nodes -- of the edge's adjoint times the
+// node's coefficient in it.
+__device__ double line_adjoint(const Line &L, const double *__restrict__ bar, i64 bar_stride,
+                               i64 base, i64 k, i64 node, int sym_lo, int sym_hi) {
+    const PhiUnit unit{node};
+    double sum = 0.0;
+    const i64 lo = max((i64)1, k - 1), hi = min(L.n - 1, k + 2);
+    for (i64 e = lo; e <= hi; ++e) sum += bar[e * bar_stride] * edge(L, unit, base, e, sym_lo, sym_hi);
+    if (k <= 3) sum += bar[0] * edge(L, unit, base, 0, sym_lo, sym_hi);
+    if (k >= L.n - 4) sum += bar[L.n * bar_stride] * edge(L, unit, base, L.n, sym_lo, sym_hi);
+    return sum;
+}
+
+// phi_bar = D^T (fx_bar, fy_bar): the potential's adjoint from the edge fields' (one
+// thread per node, the sums in a fixed order).
+__global__ void edge_field_adjoint(Line lx, Line ly, i64 nx, i64 ny, int sx_lo, int sx_hi,
+                                   int sy_lo, int sy_hi, const double *__restrict__ fx_bar,
+                                   const double *__restrict__ fy_bar,
+                                   double *__restrict__ phi_bar) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nx * ny) return;
+    const i64 i = t / ny, j = t - i * ny;
+    // along x: the line of column j, fx_bar[e, j] at e * ny + j
+    const double ax = line_adjoint(lx, fx_bar + j, ny, j, i, t, sx_lo, sx_hi);
+    // along y: the line of row i, fy_bar[i, e] at i * (ny + 1) + e
+    const double ay = line_adjoint(ly, fy_bar + i * (ny + 1), 1, i * ny, j, t, sy_lo, sy_hi);
+    phi_bar[t] = ax + ay;
 }
 
 __global__ void edge_field_x(Line L, i64 ny, int sym_lo, int sym_hi, double *__restrict__ fx) {
@@ -72,7 +118,7 @@ __global__ void edge_field_x(Line L, i64 ny, int sym_lo, int sym_hi, double *__r
     const i64 total = (L.n + 1) * ny;
     if (t >= total) return;
     const i64 e = t / ny, j = t - e * ny;
-    fx[t] = edge(L, j, e, sym_lo, sym_hi);
+    fx[t] = edge(L, PhiArray{L.phi}, j, e, sym_lo, sym_hi);
 }
 
 __global__ void edge_field_y(Line L, i64 nx, int sym_lo, int sym_hi, double *__restrict__ fy) {
@@ -80,7 +126,7 @@ __global__ void edge_field_y(Line L, i64 nx, int sym_lo, int sym_hi, double *__r
     const i64 m = L.n + 1;  // ny + 1
     if (t >= nx * m) return;
     const i64 i = t / m, e = t - i * m;
-    fy[t] = edge(L, i * L.n, e, sym_lo, sym_hi);
+    fy[t] = edge(L, PhiArray{L.phi}, i * L.n, e, sym_lo, sym_hi);
 }
 
 }  // namespace
@@ -100,6 +146,25 @@ extern "C" int bt_edge_field(bt_ctx *ctx, const double *phi, const int32_t *soli
         bt::Timed timed(ctx, "edge_field");
         BT_LAUNCH(ctx, bt::edge_field_x, bt::blocks_for((nx + 1) * ny, 256), 256, 0, ctx->stream, lx, ny, extrapolation[0], extrapolation[1], fx);
         BT_LAUNCH(ctx, bt::edge_field_y, bt::blocks_for(nx * (ny + 1), 256), 256, 0, ctx->stream, ly, nx, extrapolation[2], extrapolation[3], fy);
+        BT_CHECK_LAUNCH();
+    });
+}
+
+extern "C" int bt_edge_field_adjoint(bt_ctx *ctx, const double *fx_bar, const double *fy_bar,
+                                     const int32_t *solid, const uint8_t *near,
+                                     const double *distance, const double *dx, int64_t nx,
+                                     int64_t ny, double h, const int32_t extrapolation[4],
+                                     double *phi_bar) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx && fx_bar && fy_bar && solid && near && distance && phi_bar && extrapolation,
+                   "edge field adjoint: null argument");
+        BT_REQUIRE(nx >= 3 && ny >= 3, "edge field adjoint: the mesh needs at least 3 nodes per axis");
+        const i64 nn = nx * ny;
+        bt::Line lx{nullptr, solid, near, distance, distance + nn, dx, h, nx, ny};
+        bt::Line ly{nullptr, solid, near, distance + 2 * nn, distance + 3 * nn, nullptr, h, ny, 1};
+        BT_LAUNCH(ctx, bt::edge_field_adjoint, bt::blocks_for(nn, 256), 256, 0, ctx->stream, lx, ly,
+                  nx, ny, extrapolation[0], extrapolation[1], extrapolation[2], extrapolation[3],
+                  fx_bar, fy_bar, phi_bar);
         BT_CHECK_LAUNCH();
     });
 }

@@ -143,6 +143,59 @@ __global__ void build_fine(i64 nx, i64 ny, const double *__restrict__ x, double 
     weight[t] = lx * ly;
 }
 
+// The transposed operator, scaled by the control volumes: B = W^-1 A^T W, whose
+// neighbour coefficients are B[t][nb] = A[nb][t] W_nb / W_t (A[nb][t] the coefficient of
+// the neighbour's row pointing back at t; zero for a held node's row or a held neighbour,
+// whose rows hold none); the diagonal stays.  W A is symmetric away from the cut rows next
+// to electrodes and the faces, so B equals A there and the multigrid built for A serves
+// it: A^T z = g is solved as B y = W^-1 g, z = W y.
+__global__ void transpose_c4(i64 nx, i64 ny, const double *__restrict__ c4,
+                             const double *__restrict__ weight,
+                             const uint8_t *__restrict__ active, double *__restrict__ c4t) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const i64 n = nx * ny;
+    if (t >= n) return;
+    const i64 i = t / ny, j = t - i * ny;
+    const bool free = active[t] != 0;
+    const double wt = weight[t];
+    c4t[t] = free && i > 0 ? c4[n + (t - ny)] * weight[t - ny] / wt : 0.0;  // west's east
+    c4t[n + t] = free && i < nx - 1 ? c4[t + ny] * weight[t + ny] / wt : 0.0;  // east's west
+    c4t[2 * n + t] = free && j > 0 ? c4[3 * n + (t - 1)] * weight[t - 1] / wt : 0.0;
+    c4t[3 * n + t] = free && j < ny - 1 ? c4[2 * n + (t + 1)] * weight[t + 1] / wt : 0.0;
+}
+
+// v <- v / W (divide) or v * W on the free nodes: to and from the scaled transposed system.
+__global__ void scale_by_weight(i64 n, const double *__restrict__ weight,
+                                const uint8_t *__restrict__ active, int divide,
+                                double *__restrict__ v) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n || !active[t]) return;
+    v[t] = divide ? v[t] / weight[t] : v[t] * weight[t];
+}
+
+// The sensitivity to the held potentials of a quantity whose sensitivity to phi is
+// phi_bar, given z = A_ff^-T phi_bar (free nodes): the free rows read the held neighbours'
+// potentials through their coefficients, so out_d = phi_bar_d + sum over the free
+// neighbours i of c(i -> d) z_i; 0 on free nodes.
+__global__ void fixed_adjoint(i64 nx, i64 ny, const double *__restrict__ c4,
+                              const uint8_t *__restrict__ active, const double *__restrict__ z,
+                              const double *__restrict__ phi_bar, double *__restrict__ out) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const i64 n = nx * ny;
+    if (t >= n) return;
+    if (active[t]) {
+        out[t] = 0.0;
+        return;
+    }
+    const i64 i = t / ny, j = t - i * ny;
+    double s = phi_bar[t];
+    if (i < nx - 1 && active[t + ny]) s += c4[t + ny] * z[t + ny];              // east's west
+    if (i > 0 && active[t - ny]) s += c4[n + (t - ny)] * z[t - ny];             // west's east
+    if (j < ny - 1 && active[t + 1]) s += c4[2 * n + (t + 1)] * z[t + 1];       // north's south
+    if (j > 0 && active[t - 1]) s += c4[3 * n + (t - 1)] * z[t - 1];            // south's north
+    out[t] = s;
+}
+
 __global__ void add_diag(i64 n, const double *__restrict__ base, const double *__restrict__ reaction,
                          const uint8_t *__restrict__ active, double *__restrict__ diag) {
     const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1289,6 +1342,8 @@ struct bt_poisson {
     std::vector<bt::Level> levels;
     bt::Buffer inv, status;
     bool built = false;        // hierarchy matches the current diagonal
+    bool transposed = false;   // the fine operator is A's transpose (bt_poisson_set_transposed)
+    bt::Buffer c4_plain;       // A's own coefficients while the operator is transposed
     bool reaction_on = false;  // level-0 diagonal holds a reaction
     int restart = 30;
     // the V-cycle's settings (bt_poisson_set_options)
@@ -1364,6 +1419,13 @@ void build_operator(bt_poisson *p) {
         p->distance.as<double>(4 * n), p->neumann[0], p->neumann[1], p->neumann[2],
         p->neumann[3], L.c4.as<double>(4 * n), L.base.as<double>(n), p->src.as<double>(n),
         L.weight.as<double>(n), L.active.as<uint8_t>(n));
+    if (p->transposed) {
+        double *plain = p->c4_plain.as<double>(4 * n);
+        BT_CUDA(cudaMemcpyAsync(plain, L.c4.as<double>(4 * n), sizeof(double) * 4 * n,
+                                cudaMemcpyDeviceToDevice, st));
+        BT_LAUNCH(p->ctx, transpose_c4, blocks_for(n, 256), 256, 0, st, p->nx, p->ny, plain,
+                  L.weight.as<double>(n), L.active.as<uint8_t>(n), L.c4.as<double>(4 * n));
+    }
     BT_CHECK_LAUNCH();
     p->built = false;
     p->reaction_on = true;  // force the diagonal to be set
@@ -1888,6 +1950,14 @@ extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, d
             b, phi);
         BT_CHECK_LAUNCH();
         int total_cycles = 0, steps = 0;
+        BT_REQUIRE(!p->transposed || !(amplitude > 0.0),
+                   "poisson: the transposed solver takes linear solves only");
+        const double *weight = L0.weight.as<double>(n);
+        const uint8_t *active = L0.active.as<uint8_t>(n);
+        if (p->transposed) {  // A^T z = b as B y = W^-1 b, y = W^-1 z (transpose_c4)
+            BT_LAUNCH(p->ctx, bt::scale_by_weight, bt::blocks_for(n, 256), 256, 0, st, n, weight, active, 1, b);
+            BT_LAUNCH(p->ctx, bt::scale_by_weight, bt::blocks_for(n, 256), 256, 0, st, n, weight, active, 1, phi);
+        }
         if (!(amplitude > 0.0)) {
             if (!p->built || p->reaction_on) bt::build_hierarchy(p, nullptr);
             // r0 = b - A phi; the tolerance is relative to the larger of |b| and |r0|
@@ -1900,6 +1970,8 @@ extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, d
             const double goal = tol * (scale > 0.0 ? scale : 1.0);
             total_cycles = bt::gmres(p, r0, d, goal, max_cycles, &left);
             BT_LAUNCH(p->ctx, bt::add_into, bt::blocks_for(n, 256), 256, 0, st, d, n, phi);
+            if (p->transposed)
+                BT_LAUNCH(p->ctx, bt::scale_by_weight, bt::blocks_for(n, 256), 256, 0, st, n, weight, active, 0, phi);
             BT_CHECK_LAUNCH();
             // a residual stalled within 1e4 of the goal is the floor of its own rounding
             if (!(left <= 1e4 * goal))
@@ -1940,6 +2012,29 @@ extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, d
             throw bt::Error{BT_ERR_NOCONV, "field solve: the coarsest operator is singular (is any node held?)"};
         if (newton_steps) *newton_steps = steps;
         if (cycles) *cycles = total_cycles;
+    });
+}
+
+extern "C" int bt_poisson_set_transposed(bt_poisson *p, int32_t on) {
+    return bt::guarded([&] {
+        BT_REQUIRE(p, "poisson: null solver");
+        if ((on != 0) == p->transposed) return;
+        BT_CUDA(cudaStreamSynchronize(p->ctx->stream));
+        p->transposed = on != 0;
+        bt::build_operator(p);
+    });
+}
+
+extern "C" int bt_poisson_fixed_adjoint(bt_poisson *p, const double *z, const double *phi_bar,
+                                        double *out) {
+    return bt::guarded([&] {
+        BT_REQUIRE(p && z && phi_bar && out, "poisson: null argument");
+        const i64 n = p->n;
+        bt::Level &L0 = p->levels[0];
+        const double *c4 = p->transposed ? p->c4_plain.as<double>(4 * n) : L0.c4.as<double>(4 * n);
+        BT_LAUNCH(p->ctx, bt::fixed_adjoint, bt::blocks_for(n, 256), 256, 0, p->ctx->stream,
+                  p->nx, p->ny, c4, L0.active.as<uint8_t>(n), z, phi_bar, out);
+        BT_CHECK_LAUNCH();
     });
 }
 

@@ -93,6 +93,8 @@ class IonOpticsPoisson:
         backend: str = "multigrid",
         comm: Any = None,
         refinement=(),
+        *,
+        transposed: bool = False,
     ) -> None:
         if tuple(refinement):
             raise NotImplementedError("refined boxes are not supported by this build")
@@ -113,6 +115,12 @@ class IonOpticsPoisson:
         self._distance = np.ascontiguousarray(mesh.distance, dtype=np.float64)
         self._x = np.ascontiguousarray(mesh.x, dtype=np.float64)
         self._neumann = _neumann_values(mesh)
+        #: a solver of the transposed free block A_ff^T z = b (held values and face terms
+        #: zero), for the adjoint; linear solves only
+        self.transposed = bool(transposed)
+        if self.transposed:
+            self._value = np.zeros_like(self._value)
+            self._neumann = np.zeros_like(self._neumann)
         desc = _lib.MeshDesc(
             nx, ny, float(mesh.h), self._x.ctypes.data, float(mesh.origin[1]),
             int(mesh.cylindrical), self._fixed.ctypes.data, self._value.ctypes.data,
@@ -123,6 +131,15 @@ class IonOpticsPoisson:
                                                 ctypes.byref(handle)))  # fmt: skip
         self._handle = handle
         self._region_key: object = None
+        if self.transposed:
+            _lib.check(_lib.lib().bt_poisson_set_transposed(handle, 1))
+
+    def fixed_adjoint(self, z, phi_bar, out) -> None:
+        """``out`` (device, (nx, ny)) <- the sensitivity to the held nodes' potentials of a
+        quantity whose sensitivity to the potential is ``phi_bar``, given
+        ``z = A_ff^-T phi_bar`` on the free nodes (``bt_poisson_fixed_adjoint``)."""
+        _lib.check(_lib.lib().bt_poisson_fixed_adjoint(self._handle, _lib.dptr(z),
+                                                       _lib.dptr(phi_bar), _lib.dptr(out)))  # fmt: skip
 
     def close(self) -> None:
         if getattr(self, "_handle", None):
@@ -191,6 +208,8 @@ class IonOpticsPoisson:
         ``tolerance * max(ptp(prescribed potentials), T, 1 V)`` (``poisson.py:874-877``).
         """
         self._set_region(fixed_region, fixed_potential)
+        if self.transposed and (plasma is not None or fixed_region is not None):
+            raise NotImplementedError("the transposed solver takes linear solves only")
         steps, cycles = _lib.I32(), _lib.I32()
         if plasma is None:
             args = (0.0, 1.0, 0.0, 1, linear_tolerance, 0.0, 0)

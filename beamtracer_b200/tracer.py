@@ -553,11 +553,14 @@ class TraceEngine:
         n_planes = len(self.planes)
         slots = torch.arange(self.hits.shape[2], device=self.hits.device)
         pieces, sizes = [], []
+        #: per plane, the (trajectory, buffer slot) of every returned crossing, in order
+        self.hit_slots = []
         for p in range(n_planes):
             k, c = (slots[None, :] < self.counts[:, p, None]).nonzero(as_tuple=True)
             record = self.hits[k, p, c]
             order = torch.sort(record[:, 7], stable=True).indices
             pieces.append(torch.cat([record[order], k[order, None].to(torch.float64)], dim=1))
+            self.hit_slots.append((k[order], c[order]))
             sizes.append(int(k.numel()))
         crossings = (torch.cat(pieces).cpu().numpy() if pieces else np.zeros((0, 9)))
         ints = torch.stack([self.status, self.electrode, self.steps]).cpu().numpy()

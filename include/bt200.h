@@ -226,6 +226,15 @@ int bt_edge_field(bt_ctx *ctx, const double *phi, const int32_t *solid, const ui
                   const double *distance, const double *dx, int64_t nx, int64_t ny,
                   double h, const int32_t extrapolation[4], double *fx, double *fy);
 
+/* The transpose of bt_edge_field (no counterpart in the reference; the differentiation
+ * form): phi_bar (nx, ny) = D^T (fx_bar, fy_bar), D the linear map from the potential to
+ * the edge fields that bt_edge_field applies on the same mesh arrays.  One thread a node,
+ * its sum in a fixed order: the same bits on every call. */
+int bt_edge_field_adjoint(bt_ctx *ctx, const double *fx_bar, const double *fy_bar,
+                          const int32_t *solid, const uint8_t *near, const double *distance,
+                          const double *dx, int64_t nx, int64_t ny, double h,
+                          const int32_t extrapolation[4], double *phi_bar);
+
 /* -- the per-iteration updates (device pointers) -------------------------------------- */
 
 /* solver/vlasov.py:127-173 (AndersonMixer.update), on the device.  Anderson mixing of type
@@ -293,6 +302,22 @@ int bt_poisson_set_region(bt_poisson *p, const uint8_t *mask, double value);
 int bt_poisson_set_options(bt_poisson *p, int32_t fine_sweeps, int32_t coarse_sweeps,
                            int32_t staged, int64_t tail_nodes);
 
+/* No counterpart in the reference (the differentiation form).  on != 0: the solver's
+ * operator becomes the transpose of the free rows' block, A_ff^T (the neighbour
+ * coefficients exchanged between each pair of free nodes, the diagonal kept), so
+ * bt_poisson_solve solves A_ff^T z = rho / eps0 (+ its face and held terms: give the
+ * transposed solver zero held values and zero Neumann values for a plain A_ff^T z = b).
+ * It solves the similar system B y = W^-1 b, z = W y, B = W^-1 A^T W with W the control
+ * volumes, which equals A wherever W A is symmetric, so the multigrid serves it as it
+ * serves A.  Linear solves only (no Boltzmann species). */
+int bt_poisson_set_transposed(bt_poisson *p, int32_t on);
+
+/* No counterpart in the reference.  The held potentials' sensitivity: given phi_bar (the
+ * sensitivity of a quantity to every node's potential) and z = A_ff^-T phi_bar (free
+ * nodes), out (DEVICE, nx * ny) = phi_bar_d + sum over the free neighbours i of held
+ * node d of A's coefficient from i to d times z_i, on held nodes; 0 on free nodes. */
+int bt_poisson_fixed_adjoint(bt_poisson *p, const double *z, const double *phi_bar, double *out);
+
 /* poisson.py:809-933 (IonOpticsPoisson.solve).  phi (DEVICE (nx, ny), in/out): the first
  * guess on entry (its fixed nodes are set), the solution on return; rho (DEVICE (nx, ny),
  * C/m^3, or NULL).  With amplitude = 0 one linear solve: GMRES preconditioned by a
@@ -306,6 +331,42 @@ int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, double ampli
                      double temperature, double up, int32_t sign, double tol,
                      double newton_tol, int32_t max_newton, int32_t *newton_steps,
                      int32_t *cycles);
+
+/* -- the adjoint of the trace (the differentiation form; no counterpart in the reference) -- */
+
+/* A forward trace to reverse: RK4, one uniform patch, no magnetic field, not relativistic,
+ * planar (0) or cylindrical (1).  All arrays on the DEVICE. */
+typedef struct bt_adjoint_args {
+    const double *x0, *v0;  /* (3, n) the trajectories' start states */
+    const double *qm, *dq;  /* (n,) charge / mass, signed current */
+    const int64_t *steps;   /* (n,) the steps each took in the forward trace */
+    int64_t n;
+    const double *fx, *fy;  /* the forward trace's edge fields (nx + 1, ny), (nx, ny + 1) */
+    int64_t nx, ny;
+    double origin_x, origin_y, h;
+    int64_t cylindrical;
+    double step_fraction;
+    const double *planes;   /* (n_planes,), at most 8 */
+    int64_t n_planes;
+    const int64_t *counts;  /* (n, n_planes) the forward trace's crossing counts */
+    int64_t capacity;       /* of the hit buffers the hit adjoint is laid out as */
+    double *checkpoints;    /* (segments, 6, n): the states every 64 steps */
+    int64_t segments;       /* at least ceil(max(steps) / 64) */
+} bt_adjoint_args;
+
+/* Replays every trajectory for its forward steps (trace.cu's step, the same bits) and
+ * keeps its state every 64 steps in checkpoints; its end state (DEVICE (6, n): x then v)
+ * in end_state unless NULL. */
+int bt_adjoint_checkpoints(bt_ctx *ctx, const bt_adjoint_args *args, double *end_state);
+
+/* The reverse sweep (after bt_adjoint_checkpoints): ADDS to fx_bar (nx + 1, ny) and fy_bar
+ * (nx, ny + 1) the adjoint of the edge fields of a quantity whose adjoints of the trace's
+ * outputs are charge_seed (nx, ny; the node charges the trace deposits) and hit_seed
+ * (n, n_planes, capacity, 8; slots 1-5 the crossings' point y, z and velocity; the hits
+ * buffer's layout); either may be NULL.  The scatter adds with atomics: reproducible to
+ * rounding, not bit for bit. */
+int bt_adjoint_sweep(bt_ctx *ctx, const bt_adjoint_args *args, const double *charge_seed,
+                     const double *hit_seed, double *fx_bar, double *fy_bar);
 
 #ifdef __cplusplus
 }

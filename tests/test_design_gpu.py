@@ -4,7 +4,8 @@ The gradient of the rms angle and the current at the last plane with respect to 
 voltages and the beam current, by central differences of converged solves of the lens at
 401 x 101 with 8,000 rings, must equal the oracle's central differences of its own
 converged solves: the two solvers agree to about 1e-12 per solve, far inside what a 1e-4
-step resolves.
+step resolves.  The adjoint of one converged solve (``beamtracer_b200.adjoint``) must give
+both within 1e-4.
 """
 
 from __future__ import annotations
@@ -51,24 +52,60 @@ def _oracle_moments(design: EinzelDesign, plane: float, tolerance: float, iterat
     return plane_moments(hits, cylindrical=True, mass=mass)
 
 
-def test_gradient_matches_the_oracle_central_differences():
-    plane, tol, its, rel = 79e-3, 1e-7, 60, 1e-4
-    gpu = design_gradient(C4, plane, rel_step=rel, tolerance=tol, iterations=its)
-    assert gpu["solves"] == 2 * len(GRADIENT_PARAMETERS)
+PLANE, TOL, ITS, REL = 79e-3, 1e-7, 60, 1e-4
+
+
+@pytest.fixture(scope="module")
+def gpu_fd():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("the GPU tests need a CUDA device")
+    return design_gradient(C4, PLANE, rel_step=REL, tolerance=TOL, iterations=ITS)
+
+
+@pytest.fixture(scope="module")
+def oracle_fd():
     scale = max(abs(v) for v in resolved_voltages(C4))
+    out = {"rms_angle": np.zeros(4), "current": np.zeros(4)}
     for k, name in enumerate(GRADIENT_PARAMETERS):
-        step = rel * (C4.current if name == "current" else scale)
-        plus = _oracle_moments(_perturbed(C4, name, step), plane, tol, its)
-        minus = _oracle_moments(_perturbed(C4, name, -step), plane, tol, its)
-        angle = (plus.rms_angle - minus.rms_angle) / (2 * step)
-        current = (plus.current - minus.current) / (2 * step)
-        assert gpu["rms_angle"][k] == pytest.approx(angle, rel=1e-5, abs=1e-12), name
-        assert gpu["current"][k] == pytest.approx(current, rel=1e-5, abs=1e-12), name
-    assert np.all(np.isfinite(gpu["rms_angle"])) and gpu["rms_angle"][1] != 0.0
-    concurrent = design_gradient(C4, plane, rel_step=rel, tolerance=tol, iterations=its,
+        step = REL * (C4.current if name == "current" else scale)
+        plus = _oracle_moments(_perturbed(C4, name, step), PLANE, TOL, ITS)
+        minus = _oracle_moments(_perturbed(C4, name, -step), PLANE, TOL, ITS)
+        out["rms_angle"][k] = (plus.rms_angle - minus.rms_angle) / (2 * step)
+        out["current"][k] = (plus.current - minus.current) / (2 * step)
+    return out
+
+
+def test_gradient_matches_the_oracle_central_differences(gpu_fd, oracle_fd):
+    assert gpu_fd["solves"] == 2 * len(GRADIENT_PARAMETERS)
+    for k, name in enumerate(GRADIENT_PARAMETERS):
+        assert gpu_fd["rms_angle"][k] == pytest.approx(oracle_fd["rms_angle"][k], rel=1e-5,
+                                                       abs=1e-12), name  # fmt: skip
+        assert gpu_fd["current"][k] == pytest.approx(oracle_fd["current"][k], rel=1e-5,
+                                                     abs=1e-12), name  # fmt: skip
+    assert np.all(np.isfinite(gpu_fd["rms_angle"])) and gpu_fd["rms_angle"][1] != 0.0
+    concurrent = design_gradient(C4, PLANE, rel_step=REL, tolerance=TOL, iterations=ITS,
                                  concurrency=8)  # fmt: skip
-    np.testing.assert_array_equal(concurrent["rms_angle"], gpu["rms_angle"])
-    np.testing.assert_array_equal(concurrent["current"], gpu["current"])
+    np.testing.assert_array_equal(concurrent["rms_angle"], gpu_fd["rms_angle"])
+    np.testing.assert_array_equal(concurrent["current"], gpu_fd["current"])
+
+
+def test_adjoint_gradient_matches_central_differences(gpu_fd, oracle_fd):
+    """The adjoint of one converged solve (``torch.autograd`` through the hand-written
+    reverse) against the central differences of eight solves, on the device and in the
+    oracle: within 1e-4 relative."""
+    from beamtracer_b200.adjoint import adjoint_design_gradient
+
+    adjoint = adjoint_design_gradient(C4, PLANE, tolerance=TOL, iterations=ITS)
+    assert adjoint["adjoint_iterations"] >= 2
+    scale = np.abs(gpu_fd["rms_angle"]).max()
+    for k, name in enumerate(GRADIENT_PARAMETERS):
+        for fd in (gpu_fd, oracle_fd):
+            assert adjoint["rms_angle"][k] == pytest.approx(fd["rms_angle"][k], rel=1e-4,
+                                                            abs=1e-6 * scale), name  # fmt: skip
+            assert adjoint["current"][k] == pytest.approx(fd["current"][k], rel=1e-4,
+                                                          abs=1e-12), name  # fmt: skip
 
 
 def test_sweep_solves_this_ranks_share():
