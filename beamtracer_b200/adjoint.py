@@ -249,6 +249,8 @@ class LensProblem:
         self.adjoint_tolerance = float(adjoint_tolerance)
         #: the fixed-point iterations of the last adjoint solve
         self.adjoint_iterations = 0
+        #: whether the last forward solve met its tolerance
+        self.converged = False
 
     def config(self, params: np.ndarray):
         from beamtracer_b200.einzel import einzel_config
@@ -282,6 +284,7 @@ class LensMoments:
             def forward(ctx, params, problem):
                 values = params.detach().cpu().numpy().astype(np.float64)
                 model = problem.solve(values)
+                problem.converged = bool(model.stats["converged"])
                 hits = model.plane(problem.plane)
                 ctx.problem, ctx.model, ctx.values = problem, model, values
                 ctx.hits_current = np.array(hits.current, dtype=np.float64)
@@ -333,4 +336,5 @@ def adjoint_design_gradient(design, plane: float = 79e-3, tolerance: float = 1e-
     (transmitted,) = torch.autograd.grad(moments["current"], params)
     return {"rms_angle": angle.numpy().copy(), "current": transmitted.numpy().copy(),
             "moments": {k: float(v.detach()) for k, v in moments.items()}, "solves": 1,
-            "adjoint_iterations": problem.adjoint_iterations}  # fmt: skip
+            "adjoint_iterations": problem.adjoint_iterations,
+            "converged": problem.converged}  # fmt: skip

@@ -78,3 +78,32 @@ def field_points(seed: int, z0: float, hz: float, n: int) -> tuple[np.ndarray, n
 
 #: A configuration's solenoid sampling: (x_min, x_max, node spacing, solenoids, order).
 SAMPLING_CASE = (0.0, 8e-3, 0.1e-3, ((5e-3, 4e-3, 3e-3, 0.5), (6.5e-3, 2e-3, 1e-3, -0.1)), 3)
+
+
+#: Designs for the record's keys: (parameters (name, lower, upper), points to key).
+RECORD_DESIGNS = {
+    "v_mid": ((("v_mid", 3e3, 12e3),), [[3e3], [7.123456789e3], [12e3], [5.5e3 + 1e-9]]),
+    "lens": ((("v_mid", 3e3, 12e3), ("aperture", 3e-3, 7e-3), ("gap", 10e-3, 25e-3)),
+             [[4e3, 5e-3, 12e-3], [11.9e3, 3e-3, 25e-3], [7e3, 6.999999e-3, 17.5e-3]]),
+}  # fmt: skip
+
+#: The design whose evaluations make the reference record.
+RECORD_CASE = "lens"
+
+
+def record_evaluations(names, points) -> list[dict]:
+    """Evaluations of the record case: objectives, a constraint, flags and diagnostics,
+    one failed evaluation and one with a non-finite objective."""
+    out = []
+    for k, x in enumerate(points):
+        values = dict(zip(names, map(float, x), strict=True))
+        out.append({
+            "objectives": {"rms_angle": 1e-3 * (k + 1), "emittance": 2e-6 / (k + 1)},
+            "constraints": {"transmission": 0.05 * k - 0.05},
+            "converged": k != 1, "wall_time": 0.25 * k,
+            "failure": "RuntimeError: no convergence" if k == 1 else None,
+            "diagnostics": {"iterations": 7 + k, "note": f"case {k}", "ok_flag": True,
+                            "current": float("nan") if k == 2 else 1e-3},
+            "parameters": values, "generation": None if k == 0 else k,
+        })  # fmt: skip
+    return out

@@ -204,6 +204,44 @@ def host_goldens(root: Path) -> None:
           len(fields), "field arrays")
 
 
+def record_goldens(root: Path) -> None:
+    """``record_*``: the design keys and the record lines of the reference's
+    ``optimization/design.py`` (``Design.key``, ``Evaluation.to_dict``) and
+    ``optimization/record.py`` (``Record.append``) on the cases of
+    ``tests/golden/host_cases.py`` -- the record format a search resumes from."""
+    import json
+
+    from tests.golden import host_cases as hc
+
+    card = types.ModuleType("methodcard")
+    card.method = lambda *a, **k: (lambda obj: obj)
+    sys.modules["methodcard"] = card
+    units = types.ModuleType("plasmacoll.units")
+    units.to_unit = lambda value, unit, name=None: float(value)
+    sys.modules.setdefault("plasmacoll", types.ModuleType("plasmacoll"))
+    sys.modules["plasmacoll.units"] = units
+    opt = root / "src" / "beamtracer" / "optimization"
+    design_module = _load(opt / "design.py", "_ref_design")
+    for name in ("beamtracer", "beamtracer.optimization"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.modules["beamtracer.optimization.design"] = design_module
+    record_module = _load(opt / "record.py", "_ref_record")
+    keys = {}
+    for name, (parameters, points) in hc.RECORD_DESIGNS.items():
+        design = design_module.Design(tuple(design_module.Parameter(*p) for p in parameters))
+        keys[name] = [design.key(x) for x in points]
+    (HERE / "record_keys.json").write_text(json.dumps(keys, indent=1) + "\n")
+    parameters, points = hc.RECORD_DESIGNS[hc.RECORD_CASE]
+    design = design_module.Design(tuple(design_module.Parameter(*p) for p in parameters))
+    path = HERE / "record_reference.jsonl"
+    if path.exists():
+        path.unlink()
+    record = record_module.Record(design, path)
+    evaluations = [design_module.Evaluation(**e) for e in hc.record_evaluations(design.names, points)]
+    record.append(evaluations)
+    print("record goldens:", sum(len(v) for v in keys.values()), "keys,", len(record), "lines")
+
+
 def _save(name: str, args: list, result: list, extra: dict | None = None) -> None:
     arrays = {}
     for i, (a, r) in enumerate(zip(args, result, strict=True)):
@@ -227,6 +265,7 @@ def main() -> None:
     if not (root / "src" / "beamtracer").is_dir():
         parser.error(f"{root} holds no src/beamtracer package")
     host_goldens(root)
+    record_goldens(root)
     ref = reference_kernels(root)
 
     for seed in (4, 5, 6):
