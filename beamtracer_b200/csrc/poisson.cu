@@ -622,8 +622,91 @@ __global__ void prolong_add(Fine F, const double *__restrict__ xc, double *__res
 // operator: no node of the mesh is held).
 constexpr int kInvertThreads = 1024;
 
+// The coarsest operator is a 9-point stencil: ordered along its shorter side first its
+// matrix is banded with half-bandwidth b = min(nx, ny) + 1 (at most 17 for 256 nodes), and
+// its LU factors without pivoting fit shared memory (n rows of 2b + 1).  One block
+// factorises it (b^2 updates a step between two barriers), then one thread a column
+// solves L U x = e_c into the dense inverse the V-cycle applies.  A pivot smaller than
+// 1e-12 of its row (a matrix that needs pivoting, or a singular one) sets *fallback and the
+// pivoting Gauss-Jordan below computes the inverse instead.
+constexpr int kBandThreads = 512;
+constexpr int kBandMax = 17;
+
+__host__ __device__ __forceinline__ int band_half(i64 nx, i64 ny) {
+    return (int)(nx < ny ? nx : ny) + 1;
+}
+
+__host__ __device__ __forceinline__ size_t band_smem(i64 nx, i64 ny) {
+    return sizeof(double) * (size_t)(nx * ny) * (size_t)(2 * band_half(nx, ny) + 1);
+}
+
+__global__ void __launch_bounds__(kBandThreads) coarsest_band_invert(
+    i64 nx, i64 ny, const double *__restrict__ a9, double *__restrict__ M,
+    int *__restrict__ fallback) {
+    extern __shared__ double band[];  // row r: band[r * W + (c - r + b)], |c - r| <= b
+    const int n = (int)(nx * ny);
+    const bool across = nx < ny;  // order x fastest when x is the shorter side
+    const int b = band_half(nx, ny), W = 2 * b + 1;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    auto order_of = [&](int node) {
+        return across ? (node % (int)ny) * (int)nx + node / (int)ny : node;
+    };
+    auto node_of = [&](int o) { return across ? (o % (int)nx) * (int)ny + o / (int)nx : o; };
+    for (int e = tid; e < n * W; e += nt) band[e] = 0.0;
+    __syncthreads();
+    for (int node = tid; node < n; node += nt) {
+        const int i = node / (int)ny, j = node % (int)ny, r = order_of(node);
+        for (int di = -1; di <= 1; ++di)
+            for (int dj = -1; dj <= 1; ++dj) {
+                const int i2 = i + di, j2 = j + dj;
+                if (i2 < 0 || i2 >= nx || j2 < 0 || j2 >= ny) continue;
+                const int c = order_of(i2 * (int)ny + j2);
+                band[r * W + (c - r + b)] = a9[(i64)((di + 1) * 3 + (dj + 1)) * n + node];
+            }
+    }
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const double piv = band[k * W + b];
+        if (tid == 0) {
+            double row = 0.0;
+            for (int q = 0; q < W; ++q) row = fmax(row, fabs(band[k * W + q]));
+            if (!(fabs(piv) > 1e-12 * row)) *fallback = 1;
+        }
+        const int last = min(n - 1, k + b);
+        for (int r = k + 1 + tid; r <= last; r += nt) band[r * W + (k - r + b)] /= piv;
+        __syncthreads();
+        const int m = last - k;  // rows and columns k + 1 .. last
+        for (int e = tid; e < m * m; e += nt) {
+            const int r = k + 1 + e / m, c = k + 1 + e % m;
+            band[r * W + (c - r + b)] -= band[r * W + (k - r + b)] * band[k * W + (c - k + b)];
+        }
+        __syncthreads();
+    }
+    if (*fallback) return;
+    for (int col = tid; col < n; col += nt) {
+        const int oc = order_of(col);
+        // L y = e (unit lower, band b), y in M's column col: y_r = 0 for r < oc
+        for (int o = 0; o < oc; ++o) M[(i64)node_of(o) * n + col] = 0.0;
+        for (int o = oc; o < n; ++o) {
+            double y = o == oc ? 1.0 : 0.0;
+            for (int q = max(oc, o - b); q < o; ++q)
+                y -= band[o * W + (q - o + b)] * M[(i64)node_of(q) * n + col];
+            M[(i64)node_of(o) * n + col] = y;
+        }
+        // U x = y, in place
+        for (int o = n - 1; o >= 0; --o) {
+            double x = M[(i64)node_of(o) * n + col];
+            for (int q = o + 1; q <= min(n - 1, o + b); ++q)
+                x -= band[o * W + (q - o + b)] * M[(i64)node_of(q) * n + col];
+            M[(i64)node_of(o) * n + col] = x / band[o * W + b];
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kInvertThreads) coarsest_invert(
-    i64 nx, i64 ny, const double *__restrict__ a9, double *M, int *__restrict__ status) {
+    i64 nx, i64 ny, const double *__restrict__ a9, double *M, int *__restrict__ status,
+    const int *__restrict__ fallback) {
+    if (fallback && *fallback == 0) return;  // the banded factorisation made the inverse
     __shared__ int perm[kCoarsest];
     __shared__ double best_v[kInvertThreads / 32];
     __shared__ int best_r[kInvertThreads / 32];
@@ -1434,6 +1517,7 @@ void build_operator(bt_poisson *p) {
 // Set the level-0 diagonal (with `reaction`, or without) and rebuild the coarse levels.
 void build_hierarchy(bt_poisson *p, const double *reaction) {
     cudaStream_t st = p->ctx->stream;
+    Timed timed(p->ctx, "hierarchy");
     Level &L0 = p->levels[0];
     BT_LAUNCH(p->ctx, add_diag, blocks_for(p->n, 256), 256, 0, st, p->n, L0.base.as<double>(p->n), reaction,
                                                     L0.active.as<uint8_t>(p->n),
@@ -1449,10 +1533,19 @@ void build_hierarchy(bt_poisson *p, const double *reaction) {
         BT_LAUNCH(p->ctx, five_to_nine, blocks_for(Lc.n, 256), 256, 0, st, Lc.n,
                   Lc.c4.as<double>(4 * Lc.n), Lc.diag.as<double>(Lc.n), Lc.active.as<uint8_t>(Lc.n),
                   Lc.a9.as<double>(9 * Lc.n));
-    int *status = p->status.as<int>(1);
-    BT_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-    BT_LAUNCH(p->ctx, coarsest_invert, 1, kInvertThreads, 0, st, Lc.nx, Lc.ny,
-              Lc.a9.as<double>(9 * Lc.n), p->inv.as<double>(Lc.n * Lc.n), status);
+    int *status = p->status.as<int>(2);  // [0] singular, [1] the banded path fell back
+    BT_CUDA(cudaMemsetAsync(status, 0, 2 * sizeof(int), st));
+    double *inv = p->inv.as<double>(Lc.n * Lc.n);
+    const double *a9c = Lc.a9.as<double>(9 * Lc.n);
+    if (band_half(Lc.nx, Lc.ny) <= kBandMax) {
+        BT_LAUNCH(p->ctx, coarsest_band_invert, 1, kBandThreads, band_smem(Lc.nx, Lc.ny), st,
+                  Lc.nx, Lc.ny, a9c, inv, status + 1);
+        BT_LAUNCH(p->ctx, coarsest_invert, 1, kInvertThreads, 0, st, Lc.nx, Lc.ny, a9c, inv,
+                  status, status + 1);
+    } else {
+        BT_LAUNCH(p->ctx, coarsest_invert, 1, kInvertThreads, 0, st, Lc.nx, Lc.ny, a9c, inv,
+                  status, (const int *)nullptr);
+    }
     BT_CHECK_LAUNCH();
     refresh_tail_image(p);
     p->built = true;
@@ -1476,6 +1569,11 @@ void setup_tail(bt_poisson *p) {
     BT_CUDA(cudaFuncSetAttribute(smooth_staged<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big5));
     BT_CUDA(cudaFuncSetAttribute(smooth_staged<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big5));
     BT_CUDA(cudaFuncSetAttribute(smooth_staged<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big9));
+    {
+        const Level &Lc = p->levels.back();
+        BT_CUDA(cudaFuncSetAttribute(coarsest_band_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)band_smem(Lc.nx, Lc.ny)));
+    }
     if (p->tail_start <= 0) return;
     const TailLayout T = tail_layout(p->levels, p->tail_start);
     p->tail_smem = T.total();

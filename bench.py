@@ -292,7 +292,8 @@ def run_plasma(args) -> None:
         torch.cuda.synchronize()
     total_ms = float(sum(a.elapsed_time(b) for a, b in events))
     timers = {name: ctx.read_timer(name) for name in
-              ("trace_window", "deposit", "field_solve", "vcycle", "edge_field")}  # fmt: skip
+              ("trace_window", "deposit", "field_solve", "vcycle", "hierarchy",
+               "edge_field")}  # fmt: skip
     ctx.set_timing(False)
     launches = ctx.launch_count() - launches_before
     e2e_ms = []
@@ -536,7 +537,7 @@ def main() -> None:
         total_ms = float(t.item())
     value = world * args.steps / (total_ms / 1e3)
     timers = {name: ctx.read_timer(name) for name in
-              ("trace_window", "deposit", "field_solve", "vcycle", "edge_field",
+              ("trace_window", "deposit", "field_solve", "vcycle", "hierarchy", "edge_field",
                "vlasov_mix")}  # fmt: skip
     ctx.set_timing(False)
     history = state.history

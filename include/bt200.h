@@ -47,7 +47,8 @@ int bt_ctx_set_stream(bt_ctx *ctx, void *stream);
 int bt_ctx_synchronize(bt_ctx *ctx);
 /* Time the context's launches with CUDA events on its stream (off by default): the
  * kernels "trace_window", "deposit" (the sort and reduction of a flush of records),
- * "field_solve" (a whole bt_poisson_solve), "vcycle" (one multigrid V-cycle), "edge_field",
+ * "field_solve" (a whole bt_poisson_solve), "vcycle" (one multigrid V-cycle), "hierarchy"
+ * (the coarse operators and the coarsest inverse of a new operator), "edge_field",
  * "vlasov_mix",
  * "staggered_field_2d".  bt_ctx_read_timer waits for the recorded launches and returns
  * their summed time [ms] and count since the last reset. */
