@@ -122,6 +122,10 @@ SIGNATURES: dict[str, list] = {
     "bt_trace_trajectories_2d_magnetic": [P, ctypes.POINTER(TraceArgs),
                                           ctypes.POINTER(MagneticDesc), I64],
     "bt_trace_trajectories_2d": [P, ctypes.POINTER(TraceArgs), I64],
+    "bt_trace_trajectories_2d_fast": [P, ctypes.POINTER(TraceArgs), I64],
+    "bt_trace_trajectories_2d_magnetic_fast": [P, ctypes.POINTER(TraceArgs),
+                                               ctypes.POINTER(MagneticDesc), I64],
+    "bt_measure_fp64_peak": [P, ctypes.POINTER(F64)],
     "bt_trace_last_stats": [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64)],
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],
     "bt_edge_field_adjoint": [P, P, P, P, P, P, P, I64, I64, F64, P, P],
@@ -216,6 +220,12 @@ class Context:
         count = I64()
         check(lib().bt_ctx_deposit_records(self.handle, ctypes.byref(count)))
         return count.value
+
+    def fp64_peak(self) -> float:
+        """The FP64 pipe's measured peak [TFLOP/s] on this context's device."""
+        value = F64()
+        check(lib().bt_measure_fp64_peak(self.handle, ctypes.byref(value)))
+        return value.value
 
     def reset_timers(self) -> None:
         check(lib().bt_ctx_reset_timers(self.handle))

@@ -168,29 +168,37 @@ class SolveAdjoint:
         seed[k, plane, c, 1:6] = values
         return seed
 
-    def solve(self, hit_seed, tolerance: float = 1e-10, max_iterations: int = 100
-              ) -> FixedPointAdjoint:  # fmt: skip
-        """``lambda = (dJ/drho)^T + G_rho^T lambda`` by the fixed-point iteration, from the
-        crossings' adjoint ``hit_seed`` (hit-buffer layout)."""
+    def solve(self, hit_seed, tolerance: float = 1e-8, max_iterations: int = 100,
+              depth: int = 4) -> FixedPointAdjoint:  # fmt: skip
+        """``lambda = (dJ/drho)^T + G_rho^T lambda`` from the crossings' adjoint
+        ``hit_seed`` (hit-buffer layout): the map is affine, so its fixed point is found by
+        Anderson mixing of depth ``depth`` (`AndersonMixer`; for an affine map a Krylov
+        method) until the residual ``|K(lambda) - lambda|`` is below ``tolerance`` of
+        ``|K(lambda)|``; every transposed solve starts from the last one's solution."""
         import torch
+
+        from beamtracer_b200.vlasov import AndersonMixer
 
         nx, ny = self.mesh.shape
         volumes = self.engine.volumes.reshape(nx, ny)
         lam = torch.zeros((nx, ny), dtype=torch.float64, device="cuda")
         z = torch.zeros_like(lam)
+        mixer = AndersonMixer(depth, relaxation=1.0) if depth > 0 else None
         change = float("inf")
         for iteration in range(1, max_iterations + 1):
             charge_seed = (lam / volumes).contiguous() if iteration > 1 else None
             fx_bar, fy_bar = self.trace.sweep(charge_seed, hit_seed)
             phi_bar = edge_field_adjoint(self.arrays, fx_bar, fy_bar, self.extrapolation)
-            z.zero_()
             self.transposed.solve_device(z, self.eps0 * phi_bar, linear_tolerance=1e-12)
-            new = z / self.eps0
-            scale = float(new.abs().max())
-            change = float((new - lam).abs().max()) / scale if scale > 0 else 0.0
-            lam = new
+            image = z / self.eps0
+            scale = float(image.abs().max())
+            change = float((image - lam).abs().max()) / scale if scale > 0 else 0.0
             if change <= tolerance:
+                lam = image
                 break
+            lam = mixer.update(lam, image) if mixer is not None else image
+        # phi_bar and z are those of the last evaluation, whose input is within the
+        # tolerance of the fixed point
         return FixedPointAdjoint(lam, phi_bar, z, iteration, change)
 
     def parameter_gradient(self, adjoint: FixedPointAdjoint, current: float) -> np.ndarray:
@@ -240,8 +248,8 @@ class LensProblem:
     """An einzel design whose plate voltages and beam current are parameters: ``solve``
     converges it for a parameter vector ``(V_1, V_2, V_3, I)``, ``gradient`` reverses it."""
 
-    def __init__(self, design, plane: float = 79e-3, tolerance: float = 1e-7,
-                 iterations: int = 60, adjoint_tolerance: float = 1e-10) -> None:  # fmt: skip
+    def __init__(self, design, plane: float = 79e-3, tolerance: float = 1e-6,
+                 iterations: int = 60, adjoint_tolerance: float = 1e-8) -> None:  # fmt: skip
         self.design = design
         self.plane = float(plane)
         self.tolerance = float(tolerance)
@@ -318,11 +326,13 @@ class LensMoments:
         return cls.function().apply(params, problem)
 
 
-def adjoint_design_gradient(design, plane: float = 79e-3, tolerance: float = 1e-7,
-                            iterations: int = 60, adjoint_tolerance: float = 1e-10) -> dict:  # fmt: skip
+def adjoint_design_gradient(design, plane: float = 79e-3, tolerance: float = 1e-6,
+                            iterations: int = 60, adjoint_tolerance: float = 1e-8) -> dict:  # fmt: skip
     """The gradients of the rms angle and the current at ``plane`` with respect to the three
     plate voltages and the beam current (`GRADIENT_PARAMETERS`) by the adjoint of one
-    converged solve, through ``torch.autograd``."""
+    solve converged to ``tolerance`` [V] (the gradient is linearised there: unlike central
+    differences, which divide the solves' error by the step, it needs no tighter solve),
+    through ``torch.autograd``."""
     import torch
 
     from beamtracer_b200.einzel import resolved_voltages

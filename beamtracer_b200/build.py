@@ -2,7 +2,8 @@
 
 ``python -m beamtracer_b200.build`` compiles every ``csrc/*.cu`` with nvcc into
 ``beamtracer_b200/libbt200.so``.  No multiply-add is contracted (``--fmad=false``): the
-kernels round exactly as their expressions are written, as the reference's CPU kernels do.
+kernels round exactly as their expressions are written, as the reference's CPU kernels do
+-- except ``trace_fast.cu``, the tracer built again with contracted multiply-adds.
 """
 
 from __future__ import annotations
@@ -19,10 +20,10 @@ LIBRARY = HERE / "libbt200.so"
 INCLUDE = HERE.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = [
-    "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
-    "-Xptxas", "-warn-spills", "-shared",
-]  # fmt: skip
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]
+#: Sources built with contracted multiply-adds (every other one rounds as it is written).
+CONTRACTED = {"trace_fast.cu"}
+OBJECTS = HERE / "_build"
 
 
 def sources() -> list[Path]:
@@ -46,19 +47,36 @@ def nvcc() -> str:
     return found
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile the library if it is missing or older than its sources; return its path."""
-    if not force and not _stale():
-        return LIBRARY
-    tmp = LIBRARY.with_suffix(f".so.tmp{os.getpid()}")
-    command = [nvcc(), *ARCH, *FLAGS, f"-I{INCLUDE}", *map(str, sources()), "-o", str(tmp)]
+def _compile(source: Path, verbose: bool) -> Path:
+    fmad = "--fmad=true" if source.name in CONTRACTED else "--fmad=false"
+    out = OBJECTS / (source.stem + ".o")
+    command = [nvcc(), *ARCH, *COMMON, fmad, f"-I{INCLUDE}", "-c", str(source), "-o", str(out)]
     if verbose:
         command.insert(1, "-Xptxas=-v")
     result = subprocess.run(command, capture_output=True, text=True)
     if result.returncode != 0:
-        raise RuntimeError(f"nvcc failed:\n{result.stdout}\n{result.stderr}")
+        raise RuntimeError(f"nvcc failed on {source.name}:\n{result.stdout}\n{result.stderr}")
     if verbose:
         print(result.stdout, result.stderr, file=sys.stderr)
+    return out
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile the library if it is missing or older than its sources; return its path.
+    Every source is compiled on its own (with its own multiply-add rule), in parallel,
+    then linked."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    if not force and not _stale():
+        return LIBRARY
+    OBJECTS.mkdir(exist_ok=True)
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
+        objects = list(pool.map(lambda src: _compile(src, verbose), sources()))
+    tmp = LIBRARY.with_suffix(f".so.tmp{os.getpid()}")
+    command = [nvcc(), *ARCH, "-shared", *map(str, objects), "-o", str(tmp)]
+    result = subprocess.run(command, capture_output=True, text=True)
+    if result.returncode != 0:
+        raise RuntimeError(f"nvcc failed to link:\n{result.stdout}\n{result.stderr}")
     os.replace(tmp, LIBRARY)
     return LIBRARY
 

@@ -29,7 +29,9 @@ namespace {
 
 constexpr int kSegment = 64;   // steps between checkpoints
 constexpr int kMaxPlanes = 8;  // plane crossings the sweep follows
-constexpr int kAdjThreads = 128;
+// One warp a block: a solve's few thousand trajectories spread over every SM (128-thread
+// blocks left most of the 148 SMs idle on 8,000 trajectories).
+constexpr int kAdjThreads = 32;
 
 struct Grid {
     const double *fx, *fy;

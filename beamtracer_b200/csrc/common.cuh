@@ -146,6 +146,7 @@ struct bt_ctx {
     bt::Buffer reduce_partial;  // per-block partial results of the device reductions
     bt::Buffer kept_records;    // (device i64) records the deposits reduced while timing
     bt::Buffer anderson;        // the Anderson mixer's sums, R, Q^T f and gamma
+    bt::Buffer measure;         // the FP64 peak measurement's output
     i64 launch_count = 0;       // kernels launched on the context since its creation
     i64 last_windows = 0, last_records = 0, last_flushes = 0;
 };

@@ -954,18 +954,30 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
 }  // namespace
 }  // namespace bt
 
-extern "C" int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, int64_t window) {
+// trace_fast.cu compiles this file again with contracted multiply-adds; its entry points
+// carry the suffix _fast.
+#ifdef BT_TRACE_FAST
+#define BT_TRACE_ENTRY(name) name##_fast
+#else
+#define BT_TRACE_ENTRY(name) name
+#endif
+
+extern "C" int BT_TRACE_ENTRY(bt_trace_trajectories_2d)(bt_ctx *ctx, const bt_trace_args *args,
+                                                        int64_t window) {
     return bt::guarded([&] { bt::trace_all(ctx, args, nullptr, window); });
 }
 
-extern "C" int bt_trace_trajectories_2d_magnetic(bt_ctx *ctx, const bt_trace_args *args,
-                                                 const bt_magnetic *magnetic, int64_t window) {
+extern "C" int BT_TRACE_ENTRY(bt_trace_trajectories_2d_magnetic)(bt_ctx *ctx,
+                                                                 const bt_trace_args *args,
+                                                                 const bt_magnetic *magnetic,
+                                                                 int64_t window) {
     return bt::guarded([&] {
         BT_REQUIRE(magnetic, "trace: null magnetic field");
         bt::trace_all(ctx, args, magnetic, window);
     });
 }
 
+#ifndef BT_TRACE_FAST
 extern "C" int bt_trace_last_stats(bt_ctx *ctx, int64_t *windows, int64_t *records,
                                    int64_t *deposit_flushes) {
     return bt::guarded([&] {
@@ -975,3 +987,4 @@ extern "C" int bt_trace_last_stats(bt_ctx *ctx, int64_t *windows, int64_t *recor
         if (deposit_flushes) *deposit_flushes = ctx->last_flushes;
     });
 }
+#endif

@@ -154,7 +154,10 @@ class BeamOptics:
     Config = BeamOpticsConfig
 
     def __init__(self, config: BeamOpticsConfig | None = None, /, *, comm: Any = None,
-                 verbose: bool = False, **settings: object) -> None:  # fmt: skip
+                 verbose: bool = False, contracted_trace: bool = False,
+                 **settings: object) -> None:  # fmt: skip
+        """``contracted_trace``: trace with the build whose multiply-adds are fused (results
+        agree with the default build to rounding instead of bit for bit)."""
         if config is None:
             config = BeamOpticsConfig(**settings)  # type: ignore[arg-type]
         else:
@@ -180,6 +183,7 @@ class BeamOptics:
             integrator=config.integrator,
             relativistic=config.relativistic, max_steps=config.max_steps,
             planes=config.diagnostic_planes, save_trajectories=config.save_trajectories,
+            contracted=contracted_trace,
         )  # fmt: skip
 
     def _particles(self) -> tuple[BeamParticles, float]:

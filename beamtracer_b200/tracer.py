@@ -360,12 +360,16 @@ class TraceEngine:
         capacity: tuple[int, int] = (4, 1024),
         window: int = 64,
         magnetic: Any = None,
+        contracted: bool = False,
     ) -> None:
         import torch
 
         from beamtracer_b200 import _lib
 
         self.torch = torch
+        #: trace with the build whose multiply-adds are fused (rounding-level agreement
+        #: with the exact build instead of bit-exact)
+        self.contracted = bool(contracted)
         self.mesh = mesh
         self.planes = tuple(float(p) for p in planes)
         self.integrator = integrator
@@ -487,12 +491,15 @@ class TraceEngine:
             int(mesh.graded), d(self.x_nodes), int(self.x_nodes.numel()), self.inv_c2,
         )  # fmt: skip
         lib, ctx = _lib.lib(), _lib.context()
+        fast = self.contracted
         if self.magnetic is None:
-            _lib.check(lib.bt_trace_trajectories_2d(ctx.handle, ctypes.byref(a), self.window))
+            entry = lib.bt_trace_trajectories_2d_fast if fast else lib.bt_trace_trajectories_2d
+            _lib.check(entry(ctx.handle, ctypes.byref(a), self.window))
         else:
             m = self.magnetic.descriptor()
-            _lib.check(lib.bt_trace_trajectories_2d_magnetic(ctx.handle, ctypes.byref(a),
-                                                             ctypes.byref(m), self.window))  # fmt: skip
+            entry = (lib.bt_trace_trajectories_2d_magnetic_fast if fast
+                     else lib.bt_trace_trajectories_2d_magnetic)  # fmt: skip
+            _lib.check(entry(ctx.handle, ctypes.byref(a), ctypes.byref(m), self.window))
 
     def run(self, fx, fy) -> None:
         """Trace the loaded beam through the edge fields (device arrays)."""
@@ -620,6 +627,7 @@ class BeamTracer:
         relativistic: bool = False,
         speed_of_light: float = constants.c,
         window: int = 64,
+        contracted: bool = False,
     ) -> None:
         if not 0.0 < step_fraction <= 1.0:
             raise ValueError(f"step_fraction must be in (0, 1], got {step_fraction}")
@@ -654,6 +662,8 @@ class BeamTracer:
         self.speed_of_light = float(speed_of_light)
         self.compiled = compiled
         self.window = int(window)
+        #: the build of the trace with fused multiply-adds (`TraceEngine`)
+        self.contracted = bool(contracted)
         self._capacity = (4, 1024)
         #: Sums the node charges over ranks (set by a distributed run), or None.
         self.reduce = None
@@ -670,7 +680,9 @@ class BeamTracer:
                 inv_c2=self._inv_c2(), save_trajectories=self.save_trajectories,
                 capacity=self._capacity, window=self.window,
                 magnetic=None if self.magnetic is None else self.magnetic.profile(),
+                contracted=self.contracted,
             )  # fmt: skip
+        self._engine.contracted = self.contracted
         return self._engine
 
     def trace(self, particles: BeamParticles) -> TraceResult:

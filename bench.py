@@ -155,7 +155,7 @@ def run_profile(args) -> None:
 
     torch.cuda.set_device(0)
     config = build_workload(2, small=args.small)
-    model = BeamOptics(config)
+    model = BeamOptics(config, contracted_trace=args.trace == "contracted")
     model.tracer.window = args.window
     poisson = IonOpticsPoisson(model.mesh, backend=config.field_backend)
 
@@ -398,6 +398,11 @@ def run_design(args, rank: int, world: int, local: int) -> None:
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    from beamtracer_b200 import _lib
+
+    ctx = _lib.context()
+    ctx.set_timing(True)
+    ctx.reset_timers()
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]  # fmt: skip
     with ClockSampler(local) as clocks:
@@ -407,6 +412,13 @@ def run_design(args, rank: int, world: int, local: int) -> None:
             events[k][1].record(stream)
         torch.cuda.synchronize()
     total_ms = float(sum(a.elapsed_time(b) for a, b in events))
+    # the calling thread's context times the launches it queued (the concurrent sweep's
+    # worker threads have their own)
+    kernels = {name: {"ms": ms, "launches": n} for name, (ms, n) in
+               ((name, ctx.read_timer(name)) for name in
+                ("trace_window", "deposit", "field_solve", "vcycle", "hierarchy",
+                 "adjoint_checkpoints", "adjoint_sweep")) if n}  # fmt: skip
+    ctx.set_timing(False)
     if world > 1:
         t = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -424,7 +436,7 @@ def run_design(args, rank: int, world: int, local: int) -> None:
         "config": {"workload": workload,
                    "share_of_rank0": len(share_of_designs(designs, 0, world))
                    if args.workload == "sweep" else None},
-        "clocks": clocks.summary(),
+        "clocks": clocks.summary(), "kernels": kernels,
     }  # fmt: skip
     if args.workload == "gradient":
         line["gradient"] = {k: [float(v) for v in result[k]] for k in ("rms_angle", "current")}
@@ -446,6 +458,9 @@ def main() -> None:
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--window", type=int, default=64)
+    parser.add_argument("--trace", default="exact", choices=["exact", "contracted"],
+                        help="the trace's build: multiply-adds as written (bit-exact with the "
+                             "oracle) or contracted into fused multiply-adds")
     parser.add_argument("--profile", action="store_true",
                         help="one warm solve, then one in the NVTX range 'profiled_solve'")
     parser.add_argument("--small", action="store_true",
@@ -490,7 +505,8 @@ def main() -> None:
     from beamtracer_b200.vlasov import vlasov_iterate
 
     config = build_workload(2 + rank)
-    model = BeamOptics(config)
+    contracted = args.trace == "contracted"
+    model = BeamOptics(config, contracted_trace=contracted)
     model.tracer.window = args.window
     from beamtracer_b200.poisson import IonOpticsPoisson
 
@@ -547,10 +563,12 @@ def main() -> None:
                for name, (ms, n) in timers.items()}  # fmt: skip
     trace_ms, trace_launches = timers["trace_window"]
     flops = FLOPS_PER_RK4_STEP * steps_total
+    fp64_peak = ctx.fp64_peak()
     fp64 = {"bound": "fp64", "achieved": flops / (trace_ms / 1e3) / 1e12 if trace_ms else None,
-            "peak": NOMINAL_FP64_TFLOPS, "unit": "TFLOP/s",
-            "frac": (flops / (trace_ms / 1e3) / 1e12) / NOMINAL_FP64_TFLOPS if trace_ms else None,
-            "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)",
+            "peak": fp64_peak, "unit": "TFLOP/s",
+            "frac": (flops / (trace_ms / 1e3) / 1e12) / fp64_peak if trace_ms else None,
+            "peak_source": "measured here: independent DFMA chains on every SM, CUDA events "
+                           f"(nominal {NOMINAL_FP64_TFLOPS} TFLOP/s)",
             "kernel": "trace_window", "flops_per_step": FLOPS_PER_RK4_STEP,
             "steps_per_launch": steps_total / max(trace_launches, 1)}  # fmt: skip
     peaks = _peaks()
@@ -586,7 +604,7 @@ def main() -> None:
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         start.record(stream)
-        m = BeamOptics(config)
+        m = BeamOptics(config, contracted_trace=contracted)
         m.run()
         moments = {f"{x * 1e3:g}mm": m.beam_moments(x) for x in config.diagnostic_planes}
         stop.record(stream)
@@ -622,7 +640,7 @@ def main() -> None:
         "config": workload_config(),
         "solve": {"iterations_per_solve": len(history),
                   "vcycles_per_solve": sum(h["krylov_steps"] for h in history),
-                  "window": args.window},
+                  "window": args.window, "trace_build": args.trace},
         "roofline": hbm, "roofline_fp64": fp64, "roofline_deposit": deposit,
         "kernels": kernels,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),

@@ -61,6 +61,10 @@ int bt_ctx_reset_timers(bt_ctx *ctx);
  * the algorithmic bytes of the deposit are counted per record.  No counterpart in the
  * reference. */
 int bt_ctx_deposit_records(bt_ctx *ctx, int64_t *records);
+/* No counterpart in the reference.  The FP64 pipe's peak on the context's device
+ * (TFLOP/s, a fused multiply-add two operations): independent FMA chains on every SM, the
+ * fastest of three timed launches (CUDA events on the context's stream). */
+int bt_measure_fp64_peak(bt_ctx *ctx, double *tflops);
 /* The number of kernels the context has launched since its creation (host out-param). */
 int bt_ctx_launch_count(bt_ctx *ctx, int64_t *count);
 /* Copy the calling thread's last error message into buf (NUL-terminated); returns its length. */
@@ -153,6 +157,12 @@ typedef struct bt_trace_args {
  * window's deposit records are sorted by cell and reduced in a fixed order. */
 int bt_trace_trajectories_2d(bt_ctx *ctx, const bt_trace_args *args, int64_t window);
 
+/* No counterpart in the reference.  bt_trace_trajectories_2d built with contracted
+ * multiply-adds: the same step with every a * b + c one fused multiply-add rounded once,
+ * so results agree with the exact build to rounding (not bit for bit) in fewer dependent
+ * FP64 instructions.  bt_trace_trajectories_2d_magnetic_fast likewise. */
+int bt_trace_trajectories_2d_fast(bt_ctx *ctx, const bt_trace_args *args, int64_t window);
+
 /* An axisymmetric magnetic field from its on-axis profile (solver/fields.py:192-279,
  * AxisymmetricMagneticField): samples (DEVICE, n rows of order + 1) hold d^k B_z / dz^k,
  * k = 0..order, at z0 + hz i (fields.py:236-243); between samples they are interpolated
@@ -176,6 +186,8 @@ typedef struct bt_magnetic {
  * (tracer.py:1019-1024).  Non-relativistic (inv_c2 = 0), one patch, no symmetry plane. */
 int bt_trace_trajectories_2d_magnetic(bt_ctx *ctx, const bt_trace_args *args,
                                       const bt_magnetic *magnetic, int64_t window);
+int bt_trace_trajectories_2d_magnetic_fast(bt_ctx *ctx, const bt_trace_args *args,
+                                           const bt_magnetic *magnetic, int64_t window);
 
 /* Counters of the last bt_trace_trajectories_2d call on this context (host out-params). */
 int bt_trace_last_stats(bt_ctx *ctx, int64_t *windows, int64_t *records,

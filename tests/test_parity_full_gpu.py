@@ -5,6 +5,8 @@
   size, rms angle and emittance at 70 and 79 mm within 1e-6 of the oracle's converged
   solve (relative), and, stage-wise, the density the beam deposits in the oracle's
   converged potential within 1e-10 of its largest value.
+- The contracted-multiply-add build of the trace on the same lens: its stage-wise density
+  within 1e-10 of the exact build's, its converged solve within 1e-6 of the oracle's.
 - The planar plasma + solenoid extraction at 1025 x 513 with 100,000 trajectories: the
   first iteration's potential against the oracle's, and the stage-wise density in the
   device's second (Newton) potential within 1e-10.
@@ -82,6 +84,32 @@ def test_lens_density_stagewise(lens):
     np.testing.assert_array_equal(result.status, trace_o.status.astype(np.int8))
     np.testing.assert_allclose(result.charge_density, rho_o, rtol=0,
                                atol=1e-10 * np.abs(rho_o).max())  # fmt: skip
+
+
+def test_contracted_trace_matches_at_full_size(lens):
+    """The trace with fused multiply-adds (the benchmark's build): stage-wise against the
+    exact build, and converged against the oracle, at the bounds of the exact build."""
+    from beamtracer_b200.fields import StaggeredElectricField
+    from beamtracer_b200.model import BeamOptics
+
+    config, model, problem, particles, oracle = lens
+    phi = oracle["potential"]
+    model.tracer.electric = StaggeredElectricField(model.mesh, phi)
+    want = model.tracer.trace(particles)
+    fast = BeamOptics(config, contracted_trace=True)
+    fast.tracer.electric = StaggeredElectricField(fast.mesh, phi)
+    got = fast.tracer.trace(particles)
+    assert (got.status == want.status).mean() > 0.999
+    np.testing.assert_allclose(got.charge_density, want.charge_density, rtol=0,
+                               atol=1e-10 * np.abs(want.charge_density).max())  # fmt: skip
+    solved = BeamOptics(config, contracted_trace=True).run()
+    ref = oracle["potential"]
+    assert np.max(np.abs(solved.potential - ref)) / np.max(np.abs(ref)) <= 1e-6
+    ora = _oracle_moments(problem, oracle, particles, model.species_mass)
+    for x in config.diagnostic_planes:
+        gpu = solved.beam_moments(x)
+        for name in MOMENTS:
+            assert getattr(gpu, name) == pytest.approx(getattr(ora[x], name), rel=1e-6), (x, name)
 
 
 def test_solenoid_extraction_full_size_stagewise():
