@@ -259,6 +259,8 @@ class LensProblem:
         self.adjoint_iterations = 0
         #: whether the last forward solve met its tolerance
         self.converged = False
+        #: the largest |E| on every electrode's surface in the last forward solve [V/m]
+        self.surface_fields: dict[str, float] = {}
 
     def config(self, params: np.ndarray):
         from beamtracer_b200.einzel import einzel_config
@@ -293,6 +295,7 @@ class LensMoments:
                 values = params.detach().cpu().numpy().astype(np.float64)
                 model = problem.solve(values)
                 problem.converged = bool(model.stats["converged"])
+                problem.surface_fields = model.surface_fields()
                 hits = model.plane(problem.plane)
                 ctx.problem, ctx.model, ctx.values = problem, model, values
                 ctx.hits_current = np.array(hits.current, dtype=np.float64)
@@ -347,4 +350,4 @@ def adjoint_design_gradient(design, plane: float = 79e-3, tolerance: float = 1e-
     return {"rms_angle": angle.numpy().copy(), "current": transmitted.numpy().copy(),
             "moments": {k: float(v.detach()) for k, v in moments.items()}, "solves": 1,
             "adjoint_iterations": problem.adjoint_iterations,
-            "converged": problem.converged}  # fmt: skip
+            "converged": problem.converged, "surface_fields": dict(problem.surface_fields)}  # fmt: skip

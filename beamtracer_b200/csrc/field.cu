@@ -168,3 +168,70 @@ extern "C" int bt_edge_field_adjoint(bt_ctx *ctx, const double *fx_bar, const do
         BT_CHECK_LAUNCH();
     });
 }
+
+// -- the surface field (solver/fields.py:324-377) --------------------------------------------
+
+namespace bt {
+namespace {
+
+// One component at a node from its two edges (fields.py:323-338): the edge towards an
+// electrode neighbour (the field at the surface), the larger of the two with electrodes on
+// both sides, else their mean.
+__device__ __forceinline__ double node_component(double low, double high, bool solid_low,
+                                                 bool solid_high) {
+    if (solid_low && solid_high) return fabs(low) >= fabs(high) ? low : high;
+    if (solid_low) return low;
+    if (solid_high) return high;
+    return 0.5 * (low + high);
+}
+
+// |E| at every free node next to an electrode (NaN elsewhere) and that electrode (the first
+// of the -x, +x, -y, +y neighbours that is one; -1 elsewhere); the largest |E| of each
+// electrode by an atomic maximum on the bits of the non-negative doubles (order-free).
+__global__ void surface_field(const double *__restrict__ fx, const double *__restrict__ fy,
+                              const int32_t *__restrict__ solid, const uint8_t *__restrict__ near,
+                              i64 nx, i64 ny, int n_electrodes, double *__restrict__ magnitude,
+                              int32_t *__restrict__ electrode,
+                              unsigned long long *__restrict__ largest) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nx * ny) return;
+    const i64 i = t / ny, j = t - i * ny;
+    const int32_t nb[4] = {i > 0 ? solid[t - ny] : -1, i < nx - 1 ? solid[t + ny] : -1,
+                           j > 0 ? solid[t - 1] : -1, j < ny - 1 ? solid[t + 1] : -1};
+    if (!near[t]) {
+        magnitude[t] = __longlong_as_double(0x7ff8000000000000LL);  // a quiet NaN
+        electrode[t] = -1;
+        return;
+    }
+    const double ex = node_component(fx[t], fx[t + ny], nb[0] >= 0, nb[1] >= 0);
+    const double ey = node_component(fy[i * (ny + 1) + j], fy[i * (ny + 1) + j + 1], nb[2] >= 0,
+                                     nb[3] >= 0);
+    const double m = hypot(ex, ey);
+    int32_t e = -1;
+    for (int q = 0; q < 4 && e < 0; ++q) e = nb[q];
+    magnitude[t] = m;
+    electrode[t] = e;
+    if (largest && e >= 0 && e < n_electrodes && m == m)
+        atomicMax(largest + e, (unsigned long long)__double_as_longlong(m));
+}
+
+}  // namespace
+}  // namespace bt
+
+extern "C" int bt_surface_field(bt_ctx *ctx, const double *fx, const double *fy,
+                                const int32_t *solid, const uint8_t *near, int64_t nx, int64_t ny,
+                                int32_t n_electrodes, double *magnitude, int32_t *electrode,
+                                double *largest) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx && fx && fy && solid && near && magnitude && electrode,
+                   "surface field: null argument");
+        BT_REQUIRE(nx >= 2 && ny >= 2, "surface field: the mesh needs at least 2 nodes per axis");
+        BT_REQUIRE(n_electrodes >= 0, "surface field: negative electrode count");
+        if (largest && n_electrodes > 0)
+            BT_CUDA(cudaMemsetAsync(largest, 0, sizeof(double) * n_electrodes, ctx->stream));
+        BT_LAUNCH(ctx, bt::surface_field, bt::blocks_for(nx * ny, 256), 256, 0, ctx->stream, fx,
+                  fy, solid, near, nx, ny, n_electrodes, magnitude, electrode,
+                  reinterpret_cast<unsigned long long *>(largest));
+        BT_CHECK_LAUNCH();
+    });
+}

@@ -115,6 +115,38 @@ class StaggeredElectricField:
         return ex.cpu().numpy(), ey.cpu().numpy()
 
 
+def surface_field_device(mesh: IonOpticsMesh, field: StaggeredElectricField,
+                         arrays: MeshArrays | None = None):
+    """``(magnitude, electrode, largest)`` on the device: |E| at the free nodes next to an
+    electrode (NaN elsewhere), that electrode (-1 elsewhere) and every electrode's largest
+    |E| (``bt_surface_field``)."""
+    import torch
+
+    arrays = arrays or MeshArrays(mesh)
+    nx, ny = mesh.shape
+    magnitude = torch.empty((nx, ny), dtype=torch.float64, device="cuda")
+    electrode = torch.empty((nx, ny), dtype=torch.int32, device="cuda")
+    count = len(mesh.electrodes)
+    largest = torch.zeros(max(count, 1), dtype=torch.float64, device="cuda")
+    ctx = _lib.context()
+    _lib.check(_lib.lib().bt_surface_field(
+        ctx.handle, _lib.dptr(field.fx_device), _lib.dptr(field.fy_device),
+        _lib.dptr(arrays.solid), _lib.dptr(arrays.near), nx, ny, count, _lib.dptr(magnitude),
+        _lib.dptr(electrode), _lib.dptr(largest)))  # fmt: skip
+    return magnitude, electrode, largest[:count]
+
+
+def surface_field(mesh: IonOpticsMesh, field: StaggeredElectricField
+                  ) -> tuple[np.ndarray, np.ndarray]:  # fmt: skip
+    """|E| [V/m] at the free nodes next to an electrode and that electrode, both of the
+    mesh's shape (NaN and -1 elsewhere): the interface of ``fields.py:324-377``, computed
+    on the device.  The component along an axis with an electrode neighbour is the edge
+    towards it, taken over the bracketed distance to the surface (the field at the
+    surface).  At a sharp corner the field is singular and grows as the mesh is refined."""
+    magnitude, electrode, _ = surface_field_device(mesh, field)
+    return magnitude.cpu().numpy(), electrode.cpu().numpy()
+
+
 def _derivative_weights() -> np.ndarray:
     """(7, 7) weights of the central differences over the samples ``i - 3 .. i + 3``: row
     ``k`` gives ``h^k d^k B / dz^k`` -- orders 6, 6, 4, 4, 2, 2 for ``k = 1 .. 6`` (the widest

@@ -254,6 +254,16 @@ class BeamOptics:
             return np.zeros(self.mesh.shape)
         return self.state.charge_density
 
+    def surface_fields(self) -> dict[str, float]:
+        """The largest |E| [V/m] on the surface of every electrode, by name (the interface
+        of ``model.py:591-606``): from the solved potential at the free nodes next to each
+        electrode (`surface_field`), 0 for an electrode with no free neighbour."""
+        from beamtracer_b200.fields import surface_field_device
+
+        _, _, largest = surface_field_device(self.mesh, self.state.electric)
+        values = largest.cpu().numpy()
+        return {name: float(values[k]) for k, name in enumerate(self.config.objects)}
+
     def electric_field_at(self, x, y):
         return self.state.electric(x, y)
 

@@ -307,11 +307,14 @@ class _Budget(Exception):
 
 
 def einzel_evaluator(base, names: Sequence[str] = ("v_mid",), plane: float = 79e-3,
-                     tolerance: float = 1e-7, iterations: int = 60):  # fmt: skip
+                     tolerance: float = 1e-6, iterations: int = 60,
+                     field_limit: float | None = None):  # fmt: skip
     """An evaluation function of an einzel design for `lbfgs_search`: the rms angle and
     the current at ``plane`` of the lens with the named parameters set (``v_mid`` the middle
     plate, ``v1``-``v3`` the plates, ``current`` the beam current), and the gradient of the
-    rms angle with respect to them from the adjoint of the converged solve."""
+    rms angle with respect to them from the adjoint of the converged solve.  The largest
+    surface field [V/m] is a diagnostic and, with ``field_limit``, the constraint
+    ``field / field_limit - 1`` (the reference's einzel constraint, ``einzel.py:348``)."""
     from beamtracer_b200.adjoint import adjoint_design_gradient
     from beamtracer_b200.einzel import GRADIENT_PARAMETERS, resolved_voltages
 
@@ -329,11 +332,14 @@ def einzel_evaluator(base, names: Sequence[str] = ("v_mid",), plane: float = 79e
         grad = adjoint_design_gradient(design, plane, tolerance=tolerance, iterations=iterations)
         moments = grad["moments"]
         angle = grad["rms_angle"]
+        field = max(grad["surface_fields"].values(), default=0.0)
+        constraints = {} if field_limit is None else {"surface_field": field / field_limit - 1.0}
         return Evaluation(
             objectives={"rms_angle": moments["rms_angle"], "current": -moments["current"]},
-            converged=grad["converged"],
+            constraints=constraints, converged=grad["converged"],
             diagnostics={"gradient": {name: float(angle[columns[name]]) for name in values},
                          "emittance": moments["emittance"], "rms_size": moments["rms_size"],
+                         "field": field,
                          "adjoint_iterations": grad["adjoint_iterations"],
                          "parameters_order": list(GRADIENT_PARAMETERS)},
         )  # fmt: skip

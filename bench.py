@@ -144,6 +144,25 @@ def build_workload(seed: int, small: bool = False):
     return einzel_config(EinzelDesign(seed=seed))
 
 
+def run_profile_adjoint(args) -> None:
+    """One adjoint gradient of the lens at 401 x 101 with 2,000 rings to warm up, then one
+    inside the NVTX range "profiled_adjoint" (the range a profiler's capture selects)."""
+    import torch
+
+    from beamtracer_b200.adjoint import adjoint_design_gradient
+    from beamtracer_b200.einzel import EinzelDesign
+
+    torch.cuda.set_device(0)
+    design = EinzelDesign(shape=(401, 101), trajectories=2000, seed=2)
+    adjoint_design_gradient(design)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("profiled_adjoint")
+    out = adjoint_design_gradient(design)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile": "adjoint", "iterations": out["adjoint_iterations"]}))
+
+
 def run_profile(args) -> None:
     """One converged solve to warm up, then one inside the NVTX range "profiled_solve"
     (the range a profiler's capture selects)."""
@@ -254,6 +273,47 @@ def run_reference(args, rank: int) -> None:
         "moments": runs[-1][2],
     }  # fmt: skip
     print(json.dumps(line), flush=True)
+
+
+def design_measurements(stream) -> dict:
+    """The metric's design half, measured in the default run: gradient evaluations per
+    second of the lens at 401 x 101 with 8,000 rings by the adjoint of one solve and by the
+    plain form (central differences of 8 solves, 8 at once), and candidates per second of
+    16 seeded sweep candidates solved one at a time and 8 at once on their own streams.
+    Device time with CUDA events on the launching stream; one untimed call first."""
+    import torch
+
+    from beamtracer_b200.adjoint import adjoint_design_gradient
+    from beamtracer_b200.einzel import EinzelDesign, design_gradient, sweep, sweep_designs
+
+    def timed(fn, repeats: int) -> tuple[float, object]:
+        fn()
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(repeats):
+            out = fn()
+        stop.record(stream)
+        torch.cuda.synchronize()
+        return start.elapsed_time(stop) / repeats, out
+
+    c4 = EinzelDesign(shape=(401, 101), trajectories=8000, seed=2)
+    adj_ms, adj = timed(lambda: adjoint_design_gradient(c4), 3)
+    fd_ms, fd = timed(lambda: design_gradient(c4, concurrency=8), 3)
+    diff = float(np.max(np.abs(adj["rms_angle"] - fd["rms_angle"])) / np.max(np.abs(fd["rms_angle"])))
+    designs = sweep_designs(16)
+    one_ms, _ = timed(lambda: sweep(designs, concurrency=1), 1)
+    many_ms, _ = timed(lambda: sweep(designs, concurrency=8), 1)
+    return {
+        "gradient": {"workload": "einzel 401x101, 8,000 rings, d(rms angle, current)/d(V1, V2, "
+                                 "V3, I) at 79 mm", "unit": "gradient evals/s",
+                     "adjoint": 1e3 / adj_ms, "plain_form": 1e3 / fd_ms,
+                     "speedup_over_plain": fd_ms / adj_ms, "max_rel_diff": diff,
+                     "adjoint_iterations": adj["adjoint_iterations"]},
+        "sweep": {"workload": "16 seeded einzel candidates (257x65..1025x257, 2k-20k rings)",
+                  "unit": "candidates/s", "concurrent_8_streams": 16e3 / many_ms,
+                  "one_at_a_time": 16e3 / one_ms, "speedup_over_plain": one_ms / many_ms},
+    }  # fmt: skip
 
 
 def run_plasma(args) -> None:
@@ -457,6 +517,8 @@ def main() -> None:
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-design", action="store_true",
+                        help="leave out the design measurements of the default run")
     parser.add_argument("--window", type=int, default=64)
     parser.add_argument("--trace", default="exact", choices=["exact", "contracted"],
                         help="the trace's build: multiply-adds as written (bit-exact with the "
@@ -465,6 +527,9 @@ def main() -> None:
                         help="one warm solve, then one in the NVTX range 'profiled_solve'")
     parser.add_argument("--small", action="store_true",
                         help="with --profile: the lens at 401 x 101 with 2,000 rings")
+    parser.add_argument("--profile-adjoint", action="store_true",
+                        help="one warm adjoint gradient, then one in the NVTX range "
+                             "'profiled_adjoint' (401 x 101, 2,000 rings)")
     parser.add_argument("--workload", default="einzel",
                         choices=["einzel", "plasma", "gradient", "sweep"],
                         help="plasma: the planar plasma + solenoid extraction (one GPU); "
@@ -474,6 +539,9 @@ def main() -> None:
     parser.add_argument("--concurrency", type=int, default=8,
                         help="with --workload sweep or gradient: solves at once per GPU")
     args = parser.parse_args()
+    if args.profile_adjoint:
+        run_profile_adjoint(args)
+        return
     if args.profile:
         run_profile(args)
         return
@@ -622,6 +690,9 @@ def main() -> None:
 
     gpu_moments = {plane: {k: getattr(mo, k) for k in MOMENT_NAMES}
                    for plane, mo in moments.items()}  # fmt: skip
+    design_lines = None
+    if rank == 0 and world == 1 and not args.no_design:
+        design_lines = design_measurements(stream)
     cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import kernels as oracle_kernels
@@ -651,6 +722,7 @@ def main() -> None:
         "cpu_baseline": cpu,
         "moments": gpu_moments,
         "parity": parity,
+        "design": design_lines,
     }  # fmt: skip
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -239,6 +239,17 @@ int bt_edge_field(bt_ctx *ctx, const double *phi, const int32_t *solid, const ui
                   const double *distance, const double *dx, int64_t nx, int64_t ny,
                   double h, const int32_t extrapolation[4], double *fx, double *fy);
 
+/* solver/fields.py:324-377 (surface_field).  At every free node next to an electrode
+ * (near (nx, ny) uint8), |E| (magnitude, (nx, ny)) from its two edge fields along each
+ * axis -- the edge towards an electrode neighbour (the field at the surface), the larger of
+ * the two with electrodes on both sides, else their mean -- and that electrode (electrode,
+ * (nx, ny) int32: the first of the -x, +x, -y, +y neighbours that is solid); NaN and -1
+ * elsewhere.  largest (n_electrodes, or NULL): each electrode's largest |E| (0 for one with
+ * no free neighbour).  All arrays on the DEVICE. */
+int bt_surface_field(bt_ctx *ctx, const double *fx, const double *fy, const int32_t *solid,
+                     const uint8_t *near, int64_t nx, int64_t ny, int32_t n_electrodes,
+                     double *magnitude, int32_t *electrode, double *largest);
+
 /* The transpose of bt_edge_field (no counterpart in the reference; the differentiation
  * form): phi_bar (nx, ny) = D^T (fx_bar, fy_bar), D the linear map from the potential to
  * the edge fields that bt_edge_field applies on the same mesh arrays.  One thread a node,

@@ -74,3 +74,29 @@ def edge_fields(phi, solid, near, distance, dx, h, extrapolation):
     fy = _line_field(phi.T, is_solid.T, near.T, distance[2].T, distance[3].T, h,
                      extrapolation[2:4]).T  # fmt: skip
     return fx, np.ascontiguousarray(fy)
+
+
+def surface_field(fx, fy, solid, near):
+    """|E| at the free nodes next to an electrode and that electrode (``fields.py:324-377``):
+    per axis the edge towards the solid neighbour, the larger with both solid, else the
+    mean; NaN and -1 away from the electrodes."""
+    solid = np.asarray(solid)
+    nx, ny = solid.shape
+    pad = np.pad(solid, 1, constant_values=-1)
+    neighbours = [pad[0:nx, 1:ny + 1], pad[2:nx + 2, 1:ny + 1], pad[1:nx + 1, 0:ny],
+                  pad[1:nx + 1, 2:ny + 2]]  # fmt: skip
+
+    def component(low, high, solid_low, solid_high):
+        larger = np.where(np.abs(low) >= np.abs(high), low, high)
+        one = np.where(solid_low, low, np.where(solid_high, high, 0.5 * (low + high)))
+        return np.where(solid_low & solid_high, larger, one)
+
+    flags = [n >= 0 for n in neighbours]
+    ex = component(fx[:-1], fx[1:], flags[0], flags[1])
+    ey = component(fy[:, :-1], fy[:, 1:], flags[2], flags[3])
+    near = np.asarray(near, dtype=bool)
+    magnitude = np.where(near, np.hypot(ex, ey), np.nan)
+    electrode = np.full(solid.shape, -1, dtype=np.int32)
+    for n in neighbours:
+        electrode = np.where(electrode < 0, n, electrode)
+    return magnitude, np.where(near, electrode, -1).astype(np.int32)

@@ -96,6 +96,14 @@ def reference_edge_field(root: Path):
     return namespace["_edge_field"]
 
 
+def reference_surface_field(root: Path):
+    """The reference's ``surface_field`` and ``_node_component`` (``solver/fields.py:
+    323-377``), taken out of their module."""
+    namespace = {"np": np, "Any": object}
+    reference_definitions(root, "fields", ("_node_component", "surface_field"), namespace)
+    return namespace["surface_field"]
+
+
 def reference_definitions(root: Path, module: str, names: tuple[str, ...],
                           namespace: dict) -> dict:  # fmt: skip
     """Top-level definitions of a reference module, taken out of its source and run in
@@ -300,6 +308,10 @@ def main() -> None:
             edge_field(phi.T, solid.T, near.T, mesh.distance[2].T, mesh.distance[3].T,
                        mesh.h, extrapolation[2:4]).T
         )  # fmt: skip
+        surface = reference_surface_field(root)
+        magnitude, electrode = surface(mesh, types.SimpleNamespace(fx=fx, fy=fy))
+        np.savez_compressed(HERE / f"surface_{name}.npz", magnitude=magnitude,
+                            electrode=electrode)  # fmt: skip
         np.savez_compressed(
             HERE / f"mesh_{name}.npz", solid=mesh.solid, fixed=mesh.fixed,
             fixed_value=mesh.fixed_value, distance=mesh.distance,

@@ -68,3 +68,18 @@ def test_wall_distance_is_bracketed_in_255ths():
     assert mesh.near_solid[5].all() and not mesh.near_solid[4].any()
     assert np.allclose(mesh.distance[1, 5], np.floor(0.3 * 255 + 1) / 255, atol=1 / 255)
     assert (mesh.fixed_value[6:] == 10.0).all()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_surface_field_matches_the_reference(name):
+    """The oracle's restatement of ``surface_field`` (``fields.py:324-377``) against the
+    reference's own on the golden meshes and edge fields."""
+    from oracle.field import surface_field
+
+    mesh = build_mesh(name)
+    golden = np.load(GOLDEN / f"mesh_{name}.npz")
+    want = np.load(GOLDEN / f"surface_{name}.npz")
+    magnitude, electrode = surface_field(golden["fx"], golden["fy"], mesh.solid, mesh.near_solid)
+    np.testing.assert_array_equal(electrode, want["electrode"])
+    np.testing.assert_array_equal(np.isnan(magnitude), np.isnan(want["magnitude"]))
+    np.testing.assert_array_equal(magnitude, want["magnitude"])
