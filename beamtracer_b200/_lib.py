@@ -64,6 +64,12 @@ class TraceArgs(ctypes.Structure):
     ]  # fmt: skip
 
 
+class TraceBatch(ctypes.Structure):
+    """``bt_trace_batch`` of ``include/bt200.h``."""
+
+    _fields_ = [("n_candidates", I64), ("candidate", P), ("cell_offset", P), ("group", I64)]
+
+
 class MagneticDesc(ctypes.Structure):
     """``bt_magnetic`` of ``include/bt200.h``."""
 
@@ -125,6 +131,10 @@ SIGNATURES: dict[str, list] = {
     "bt_trace_trajectories_2d_fast": [P, ctypes.POINTER(TraceArgs), I64],
     "bt_trace_trajectories_2d_magnetic_fast": [P, ctypes.POINTER(TraceArgs),
                                                ctypes.POINTER(MagneticDesc), I64],
+    "bt_trace_trajectories_2d_batch": [P, ctypes.POINTER(TraceArgs),
+                                       ctypes.POINTER(TraceBatch), I64],
+    "bt_trace_trajectories_2d_batch_fast": [P, ctypes.POINTER(TraceArgs),
+                                            ctypes.POINTER(TraceBatch), I64],
     "bt_measure_fp64_peak": [P, ctypes.POINTER(F64)],
     "bt_trace_last_stats": [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64)],
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],

@@ -228,6 +228,8 @@ struct NodeLayout {
     i64 n_patches;
     i64 nx, ny;            // the single patch's shape when patch_int is NULL
     i64 n_nodes;
+    bool ascending = false;  // the patches' node ranges follow one another (a batch of
+                             // candidates): a node's patch is found by bisection
 };
 
 // A record's payload: the charge it adds to the four nodes of its cell, (i, j), (i, j+1),

@@ -320,11 +320,23 @@ __global__ void seg_reduce_chains(const uint32_t *__restrict__ K, i64 R_host,
 // (i-1, j-1): the corners (0,0), (0,1), (1,0), (1,1) of those cells.
 __global__ void node_accumulate(const double4 *__restrict__ cells, double *__restrict__ charge,
                                 const i64 *__restrict__ patch_int, i64 n_patches, i64 nx0,
-                                i64 ny0, i64 n_nodes) {
+                                i64 ny0, i64 n_nodes, int ascending) {
     const i64 node = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= n_nodes) return;
     i64 ny = ny0, offset = 0;
-    if (patch_int) {
+    if (patch_int && ascending) {
+        // the last patch whose first node is at or before this one
+        i64 lo = 0, hi = n_patches - 1;
+        while (lo < hi) {
+            const i64 mid = (lo + hi + 1) / 2;
+            if (__ldg(patch_int + mid * 6 + 5) <= node)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        ny = __ldg(patch_int + lo * 6 + 1);
+        offset = __ldg(patch_int + lo * 6 + 5);
+    } else if (patch_int) {
         for (i64 p = 0; p < n_patches; ++p) {
             const i64 off = patch_int[p * 6 + 5];
             if (node >= off && node < off + patch_int[p * 6 + 4]) {
@@ -492,7 +504,7 @@ void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i
     BT_LAUNCH(ctx, seg_reduce_chains, blocks_for(n_warps, threads), threads, 0, st, sk, n_records,
               n_sorted, cells, first, last, flags, flags + n_warps);
     BT_LAUNCH(ctx, node_accumulate, blocks_for(layout.n_nodes, threads), threads, 0, st, cells, charge, layout.patch_int, layout.n_patches, layout.nx, layout.ny,
-        layout.n_nodes);
+        layout.n_nodes, layout.ascending ? 1 : 0);
     BT_CHECK_LAUNCH();
 }
 
@@ -639,7 +651,7 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
         seg_reduce_chains<<<blocks_for(n_warps, 256), 256, 0, st>>>(
             src_k, n, nullptr, cells, first, last, flags, flags + n_warps);
         node_accumulate<<<blocks_for(n_nodes, 256), 256, 0, st>>>(cells, charge, nullptr, 1, nx,
-                                                                 ny, n_nodes);
+                                                                 ny, n_nodes, 0);
         BT_CHECK_LAUNCH();
     });
 }

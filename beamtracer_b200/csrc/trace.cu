@@ -26,6 +26,11 @@ struct Trace {
     bt_trace_args a;
     i64 nx, ny;       // the last patch's node counts
     bt_magnetic mag;  // the magnetic field of the MAG kernels
+    // A batch of candidate meshes (the BATCH kernels): every trajectory's candidate, and
+    // where each candidate's cell table starts in a.cells.  Row c of a.patch_int /
+    // a.patch_real is candidate c's one patch (shape, offsets, origin, spacing, extent).
+    const int32_t *cand;
+    const i64 *cell_off;
 };
 
 __device__ __forceinline__ i64 node_cell(double x, const double *__restrict__ nodes, i64 n) {
@@ -225,7 +230,7 @@ __device__ __forceinline__ double inv_gamma(double u0, double u1, double u2, dou
 // faster on larger windows and on concurrent solves, whose warps hide each other's latency.
 //
 // One thread's window (m < stride): whether its trajectory is still live afterwards.
-template <int CYL, int INTEG, bool GENERAL, bool MAG>
+template <int CYL, int INTEG, bool GENERAL, bool MAG, bool BATCH>
 __device__ __forceinline__ bool trace_thread(const Trace &tr, const i64 *__restrict__ act,
                                              i64 m, i64 n_act, i64 stride, int S,
                                              uint32_t *__restrict__ keys,
@@ -237,11 +242,18 @@ __device__ __forceinline__ bool trace_thread(const Trace &tr, const i64 *__restr
     const bt_trace_args &a = tr.a;
     const i64 k = act[m];
     const i64 P = GENERAL ? a.n_patches : 1;
-    PatchGeom base = patch_geom(a, 0);  // the one patch of a non-general mesh
+    // the one patch of a non-general mesh (of the trajectory's candidate in a batch)
+    const i64 cand = BATCH ? (i64)__ldg(tr.cand + k) : 0;
+    PatchGeom base = patch_geom(a, cand);
     base.rphh = known_reciprocal(base.phh);
-    const double rh = known_reciprocal(a.h);
-    const i64 nx = tr.nx, ny = tr.ny;
-    const double origin_x = a.origin_x, origin_y = a.origin_y, h = a.h;
+    const double rh = BATCH ? base.rphh : known_reciprocal(a.h);
+    const i64 nx = BATCH ? base.pnx : tr.nx, ny = BATCH ? base.pny : tr.ny;
+    const double origin_x = BATCH ? base.pox : a.origin_x;
+    const double origin_y = BATCH ? base.poy : a.origin_y;
+    const double h = BATCH ? base.phh : a.h;
+    const double upper_x = BATCH ? __ldg(a.patch_real + cand * 7 + 5) : a.upper_x;
+    const double upper_y = BATCH ? __ldg(a.patch_real + cand * 7 + 6) : a.upper_y;
+    const i64 *__restrict__ cells = BATCH ? a.cells + __ldg(tr.cell_off + cand) : a.cells;
     constexpr int cyl = CYL;
     const double inv_c2 = a.inv_c2;
     const i64 n = a.n;
@@ -609,11 +621,11 @@ __device__ __forceinline__ bool trace_thread(const Trace &tr, const i64 *__restr
             a.path_count[slot] = c + 1;
         }
         if (graded) px = uniform_x(px, a.x_nodes, a.n_x_nodes, origin_x, h);
-        if (px >= a.upper_x) {
+        if (px >= upper_x) {
             st = 0;
         } else if (px < origin_x) {
             st = 1;
-        } else if (py > a.upper_y || (cyl == 0 && py < origin_y)) {
+        } else if (py > upper_y || (cyl == 0 && py < origin_y)) {
             st = 2;
         } else {
             const double ux = div_known(px - origin_x, h, rh);
@@ -625,7 +637,7 @@ __device__ __forceinline__ bool trace_thread(const Trace &tr, const i64 *__restr
             // its first cell, where the reference indexes outside the table
             const int i = max(min(__double2int_rz(ux), (int)nx - 2), 0);
             const int j = max(min(__double2int_rz(uy), (int)ny - 2), 0);
-            const i64 cell = __ldg(a.cells + (i64)i * (ny - 1) + j);
+            const i64 cell = __ldg(cells + (i64)i * (ny - 1) + j);
             if (MAG && cell >= 0) {
                 st = -2;  // the caller tests the electrodes' shapes
             } else if (cell >= 0) {
@@ -673,8 +685,9 @@ __device__ __forceinline__ bool trace_thread(const Trace &tr, const i64 *__restr
 }
 
 // The window: every thread's trajectory, then each block's count of live trajectories and
-// every thread's flag, for compact_live.
-template <int CYL, int INTEG, bool GENERAL, bool MAG>
+// every thread's flag, for compact_live.  BATCH: the trajectories of many candidate meshes
+// in one launch (Trace::cand).
+template <int CYL, int INTEG, bool GENERAL, bool MAG, bool BATCH>
 __global__ void __launch_bounds__(128, 3)
     trace_window(Trace tr, const i64 *__restrict__ act, const i64 *__restrict__ live, i64 stride,
                  int S, uint32_t *__restrict__ keys, DepositRec *__restrict__ rec,
@@ -685,8 +698,8 @@ __global__ void __launch_bounds__(128, 3)
     if (m == 0 && n_act > 0) *records_end = end;
     bool still = false;
     if (m < stride)
-        still = trace_thread<CYL, INTEG, GENERAL, MAG>(tr, act, m, n_act, stride, S, keys, rec,
-                                                       sentinel);
+        still = trace_thread<CYL, INTEG, GENERAL, MAG, BATCH>(tr, act, m, n_act, stride, S, keys,
+                                                              rec, sentinel);
     const int count = __syncthreads_count(still);
     if (m < stride) alive[m] = still ? 1 : 0;
     if (threadIdx.x == 0) block_live[blockIdx.x] = (uint32_t)count;
@@ -790,7 +803,12 @@ struct SideStream {
     ~SideStream() { ctx->stream = saved; }
 };
 
-void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, int64_t window) {
+// Windows between reads of the live count for a batch: as many as keep a group's record
+// slots within kBatchGroupRecords (at least one, at most kGroup).
+constexpr int64_t kBatchGroupRecords = (int64_t)1 << 26;
+
+void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, int64_t window,
+               const bt_trace_batch *batch = nullptr) {
     {
         BT_REQUIRE(ctx && args, "trace: null argument");
         const bt_trace_args &a = *args;
@@ -815,17 +833,46 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                        "trace: the magnetic trace is non-relativistic on one patch");
             BT_REQUIRE(a.cylindrical != 2, "trace: no magnetic field with a symmetry plane");
         }
-        // the last patch's shape, for the exit and electrode tests
-        int64_t last[6];
-        BT_CUDA(cudaMemcpyAsync(last, a.patch_int + (a.n_patches - 1) * 6, sizeof(last),
-                                cudaMemcpyDeviceToHost, ctx->stream));
-        BT_CUDA(cudaStreamSynchronize(ctx->stream));
-        tr.nx = last[0];
-        tr.ny = last[1];
-        BT_REQUIRE(tr.nx >= 2 && tr.ny >= 2, "trace: the mesh needs at least 2 x 2 nodes");
+        tr.cand = nullptr;
+        tr.cell_off = nullptr;
+        if (batch) {
+            // every candidate's one patch: shapes of at least 2 x 2 nodes whose node ranges
+            // tile [0, n_nodes) in order (the deposit finds a node's candidate by bisection)
+            BT_REQUIRE(!mag, "trace: a batch takes no magnetic field");
+            BT_REQUIRE(batch->n_candidates >= 1 && batch->n_candidates == a.n_patches,
+                       "trace: a batch needs one patch row per candidate");
+            BT_REQUIRE(batch->candidate && batch->cell_offset, "trace: null batch table");
+            BT_REQUIRE(!a.graded && a.inv_c2 == 0.0,
+                       "trace: a batch takes uniform, non-relativistic meshes");
+            std::vector<int64_t> rows((size_t)6 * a.n_patches);
+            BT_CUDA(cudaMemcpyAsync(rows.data(), a.patch_int, sizeof(int64_t) * rows.size(),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+            BT_CUDA(cudaStreamSynchronize(ctx->stream));
+            int64_t next = 0;
+            for (int64_t c = 0; c < a.n_patches; ++c) {
+                const int64_t *r = rows.data() + 6 * c;
+                BT_REQUIRE(r[0] >= 2 && r[1] >= 2, "trace: a candidate needs at least 2 x 2 nodes");
+                BT_REQUIRE(r[4] == r[0] * r[1] && r[5] == next,
+                           "trace: the candidates' nodes must follow one another from 0");
+                next += r[4];
+            }
+            BT_REQUIRE(next == a.n_nodes, "trace: the candidates' nodes must fill n_nodes");
+            tr.cand = batch->candidate;
+            tr.cell_off = batch->cell_offset;
+            tr.nx = tr.ny = 0;
+        } else {
+            // the last patch's shape, for the exit and electrode tests
+            int64_t last[6];
+            BT_CUDA(cudaMemcpyAsync(last, a.patch_int + (a.n_patches - 1) * 6, sizeof(last),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+            BT_CUDA(cudaStreamSynchronize(ctx->stream));
+            tr.nx = last[0];
+            tr.ny = last[1];
+            BT_REQUIRE(tr.nx >= 2 && tr.ny >= 2, "trace: the mesh needs at least 2 x 2 nodes");
+        }
         BT_REQUIRE(a.cylindrical >= 0 && a.cylindrical <= 2, "trace: geometry must be 0, 1 or 2");
         const int S = window > 0 ? (int)window : 64;
-        const bool general = a.n_patches > 1 || a.graded != 0 || a.inv_c2 != 0.0;
+        const bool general = !batch && (a.n_patches > 1 || a.graded != 0 || a.inv_c2 != 0.0);
         ctx->last_windows = ctx->last_records = ctx->last_flushes = 0;
         if (a.n_active == 0) return;
         bt::TraceScratch &ts = ctx->trace;
@@ -835,10 +882,16 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         // and reduced into charge[0] on the side stream, in the order the buffers were
         // filled, so the deposit runs under the next windows and the sums are the same
         // whatever the timing.  A buffer is deposited at the end of the group that brought
-        // it to `batch` records (or on filling up within a group).
+        // it to `flush_at` records (or on filling up within a group).  A batch's windows
+        // are large: its groups hold fewer of them, so the buffers stay within a few GB.
         const int64_t per_window = a.n_active * (int64_t)S;
-        const int64_t batch = std::min<int64_t>(kBatchRecords, kGroup * per_window);
-        const int64_t capacity = batch + kGroup * per_window;
+        int group = kGroup;
+        if (batch) {
+            const int64_t fit = std::max<int64_t>(1, kBatchGroupRecords / std::max<int64_t>(per_window, 1));
+            group = (int)std::min<int64_t>(batch->group > 0 ? batch->group : fit, kGroup);
+        }
+        const int64_t flush_at = std::min<int64_t>(kBatchRecords, group * per_window);
+        const int64_t capacity = flush_at + group * per_window;
         uint32_t *keys[2];
         bt::DepositRec *rec[2];
         for (int b = 0; b < 2; ++b) {
@@ -867,7 +920,7 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                                 cudaMemcpyDeviceToDevice, st));
         BT_CUDA(cudaMemsetAsync(records_end, 0, 2 * sizeof(int64_t), st));
         BT_LAUNCH(ctx, bt::set_count, 1, 1, 0, st, live, a.n_active);
-        bt::NodeLayout layout{a.patch_int, a.n_patches, tr.nx, tr.ny, a.n_nodes};
+        bt::NodeLayout layout{a.patch_int, a.n_patches, tr.nx, tr.ny, a.n_nodes, batch != nullptr};
         int64_t bound = a.n_active, used = 0;
         int lv = 0;
         int cur = 0;
@@ -895,7 +948,7 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         // The windows go in groups of kGroup between reads of the live count: each reads
         // the count on the device, and a window after the last trajectory ended does no work.
         while (bound > 0) {
-            for (int g = 0; g < kGroup; ++g) {
+            for (int g = 0; g < group; ++g) {
                 const int64_t need = bound * (int64_t)S;
                 if (used + need > capacity) flush();
                 unsigned grid = 0;
@@ -903,12 +956,13 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                     bt::Timed timed(ctx, "trace_window");
                     grid = (unsigned)bt::blocks_for(bound, 128);
                     const int64_t launched = ctx->launch_count;
-#define BT_TRACE_CASE(C, I, G, M)                                                               \
+#define BT_TRACE_CASE_B(C, I, G, M, B)                                                          \
     if (a.cylindrical == C && (a.integrator != 0) == (I != 0) && general == G &&                 \
-        (mag != nullptr) == M)                                                                   \
-        BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M>), grid, 128, 0, st, tr, act_a, live + lv,   \
-                  bound, S, keys[cur] + used, rec[cur] + used, sentinel, records_end + cur,       \
-                  used + need, block_live, alive);
+        (mag != nullptr) == M && (batch != nullptr) == B)                                        \
+        BT_LAUNCH(ctx, (bt::trace_window<C, I, G, M, B>), grid, 128, 0, st, tr, act_a,            \
+                  live + lv, bound, S, keys[cur] + used, rec[cur] + used, sentinel,               \
+                  records_end + cur, used + need, block_live, alive);
+#define BT_TRACE_CASE(C, I, G, M) BT_TRACE_CASE_B(C, I, G, M, false)
                     BT_TRACE_CASE(0, 0, false, false) BT_TRACE_CASE(0, 0, true, false)
                     BT_TRACE_CASE(0, 1, false, false) BT_TRACE_CASE(0, 1, true, false)
                     BT_TRACE_CASE(1, 0, false, false) BT_TRACE_CASE(1, 0, true, false)
@@ -919,7 +973,11 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                     BT_TRACE_CASE(0, 1, false, true) BT_TRACE_CASE(0, 1, true, true)
                     BT_TRACE_CASE(1, 0, false, true) BT_TRACE_CASE(1, 0, true, true)
                     BT_TRACE_CASE(1, 1, false, true) BT_TRACE_CASE(1, 1, true, true)
+                    BT_TRACE_CASE_B(0, 0, false, false, true) BT_TRACE_CASE_B(0, 1, false, false, true)
+                    BT_TRACE_CASE_B(1, 0, false, false, true) BT_TRACE_CASE_B(1, 1, false, false, true)
+                    BT_TRACE_CASE_B(2, 0, false, false, true) BT_TRACE_CASE_B(2, 1, false, false, true)
 #undef BT_TRACE_CASE
+#undef BT_TRACE_CASE_B
                     BT_REQUIRE(ctx->launch_count > launched,
                                "trace: no kernel for these settings");
                 }
@@ -942,7 +1000,7 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                                     cudaMemcpyDeviceToHost, st));
             BT_CUDA(cudaStreamSynchronize(st));
             bound = *n_alive_host;
-            if (used >= batch) flush();
+            if (used >= flush_at) flush();
         }
         flush();
         // the caller's stream continues once every deposit is in charge[0]
@@ -974,6 +1032,16 @@ extern "C" int BT_TRACE_ENTRY(bt_trace_trajectories_2d_magnetic)(bt_ctx *ctx,
     return bt::guarded([&] {
         BT_REQUIRE(magnetic, "trace: null magnetic field");
         bt::trace_all(ctx, args, magnetic, window);
+    });
+}
+
+extern "C" int BT_TRACE_ENTRY(bt_trace_trajectories_2d_batch)(bt_ctx *ctx,
+                                                              const bt_trace_args *args,
+                                                              const bt_trace_batch *batch,
+                                                              int64_t window) {
+    return bt::guarded([&] {
+        BT_REQUIRE(batch, "trace: null batch");
+        bt::trace_all(ctx, args, nullptr, window, batch);
     });
 }
 

@@ -189,6 +189,35 @@ int bt_trace_trajectories_2d_magnetic(bt_ctx *ctx, const bt_trace_args *args,
 int bt_trace_trajectories_2d_magnetic_fast(bt_ctx *ctx, const bt_trace_args *args,
                                            const bt_magnetic *magnetic, int64_t window);
 
+/* The candidates of a batched trace: many independent meshes traced in one launch.  The
+ * reference's design search traces its candidates one at a time
+ * (optimization/einzel.py:389-403); this has no single-call counterpart there.
+ * args->patch_int / patch_real hold one row per candidate (n_patches = n_candidates), as
+ * the trace's one-patch rows: (nx, ny, offset into fxs, offset into fys, nodes, offset of
+ * the first node) and (origin x, origin y, h, origin x, origin y, upper x, upper y), the
+ * node offsets ascending and contiguous from 0 to args->n_nodes.  All DEVICE. */
+typedef struct bt_trace_batch {
+    int64_t n_candidates;
+    const int32_t *candidate;  /* (n,) the candidate of every trajectory */
+    const int64_t *cell_offset; /* (n_candidates,) where its cell table starts in cells */
+    int64_t group;              /* windows between reads of the live count (0: chosen) */
+} bt_trace_batch;
+
+/* No counterpart in the reference (see bt_trace_batch).  bt_trace_trajectories_2d over a
+ * batch of candidate meshes: one window launch advances every candidate's live
+ * trajectories, and one deposit sorts and reduces the records of all of them (keys are the
+ * candidates' concatenated node indices).  Each trajectory's steps, crossings and end are
+ * those it has traced alone; its charges are summed in the same record order, grouped
+ * into deposits differently.  One patch per candidate, uniform axes, non-relativistic, no
+ * magnetic field. */
+int bt_trace_trajectories_2d_batch(bt_ctx *ctx, const bt_trace_args *args,
+                                   const bt_trace_batch *batch, int64_t window);
+
+/* No counterpart in the reference: bt_trace_trajectories_2d_batch built with contracted
+ * multiply-adds (as bt_trace_trajectories_2d_fast). */
+int bt_trace_trajectories_2d_batch_fast(bt_ctx *ctx, const bt_trace_args *args,
+                                        const bt_trace_batch *batch, int64_t window);
+
 /* Counters of the last bt_trace_trajectories_2d call on this context (host out-params). */
 int bt_trace_last_stats(bt_ctx *ctx, int64_t *windows, int64_t *records,
                         int64_t *deposit_flushes);
