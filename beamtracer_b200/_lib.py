@@ -67,7 +67,10 @@ class TraceArgs(ctypes.Structure):
 class TraceBatch(ctypes.Structure):
     """``bt_trace_batch`` of ``include/bt200.h``."""
 
-    _fields_ = [("n_candidates", I64), ("candidate", P), ("cell_offset", P), ("group", I64)]
+    _fields_ = [
+        ("n_candidates", I64), ("candidate", P), ("cell_offset", P), ("group", I64),
+        ("shape_first", P), ("shape_kind", P), ("shape_offset", P), ("shape_params", P),
+    ]  # fmt: skip
 
 
 class MagneticDesc(ctypes.Structure):
@@ -151,6 +154,9 @@ SIGNATURES: dict[str, list] = {
     "bt_poisson_destroy": [P],
     "bt_poisson_set_region": [P, P, F64],
     "bt_poisson_set_options": [P, I32, I32, I32, I64],
+    "bt_poisson_batch_create": [P, P, I64, P, ctypes.POINTER(P)],
+    "bt_poisson_batch_destroy": [P],
+    "bt_poisson_batch_solve": [P, P, P, P, F64, I32, P, P],
     "bt_poisson_solve": [
         P, P, P, F64, F64, F64, I32, F64, F64, I32,
         ctypes.POINTER(I32), ctypes.POINTER(I32),

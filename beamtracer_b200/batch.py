@@ -121,7 +121,8 @@ class BatchedVlasov:
     """
 
     def __init__(self, configs: Sequence[BeamOpticsConfig], *, window: int = 64,
-                 contracted: bool = False, capacity: tuple[int, int] = (4, 1024)) -> None:  # fmt: skip
+                 contracted: bool = False, capacity: tuple[int, int] = (4, 1024),
+                 field: str = "batched") -> None:  # fmt: skip
         import torch
 
         from beamtracer_b200.model import config_mesh, config_particles
@@ -138,6 +139,9 @@ class BatchedVlasov:
             for name in shared:
                 if getattr(config, name) != getattr(first, name):
                     raise ValueError(f"every configuration of a batch needs the same {name}")
+        if field not in ("batched", "single"):
+            raise ValueError(f"field must be 'batched' or 'single', got {field!r}")
+        self.field = field
         self.torch = torch
         self.window = int(window)
         self.contracted = bool(contracted)
@@ -228,6 +232,10 @@ class BatchedVlasov:
         self.subcells = torch.cat(subcells) if blocks else torch.full((1,), -1, dtype=torch.int64,
                                                                      device=dev)  # fmt: skip
         self.cell_offset = torch.tensor(cell_offset, dtype=torch.int64, device=dev)
+        # the candidates' electrode shapes end to end, for the trace's own electrode test
+        # (None when one candidate's electrodes are not configuration shapes: its paused
+        # trajectories are tested here, on the host)
+        self.shapes = self._shape_tables()
         self.planes_dev = torch.tensor(self.planes or (np.nan,), dtype=torch.float64, device=dev)
         self.capacity = tuple(capacity)
         self._allocate_hits()
@@ -238,6 +246,30 @@ class BatchedVlasov:
         # per candidate: max |phi - previous|, max |rho_new - rho_old|, max |rho_new|
         self.scalars = torch.zeros((len(cands), 4), **f64)
         self.trace_launches = 0
+        self.poisson_batch = PoissonBatch([c.poisson for c in cands], [c.node0 for c in cands])
+
+    def _shape_tables(self):
+        torch = self.torch
+        from beamtracer_b200.shapes import shape_table
+
+        kinds, offsets, params, first = [], [], [], [0]
+        for c in self.candidates:
+            table = shape_table(c.mesh) if c.mesh.electrodes else (
+                np.zeros(0, np.int32), np.zeros(0, np.int64), np.zeros(0))  # fmt: skip
+            if table is None:
+                return None
+            kind, offset, param = table
+            kinds.append(kind)
+            offsets.append(offset + sum(p.size for p in params))
+            params.append(param)
+            first.append(first[-1] + kind.size)
+        if first[-1] == 0:
+            return None  # no electrodes: nothing to test
+        dev = "cuda"
+        return (torch.from_numpy(np.array(first, dtype=np.int64)).to(dev),
+                torch.from_numpy(np.concatenate(kinds).astype(np.int32)).to(dev),
+                torch.from_numpy(np.concatenate(offsets).astype(np.int64)).to(dev),
+                torch.from_numpy(np.concatenate(params).astype(np.float64)).to(dev))  # fmt: skip
 
     # -- the trace ---------------------------------------------------------------------
 
@@ -271,7 +303,9 @@ class BatchedVlasov:
             d(self.path_slot), d(self.paths), 1, d(self.path_count), 1, d(self.charge),
             self.n_nodes, 0, d(self.x_nodes), 2, 0.0,
         )  # fmt: skip
-        b = _lib.TraceBatch(len(self.candidates), d(self.candidate_dev), d(self.cell_offset), 0)
+        shapes = (d(t) for t in self.shapes) if self.shapes is not None else (None,) * 4
+        b = _lib.TraceBatch(len(self.candidates), d(self.candidate_dev), d(self.cell_offset), 0,
+                            *shapes)  # fmt: skip
         lib = _lib.lib()
         entry = lib.bt_trace_trajectories_2d_batch_fast if self.contracted else lib.bt_trace_trajectories_2d_batch
         _lib.check(entry(self.ctx.handle, ctypes.byref(a), ctypes.byref(b), self.window))
@@ -386,10 +420,14 @@ class BatchedVlasov:
 
     def solve_fields(self, members: Sequence[int]) -> None:
         """The potential of every member candidate from its density, each from its last
-        potential (one candidate at a time)."""
-        for k in members:
-            c = self.candidates[k]
-            c.poisson.solve_device(self.node_view(self.phi, k), self.node_view(self.rho, k))
+        potential: one batched multigrid iteration over all of them
+        (``bt_poisson_batch_solve``), or one candidate at a time (``field="single"``)."""
+        if self.field == "single":
+            for k in members:
+                c = self.candidates[k]
+                c.poisson.solve_device(self.node_view(self.phi, k), self.node_view(self.rho, k))
+            return
+        self.poisson_batch.solve(self.phi, self.rho, members)
 
     # -- views ---------------------------------------------------------------------------
 
@@ -403,6 +441,46 @@ class BatchedVlasov:
         fx = self.fx[c.fx0 : c.fx0 + (nx + 1) * ny].view(nx + 1, ny)
         fy = self.fy[c.fy0 : c.fy0 + nx * (ny + 1)].view(nx, ny + 1)
         return fx, fy
+
+
+class PoissonBatch:
+    """The field solves of many candidates' solvers at once (``bt_poisson_batch_*``):
+    candidate k's nodes at ``offsets[k]`` of the concatenated potential and density."""
+
+    def __init__(self, solvers: Sequence[IonOpticsPoisson], offsets: Sequence[int]) -> None:
+        self.solvers = list(solvers)  # kept alive: the batch reads their hierarchies
+        self.count = len(self.solvers)
+        handles = (_lib.P * self.count)(*[s._handle.value for s in self.solvers])
+        self._offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        handle = _lib.P()
+        ctx = _lib.context()
+        _lib.check(_lib.lib().bt_poisson_batch_create(
+            ctx.handle, ctypes.cast(handles, _lib.P), self.count, self._offsets.ctypes.data,
+            ctypes.byref(handle)))  # fmt: skip
+        self._handle = handle
+        self.cycles = np.zeros(self.count, dtype=np.int32)
+        self.residual = np.zeros(self.count)
+
+    def solve(self, phi, rho, members: Sequence[int], tolerance: float = 1e-13,
+              max_cycles: int = 400) -> None:  # fmt: skip
+        """Solve the members' fields in place on the concatenated device arrays."""
+        flags = np.zeros(self.count, dtype=np.uint8)
+        flags[list(members)] = 1
+        d = _lib.dptr
+        _lib.check(_lib.lib().bt_poisson_batch_solve(
+            self._handle, d(phi), d(rho), flags.ctypes.data, float(tolerance), int(max_cycles),
+            self.cycles.ctypes.data, self.residual.ctypes.data))  # fmt: skip
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None) is not None and self._handle.value:
+            _lib.lib().bt_poisson_batch_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self) -> None:  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _atomic_mass() -> float:

@@ -11,55 +11,6 @@
 namespace bt {
 namespace {
 
-// shape kinds; 3 is an aperture (a polygon and its mirror image)
-constexpr int kShapeRect = 0, kShapeCircle = 1, kShapePolygon = 2;
-constexpr int kEdgeWords = 9;  // x1, y1, x2, y2, threshold, x_lo, x_hi, y_lo, y_hi
-
-// Inside the polygon at p (p[0] its edge count, then its edges) or on its boundary.
-__device__ bool polygon_inside(const double *__restrict__ p, double x, double y) {
-    const i64 n = (i64)p[0];
-    const double *e = p + 1;
-    bool inside = false, boundary = false;
-    for (i64 k = 0; k < n; ++k, e += kEdgeWords) {
-        const double x1 = e[0], y1 = e[1], x2 = e[2], y2 = e[3];
-        if ((y1 > y) != (y2 > y)) {
-            const double at = x1 + (y - y1) * (x2 - x1) / (y2 - y1);
-            if (x < at) inside = !inside;
-        }
-        const double cross = (x2 - x1) * (y - y1) - (y2 - y1) * (x - x1);
-        if (fabs(cross) <= e[4] && x >= e[5] && x <= e[6] && y >= e[7] && y <= e[8])
-            boundary = true;
-    }
-    return inside || boundary;
-}
-
-__device__ bool shape_inside(int kind, const double *__restrict__ p, double x, double y) {
-    if (kind == kShapeRect) return fabs(x - p[0]) <= p[2] && fabs(y - p[1]) <= p[3];
-    if (kind == kShapeCircle) {
-        const double dx = x - p[0], dy = y - p[1];
-        return dx * dx + dy * dy <= p[2];
-    }
-    if (kind == kShapePolygon) return polygon_inside(p, x, y);
-    // an aperture: the polygon and its mirror image, one after the other
-    const bool first = polygon_inside(p, x, y);
-    const double *q = p + 1 + (i64)p[0] * kEdgeWords;
-    return first || polygon_inside(q, x, y);
-}
-
-struct Shapes {
-    i64 count;
-    const int32_t *kind;
-    const i64 *offset;
-    const double *params;
-};
-
-// The first electrode holding (x, y), or -1 (mesh.inside_solid).
-__device__ i64 inside_solid(const Shapes &S, double x, double y) {
-    for (i64 s = 0; s < S.count; ++s)
-        if (shape_inside(S.kind[s], S.params + S.offset[s], x, y)) return s;
-    return -1;
-}
-
 // The position along x of the fractional node index `index` (mesh.position_x).
 __device__ double position_x(double index, double origin_x, double h, const double *nodes,
                              i64 n_nodes) {

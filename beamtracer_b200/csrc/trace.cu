@@ -31,6 +31,10 @@ struct Trace {
     // a.patch_real is candidate c's one patch (shape, offsets, origin, spacing, extent).
     const int32_t *cand;
     const i64 *cell_off;
+    // the candidates' electrode shapes (candidate c's: shape_first[c] .. shape_first[c + 1]
+    // - 1 of `shapes`), or shape_first NULL: pause for the caller's test
+    const i64 *shape_first;
+    Shapes shapes;
 };
 
 __device__ __forceinline__ i64 node_cell(double x, const double *__restrict__ nodes, i64 n) {
@@ -656,6 +660,17 @@ __device__ __forceinline__ bool trace_thread(const Trace &tr, const i64 *__restr
                 if (e >= 0) {
                     st = 3;
                     a.electrode[k] = e;
+                } else if (e == -2 && BATCH && tr.shape_first) {
+                    // the candidate's own electrodes, tested here at the point's mesh
+                    // coordinates: the caller's test of a paused trajectory
+                    const i64 s0 = __ldg(tr.shape_first + cand);
+                    const Shapes S{__ldg(tr.shape_first + cand + 1) - s0, tr.shapes.kind + s0,
+                                   tr.shapes.offset + s0, tr.shapes.params};
+                    const i64 hit = inside_solid(S, px, py);
+                    if (hit >= 0) {
+                        st = 3;
+                        a.electrode[k] = hit;
+                    }
                 } else if (e == -2) {
                     st = -2;
                 }
@@ -835,6 +850,8 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         }
         tr.cand = nullptr;
         tr.cell_off = nullptr;
+        tr.shape_first = nullptr;
+        tr.shapes = bt::Shapes{0, nullptr, nullptr, nullptr};
         if (batch) {
             // every candidate's one patch: shapes of at least 2 x 2 nodes whose node ranges
             // tile [0, n_nodes) in order (the deposit finds a node's candidate by bisection)
@@ -859,6 +876,13 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
             BT_REQUIRE(next == a.n_nodes, "trace: the candidates' nodes must fill n_nodes");
             tr.cand = batch->candidate;
             tr.cell_off = batch->cell_offset;
+            if (batch->shape_first) {
+                BT_REQUIRE(batch->shape_kind && batch->shape_offset && batch->shape_params,
+                           "trace: a batch's shapes need their kind, offset and parameters");
+                tr.shape_first = batch->shape_first;
+                tr.shapes = bt::Shapes{0, batch->shape_kind, batch->shape_offset,
+                                       batch->shape_params};
+            }
             tr.nx = tr.ny = 0;
         } else {
             // the last patch's shape, for the exit and electrode tests

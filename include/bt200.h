@@ -201,6 +201,16 @@ typedef struct bt_trace_batch {
     const int32_t *candidate;  /* (n,) the candidate of every trajectory */
     const int64_t *cell_offset; /* (n_candidates,) where its cell table starts in cells */
     int64_t group;              /* windows between reads of the live count (0: chosen) */
+    /* The candidates' electrodes as shapes (the bt_shapes tables of all candidates end to
+     * end; candidate c's electrodes are shapes shape_first[c] .. shape_first[c + 1] - 1, in
+     * its electrode order), or shape_first NULL.  With them a trajectory whose step ends in
+     * a sub-cell an electrode surface cuts is tested against its candidate's shapes in the
+     * kernel (at its mesh coordinates (x, r) or (x, y)) instead of pausing with status -2
+     * for the caller's test. */
+    const int64_t *shape_first;  /* (n_candidates + 1,) */
+    const int32_t *shape_kind;
+    const int64_t *shape_offset;
+    const double *shape_params;
 } bt_trace_batch;
 
 /* No counterpart in the reference (see bt_trace_batch).  bt_trace_trajectories_2d over a
@@ -354,6 +364,31 @@ int bt_poisson_set_region(bt_poisson *p, const uint8_t *mask, double value);
  * and the size above which a level is never part of the one-block tail. */
 int bt_poisson_set_options(bt_poisson *p, int32_t fine_sweeps, int32_t coarse_sweeps,
                            int32_t staged, int64_t tail_nodes);
+
+/* -- the batched field solve (no counterpart in the reference, which solves each design
+ * candidate's field on its own: optimization/einzel.py:389-403) ------------------------- */
+
+typedef struct bt_poisson_batch bt_poisson_batch;
+
+/* A batch of `count` solvers on one context (each candidate mesh's own bt_poisson, kept
+ * alive and unchanged -- no bt_poisson_set_options -- while the batch lives), candidate c's
+ * nodes at offset[c] (HOST) of the batch's concatenated potential and density.  Every
+ * solver needs the staged smoother, at most 2 coarse sweeps and a hierarchy of at least two
+ * levels with a one-block tail. */
+int bt_poisson_batch_create(bt_ctx *ctx, bt_poisson *const *solvers, int64_t count,
+                            const int64_t *offset, bt_poisson_batch **out);
+int bt_poisson_batch_destroy(bt_poisson_batch *batch);
+
+/* The linear field solve of every candidate c with members[c] != 0 (HOST flags), in place on
+ * the DEVICE arrays phi and rho (rho NULL: no charge): the multigrid iteration
+ * d <- d + V(r0 - A d) with one V-cycle over all members per step (a launch per level step
+ * and kind, the coarse levels in one block per candidate), each member until its residual
+ * is at most tol max(|b|, |r0|) -- the criterion of bt_poisson_solve -- or stops falling.
+ * cycles and residual (HOST, count entries, may be NULL) get each member's V-cycles and
+ * final residual norm.  BT_ERR_NOCONV if a member ends above 1e4 times its goal. */
+int bt_poisson_batch_solve(bt_poisson_batch *batch, double *phi, const double *rho,
+                           const uint8_t *members, double tol, int32_t max_cycles,
+                           int32_t *cycles, double *residual);
 
 /* No counterpart in the reference (the differentiation form).  on != 0: the solver's
  * operator becomes the transpose of the free rows' block, A_ff^T (the neighbour
