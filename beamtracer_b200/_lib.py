@@ -157,6 +157,7 @@ SIGNATURES: dict[str, list] = {
     "bt_poisson_batch_create": [P, P, I64, P, ctypes.POINTER(P)],
     "bt_poisson_batch_destroy": [P],
     "bt_poisson_batch_solve": [P, P, P, P, F64, I32, P, P],
+    "bt_poisson_batch_tiling": [P, I32, P],
     "bt_poisson_solve": [
         P, P, P, F64, F64, F64, I32, F64, F64, I32,
         ctypes.POINTER(I32), ctypes.POINTER(I32),

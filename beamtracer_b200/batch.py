@@ -429,6 +429,10 @@ class BatchedVlasov:
             return
         self.poisson_batch.solve(self.phi, self.rho, members)
 
+    def close(self) -> None:
+        """Release the batched field solver (the candidates' own solvers stay usable)."""
+        self.poisson_batch.close()
+
     # -- views ---------------------------------------------------------------------------
 
     def node_view(self, array, k: int):
@@ -471,6 +475,19 @@ class PoissonBatch:
             self._handle, d(phi), d(rho), flags.ctypes.data, float(tolerance), int(max_cycles),
             self.cycles.ctypes.data, self.residual.ctypes.data))  # fmt: skip
 
+    @property
+    def tiling(self) -> dict:
+        """The V-cycle's smoothing tiles (chosen by timing at the first solve)."""
+        t = np.zeros(6, dtype=np.int32)
+        _lib.check(_lib.lib().bt_poisson_batch_tiling(self._handle, 0, t.ctypes.data))
+        return {"level0": (int(t[0]), int(t[1])), "nine_point": (int(t[2]), int(t[3])),
+                "nine_point_launches": int(t[4]), "tuned": bool(t[5])}  # fmt: skip
+
+    def set_tiling(self, level0=(32, 32), nine_point=(16, 32), launches: int = 1) -> None:
+        """Fix the smoothing tiles (no tuning)."""
+        t = np.array([*level0, *nine_point, launches, 1], dtype=np.int32)
+        _lib.check(_lib.lib().bt_poisson_batch_tiling(self._handle, 1, t.ctypes.data))
+
     def close(self) -> None:
         if getattr(self, "_handle", None) is not None and self._handle.value:
             _lib.lib().bt_poisson_batch_destroy(self._handle)
@@ -487,3 +504,25 @@ def _atomic_mass() -> float:
     from scipy import constants
 
     return constants.atomic_mass
+
+
+def batched_sweep(designs, rank: int = 0, world: int = 1, plane: float = 79e-3,
+                  **settings) -> dict[int, dict]:  # fmt: skip
+    """This rank's share of the einzel candidates ``designs`` (`einzel.share_of_designs`)
+    converged together in one `BatchedVlasov`: ``{candidate index: result}`` with the
+    result of `einzel.evaluate_design` (moments at ``plane``, iterations, convergence)."""
+    from beamtracer_b200.einzel import einzel_config, share_of_designs
+
+    mine = share_of_designs(designs, rank, world)
+    if not mine:
+        return {}
+    batch = BatchedVlasov([einzel_config(designs[k], **settings) for k in mine]).run()
+    out = {}
+    for j, k in enumerate(mine):
+        c = batch.candidates[j]
+        m = c.moments(plane)
+        out[k] = {"current": m.current, "rms_size": m.rms_size, "rms_angle": m.rms_angle,
+                  "emittance": m.emittance, "iterations": len(c.history),
+                  "converged": int(c.converged)}  # fmt: skip
+    batch.close()
+    return out

@@ -308,9 +308,9 @@ class ParticleBeam:
         current = np.asarray(self.current, dtype=float).ravel()
         if not position.shape[0] == velocity.shape[0] == current.size:
             raise ValueError("position, velocity and current need one row per trajectory")
-        object.__setattr__(self, "position", tuple(map(tuple, position)))
-        object.__setattr__(self, "velocity", tuple(map(tuple, velocity)))
-        object.__setattr__(self, "current", tuple(current))
+        object.__setattr__(self, "position", tuple(map(tuple, position.tolist())))
+        object.__setattr__(self, "velocity", tuple(map(tuple, velocity.tolist())))
+        object.__setattr__(self, "current", tuple(current.tolist()))
         # the arrays the tuples were made from, so a model reads them without rebuilding
         object.__setattr__(self, "_arrays", (position, velocity, current))
 

@@ -17,10 +17,24 @@ namespace {
 
 constexpr size_t kPoolMaxBytes = (size_t)8 << 30;
 
+constexpr size_t kCarveMax = (size_t)4 << 20;
+constexpr size_t kSlabBytes = (size_t)128 << 20;
+
+struct Cached {
+    void *ptr;
+    bool carved;
+};
+
+struct Slab {
+    char *base = nullptr;
+    size_t used = 0;
+};
+
 struct Pool {
     std::mutex mu;
-    std::multimap<std::pair<int, size_t>, void *> blocks;  // (device, bytes) -> block
-    size_t cached = 0;
+    std::multimap<std::pair<int, size_t>, Cached> blocks;  // (device, bytes) -> block
+    size_t cached = 0;                                     // bytes of uncarved blocks
+    std::map<int, Slab> slabs;                             // the slab carved from, per device
 };
 
 Pool &pool() {
@@ -31,23 +45,42 @@ Pool &pool() {
 }  // namespace
 
 // A cached block on the current device of at least `need` bytes and at most twice that
-// (plus 1 MB), else a new one.
-void *pool_take(size_t need, size_t *got, int *device_out) {
+// (plus 1 MB), else a new one: a piece of the device's slab for a small block, else its own
+// cudaMalloc.
+void *pool_take(size_t need, size_t *got, int *device_out, bool *carved) {
     int device = 0;
     cudaGetDevice(&device);
     *device_out = device;
-    {
-        Pool &p = pool();
-        std::lock_guard<std::mutex> lock(p.mu);
-        auto it = p.blocks.lower_bound({device, need});
-        if (it != p.blocks.end() && it->first.first == device &&
-            it->first.second <= 2 * need + ((size_t)1 << 20)) {
-            void *ptr = it->second;
-            *got = it->first.second;
-            p.cached -= it->first.second;
-            p.blocks.erase(it);
-            return ptr;
+    Pool &p = pool();
+    std::lock_guard<std::mutex> lock(p.mu);
+    auto it = p.blocks.lower_bound({device, need});
+    if (it != p.blocks.end() && it->first.first == device &&
+        it->first.second <= 2 * need + ((size_t)1 << 20)) {
+        const Cached block = it->second;
+        *got = it->first.second;
+        if (!block.carved) p.cached -= it->first.second;
+        p.blocks.erase(it);
+        *carved = block.carved;
+        return block.ptr;
+    }
+    if (need <= kCarveMax) {
+        const size_t size = (need + 255) & ~(size_t)255;
+        Slab &slab = p.slabs[device];
+        if (!slab.base || slab.used + size > kSlabBytes) {
+            void *base = nullptr;
+            cudaError_t e = cudaMalloc(&base, kSlabBytes);
+            if (e != cudaSuccess) {
+                (void)cudaGetLastError();
+                throw Error{BT_ERR_ALLOC, std::string("cudaMalloc of a slab: ") + cudaGetErrorString(e)};
+            }
+            slab.base = static_cast<char *>(base);
+            slab.used = 0;
         }
+        void *ptr = slab.base + slab.used;
+        slab.used += size;
+        *got = size;
+        *carved = true;
+        return ptr;
     }
     void *ptr = nullptr;
     cudaError_t e = cudaMalloc(&ptr, need);
@@ -57,17 +90,18 @@ void *pool_take(size_t need, size_t *got, int *device_out) {
                                       " bytes: " + cudaGetErrorString(e)};
     }
     *got = need;
+    *carved = false;
     return ptr;
 }
 
-void pool_give(void *ptr, size_t bytes, int device) {
+void pool_give(void *ptr, size_t bytes, int device, bool carved) {
     if (!ptr) return;
     {
         Pool &p = pool();
         std::lock_guard<std::mutex> lock(p.mu);
-        if (p.cached + bytes <= kPoolMaxBytes) {
-            p.blocks.insert({{device, bytes}, ptr});
-            p.cached += bytes;
+        if (carved || p.cached + bytes <= kPoolMaxBytes) {
+            p.blocks.insert({{device, bytes}, Cached{ptr, carved}});
+            if (!carved) p.cached += bytes;
             return;
         }
     }
@@ -81,18 +115,24 @@ void pool_give(void *ptr, size_t bytes, int device) {
 void *Buffer::get(size_t need) {
     if (need == 0) need = 1;
     if (need <= bytes) return ptr;
-    // the old block may still be read by queued work: free it the waiting way
-    if (ptr) cudaFree(ptr);
+    // the old block may still be read by queued work: free it the waiting way (a carved
+    // one goes to the cache once the device is idle)
+    if (ptr && carved) {
+        cudaDeviceSynchronize();
+        pool_give(ptr, bytes, device, true);
+    } else if (ptr) {
+        cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
     size_t got = 0;
-    ptr = pool_take(need + need / 4, &got, &device);
+    ptr = pool_take(need + need / 4, &got, &device, &carved);
     bytes = got;
     return ptr;
 }
 
 void Buffer::release() {
-    pool_give(ptr, bytes, device);
+    pool_give(ptr, bytes, device, carved);
     ptr = nullptr;
     bytes = 0;
 }

@@ -58,17 +58,20 @@ struct Error {
 // synchronise their stream before they destroy their buffers.  The cache keeps at most
 // kPoolMaxBytes; cudaMalloc and cudaFree stay off the path of a solver made and dropped
 // per call.
-void *pool_take(size_t need, size_t *got, int *device);
-void pool_give(void *ptr, size_t bytes, int device);
+// Blocks of at most 4 MB are carved from 128 MB slabs (one cudaMalloc for many of a
+// solver's arrays); a carved block is never freed, only cached.
+void *pool_take(size_t need, size_t *got, int *device, bool *carved);
+void pool_give(void *ptr, size_t bytes, int device, bool carved);
 
 struct Buffer {
     void *ptr = nullptr;
     size_t bytes = 0;
-    int device = 0;  // where the block lives
+    int device = 0;       // where the block lives
+    bool carved = false;  // a slab's piece (pool_take)
     Buffer() = default;
     Buffer(const Buffer &) = delete;
     Buffer &operator=(const Buffer &) = delete;
-    Buffer(Buffer &&o) noexcept : ptr(o.ptr), bytes(o.bytes), device(o.device) {
+    Buffer(Buffer &&o) noexcept : ptr(o.ptr), bytes(o.bytes), device(o.device), carved(o.carved) {
         o.ptr = nullptr;
         o.bytes = 0;
     }
@@ -78,6 +81,7 @@ struct Buffer {
             ptr = o.ptr;
             bytes = o.bytes;
             device = o.device;
+            carved = o.carved;
             o.ptr = nullptr;
             o.bytes = 0;
         }

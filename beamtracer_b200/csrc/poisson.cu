@@ -2255,58 +2255,63 @@ __device__ __forceinline__ int find_entry(const int *__restrict__ start, int n, 
     return lo;
 }
 
-// Pre-smoothing (x -> x2; level 0 from a zero x) or post-smoothing with the prolonged
-// correction added as x2 is read (x2 -> x) of every entry's level, a staged tile a block.
+// Smoothing phases of every entry's level, a staged tile a block: from one of the level's
+// x buffers (0: x, 1: x2) into the other; `zero_in`: x starts at zero (not read);
+// `prolong`: the prolonged coarse correction is added as x is read.
 template <bool NINE, int R>
 __global__ void __launch_bounds__(kStageThreads)
-    batch_smooth(const BatchLevel *__restrict__ E, const int *__restrict__ start, int ne,
-                 const uint8_t *__restrict__ live, int tx, int ty, Phases ph, int post) {
-    const int e = find_entry(start, ne, blockIdx.x);
-    const BatchLevel &L = E[e];
+    batch_smooth(const BatchLevel *__restrict__ E, const int *__restrict__ ids,
+                 const int *__restrict__ start, int ne, const uint8_t *__restrict__ live,
+                 int tx, int ty, Phases ph, int from, int prolong, int zero_in) {
+    const int slot = find_entry(start, ne, blockIdx.x);
+    const BatchLevel &L = E[ids[slot]];
     if (!live[L.cand]) return;
-    const i64 local = (i64)blockIdx.x - start[e];
+    const i64 local = (i64)blockIdx.x - start[slot];
     const i64 tiles_y = (L.ny + ty - 1) / ty;
     const i64 bx = local / tiles_y, by = local - bx * tiles_y;
-    if (post) {
-        smooth_staged_tile<NINE, R>(L.nx, L.ny, L.c4, L.diag, L.a9, L.active, L.b, L.x2, L.x,
-                                    tx, ty, ph, L.F, L.xc, bx, by);
-    } else {
-        const Fine none{};
-        smooth_staged_tile<NINE, R>(L.nx, L.ny, L.c4, L.diag, L.a9, L.active, L.b, L.x, L.x2,
-                                    tx, ty, ph, none, nullptr, bx, by, !NINE);
-    }
+    const double *in = from ? L.x2 : L.x;
+    double *out = from ? L.x : L.x2;
+    const Fine none{};
+    smooth_staged_tile<NINE, R>(L.nx, L.ny, L.c4, L.diag, L.a9, L.active, L.b, in, out, tx, ty,
+                                ph, prolong ? L.F : none, prolong ? L.xc : nullptr, bx, by,
+                                zero_in != 0);
 }
 
-// r = b - A x2 on every entry's level, then (after the launch) its restriction.
+// r = b - A x on every entry's level (x in the buffer `from` names: 0 x, 1 x2), then
+// (after the launch) its restriction.
 template <bool NINE>
-__global__ void batch_residual(const BatchLevel *__restrict__ E, const int *__restrict__ start,
-                               int ne, const uint8_t *__restrict__ live) {
-    const int e = find_entry(start, ne, blockIdx.x);
-    const BatchLevel &L = E[e];
+__global__ void batch_residual(const BatchLevel *__restrict__ E, const int *__restrict__ ids,
+                               const int *__restrict__ start,
+                               int ne, const uint8_t *__restrict__ live, int from) {
+    const int slot = find_entry(start, ne, blockIdx.x);
+    const BatchLevel &L = E[ids[slot]];
     if (!live[L.cand]) return;
-    const i64 f = ((i64)blockIdx.x - start[e]) * kBatchThreads + threadIdx.x;
+    const i64 f = ((i64)blockIdx.x - start[slot]) * kBatchThreads + threadIdx.x;
     if (f >= L.n) return;
+    const double *x = from ? L.x2 : L.x;
     if (NINE)
-        residual9_item(f, L.nx, L.ny, L.a9, L.active, L.x2, L.b, L.r, PlainLoad{});
+        residual9_item(f, L.nx, L.ny, L.a9, L.active, x, L.b, L.r, PlainLoad{});
     else
-        apply5_item(f, L.nx, L.ny, L.c4, L.diag, L.active, L.x2, L.b, L.r);
+        apply5_item(f, L.nx, L.ny, L.c4, L.diag, L.active, x, L.b, L.r);
 }
 
 // b of the next level = R r, its x = 0.
-__global__ void batch_restrict(const BatchLevel *__restrict__ E, const int *__restrict__ start,
+__global__ void batch_restrict(const BatchLevel *__restrict__ E, const int *__restrict__ ids,
+                               const int *__restrict__ start,
                                int ne, const uint8_t *__restrict__ live) {
-    const int e = find_entry(start, ne, blockIdx.x);
-    const BatchLevel &L = E[e];
+    const int slot = find_entry(start, ne, blockIdx.x);
+    const BatchLevel &L = E[ids[slot]];
     if (!live[L.cand]) return;
-    const i64 t = ((i64)blockIdx.x - start[e]) * kBatchThreads + threadIdx.x;
+    const i64 t = ((i64)blockIdx.x - start[slot]) * kBatchThreads + threadIdx.x;
     if (t >= L.ncn) return;
     restrict_item(t, L.F, L.r, L.bc, L.xc, PlainLoad{});
 }
 
 // Every candidate's coarse levels, one block each.
 __global__ void __launch_bounds__(kTailThreads, 1)
-    batch_tail(const BatchTail *__restrict__ T, const uint8_t *__restrict__ live) {
-    const BatchTail &t = T[blockIdx.x];
+    batch_tail(const BatchTail *__restrict__ T, const int *__restrict__ ids,
+               const uint8_t *__restrict__ live) {
+    const BatchTail &t = T[ids[blockIdx.x]];
     if (!live[t.cand]) return;
     vcycle_tail_run(t.levels, t.plans, t.count, t.image, t.words, t.doubles, t.ints, t.inv,
                     t.sweeps);
@@ -2338,12 +2343,13 @@ __device__ __forceinline__ void block_sums(double a, double b, double *__restric
 
 // The right-hand side and the held potentials (prepare), then r0 = b - A phi (a second
 // launch: it reads the neighbours' held values).
-__global__ void batch_prepare(const BatchFine *__restrict__ E, const int *__restrict__ start,
+__global__ void batch_prepare(const BatchFine *__restrict__ E, const int *__restrict__ ids,
+                              const int *__restrict__ start,
                               int ne, const uint8_t *__restrict__ live) {
-    const int e = find_entry(start, ne, blockIdx.x);
-    const BatchFine &F = E[e];
+    const int slot = find_entry(start, ne, blockIdx.x);
+    const BatchFine &F = E[ids[slot]];
     if (!live[F.cand]) return;
-    const i64 f = ((i64)blockIdx.x - start[e]) * kBatchThreads + threadIdx.x;
+    const i64 f = ((i64)blockIdx.x - start[slot]) * kBatchThreads + threadIdx.x;
     if (f >= F.n) return;
     if (F.active[f]) {
         F.b[f] = (F.rho ? F.rho[f] / kEps0 : 0.0) + F.src[f];
@@ -2354,12 +2360,13 @@ __global__ void batch_prepare(const BatchFine *__restrict__ E, const int *__rest
 }
 
 // r0 = b - A phi, the V-cycle's first input r0, d = 0; the partial sums of |b|^2, |r0|^2.
-__global__ void batch_initial(const BatchFine *__restrict__ E, const int *__restrict__ start,
+__global__ void batch_initial(const BatchFine *__restrict__ E, const int *__restrict__ ids,
+                              const int *__restrict__ start,
                               int ne, const uint8_t *__restrict__ live, double *__restrict__ part) {
-    const int e = find_entry(start, ne, blockIdx.x);
-    const BatchFine &F = E[e];
+    const int slot = find_entry(start, ne, blockIdx.x);
+    const BatchFine &F = E[ids[slot]];
     if (!live[F.cand]) return;
-    const i64 f = ((i64)blockIdx.x - start[e]) * kBatchThreads + threadIdx.x;
+    const i64 f = ((i64)blockIdx.x - start[slot]) * kBatchThreads + threadIdx.x;
     double bb = 0.0, rr = 0.0;
     if (f < F.n) {
         const double r = apply5_item(f, F.nx, F.ny, F.c4, F.diag, F.active, F.phi, F.b, F.r0);
@@ -2373,23 +2380,25 @@ __global__ void batch_initial(const BatchFine *__restrict__ E, const int *__rest
 }
 
 // d += the V-cycle's correction.
-__global__ void batch_correct(const BatchFine *__restrict__ E, const int *__restrict__ start,
+__global__ void batch_correct(const BatchFine *__restrict__ E, const int *__restrict__ ids,
+                              const int *__restrict__ start,
                               int ne, const uint8_t *__restrict__ live) {
-    const int e = find_entry(start, ne, blockIdx.x);
-    const BatchFine &F = E[e];
+    const int slot = find_entry(start, ne, blockIdx.x);
+    const BatchFine &F = E[ids[slot]];
     if (!live[F.cand]) return;
-    const i64 f = ((i64)blockIdx.x - start[e]) * kBatchThreads + threadIdx.x;
+    const i64 f = ((i64)blockIdx.x - start[slot]) * kBatchThreads + threadIdx.x;
     if (f < F.n) F.d[f] += F.vx[f];
 }
 
 // The true residual r = r0 - A d as the next V-cycle's input; the partial sums of |r|^2.
-__global__ void batch_residual0(const BatchFine *__restrict__ E, const int *__restrict__ start,
+__global__ void batch_residual0(const BatchFine *__restrict__ E, const int *__restrict__ ids,
+                              const int *__restrict__ start,
                                 int ne, const uint8_t *__restrict__ live,
                                 double *__restrict__ part) {
-    const int e = find_entry(start, ne, blockIdx.x);
-    const BatchFine &F = E[e];
+    const int slot = find_entry(start, ne, blockIdx.x);
+    const BatchFine &F = E[ids[slot]];
     if (!live[F.cand]) return;
-    const i64 f = ((i64)blockIdx.x - start[e]) * kBatchThreads + threadIdx.x;
+    const i64 f = ((i64)blockIdx.x - start[slot]) * kBatchThreads + threadIdx.x;
     double rr = 0.0;
     if (f < F.n) {
         const double r = apply5_item(f, F.nx, F.ny, F.c4, F.diag, F.active, F.d, F.r0, F.vb);
@@ -2399,12 +2408,13 @@ __global__ void batch_residual0(const BatchFine *__restrict__ E, const int *__re
 }
 
 // phi += d.
-__global__ void batch_finish(const BatchFine *__restrict__ E, const int *__restrict__ start,
+__global__ void batch_finish(const BatchFine *__restrict__ E, const int *__restrict__ ids,
+                              const int *__restrict__ start,
                              int ne, const uint8_t *__restrict__ solving) {
-    const int e = find_entry(start, ne, blockIdx.x);
-    const BatchFine &F = E[e];
+    const int slot = find_entry(start, ne, blockIdx.x);
+    const BatchFine &F = E[ids[slot]];
     if (!solving[F.cand]) return;
-    const i64 f = ((i64)blockIdx.x - start[e]) * kBatchThreads + threadIdx.x;
+    const i64 f = ((i64)blockIdx.x - start[slot]) * kBatchThreads + threadIdx.x;
     if (f < F.n) F.phi[f] += F.d[f];
 }
 
@@ -2413,16 +2423,19 @@ __global__ void batch_finish(const BatchFine *__restrict__ E, const int *__restr
 // after the cycle, and whether the candidate stops -- at the goal, or after three cycles
 // that did not halve its best residual (its rounding floor).  state[4 e ..]: goal, best,
 // last residual, cycles without halving; cycles[e]: the cycles it ran.
-__global__ void batch_check(const BatchFine *__restrict__ E, const int *__restrict__ start,
+__global__ void batch_check(const BatchFine *__restrict__ E, const int *__restrict__ ids,
+                              const int *__restrict__ start,
                             int ne, const double *__restrict__ part, double tol, int cycle,
                             uint8_t *__restrict__ live, double *__restrict__ state,
                             int32_t *__restrict__ cycles, int32_t *__restrict__ remaining) {
-    const int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (e >= ne) return;
+    if (slot >= ne) return;
+    const int e = ids[slot];
     const BatchFine &F = E[e];
     if (!live[F.cand]) return;
-    const int b0 = start[e], b1 = e + 1 < ne ? start[e + 1] : b0 + (int)((F.n + kBatchThreads - 1) / kBatchThreads);
+    const int b0 = start[slot];
+    const int b1 = slot + 1 < ne ? start[slot + 1] : b0 + (int)((F.n + kBatchThreads - 1) / kBatchThreads);
     double s0 = 0.0, s1 = 0.0;
     for (int k = b0 + lane; k < b1; k += 32) {
         s0 += part[2 * k];
@@ -2466,25 +2479,43 @@ __global__ void batch_check(const BatchFine *__restrict__ E, const int *__restri
 }  // namespace
 }  // namespace bt
 
+
 struct bt_poisson_batch {
     bt_ctx *ctx = nullptr;
     std::vector<bt_poisson *> solvers;
     std::vector<i64> offset;  // each candidate's first node in the batch's arrays
     int steps = 0;            // level steps above the tails
-    // per step: the entries and, per kind of launch, each entry's first block
+    // A level step: all its entries (device) with their candidates and block counts (host),
+    // and the launch tables of the entries whose candidates are live: their numbers and,
+    // per kind of launch, each one's first block.
     struct Step {
-        bt::Buffer entries, smooth_start, node_start, coarse_start;
+        bt::Buffer entries;
+        std::vector<int> cand, nx, ny, nodes, coarse;
+        bt::Buffer ids, smooth_start, node_start, coarse_start;
         int n = 0, smooth_blocks = 0, node_blocks = 0, coarse_blocks = 0;
     };
     std::vector<Step> level;
-    bt::Buffer tails;
+    bt::Buffer tails, tail_ids;  // one block per live candidate
+    int n_tails = 0;
     size_t tail_smem = 0;
-    bt::Buffer fine, fine_start;
+    bt::Buffer fine, fine_ids, fine_start;
     std::vector<bt::BatchFine> fine_host;  // the device table's copy
-    int fine_blocks = 0;
+    std::vector<int> fine_nodes;           // blocks of each candidate's finest level
+    int n_fine = 0, fine_blocks = 0;
+    std::vector<uint8_t> compacted;        // the live set of the launch tables
     bt::Buffer live, solving, part, state, cycles, remaining;
     bt::HostBuffer host;
     int fine_sweeps = 2, coarse_sweeps = 2;
+    // The smoothing tiles (interior nodes along x and y) of level 0 and of the 9-point
+    // levels, and the launches a 9-point smoothing is split into (1 or 2); chosen by timing
+    // at the first solve unless set (tuned == false: still to be chosen).
+    int tile5[2] = {32, 32}, tile9[2] = {16, 32}, split9 = 1;
+    bool tuned = false;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ~bt_poisson_batch() {
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+    }
 };
 
 namespace bt {
@@ -2497,11 +2528,124 @@ void upload(Buffer &dst, const std::vector<T> &src, cudaStream_t st) {
                             cudaMemcpyHostToDevice, st));
 }
 
-// The staged 5-point smoother's nodes a thread per colour for `count` phases (as smooth()).
-int fine_own(int count) {
+// The launch tables of the candidates flagged in `alive` (host): the finished ones launch
+// no blocks.  Queued on the stream, after the launches that read the old tables.
+void compact(bt_poisson_batch *B, const uint8_t *alive) {
+    cudaStream_t st = B->ctx->stream;
+    const int count = (int)B->solvers.size();
+    for (auto &S : B->level) {
+        std::vector<int> ids, smooth, node, coarse;
+        int sb = 0, nb = 0, cb = 0;
+        const bool five = &S == &B->level[0];
+        const int tx = five ? B->tile5[0] : B->tile9[0], ty = five ? B->tile5[1] : B->tile9[1];
+        for (int e = 0; e < (int)S.cand.size(); ++e) {
+            if (!alive[S.cand[e]]) continue;
+            ids.push_back(e);
+            smooth.push_back(sb);
+            node.push_back(nb);
+            coarse.push_back(cb);
+            sb += ((S.nx[e] + tx - 1) / tx) * ((S.ny[e] + ty - 1) / ty);
+            nb += S.nodes[e];
+            cb += S.coarse[e];
+        }
+        S.n = (int)ids.size();
+        S.smooth_blocks = sb;
+        S.node_blocks = nb;
+        S.coarse_blocks = cb;
+        upload(S.ids, ids, st);
+        upload(S.smooth_start, smooth, st);
+        upload(S.node_start, node, st);
+        upload(S.coarse_start, coarse, st);
+    }
+    std::vector<int> tails, fine, start;
+    int fb = 0;
+    for (int c = 0; c < count; ++c) {
+        if (!alive[c]) continue;
+        tails.push_back(c);
+        fine.push_back(c);
+        start.push_back(fb);
+        fb += B->fine_nodes[c];
+    }
+    B->n_tails = (int)tails.size();
+    B->n_fine = (int)fine.size();
+    B->fine_blocks = fb;
+    upload(B->tail_ids, tails, st);
+    upload(B->fine_ids, fine, st);
+    upload(B->fine_start, start, st);
+    B->compacted.assign(alive, alive + count);
+}
+
+// The staged smoother's nodes a thread per colour for a tile (tx, ty) and `count` phases.
+int stage_own(bool nine, int tx, int ty, int count) {
     const int halo = stage_halo(count);
-    const int per = (kStage5X + 2 * halo) * (kStage5Y + 2 * halo) / 2;
+    const int per = (tx + 2 * halo) * (ty + 2 * halo) / (nine ? 4 : 2);
     return (per + kStageThreads - 1) / kStageThreads;
+}
+
+int fine_own(int count) { return stage_own(false, kStage5X, kStage5Y, count); }
+
+Phases batch_phases(int sweeps, int colours, bool pre, int first, int count) {
+    Phases ph{};
+    std::vector<int> order;
+    for (int s = 0; s < sweeps; ++s)
+        for (int c = 0; c < colours; ++c) order.push_back(pre ? c : colours - 1 - c);
+    ph.count = count;
+    for (int k = 0; k < count; ++k) ph.colour[k] = order[first + k];
+    return ph;
+}
+
+// One staged launch over step l's live entries: phases [first, first + count) of the
+// smoothing, from buffer `from` into the other.
+void batch_smooth_launch(bt_poisson_batch *B, int l, bool pre, int first, int count, int from,
+                         int prolong, int zero_in) {
+    bt_ctx *ctx = B->ctx;
+    auto &S = B->level[l];
+    const bool nine = l > 0;
+    const uint8_t *live = B->live.as<uint8_t>(B->solvers.size());
+    const BatchLevel *E = S.entries.as<BatchLevel>(S.cand.size());
+    const int *ids = S.ids.as<int>(S.n), *start = S.smooth_start.as<int>(S.n);
+    const int tx = nine ? B->tile9[0] : B->tile5[0], ty = nine ? B->tile9[1] : B->tile5[1];
+    const Phases ph = batch_phases(nine ? B->coarse_sweeps : B->fine_sweeps, nine ? 4 : 2, pre,
+                                   first, count);
+    const size_t smem = stage_smem(nine, tx, ty, stage_halo(count));
+    const int own = stage_own(nine, tx, ty, count);
+#define BT_BATCH_SMOOTH(N, R)                                                                 \
+    BT_LAUNCH(ctx, (batch_smooth<N, R>), S.smooth_blocks, kStageThreads, smem, ctx->stream, E, \
+              ids, start, S.n, live, tx, ty, ph, from, prolong, zero_in)
+    if (!nine && own == 1)
+        BT_BATCH_SMOOTH(false, 1);
+    else if (!nine && own == 2)
+        BT_BATCH_SMOOTH(false, 2);
+    else if (!nine && own == 3)
+        BT_BATCH_SMOOTH(false, 3);
+    else if (nine && own == 1)
+        BT_BATCH_SMOOTH(true, 1);
+    else if (nine && own == 2)
+        BT_BATCH_SMOOTH(true, 2);
+    else
+        BT_REQUIRE(false, "poisson batch: a smoothing tile too large for its block");
+#undef BT_BATCH_SMOOTH
+}
+
+// The smoothing of step l's live entries before (pre) or after the coarse correction;
+// returns the buffer that holds the result (0: x, 1: x2).  Level 0's pre-smoothing starts
+// from zero; the post-smoothing adds the prolonged correction as it reads.  Before the
+// correction the input is the pre-smoothing's result `from`.
+int batch_smooth_step(bt_poisson_batch *B, int l, bool pre, int from = 0) {
+    auto &S = B->level[l];
+    if (S.n == 0) return from;
+    const bool nine = l > 0;
+    const int phases = nine ? 4 * B->coarse_sweeps : 2 * B->fine_sweeps;
+    const int split = nine ? B->split9 : 1;
+    const int per = (phases + split - 1) / split;
+    int in = pre ? 0 : from;
+    for (int first = 0, k = 0; first < phases; first += per, ++k) {
+        const int count = std::min(per, phases - first);
+        batch_smooth_launch(B, l, pre, first, count, in, (!pre && k == 0) ? 1 : 0,
+                            (pre && k == 0 && !nine) ? 1 : 0);
+        in ^= 1;
+    }
+    return in;
 }
 
 // One V-cycle of every live candidate: level 0's b (its residual) into level 0's x.
@@ -2509,61 +2653,100 @@ void batch_vcycle(bt_poisson_batch *B) {
     bt_ctx *ctx = B->ctx;
     cudaStream_t st = ctx->stream;
     const uint8_t *live = B->live.as<uint8_t>(B->solvers.size());
-    auto phases = [](int sweeps, int colours, bool pre) {
-        Phases ph{};
-        ph.count = sweeps * colours;
-        int k = 0;
-        for (int s = 0; s < sweeps; ++s)
-            for (int c = 0; c < colours; ++c) ph.colour[k++] = pre ? c : colours - 1 - c;
-        return ph;
-    };
+    std::vector<int> held(B->steps, 0);  // where each step's pre-smoothing left x
     for (int l = 0; l < B->steps; ++l) {
         auto &S = B->level[l];
-        const BatchLevel *E = S.entries.as<BatchLevel>(S.n);
-        if (l == 0) {
-            const Phases ph = phases(B->fine_sweeps, 2, true);
-            const size_t smem = stage_smem(false, kStage5X, kStage5Y, stage_halo(ph.count));
-            if (fine_own(ph.count) <= 2)
-                BT_LAUNCH(ctx, (batch_smooth<false, 2>), S.smooth_blocks, kStageThreads, smem, st,
-                          E, S.smooth_start.as<int>(S.n), S.n, live, kStage5X, kStage5Y, ph, 0);
-            else
-                BT_LAUNCH(ctx, (batch_smooth<false, 3>), S.smooth_blocks, kStageThreads, smem, st,
-                          E, S.smooth_start.as<int>(S.n), S.n, live, kStage5X, kStage5Y, ph, 0);
-            BT_LAUNCH(ctx, batch_residual<false>, S.node_blocks, kBatchThreads, 0, st, E,
-                      S.node_start.as<int>(S.n), S.n, live);
-        } else {
-            const Phases ph = phases(B->coarse_sweeps, 4, true);
-            BT_LAUNCH(ctx, (batch_smooth<true, 1>), S.smooth_blocks, kStageThreads,
-                      stage_smem(true, kStage9X, kStage9Y, stage_halo(ph.count)), st, E,
-                      S.smooth_start.as<int>(S.n), S.n, live, kStage9X, kStage9Y, ph, 0);
-            BT_LAUNCH(ctx, batch_residual<true>, S.node_blocks, kBatchThreads, 0, st, E,
-                      S.node_start.as<int>(S.n), S.n, live);
-        }
-        BT_LAUNCH(ctx, batch_restrict, S.coarse_blocks, kBatchThreads, 0, st, E,
+        if (S.n == 0) continue;
+        const BatchLevel *E = S.entries.as<BatchLevel>(S.cand.size());
+        const int *ids = S.ids.as<int>(S.n);
+        held[l] = batch_smooth_step(B, l, true);
+        if (l == 0)
+            BT_LAUNCH(ctx, batch_residual<false>, S.node_blocks, kBatchThreads, 0, st, E, ids,
+                      S.node_start.as<int>(S.n), S.n, live, held[l]);
+        else
+            BT_LAUNCH(ctx, batch_residual<true>, S.node_blocks, kBatchThreads, 0, st, E, ids,
+                      S.node_start.as<int>(S.n), S.n, live, held[l]);
+        BT_LAUNCH(ctx, batch_restrict, S.coarse_blocks, kBatchThreads, 0, st, E, ids,
                   S.coarse_start.as<int>(S.n), S.n, live);
     }
-    BT_LAUNCH(ctx, batch_tail, (unsigned)B->solvers.size(), kTailThreads, B->tail_smem, st,
-              B->tails.as<BatchTail>(B->solvers.size()), live);
+    if (B->n_tails)
+        BT_LAUNCH(ctx, batch_tail, (unsigned)B->n_tails, kTailThreads, B->tail_smem, st,
+                  B->tails.as<BatchTail>(B->solvers.size()), B->tail_ids.as<int>(B->n_tails),
+                  live);
     for (int l = B->steps - 1; l >= 0; --l) {
-        auto &S = B->level[l];
-        const BatchLevel *E = S.entries.as<BatchLevel>(S.n);
-        if (l == 0) {
-            const Phases ph = phases(B->fine_sweeps, 2, false);
-            const size_t smem = stage_smem(false, kStage5X, kStage5Y, stage_halo(ph.count));
-            if (fine_own(ph.count) <= 2)
-                BT_LAUNCH(ctx, (batch_smooth<false, 2>), S.smooth_blocks, kStageThreads, smem, st,
-                          E, S.smooth_start.as<int>(S.n), S.n, live, kStage5X, kStage5Y, ph, 1);
-            else
-                BT_LAUNCH(ctx, (batch_smooth<false, 3>), S.smooth_blocks, kStageThreads, smem, st,
-                          E, S.smooth_start.as<int>(S.n), S.n, live, kStage5X, kStage5Y, ph, 1);
-        } else {
-            const Phases ph = phases(B->coarse_sweeps, 4, false);
-            BT_LAUNCH(ctx, (batch_smooth<true, 1>), S.smooth_blocks, kStageThreads,
-                      stage_smem(true, kStage9X, kStage9Y, stage_halo(ph.count)), st, E,
-                      S.smooth_start.as<int>(S.n), S.n, live, kStage9X, kStage9Y, ph, 1);
-        }
+        // the post-smoothing must leave x in the level's x buffer (the next coarser level's
+        // x, or level 0's output)
+        const int at = batch_smooth_step(B, l, false, held[l]);
+        BT_REQUIRE(B->level[l].n == 0 || at == 0, "poisson batch: smoothing left x in x2");
     }
     BT_CHECK_LAUNCH();
+}
+
+}  // namespace
+}  // namespace bt
+
+namespace bt {
+namespace {
+
+// The project's autotuner of the batched V-cycle: the staged smoothing tiles of level 0 and
+// of the 9-point levels (and whether a 9-point smoothing is one launch of all its phases,
+// with a halo as wide as them, or two of half as many), timed on this batch's own V-cycle
+// (two cycles each, CUDA events on the stream) from the residual of its first solve; the
+// fastest is kept.  The choices trade a tile's re-read halo against blocks per SM.
+void tune_tiling(bt_poisson_batch *B) {
+    cudaStream_t st = B->ctx->stream;
+    const std::vector<uint8_t> set = B->compacted;
+    auto time_cycle = [&]() {
+        compact(B, set.data());
+        BT_CUDA(cudaEventRecord(B->ev[0], st));
+        for (int k = 0; k < 2; ++k) batch_vcycle(B);
+        BT_CUDA(cudaEventRecord(B->ev[1], st));
+        BT_CUDA(cudaEventSynchronize(B->ev[1]));
+        float ms = 0.0f;
+        BT_CUDA(cudaEventElapsedTime(&ms, B->ev[0], B->ev[1]));
+        return ms;
+    };
+    const int tiles5[][2] = {{32, 32}, {32, 16}, {16, 32}, {64, 16}};
+    float best = 1e30f;
+    int pick5[2] = {B->tile5[0], B->tile5[1]};
+    for (const auto &t : tiles5) {
+        if (stage_own(false, t[0], t[1], 2 * B->fine_sweeps) > 3) continue;
+        B->tile5[0] = t[0];
+        B->tile5[1] = t[1];
+        const float ms = time_cycle();
+        if (ms < best) {
+            best = ms;
+            pick5[0] = t[0];
+            pick5[1] = t[1];
+        }
+    }
+    B->tile5[0] = pick5[0];
+    B->tile5[1] = pick5[1];
+    const int tiles9[][3] = {{16, 32, 1}, {16, 32, 2}, {16, 16, 2}, {32, 16, 2}, {32, 32, 2}};
+    best = 1e30f;
+    int pick9[3] = {B->tile9[0], B->tile9[1], B->split9};
+    for (const auto &t : tiles9) {
+        const int phases = 4 * B->coarse_sweeps;
+        const int count = (phases + t[2] - 1) / t[2];
+        if (stage_own(true, t[0], t[1], count) > 2 ||
+            stage_smem(true, t[0], t[1], stage_halo(count)) > 200 * 1024)
+            continue;
+        B->tile9[0] = t[0];
+        B->tile9[1] = t[1];
+        B->split9 = t[2];
+        const float ms = time_cycle();
+        if (ms < best) {
+            best = ms;
+            pick9[0] = t[0];
+            pick9[1] = t[1];
+            pick9[2] = t[2];
+        }
+    }
+    B->tile9[0] = pick9[0];
+    B->tile9[1] = pick9[1];
+    B->split9 = pick9[2];
+    compact(B, set.data());
+    B->tuned = true;
 }
 
 }  // namespace
@@ -2581,6 +2764,7 @@ extern "C" int bt_poisson_batch_create(bt_ctx *ctx, bt_poisson *const *solvers, 
             B->solvers.assign(solvers, solvers + count);
             B->offset.assign(offset, offset + count);
             bt_poisson *first = B->solvers[0];
+            BT_REQUIRE(first, "poisson batch: null solver");
             B->fine_sweeps = first->fine_sweeps;
             B->coarse_sweeps = first->coarse_sweeps;
             for (i64 c = 0; c < count; ++c) {
@@ -2603,10 +2787,8 @@ extern "C" int bt_poisson_batch_create(bt_ctx *ctx, bt_poisson *const *solvers, 
             B->level.resize(B->steps);
             for (int l = 0; l < B->steps; ++l) {
                 std::vector<bt::BatchLevel> E;
-                std::vector<int> smooth, node, coarse;
-                int sb = 0, nb = 0, cb = 0;
+                auto &S = B->level[l];
                 const bool five = l == 0;
-                const int tx = five ? bt::kStage5X : bt::kStage9X, ty = five ? bt::kStage5Y : bt::kStage9Y;
                 for (i64 c = 0; c < count; ++c) {
                     bt_poisson *p = B->solvers[c];
                     if (l >= p->tail_start) continue;
@@ -2632,27 +2814,17 @@ extern "C" int bt_poisson_batch_create(bt_ctx *ctx, bt_poisson *const *solvers, 
                     e.bc = C.b.as<double>(C.n);
                     e.ncn = C.n;
                     E.push_back(e);
-                    smooth.push_back(sb);
-                    node.push_back(nb);
-                    coarse.push_back(cb);
-                    sb += (int)(((L.nx + tx - 1) / tx) * ((L.ny + ty - 1) / ty));
-                    nb += (int)bt::blocks_for(L.n, bt::kBatchThreads);
-                    cb += (int)bt::blocks_for(C.n, bt::kBatchThreads);
+                    S.cand.push_back((int)c);
+                    S.nx.push_back((int)L.nx);
+                    S.ny.push_back((int)L.ny);
+                    S.nodes.push_back((int)bt::blocks_for(L.n, bt::kBatchThreads));
+                    S.coarse.push_back((int)bt::blocks_for(C.n, bt::kBatchThreads));
                 }
-                auto &S = B->level[l];
-                S.n = (int)E.size();
-                S.smooth_blocks = sb;
-                S.node_blocks = nb;
-                S.coarse_blocks = cb;
                 bt::upload(S.entries, E, st);
-                bt::upload(S.smooth_start, smooth, st);
-                bt::upload(S.node_start, node, st);
-                bt::upload(S.coarse_start, coarse, st);
             }
             std::vector<bt::BatchTail> T;
             std::vector<bt::BatchFine> F;
-            std::vector<int> fine_start;
-            int fb = 0;
+            int all_blocks = 0;
             for (i64 c = 0; c < count; ++c) {
                 bt_poisson *p = B->solvers[c];
                 const int first_tail = p->tail_start;
@@ -2688,29 +2860,27 @@ extern "C" int bt_poisson_batch_create(bt_ctx *ctx, bt_poisson *const *solvers, 
                 f.vb = L0.b.as<double>(n);
                 f.vx = L0.x.as<double>(n);
                 F.push_back(f);
-                fine_start.push_back(fb);
-                fb += (int)bt::blocks_for(n, bt::kBatchThreads);
+                B->fine_nodes.push_back((int)bt::blocks_for(n, bt::kBatchThreads));
+                all_blocks += B->fine_nodes.back();
             }
-            B->fine_blocks = fb;
             B->fine_host = F;
             bt::upload(B->tails, T, st);
             bt::upload(B->fine, F, st);
             {
-                const int big5 = (int)bt::stage_smem(false, bt::kStage5X, bt::kStage5Y, bt::kMaxPhases);
-                const int big9 = (int)bt::stage_smem(true, bt::kStage9X, bt::kStage9Y, bt::kMaxPhases);
-                BT_CUDA(cudaFuncSetAttribute(bt::batch_smooth<false, 2>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, big5));
-                BT_CUDA(cudaFuncSetAttribute(bt::batch_smooth<false, 3>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, big5));
-                BT_CUDA(cudaFuncSetAttribute(bt::batch_smooth<true, 1>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, big9));
+                // the largest staged tile the tuner tries (bt::tune_tiling)
+                const int big = 200 * 1024;
+                BT_CUDA(cudaFuncSetAttribute(bt::batch_smooth<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+                BT_CUDA(cudaFuncSetAttribute(bt::batch_smooth<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+                BT_CUDA(cudaFuncSetAttribute(bt::batch_smooth<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+                BT_CUDA(cudaFuncSetAttribute(bt::batch_smooth<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+                BT_CUDA(cudaFuncSetAttribute(bt::batch_smooth<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
                 BT_CUDA(cudaFuncSetAttribute(bt::batch_tail, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)bt::kTailSmemMax));
             }
-            bt::upload(B->fine_start, fine_start, st);
+            for (auto &e : B->ev) BT_CUDA(cudaEventCreate(&e));
             B->live.as<uint8_t>(count);
             B->solving.as<uint8_t>(count);
-            B->part.as<double>(2 * (size_t)fb);
+            B->part.as<double>(2 * (size_t)all_blocks);
             B->state.as<double>(4 * (size_t)count);
             B->cycles.as<int32_t>(count);
             B->remaining.as<int32_t>(1);
@@ -2742,7 +2912,7 @@ extern "C" int bt_poisson_batch_solve(bt_poisson_batch *B, double *phi, const do
         cudaStream_t st = ctx->stream;
         const i64 count = (i64)B->solvers.size();
         bt::Timed timed(ctx, "field_solve");
-        // every member's hierarchy of its plain operator; the batch's arrays in its entries
+        // every member's hierarchy of its plain operator
         int members_n = 0;
         for (i64 c = 0; c < count; ++c) {
             if (!members[c]) continue;
@@ -2769,37 +2939,53 @@ extern "C" int bt_poisson_batch_solve(bt_poisson_batch *B, double *phi, const do
         BT_CUDA(cudaMemcpyAsync(live, members, count, cudaMemcpyHostToDevice, st));
         BT_CUDA(cudaMemcpyAsync(solving, members, count, cudaMemcpyHostToDevice, st));
         int32_t *remaining = B->remaining.as<int32_t>(1);
-        int32_t *host_remaining = static_cast<int32_t *>(B->host.get(64));
+        uint8_t *flags = static_cast<uint8_t *>(B->host.get((size_t)count + 64));
+        int32_t *host_remaining = reinterpret_cast<int32_t *>(flags + ((count + 15) / 16) * 16);
         *host_remaining = members_n;
         BT_CUDA(cudaMemcpyAsync(remaining, host_remaining, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        bt::compact(B, members);
         const bt::BatchFine *F = B->fine.as<bt::BatchFine>(count);
-        const int *fs = B->fine_start.as<int>(count);
-        double *part = B->part.as<double>(2 * (size_t)B->fine_blocks);
+        double *part = B->part.as<double>(1);
         double *state = B->state.as<double>(4 * (size_t)count);
         int32_t *cyc = B->cycles.as<int32_t>(count);
-        const int fb = B->fine_blocks, T = bt::kBatchThreads, ne = (int)count;
-        const unsigned check_blocks = bt::blocks_for(count * 32, 256);
-        BT_LAUNCH(ctx, bt::batch_prepare, fb, T, 0, st, F, fs, ne, live);
-        BT_LAUNCH(ctx, bt::batch_initial, fb, T, 0, st, F, fs, ne, live, part);
-        BT_LAUNCH(ctx, bt::batch_check, check_blocks, 256, 0, st, F, fs, ne, part, tol, 0, live,
-                  state, cyc, remaining);
+        const int T = bt::kBatchThreads;
+        auto fine_launch = [&](auto kernel, auto... more) {
+            if (B->fine_blocks)
+                BT_LAUNCH(ctx, kernel, B->fine_blocks, T, 0, st, F, B->fine_ids.as<int>(B->n_fine),
+                          B->fine_start.as<int>(B->n_fine), B->n_fine, more...);
+        };
+        auto check = [&](int cycle) {
+            BT_LAUNCH(ctx, bt::batch_check, bt::blocks_for((i64)B->n_fine * 32, 256), 256, 0, st, F,
+                      B->fine_ids.as<int>(B->n_fine), B->fine_start.as<int>(B->n_fine),
+                      B->n_fine, (const double *)part, tol, cycle, live, state, cyc, remaining);
+        };
+        fine_launch(bt::batch_prepare, (const uint8_t *)live);
+        fine_launch(bt::batch_initial, (const uint8_t *)live, part);
+        check(0);
         BT_CHECK_LAUNCH();
+        if (!B->tuned) bt::tune_tiling(B);
         for (int cycle = 1; cycle <= max_cycles; ++cycle) {
-            BT_CUDA(cudaMemcpyAsync(host_remaining, remaining, sizeof(int32_t),
-                                    cudaMemcpyDeviceToHost, st));
+            BT_CUDA(cudaMemcpyAsync(flags, live, count, cudaMemcpyDeviceToHost, st));
             BT_CUDA(cudaStreamSynchronize(st));
-            if (*host_remaining <= 0) break;
+            int alive = 0, before = 0;
+            for (i64 c = 0; c < count; ++c) {
+                alive += flags[c] != 0;
+                before += B->compacted[c] != 0;
+            }
+            if (alive == 0) break;
+            // launch tables of the live candidates only, once enough of them have finished
+            if (10 * alive <= 9 * before) bt::compact(B, flags);
             {
                 bt::Timed vt(ctx, "vcycle");
                 bt::batch_vcycle(B);
             }
-            BT_LAUNCH(ctx, bt::batch_correct, fb, T, 0, st, F, fs, ne, live);
-            BT_LAUNCH(ctx, bt::batch_residual0, fb, T, 0, st, F, fs, ne, live, part);
-            BT_LAUNCH(ctx, bt::batch_check, check_blocks, 256, 0, st, F, fs, ne, part, tol, cycle,
-                      live, state, cyc, remaining);
+            fine_launch(bt::batch_correct, (const uint8_t *)live);
+            fine_launch(bt::batch_residual0, (const uint8_t *)live, part);
+            check(cycle);
             BT_CHECK_LAUNCH();
         }
-        BT_LAUNCH(ctx, bt::batch_finish, fb, T, 0, st, F, fs, ne, solving);
+        bt::compact(B, members);
+        fine_launch(bt::batch_finish, (const uint8_t *)solving);
         BT_CHECK_LAUNCH();
         std::vector<double> S(4 * count);
         std::vector<int32_t> C(count);
@@ -2814,5 +3000,40 @@ extern "C" int bt_poisson_batch_solve(bt_poisson_batch *B, double *phi, const do
             if (!(S[4 * c + 2] <= 1e4 * S[4 * c]))
                 throw bt::Error{BT_ERR_NOCONV, "batched field solve: a candidate did not reach the tolerance"};
         }
+    });
+}
+
+extern "C" int bt_poisson_batch_tiling(bt_poisson_batch *B, int32_t set, int32_t *tiling) {
+    return bt::guarded([&] {
+        BT_REQUIRE(B && tiling, "poisson batch: null argument");
+        if (set) {
+            if (tiling[0] <= 0) {
+                B->tuned = false;
+                return;
+            }
+            for (int q = 0; q < 5; ++q)
+                BT_REQUIRE(tiling[q] > 0, "poisson batch: tile sizes and split must be positive");
+            BT_REQUIRE(tiling[4] <= 2, "poisson batch: a 9-point smoothing splits into 1 or 2 launches");
+            const int phases9 = 4 * B->coarse_sweeps, count9 = (phases9 + tiling[4] - 1) / tiling[4];
+            BT_REQUIRE(bt::stage_own(false, tiling[0], tiling[1], 2 * B->fine_sweeps) <= 3 &&
+                           bt::stage_smem(false, tiling[0], tiling[1], bt::stage_halo(2 * B->fine_sweeps)) <= 200 * 1024,
+                       "poisson batch: the level-0 tile is too large for its block");
+            BT_REQUIRE(bt::stage_own(true, tiling[2], tiling[3], count9) <= 2 &&
+                           bt::stage_smem(true, tiling[2], tiling[3], bt::stage_halo(count9)) <= 200 * 1024,
+                       "poisson batch: the 9-point tile is too large for its block");
+            B->tile5[0] = tiling[0];
+            B->tile5[1] = tiling[1];
+            B->tile9[0] = tiling[2];
+            B->tile9[1] = tiling[3];
+            B->split9 = tiling[4];
+            B->tuned = true;
+            return;
+        }
+        tiling[0] = B->tile5[0];
+        tiling[1] = B->tile5[1];
+        tiling[2] = B->tile9[0];
+        tiling[3] = B->tile9[1];
+        tiling[4] = B->split9;
+        tiling[5] = B->tuned ? 1 : 0;
     });
 }

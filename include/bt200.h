@@ -390,6 +390,14 @@ int bt_poisson_batch_solve(bt_poisson_batch *batch, double *phi, const double *r
                            const uint8_t *members, double tol, int32_t max_cycles,
                            int32_t *cycles, double *residual);
 
+/* The batched V-cycle's smoothing tiles (HOST tiling[6]): level 0's tile (x, y interior
+ * nodes), the 9-point levels' tile, the launches a 9-point smoothing is split into (1 or 2)
+ * and whether they were chosen (1) or are still to be tuned (0).  set == 0 reads them;
+ * set != 0 fixes the first five (tiling[0] <= 0: tune again at the next solve).  By
+ * default the first solve times a few tilings on the batch's own V-cycle and keeps the
+ * fastest.  No counterpart in the reference. */
+int bt_poisson_batch_tiling(bt_poisson_batch *batch, int32_t set, int32_t *tiling);
+
 /* No counterpart in the reference (the differentiation form).  on != 0: the solver's
  * operator becomes the transpose of the free rows' block, A_ff^T (the neighbour
  * coefficients exchanged between each pair of free nodes, the diagonal kept), so

@@ -99,6 +99,25 @@ def test_batched_field_solve_equals_each_solve():
             assert float((got - alone).abs().max()) <= 1e-9 * scale, (sweep, k)
         assert torch.equal(batch.node_view(batch.phi, 2), keep)
         batch.rho.mul_(1.5)
+    assert batch.poisson_batch.tiling["tuned"]
+
+
+@pytest.mark.parametrize("tiling", [((32, 16), (16, 16), 2), ((64, 16), (32, 32), 2),
+                                    ((16, 32), (16, 32), 1)])
+def test_batched_field_solve_with_every_tiling(tiling):
+    import torch
+
+    batch = _batch(DESIGNS)
+    batch.poisson_batch.set_tiling(*tiling)
+    rng = np.random.default_rng(4)
+    batch.rho.copy_(torch.from_numpy(rng.uniform(0.0, 2e-5, batch.n_nodes)))
+    batch.poisson_batch.solve(batch.phi, batch.rho, range(len(DESIGNS)))
+    assert batch.poisson_batch.tiling["level0"] == tiling[0]
+    for k, c in enumerate(batch.candidates):
+        alone = torch.zeros(c.shape, dtype=torch.float64, device="cuda")
+        c.poisson.solve_device(alone, batch.node_view(batch.rho, k))
+        scale = float(alone.abs().max())
+        assert float((batch.node_view(batch.phi, k) - alone).abs().max()) <= 1e-9 * scale
 
 
 @pytest.mark.parametrize("field", ["batched", "single"])
