@@ -41,14 +41,15 @@ __global__ void radix_hist(const uint32_t *__restrict__ keys, i64 n_host,
     for (int d = threadIdx.x; d < R; d += kThreads) h[d] = 0;
     __syncthreads();
     const i64 base = (i64)blockIdx.x * kTile;
-#pragma unroll 4
-    for (int i = 0; i < kItems; ++i) {
+    uint32_t key[kItems];
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {  // the loads first, all in flight
         const i64 r = base + (i64)i * kThreads + threadIdx.x;
-        if (r < n) {
-            const uint32_t key = keys[r];
-            if (key != skip) atomicAdd(&h[(key >> shift) & (R - 1)], 1u);
-        }
+        key[i] = r < n ? keys[r] : skip;
     }
+#pragma unroll
+    for (int i = 0; i < kItems; ++i)
+        if (key[i] != skip) atomicAdd(&h[(key[i] >> shift) & (R - 1)], 1u);
     __syncthreads();
     for (int d = threadIdx.x; d < R; d += kThreads) hist[(i64)d * nblocks + blockIdx.x] = h[d];
 }
@@ -153,13 +154,19 @@ __global__ void __launch_bounds__(kThreads) radix_scatter(
     const unsigned below = (1u << lane) - 1u;
     uint32_t key[kItems], val[kItems], pos[kItems];
     unsigned valid_mask = 0;  // bit i: item i is sorted
+    // every load of the tile first (all in flight at once), then the ranking
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
         const i64 r = tile + (i64)warp * kPerWarp + (i64)i * 32 + lane;
         key[i] = r < n ? keys_in[r] : skip;
+        val[i] = r < n ? (vals_in ? vals_in[r] : (uint32_t)r) : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        const i64 r = tile + (i64)warp * kPerWarp + (i64)i * 32 + lane;
         const bool valid = r < n && key[i] != skip;
         if (valid) valid_mask |= 1u << i;
-        val[i] = valid ? (vals_in ? vals_in[r] : (uint32_t)r) : 0u;
+        if (!valid) val[i] = 0u;
         const uint32_t d = (key[i] >> shift) & (R - 1);
         const unsigned peers = __match_any_sync(kFull, valid ? d : 0xffffffffu);
         uint32_t *c = count + warp * R + d;

@@ -428,6 +428,9 @@ __device__ __forceinline__ void smooth_staged_tile(
     };
     const i64 i0 = bx * tx - halo, j0 = by * ty - halo;
     const i64 n = nx * ny;
+    // Every array of a node is loaded at once, whether or not the node is active (the
+    // flag selects afterwards): one round trip to memory a node, not two.  An inactive
+    // node's coefficients are stored but never read.
 #pragma unroll 4
     for (int e = tid; e < m; e += nt) {
         const int a = e / wy, c = e - a * wy;
@@ -439,17 +442,24 @@ __device__ __forceinline__ void smooth_staged_tile(
             const i64 f = i * ny + j;
             xv = zero_in ? 0.0 : xin[f];
             av = active[f];
+            const double bf = b[f];
+            if (NINE) {
+                double q9[9];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) q9[q] = a9[(i64)q * n + f];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) coef[q * m + pos] = q9[q];
+            } else {
+                double q5[5];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) q5[q] = c4[(i64)q * n + f];
+                q5[4] = diag[f];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) coef[q * m + pos] = q5[q];
+            }
             if (av) {
                 if (xc) xv = xv + prolong_sum(F, f, xc, PlainLoad{});
-                bv = b[f];
-                if (NINE) {
-#pragma unroll
-                    for (int q = 0; q < 9; ++q) coef[q * m + pos] = a9[(i64)q * n + f];
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) coef[q * m + pos] = c4[(i64)q * n + f];
-                    coef[4 * m + pos] = diag[f];
-                }
+                bv = bf;
             }
         }
         xs[e] = xv;
