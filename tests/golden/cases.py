@@ -199,3 +199,99 @@ def mesh_cases() -> dict[str, dict]:
             faces={"x_min": ("dirichlet", 0.0), "y_min": ("dirichlet", 50.0)},
         ),
     }
+
+
+# -- the 3D tracer --------------------------------------------------------------------------
+
+
+def trace3d_case(
+    integrator: int,
+    refined: bool = False,
+    mirror: bool = False,
+    has_b: bool = False,
+    has_j: bool = False,
+    seed: int = 31,
+    n: int = 32,
+    max_steps: int = 300,
+) -> list:
+    """The 41 positional arguments of ``trace_trajectories_3d`` for one branch combination
+    (non-relativistic: ``inv_c2`` 0)."""
+    rng = np.random.default_rng(seed + 10 * integrator + 3 * int(refined) + 5 * int(mirror))
+    nx, ny, nz, h = 20, 9, 9, 1.0e-3
+    oy = oz = 0.0 if mirror else -4.0e-3
+    patches = [(nx, ny, nz, 0.0, oy, oz, h)]
+    if refined:
+        # a box of half the spacing, finest first
+        patches.insert(0, (15, 9, 9, 6.0e-3, oy + 2.0e-3, oz + 2.0e-3, 0.5 * h))
+    fxs, fys, fzs, patch_int, patch_real = [], [], [], [], []
+    ofx = ofy = ofz = ofn = 0
+    for pnx, pny, pnz, px0, py0, pz0, ph in patches:
+        fxs.append((3.0e5 + 1.5e4 * rng.normal(size=(pnx + 1, pny, pnz))).ravel())
+        fys.append((1.5e4 * rng.normal(size=(pnx, pny + 1, pnz))).ravel())
+        fzs.append((1.5e4 * rng.normal(size=(pnx, pny, pnz + 1))).ravel())
+        patch_int.append((pnx, pny, pnz, ofx, ofy, ofz, pnx * pny * pnz, ofn))
+        patch_real.append((px0, py0, pz0, ph, px0, py0, pz0, px0 + (pnx - 1) * ph,
+                           py0 + (pny - 1) * ph, pz0 + (pnz - 1) * ph))  # fmt: skip
+        ofx += fxs[-1].size
+        ofy += fys[-1].size
+        ofz += fzs[-1].size
+        ofn += pnx * pny * pnz
+    bn = 0.05 * rng.normal(size=(3, nx, ny, nz)) + np.array([0.2, 0.0, 0.0])[:, None, None, None]
+    if not has_b:
+        bn = np.zeros((3, 2, 2, 2))
+    upper = (0.0 + (nx - 1) * h, oy + (ny - 1) * h, oz + (nz - 1) * h)
+    lo = oy + (0.3e-3 if mirror else 1.0e-3)
+    x = np.stack([rng.uniform(0.0, 3.0e-3, n), rng.uniform(lo, upper[1] - 1.0e-3, n),
+                  rng.uniform(lo, upper[2] - 1.0e-3, n)])  # fmt: skip
+    v = np.stack([np.full(n, 3.0e5) + 2.0e4 * rng.normal(size=n),
+                  3.0e4 * rng.normal(size=n), 3.0e4 * rng.normal(size=n)])  # fmt: skip
+    if mirror:
+        # near the symmetry planes and heading across them
+        x[1, : n // 2] = oy + 0.2e-3 * rng.uniform(size=n // 2)
+        v[1, : n // 2] = -2.5 * np.abs(v[1, : n // 2])
+        x[2, n // 2 :] = oz + 0.2e-3 * rng.uniform(size=n - n // 2)
+        v[2, n // 2 :] = -2.5 * np.abs(v[2, n // 2 :])
+    x[:, 0] = (-1.0e-3, 0.5 * (oy + upper[1]), 0.5 * (oz + upper[2]))  # backward at once
+    cells = np.full((nx - 1, ny - 1, nz - 1), -1, dtype=np.int64)
+    cells[12, 2:6, 3] = np.arange(4)
+    cells[15, 3:7, 2:4] = np.arange(4, 12).reshape(4, 2)
+    refine = 4
+    subcells = rng.choice(np.array([-2, -1, -1, -1, -1, -1, 0, 1], dtype=np.int64),
+                          size=12 * refine**3)  # fmt: skip
+    slot = np.full(n, -1, dtype=np.int64)
+    slot[::4] = np.arange(len(slot[::4]))
+    slots = int(slot.max()) + 1
+    threads = 2
+    planes = np.array([5.5e-3, 14.25e-3])
+    n_nodes = sum(p[0] * p[1] * p[2] for p in patches)
+    nb = nx * ny * nz
+    return [
+        np.arange(n, dtype=np.int64), x, v,
+        np.full(n, 9.58e7) * (1.0 + 0.1 * rng.uniform(size=n)),
+        1.0e-6 * (1.0 + rng.uniform(size=n)),
+        np.zeros(n, dtype=np.int64), np.full(n, -1, dtype=np.int64),
+        np.full(n, -1, dtype=np.int64),
+        np.concatenate(fxs), np.concatenate(fys), np.concatenate(fzs),
+        np.array(patch_int, dtype=np.int64), np.array(patch_real, dtype=np.float64),
+        bn, int(has_b), 0.0, oy, oz, h, upper[0], upper[1], upper[2], int(mirror), int(mirror),
+        integrator, 0.5, max_steps, cells, subcells, refine, planes,
+        np.zeros((n, len(planes), 4, 8)), np.zeros((n, len(planes)), dtype=np.int64),
+        slot, np.zeros((slots, 64, 3)), np.zeros(slots, dtype=np.int64), threads,
+        np.zeros((threads, n_nodes)), int(has_j),
+        np.zeros((threads, 3 * nb)) if has_j else np.zeros((threads, 1)), 0.0,
+    ]  # fmt: skip
+
+
+def trace3d_case_names() -> list[tuple[str, tuple]]:
+    """The 3D branch combinations, named ``trace3d_i{integrator}_r_m_b_j``."""
+    out = []
+    for integrator in (0, 1):
+        for refined in (False, True):
+            for mirror in (False, True):
+                for has_b in (False, True):
+                    has_j = refined != mirror
+                    name = (f"trace3d_i{integrator}_r{int(refined)}_m{int(mirror)}"
+                            f"_b{int(has_b)}_j{int(has_j)}")  # fmt: skip
+                    out.append((name, (integrator, refined, mirror, has_b, has_j)))
+    out.append(("trace3d_i0_max_steps", (0, False, False, True, False, 32, 32, 25)))
+    return out

@@ -49,6 +49,23 @@ def _lorentz_factor(u0, u1, u2, inv_c2):
     return math.sqrt(1.0 + (u0 * u0 + u1 * u1 + u2 * u2) * inv_c2)
 
 
+def _relativistic_boris_update(u0, u1, u2, e0, e1, e2, b0, b1, b2, inv_c2):
+    """The relativistic Boris push (J. P. Boris, 1970) as the 3D kernel calls
+    ``mpiparticles``' ``relativistic_boris_update`` (absent here): a kick by the scaled
+    field ``e``, the rotation by ``t = b / gamma`` with ``s = 2 t / (1 + t^2)``, and a
+    second kick."""
+    m0, m1, m2 = u0 + e0, u1 + e1, u2 + e2
+    g = math.sqrt(1.0 + (m0 * m0 + m1 * m1 + m2 * m2) * inv_c2)
+    t0, t1, t2 = b0 / g, b1 / g, b2 / g
+    f = 2.0 / (1.0 + (t0 * t0 + t1 * t1 + t2 * t2))
+    s0, s1, s2 = f * t0, f * t1, f * t2
+    p0 = m0 + (m1 * t2 - m2 * t1)
+    p1 = m1 + (m2 * t0 - m0 * t2)
+    p2 = m2 + (m0 * t1 - m1 * t0)
+    return (m0 + (p1 * s2 - p2 * s1) + e0, m1 + (p2 * s0 - p0 * s2) + e1,
+            m2 + (p0 * s1 - p1 * s0) + e2)  # fmt: skip
+
+
 def _load(path: Path, name: str) -> types.ModuleType:
     spec = importlib.util.spec_from_file_location(name, path)
     module = importlib.util.module_from_spec(spec)
@@ -61,12 +78,14 @@ def reference_kernels(root: Path) -> dict:
     """The reference's kernel functions, by name and version."""
     shim = types.ModuleType("mpiparticles.kernels.boris_pyccel")
     shim.lorentz_factor = _lorentz_factor
+    shim.relativistic_boris_update = _relativistic_boris_update
     sys.modules.setdefault("mpiparticles", types.ModuleType("mpiparticles"))
     sys.modules.setdefault("mpiparticles.kernels", types.ModuleType("mpiparticles.kernels"))
     sys.modules["mpiparticles.kernels.boris_pyccel"] = shim
     kernels = root / "src" / "beamtracer" / "kernels"
     out = {}
-    for name in ("staggered_field_2d", "deposit_trajectories_2d", "trace_trajectories_2d"):
+    for name in ("staggered_field_2d", "deposit_trajectories_2d", "trace_trajectories_2d",
+                 "trace_trajectories_3d"):
         for version in ("pyccel", "numpy"):
             path = kernels / name / f"{name}_{version}.py"
             if path.exists():
@@ -250,6 +269,24 @@ def record_goldens(root: Path) -> None:
     print("record goldens:", sum(len(v) for v in keys.values()), "keys,", len(record), "lines")
 
 
+def trace3d_goldens(root: Path) -> None:
+    """The reference's 3D trace kernel (its Pyccel source run as Python) on the cases of
+    ``trace3d_case_names``.  Its Boris steps go through the stand-in for
+    ``relativistic_boris_update`` above (mpiparticles is absent); its Runge--Kutta steps
+    need only the Lorentz factor, 1 for these non-relativistic cases."""
+    from tests.golden.cases import trace3d_case, trace3d_case_names
+
+    kernel = reference_kernels(root)[("trace_trajectories_3d", "pyccel")]
+    for name, combo in trace3d_case_names():
+        args = trace3d_case(*combo)
+        result = copy_args(args)
+        kernel(*result)
+        _save(name, args, result)
+        status = result[6]
+        print(name, "statuses", dict(zip(*np.unique(status, return_counts=True))),
+              "max steps", int(result[5].max()))  # fmt: skip
+
+
 def _save(name: str, args: list, result: list, extra: dict | None = None) -> None:
     arrays = {}
     for i, (a, r) in enumerate(zip(args, result, strict=True)):
@@ -266,12 +303,18 @@ def main() -> None:
         "--reference", default=os.environ.get("BEAMTRACER_REFERENCE"),
         help="the reference checkout (default: $BEAMTRACER_REFERENCE)",
     )  # fmt: skip
-    given = parser.parse_args().reference
+    parser.add_argument("--only", choices=["trace3d"], default=None,
+                        help="generate only the 3D tracer's fixtures")
+    args = parser.parse_args()
+    given = args.reference
     if not given:
         parser.error("give --reference or set BEAMTRACER_REFERENCE to the reference checkout")
     root = Path(given)
     if not (root / "src" / "beamtracer").is_dir():
         parser.error(f"{root} holds no src/beamtracer package")
+    trace3d_goldens(root)
+    if args.only == "trace3d":
+        return
     host_goldens(root)
     record_goldens(root)
     ref = reference_kernels(root)

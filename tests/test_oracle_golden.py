@@ -15,7 +15,13 @@ import numpy as np
 import pytest
 
 from oracle import kernels as oracle
-from tests.golden.cases import TRACE_CHARGE, TRACE_OUTPUTS, trace_case_names
+from tests.golden.cases import (
+    TRACE_CHARGE,
+    TRACE_OUTPUTS,
+    copy_args,
+    trace3d_case_names,
+    trace_case_names,
+)
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 EXACT = ("steps", "status", "electrode", "counts", "path_count")
@@ -64,3 +70,17 @@ def test_trace_matches_the_reference(name):
         args[TRACE_CHARGE].sum(0), expected[TRACE_CHARGE].sum(0), rtol=1e-12,
         atol=1e-12 * np.abs(expected[TRACE_CHARGE]).max(),
     )  # fmt: skip
+
+
+@pytest.mark.parametrize("name", [name for name, _ in trace3d_case_names()])
+def test_trace3d_matches_the_reference(name):
+    """The 3D oracle restates the reference's 3D kernel: every output bit for bit (the
+    Boris cases through the stand-in for mpiparticles' Boris push in both)."""
+    from oracle.trace3d import trace_trajectories_3d
+    from tests.gpu_util import load_golden
+
+    args, out = load_golden(name)
+    result = copy_args(args)
+    trace_trajectories_3d(*result)
+    for i, (got, want) in enumerate(zip(result, out, strict=True)):
+        np.testing.assert_array_equal(np.asarray(got), np.asarray(want), err_msg=f"argument {i}")
