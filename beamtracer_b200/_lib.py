@@ -64,6 +64,23 @@ class TraceArgs(ctypes.Structure):
     ]  # fmt: skip
 
 
+class Trace3DArgs(ctypes.Structure):
+    """``bt_trace3d_args`` of ``include/bt200.h``."""
+
+    _fields_ = [
+        ("active", P), ("n_active", I64), ("x", P), ("v", P), ("n", I64), ("qm", P),
+        ("dq", P), ("steps", P), ("status", P), ("electrode", P), ("fxs", P), ("fys", P),
+        ("fzs", P), ("patch_int", P), ("patch_real", P), ("n_patches", I64), ("bn", P),
+        ("has_b", I64), ("origin_x", F64), ("origin_y", F64), ("origin_z", F64), ("h", F64),
+        ("upper_x", F64), ("upper_y", F64), ("upper_z", F64), ("mirror_y", I64),
+        ("mirror_z", I64), ("integrator", I64), ("step_fraction", F64), ("max_steps", I64),
+        ("cells", P), ("subcells", P), ("refine", I64), ("planes", P), ("n_planes", I64),
+        ("hits", P), ("capacity", I64), ("counts", P), ("path_slot", P), ("paths", P),
+        ("path_capacity", I64), ("path_count", P), ("num_threads", I64), ("charge", P),
+        ("n_nodes", I64), ("has_j", I64), ("current", P), ("inv_c2", F64),
+    ]  # fmt: skip
+
+
 class TraceBatch(ctypes.Structure):
     """``bt_trace_batch`` of ``include/bt200.h``."""
 
@@ -138,6 +155,7 @@ SIGNATURES: dict[str, list] = {
                                        ctypes.POINTER(TraceBatch), I64],
     "bt_trace_trajectories_2d_batch_fast": [P, ctypes.POINTER(TraceArgs),
                                             ctypes.POINTER(TraceBatch), I64],
+    "bt_trace_trajectories_3d": [P, ctypes.POINTER(Trace3DArgs), I64],
     "bt_measure_fp64_peak": [P, ctypes.POINTER(F64)],
     "bt_trace_last_stats": [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64)],
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],

@@ -166,7 +166,7 @@ class BatchedVlasov:
             engine = TraceEngine(mesh, planes=self.planes, integrator=config.integrator,
                                  step_fraction=config.step_fraction, max_steps=config.max_steps,
                                  capacity=capacity, window=self.window)  # fmt: skip
-            engine.load(particles)
+            engine.load(particles, buffers=False)
             mass = np.array([beam.mass for beam in config.beams]) * _atomic_mass()
             cand = Candidate(config, mesh, IonOpticsPoisson(mesh), MeshArrays(mesh), engine, mass)
             nx, ny = mesh.shape

@@ -10,6 +10,11 @@ kernel of this package:
   patch_int, patch_real, origin_x, origin_y, h, upper_x, upper_y, cylindrical, integrator,
   step_fraction, max_steps, cells, subcells, refine, planes, hits, counts, path_slot, paths,
   path_count, num_threads, charge, graded, x_nodes, inv_c2)``
+- ``trace_trajectories_3d(active, x, v, qm, dq, steps, status, electrode, fxs, fys, fzs,
+  patch_int, patch_real, bn, has_b, origin_x, origin_y, origin_z, h, upper_x, upper_y,
+  upper_z, mirror_y, mirror_z, integrator, step_fraction, max_steps, cells, subcells,
+  refine, planes, hits, counts, path_slot, paths, path_count, num_threads, charge, has_j,
+  current, inv_c2)``
 
 The arrays are written in place.  Device arrays (anything with
 ``__cuda_array_interface__``: torch CUDA tensors, CuPy arrays) are used where they lie, as
@@ -201,6 +206,67 @@ def trace_trajectories_2d(*args, window: int = 0, magnetic=None) -> None:
     s.finish()
 
 
+_TRACE3D_ARRAYS = {
+    # name: (position, dtype, output)
+    "active": (0, np.int64, False), "x": (1, np.float64, True), "v": (2, np.float64, True),
+    "qm": (3, np.float64, False), "dq": (4, np.float64, False),
+    "steps": (5, np.int64, True), "status": (6, np.int64, True),
+    "electrode": (7, np.int64, True), "fxs": (8, np.float64, False),
+    "fys": (9, np.float64, False), "fzs": (10, np.float64, False),
+    "patch_int": (11, np.int64, False), "patch_real": (12, np.float64, False),
+    "bn": (13, np.float64, False), "cells": (27, np.int64, False),
+    "subcells": (28, np.int64, False), "planes": (30, np.float64, False),
+    "hits": (31, np.float64, True), "counts": (32, np.int64, True),
+    "path_slot": (33, np.int64, False), "paths": (34, np.float64, True),
+    "path_count": (35, np.int64, True), "charge": (37, np.float64, True),
+    "current": (39, np.float64, True),
+}  # fmt: skip
+
+
+def trace_trajectories_3d(*args, window: int = 0) -> None:
+    """Trace the ``active`` trajectories of a 3D mesh until they end, or reach a cut
+    electrode sub-cell (status -2): the 41 arguments of the reference kernel
+    (``trace_trajectories_3d_pyccel.py:19-61``), in its order; ``window`` is the number of
+    steps a launch advances every trajectory (0: the library's default).  The space charge
+    goes to ``charge[0]``, the current elements (``has_j``) to ``current[0]``."""
+    if len(args) != 41:
+        raise TypeError(f"trace_trajectories_3d takes 41 arguments, got {len(args)}")
+    s = _Staging()
+    arrays = list(args)
+    for name, (i, dtype, output) in _TRACE3D_ARRAYS.items():
+        arrays[i] = s.device(args[i], dtype, name, output=output)
+    (active, x, v, qm, dq, steps, status, electrode, fxs, fys, fzs, patch_int, patch_real, bn,
+     has_b, origin_x, origin_y, origin_z, h, upper_x, upper_y, upper_z, mirror_y, mirror_z,
+     integrator, step_fraction, max_steps, cells, subcells, refine, planes, hits, counts,
+     path_slot, paths, path_count, num_threads, charge, has_j, current, inv_c2) = arrays  # fmt: skip
+    n = _shape(x)[1]
+    hits_shape = _shape(hits)
+    if _shape(x) != (3, n) or _shape(v) != (3, n):
+        raise ValueError("x and v must be (3, n)")
+    if len(hits_shape) != 4 or hits_shape[:2] != (n, _size(planes)) or hits_shape[3] != 8:
+        raise ValueError("hits must be (n, planes, capacity, 8)")
+    if len(_shape(charge)) != 2 or len(_shape(patch_int)) != 2 or _shape(patch_int)[1] != 8:
+        raise ValueError("charge must be (threads, nodes) and patch_int (patches, 8)")
+    if len(_shape(paths)) != 3 or _shape(paths)[2] != 3:
+        raise ValueError("paths must be (slots, capacity, 3)")
+    a = _lib.Trace3DArgs(
+        _lib.dptr(active), _size(active), _lib.dptr(x), _lib.dptr(v), n, _lib.dptr(qm),
+        _lib.dptr(dq), _lib.dptr(steps), _lib.dptr(status), _lib.dptr(electrode),
+        _lib.dptr(fxs), _lib.dptr(fys), _lib.dptr(fzs), _lib.dptr(patch_int),
+        _lib.dptr(patch_real), _shape(patch_int)[0], _lib.dptr(bn), int(has_b),
+        float(origin_x), float(origin_y), float(origin_z), float(h), float(upper_x),
+        float(upper_y), float(upper_z), int(mirror_y), int(mirror_z), int(integrator),
+        float(step_fraction), int(max_steps), _lib.dptr(cells), _lib.dptr(subcells),
+        int(refine), _lib.dptr(planes), _size(planes), _lib.dptr(hits), hits_shape[2],
+        _lib.dptr(counts), _lib.dptr(path_slot), _lib.dptr(paths), _shape(paths)[1],
+        _lib.dptr(path_count), int(num_threads), _lib.dptr(charge), _shape(charge)[1],
+        int(has_j), _lib.dptr(current), float(inv_c2),
+    )  # fmt: skip
+    ctx = _lib.context()
+    _lib.check(_lib.lib().bt_trace_trajectories_3d(ctx.handle, ctypes.byref(a), int(window)))
+    s.finish()
+
+
 def last_trace_stats() -> dict[str, int]:
     """Windows, deposit records and deposit flushes of the calling thread's last trace."""
     windows, records, flushes = _lib.I64(), _lib.I64(), _lib.I64()
@@ -218,5 +284,6 @@ KERNELS = {
     "staggered_field_2d": staggered_field_2d,
     "deposit_trajectories_2d": deposit_trajectories_2d,
     "trace_trajectories_2d": trace_trajectories_2d,
+    "trace_trajectories_3d": trace_trajectories_3d,
 }
 KERNEL_NAMES = tuple(KERNELS)

@@ -396,13 +396,23 @@ class TraceEngine:
         self.planes_dev = torch.tensor(self.planes or (np.nan,), dtype=torch.float64, device=dev)
         self.volumes = torch.from_numpy(node_volumes(mesh)).to(dev)
         self.n_nodes = nx * ny
-        self.charge = torch.zeros((1, self.n_nodes), dtype=torch.float64, device=dev)
+        self._charge = None
         self.particles: BeamParticles | None = None
+
+    @property
+    def charge(self):
+        """The node charges of the last run (device (1, nodes))."""
+        if self._charge is None:
+            self._charge = self.torch.zeros((1, self.n_nodes), dtype=self.torch.float64,
+                                            device="cuda")  # fmt: skip
+        return self._charge
 
     # -- the beam -------------------------------------------------------------------------
 
-    def load(self, particles: BeamParticles) -> None:
-        """Copy a beam to the device (its start states are kept for every run)."""
+    def load(self, particles: BeamParticles, buffers: bool = True) -> None:
+        """Copy a beam to the device (its start states are kept for every run);
+        ``buffers=False`` leaves the trace's state and result buffers to the first `run`
+        (a caller that traces the start states elsewhere, as a batch, needs none)."""
         torch = self.torch
         mesh = self.mesh
         n = len(particles)
@@ -438,12 +448,19 @@ class TraceEngine:
         self.path_slot = torch.from_numpy(slot).to(dev)
         px, py = _project(mesh, x[:, self.saved_ids])
         self.first_points = torch.from_numpy(np.stack([px, py], axis=1).copy()).to(dev)
+        self._have_buffers = False
+        if buffers:
+            self._state_buffers()
+
+    def _state_buffers(self) -> None:
+        torch = self.torch
         self.x = torch.empty_like(self.x0)
         self.v = torch.empty_like(self.v0)
-        self.steps = torch.zeros(n, dtype=torch.int64, device=dev)
+        self.steps = torch.zeros(self.n, dtype=torch.int64, device="cuda")
         self.status = torch.empty_like(self.status0)
         self.electrode = torch.empty_like(self.electrode0)
         self._allocate_buffers()
+        self._have_buffers = True
 
     def _allocate_buffers(self) -> None:
         torch = self.torch
@@ -506,6 +523,8 @@ class TraceEngine:
         torch = self.torch
         mesh = self.mesh
         fx, fy = fx.reshape(-1), fy.reshape(-1)
+        if not self._have_buffers:
+            self._state_buffers()
         zero = torch.zeros(1, dtype=torch.int64, device="cuda")
         while True:
             self._reset()

@@ -228,6 +228,60 @@ int bt_trace_trajectories_2d_batch(bt_ctx *ctx, const bt_trace_args *args,
 int bt_trace_trajectories_2d_batch_fast(bt_ctx *ctx, const bt_trace_args *args,
                                         const bt_trace_batch *batch, int64_t window);
 
+/* The arguments of kernels/trace_trajectories_3d/trace_trajectories_3d_pyccel.py:19-61, all
+ * arrays on the device: positions and velocities (3, n); patch_int (n_patches, 8): node
+ * counts (nx, ny, nz), offsets of the three edge fields, node count, offset of the nodes in
+ * charge; patch_real (n_patches, 10): origin (3), spacing, node box (x0, y0, z0, x1, y1, z1),
+ * finest first and the base mesh last; bn (3, nx, ny, nz) of the base mesh when has_b;
+ * cells (nx - 1, ny - 1, nz - 1); hits (n, n_planes, capacity, 8); paths (slots,
+ * path_capacity, 3); charge (num_threads, nodes) and, with has_j, current (num_threads,
+ * 3 nx ny nz): the GPU adds into row 0. */
+typedef struct bt_trace3d_args {
+    const int64_t *active;
+    int64_t n_active;
+    double *x, *v;
+    int64_t n;
+    const double *qm, *dq;
+    int64_t *steps, *status, *electrode;
+    const double *fxs, *fys, *fzs;
+    const int64_t *patch_int;
+    const double *patch_real;
+    int64_t n_patches;
+    const double *bn;
+    int64_t has_b;
+    double origin_x, origin_y, origin_z, h, upper_x, upper_y, upper_z;
+    int64_t mirror_y, mirror_z, integrator;
+    double step_fraction;
+    int64_t max_steps;
+    const int64_t *cells;
+    const int64_t *subcells;
+    int64_t refine;
+    const double *planes;
+    int64_t n_planes;
+    double *hits;
+    int64_t capacity;
+    int64_t *counts;
+    const int64_t *path_slot;
+    double *paths;
+    int64_t path_capacity;
+    int64_t *path_count;
+    int64_t num_threads; /* the reference's host threads: ignored on the GPU */
+    double *charge;
+    int64_t n_nodes;
+    int64_t has_j;
+    double *current;
+    double inv_c2;
+} bt_trace3d_args;
+
+/* kernels/trace_trajectories_3d/trace_trajectories_3d_pyccel.py:19-657 (CUDA:
+ * *_cuda.cu:120-399): every active trajectory to its end (status 0-4) or to a sub-cell an
+ * electrode surface cuts (-2, for the caller's test), in windows of `window` steps (0: the
+ * default), one thread per trajectory, the reference's step term by term in FP64 (RK4, or
+ * Boris with the relativistic push of mpiparticles as published); the space charge (and,
+ * with has_j, the current elements) deposited deterministically: every step's eight node
+ * shares as (node, value) records, sorted by node and summed in record order. */
+int bt_trace_trajectories_3d(bt_ctx *ctx, const bt_trace3d_args *args, int64_t window);
+
 /* Counters of the last bt_trace_trajectories_2d call on this context (host out-params). */
 int bt_trace_last_stats(bt_ctx *ctx, int64_t *windows, int64_t *records,
                         int64_t *deposit_flushes);
