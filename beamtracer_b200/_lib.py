@@ -160,6 +160,7 @@ SIGNATURES: dict[str, list] = {
     "bt_trace_last_stats": [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64)],
     "bt_edge_field": [P, P, P, P, P, P, I64, I64, F64, P, P, P],
     "bt_edge_field_adjoint": [P, P, P, P, P, P, P, I64, I64, F64, P, P],
+    "bt_edge_field_3d": [P, P, P, P, P, I64, I64, I64, F64, P, P, P, P],
     "bt_surface_field": [P, P, P, P, P, I64, I64, I32, P, P, P],
     "bt_adjoint_checkpoints": [P, ctypes.POINTER(AdjointArgs), P],
     "bt_adjoint_sweep": [P, ctypes.POINTER(AdjointArgs), P, P, P, P],

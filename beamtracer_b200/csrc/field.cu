@@ -129,8 +129,53 @@ __global__ void edge_field_y(Line L, i64 nx, int sym_lo, int sym_hi, double *__r
     fy[t] = edge(L, PhiArray{L.phi}, i * L.n, e, sym_lo, sym_hi);
 }
 
+// The edges along one axis of a 3D mesh (n nodes along it, `stride` between them): edge e
+// of the line through the other two coordinates (u, w), u over `count_u` values with line
+// step `step_u`, w over `count_w` with step `step_w`; out (n + 1 edges, in the mesh's C
+// order with the axis lengthened by one).
+__global__ void edge_field_3d(Line L, i64 count_u, i64 step_u, i64 count_w, i64 step_w,
+                              i64 out_u, i64 out_w, i64 out_e, int sym_lo, int sym_hi,
+                              double *__restrict__ out) {
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const i64 m = L.n + 1;
+    if (t >= m * count_u * count_w) return;
+    const i64 e = t % m, uw = t / m, u = uw / count_w, w = uw - u * count_w;
+    out[u * out_u + w * out_w + e * out_e] =
+        edge(L, PhiArray{L.phi}, u * step_u + w * step_w, e, sym_lo, sym_hi);
+}
+
 }  // namespace
 }  // namespace bt
+
+extern "C" int bt_edge_field_3d(bt_ctx *ctx, const double *phi, const int32_t *solid,
+                                const uint8_t *near, const double *distance, int64_t nx,
+                                int64_t ny, int64_t nz, double h,
+                                const int32_t extrapolation[6], double *fx, double *fy,
+                                double *fz) {
+    return bt::guarded([&] {
+        BT_REQUIRE(ctx && phi && solid && near && distance && fx && fy && fz && extrapolation,
+                   "edge field 3d: null argument");
+        BT_REQUIRE(nx >= 3 && ny >= 3 && nz >= 3, "edge field 3d: 3 nodes per axis at least");
+        const i64 nn = nx * ny * nz;
+        const int T = 256;
+        // along x: lines (j, k), nodes i at stride ny nz; fx (nx + 1, ny, nz)
+        bt::Line lx{phi, solid, near, distance, distance + nn, nullptr, h, nx, ny * nz};
+        BT_LAUNCH(ctx, bt::edge_field_3d, bt::blocks_for((nx + 1) * ny * nz, T), T, 0, ctx->stream,
+                  lx, ny, nz, nz, (i64)1, nz, (i64)1, ny * nz, extrapolation[0], extrapolation[1],
+                  fx);
+        // along y: lines (i, k), stride nz; fy (nx, ny + 1, nz)
+        bt::Line ly{phi, solid, near, distance + 2 * nn, distance + 3 * nn, nullptr, h, ny, nz};
+        BT_LAUNCH(ctx, bt::edge_field_3d, bt::blocks_for(nx * (ny + 1) * nz, T), T, 0, ctx->stream,
+                  ly, nx, ny * nz, nz, (i64)1, (ny + 1) * nz, (i64)1, nz, extrapolation[2],
+                  extrapolation[3], fy);
+        // along z: lines (i, j), stride 1; fz (nx, ny, nz + 1)
+        bt::Line lz{phi, solid, near, distance + 4 * nn, distance + 5 * nn, nullptr, h, nz, 1};
+        BT_LAUNCH(ctx, bt::edge_field_3d, bt::blocks_for(nx * ny * (nz + 1), T), T, 0, ctx->stream,
+                  lz, nx, ny * nz, ny, nz, ny * (nz + 1), nz + 1, (i64)1, extrapolation[4],
+                  extrapolation[5], fz);
+        BT_CHECK_LAUNCH();
+    });
+}
 
 extern "C" int bt_edge_field(bt_ctx *ctx, const double *phi, const int32_t *solid,
                              const uint8_t *near, const double *distance, const double *dx,

@@ -273,6 +273,15 @@ typedef struct bt_trace3d_args {
     double inv_c2;
 } bt_trace3d_args;
 
+/* solver/fields3d.py:66-107 (StaggeredElectricField3D): the edge fields of a potential phi
+ * (nx, ny, nz) along each axis by the 2D rule of bt_edge_field (solver/fields.py:18-67) on
+ * every line of nodes: fx (nx + 1, ny, nz), fy (nx, ny + 1, nz), fz (nx, ny, nz + 1);
+ * solid (nx, ny, nz) int32, near uint8, distance (6, nx, ny, nz) towards -x, +x, -y, +y,
+ * -z, +z; extrapolation[6] per face (x min, x max, y min, ...): 1 symmetric, 0 linear. */
+int bt_edge_field_3d(bt_ctx *ctx, const double *phi, const int32_t *solid, const uint8_t *near,
+                     const double *distance, int64_t nx, int64_t ny, int64_t nz, double h,
+                     const int32_t extrapolation[6], double *fx, double *fy, double *fz);
+
 /* kernels/trace_trajectories_3d/trace_trajectories_3d_pyccel.py:19-657 (CUDA:
  * *_cuda.cu:120-399): every active trajectory to its end (status 0-4) or to a sub-cell an
  * electrode surface cuts (-2, for the caller's test), in windows of `window` steps (0: the

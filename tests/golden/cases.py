@@ -295,3 +295,26 @@ def trace3d_case_names() -> list[tuple[str, tuple]]:
                     out.append((name, (integrator, refined, mirror, has_b, has_j)))
     out.append(("trace3d_i0_max_steps", (0, False, False, True, False, 32, 32, 25)))
     return out
+
+
+# -- the 3D mesh ------------------------------------------------------------------------------
+
+
+def mesh3d_case() -> dict:
+    """A 3D mesh with a plate with a round hole (0 V) and a sphere (1.5 kV), a Dirichlet
+    face at x max (800 V) and a symmetry plane at y min: the settings both the reference's
+    and this package's ``IonOpticsMesh3D`` take (the electrodes as ``(inside, potential)``,
+    the faces as ``(kind, value)``)."""
+
+    def plate(x, y, z):
+        return (np.abs(x - 4.0e-3) <= 0.6e-3) & (y * y + (z - 2.5e-3) ** 2 >= (2.1e-3) ** 2)
+
+    def sphere(x, y, z):
+        return (x - 9.0e-3) ** 2 + (y - 3.0e-3) ** 2 + (z - 3.0e-3) ** 2 <= (1.3e-3) ** 2
+
+    return {
+        "shape": (25, 13, 11), "origin": (0.0, 0.0, 0.0), "h": 0.5e-3,
+        "electrodes": [(plate, 0.0), (sphere, 1500.0)],
+        "faces": {"x_max": ("dirichlet", 800.0), "y_min": ("neumann", 0.0)},
+        "symmetry_planes": ("y_min",),
+    }  # fmt: skip

@@ -269,6 +269,39 @@ def record_goldens(root: Path) -> None:
     print("record goldens:", sum(len(v) for v in keys.values()), "keys,", len(record), "lines")
 
 
+def mesh3d_goldens(root: Path) -> None:
+    """The reference's ``IonOpticsMesh3D`` (``solver/mesh3d.py``) and
+    ``StaggeredElectricField3D`` (``solver/fields3d.py``) on ``mesh3d_case``: the node
+    classification and the edge fields of a seeded potential."""
+    from collections.abc import Sequence
+
+    from tests.golden.cases import mesh3d_case
+
+    mesh2d = reference_mesh_module(root)
+    for name in ("beamtracer", "beamtracer.solver"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.modules["beamtracer.solver.mesh"] = mesh2d
+    mesh3d = _load(root / "src" / "beamtracer" / "solver" / "mesh3d.py", "_ref_mesh3d")
+    namespace = {"np": np, "Sequence": Sequence, "_edge_field": reference_edge_field(root),
+                 "IonOpticsMesh3D": mesh3d.IonOpticsMesh3D}  # fmt: skip
+    reference_definitions(root, "fields3d", ("_trilinear", "StaggeredElectricField3D"), namespace)
+    settings = mesh3d_case()
+    mesh = mesh3d.IonOpticsMesh3D(
+        shape=settings["shape"], origin=settings["origin"], h=settings["h"],
+        electrodes=[mesh3d.Electrode3D(f, v) for f, v in settings["electrodes"]],
+        faces={k: mesh2d.FaceCondition(*v) for k, v in settings["faces"].items()},
+        symmetry_planes=settings["symmetry_planes"],
+    )  # fmt: skip
+    rng = np.random.default_rng(23)
+    phi = np.where(mesh.fixed, mesh.fixed_value, rng.normal(size=mesh.shape) * 100.0)
+    field = namespace["StaggeredElectricField3D"](mesh, phi)
+    np.savez_compressed(HERE / "mesh3d_plate_sphere.npz", solid=mesh.solid,
+                        near_solid=mesh.near_solid, distance=mesh.distance, fixed=mesh.fixed,
+                        fixed_value=mesh.fixed_value, phi=phi, fx=field.fx, fy=field.fy,
+                        fz=field.fz)  # fmt: skip
+    print("mesh3d near", int(mesh.near_solid.sum()), "solid", int((mesh.solid >= 0).sum()))
+
+
 def trace3d_goldens(root: Path) -> None:
     """The reference's 3D trace kernel (its Pyccel source run as Python) on the cases of
     ``trace3d_case_names``.  Its Boris steps go through the stand-in for
@@ -304,7 +337,7 @@ def main() -> None:
         help="the reference checkout (default: $BEAMTRACER_REFERENCE)",
     )  # fmt: skip
     parser.add_argument("--only", choices=["trace3d"], default=None,
-                        help="generate only the 3D tracer's fixtures")
+                        help="generate only the 3D fixtures (tracer, mesh, edge fields)")
     args = parser.parse_args()
     given = args.reference
     if not given:
@@ -313,6 +346,7 @@ def main() -> None:
     if not (root / "src" / "beamtracer").is_dir():
         parser.error(f"{root} holds no src/beamtracer package")
     trace3d_goldens(root)
+    mesh3d_goldens(root)
     if args.only == "trace3d":
         return
     host_goldens(root)
