@@ -173,6 +173,7 @@ SIGNATURES: dict[str, list] = {
     "bt_poisson_destroy": [P],
     "bt_poisson_set_region": [P, P, F64],
     "bt_poisson_set_options": [P, I32, I32, I32, I64],
+    "bt_poisson_set_context": [P, P],
     "bt_poisson_batch_create": [P, P, I64, P, ctypes.POINTER(P)],
     "bt_poisson_batch_destroy": [P],
     "bt_poisson_batch_solve": [P, P, P, P, F64, I32, P, P],

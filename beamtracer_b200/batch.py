@@ -117,12 +117,13 @@ class BatchedVlasov:
     Every configuration must share the diagnostic planes, the integrator, the step fraction,
     the step limit, the iteration limit, the tolerance and the relaxation; meshes, electrodes
     and beams may differ.  ``window``: trace steps per launch; ``contracted``: the trace
-    build with fused multiply-adds (moments agree with the exact build to rounding).
+    build with fused multiply-adds (moments agree with the exact build to rounding);
+    ``builders``: host threads that set the candidates up.
     """
 
     def __init__(self, configs: Sequence[BeamOpticsConfig], *, window: int = 64,
                  contracted: bool = False, capacity: tuple[int, int] = (4, 1024),
-                 field: str = "batched") -> None:  # fmt: skip
+                 field: str = "batched", builders: int = 6) -> None:  # fmt: skip
         import torch
 
         from beamtracer_b200.model import config_mesh, config_particles
@@ -153,15 +154,16 @@ class BatchedVlasov:
         dev = "cuda"
         self.candidates: list[Candidate] = []
         node = fx = fy = traj = 0
-        cylindrical = None
-        for config in configs:
+        device = torch.cuda.current_device()
+        #: the library contexts of the threads that built candidates (their solvers are
+        #: bound to them: kept for the batch's life)
+        self._builder_contexts: list[Any] = []
+
+        def build(config: BeamOpticsConfig) -> Candidate:
+            torch.cuda.set_device(device)
             mesh = config_mesh(config)
             if mesh.graded:
                 raise NotImplementedError("a batch takes uniform meshes")
-            if cylindrical is None:
-                cylindrical = (mesh.cylindrical, mesh.symmetry_plane)
-            elif cylindrical != (mesh.cylindrical, mesh.symmetry_plane):
-                raise ValueError("every configuration of a batch needs the same geometry")
             particles, _ = config_particles(config)
             engine = TraceEngine(mesh, planes=self.planes, integrator=config.integrator,
                                  step_fraction=config.step_fraction, max_steps=config.max_steps,
@@ -169,9 +171,30 @@ class BatchedVlasov:
             engine.load(particles, buffers=False)
             mass = np.array([beam.mass for beam in config.beams]) * _atomic_mass()
             cand = Candidate(config, mesh, IonOpticsPoisson(mesh), MeshArrays(mesh), engine, mass)
+            cand.n_traj = len(particles)
+            torch.cuda.current_stream().synchronize()
+            return cand, _lib.context()
+
+        if builders > 1 and len(configs) > 1:
+            # the candidates' host work (meshes, tables, beams) on several threads; each
+            # thread's device work queues on its own context
+            from concurrent.futures import ThreadPoolExecutor
+
+            with ThreadPoolExecutor(max_workers=min(builders, len(configs))) as pool:
+                built = list(pool.map(build, configs))
+        else:
+            built = [build(config) for config in configs]
+        contexts = {id(c): c for _, c in built}
+        self._builder_contexts = list(contexts.values())
+        cylindrical = None
+        for cand, _ in built:
+            mesh = cand.mesh
+            if cylindrical is None:
+                cylindrical = (mesh.cylindrical, mesh.symmetry_plane)
+            elif cylindrical != (mesh.cylindrical, mesh.symmetry_plane):
+                raise ValueError("every configuration of a batch needs the same geometry")
             nx, ny = mesh.shape
             cand.node0, cand.fx0, cand.fy0, cand.traj0 = node, fx, fy, traj
-            cand.n_traj = len(particles)
             node += nx * ny
             fx += (nx + 1) * ny
             fy += nx * (ny + 1)
@@ -246,6 +269,8 @@ class BatchedVlasov:
         # per candidate: max |phi - previous|, max |rho_new - rho_old|, max |rho_new|
         self.scalars = torch.zeros((len(cands), 4), **f64)
         self.trace_launches = 0
+        for c in cands:
+            c.poisson.rebind(self.ctx)  # built on other threads' contexts
         self.poisson_batch = PoissonBatch([c.poisson for c in cands], [c.node0 for c in cands])
 
     def _shape_tables(self):

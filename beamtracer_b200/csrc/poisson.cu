@@ -3047,3 +3047,15 @@ extern "C" int bt_poisson_batch_tiling(bt_poisson_batch *B, int32_t set, int32_t
         tiling[5] = B->tuned ? 1 : 0;
     });
 }
+
+extern "C" int bt_poisson_set_context(bt_poisson *p, bt_ctx *ctx) {
+    return bt::guarded([&] {
+        BT_REQUIRE(p && ctx, "poisson: null argument");
+        if (p->ctx == ctx) return;
+        BT_REQUIRE(p->ctx->device == ctx->device, "poisson: the new context is on another device");
+        // the old context's queued work first; its captured V-cycle is its own
+        BT_CUDA(cudaStreamSynchronize(p->ctx->stream));
+        bt::drop_graphs(p);
+        p->ctx = ctx;
+    });
+}

@@ -141,6 +141,13 @@ class IonOpticsPoisson:
         _lib.check(_lib.lib().bt_poisson_fixed_adjoint(self._handle, _lib.dptr(z),
                                                        _lib.dptr(phi_bar), _lib.dptr(out)))  # fmt: skip
 
+    def rebind(self, ctx) -> None:
+        """Queue this solver's later work on the library context ``ctx`` (same device)."""
+        if ctx is self._ctx:
+            return
+        _lib.check(_lib.lib().bt_poisson_set_context(self._handle, ctx.handle))
+        self._ctx = ctx
+
     def close(self) -> None:
         if getattr(self, "_handle", None):
             _lib.lib().bt_poisson_destroy(self._handle)

@@ -428,6 +428,10 @@ int bt_poisson_set_region(bt_poisson *p, const uint8_t *mask, double value);
 int bt_poisson_set_options(bt_poisson *p, int32_t fine_sweeps, int32_t coarse_sweeps,
                            int32_t staged, int64_t tail_nodes);
 
+/* Move a solver to another context on the same device (after its queued work finishes):
+ * its later work queues on that context's stream.  No counterpart in the reference. */
+int bt_poisson_set_context(bt_poisson *p, bt_ctx *ctx);
+
 /* -- the batched field solve (no counterpart in the reference, which solves each design
  * candidate's field on its own: optimization/einzel.py:389-403) ------------------------- */
 
