@@ -30,7 +30,8 @@ struct Error {
     do {                                                                                  \
         cudaError_t bt_e_ = (call);                                                       \
         if (bt_e_ != cudaSuccess)                                                         \
-            throw ::bt::Error{BT_ERR_CUDA, std::string(#call) + ": " +                    \
+            throw ::bt::Error{BT_ERR_CUDA, std::string(#call) + " (" + __FILE__ + ":" +   \
+                                               std::to_string(__LINE__) + "): " +         \
                                                cudaGetErrorString(bt_e_)};                \
     } while (0)
 

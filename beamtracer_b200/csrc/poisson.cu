@@ -1614,11 +1614,10 @@ void setup_tail(bt_poisson *p) {
     BT_CUDA(cudaFuncSetAttribute(smooth_staged<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big5));
     BT_CUDA(cudaFuncSetAttribute(smooth_staged<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big5));
     BT_CUDA(cudaFuncSetAttribute(smooth_staged<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big9));
-    {
-        const Level &Lc = p->levels.back();
-        BT_CUDA(cudaFuncSetAttribute(coarsest_band_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)band_smem(Lc.nx, Lc.ny)));
-    }
+    // the largest band any solver's coarsest level needs (the attribute is the kernel's,
+    // shared by every solver of the process: never set it to one mesh's own size)
+    BT_CUDA(cudaFuncSetAttribute(coarsest_band_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(double) * kCoarsest * (2 * kBandMax + 1))));
     if (p->tail_start <= 0) return;
     const TailLayout T = tail_layout(p->levels, p->tail_start);
     p->tail_smem = T.total();
