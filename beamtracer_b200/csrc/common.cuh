@@ -153,7 +153,7 @@ struct bt_ctx {
     bt::Buffer anderson;        // the Anderson mixer's sums, R, Q^T f and gamma
     bt::Buffer measure;         // the FP64 peak measurement's output
     // the 3D tracer's records (charge, current), live flags and live count
-    bt::Buffer t3_keys, t3_vals, t3_jkeys, t3_jvals, t3_alive, t3_live;
+    bt::Buffer t3_keys, t3_vals, t3_jkeys, t3_jvals, t3_alive, t3_live, t3_cells;
     i64 launch_count = 0;       // kernels launched on the context since its creation
     i64 last_windows = 0, last_records = 0, last_flushes = 0;
 };

@@ -172,6 +172,25 @@ __device__ __forceinline__ Box box3(i64 first, int bnx, int bny, int bnz, double
     return {first + (i64)i * bny * bnz + (i64)j * bnz + k, bnz, (i64)bny * bnz, a, b, c};
 }
 
+// A cell's charge record: the shares of its eight corners, in the corner order (k, then j,
+// then i offsets: q = 4 di + 2 dj + dk), two 32-byte sectors.
+struct __align__(64) CellRec {
+    double c[8];
+};
+
+// The eight shares of q, in the reference's corner order (:512-519).
+__device__ __forceinline__ void shares8(const Box &B, double q, double *w) {
+    const double a = B.a, b = B.b, c = B.c;
+    w[0] = (1.0 - a) * (1.0 - b) * (1.0 - c) * q;
+    w[1] = (1.0 - a) * (1.0 - b) * c * q;
+    w[2] = (1.0 - a) * b * (1.0 - c) * q;
+    w[3] = (1.0 - a) * b * c * q;
+    w[4] = a * (1.0 - b) * (1.0 - c) * q;
+    w[5] = a * (1.0 - b) * c * q;
+    w[6] = a * b * (1.0 - c) * q;
+    w[7] = a * b * c * q;
+}
+
 // The eight shares of q as records, in the reference's corner order (:512-519).
 __device__ __forceinline__ void records8(const Box &B, double q, uint32_t *key, double *val) {
     const double a = B.a, b = B.b, c = B.c;
@@ -201,14 +220,15 @@ struct Trace3 {
     uint32_t jsentinel;   // a slot with no current record
 };
 
-// One window of trajectory m (of the active list): at most S steps from its state, each
-// step's charge shares into the slots ((s n_active + m) 8 + corner) and, with has_j, its
-// current shares into ((s n_active + m) 24 + 8 component + corner); the slots of the steps
-// not taken hold the sentinels.  alive[m]: the trajectory has not ended (cleared here when
+// One window of trajectory m (of the active list): at most S steps from its state.  The
+// charge of a run of consecutive steps in one cell is summed into one cell record (key: the
+// cell's lower corner node), written to the slot (s n_active + m) of the run's last step s;
+// with has_j, each step's current shares go to the slots ((s n_active + m) 24 + 8 component
+// + corner).  The slots with no record hold the sentinels.  alive[m]: the trajectory has not ended (cleared here when
 // it does, with its status written); *live counts the ones still going after the window.
 __global__ void __launch_bounds__(128) trace3d_window(Trace3 T, uint8_t *__restrict__ alive,
                                                       uint32_t *__restrict__ keys,
-                                                      double *__restrict__ vals,
+                                                      CellRec *__restrict__ recs,
                                                       uint32_t *__restrict__ jkeys,
                                                       double *__restrict__ jvals,
                                                       unsigned long long *__restrict__ live) {
@@ -231,6 +251,10 @@ __global__ void __launch_bounds__(128) trace3d_window(Trace3 T, uint8_t *__restr
         i64 st = -1;
         bool have = false;
         Fields3 cache{};
+        // the current run of steps in one cell: its slot, key and summed shares
+        i64 run_slot = -1;
+        uint32_t run_key = T.sentinel;
+        double run[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (; s < S && ns < a.max_steps; ++s) {
             // the spacing of the finest patch at the step's start (:148-163)
             double p1 = x1, p2 = x2;
@@ -340,8 +364,28 @@ __global__ void __launch_bounds__(128) trace3d_window(Trace3 T, uint8_t *__restr
                 const Box B = box3(__ldg(pi + 7), (int)__ldg(pi), (int)__ldg(pi + 1),
                                    (int)__ldg(pi + 2), (m0 - __ldg(pr)) / phh,
                                    (m1 - __ldg(pr + 1)) / phh, (m2 - __ldg(pr + 2)) / phh);
-                const i64 at = ((i64)s * na + m) * 8;
-                records8(B, dqk * dt, keys + at, vals + at);
+                double w[8];
+                shares8(B, dqk * dt, w);
+                const uint32_t key = (uint32_t)B.cc;
+                const i64 at = (i64)s * na + m;
+                if (run_slot >= 0 && key == run_key) {
+                    keys[run_slot] = T.sentinel;  // the run moves on to this step's slot
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) run[q] = run[q] + w[q];
+                } else {
+                    if (run_slot >= 0) {
+                        keys[run_slot] = run_key;
+                        CellRec r;
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) r.c[q] = run[q];
+                        recs[run_slot] = r;
+                    }
+                    run_key = key;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) run[q] = w[q];
+                }
+                run_slot = at;
+                keys[at] = T.sentinel;
             }
             if (j_on) {
                 // the current element dq (x' - x) on the base mesh (:520-565)
@@ -434,6 +478,13 @@ __global__ void __launch_bounds__(128) trace3d_window(Trace3 T, uint8_t *__restr
                 break;
             }
         }
+        if (run_slot >= 0) {
+            keys[run_slot] = run_key;
+            CellRec r;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) r.c[q] = run[q];
+            recs[run_slot] = r;
+        }
         if (st == -1 && ns >= a.max_steps) st = 4;
         a.x[k] = x0;
         a.x[n + k] = x1;
@@ -451,9 +502,7 @@ __global__ void __launch_bounds__(128) trace3d_window(Trace3 T, uint8_t *__restr
     }
     // the slots of the steps not taken hold no record
     for (; s < S; ++s) {
-        const i64 at = ((i64)s * na + m) * 8;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) keys[at + q] = T.sentinel;
+        keys[(i64)s * na + m] = T.sentinel;
         if (j_on) {
             const i64 jt = ((i64)s * na + m) * 24;
             for (int q = 0; q < 24; ++q) jkeys[jt + q] = T.jsentinel;
@@ -474,6 +523,50 @@ __global__ void run_sums(const uint32_t *__restrict__ K, const uint32_t *__restr
     double s = target[key];
     for (i64 q = r; q < n && K[q] == key; ++q) s += vals[I[q]];
     target[key] = s;
+}
+
+// cells[key] = the sum of each run of equal sorted keys' records, in record order (one
+// thread a run, from its head); the cells of no record hold zeros.
+__global__ void cell_runs(const uint32_t *__restrict__ K, const uint32_t *__restrict__ I,
+                          const CellRec *__restrict__ recs, const i64 *__restrict__ count,
+                          CellRec *__restrict__ cells) {
+    const i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const i64 n = *count;
+    if (r >= n) return;
+    const uint32_t key = K[r];
+    if (r > 0 && K[r - 1] == key) return;
+    CellRec sum = recs[I[r]];
+    for (i64 q = r + 1; q < n && K[q] == key; ++q) {
+        const CellRec add = recs[I[q]];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) sum.c[c] = sum.c[c] + add.c[c];
+    }
+    cells[key] = sum;
+}
+
+// charge[node] += its shares of the eight cells it is a corner of, in a fixed order (the
+// corner q = 4 di + 2 dj + dk of the cell at node - (di, dj, dk)), within its patch.
+__global__ void node_gather3(const CellRec *__restrict__ cells, const i64 *__restrict__ patch_int,
+                             int n_patches, i64 n_nodes, double *__restrict__ charge) {
+    const i64 node = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= n_nodes) return;
+    int p = 0;
+    while (p < n_patches - 1 &&
+           !(node >= patch_int[p * 8 + 7] && node < patch_int[p * 8 + 7] + patch_int[p * 8 + 6]))
+        ++p;
+    const i64 *pi = patch_int + p * 8;
+    const i64 pnx = pi[0], pny = pi[1], pnz = pi[2], local = node - pi[7];
+    if (local < 0 || local >= pnx * pny * pnz) return;
+    const i64 i = local / (pny * pnz), j = (local / pnz) % pny, k = local % pnz;
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int di = q >> 2, dj = (q >> 1) & 1, dk = q & 1;
+        const i64 ci = i - di, cj = j - dj, ck = k - dk;
+        if (ci < 0 || cj < 0 || ck < 0 || ci > pnx - 2 || cj > pny - 2 || ck > pnz - 2) continue;
+        s = s + cells[node - di * pny * pnz - dj * pnz - dk].c[q];
+    }
+    charge[node] += s;
 }
 
 __global__ void fill_flags(uint8_t *__restrict__ flags, i64 n, uint8_t value) {
@@ -545,11 +638,12 @@ void trace3d_all(bt_ctx *ctx, const bt_trace3d_args *args, int64_t window) {
     T.sentinel = (uint32_t)a.n_nodes;
     T.jsentinel = (uint32_t)(3 * nb);
     const i64 na = a.n_active;
-    const i64 slots = (i64)T.S * na * 8, jslots = a.has_j ? (i64)T.S * na * 24 : 0;
+    const i64 slots = (i64)T.S * na, jslots = a.has_j ? (i64)T.S * na * 24 : 0;
     BT_REQUIRE(slots < (i64)0xffffffffLL && jslots < (i64)0xffffffffLL,
                "trace3d: too many records a window (use a shorter window)");
     uint32_t *keys = ctx->t3_keys.as<uint32_t>(slots);
-    double *vals = ctx->t3_vals.as<double>(slots);
+    CellRec *recs = ctx->t3_vals.as<CellRec>(slots);
+    CellRec *cells = ctx->t3_cells.as<CellRec>(a.n_nodes);
     uint32_t *jkeys = a.has_j ? ctx->t3_jkeys.as<uint32_t>(jslots) : nullptr;
     double *jvals = a.has_j ? ctx->t3_jvals.as<double>(jslots) : nullptr;
     uint8_t *alive = ctx->t3_alive.as<uint8_t>(na);
@@ -563,11 +657,22 @@ void trace3d_all(bt_ctx *ctx, const bt_trace3d_args *args, int64_t window) {
         BT_CUDA(cudaMemsetAsync(live, 0, sizeof(unsigned long long), st));
         {
             Timed timed(ctx, "trace3d_window");
-            BT_LAUNCH(ctx, trace3d_window, blocks_for(na, 128), 128, 0, st, T, alive, keys, vals,
+            BT_LAUNCH(ctx, trace3d_window, blocks_for(na, 128), 128, 0, st, T, alive, keys, recs,
                       jkeys, jvals, live);
         }
         BT_CHECK_LAUNCH();
-        deposit_runs(ctx, keys, vals, slots, T.sentinel, a.charge);
+        {
+            // the window's cell records: sorted by cell, summed per cell, gathered per node
+            uint32_t *sk = nullptr, *sv = nullptr;
+            const i64 *count = nullptr;
+            radix_sort_pairs(ctx, keys, slots, nullptr, key_bits(T.sentinel), T.sentinel, &sk, &sv,
+                             &count);
+            BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(CellRec) * a.n_nodes, st));
+            BT_LAUNCH(ctx, cell_runs, blocks_for(slots, 256), 256, 0, st, sk, sv, recs, count, cells);
+            BT_LAUNCH(ctx, node_gather3, blocks_for(a.n_nodes, 256), 256, 0, st, cells, a.patch_int,
+                      (int)a.n_patches, a.n_nodes, a.charge);
+            BT_CHECK_LAUNCH();
+        }
         if (a.has_j) deposit_runs(ctx, jkeys, jvals, jslots, T.jsentinel, a.current);
         BT_CUDA(cudaMemcpyAsync(host, live, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         BT_CUDA(cudaStreamSynchronize(st));

@@ -422,39 +422,59 @@ class BeamTracer3D:
         planes = np.array(self.planes or (np.nan,), dtype=float)
         mirror_y = int("y_min" in mesh.symmetry_planes)
         mirror_z = int("z_min" in mesh.symmetry_planes)
-        initial = (x.copy(), v.copy(), status.copy(), electrode.copy())
+        # the device path keeps every array on the device across the pause rounds (the
+        # oracle's kernel takes host arrays)
+        on_device = self.kernel is None
+        if on_device:
+            import torch
+
+            put = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+            get = lambda a: a.cpu().numpy()  # noqa: E731
+        else:
+            put = get = lambda a: a  # noqa: E731
+        x, v, qm, dq, steps, status, electrode = map(put, (x, v, qm, dq, steps, status, electrode))
+        start, path_slot, cells, subcells, planes, magnetic = map(
+            put, (start, path_slot, cells, subcells, planes, magnetic))  # fmt: skip
+        patch_int, patch_real = put(patch_int), put(patch_real)
+        initial = [a.clone() if on_device else a.copy() for a in (x, v, status, electrode)]
         while True:
             capacity, path_capacity = self._capacity
-            charge = np.zeros((1, nodes))
-            current_nodes = np.zeros((1, 3 * nodes) if has_j else (1, 1))
-            hits = np.zeros((n, planes.size, capacity, 8))
-            counts = np.zeros((n, planes.size), dtype=np.int64)
-            paths = np.zeros((max(saved.size, 1), path_capacity, 3))
-            path_count = np.ones(max(saved.size, 1), dtype=np.int64)
-            paths[: saved.size, 0] = first.T
+            charge = put(np.zeros((1, nodes)))
+            current_nodes = put(np.zeros((1, 3 * nodes) if has_j else (1, 1)))
+            hits = put(np.zeros((n, len(planes), capacity, 8)))
+            counts = put(np.zeros((n, len(planes)), dtype=np.int64))
+            first_paths = np.zeros((max(saved.size, 1), path_capacity, 3))
+            first_paths[: saved.size, 0] = first.T
+            paths = put(first_paths)
+            path_count = put(np.ones(max(saved.size, 1), dtype=np.int64))
             active = start
-            while active.size:
+            while len(active):
                 kernel(active, x, v, qm, dq, steps, status, electrode, *fields, patch_int,
                        patch_real, magnetic, has_b, *mesh.origin, mesh.h, *mesh.upper, mirror_y,
                        mirror_z, INTEGRATORS.index(self.integrator), self.step_fraction,
                        self.max_steps, cells, subcells, SUBCELLS_3D, planes, hits, counts,
                        path_slot, paths, path_count, 1, charge, has_j, current_nodes, inv_c2)  # fmt: skip
                 paused = active[status[active] == _PAUSED]
-                if not paused.size:
+                if not len(paused):
                     break
-                hit = mesh.inside_solid(*self.mesh_points(x[:, paused]))
-                inside = hit >= 0
+                hit = mesh.inside_solid(*self.mesh_points(get(x[:, paused])))
+                inside = put(hit >= 0)
                 status[paused[inside]] = ELECTRODE
-                electrode[paused[inside]] = hit[inside]
+                electrode[paused[inside]] = put(hit)[inside]
                 active = paused[~inside]
                 status[active] = _ALIVE
-            most = int(counts.max()) if counts.size else 0
+            most = int(counts.max()) if len(counts) else 0
             longest = int(path_count.max())
             if most <= capacity and longest <= path_capacity:
                 break
             self._capacity = (max(capacity, most), max(path_capacity, longest))
-            x, v, status, electrode = (a.copy() for a in initial)
+            x, v, status, electrode = (a.clone() if on_device else a.copy() for a in initial)
             steps[:] = 0
+        x, v, steps, status, electrode = map(get, (x, v, steps, status, electrode))
+        charge, current_nodes, hits, counts, paths, path_count = map(
+            get, (charge, current_nodes, hits, counts, paths, path_count))  # fmt: skip
+        #: the steps each trajectory took in the last trace
+        self.steps = steps
         current_density = None
         if has_j:
             current_density = np.stack([self._finalize(c) for c in
