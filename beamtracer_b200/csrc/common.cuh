@@ -302,9 +302,13 @@ struct __align__(32) DepositRec {
 
 // n_records sizes the launches; n_dev, when not NULL, is the device-held count of the
 // records to deposit (at most n_records): the first ones, the rest ignored.
+// accumulate: the per-cell sums are added to those of the deposits before (no node charges
+// yet): deposit_cells_reset zeroes them, deposit_cells_finish adds them to the nodes once.
 void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i64 n_records,
                      const i64 *n_dev, uint32_t sentinel, double *charge,
-                     const NodeLayout &layout);
+                     const NodeLayout &layout, bool accumulate = false);
+void deposit_cells_reset(bt_ctx *ctx, i64 n_nodes);
+void deposit_cells_finish(bt_ctx *ctx, double *charge, const NodeLayout &layout);
 
 // Stable LSD radix sort of (key, index) pairs: sorted keys and the permutation, leaving
 // out the keys equal to `skip`.  Returns the device pointers of the sorted keys and values

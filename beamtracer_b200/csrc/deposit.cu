@@ -232,6 +232,11 @@ __global__ void __launch_bounds__(kThreads) radix_scatter(
     }
 }
 
+// a + b, componentwise in order.
+__device__ __forceinline__ double4 add4(double4 a, double4 b) {
+    return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+
 // Warp segmented reduction of the sorted records.  A segment (one cell) wholly inside a
 // warp is written to its cell; pieces of segments crossing warp boundaries are left for
 // `seg_reduce_chains`: `first` is a warp's leading piece of a segment begun earlier
@@ -242,7 +247,7 @@ __global__ void seg_reduce_warps(const uint32_t *__restrict__ K, const uint32_t 
                                  const i64 *__restrict__ R_dev, uint32_t sentinel,
                                  double4 *__restrict__ cells, double4 *__restrict__ first,
                                  double4 *__restrict__ last, uint8_t *__restrict__ tail_flag,
-                                 uint8_t *__restrict__ owner_flag) {
+                                 uint8_t *__restrict__ owner_flag, int accumulate) {
     const i64 R = record_count(R_host, R_dev);
     const i64 gw = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -283,7 +288,7 @@ __global__ void seg_reduce_warps(const uint32_t *__restrict__ K, const uint32_t 
     const double4 sum = make_double4(c00, c01, c10, c11);
     if (tail) {
         if (f) {
-            cells[key] = sum;
+            cells[key] = accumulate ? add4(cells[key], sum) : sum;
         } else {
             first[gw] = sum;
             tail_flag[gw] = 1;
@@ -307,7 +312,7 @@ __global__ void seg_reduce_chains(const uint32_t *__restrict__ K, i64 R_host,
                                   const double4 *__restrict__ first,
                                   const double4 *__restrict__ last,
                                   const uint8_t *__restrict__ tail_flag,
-                                  const uint8_t *__restrict__ owner_flag) {
+                                  const uint8_t *__restrict__ owner_flag, int accumulate) {
     const i64 n_warps = (record_count(R_host, R_dev) + 31) / 32;
     const i64 gw = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (gw >= n_warps || !owner_flag[gw]) return;
@@ -320,7 +325,8 @@ __global__ void seg_reduce_chains(const uint32_t *__restrict__ K, i64 R_host,
         s.w = s.w + p.w;
         if (tail_flag[w]) break;
     }
-    cells[K[gw * 32 + 31]] = s;
+    const uint32_t key = K[gw * 32 + 31];
+    cells[key] = accumulate ? add4(cells[key], s) : s;
 }
 
 // charge[node] += the four cells around it, in the fixed order (i, j), (i, j-1), (i-1, j),
@@ -486,9 +492,22 @@ __global__ void add_kept(const i64 *__restrict__ kept, i64 n_records, i64 *__res
     *total += kept ? *kept : n_records;
 }
 
+void deposit_cells_reset(bt_ctx *ctx, i64 n_nodes) {
+    double4 *cells = ctx->deposit.cell_sums.as<double4>((size_t)n_nodes);
+    BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * n_nodes, ctx->stream));
+}
+
+void deposit_cells_finish(bt_ctx *ctx, double *charge, const NodeLayout &layout) {
+    double4 *cells = ctx->deposit.cell_sums.as<double4>((size_t)layout.n_nodes);
+    BT_LAUNCH(ctx, node_accumulate, blocks_for(layout.n_nodes, 256), 256, 0, ctx->stream, cells,
+              charge, layout.patch_int, layout.n_patches, layout.nx, layout.ny, layout.n_nodes,
+              layout.ascending ? 1 : 0);
+    BT_CHECK_LAUNCH();
+}
+
 void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i64 n_records,
                      const i64 *n_dev, uint32_t sentinel, double *charge,
-                     const NodeLayout &layout) {
+                     const NodeLayout &layout, bool accumulate) {
     if (n_records == 0) return;
     DepositScratch &s = ctx->deposit;
     cudaStream_t st = ctx->stream;
@@ -504,12 +523,17 @@ void deposit_records(bt_ctx *ctx, const uint32_t *keys, const DepositRec *rec, i
     double4 *first = s.warp_first.as<double4>((size_t)n_warps);
     double4 *last = s.warp_last.as<double4>((size_t)n_warps);
     uint8_t *flags = s.warp_flags.as<uint8_t>((size_t)2 * n_warps);
-    BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * layout.n_nodes, st));
+    if (!accumulate) BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * layout.n_nodes, st));
     const int threads = 256;
     BT_LAUNCH(ctx, seg_reduce_warps, blocks_for(n_warps * 32, threads), threads, 0, st, sk, sv,
-              rec, n_records, n_sorted, sentinel, cells, first, last, flags, flags + n_warps);
+              rec, n_records, n_sorted, sentinel, cells, first, last, flags, flags + n_warps,
+              accumulate ? 1 : 0);
     BT_LAUNCH(ctx, seg_reduce_chains, blocks_for(n_warps, threads), threads, 0, st, sk, n_records,
-              n_sorted, cells, first, last, flags, flags + n_warps);
+              n_sorted, cells, first, last, flags, flags + n_warps, accumulate ? 1 : 0);
+    if (accumulate) {
+        BT_CHECK_LAUNCH();
+        return;  // the cells carry over to the next deposit; deposit_cells_finish adds them
+    }
     BT_LAUNCH(ctx, node_accumulate, blocks_for(layout.n_nodes, threads), threads, 0, st, cells, charge, layout.patch_int, layout.n_patches, layout.nx, layout.ny,
         layout.n_nodes, layout.ascending ? 1 : 0);
     BT_CHECK_LAUNCH();
@@ -654,9 +678,9 @@ extern "C" int bt_deposit_trajectories_2d_noalloc(void *stream, const double *px
         BT_CUDA(cudaMemsetAsync(cells, 0, sizeof(double4) * n_nodes, st));
         seg_reduce_warps<<<blocks_for(n_warps * 32, 256), 256, 0, st>>>(
             src_k, src_v, rec, n, nullptr, sentinel, cells, first, last, flags,
-            flags + n_warps);
+            flags + n_warps, 0);
         seg_reduce_chains<<<blocks_for(n_warps, 256), 256, 0, st>>>(
-            src_k, n, nullptr, cells, first, last, flags, flags + n_warps);
+            src_k, n, nullptr, cells, first, last, flags, flags + n_warps, 0);
         node_accumulate<<<blocks_for(n_nodes, 256), 256, 0, st>>>(cells, charge, nullptr, 1, nx,
                                                                  ny, n_nodes, 0);
         BT_CHECK_LAUNCH();

@@ -944,6 +944,10 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                                 cudaMemcpyDeviceToDevice, st));
         BT_CUDA(cudaMemsetAsync(records_end, 0, 2 * sizeof(int64_t), st));
         BT_LAUNCH(ctx, bt::set_count, 1, 1, 0, st, live, a.n_active);
+        // A batch's deposits add their per-cell sums up over the whole trace and reach the
+        // nodes once at its end (a flush then costs only its records, not every node of
+        // every candidate).
+        if (batch) bt::deposit_cells_reset(ctx, a.n_nodes);
         bt::NodeLayout layout{a.patch_int, a.n_patches, tr.nx, tr.ny, a.n_nodes, batch != nullptr};
         int64_t bound = a.n_active, used = 0;
         int lv = 0;
@@ -958,7 +962,7 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
                 SideStream on_side(ctx, ts.side);
                 bt::Timed timed(ctx, "deposit");
                 bt::deposit_records(ctx, keys[cur], rec[cur], used, records_end + cur, sentinel,
-                                    a.charge, layout);
+                                    a.charge, layout, batch != nullptr);
             }
             BT_CUDA(cudaMemsetAsync(records_end + cur, 0, sizeof(int64_t), ts.side));
             BT_CUDA(cudaEventRecord(ts.drained[cur], ts.side));
@@ -1030,6 +1034,7 @@ void trace_all(bt_ctx *ctx, const bt_trace_args *args, const bt_magnetic *mag, i
         // the caller's stream continues once every deposit is in charge[0]
         for (int b = 0; b < 2; ++b)
             if (pending[b]) BT_CUDA(cudaStreamWaitEvent(st, ts.drained[b], 0));
+        if (batch) bt::deposit_cells_finish(ctx, a.charge, layout);
     }
 }
 
