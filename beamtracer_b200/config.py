@@ -302,29 +302,50 @@ class ParticleBeam:
     charge: float = 1.0
     mass: float = 1.007276
 
+    #: The fields read as nested tuples; each is built from its array at its first read
+    #: (a million trajectories take a second to turn into tuples, which a model that
+    #: reads the arrays never needs).
+    _TUPLE_FIELDS: ClassVar[tuple[str, ...]] = ("position", "velocity", "current")
+
     def __post_init__(self) -> None:
-        position = np.asarray(self.position, dtype=float).reshape(-1, 3)
-        velocity = np.asarray(self.velocity, dtype=float).reshape(-1, 3)
-        current = np.asarray(self.current, dtype=float).ravel()
+        position = np.array(self.position, dtype=float).reshape(-1, 3)
+        velocity = np.array(self.velocity, dtype=float).reshape(-1, 3)
+        current = np.array(self.current, dtype=float).ravel()
         if not position.shape[0] == velocity.shape[0] == current.size:
             raise ValueError("position, velocity and current need one row per trajectory")
-        object.__setattr__(self, "position", tuple(map(tuple, position.tolist())))
-        object.__setattr__(self, "velocity", tuple(map(tuple, velocity.tolist())))
-        object.__setattr__(self, "current", tuple(current.tolist()))
-        # the arrays the tuples were made from, so a model reads them without rebuilding
+        for array in (position, velocity, current):
+            array.flags.writeable = False
         object.__setattr__(self, "_arrays", (position, velocity, current))
+        for name, array in zip(self._TUPLE_FIELDS, self._arrays, strict=True):
+            object.__setattr__(self, name, _PendingRows(array))
+
+    def __getattribute__(self, name: str) -> Any:
+        value = object.__getattribute__(self, name)
+        if type(value) is _PendingRows:
+            value = value.rows()
+            object.__setattr__(self, name, value)
+        return value
 
     def arrays(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
-        """Positions and velocities (N, 3) and currents (N,) as float arrays."""
-        arrays = getattr(self, "_arrays", None)
-        if arrays is None or len(arrays[2]) != len(self.current):
-            arrays = (np.asarray(self.position, dtype=float).reshape(-1, 3),
-                      np.asarray(self.velocity, dtype=float).reshape(-1, 3),
-                      np.asarray(self.current, dtype=float).ravel())  # fmt: skip
-        return arrays
+        """Positions and velocities (N, 3) and currents (N,) as read-only float arrays."""
+        return self._arrays
 
     def __len__(self) -> int:
-        return len(self.current)
+        return int(self._arrays[2].size)
+
+
+class _PendingRows:
+    """A `ParticleBeam` field not yet read: the array its tuple is made from."""
+
+    __slots__ = ("array",)
+
+    def __init__(self, array: np.ndarray) -> None:
+        self.array = array
+
+    def rows(self) -> tuple:
+        if self.array.ndim == 1:
+            return tuple(self.array.tolist())
+        return tuple(map(tuple, self.array.tolist()))
 
 
 @dataclass(frozen=True)
