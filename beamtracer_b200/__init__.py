@@ -17,6 +17,7 @@ from beamtracer_b200.config import (
     NegativeExtractionPlasma,
     ObjectParams,
     ParticleBeam,
+    RefinementParams,
     Solenoid,
     SpaceChargeCompensation,
 )
@@ -41,6 +42,7 @@ __all__ = [
     "NegativeExtractionPlasma",
     "ObjectParams",
     "ParticleBeam",
+    "RefinementParams",
     "Solenoid",
     "SpaceChargeCompensation",
     "mismatch",

@@ -166,6 +166,8 @@ SIGNATURES: dict[str, list] = {
     "bt_adjoint_sweep": [P, ctypes.POINTER(AdjointArgs), P, P, P, P],
     "bt_poisson_set_transposed": [P, I32],
     "bt_poisson_fixed_adjoint": [P, P, P, P],
+    "bt_poisson_residual": [P, P, P, P],
+    "bt_csr_apply": [P, I64, P, P, P, P, P, I32, P, P],
     "bt_vlasov_mix": [P, P, P, P, I64, I64, F64, I32, P, P],
     "bt_max_abs_diff": [P, P, P, I64, P],
     "bt_anderson_mix": [P, P, P, P, I64, I64, I32, I32, I32, F64, P, P, P, P, P],

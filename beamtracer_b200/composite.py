@@ -1,0 +1,421 @@
+"""Refined boxes on the B200: the composite field solve and the patches' electric field.
+
+The reference solves the field of refined boxes with patchwork's composite ``NodalPoisson``
+(``solver/poisson.py:169-335``) and takes a trajectory's field and deposit on the finest
+patch holding it (``solver/refinement.py:299-387``, ``tracer.py:1141-1183``).  Here:
+
+- every patch keeps its own device field solver (`IonOpticsPoisson` of its mesh): its rows
+  are the equations of the composite nodes it owns (`beamtracer_b200.refinement`), and its
+  multigrid solves the corrections;
+- the composite solve is a fast adaptive composite (FAC) iteration: per sweep, coarse to
+  fine, the composite residual is taken on a patch's nodes, the patch's homogeneous
+  problem (its held nodes and, for a box, its sides inside the domain at zero) is solved
+  by its multigrid, and the correction is added to the composite nodes in the patch's box
+  (bilinear between the patch's nodes at the finer nodes); sweeps stop when the largest
+  change falls below 1e-12 of the potential's scale;
+- the maps between composite nodes and patch arrays are row-compressed matrices applied
+  by one kernel (``bt_csr_apply``) in a fixed order: the patches' potentials and the wider
+  meshes of their fields (the margin bilinear from the coarser patches, finest wins, as
+  ``solver/refinement.py:299-325``), the composite charges from the patches' deposits, the
+  hanging nodes.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+from scipy import sparse
+from scipy.constants import epsilon_0
+
+from beamtracer_b200 import _lib
+from beamtracer_b200.refinement import Layout, _inside
+
+
+class DeviceCSR:
+    """A row-compressed matrix on the device: ``y[out] = (y[out] or c) + A x`` per row."""
+
+    def __init__(self, matrix: sparse.csr_matrix, out_rows=None, constant=None) -> None:
+        import torch
+
+        matrix = sparse.csr_matrix(matrix)
+        matrix.sort_indices()
+        self.rows = int(matrix.shape[0])
+        self.cols = int(matrix.shape[1])
+        dev = "cuda"
+        self.ptr = torch.from_numpy(matrix.indptr.astype(np.int64)).to(dev)
+        self.col = torch.from_numpy(matrix.indices.astype(np.int64)).to(dev)
+        self.val = torch.from_numpy(matrix.data.astype(np.float64)).to(dev)
+        self.out = (None if out_rows is None
+                    else torch.from_numpy(np.asarray(out_rows, dtype=np.int64)).to(dev))  # fmt: skip
+        self.constant = (None if constant is None
+                         else torch.from_numpy(np.asarray(constant, dtype=np.float64)).to(dev))  # fmt: skip
+
+    def apply(self, x, y, accumulate: bool = False) -> None:
+        d = _lib.dptr
+        _lib.check(_lib.lib().bt_csr_apply(
+            _lib.context().handle, self.rows, d(self.out), d(self.ptr), d(self.col),
+            d(self.val), d(self.constant), int(accumulate), d(x), d(y)))  # fmt: skip
+
+
+def _selection(index: np.ndarray, size: int, value: float = 1.0) -> sparse.csr_matrix:
+    """Rows picking ``index`` out of ``size`` entries (times ``value``)."""
+    index = np.asarray(index, dtype=np.int64).ravel()
+    return sparse.csr_matrix((np.full(index.size, value), (np.arange(index.size), index)),
+                             shape=(index.size, size))  # fmt: skip
+
+
+def prolongation(layout: Layout, number: int) -> tuple[sparse.csr_matrix, np.ndarray]:
+    """The free composite nodes in patch ``number``'s box and, per node, the bilinear weights
+    of the patch's nodes at it (the node's own value where it is one of them)."""
+    patch = layout.patches[number]
+    finest = max(p.level for p in layout.patches)
+    s = 2 ** (finest - patch.level)
+    (i0, _), (j0, _) = patch.box
+    nxp, nyp = patch.mesh.shape
+    li = layout.lattice[:, 0] / s - i0
+    lj = layout.lattice[:, 1] / s - j0
+    mine = np.flatnonzero((li >= 0) & (li <= nxp - 1) & (lj >= 0) & (lj <= nyp - 1)
+                          & ~layout.fixed)  # fmt: skip
+    a = np.clip(np.floor(li[mine]).astype(np.int64), 0, nxp - 2)
+    b = np.clip(np.floor(lj[mine]).astype(np.int64), 0, nyp - 2)
+    u, w = li[mine] - a, lj[mine] - b
+    rows = np.tile(np.arange(mine.size), 4)
+    cols = np.concatenate([a * nyp + b, a * nyp + b + 1, (a + 1) * nyp + b, (a + 1) * nyp + b + 1])
+    vals = np.concatenate([(1 - u) * (1 - w), (1 - u) * w, u * (1 - w), u * w])
+    keep = vals != 0.0
+    matrix = sparse.csr_matrix((vals[keep], (rows[keep], cols[keep])),
+                               shape=(mine.size, nxp * nyp))  # fmt: skip
+    return matrix, mine
+
+
+class CompositePoisson:
+    """The field of a refined layout solved on the device (linear; see the module).
+
+    ``solve_device(phi, rho)`` takes composite device vectors: ``phi`` the first guess (its
+    held and hanging nodes are set) and the result, ``rho`` [C/m^3] or None.
+    """
+
+    def __init__(self, layout: Layout, *, tolerance: float = 1e-12, max_sweeps: int = 100,
+                 correction_tolerance: float = 1e-10) -> None:  # fmt: skip
+        import torch
+
+        from beamtracer_b200.poisson import IonOpticsPoisson
+
+        self.layout = layout
+        self.tolerance = float(tolerance)
+        self.max_sweeps = int(max_sweeps)
+        self.correction_tolerance = float(correction_tolerance)
+        patches = layout.patches
+        n = layout.size
+        base_shape = layout.base.mesh.shape
+        #: every patch's own operator (its rows: the equations of the nodes it owns)
+        self.rows = [IonOpticsPoisson(p.mesh) for p in patches]
+        #: the corrections' solvers: held values and face terms zero, a box's sides held
+        self.corrections = []
+        #: the nodes each correction holds besides the patch's own (a box's sides)
+        self._sides = []
+        for number, patch in enumerate(patches):
+            solver = IonOpticsPoisson(patch.mesh, homogeneous=True)
+            self._sides.append(None if number == 0 else ~_inside(patch, base_shape))
+            self.corrections.append(solver)
+        sizes = [int(np.prod(p.mesh.shape)) for p in patches]
+        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        total = int(self.offsets[-1])
+        dev = "cuda"
+        f64 = torch.float64
+        self._phi_p = torch.zeros(total, dtype=f64, device=dev)
+        self._rho_p = torch.zeros(total, dtype=f64, device=dev)
+        self._res_p = torch.zeros(total, dtype=f64, device=dev)
+        self._rhs_p = torch.zeros(total, dtype=f64, device=dev)
+        self._e_p = torch.zeros(total, dtype=f64, device=dev)
+        self._r = torch.zeros(n, dtype=f64, device=dev)
+        self._prev = torch.zeros(n, dtype=f64, device=dev)
+        self._zero = torch.zeros(max(n, 1), dtype=f64, device=dev)
+        self._scalars = torch.zeros(2, dtype=f64, device=dev)
+        self._gather = [DeviceCSR(_selection(p.index, n)) for p in patches]
+        self._gather_eps = [DeviceCSR(_selection(p.index, n, epsilon_0)) for p in patches]
+        owned = np.flatnonzero((layout.owner >= 0) & ~layout.fixed)
+        cols = self.offsets[layout.owner[owned]] + layout.owner_node[owned]
+        self._owned = DeviceCSR(sparse.csr_matrix(
+            (np.ones(owned.size), (owned, cols)), shape=(n, total)))  # fmt: skip
+        self._prolong = []
+        for number in range(len(patches)):
+            matrix, rows = prolongation(layout, number)
+            self._prolong.append(DeviceCSR(matrix, out_rows=rows))
+        held = np.flatnonzero(layout.fixed)
+        self._held = DeviceCSR(sparse.csr_matrix((held.size, 1)), out_rows=held,
+                               constant=layout.fixed_value[held])  # fmt: skip
+        self._hang = (DeviceCSR(layout.interpolation, out_rows=layout.hanging)
+                      if layout.hanging.size else None)  # fmt: skip
+        #: FAC sweeps of the last solve, and their corrections' V-cycles
+        self.sweeps = 0
+        self.krylov_steps = 0
+
+    def _view(self, buffer, number: int):
+        lo, hi = self.offsets[number], self.offsets[number + 1]
+        return buffer[lo:hi].view(self.layout.patches[number].mesh.shape)
+
+    def fill_hanging(self, phi) -> None:
+        if self._hang is not None:
+            self._hang.apply(phi, phi)
+
+    def residual(self, phi, r) -> None:
+        """``r`` <- the composite residual of ``phi`` (zero on held and hanging nodes), with
+        the charge density last given to `solve_device`."""
+        self.fill_hanging(phi)
+        lib = _lib.lib()
+        for number, solver in enumerate(self.rows):
+            phi_p = self._view(self._phi_p, number)
+            self._gather[number].apply(phi, phi_p)
+            _lib.check(lib.bt_poisson_residual(solver._handle, _lib.dptr(phi_p),
+                                               _lib.dptr(self._view(self._rho_p, number)),
+                                               _lib.dptr(self._view(self._res_p, number))))  # fmt: skip
+        self._owned.apply(self._res_p, r)
+
+    def _max(self, a, b=None) -> float:
+        n = self.layout.size
+        _lib.check(_lib.lib().bt_max_abs_diff(_lib.context().handle, _lib.dptr(a),
+                                              _lib.dptr(self._zero if b is None else b), n,
+                                              _lib.dptr(self._scalars)))  # fmt: skip
+        return float(self._scalars[0])
+
+    def solve_device(self, phi, rho=None) -> None:
+        n = self.layout.size
+        if tuple(phi.shape) != (n,) or (rho is not None and tuple(rho.shape) != (n,)):
+            raise ValueError(f"the composite solve takes ({n},) composite vectors")
+        if rho is None:
+            self._rho_p.zero_()
+        else:
+            for number in range(len(self.rows)):
+                self._gather[number].apply(rho, self._view(self._rho_p, number))
+        self._held.apply(phi, phi)
+        self.fill_hanging(phi)
+        cycles = 0
+        for sweep in range(1, self.max_sweeps + 1):
+            self._prev.copy_(phi)
+            for number, solver in enumerate(self.corrections):
+                self.residual(phi, self._r)
+                rhs = self._view(self._rhs_p, number)
+                e = self._view(self._e_p, number)
+                self._gather_eps[number].apply(self._r, rhs)
+                e.zero_()
+                solver.solve_device(e, rhs, fixed_region=self._sides[number],
+                                    linear_tolerance=self.correction_tolerance)
+                cycles += solver.krylov_steps
+                self._prolong[number].apply(e.reshape(-1), phi, accumulate=True)
+            self.fill_hanging(phi)
+            change = self._max(phi, self._prev)
+            scale = max(self._max(phi), 1.0)
+            if not np.isfinite(change):
+                raise RuntimeError("the composite field solve diverged (a non-finite update)")
+            if change <= self.tolerance * scale:
+                break
+        else:
+            raise RuntimeError(f"the composite field solve did not converge in "
+                               f"{self.max_sweeps} sweeps")  # fmt: skip
+        self.sweeps = sweep
+        self.krylov_steps = cycles
+
+    def close(self) -> None:
+        for solver in (*self.rows, *self.corrections):
+            solver.close()
+
+
+def _extrapolation(mesh) -> list[str]:
+    """Linear extrapolation on every face, mirror on the y_min face where it is the axis or
+    a symmetry plane (``solver/refinement.py:289-295``)."""
+    faces = ["extrapolate"] * 4
+    on_axis = mesh.cylindrical and abs(mesh.origin[1]) <= 1e-12 * mesh.h
+    if on_axis or mesh.symmetry_plane:
+        faces[2] = "symmetric"
+    return faces
+
+
+class PatchedFieldMaps:
+    """What the electric field of a layout needs on the device, built once per layout: per
+    patch the map from composite potentials to its field mesh's nodes, the field meshes'
+    classification, the edge fields' flat buffers and the tracer's patch tables (finest
+    first, the base last: ``tracer.py:1141-1183``), and the map from the deposit's patch
+    charges (their boxes' nodes) to composite charges."""
+
+    def __init__(self, layout: Layout) -> None:
+        import torch
+
+        from beamtracer_b200.fields import MeshArrays
+
+        self.layout = layout
+        patches = layout.patches
+        n = layout.size
+        self.meshes = [p.field_mesh if p.field_mesh is not None else p.mesh for p in patches]
+        matrices, constants = [], []
+        for number, patch in enumerate(patches):
+            mesh = self.meshes[number]
+            nxf, nyf = mesh.shape
+            if patch.field_mesh is None:
+                matrix = _selection(patch.index, n)
+                constant = np.zeros(nxf * nyf)
+            else:
+                matrix, constant = self._margin(matrices, constants, mesh)
+                solid = np.asarray(mesh.solid).ravel() >= 0
+                keep = sparse.diags((~solid).astype(float))
+                matrix = (keep @ matrix).tocsr()
+                constant = np.where(solid, np.asarray(mesh.fixed_value).ravel(), constant)
+                inner = np.zeros((nxf, nyf), dtype=bool)
+                inner[patch.inner] = True
+                inner = inner.ravel()
+                rows = np.flatnonzero(inner)
+                matrix = sparse.lil_matrix(matrix)
+                for r, k in zip(rows, patch.index.ravel()):
+                    matrix.rows[r] = [int(k)]
+                    matrix.data[r] = [1.0]
+                matrix = matrix.tocsr()
+                constant = np.where(inner, 0.0, constant)
+            matrix.eliminate_zeros()
+            matrices.append(matrix)
+            constants.append(constant)
+        self.potential_maps = [DeviceCSR(m, constant=c) for m, c in zip(matrices, constants)]
+        self.arrays = [MeshArrays(mesh) for mesh in self.meshes]
+        # flat edge-field buffers and the tracer's tables, finest first
+        order = list(range(len(patches)))[::-1]
+        fx_sizes = [(self.meshes[q].shape[0] + 1) * self.meshes[q].shape[1] for q in order]
+        fy_sizes = [self.meshes[q].shape[0] * (self.meshes[q].shape[1] + 1) for q in order]
+        node_sizes = [self.meshes[q].shape[0] * self.meshes[q].shape[1] for q in order]
+        fx_off = np.concatenate([[0], np.cumsum(fx_sizes)]).astype(np.int64)
+        fy_off = np.concatenate([[0], np.cumsum(fy_sizes)]).astype(np.int64)
+        node_off = np.concatenate([[0], np.cumsum(node_sizes)]).astype(np.int64)
+        dev = "cuda"
+        self.fx = torch.zeros(int(fx_off[-1]), dtype=torch.float64, device=dev)
+        self.fy = torch.zeros(int(fy_off[-1]), dtype=torch.float64, device=dev)
+        self.values = [torch.zeros(m.shape, dtype=torch.float64, device=dev) for m in self.meshes]
+        self.field_views = {}
+        ints, reals = [], []
+        for slot, q in enumerate(order):
+            mesh = self.meshes[q]
+            nxf, nyf = mesh.shape
+            self.field_views[q] = (
+                self.fx[fx_off[slot]:fx_off[slot + 1]].view(nxf + 1, nyf),
+                self.fy[fy_off[slot]:fy_off[slot + 1]].view(nxf, nyf + 1),
+            )
+            ints.append([nxf, nyf, fx_off[slot], fy_off[slot], nxf * nyf, node_off[slot]])
+            x0, y0, x1, y1 = patches[q].bounds
+            reals.append([mesh.origin[0], mesh.origin[1], mesh.h, x0, y0, x1, y1])
+        self.patch_int = torch.tensor(ints, dtype=torch.int64, device=dev)
+        self.patch_real = torch.tensor(reals, dtype=torch.float64, device=dev)
+        self.n_field_nodes = int(node_off[-1])
+        # composite charges: each node sums its boxes' node charges, coarse to fine
+        rows, cols = [], []
+        for q, patch in enumerate(patches):
+            slot = order.index(q)
+            nxf, nyf = self.meshes[q].shape
+            local = np.arange(nxf * nyf).reshape(nxf, nyf)[patch.inner]
+            rows.append(patch.index.ravel())
+            cols.append(node_off[slot] + local.ravel())
+        rows = np.concatenate(rows)
+        cols = np.concatenate(cols)
+        order_rows = np.argsort(rows, kind="stable")
+        self.charge_map = DeviceCSR(sparse.csr_matrix(
+            (np.ones(rows.size), (rows[order_rows], cols[order_rows])),
+            shape=(n, self.n_field_nodes)))  # fmt: skip
+        self.volumes = torch.from_numpy(np.ascontiguousarray(layout.volumes)).to(dev)
+
+    def _margin(self, matrices, constants, mesh):
+        """The field mesh's nodes from the patches done so far (finest containing wins)."""
+        xn, yn = mesh.nodes()
+        x, y = xn.ravel(), yn.ravel()
+        total = x.size
+        n = self.layout.size
+        matrix = sparse.csr_matrix((total, n))
+        constant = np.zeros(total)
+        for number, (done, c_done) in enumerate(zip(matrices, constants)):
+            patch = self.layout.patches[number]
+            dmesh = self.meshes[number]
+            x0, y0, x1, y1 = patch.bounds
+            inside = np.flatnonzero((x >= x0) & (x <= x1) & (y >= y0) & (y <= y1))
+            if not inside.size:
+                continue
+            nxd, nyd = dmesh.shape
+            s = (x[inside] - dmesh.origin[0]) / dmesh.h
+            t = (y[inside] - dmesh.origin[1]) / dmesh.h
+            i = np.clip(np.floor(s).astype(np.int64), 0, nxd - 2)
+            j = np.clip(np.floor(t).astype(np.int64), 0, nyd - 2)
+            u, w = s - i, t - j
+            rows = np.tile(np.arange(inside.size), 4)
+            cols = np.concatenate([i * nyd + j, i * nyd + j + 1, (i + 1) * nyd + j,
+                                   (i + 1) * nyd + j + 1])  # fmt: skip
+            vals = np.concatenate([(1 - u) * (1 - w), (1 - u) * w, u * (1 - w), u * w])
+            weights = sparse.csr_matrix((vals, (rows, cols)), shape=(inside.size, nxd * nyd))
+            part = (weights @ done).tocsr()
+            part_c = weights @ c_done
+            pick = sparse.csr_matrix((np.ones(inside.size), (inside, np.arange(inside.size))),
+                                     shape=(total, inside.size))  # fmt: skip
+            drop = np.ones(total)
+            drop[inside] = 0.0
+            matrix = (sparse.diags(drop) @ matrix + pick @ part).tocsr()
+            constant = drop * constant + pick @ part_c
+        return matrix, constant
+
+
+class PatchedElectricField:
+    """The electric field of a composite potential: a `StaggeredElectricField` per patch on
+    its field mesh (``solver/refinement.py:328-387``).  At a point the field is that of the
+    finest patch containing it; ``fx``, ``fy`` are the base patch's."""
+
+    def __init__(self, layout: Layout, potential, *, maps: PatchedFieldMaps | None = None) -> None:
+        import torch
+
+        from beamtracer_b200.fields import StaggeredElectricField
+
+        self.layout = layout
+        self.patches = layout.patches
+        self.maps = maps or PatchedFieldMaps(layout)
+        if _lib.is_device_array(potential):
+            phi = potential
+        else:
+            phi = torch.from_numpy(np.ascontiguousarray(potential, dtype=np.float64)).cuda()
+        if tuple(phi.shape) != (layout.size,):
+            raise ValueError("the potential needs the layout's composite nodes")
+        self.fields = []
+        for number, mesh in enumerate(self.maps.meshes):
+            values = self.maps.values[number]
+            self.maps.potential_maps[number].apply(phi, values)
+            self.fields.append(StaggeredElectricField(
+                mesh, values, _extrapolation(mesh), arrays=self.maps.arrays[number],
+                out=self.maps.field_views[number]))  # fmt: skip
+        self.mesh = layout.base.mesh
+        self.fx_device = self.maps.fx
+        self.fy_device = self.maps.fy
+
+    @property
+    def fx(self) -> np.ndarray:
+        return self.fields[0].fx
+
+    @property
+    def fy(self) -> np.ndarray:
+        return self.fields[0].fy
+
+    def patch_of(self, x, y) -> np.ndarray:
+        """The finest patch containing each point."""
+        x, y = np.asarray(x, dtype=float), np.asarray(y, dtype=float)
+        which = np.zeros(np.shape(x), dtype=np.int64)
+        for number, patch in enumerate(self.patches[1:], start=1):
+            x0, y0, x1, y1 = patch.bounds
+            which[(x >= x0) & (x <= x1) & (y >= y0) & (y <= y1)] = number
+        return which
+
+    def __call__(self, x, y) -> tuple[np.ndarray, np.ndarray]:
+        """``(E_x, E_y)`` [V/m] at the points ``(x, y)``."""
+        x = np.ascontiguousarray(x, dtype=float).ravel()
+        y = np.ascontiguousarray(y, dtype=float).ravel()
+        ex, ey = self.fields[0](x, y)
+        ex, ey = np.array(ex), np.array(ey)
+        which = self.patch_of(x, y)
+        for number in range(1, len(self.patches)):
+            inside = which == number
+            if inside.any():
+                ex[inside], ey[inside] = self.fields[number](x[inside], y[inside])
+        return ex, ey
+
+
+def composite_density(maps: PatchedFieldMaps, charge, out) -> None:
+    """``out`` (composite) <- the patches' node charges ``charge`` (flat, finest first) summed
+    on the composite nodes (coarse to fine), not yet divided by the volumes."""
+    maps.charge_map.apply(charge.reshape(-1), out)

@@ -397,6 +397,30 @@ class Solenoid:
 
 
 @dataclass(frozen=True)
+class RefinementParams:
+    """A box refined to ``level`` (cells ``2**level`` times smaller than the grid's;
+    ``config.py:437-464``).  ``lower`` and ``upper`` are its corners ``(x, y)`` [m]
+    (``(x, r)`` in cylindrical geometry), widened to the cells of the level below; a
+    level's boxes lie inside those of the level below."""
+
+    level: int
+    lower: tuple[float, ...]
+    upper: tuple[float, ...]
+
+    def __post_init__(self) -> None:
+        if int(self.level) != self.level or self.level < 1:
+            raise ValueError(f"level must be a positive integer, got {self.level}")
+        object.__setattr__(self, "level", int(self.level))
+        lower = tuple(float(v) for v in self.lower)
+        upper = tuple(float(v) for v in self.upper)
+        if (len(lower) not in (2, 3) or len(upper) != len(lower)
+                or not all(a < b for a, b in zip(lower, upper))):  # fmt: skip
+            raise ValueError(f"a refined box needs lower < upper, got {lower}, {upper}")
+        object.__setattr__(self, "lower", lower)
+        object.__setattr__(self, "upper", upper)
+
+
+@dataclass(frozen=True)
 class SpaceChargeCompensation:
     """The beam's space charge reduced by ``fraction`` between ``x_min`` and ``x_max``."""
 
@@ -497,6 +521,13 @@ class BeamOpticsConfig:
         if not 0 <= int(self.field_order) <= 6:
             raise ValueError(f"field_order must be 0 to 6, got {self.field_order}")
         self.compensation = [_coerce(SpaceChargeCompensation, c) for c in self.compensation]
+        self.refinement = [
+            box if isinstance(box, RefinementParams)
+            else RefinementParams(**box) if isinstance(box, Mapping) else RefinementParams(*box)
+            for box in (self.refinement or [])
+        ]  # fmt: skip
+        if any(len(box.lower) != 2 for box in self.refinement):
+            raise ValueError("a 2D grid takes refined boxes of (x, y) corners")
         self.diagnostic_planes = [float(p) for p in self.diagnostic_planes]
         if (self.solenoids or self.axial_field) and self.grid.coordinates != "cylindrical":
             raise ValueError("solenoids need cylindrical coordinates (or a 3D grid, on the x axis)")
@@ -523,7 +554,7 @@ class BeamOpticsConfig:
             raise ValueError("symmetry_plane needs a planar (cartesian) grid")
         unsupported = {
             "field_map": self.field_map, "charge_changing": self.charge_changing,
-            "refinement": self.refinement, "adaptive_refinement": self.adaptive_refinement,
+            "adaptive_refinement": self.adaptive_refinement,
             "self_magnetic_field": self.self_magnetic_field,
         }  # fmt: skip
         given = sorted(name for name, value in unsupported.items() if value)
@@ -556,6 +587,7 @@ class BeamOpticsConfig:
         if self.axial_field is not None:
             params["axial_field"] = asdict(self.axial_field)
         params["compensation"] = [asdict(c) for c in self.compensation]
+        params["refinement"] = [asdict(box) for box in self.refinement]
         return params
 
     @classmethod

@@ -59,7 +59,7 @@ __device__ __forceinline__ double pw(const int32_t *lo, const double *w, i64 k, 
 // -- the fine operator (mirrors oracle/poisson.py:coefficients) ---------------------------
 
 __global__ void build_fine(i64 nx, i64 ny, const double *__restrict__ x, double h, int cyl,
-                           const uint8_t *__restrict__ fixed, const double *__restrict__ dist,
+                           i64 j0, const uint8_t *__restrict__ fixed, const double *__restrict__ dist,
                            double g0, double g1, double g2, double g3,
                            double *__restrict__ c4, double *__restrict__ base,
                            double *__restrict__ src, double *__restrict__ weight,
@@ -111,7 +111,8 @@ __global__ void build_fine(i64 nx, i64 ny, const double *__restrict__ x, double 
             s += 2.0 * g3 / h;
         }
     } else {
-        const double jj = j > 1 ? (double)j : 1.0;
+        // the radial index of the row: j0 = r_0 / h for a refined patch off the axis
+        const double jj = j + j0 > 1 ? (double)(j + j0) : 1.0;
         const double h2 = h * h;
         if (mid) {
             if (four) {
@@ -122,7 +123,9 @@ __global__ void build_fine(i64 nx, i64 ny, const double *__restrict__ x, double 
                 cn = (1.0 + 0.5 / jj) / (by * h2);
             }
         } else if (j == 0) {
-            cn = 4.0 / (by * h2);
+            // the axis; off the axis (a patch's side inside the domain, a row the
+            // composite operator does not use) a face row
+            cn = (j0 == 0 ? 4.0 : 2.0) / (by * h2);
         } else {
             cs = 2.0 / (ay * h2);
             s += (1.0 + 0.5 / jj) * 2.0 * g3 / h;
@@ -139,7 +142,7 @@ __global__ void build_fine(i64 nx, i64 ny, const double *__restrict__ x, double 
     // the control volume (divided by 2 pi in cylindrical geometry)
     const double lx = 0.5 * (h_lo + h_hi);  // half an edge at an x face
     double ly = (j > 0 && j < ny - 1) ? h : 0.5 * h;
-    if (cyl) ly = j == 0 ? 0.125 * h * h : (double)j * h * ly;
+    if (cyl) ly = j + j0 == 0 ? 0.125 * h * h : (double)(j + j0) * h * ly;
     weight[t] = lx * ly;
 }
 
@@ -1462,6 +1465,7 @@ struct bt_poisson {
     i64 nx = 0, ny = 0, n = 0;
     double h = 0.0;
     int cyl = 0;
+    i64 j0 = 0;  // the radial index of the first row (origin_y / h; cylindrical)
     double neumann[4] = {0, 0, 0, 0};
     bt::Buffer x, fixed, value, distance, region;  // mesh; region: the extra held nodes
     bt::Buffer fixed_eff, value_eff, src;
@@ -1543,7 +1547,7 @@ void build_operator(bt_poisson *p) {
     cudaStream_t st = p->ctx->stream;
     Level &L = p->levels[0];
     const i64 n = p->n;
-    BT_LAUNCH(p->ctx, build_fine, blocks_for(n, 256), 256, 0, st, p->nx, p->ny, p->x.as<double>(p->nx), p->h, p->cyl, p->fixed_eff.as<uint8_t>(n),
+    BT_LAUNCH(p->ctx, build_fine, blocks_for(n, 256), 256, 0, st, p->nx, p->ny, p->x.as<double>(p->nx), p->h, p->cyl, p->j0, p->fixed_eff.as<uint8_t>(n),
         p->distance.as<double>(4 * n), p->neumann[0], p->neumann[1], p->neumann[2],
         p->neumann[3], L.c4.as<double>(4 * n), L.base.as<double>(n), p->src.as<double>(n),
         L.weight.as<double>(n), L.active.as<uint8_t>(n));
@@ -1991,6 +1995,13 @@ extern "C" int bt_poisson_create(bt_ctx *ctx, const bt_mesh_desc *m, bt_poisson 
             p->n = m->nx * m->ny;
             p->h = m->h;
             p->cyl = m->cylindrical;
+            if (p->cyl) {
+                const double rows = m->origin_y / m->h;
+                p->j0 = (i64)llround(rows);
+                BT_REQUIRE(p->j0 >= 0 && std::fabs(rows - (double)p->j0) <= 1e-6,
+                           "poisson: a cylindrical mesh starts on the axis or a multiple of h "
+                           "above it");
+            }
             for (int q = 0; q < 4; ++q) p->neumann[q] = m->neumann ? m->neumann[q] : 0.0;
             const i64 n = p->n;
             BT_CUDA(cudaMemcpy(p->x.as<double>(p->nx), m->x, sizeof(double) * p->nx, cudaMemcpyHostToDevice));
@@ -2154,6 +2165,46 @@ extern "C" int bt_poisson_solve(bt_poisson *p, double *phi, const double *rho, d
             throw bt::Error{BT_ERR_NOCONV, "field solve: the coarsest operator is singular (is any node held?)"};
         if (newton_steps) *newton_steps = steps;
         if (cycles) *cycles = total_cycles;
+    });
+}
+
+namespace bt {
+namespace {
+// r = rho / eps0 + c - A phi on the free nodes of the level-0 operator (its diagonal
+// without a Newton reaction), 0 on the held ones
+__global__ void linear_residual(i64 nx, i64 ny, const double *__restrict__ c4,
+                                const double *__restrict__ base, const double *__restrict__ src,
+                                const uint8_t *__restrict__ active, const double *__restrict__ phi,
+                                const double *__restrict__ rho, double *__restrict__ r) {
+    const i64 n = nx * ny;
+    const i64 f = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    if (!active[f]) {
+        r[f] = 0.0;
+        return;
+    }
+    const i64 i = f / ny, j = f - i * ny;
+    double s = base[f] * phi[f];
+    if (i > 0) s -= c4[f] * phi[f - ny];
+    if (i < nx - 1) s -= c4[n + f] * phi[f + ny];
+    if (j > 0) s -= c4[2 * n + f] * phi[f - 1];
+    if (j < ny - 1) s -= c4[3 * n + f] * phi[f + 1];
+    r[f] = (rho ? rho[f] / kEps0 : 0.0) + src[f] - s;
+}
+}  // namespace
+}  // namespace bt
+
+extern "C" int bt_poisson_residual(bt_poisson *p, const double *phi, const double *rho,
+                                   double *r) {
+    return bt::guarded([&] {
+        BT_REQUIRE(p && phi && r, "poisson residual: null argument");
+        BT_REQUIRE(!p->transposed, "poisson residual: the solver is transposed");
+        const i64 n = p->n;
+        bt::Level &L0 = p->levels[0];
+        BT_LAUNCH(p->ctx, bt::linear_residual, bt::blocks_for(n, 256), 256, 0, p->ctx->stream, p->nx, p->ny,
+                  L0.c4.as<double>(4 * n), L0.base.as<double>(n), p->src.as<double>(n),
+                  L0.active.as<uint8_t>(n), phi, rho, r);
+        BT_CHECK_LAUNCH();
     });
 }
 

@@ -25,6 +25,7 @@ from beamtracer_b200.config import (
 from beamtracer_b200.diagnostics import BeamMoments, plane_moments
 from beamtracer_b200.fields import AxisymmetricMagneticField, solenoid_on_axis
 from beamtracer_b200.mesh import Electrode, FaceCondition, IonOpticsMesh
+from beamtracer_b200.refinement import Refinement
 from beamtracer_b200.tracer import (
     STATUS_NAMES,
     BeamParticles,
@@ -226,6 +227,7 @@ class BeamOptics:
             anderson_depth=config.anderson_depth, coarse_particles=config.coarse_particles,
             coarse_tolerance=config.coarse_tolerance, field_backend=config.field_backend,
             callback=callback, density_tolerance=density_tolerance,
+            refinement=[Refinement(b.level, b.lower, b.upper) for b in config.refinement],
         )  # fmt: skip
         if self.size > 1:
             from beamtracer_b200.distributed import gather_trace

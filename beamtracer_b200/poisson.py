@@ -82,8 +82,11 @@ class IonOpticsPoisson:
     """Solve ``laplace(phi) = -rho / epsilon_0`` (plus a Boltzmann species) on a mesh.
 
     ``backend`` is accepted for the reference's signature; every backend is the device's
-    multigrid-preconditioned GMRES.  Refined boxes (``refinement``) and a distributed
-    solve (``comm``) are not part of this build.
+    multigrid-preconditioned GMRES.  With refined boxes (``refinement``, linear solves) the
+    potential and charge density live on the composite nodes of `layout`
+    (`beamtracer_b200.composite.CompositePoisson`).  A distributed solve (``comm``) is not
+    part of this build.  ``homogeneous`` zeroes the held values and face terms (the
+    corrections of the composite solve).
     """
 
     def __init__(
@@ -95,14 +98,23 @@ class IonOpticsPoisson:
         refinement=(),
         *,
         transposed: bool = False,
+        homogeneous: bool = False,
     ) -> None:
-        if tuple(refinement):
-            raise NotImplementedError("refined boxes are not supported by this build")
         self.mesh = mesh
         self.reuse_jacobian = bool(reuse_jacobian)
         self.backend = backend
         self.comm = comm
-        self.refinement = ()
+        self.refinement = tuple(refinement)
+        self._layout = None
+        self._composite = None
+        if self.refinement:
+            if transposed:
+                raise NotImplementedError("the transposed solver takes no refined boxes")
+            from beamtracer_b200.composite import CompositePoisson
+            from beamtracer_b200.refinement import layout_of_mesh
+
+            self._layout = layout_of_mesh(mesh, self.refinement)
+            self._composite = CompositePoisson(self._layout)
         #: Newton steps, V-cycles of the last solve (the reference's factorisations and
         #: Krylov steps have no counterpart: every step is a Krylov solve).
         self.newton_iterations = 0
@@ -118,7 +130,7 @@ class IonOpticsPoisson:
         #: a solver of the transposed free block A_ff^T z = b (held values and face terms
         #: zero), for the adjoint; linear solves only
         self.transposed = bool(transposed)
-        if self.transposed:
+        if self.transposed or homogeneous:
             self._value = np.zeros_like(self._value)
             self._neumann = np.zeros_like(self._neumann)
         desc = _lib.MeshDesc(
@@ -133,6 +145,16 @@ class IonOpticsPoisson:
         self._region_key: object = None
         if self.transposed:
             _lib.check(_lib.lib().bt_poisson_set_transposed(handle, 1))
+
+    @property
+    def layout(self):
+        """The composite nodes the potential lives on (the mesh's own nodes without refined
+        boxes; ``poisson.py:611-616``)."""
+        if self._layout is None:
+            from beamtracer_b200.refinement import layout_of_mesh
+
+            self._layout = layout_of_mesh(self.mesh)
+        return self._layout
 
     def fixed_adjoint(self, z, phi_bar, out) -> None:
         """``out`` (device, (nx, ny)) <- the sensitivity to the held nodes' potentials of a
@@ -149,6 +171,9 @@ class IonOpticsPoisson:
         self._ctx = ctx
 
     def close(self) -> None:
+        if getattr(self, "_composite", None) is not None:
+            self._composite.close()
+            self._composite = None
         if getattr(self, "_handle", None):
             _lib.lib().bt_poisson_destroy(self._handle)
             self._handle = None
@@ -214,6 +239,14 @@ class IonOpticsPoisson:
         With ``plasma`` Newton's method stops when its largest update is below
         ``tolerance * max(ptp(prescribed potentials), T, 1 V)`` (``poisson.py:874-877``).
         """
+        if self._composite is not None:
+            if plasma is not None or fixed_region is not None:
+                raise NotImplementedError(
+                    "refined boxes take linear field solves (no plasma, no held region)")
+            self._composite.solve_device(phi, rho)
+            self.newton_iterations = 0
+            self.krylov_steps = self._composite.krylov_steps
+            return
         self._set_region(fixed_region, fixed_potential)
         if self.transposed and (plasma is not None or fixed_region is not None):
             raise NotImplementedError("the transposed solver takes linear solves only")
@@ -261,13 +294,14 @@ class IonOpticsPoisson:
         """
         import torch
 
-        shape = self.mesh.shape
+        shape = self.mesh.shape if self._composite is None else (self._layout.size,)
         phi = torch.zeros(shape, dtype=torch.float64, device="cuda")
         rho_dev = None
         if rho is not None:
             rho = np.asarray(rho, dtype=np.float64)
             if rho.shape != shape:
-                raise ValueError("rho needs the mesh's shape (refined layouts are not supported)")
+                raise ValueError(f"rho needs the shape {shape} (the mesh's, or the refined "
+                                 "layout's composite nodes)")
             rho_dev = torch.from_numpy(np.ascontiguousarray(rho)).cuda()
         if initial is not None:
             phi.copy_(torch.from_numpy(np.ascontiguousarray(initial, dtype=np.float64)))

@@ -399,6 +399,20 @@ class TraceEngine:
         self._charge = None
         self.particles: BeamParticles | None = None
 
+    def set_patches(self, patch_int, patch_real, n_nodes: int) -> None:
+        """Trace through the patches of refined boxes (device tables of the kernel's
+        ``patch_int`` (P, 6) and ``patch_real`` (P, 7), finest first and the base mesh last,
+        ``tracer.py:1141-1183``): the edge fields given to `run` are the patches' flattened
+        one after the other, and the node charges fill ``n_nodes`` (every patch's field
+        mesh nodes, in the same order)."""
+        if self.mesh.graded:
+            raise NotImplementedError("refined boxes on a graded x axis")
+        self.patch_int = patch_int
+        self.patch_real = patch_real
+        if int(n_nodes) != self.n_nodes:
+            self.n_nodes = int(n_nodes)
+            self._charge = None
+
     @property
     def charge(self):
         """The node charges of the last run (device (1, nodes))."""
@@ -499,7 +513,8 @@ class TraceEngine:
         a = _lib.TraceArgs(
             d(active), int(active.numel()), d(self.x), d(self.v), self.n, d(self.qm),
             d(self.dq), d(self.steps), d(self.status), d(self.electrode), d(fx), d(fy),
-            d(self.patch_int), d(self.patch_real), 1, float(lo_x), float(lo_y), float(mesh.h),
+            d(self.patch_int), d(self.patch_real), int(self.patch_int.shape[0]), float(lo_x),
+            float(lo_y), float(mesh.h),
             float(up_x), float(up_y), geometry_code(mesh), INTEGRATORS.index(self.integrator),
             self.step_fraction, self.max_steps, d(self.cells), d(self.subcells), SUBCELLS,
             d(self.planes_dev), int(self.planes_dev.numel()), d(self.hits),
@@ -562,6 +577,8 @@ class TraceEngine:
 
     def density(self):
         """The charge density on the nodes (device (nx, ny)): charges over volumes."""
+        if int(self.patch_int.shape[0]) > 1:
+            raise RuntimeError("a trace through refined boxes has composite densities")
         return (self.charge[0] / self.volumes.reshape(-1)).reshape(self.mesh.shape)
 
     def result(self, density=None) -> TraceResult:

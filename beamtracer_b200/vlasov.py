@@ -247,11 +247,22 @@ def vlasov_iterate(
         raise ValueError(f"mixing must be 'linear' or 'anderson', got {mixing!r}")
     if not 0.0 < coarse_particles <= 1.0:
         raise ValueError(f"coarse_particles must be in (0, 1], got {coarse_particles}")
-    if tuple(refinement) or adaptive is not None or self_magnetic:
+    if adaptive is not None or self_magnetic:
         raise NotImplementedError(
-            "refined boxes, adaptive refinement and the self magnetic field are not part "
-            "of this build"
+            "adaptive refinement and the self magnetic field are not part of this build"
         )
+    if tuple(refinement):
+        if plasma is not None or tuple(compensation) or coarse_particles < 1.0:
+            raise NotImplementedError(
+                "refined boxes take a linear field solve (no plasma), no compensation and "
+                "no coarse phase in this build"
+            )
+        return _iterate_refined(
+            mesh, make_particles, tracer, iterations=iterations, tolerance=tolerance,
+            relaxation=relaxation, mixing=mixing, anderson_depth=anderson_depth,
+            refinement=tuple(refinement), callback=callback,
+            density_tolerance=density_tolerance, poisson=poisson,
+        )  # fmt: skip
     stride = int(np.ceil(1.0 / coarse_particles - 1e-9))
     coarse = stride > 1
     if coarse and not coarse_tolerance > 0.0:
@@ -358,5 +369,115 @@ def vlasov_iterate(
                 break
             if density_tolerance is not None and iteration > 0 and density_change < density_tolerance:
                 break
+    assert state is not None
+    return state
+
+
+class RefinedVlasovState(VlasovState):
+    """The last iteration on refined boxes: ``composite_potential`` and
+    ``composite_charge_density`` on the layout's composite nodes, ``potential`` and
+    ``charge_density`` their values at the base mesh's nodes (``Layout.on_base``)."""
+
+    def __init__(self, layout, potential, rho, electric, trace, history) -> None:
+        super().__init__(potential, rho, electric, trace, history, None)
+        self.layout = layout
+
+    @property
+    def composite_potential(self) -> np.ndarray:
+        return self._host_copy("potential", self.potential_device)
+
+    @property
+    def composite_charge_density(self) -> np.ndarray:
+        return self._host_copy("charge_density", self.charge_density_device)
+
+    @property
+    def potential(self) -> np.ndarray:
+        return self.layout.on_base(self.composite_potential)
+
+    @property
+    def charge_density(self) -> np.ndarray:
+        return self.layout.on_base(self.composite_charge_density)
+
+
+def _iterate_refined(mesh, make_particles, tracer, *, iterations, tolerance, relaxation,
+                     mixing, anderson_depth, refinement, callback, density_tolerance,
+                     poisson) -> RefinedVlasovState:  # fmt: skip
+    """`vlasov_iterate` on refined boxes (``vlasov.py:304-427`` with a `Layout`): the
+    composite field solve, the patches' edge fields, one trace through every patch, the
+    patches' deposits summed on the composite nodes and divided by their volumes, mixing.
+    """
+    import torch
+
+    from beamtracer_b200.composite import PatchedElectricField, PatchedFieldMaps
+
+    if poisson is None or tuple(poisson.refinement) != tuple(refinement):
+        poisson = IonOpticsPoisson(mesh, refinement=refinement)
+    layout = poisson.layout
+    maps = PatchedFieldMaps(layout)
+    mixer = AndersonMixer(anderson_depth, relaxation) if mixing == "anderson" else None
+    ctx = _lib.context()
+    n = layout.size
+    dev = "cuda"
+    rho = torch.zeros(n, dtype=torch.float64, device=dev)
+    phi = torch.zeros(n, dtype=torch.float64, device=dev)
+    previous = torch.zeros_like(phi)
+    charge = torch.zeros(n, dtype=torch.float64, device=dev)
+    scalars = torch.zeros(5, dtype=torch.float64, device=dev)
+    engine = tracer.engine()
+    engine.set_patches(maps.patch_int, maps.patch_real, maps.n_field_nodes)
+    loaded = None
+    history: list[dict[str, float]] = []
+    state = None
+    for iteration in range(iterations):
+        previous.copy_(phi)
+        poisson.solve_device(phi, rho)
+        _lib.check(_lib.lib().bt_max_abs_diff(ctx.handle, _lib.dptr(phi), _lib.dptr(previous),
+                                              n, _lib.dptr(scalars)))  # fmt: skip
+        efield = PatchedElectricField(layout, phi, maps=maps)
+        tracer.electric = efield
+        particles, _ = make_particles()
+        if particles is not loaded and particles is not engine.particles:
+            engine.load(particles)
+        loaded = particles
+        engine.run(maps.fx, maps.fy)
+        if tracer.reduce is not None:
+            tracer.reduce(engine.charge)
+        tracer._capacity = engine.capacity
+        maps.charge_map.apply(engine.charge.reshape(-1), charge)
+        if mixer is not None and iteration > 0:
+            mixer.mix(rho.view(n, 1), charge.view(n, 1), maps.volumes, None, scalars[1:3])
+        else:
+            _lib.check(_lib.lib().bt_vlasov_mix(
+                ctx.handle, _lib.dptr(charge), _lib.dptr(maps.volumes), None, n, 1,
+                float(relaxation), int(iteration == 0), _lib.dptr(rho), _lib.dptr(scalars) + 8,
+            ))  # fmt: skip
+        if engine.n:
+            scalars[3] = engine.steps.max().to(torch.float64)
+            scalars[4] = engine.steps.sum().to(torch.float64)
+        host = scalars.cpu().numpy()
+        change = float(host[0]) if iteration > 0 else float("inf")
+        density_change = float(host[1] / host[2]) if host[2] > 0 else 0.0
+        history.append({
+            "iteration": iteration,
+            "max_potential_change": change,
+            "relative_density_change": density_change if iteration > 0 else float("inf"),
+            "newton_iterations": 0,
+            "krylov_steps": poisson.krylov_steps,
+            "steps": int(host[3]) if engine.n else 0,
+            "total_steps": int(host[4]) if engine.n else 0,
+            "trajectories": len(particles),
+            "boxes": len(layout.patches),
+            "max_self_magnetic": 0.0,
+        })  # fmt: skip
+        density_now = charge / maps.volumes
+        state = RefinedVlasovState(layout, phi, rho, efield,
+                                   lambda d=density_now: engine.result(d), history)  # fmt: skip
+        if callback is not None:
+            _ = state.trace
+            callback(iteration, state)
+        if change < tolerance:
+            break
+        if density_tolerance is not None and iteration > 0 and density_change < density_tolerance:
+            break
     assert state is not None
     return state

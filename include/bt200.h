@@ -481,6 +481,22 @@ int bt_poisson_set_transposed(bt_poisson *p, int32_t on);
  * node d of A's coefficient from i to d times z_i, on held nodes; 0 on free nodes. */
 int bt_poisson_fixed_adjoint(bt_poisson *p, const double *z, const double *phi_bar, double *out);
 
+/* The residual r = rho / eps0 + c - A phi of the mesh's field equation on its free nodes (0
+ * on the held ones), all DEVICE (nx, ny); rho may be NULL.  The composite solve of refined
+ * boxes (solver/poisson.py:169-335 through patchwork, absent here) evaluates each node's
+ * equation as its owner patch's row with it. */
+int bt_poisson_residual(bt_poisson *p, const double *phi, const double *rho, double *r);
+
+/* solver/refinement.py:201-231, 286-296, 330-377 (the composite nodes' maps:
+ * Layout.on_base, deposit_total, PatchedElectricField's potentials of the patches,
+ * fill_hanging): y[out_rows[r]] = (accumulate ? y[out_rows[r]] : constant[r]) +
+ * sum over e in [row_ptr[r], row_ptr[r + 1]) of val[e] x[col[e]], in that order (no
+ * atomics: the same bits on every run).  out_rows NULL: row r writes y[r]; constant NULL:
+ * zero.  A row may read y's own entries only where no row writes them.  All DEVICE. */
+int bt_csr_apply(bt_ctx *ctx, int64_t rows, const int64_t *out_rows, const int64_t *row_ptr,
+                 const int64_t *col, const double *val, const double *constant,
+                 int32_t accumulate, const double *x, double *y);
+
 /* poisson.py:809-933 (IonOpticsPoisson.solve).  phi (DEVICE (nx, ny), in/out): the first
  * guess on entry (its fixed nodes are set), the solution on return; rho (DEVICE (nx, ny),
  * C/m^3, or NULL).  With amplitude = 0 one linear solve: GMRES preconditioned by a

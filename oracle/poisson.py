@@ -49,8 +49,13 @@ class Operator:
     coefficients: tuple[np.ndarray, ...]  # cW, cE, cS, cN (nx, ny)
 
 
-def coefficients(x, h, cylindrical, fixed, distance, neumann=(0.0, 0.0, 0.0, 0.0)):
-    """The four neighbour coefficients and the face source of every node (see the module)."""
+def coefficients(x, h, cylindrical, fixed, distance, neumann=(0.0, 0.0, 0.0, 0.0), j0=0):
+    """The four neighbour coefficients and the face source of every node (see the module).
+
+    ``j0`` is the radial index ``r_0 / h`` of the first row (a refined patch off the axis,
+    cylindrical geometry): the radial weights take ``j + j0``, and a first row off the axis
+    takes the face row ``2 / (beta h^2)`` (a patch's side inside the domain, whose rows the
+    composite operator does not use)."""
     x = np.asarray(x, dtype=float)
     nx, ny = fixed.shape
     cw, ce, cs, cn = (np.zeros((nx, ny)) for _ in range(4))
@@ -92,7 +97,7 @@ def coefficients(x, h, cylindrical, fixed, distance, neumann=(0.0, 0.0, 0.0, 0.0
             src += np.where(bottom, 2.0 * neumann[2] / h, 0.0)
             src += np.where(top, 2.0 * neumann[3] / h, 0.0)
         else:
-            jj = np.maximum(j, 1).astype(float)
+            jj = np.maximum(j + j0, 1).astype(float)
             h2 = h * h
             sw_s = (2.0 / a - 1.0 / jj) / ((a + b) * h2)
             sw_n = (2.0 / b + 1.0 / jj) / ((a + b) * h2)
@@ -100,7 +105,7 @@ def coefficients(x, h, cylindrical, fixed, distance, neumann=(0.0, 0.0, 0.0, 0.0
             tp_n = (1.0 + 0.5 / jj) / (b * h2)
             cs = np.where(mid, np.where(four, sw_s, tp_s), 0.0)
             cn = np.where(mid, np.where(four, sw_n, tp_n), 0.0)
-            cn = np.where(bottom, 4.0 / (b * h2), cn)
+            cn = np.where(bottom, (4.0 if j0 == 0 else 2.0) / (b * h2), cn)
             cs = np.where(top, 2.0 / (a * h2), cs)
             src += np.where(top, (1.0 + 0.5 / jj) * 2.0 * neumann[3] / h, 0.0)
     free = ~np.asarray(fixed, dtype=bool)
@@ -108,12 +113,12 @@ def coefficients(x, h, cylindrical, fixed, distance, neumann=(0.0, 0.0, 0.0, 0.0
     return (*out, np.where(free, src, 0.0))
 
 
-def assemble(x, h, cylindrical, fixed, value, distance, neumann=(0.0, 0.0, 0.0, 0.0)):
+def assemble(x, h, cylindrical, fixed, value, distance, neumann=(0.0, 0.0, 0.0, 0.0), j0=0):
     """The operator of a classified mesh (``fixed``, ``value`` and ``distance`` as the
     mesh's ``fixed``, ``fixed_value``, ``distance``)."""
     fixed = np.asarray(fixed, dtype=bool)
     nx, ny = fixed.shape
-    cw, ce, cs, cn, src = coefficients(x, h, cylindrical, fixed, distance, neumann)
+    cw, ce, cs, cn, src = coefficients(x, h, cylindrical, fixed, distance, neumann, j0)
     n = nx * ny
     idx = np.arange(n).reshape(nx, ny)
     diag = cw + ce + cs + cn
@@ -195,4 +200,5 @@ def operator_of_mesh(mesh, region=None, region_value=0.0) -> Operator:
         else float(mesh.faces[f].value)
         for f in ("x_min", "x_max", "y_min", "y_max")
     ]  # fmt: skip
-    return assemble(mesh.x, mesh.h, mesh.cylindrical, fixed, value, mesh.distance, neumann)
+    j0 = int(round(mesh.origin[1] / mesh.h)) if mesh.cylindrical else 0
+    return assemble(mesh.x, mesh.h, mesh.cylindrical, fixed, value, mesh.distance, neumann, j0)

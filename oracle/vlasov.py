@@ -96,8 +96,12 @@ class Trace:
     counts: np.ndarray
 
 
-def trace(p: Problem, fx, fy, particles) -> Trace:
-    """One trace of ``particles`` (positions, velocities, charge, mass, current arrays)."""
+def trace(p: Problem, fx, fy, particles, patches=None) -> Trace:
+    """One trace of ``particles`` (positions, velocities, charge, mass, current arrays).
+
+    ``patches``: ``(patch_int, patch_real, nodes)`` of refined boxes (finest first, the base
+    last; ``fx``, ``fy`` their edge fields flattened in that order); the charges are then
+    the flat node charges of every patch."""
     nx, ny = p.shape
     n = particles.position.shape[1]
     x0 = np.array(particles.position, dtype=float, order="C")
@@ -118,6 +122,9 @@ def trace(p: Problem, fx, fy, particles) -> Trace:
     planes = np.array(p.planes or (np.nan,), dtype=float)
     patch_int = np.array([[nx, ny, 0, 0, nx * ny, 0]], dtype=np.int64)
     patch_real = np.array([[*p.logical_origin, p.h, *p.logical_origin, *p.logical_upper]])
+    nodes = nx * ny
+    if patches is not None:
+        patch_int, patch_real, nodes = patches
     x_nodes = np.ascontiguousarray(p.x if p.graded else np.zeros(2))
     fxs, fys = np.ascontiguousarray(fx).ravel(), np.ascontiguousarray(fy).ravel()
     while True:
@@ -125,7 +132,7 @@ def trace(p: Problem, fx, fy, particles) -> Trace:
         x, v = x0.copy(), v0.copy()
         status, electrode = status0.copy(), electrode0.copy()
         steps = np.zeros(n, dtype=np.int64)
-        charge = np.zeros((threads, nx * ny))
+        charge = np.zeros((threads, nodes))
         hits = np.zeros((n, planes.size, capacity, 8))
         counts = np.zeros((n, planes.size), dtype=np.int64)
         slot = np.full(n, -1, dtype=np.int64)
@@ -153,7 +160,9 @@ def trace(p: Problem, fx, fy, particles) -> Trace:
         if most <= capacity:
             break
         p.capacity = (max(capacity, most), path_capacity)
-    return Trace(charge.sum(axis=0).reshape(nx, ny), status, electrode, steps, hits, counts)
+    total = charge.sum(axis=0)
+    return Trace(total if patches is not None else total.reshape(nx, ny), status, electrode,
+                 steps, hits, counts)  # fmt: skip
 
 
 def plane_hits(p: Problem, t: Trace, current, species):

@@ -1,0 +1,135 @@
+"""Refined boxes on the host: the patches, the composite nodes and the oracle's composite
+solve (the cases of the reference's ``tests/unit/test_refinement.py:36-131``)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from scipy.constants import epsilon_0
+
+from beamtracer_b200.mesh import Electrode, FaceCondition, IonOpticsMesh
+from beamtracer_b200.refinement import Refinement, layout_of_mesh, patches_of
+from oracle import composite
+
+DIRICHLET_X = {"x_min": FaceCondition("dirichlet", 0.0), "x_max": FaceCondition("dirichlet", 0.0)}
+
+
+def _plates(geometry: str = "planar") -> IonOpticsMesh:
+    return IonOpticsMesh((21, 11), (0.0, 0.0), 1e-3, geometry, faces=DIRICHLET_X,
+                         classify_on_device=False)  # fmt: skip
+
+
+def test_boxes_snap_to_the_level_below_and_their_fields_get_a_margin() -> None:
+    mesh = _plates()
+    patches = patches_of(mesh, [Refinement(1, (2.6e-3, 0.0), (7.2e-3, 4.1e-3)),
+                                Refinement(2, (3e-3, 0), (5e-3, 2e-3))])  # fmt: skip
+    one, two = patches[1], patches[2]
+    assert one.box == ((4, 16), (0, 10))  # level-1 nodes: base nodes 2..8, 0..5
+    assert one.mesh.origin == pytest.approx((2e-3, 0.0))
+    assert one.mesh.h == pytest.approx(0.5e-3)
+    assert one.field_mesh.origin == pytest.approx((1e-3, 0.0))
+    assert one.field_mesh.shape == (one.mesh.shape[0] + 4, one.mesh.shape[1] + 2)
+    assert two.box == ((12, 20), (0, 8)) and two.mesh.h == pytest.approx(0.25e-3)
+    with pytest.raises(ValueError, match="outside"):
+        patches_of(mesh, [Refinement(1, (0.03, 0.0), (0.04, 0.01))])
+    with pytest.raises(ValueError, match="level"):
+        patches_of(mesh, [Refinement(0, (0.0, 0.0), (0.01, 0.01))])
+
+
+@pytest.mark.parametrize("geometry", ["planar", "cylindrical"])
+def test_the_volumes_fill_the_domain(geometry) -> None:
+    mesh = _plates(geometry)
+    plain = layout_of_mesh(mesh)
+    refined = layout_of_mesh(mesh, [Refinement(1, (5e-3, 0.0), (12e-3, 6e-3))])
+    assert refined.size > plain.size
+    total = 20e-3 * 10e-3 if geometry == "planar" else np.pi * 10e-3**2 * 20e-3
+    assert plain.volumes.sum() == pytest.approx(total)
+    assert refined.volumes.sum() == pytest.approx(total)
+    values = np.arange(231.0).reshape(21, 11)
+    np.testing.assert_array_equal(plain.from_base(values)[plain.base.index], values)
+    with pytest.raises(ValueError, match="composite"):
+        refined.from_base(np.zeros(mesh.shape))
+
+
+def test_the_nodes_hang_on_coarse_edges_and_interpolate_planes_exactly() -> None:
+    mesh = _plates()
+    layout = layout_of_mesh(mesh, [Refinement(1, (4e-3, 2e-3), (14e-3, 6e-3)),
+                                   Refinement(2, (6e-3, 2e-3), (10e-3, 4e-3))])  # fmt: skip
+    assert layout.hanging.size > 0
+    # no base node hangs, and every hanging node is a node of a box only
+    base = set(layout.base.index.ravel().tolist())
+    assert not base & set(layout.hanging.tolist())
+    plane = 3.0 * layout.x - 7.0 * layout.y + 1.0
+    filled = plane.copy()
+    filled[layout.hanging] = 0.0
+    layout.fill_hanging(filled)
+    np.testing.assert_allclose(filled, plane, rtol=0, atol=1e-14)
+    # the interpolation reads only nodes that do not hang
+    assert not set(layout.interpolation.indices.tolist()) & set(layout.hanging.tolist())
+
+
+def test_a_box_must_lie_inside_the_level_below() -> None:
+    with pytest.raises(ValueError, match="inside those of level 1"):
+        layout_of_mesh(_plates(), [Refinement(1, (2e-3, 0.0), (6e-3, 4e-3)),
+                                   Refinement(2, (8e-3, 0.0), (10e-3, 2e-3))])  # fmt: skip
+
+
+def test_a_graded_axis_takes_no_boxes() -> None:
+    mesh = IonOpticsMesh((5, 5), (0.0, 0.0), 1.0, "planar",
+                         x_nodes=[0.0, 1.0, 1.5, 3.0, 4.0], classify_on_device=False)  # fmt: skip
+    with pytest.raises(NotImplementedError, match="graded"):
+        patches_of(mesh, [Refinement(1, (0.0, 0.0), (2.0, 2.0))])
+
+
+def test_a_uniform_charge_between_plates_on_refined_boxes() -> None:
+    """The reference's known answer (``test_refinement.py:105-131``): the parabola of a
+    uniform charge between grounded plates, within 1e-2 on two nested boxes, the error
+    falling with the cells (first order at the coarse-fine nodes)."""
+    rho = 1e-6
+    errors = []
+    for n in (21, 41):
+        mesh = IonOpticsMesh((n, (n + 1) // 2), (0.0, 0.0), 20e-3 / (n - 1), "planar",
+                             faces=DIRICHLET_X, classify_on_device=False)  # fmt: skip
+        layout = layout_of_mesh(mesh, [Refinement(1, (4e-3, 0.0), (14e-3, 6e-3)),
+                                       Refinement(2, (6e-3, 0.0), (10e-3, 4e-3))])  # fmt: skip
+        phi = composite.solve(layout, np.full(layout.size, rho))
+        exact = rho / (2 * epsilon_0) * layout.x * (20e-3 - layout.x)
+        errors.append(np.abs(phi - exact).max() / exact.max())
+    assert errors[0] < 1e-2
+    assert errors[1] < 0.6 * errors[0]
+
+
+def test_without_boxes_the_composite_solve_is_the_mesh_solve() -> None:
+    from oracle import poisson as oracle_poisson
+
+    plate = lambda x, y: (x >= 8e-3) & (x <= 10e-3) & (y >= 4e-3)  # noqa: E731
+    faces = {"x_min": FaceCondition("dirichlet", 0.0), "x_max": FaceCondition("dirichlet", -50.0)}
+    for geometry in ("planar", "cylindrical"):
+        mesh = IonOpticsMesh((21, 11), (0.0, 0.0), 1e-3, geometry, faces=faces,
+                             electrodes=[Electrode(plate, 100.0)], classify_on_device=False)  # fmt: skip
+        layout = layout_of_mesh(mesh)
+        rho = np.linspace(0.0, 1e-7, layout.size)
+        phi = composite.solve(layout, rho)
+        direct = oracle_poisson.solve(oracle_poisson.operator_of_mesh(mesh),
+                                      layout.on_base(rho)).ravel()  # fmt: skip
+        np.testing.assert_allclose(layout.on_base(phi).ravel(), direct, rtol=0, atol=1e-10)
+
+
+def test_the_setting_is_checked_and_round_trips() -> None:
+    """``config.py:437-464``: the level and the corners are checked, and a configuration's
+    boxes survive ``to_dict`` / ``from_dict`` (``test_refinement.py:17-27``)."""
+    from beamtracer_b200 import BeamOpticsConfig, GridParams, RefinementParams
+
+    with pytest.raises(ValueError, match="level"):
+        RefinementParams(0, (0, 0), (1e-3, 1e-3))
+    with pytest.raises(ValueError, match="lower < upper"):
+        RefinementParams(1, (2e-3, 0), (1e-3, 1e-3))
+    grid = GridParams(num_gridpoints=(81, 31), lower_bound=(0.0, 0.0), upper_bound=(8e-3, 3e-3),
+                      coordinates="cylindrical")  # fmt: skip
+    config = BeamOpticsConfig(grid=grid,
+                              refinement=[RefinementParams(1, (0.5e-3, 0.0), (3e-3, 1.5e-3))])
+    again = type(config).from_dict(config.to_dict())
+    assert again.refinement == config.refinement
+    assert again.refinement[0].upper == pytest.approx((3e-3, 1.5e-3))
+    with pytest.raises(ValueError, match="2D grid"):
+        BeamOpticsConfig(grid=grid, refinement=[RefinementParams(1, (0, 0, 0), (1, 1, 1))])

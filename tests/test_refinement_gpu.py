@@ -1,0 +1,192 @@
+"""Refined boxes on the device against the oracle: the sparse maps, the composite field
+solve, the patches' field and the Vlasov iteration through them."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from scipy import sparse
+from scipy.constants import epsilon_0
+
+from beamtracer_b200.mesh import Electrode, FaceCondition, IonOpticsMesh
+from beamtracer_b200.refinement import Refinement, layout_of_mesh
+from oracle import composite as oracle_composite
+
+pytestmark = pytest.mark.gpu
+
+
+def _box(x0, x1, y0, y1):
+    return lambda x, y: (x >= x0) & (x <= x1) & (y >= y0) & (y <= y1)
+
+
+def _extraction_mesh(geometry: str) -> IonOpticsMesh:
+    """The reference's extraction geometry (``test_beam_optics.py:211-261``) without the
+    plasma: 81 x 31 on 8 x 3 mm, two plates, Dirichlet x faces."""
+    faces = {"x_min": FaceCondition("dirichlet", 5.0), "x_max": FaceCondition("dirichlet", -2000.0)}
+    electrodes = [Electrode(_box(0.5e-3, 1e-3, 1e-3, 3.1e-3), 0.0),
+                  Electrode(_box(3e-3, 4e-3, 1.2e-3, 3.1e-3), -2000.0)]  # fmt: skip
+    return IonOpticsMesh((81, 31), (0.0, 0.0), 1e-4, geometry, electrodes=electrodes,
+                         faces=faces, classify_on_device=False)  # fmt: skip
+
+
+BOXES = {
+    "axis": [Refinement(1, (0.0, 0.0), (2e-3, 1.5e-3)), Refinement(2, (0.0, 0.0), (1.5e-3, 1.2e-3))],
+    "inside": [Refinement(1, (2.2e-3, 0.6e-3), (5e-3, 2.2e-3)),
+               Refinement(2, (2.6e-3, 0.8e-3), (4.2e-3, 1.6e-3))],
+}  # fmt: skip
+
+
+def test_the_sparse_map_kernel_equals_scipy() -> None:
+    import torch
+
+    from beamtracer_b200.composite import DeviceCSR
+
+    rng = np.random.default_rng(4)
+    matrix = sparse.random(300, 500, density=0.02, random_state=5, format="csr")
+    x = rng.standard_normal(500)
+    constant = rng.standard_normal(300)
+    y = torch.zeros(300, dtype=torch.float64, device="cuda")
+    DeviceCSR(matrix, constant=constant).apply(torch.from_numpy(x).cuda(), y)
+    np.testing.assert_allclose(y.cpu().numpy(), matrix @ x + constant, rtol=1e-14, atol=1e-14)
+    # rows written to chosen places, added to what is there
+    out_rows = rng.permutation(1000)[:300]
+    z0 = rng.standard_normal(1000)
+    z = torch.from_numpy(z0.copy()).cuda()
+    DeviceCSR(matrix, out_rows=out_rows).apply(torch.from_numpy(x).cuda(), z, accumulate=True)
+    want = z0.copy()
+    want[out_rows] += matrix @ x
+    np.testing.assert_allclose(z.cpu().numpy(), want, rtol=1e-14, atol=1e-14)
+
+
+@pytest.mark.parametrize("geometry", ["planar", "cylindrical"])
+@pytest.mark.parametrize("boxes", ["axis", "inside"])
+def test_the_composite_solve_equals_the_oracle(geometry, boxes) -> None:
+    import torch
+
+    from beamtracer_b200.poisson import IonOpticsPoisson
+
+    mesh = _extraction_mesh(geometry)
+    solver = IonOpticsPoisson(mesh, refinement=BOXES[boxes])
+    layout = solver.layout
+    assert layout.refined and layout.hanging.size > 0
+    rho = 1e-4 * np.exp(-((layout.x - 2e-3) ** 2 + layout.y**2) / (1e-3) ** 2)
+    phi = solver.solve(rho)
+    ora = oracle_composite.solve(oracle_layout(mesh, BOXES[boxes]), rho)
+    span = np.ptp(ora)
+    assert np.abs(phi - ora).max() <= 1e-9 * span
+    assert solver._composite.sweeps < 40
+    # a second solve from the first's potential changes nothing
+    again = torch.from_numpy(phi.copy()).cuda()
+    solver.solve_device(again, torch.from_numpy(rho).cuda())
+    assert np.abs(again.cpu().numpy() - phi).max() <= 1e-10 * span
+
+
+def oracle_layout(mesh, boxes):
+    """The layout of the same mesh classified again on the host."""
+    from tests.vlasov_cases import host_twin
+
+    return layout_of_mesh(host_twin(mesh), boxes)
+
+
+def test_a_uniform_charge_between_plates_on_refined_boxes_on_the_device() -> None:
+    """The reference's known answer (``test_refinement.py:105-131``) through the device."""
+    from beamtracer_b200.poisson import IonOpticsPoisson
+
+    rho = 1e-6
+    errors = []
+    for n in (21, 41):
+        faces = {"x_min": FaceCondition("dirichlet", 0.0),
+                 "x_max": FaceCondition("dirichlet", 0.0)}  # fmt: skip
+        mesh = IonOpticsMesh((n, (n + 1) // 2), (0.0, 0.0), 20e-3 / (n - 1), "planar",
+                             faces=faces)  # fmt: skip
+        solver = IonOpticsPoisson(mesh, refinement=[Refinement(1, (4e-3, 0.0), (14e-3, 6e-3)),
+                                                    Refinement(2, (6e-3, 0.0), (10e-3, 4e-3))])  # fmt: skip
+        layout = solver.layout
+        phi = solver.solve(np.full(layout.size, rho))
+        exact = rho / (2 * epsilon_0) * layout.x * (20e-3 - layout.x)
+        errors.append(np.abs(phi - exact).max() / exact.max())
+    assert errors[0] < 1e-2
+    assert errors[1] < 0.6 * errors[0]
+
+
+@pytest.mark.parametrize("geometry", ["planar", "cylindrical"])
+def test_the_patches_fields_equal_the_oracle(geometry) -> None:
+    from beamtracer_b200.composite import PatchedElectricField
+
+    mesh = _extraction_mesh(geometry)
+    boxes = BOXES["axis"] + [Refinement(1, (5.2e-3, 0.4e-3), (6.4e-3, 2.4e-3))]
+    layout = layout_of_mesh(mesh, boxes)
+    rng = np.random.default_rng(7)
+    phi = np.where(layout.fixed, layout.fixed_value, 100.0 * rng.standard_normal(layout.size))
+    field = PatchedElectricField(layout, phi)
+    ora_layout = oracle_layout(mesh, boxes)
+    for number, values in enumerate(oracle_composite.field_values(ora_layout, phi)):
+        got = field.maps.values[number].cpu().numpy()
+        np.testing.assert_allclose(got, values, rtol=0, atol=1e-12 * np.abs(values).max())
+    fields, _ = oracle_composite.edge_fields(ora_layout, phi)
+    for number, (fx, fy) in enumerate(fields):
+        scale = max(np.abs(fx).max(), np.abs(fy).max())
+        np.testing.assert_allclose(field.fields[number].fx, fx, rtol=0, atol=1e-11 * scale)
+        np.testing.assert_allclose(field.fields[number].fy, fy, rtol=0, atol=1e-11 * scale)
+    # at points the finest patch's field is taken
+    x = np.array([1.0e-3, 1.4e-3, 5.8e-3, 7.5e-3])
+    y = np.array([0.5e-3, 1.1e-3, 1.0e-3, 2.0e-3])
+    # (the patches by level: the two level-1 boxes, then the level-2 box)
+    assert field.patch_of(x, y).tolist() == [3, 3, 2, 0]
+
+
+def _device_density(config, layout_host, potential):
+    """G(phi) through the product's pieces: the patches' field of a composite potential,
+    one trace through them, the composite density."""
+    import torch
+
+    from beamtracer_b200.composite import PatchedElectricField, PatchedFieldMaps
+    from beamtracer_b200.model import BeamOptics
+
+    model = BeamOptics(config)
+    layout = layout_of_mesh(model.mesh, [Refinement(b.level, b.lower, b.upper)
+                                         for b in config.refinement])  # fmt: skip
+    assert layout.size == layout_host.size
+    maps = PatchedFieldMaps(layout)
+    PatchedElectricField(layout, torch.from_numpy(potential).cuda(), maps=maps)
+    engine = model.tracer.engine()
+    engine.set_patches(maps.patch_int, maps.patch_real, maps.n_field_nodes)
+    particles, _ = model._particles()
+    engine.load(particles)
+    engine.run(maps.fx, maps.fy)
+    charge = torch.zeros(layout.size, dtype=torch.float64, device="cuda")
+    maps.charge_map.apply(engine.charge.reshape(-1), charge)
+    return (charge / maps.volumes).cpu().numpy(), engine
+
+
+def test_the_refined_vlasov_iteration_equals_the_oracle() -> None:
+    """The reference's refined planar case (``test_refinement.py:134-165``: IBSimu's
+    vlasov2d with a level-1 box over the emitter): per iteration the composite potential
+    and density against the oracle's, and stage-wise the density the beam deposits in the
+    oracle's potential within 1e-10 of its largest value."""
+    from beamtracer_b200 import BeamOptics, RefinementParams
+    from tests.vlasov_cases import refined_problem, slit_lens
+
+    config = slit_lens(refinement=[RefinementParams(1, (0.0, 0.0), (0.04, 0.02))])
+    gpu = []
+    model = BeamOptics(config)
+    model.run(lambda it, s: gpu.append((s.composite_potential.copy(),
+                                        s.composite_charge_density.copy())))  # fmt: skip
+    state = model.state
+    assert state.layout.refined and state.composite_potential.size > state.potential.size
+    assert state.potential.shape == model.mesh.shape
+    problem, particles, _, layout = refined_problem(config)
+    ora = []
+    oracle_composite.vlasov(problem, layout, particles, iterations=3, callback=lambda it, o: ora.append(
+        (o["potential"].copy(), o["charge_density"].copy())))  # fmt: skip
+    assert len(gpu) == len(ora) == 3
+    span = np.ptp(ora[0][0])
+    for (phi_g, rho_g), (phi_o, rho_o) in zip(gpu, ora):
+        assert np.abs(phi_g - phi_o).max() <= 1e-8 * span
+        assert np.abs(rho_g - rho_o).max() <= 1e-6 * np.abs(rho_o).max()
+    # stage-wise: G(phi) in the oracle's own last potential
+    phi_o = ora[-1][0]
+    rho_dev, engine = _device_density(config, layout, phi_o)
+    rho_ora, t = oracle_composite.density_of(problem, layout, phi_o, particles)
+    assert np.abs(rho_dev - rho_ora).max() <= 1e-10 * np.abs(rho_ora).max()
+    np.testing.assert_array_equal(engine.status.cpu().numpy(), t.status)

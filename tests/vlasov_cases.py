@@ -133,3 +133,40 @@ def oracle_problem(model) -> oracle_vlasov.Problem:
                         integrator=INTEGRATORS.index(config.integrator),
                         step_fraction=config.step_fraction, max_steps=config.max_steps,
                         magnetic=model.tracer.magnetic)  # fmt: skip
+
+
+def slit_lens(**settings) -> BeamOpticsConfig:
+    """IBSimu's vlasov2d, coarse: protons from a slit through three planar electrodes (the
+    reference's ``tests/unit/test_compiled_tracer.py:40-94``), 121 x 51 on 120 x 50 mm."""
+    neumann = FieldBoundaryCondition.neumann(0.0)
+    objects = {
+        "plasma": ObjectParams("rectangle", "dirichlet", -3000.0, midpoint=(0.01, 0.034),
+                               side_lengths=(0.02, 0.032)),
+        "puller": ObjectParams("rectangle", "dirichlet", -14000.0, midpoint=(0.035, 0.035),
+                               side_lengths=(0.01, 0.03)),
+        "ground": ObjectParams("polygon", "dirichlet", -1000.0,
+                               vertices=((0.06, 0.04), (0.08, 0.03), (0.12, 0.03), (0.12, 0.05),
+                                         (0.06, 0.05))),
+    }  # fmt: skip
+    return BeamOpticsConfig(
+        grid=GridParams(num_gridpoints=(121, 51), upper_bound=(0.12, 0.05)),
+        objects=objects,
+        bcs_field=FieldBCs(x_lower=FieldBoundaryCondition.dirichlet(-3000.0),
+                           x_upper=FieldBoundaryCondition.dirichlet(-1000.0),
+                           y_lower=neumann, y_upper=neumann),
+        beams=[BeamSpecies("H+", 50.0, (0.0, 0.0), (0.0, 0.012), mass=1.0, energy=3000.0,
+                           transverse_temperature=0.0, num_particles=300)],
+        **{"iterations": 3, "tolerance": 0.0, "diagnostic_planes": [0.05, 0.115], **settings},
+    )  # fmt: skip
+
+
+def refined_problem(config):
+    """`config_problem` of a configuration with refined boxes, and the boxes' layout (built
+    on the host alone)."""
+    from beamtracer_b200.model import config_mesh
+    from beamtracer_b200.refinement import Refinement, layout_of_mesh
+
+    problem, particles, j_over_v = config_problem(config)
+    mesh = config_mesh(config, classify_on_device=False)
+    boxes = [Refinement(b.level, b.lower, b.upper) for b in config.refinement]
+    return problem, particles, j_over_v, layout_of_mesh(mesh, boxes)
