@@ -168,6 +168,10 @@ SIGNATURES: dict[str, list] = {
     "bt_poisson_fixed_adjoint": [P, P, P, P],
     "bt_poisson_residual": [P, P, P, P],
     "bt_csr_apply": [P, I64, P, P, P, P, P, I32, P, P],
+    "bt_poisson_solve_reaction": [P, P, P, P, F64, ctypes.POINTER(I32)],
+    "bt_boltzmann_terms": [P, I64, P, P, F64, F64, F64, I32, P, P],
+    "bt_newton_residual": [P, I64, P, P, P, P, P],
+    "bt_poisson_vcycle": [P, P, P, I32, P],
     "bt_vlasov_mix": [P, P, P, P, I64, I64, F64, I32, P, P],
     "bt_max_abs_diff": [P, P, P, I64, P],
     "bt_anderson_mix": [P, P, P, P, I64, I64, I32, I32, I32, F64, P, P, P, P, P],

@@ -22,6 +22,8 @@ patch holding it (``solver/refinement.py:299-387``, ``tracer.py:1141-1183``).  H
 
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 from scipy import sparse
 from scipy.constants import epsilon_0
@@ -63,9 +65,12 @@ def _selection(index: np.ndarray, size: int, value: float = 1.0) -> sparse.csr_m
                              shape=(index.size, size))  # fmt: skip
 
 
-def prolongation(layout: Layout, number: int) -> tuple[sparse.csr_matrix, np.ndarray]:
-    """The free composite nodes in patch ``number``'s box and, per node, the bilinear weights
-    of the patch's nodes at it (the node's own value where it is one of them)."""
+def prolongation(layout: Layout, number: int,
+                 held: np.ndarray | None = None) -> tuple[sparse.csr_matrix, np.ndarray]:
+    """The composite nodes in patch ``number``'s box not ``held`` (default: the layout's
+    held nodes) and, per node, the bilinear weights of the patch's nodes at it (the node's
+    own value where it is one of them)."""
+    held = layout.fixed if held is None else held
     patch = layout.patches[number]
     finest = max(p.level for p in layout.patches)
     s = 2 ** (finest - patch.level)
@@ -74,7 +79,7 @@ def prolongation(layout: Layout, number: int) -> tuple[sparse.csr_matrix, np.nda
     li = layout.lattice[:, 0] / s - i0
     lj = layout.lattice[:, 1] / s - j0
     mine = np.flatnonzero((li >= 0) & (li <= nxp - 1) & (lj >= 0) & (lj <= nyp - 1)
-                          & ~layout.fixed)  # fmt: skip
+                          & ~held)  # fmt: skip
     a = np.clip(np.floor(li[mine]).astype(np.int64), 0, nxp - 2)
     b = np.clip(np.floor(lj[mine]).astype(np.int64), 0, nyp - 2)
     u, w = li[mine] - a, lj[mine] - b
@@ -87,15 +92,51 @@ def prolongation(layout: Layout, number: int) -> tuple[sparse.csr_matrix, np.nda
     return matrix, mine
 
 
+class _Held:
+    """What depends on the held composite nodes (the mesh's, plus an initial plasma region):
+    the rows that carry an equation, the values to hold, the corrections' spread and the
+    nodes each patch's correction holds."""
+
+    def __init__(self, layout: Layout, held: np.ndarray, values: np.ndarray,
+                 offsets: np.ndarray) -> None:  # fmt: skip
+        import torch
+
+        n = layout.size
+        base_shape = layout.base.mesh.shape
+        own = (layout.owner >= 0) & ~held
+        rows = np.flatnonzero(own)
+        cols = offsets[layout.owner[rows]] + layout.owner_node[rows]
+        self.owned = DeviceCSR(sparse.csr_matrix((np.ones(rows.size), (rows, cols)),
+                                                 shape=(n, int(offsets[-1]))))  # fmt: skip
+        self.own = torch.from_numpy(own.astype(np.uint8)).cuda()
+        kept = np.flatnonzero(held)
+        self.setter = DeviceCSR(sparse.csr_matrix((kept.size, 1)), out_rows=kept,
+                                constant=values[kept])  # fmt: skip
+        self.prolong = []
+        self.sides = []
+        for number, patch in enumerate(layout.patches):
+            matrix, where = prolongation(layout, number, held)
+            self.prolong.append(DeviceCSR(matrix, out_rows=where))
+            local = held[patch.index] & ~np.asarray(patch.mesh.fixed, dtype=bool)
+            sides = local if number == 0 else (~_inside(patch, base_shape) | local)
+            self.sides.append(sides if sides.any() else None)
+
+
 class CompositePoisson:
-    """The field of a refined layout solved on the device (linear; see the module).
+    """The field of a refined layout solved on the device (see the module).
 
     ``solve_device(phi, rho)`` takes composite device vectors: ``phi`` the first guess (its
-    held and hanging nodes are set) and the result, ``rho`` [C/m^3] or None.
+    held and hanging nodes are set) and the result, ``rho`` [C/m^3] or None.  With
+    ``fixed_region`` (a mask of the composite nodes, or a function of their ``(x, y)``) those
+    nodes are held at ``fixed_potential`` as well; with ``plasma`` (a Boltzmann species:
+    ``amplitude`` rho_0 / eps0, ``temperature``, ``up``, ``sign``) Newton's method from
+    ``phi``, each step's correction by the same sweeps with the Jacobian's reaction in every
+    patch's solver, until its largest update is below ``newton_tolerance``.
     """
 
-    def __init__(self, layout: Layout, *, tolerance: float = 1e-12, max_sweeps: int = 100,
-                 correction_tolerance: float = 1e-10) -> None:  # fmt: skip
+    def __init__(self, layout: Layout, *, tolerance: float = 1e-12, max_sweeps: int = 200,
+                 correction_tolerance: float = 1e-6, newton_sweep_tolerance: float = 1e-10,
+                 local: str = "vcycle") -> None:  # fmt: skip
         import torch
 
         from beamtracer_b200.poisson import IonOpticsPoisson
@@ -104,19 +145,21 @@ class CompositePoisson:
         self.tolerance = float(tolerance)
         self.max_sweeps = int(max_sweeps)
         self.correction_tolerance = float(correction_tolerance)
+        #: the sweeps' tolerance for a Newton step's correction (an inexact Newton step:
+        #: the steps continue until their own update is below Newton's tolerance)
+        self.newton_sweep_tolerance = float(newton_sweep_tolerance)
+        if local not in ("vcycle", "solve"):
+            raise ValueError(f"local must be 'vcycle' or 'solve', got {local!r}")
+        #: a patch's correction per sweep: one multigrid V-cycle of its operator
+        #: (``bt_poisson_vcycle``, no host round trip) or a GMRES solve to
+        #: ``correction_tolerance``
+        self.local = local
         patches = layout.patches
         n = layout.size
-        base_shape = layout.base.mesh.shape
         #: every patch's own operator (its rows: the equations of the nodes it owns)
         self.rows = [IonOpticsPoisson(p.mesh) for p in patches]
         #: the corrections' solvers: held values and face terms zero, a box's sides held
-        self.corrections = []
-        #: the nodes each correction holds besides the patch's own (a box's sides)
-        self._sides = []
-        for number, patch in enumerate(patches):
-            solver = IonOpticsPoisson(patch.mesh, homogeneous=True)
-            self._sides.append(None if number == 0 else ~_inside(patch, base_shape))
-            self.corrections.append(solver)
+        self.corrections = [IonOpticsPoisson(p.mesh, homogeneous=True) for p in patches]
         sizes = [int(np.prod(p.mesh.shape)) for p in patches]
         self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
         total = int(self.offsets[-1])
@@ -127,28 +170,25 @@ class CompositePoisson:
         self._res_p = torch.zeros(total, dtype=f64, device=dev)
         self._rhs_p = torch.zeros(total, dtype=f64, device=dev)
         self._e_p = torch.zeros(total, dtype=f64, device=dev)
+        self._reaction_p = torch.zeros(total, dtype=f64, device=dev)
         self._r = torch.zeros(n, dtype=f64, device=dev)
+        self._r0 = torch.zeros(n, dtype=f64, device=dev)
+        self._reaction = torch.zeros(n, dtype=f64, device=dev)
+        self._delta = torch.zeros(n, dtype=f64, device=dev)
         self._prev = torch.zeros(n, dtype=f64, device=dev)
         self._zero = torch.zeros(max(n, 1), dtype=f64, device=dev)
         self._scalars = torch.zeros(2, dtype=f64, device=dev)
         self._gather = [DeviceCSR(_selection(p.index, n)) for p in patches]
         self._gather_eps = [DeviceCSR(_selection(p.index, n, epsilon_0)) for p in patches]
-        owned = np.flatnonzero((layout.owner >= 0) & ~layout.fixed)
-        cols = self.offsets[layout.owner[owned]] + layout.owner_node[owned]
-        self._owned = DeviceCSR(sparse.csr_matrix(
-            (np.ones(owned.size), (owned, cols)), shape=(n, total)))  # fmt: skip
-        self._prolong = []
-        for number in range(len(patches)):
-            matrix, rows = prolongation(layout, number)
-            self._prolong.append(DeviceCSR(matrix, out_rows=rows))
-        held = np.flatnonzero(layout.fixed)
-        self._held = DeviceCSR(sparse.csr_matrix((held.size, 1)), out_rows=held,
-                               constant=layout.fixed_value[held])  # fmt: skip
         self._hang = (DeviceCSR(layout.interpolation, out_rows=layout.hanging)
                       if layout.hanging.size else None)  # fmt: skip
-        #: FAC sweeps of the last solve, and their corrections' V-cycles
+        self._plain = _Held(layout, layout.fixed, layout.fixed_value, self.offsets)
+        self._region_key: object = None
+        self._region: _Held | None = None
+        #: FAC sweeps of the last solve, and their corrections' V-cycles; Newton steps
         self.sweeps = 0
         self.krylov_steps = 0
+        self.newton_iterations = 0
 
     def _view(self, buffer, number: int):
         lo, hi = self.offsets[number], self.offsets[number + 1]
@@ -158,9 +198,26 @@ class CompositePoisson:
         if self._hang is not None:
             self._hang.apply(phi, phi)
 
-    def residual(self, phi, r) -> None:
+    def _held(self, region, potential: float) -> _Held:
+        if region is None:
+            return self._plain
+        layout = self.layout
+        mask = np.asarray(region(layout.x, layout.y) if callable(region) else region, dtype=bool)
+        if mask.shape != (layout.size,):
+            raise ValueError("the held region needs the layout's composite nodes")
+        mask = mask & ~layout.fixed
+        mask[layout.hanging] = False
+        key = (np.packbits(mask).tobytes(), float(potential))
+        if key != self._region_key:
+            values = np.where(mask, float(potential), layout.fixed_value)
+            self._region = _Held(layout, layout.fixed | mask, values, self.offsets)
+            self._region_key = key
+        return self._region
+
+    def residual(self, phi, r, held: _Held | None = None) -> None:
         """``r`` <- the composite residual of ``phi`` (zero on held and hanging nodes), with
         the charge density last given to `solve_device`."""
+        held = held or self._plain
         self.fill_hanging(phi)
         lib = _lib.lib()
         for number, solver in enumerate(self.rows):
@@ -169,7 +226,23 @@ class CompositePoisson:
             _lib.check(lib.bt_poisson_residual(solver._handle, _lib.dptr(phi_p),
                                                _lib.dptr(self._view(self._rho_p, number)),
                                                _lib.dptr(self._view(self._res_p, number))))  # fmt: skip
-        self._owned.apply(self._res_p, r)
+        held.owned.apply(self._res_p, r)
+
+    def _step_residual(self, delta, r, held: _Held) -> None:
+        """``r`` <- the residual of a Newton step's correction ``delta``: the step's own
+        residual less (K + diag(reaction)) delta, at the nodes with an equation."""
+        self.fill_hanging(delta)
+        lib = _lib.lib()
+        for number, solver in enumerate(self.corrections):
+            d_p = self._view(self._phi_p, number)
+            self._gather[number].apply(delta, d_p)
+            solver._set_region(held.sides[number], 0.0)
+            _lib.check(lib.bt_poisson_residual(solver._handle, _lib.dptr(d_p), None,
+                                               _lib.dptr(self._view(self._res_p, number))))  # fmt: skip
+        held.owned.apply(self._res_p, r)
+        d = _lib.dptr
+        _lib.check(lib.bt_newton_residual(_lib.context().handle, self.layout.size, d(held.own),
+                                          d(self._r0), d(self._reaction), d(delta), d(r)))  # fmt: skip
 
     def _max(self, a, b=None) -> float:
         n = self.layout.size
@@ -178,41 +251,113 @@ class CompositePoisson:
                                               _lib.dptr(self._scalars)))  # fmt: skip
         return float(self._scalars[0])
 
-    def solve_device(self, phi, rho=None) -> None:
+    def _max_pair(self, x, previous) -> tuple[float, float]:
+        """max |x - previous| and max |x| in one read."""
+        n = self.layout.size
+        ctx = _lib.context().handle
+        d = _lib.dptr
+        _lib.check(_lib.lib().bt_max_abs_diff(ctx, d(x), d(previous), n, d(self._scalars)))
+        _lib.check(_lib.lib().bt_max_abs_diff(ctx, d(x), d(self._zero), n,
+                                              d(self._scalars) + 8))  # fmt: skip
+        change, largest = self._scalars.cpu().tolist()
+        return change, largest
+
+    def _sweeps(self, x, held: _Held, newton: bool, floor: float = 0.0) -> int:
+        """FAC sweeps on ``x`` until the largest change is below the tolerance (the linear
+        one, or a Newton step's) of the larger of max |x| and ``floor``; returns the
+        corrections' V-cycles.  Each correction is solved to ``correction_tolerance`` of its
+        right-hand side: the sweeps themselves converge the composite system."""
+        tolerance = self.newton_sweep_tolerance if newton else self.tolerance
+        lib = _lib.lib()
+        cycles = 0
+        for sweep in range(1, self.max_sweeps + 1):
+            self._prev.copy_(x)
+            for number, solver in enumerate(self.corrections):
+                if newton:
+                    self._step_residual(x, self._r, held)
+                else:
+                    self.residual(x, self._r, held)
+                rhs = self._view(self._rhs_p, number)
+                e = self._view(self._e_p, number)
+                if self.local == "vcycle":
+                    self._gather[number].apply(self._r, rhs)
+                    solver._set_region(held.sides[number], 0.0)
+                    reaction = None
+                    if newton:
+                        reaction = self._view(self._reaction_p, number)
+                        self._gather[number].apply(self._reaction, reaction)
+                    _lib.check(lib.bt_poisson_vcycle(solver._handle, _lib.dptr(rhs),
+                                                     _lib.dptr(reaction),
+                                                     int(newton and sweep == 1),
+                                                     _lib.dptr(e)))  # fmt: skip
+                    cycles += 1
+                    held.prolong[number].apply(e.reshape(-1), x, accumulate=True)
+                    continue
+                self._gather_eps[number].apply(self._r, rhs)
+                e.zero_()
+                if newton:
+                    solver._set_region(held.sides[number], 0.0)
+                    reaction = self._view(self._reaction_p, number)
+                    self._gather[number].apply(self._reaction, reaction)
+                    taken = _lib.I32()
+                    _lib.check(lib.bt_poisson_solve_reaction(
+                        solver._handle, _lib.dptr(e), _lib.dptr(rhs), _lib.dptr(reaction),
+                        self.correction_tolerance, ctypes.byref(taken)))  # fmt: skip
+                    cycles += taken.value
+                else:
+                    solver.solve_device(e, rhs, fixed_region=held.sides[number],
+                                        linear_tolerance=self.correction_tolerance)
+                    cycles += solver.krylov_steps
+                held.prolong[number].apply(e.reshape(-1), x, accumulate=True)
+            self.fill_hanging(x)
+            change, largest = self._max_pair(x, self._prev)
+            scale = max(largest, floor, 1e-300)
+            if not np.isfinite(change):
+                raise RuntimeError("the composite field solve diverged (a non-finite update)")
+            if change <= tolerance * scale:
+                self.sweeps = sweep
+                return cycles
+        raise RuntimeError(f"the composite field solve did not converge in {self.max_sweeps} "
+                           "sweeps")  # fmt: skip
+
+    def solve_device(self, phi, rho=None, *, fixed_region=None, fixed_potential: float = 0.0,
+                     plasma: tuple[float, float, float, int] | None = None,
+                     newton_tolerance: float = 1e-6, max_newton: int = 100) -> None:  # fmt: skip
         n = self.layout.size
         if tuple(phi.shape) != (n,) or (rho is not None and tuple(rho.shape) != (n,)):
             raise ValueError(f"the composite solve takes ({n},) composite vectors")
+        held = self._held(fixed_region, fixed_potential)
         if rho is None:
             self._rho_p.zero_()
         else:
             for number in range(len(self.rows)):
                 self._gather[number].apply(rho, self._view(self._rho_p, number))
-        self._held.apply(phi, phi)
+        held.setter.apply(phi, phi)
         self.fill_hanging(phi)
+        self.newton_iterations = 0
+        if plasma is None:
+            self.krylov_steps = self._sweeps(phi, held, newton=False, floor=1.0)
+            return
+        amplitude, temperature, up, sign = plasma
+        lib = _lib.lib()
         cycles = 0
-        for sweep in range(1, self.max_sweeps + 1):
-            self._prev.copy_(phi)
-            for number, solver in enumerate(self.corrections):
-                self.residual(phi, self._r)
-                rhs = self._view(self._rhs_p, number)
-                e = self._view(self._e_p, number)
-                self._gather_eps[number].apply(self._r, rhs)
-                e.zero_()
-                solver.solve_device(e, rhs, fixed_region=self._sides[number],
-                                    linear_tolerance=self.correction_tolerance)
-                cycles += solver.krylov_steps
-                self._prolong[number].apply(e.reshape(-1), phi, accumulate=True)
+        d = _lib.dptr
+        for step in range(1, int(max_newton) + 1):
+            self.residual(phi, self._r0, held)
+            _lib.check(lib.bt_boltzmann_terms(_lib.context().handle, n, d(held.own), d(phi),
+                                              float(amplitude), float(temperature), float(up),
+                                              int(sign), d(self._r0), d(self._reaction)))  # fmt: skip
+            self._delta.zero_()
+            cycles += self._sweeps(self._delta, held, newton=True,
+                                   floor=1e-3 * float(newton_tolerance))
+            phi.add_(self._delta)
             self.fill_hanging(phi)
-            change = self._max(phi, self._prev)
-            scale = max(self._max(phi), 1.0)
-            if not np.isfinite(change):
-                raise RuntimeError("the composite field solve diverged (a non-finite update)")
-            if change <= self.tolerance * scale:
+            update = self._max(self._delta)
+            if not np.isfinite(update):
+                raise RuntimeError("the composite Newton update is not finite")
+            self.newton_iterations = step
+            if update < newton_tolerance:
                 break
-        else:
-            raise RuntimeError(f"the composite field solve did not converge in "
-                               f"{self.max_sweeps} sweeps")  # fmt: skip
-        self.sweeps = sweep
         self.krylov_steps = cycles
 
     def close(self) -> None:

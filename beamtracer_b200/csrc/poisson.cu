@@ -2208,6 +2208,55 @@ extern "C" int bt_poisson_residual(bt_poisson *p, const double *phi, const doubl
     });
 }
 
+extern "C" int bt_poisson_solve_reaction(bt_poisson *p, double *phi, const double *rho,
+                                         const double *reaction, double tol, int32_t *cycles) {
+    return bt::guarded([&] {
+        BT_REQUIRE(p && phi && reaction, "poisson: null argument");
+        BT_REQUIRE(tol > 0.0, "poisson: the tolerance must be positive");
+        BT_REQUIRE(!p->transposed, "poisson: the transposed solver takes no reaction");
+        const i64 n = p->n;
+        cudaStream_t st = p->ctx->stream;
+        bt::Level &L0 = p->levels[0];
+        double *b = p->rhs.as<double>(n);
+        double *r0 = p->r0.as<double>(n);
+        double *d = p->delta.as<double>(n);
+        bt::Timed timed(p->ctx, "field_solve");
+        BT_LAUNCH(p->ctx, bt::prepare, bt::blocks_for(n, 256), 256, 0, st, n, rho, p->src.as<double>(n),
+                  L0.active.as<uint8_t>(n), p->value_eff.as<double>(n), b, phi);
+        bt::build_hierarchy(p, reaction);
+        BT_LAUNCH(p->ctx, bt::apply5, bt::blocks_for(n, 256), 256, 0, st, p->nx, p->ny, L0.c4.as<double>(4 * n),
+                  L0.diag.as<double>(n), L0.active.as<uint8_t>(n), phi, b, r0);
+        BT_CHECK_LAUNCH();
+        const double scale = std::max(bt::norm2(p, b), bt::norm2(p, r0));
+        BT_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n, st));
+        double left = 0.0;
+        const double goal = tol * (scale > 0.0 ? scale : 1.0);
+        const int total = bt::gmres(p, r0, d, goal, 4000, &left);
+        BT_LAUNCH(p->ctx, bt::add_into, bt::blocks_for(n, 256), 256, 0, st, d, n, phi);
+        BT_CHECK_LAUNCH();
+        if (!(left <= 1e4 * goal))
+            throw bt::Error{BT_ERR_NOCONV, "field solve: GMRES did not reach the tolerance"};
+        int status = 0;
+        BT_CUDA(cudaMemcpyAsync(&status, p->status.as<int>(1), sizeof(int), cudaMemcpyDeviceToHost, st));
+        BT_CUDA(cudaStreamSynchronize(st));
+        if (status)
+            throw bt::Error{BT_ERR_NOCONV, "field solve: the coarsest operator is singular (is any node held?)"};
+        if (cycles) *cycles = total;
+    });
+}
+
+extern "C" int bt_poisson_vcycle(bt_poisson *p, const double *b, const double *reaction,
+                                 int32_t rebuild, double *z) {
+    return bt::guarded([&] {
+        BT_REQUIRE(p && b && z, "poisson: null argument");
+        BT_REQUIRE(!p->transposed, "poisson: the transposed solver takes no V-cycle here");
+        if (rebuild || !p->built || p->reaction_on != (reaction != nullptr))
+            bt::build_hierarchy(p, reaction);
+        bt::precondition(p, b, z);
+        BT_CHECK_LAUNCH();
+    });
+}
+
 extern "C" int bt_poisson_set_transposed(bt_poisson *p, int32_t on) {
     return bt::guarded([&] {
         BT_REQUIRE(p, "poisson: null solver");

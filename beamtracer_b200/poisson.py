@@ -240,11 +240,21 @@ class IonOpticsPoisson:
         ``tolerance * max(ptp(prescribed potentials), T, 1 V)`` (``poisson.py:874-877``).
         """
         if self._composite is not None:
-            if plasma is not None or fixed_region is not None:
-                raise NotImplementedError(
-                    "refined boxes take linear field solves (no plasma, no held region)")
-            self._composite.solve_device(phi, rho)
-            self.newton_iterations = 0
+            species, newton_tol = None, 0.0
+            if plasma is not None:
+                layout = self._layout
+                prescribed = layout.fixed_value[layout.fixed]
+                scale = max(float(np.ptp(prescribed)) if prescribed.size else 0.0,
+                            float(plasma.temperature), 1.0)  # fmt: skip
+                from scipy.constants import epsilon_0
+
+                species = (float(plasma.density) / epsilon_0, float(plasma.temperature),
+                           float(plasma.plasma_potential), int(plasma.sign))  # fmt: skip
+                newton_tol = float(tolerance) * scale
+            self._composite.solve_device(phi, rho, fixed_region=fixed_region,
+                                         fixed_potential=fixed_potential, plasma=species,
+                                         newton_tolerance=newton_tol, max_newton=max_newton)  # fmt: skip
+            self.newton_iterations = self._composite.newton_iterations
             self.krylov_steps = self._composite.krylov_steps
             return
         self._set_region(fixed_region, fixed_potential)

@@ -252,15 +252,14 @@ def vlasov_iterate(
             "adaptive refinement and the self magnetic field are not part of this build"
         )
     if tuple(refinement):
-        if plasma is not None or tuple(compensation) or coarse_particles < 1.0:
+        if tuple(compensation) or coarse_particles < 1.0:
             raise NotImplementedError(
-                "refined boxes take a linear field solve (no plasma), no compensation and "
-                "no coarse phase in this build"
+                "refined boxes take no compensation and no coarse phase in this build"
             )
         return _iterate_refined(
-            mesh, make_particles, tracer, iterations=iterations, tolerance=tolerance,
-            relaxation=relaxation, mixing=mixing, anderson_depth=anderson_depth,
-            refinement=tuple(refinement), callback=callback,
+            mesh, make_particles, tracer, iterations=iterations, plasma=plasma,
+            tolerance=tolerance, relaxation=relaxation, mixing=mixing,
+            anderson_depth=anderson_depth, refinement=tuple(refinement), callback=callback,
             density_tolerance=density_tolerance, poisson=poisson,
         )  # fmt: skip
     stride = int(np.ceil(1.0 / coarse_particles - 1e-9))
@@ -399,9 +398,9 @@ class RefinedVlasovState(VlasovState):
         return self.layout.on_base(self.composite_charge_density)
 
 
-def _iterate_refined(mesh, make_particles, tracer, *, iterations, tolerance, relaxation,
-                     mixing, anderson_depth, refinement, callback, density_tolerance,
-                     poisson) -> RefinedVlasovState:  # fmt: skip
+def _iterate_refined(mesh, make_particles, tracer, *, iterations, plasma, tolerance,
+                     relaxation, mixing, anderson_depth, refinement, callback,
+                     density_tolerance, poisson) -> RefinedVlasovState:  # fmt: skip
     """`vlasov_iterate` on refined boxes (``vlasov.py:304-427`` with a `Layout`): the
     composite field solve, the patches' edge fields, one trace through every patch, the
     patches' deposits summed on the composite nodes and divided by their volumes, mixing.
@@ -428,14 +427,26 @@ def _iterate_refined(mesh, make_particles, tracer, *, iterations, tolerance, rel
     loaded = None
     history: list[dict[str, float]] = []
     state = None
+    region_x = None if plasma is None else plasma.initial_plasma_x
+    boltzmann = None
+    j_over_v = None
     for iteration in range(iterations):
         previous.copy_(phi)
-        poisson.solve_device(phi, rho)
+        if plasma is not None and iteration == 0:
+            poisson.solve_device(phi, rho, fixed_region=lambda x, y: x < region_x,
+                                 fixed_potential=plasma.plasma_potential)  # fmt: skip
+        elif plasma is not None:
+            if boltzmann is None:
+                density = plasma.density if plasma.density is not None else j_over_v
+                boltzmann = plasma.boltzmann(density)
+            poisson.solve_device(phi, rho, plasma=boltzmann)
+        else:
+            poisson.solve_device(phi, rho)
         _lib.check(_lib.lib().bt_max_abs_diff(ctx.handle, _lib.dptr(phi), _lib.dptr(previous),
                                               n, _lib.dptr(scalars)))  # fmt: skip
         efield = PatchedElectricField(layout, phi, maps=maps)
         tracer.electric = efield
-        particles, _ = make_particles()
+        particles, j_over_v = make_particles()
         if particles is not loaded and particles is not engine.particles:
             engine.load(particles)
         loaded = particles
@@ -461,7 +472,7 @@ def _iterate_refined(mesh, make_particles, tracer, *, iterations, tolerance, rel
             "iteration": iteration,
             "max_potential_change": change,
             "relative_density_change": density_change if iteration > 0 else float("inf"),
-            "newton_iterations": 0,
+            "newton_iterations": poisson.newton_iterations,
             "krylov_steps": poisson.krylov_steps,
             "steps": int(host[3]) if engine.n else 0,
             "total_steps": int(host[4]) if engine.n else 0,
@@ -472,6 +483,7 @@ def _iterate_refined(mesh, make_particles, tracer, *, iterations, tolerance, rel
         density_now = charge / maps.volumes
         state = RefinedVlasovState(layout, phi, rho, efield,
                                    lambda d=density_now: engine.result(d), history)  # fmt: skip
+        state.plasma = boltzmann
         if callback is not None:
             _ = state.trace
             callback(iteration, state)

@@ -394,6 +394,70 @@ def run_plasma(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_refined(args) -> None:
+    """Refined boxes: the reference's refined extraction (``tests/unit/test_refinement.py``:
+    81 x 31 cylindrical, boxes of levels 1 and 2 over the aperture, a Boltzmann electron
+    plasma, 100 ions), converged solves per second through ``BeamOptics(config).run()``,
+    beside the oracle's converged solve of the same case (composite LU, the C trace on the
+    host cores) and the two potentials' largest difference."""
+    import torch
+
+    from beamtracer_b200 import BeamOptics, RefinementParams
+    from oracle import composite as oracle_composite
+    from oracle import kernels as oracle_kernels
+    from oracle import vlasov as oracle_vlasov
+    from tests.vlasov_cases import extraction, refined_problem
+
+    torch.cuda.set_device(0)
+    mm = 1e-3
+    config = extraction(1.0, refinement=[RefinementParams(1, (0.0, 0.0), (2.0 * mm, 1.5 * mm)),
+                                         RefinementParams(2, (0.0, 0.0), (1.5 * mm, 1.2 * mm))])
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        BeamOptics(config).run()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            model = BeamOptics(config).run()
+            stop.record(stream)
+            torch.cuda.synchronize()
+            times.append(start.elapsed_time(stop))
+    state = model.state
+    iterations = len(state.history)
+    problem, particles, j_over_v, layout = refined_problem(config)
+    t0 = time.perf_counter()
+    out = oracle_composite.vlasov(problem, layout, particles, iterations=iterations,
+                                  relaxation=config.relaxation,
+                                  plasma=oracle_vlasov.Plasma(5.0, 5.0, 0.6e-3, -1),
+                                  j_over_v=j_over_v)  # fmt: skip
+    cpu_s = time.perf_counter() - t0
+    phi_o = out["potential"]
+    total_ms = float(sum(times))
+    line = {
+        "metric": "converged refined-box extraction solves/s (81x31 cyl. + boxes of levels 1, 2; "
+                  "Boltzmann plasma)", "value": args.steps / (total_ms / 1e3), "unit": UNIT,
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "refined extraction: the reference's refined cylindrical case",
+                   "composite_nodes": layout.size, "patches": len(layout.patches),
+                   "iterations_per_solve": iterations,
+                   "newton_steps_per_solve": sum(h["newton_iterations"] for h in state.history)},
+        "e2e": {"value": args.steps / (total_ms / 1e3), "unit": UNIT,
+                "note": "the timed call is the public BeamOptics(config).run() from host inputs"},
+        "cpu_baseline": {"value": 1.0 / cpu_s, "unit": UNIT, "cores": oracle_kernels.host_cores(),
+                         "kind": "port", "sample": f"one solve of {iterations} iterations by the "
+                         "oracle (composite LU, C trace with OpenMP)"},
+        "parity": {"potential_max_rel": float(np.abs(state.composite_potential - phi_o).max()
+                                              / np.ptp(phi_o))},
+        "clocks": clocks.summary(),
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def run_design(args, rank: int, world: int, local: int) -> None:
     """Design workloads: ``gradient`` -- the gradient of the rms angle and the current at
     79 mm with respect to the three plate voltages and the beam current of the einzel lens
@@ -560,8 +624,9 @@ def main() -> None:
                         help="one warm adjoint gradient, then one in the NVTX range "
                              "'profiled_adjoint' (401 x 101, 2,000 rings)")
     parser.add_argument("--workload", default="einzel",
-                        choices=["einzel", "plasma", "gradient", "sweep"],
+                        choices=["einzel", "plasma", "gradient", "sweep", "refined"],
                         help="plasma: the planar plasma + solenoid extraction (one GPU); "
+                             "refined: the refined-box extraction (one GPU); "
                              "gradient: einzel design gradients; sweep: the design sweep")
     parser.add_argument("--sweep-count", type=int, default=32,
                         help="with --workload sweep: the candidates of one step")
@@ -576,6 +641,9 @@ def main() -> None:
         return
     if args.workload == "plasma" and args.impl == "b200":
         run_plasma(args)
+        return
+    if args.workload == "refined" and args.impl == "b200":
+        run_refined(args)
         return
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)

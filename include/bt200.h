@@ -497,6 +497,37 @@ int bt_csr_apply(bt_ctx *ctx, int64_t rows, const int64_t *out_rows, const int64
                  const int64_t *col, const double *val, const double *constant,
                  int32_t accumulate, const double *x, double *y);
 
+/* A linear solve of (A + diag(reaction)) phi = rho / eps0 + c on the free nodes, the held
+ * ones at their values (phi DEVICE (nx, ny) in/out: first guess, solution; rho DEVICE or
+ * NULL; reaction DEVICE (nx, ny)): one Newton step of solver/poisson.py:627-757 on a
+ * patch of refined boxes, where the composite Newton iteration supplies the Jacobian's
+ * reaction.  Relative residual tol; *cycles the V-cycles taken. */
+int bt_poisson_solve_reaction(bt_poisson *p, double *phi, const double *rho,
+                              const double *reaction, double tol, int32_t *cycles);
+
+/* solver/poisson.py:76-141, 898-903 on the composite nodes of refined boxes: at the nodes
+ * with own[k] != 0, e = amplitude exp(min(-sign (phi - up) / temperature, 50)) is added to
+ * r as sign e and reaction[k] = e / temperature; elsewhere reaction[k] = 0.  All DEVICE
+ * (n,). */
+int bt_boltzmann_terms(bt_ctx *ctx, int64_t n, const uint8_t *own, const double *phi,
+                       double amplitude, double temperature, double up, int32_t sign,
+                       double *r, double *reaction);
+
+/* One multigrid V-cycle from zero: z = M b (DEVICE (nx, ny); b a right-hand side of the
+ * mesh's equation as the residual of bt_poisson_residual is one, zero on held nodes), the
+ * operator's diagonal plus `reaction` (DEVICE, or NULL for none); the hierarchy is rebuilt
+ * when `rebuild` is set, the reaction's presence changed or the held nodes did.  The
+ * inexact local solve of each patch in the composite sweeps of refined boxes
+ * (solver/poisson.py:169-335 through patchwork, absent here). */
+int bt_poisson_vcycle(bt_poisson *p, const double *b, const double *reaction, int32_t rebuild,
+                      double *z);
+
+/* The residual of a composite Newton step's correction x (poisson.py:627-757 on refined
+ * boxes): y = base + y - reaction x at the nodes with own[k] != 0 (y holding -K x there on
+ * entry, base the step's residual), 0 elsewhere.  All DEVICE (n,). */
+int bt_newton_residual(bt_ctx *ctx, int64_t n, const uint8_t *own, const double *base,
+                       const double *reaction, const double *x, double *y);
+
 /* poisson.py:809-933 (IonOpticsPoisson.solve).  phi (DEVICE (nx, ny), in/out): the first
  * guess on entry (its fixed nodes are set), the solution on return; rho (DEVICE (nx, ny),
  * C/m^3, or NULL).  With amplitude = 0 one linear solve: GMRES preconditioned by a

@@ -219,15 +219,29 @@ def density_of(p, layout, potential, particles):
 
 
 def vlasov(p, layout, particles, *, iterations: int, tolerance: float = 0.0,
-           relaxation: float = 1.0, callback=None) -> dict:  # fmt: skip
-    """The Vlasov iteration on refined boxes (``vlasov.py:327-427``; linear field, linear
-    mixing): the composite potential and density of the last iteration and the history."""
+           relaxation: float = 1.0, plasma=None, j_over_v: float = 0.0,
+           callback=None) -> dict:  # fmt: skip
+    """The Vlasov iteration on refined boxes (``vlasov.py:327-427``, linear mixing): the
+    first iteration with a plasma holds the nodes below its initial x at the plasma
+    potential, the later ones solve with its Boltzmann species by Newton's method from the
+    last potential; the composite potential and density of the last iteration and the
+    history."""
+    from scipy import constants
+
     rho = np.zeros(layout.size)
     potential = None
     history = []
     out: dict = {}
     for iteration in range(iterations):
-        new = solve(layout, rho)
+        if plasma is not None and iteration == 0:
+            new = solve_region(layout, rho, lambda x, y: x < plasma.initial_x, plasma.potential)
+        elif plasma is not None:
+            density = plasma.density if plasma.density is not None else j_over_v
+            new, _ = solve_newton(layout, rho, density / constants.epsilon_0,
+                                  plasma.temperature, plasma.potential, plasma.sign,
+                                  initial=potential, tol=1e-11)  # fmt: skip
+        else:
+            new = solve(layout, rho)
         change = float("inf") if potential is None else float(np.max(np.abs(new - potential)))
         potential = new
         deposit, t = density_of(p, layout, potential, particles)
@@ -240,3 +254,58 @@ def vlasov(p, layout, particles, *, iterations: int, tolerance: float = 0.0,
         if change < tolerance:
             break
     return out
+
+
+def held_region(layout, region) -> np.ndarray:
+    """The nodes an initial plasma region holds (``poisson.py:279-309``): ``region(x, y)``
+    at the composite nodes, less those already held and the hanging ones."""
+    mask = np.asarray(region(layout.x, layout.y), dtype=bool) & ~layout.fixed
+    mask[layout.hanging] = False
+    return mask
+
+
+def _with_region(K, b, region_mask, value):
+    K = K.tolil()
+    for k in np.flatnonzero(region_mask):
+        K.rows[k] = [int(k)]
+        K.data[k] = [1.0]
+    b = b.copy()
+    b[region_mask] = value
+    return K.tocsr(), b
+
+
+def _equilibrated_solve(K, b, refine: int = 3) -> np.ndarray:
+    scale = 1.0 / abs(K).max(axis=1).toarray().ravel()
+    lu = splu((sparse.diags(scale) @ K).tocsc())
+    x = lu.solve(scale * b)
+    for _ in range(refine):
+        x += lu.solve(scale * (b - K @ x))
+    return x
+
+
+def solve_region(layout, rho, region, value) -> np.ndarray:
+    """The composite potential with the nodes of ``region`` held at ``value``."""
+    K, b = assemble(layout, rho)
+    K, b = _with_region(K, b, held_region(layout, region), value)
+    return _equilibrated_solve(K, b)
+
+
+def solve_newton(layout, rho, amplitude, temperature, up, sign, initial=None, tol=1e-11,
+                 max_newton=100):  # fmt: skip
+    """The composite potential with the Boltzmann species ``sign * amplitude
+    exp(-sign (phi - up) / T)`` in the source of every node with an equation of its own
+    (``poisson.py:860-933``): Newton from ``initial`` (default: the linear solution), a
+    full step each, until the largest update is below ``tol``."""
+    K, b = assemble(layout, rho)
+    own = (layout.owner >= 0) & ~layout.fixed
+    phi = _equilibrated_solve(K, b) if initial is None else np.array(initial, dtype=float)
+    steps = 0
+    for steps in range(1, max_newton + 1):
+        e = amplitude * np.exp(np.minimum(-sign * (phi - up) / temperature, 50.0))
+        residual = b + np.where(own, sign * e, 0.0) - K @ phi
+        jac = (K + sparse.diags(np.where(own, e / temperature, 0.0))).tocsr()
+        delta = _equilibrated_solve(jac, residual)
+        phi += delta
+        if np.max(np.abs(delta)) < tol:
+            break
+    return phi, steps
