@@ -441,8 +441,11 @@ class PatchedFieldMaps:
                 self.fy[fy_off[slot]:fy_off[slot + 1]].view(nxf, nyf + 1),
             )
             ints.append([nxf, nyf, fx_off[slot], fy_off[slot], nxf * nyf, node_off[slot]])
+            # along a graded x the kernel locates points by their uniform coordinate
             x0, y0, x1, y1 = patches[q].bounds
-            reals.append([mesh.origin[0], mesh.origin[1], mesh.h, x0, y0, x1, y1])
+            base = layout.base.mesh
+            lx0, lx1 = float(base.logical_x(x0)), float(base.logical_x(x1))
+            reals.append([*mesh.logical_origin, mesh.h, lx0, y0, lx1, y1])
         self.patch_int = torch.tensor(ints, dtype=torch.int64, device=dev)
         self.patch_real = torch.tensor(reals, dtype=torch.float64, device=dev)
         self.n_field_nodes = int(node_off[-1])
@@ -478,7 +481,7 @@ class PatchedFieldMaps:
             if not inside.size:
                 continue
             nxd, nyd = dmesh.shape
-            s = (x[inside] - dmesh.origin[0]) / dmesh.h
+            s = np.asarray(dmesh.index_x(x[inside]), dtype=float)
             t = (y[inside] - dmesh.origin[1]) / dmesh.h
             i = np.clip(np.floor(s).astype(np.int64), 0, nxd - 2)
             j = np.clip(np.floor(t).astype(np.int64), 0, nyd - 2)

@@ -21,8 +21,9 @@ are built from their definition:
   value is the linear interpolation of the edge's two ends (recursively, where an end
   hangs itself).
 
-Boxes of a level must lie inside the boxes of the level below (nested), and the x axis must
-be uniform.
+Boxes of a level must lie inside the boxes of the level below (nested).  Along a graded x
+axis a box is placed in the uniform coordinate of the node indices, and a level's nodes lie
+evenly between the base nodes (``solver/refinement.py:60-82``).
 """
 
 from __future__ import annotations
@@ -92,8 +93,6 @@ def patches_of(mesh: IonOpticsMesh, refinement: Sequence[Refinement]) -> list[Pa
     A box is widened to the cells of the level below, so it starts and ends on that level's
     nodes, and clipped to the mesh (``solver/refinement.py:85-152``).
     """
-    if mesh.graded and tuple(refinement):
-        raise NotImplementedError("refined boxes on a graded x axis are not part of this build")
     nx, ny = mesh.shape
     origin = mesh.origin
     upper = mesh.upper
@@ -105,8 +104,15 @@ def patches_of(mesh: IonOpticsMesh, refinement: Sequence[Refinement]) -> list[Pa
         parent = 2 ** (level - 1)  # the parent level's cells per base cell
         spans = []
         for axis, n in enumerate((nx, ny)):
-            c0, c1 = _parent_span(float(box.lower[axis]), float(box.upper[axis]), origin[axis],
-                                  upper[axis], mesh.h / parent, (n - 1) * parent)  # fmt: skip
+            lower, upper_ = float(box.lower[axis]), float(box.upper[axis])
+            start, end = origin[axis], upper[axis]
+            if axis == 0 and mesh.graded:
+                # along a graded x, the box in the uniform coordinate of the node indices
+                clip = lambda v: min(max(v, origin[0]), upper[0])  # noqa: E731
+                lower = float(mesh.logical_x(clip(lower)))
+                upper_ = float(mesh.logical_x(clip(upper_)))
+                start, end = mesh.logical_origin[0], mesh.logical_upper[0]
+            c0, c1 = _parent_span(lower, upper_, start, end, mesh.h / parent, (n - 1) * parent)
             if c1 <= c0:
                 raise ValueError(f"the refined box {box} is outside the mesh")
             spans.append((2 * c0, 2 * c1))
@@ -119,11 +125,19 @@ def patches_of(mesh: IonOpticsMesh, refinement: Sequence[Refinement]) -> list[Pa
         plane = bool(mesh.symmetry_plane and spans[1][0] == 0)
 
         def part(first_x: int, first_y: int, size: tuple[int, int]) -> IonOpticsMesh:
+            graded = {}
+            x0 = origin[0] + first_x * h
+            if mesh.graded:
+                # the level's nodes evenly between the base nodes of a graded x
+                nodes = np.asarray(mesh.position_x(np.arange(first_x, first_x + size[0])
+                                                   / 2**level), dtype=float)  # fmt: skip
+                x0 = float(nodes[0])
+                graded = {"x_nodes": nodes, "logical_x0": mesh.logical_x0 + first_x * h}
             return IonOpticsMesh(
-                shape=size, origin=(origin[0] + first_x * h, origin[1] + first_y * h), h=h,
+                shape=size, origin=(x0, origin[1] + first_y * h), h=h,
                 geometry=mesh.geometry, electrodes=mesh.electrodes,
                 faces=_patch_faces(mesh, touches), patch=True, symmetry_plane=plane,
-                classify_on_device=mesh.classify_on_device,
+                classify_on_device=mesh.classify_on_device, **graded,
             )  # fmt: skip
 
         patch_mesh = part(spans[0][0], spans[1][0], shape)
@@ -253,7 +267,8 @@ def layout_of(mesh: IonOpticsMesh, patches: list[Patch]) -> Layout:
     n = keys.size
     I, J = keys // span, keys % span
     hf = mesh.h / 2**finest
-    x = mesh.origin[0] + I * hf
+    x = (np.asarray(mesh.position_x(I / 2**finest), dtype=float) if mesh.graded
+         else mesh.origin[0] + I * hf)  # fmt: skip
     y = mesh.origin[1] + J * hf
     # owners: the finest patch whose inside holds the node
     owner = np.full(n, -1, dtype=np.int64)
@@ -347,11 +362,16 @@ def _leaf_volumes(mesh, patches, keys, span, finest):
         if not ci.size:
             continue
         h = mesh.h / 2**level
+        if mesh.graded:  # the cell's width between its two nodes along the graded x
+            width = (np.asarray(mesh.position_x((ci + 1) / 2**level), dtype=float)
+                     - np.asarray(mesh.position_x(ci / 2**level), dtype=float))  # fmt: skip
+        else:
+            width = np.full(ci.size, h)
         if mesh.cylindrical:
             rc = mesh.origin[1] + (cj + 0.5) * h
-            cell = 2.0 * np.pi * rc * h * h
+            cell = 2.0 * np.pi * rc * width * h
         else:
-            cell = np.full(ci.size, h * h)
+            cell = width * h
         s = 2 ** (finest - level)
         for di in (0, 1):
             for dj in (0, 1):

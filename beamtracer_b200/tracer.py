@@ -405,8 +405,6 @@ class TraceEngine:
         ``tracer.py:1141-1183``): the edge fields given to `run` are the patches' flattened
         one after the other, and the node charges fill ``n_nodes`` (every patch's field
         mesh nodes, in the same order)."""
-        if self.mesh.graded:
-            raise NotImplementedError("refined boxes on a graded x axis")
         self.patch_int = patch_int
         self.patch_real = patch_real
         if int(n_nodes) != self.n_nodes:

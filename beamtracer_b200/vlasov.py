@@ -252,9 +252,10 @@ def vlasov_iterate(
             "adaptive refinement and the self magnetic field are not part of this build"
         )
     if tuple(refinement):
-        if tuple(compensation) or coarse_particles < 1.0:
+        if tuple(compensation) or coarse_particles < 1.0 or tracer.magnetic is not None:
             raise NotImplementedError(
-                "refined boxes take no compensation and no coarse phase in this build"
+                "refined boxes take no compensation, no coarse phase and no magnetic field "
+                "in this build"
             )
         return _iterate_refined(
             mesh, make_particles, tracer, iterations=iterations, plasma=plasma,

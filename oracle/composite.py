@@ -141,7 +141,7 @@ def field_values(layout, potential) -> list[np.ndarray]:
                 if not inside.any():
                     continue
                 nxd, nyd = dmesh.shape
-                s = (x[inside] - dmesh.origin[0]) / dmesh.h
+                s = np.asarray(dmesh.index_x(x[inside]), dtype=float)
                 t = (y[inside] - dmesh.origin[1]) / dmesh.h
                 i = np.clip(np.floor(s).astype(np.int64), 0, nxd - 2)
                 j = np.clip(np.floor(t).astype(np.int64), 0, nyd - 2)
@@ -186,7 +186,10 @@ def trace_tables(layout, fields, meshes):
         fx_off += fx.size
         fy_off += fy.size
         node_off += nxf * nyf
-        reals.append([*mesh.origin, mesh.h, *layout.patches[q].bounds])
+        x0, y0, x1, y1 = layout.patches[q].bounds
+        base = layout.base.mesh
+        reals.append([*mesh.logical_origin, mesh.h, float(base.logical_x(x0)), y0,
+                      float(base.logical_x(x1)), y1])  # fmt: skip
         fxs.append(np.ravel(fx))
         fys.append(np.ravel(fy))
     return (np.array(ints, dtype=np.int64), np.array(reals, dtype=float), node_off,

@@ -74,11 +74,43 @@ def test_a_box_must_lie_inside_the_level_below() -> None:
                                    Refinement(2, (8e-3, 0.0), (10e-3, 2e-3))])  # fmt: skip
 
 
-def test_a_graded_axis_takes_no_boxes() -> None:
-    mesh = IonOpticsMesh((5, 5), (0.0, 0.0), 1.0, "planar",
-                         x_nodes=[0.0, 1.0, 1.5, 3.0, 4.0], classify_on_device=False)  # fmt: skip
-    with pytest.raises(NotImplementedError, match="graded"):
-        patches_of(mesh, [Refinement(1, (0.0, 0.0), (2.0, 2.0))])
+def graded_nodes(n: int, lower: float, upper: float) -> np.ndarray:
+    """``n`` nodes of a smooth map, cells from 0.7 to 1.3 of the mean (the reference's
+    ``test_graded_mesh.py:26-29`` case)."""
+    s = np.linspace(0.0, 1.0, n)
+    return lower + (upper - lower) * (s + 0.3 * np.sin(2.0 * np.pi * s) / (2.0 * np.pi))
+
+
+def test_refined_boxes_continue_the_grading() -> None:
+    """``test_graded_mesh.py:95-111``: every other node of a box is a base node, the others
+    halve the base edges; the box's uniform coordinate is the mesh's."""
+    nodes = graded_nodes(21, 0.0, 2.0)
+    mesh = IonOpticsMesh((21, 11), (0.0, 0.0), 0.1, "planar", x_nodes=nodes,
+                         classify_on_device=False)  # fmt: skip
+    base, patch = patches_of(mesh, [Refinement(1, (0.5, 0.2), (1.2, 0.6))])
+    first = patch.box[0][0] // 2
+    np.testing.assert_allclose(patch.mesh.x[::2], nodes[first : first + patch.mesh.x[::2].size])
+    np.testing.assert_allclose(patch.mesh.x[1::2], 0.5 * (patch.mesh.x[:-1:2] + patch.mesh.x[2::2]))
+    assert patch.mesh.logical_x0 == pytest.approx(patch.box[0][0] * 0.05)
+    x = np.linspace(patch.mesh.x[0], patch.mesh.x[-1], 7)
+    np.testing.assert_allclose(patch.mesh.logical_x(x), mesh.logical_x(x))
+    assert patch.field_mesh.x[2] == patch.mesh.x[0]
+
+
+@pytest.mark.parametrize("geometry", ["planar", "cylindrical"])
+def test_graded_volumes_fill_the_domain_and_the_plates_parabola_holds(geometry) -> None:
+    rho = 1e-6
+    nodes = graded_nodes(41, 0.0, 20e-3)
+    mesh = IonOpticsMesh((41, 21), (0.0, 0.0), 0.5e-3, geometry, x_nodes=nodes,
+                         faces=DIRICHLET_X, classify_on_device=False)  # fmt: skip
+    layout = layout_of_mesh(mesh, [Refinement(1, (4e-3, 0.0), (14e-3, 6e-3)),
+                                   Refinement(2, (6e-3, 0.0), (10e-3, 4e-3))])  # fmt: skip
+    total = 20e-3 * 10e-3 if geometry == "planar" else np.pi * 10e-3**2 * 20e-3
+    assert layout.volumes.sum() == pytest.approx(total)
+    if geometry == "planar":
+        phi = composite.solve(layout, np.full(layout.size, rho))
+        exact = rho / (2 * epsilon_0) * layout.x * (20e-3 - layout.x)
+        assert np.abs(phi - exact).max() < 1e-2 * exact.max()
 
 
 def test_a_uniform_charge_between_plates_on_refined_boxes() -> None:

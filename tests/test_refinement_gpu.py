@@ -248,3 +248,58 @@ def test_the_refined_extraction_with_plasma_equals_the_oracle() -> None:
         np.testing.assert_allclose(phi_g, phi_o, rtol=0, atol=1e-7 * 2000.0, err_msg=f"{k}")
         np.testing.assert_allclose(rho_g, rho_o, rtol=0, atol=1e-7 * np.abs(rho_o).max(),
                                    err_msg=f"{k}")  # fmt: skip
+
+
+@pytest.mark.parametrize("geometry", ["planar", "cylindrical"])
+def test_refined_boxes_on_a_graded_axis_equal_the_oracle(geometry) -> None:
+    """Boxes on a graded x (``test_graded_mesh.py:95-155``): the composite solve, the
+    patches' fields and, stage-wise, the density a beam deposits through them, against the
+    oracle."""
+    import torch
+    from scipy import constants
+
+    from beamtracer_b200.composite import PatchedElectricField, PatchedFieldMaps
+    from beamtracer_b200.poisson import IonOpticsPoisson
+    from beamtracer_b200.tracer import BeamParticles, TraceEngine
+    from tests.test_refinement import graded_nodes
+    from tests.vlasov_cases import host_twin, mesh_problem
+
+    faces = {"x_min": FaceCondition("dirichlet", 5.0), "x_max": FaceCondition("dirichlet", -2000.0)}
+    electrodes = [Electrode(_box(0.5e-3, 1e-3, 1e-3, 3.1e-3), 0.0),
+                  Electrode(_box(3e-3, 4e-3, 1.2e-3, 3.1e-3), -2000.0)]  # fmt: skip
+    mesh = IonOpticsMesh((81, 31), (0.0, 0.0), 1e-4, geometry, x_nodes=graded_nodes(81, 0.0, 8e-3),
+                         electrodes=electrodes, faces=faces)  # fmt: skip
+    boxes = BOXES["axis"]
+    solver = IonOpticsPoisson(mesh, refinement=boxes)
+    layout = solver.layout
+    ora_layout = layout_of_mesh(host_twin(mesh), boxes)
+    np.testing.assert_array_equal(layout.x, ora_layout.x)
+    rho = 1e-4 * np.exp(-((layout.x - 2e-3) ** 2 + layout.y**2) / (1e-3) ** 2)
+    phi = solver.solve(rho)
+    ora = oracle_composite.solve(ora_layout, rho)
+    assert np.abs(phi - ora).max() <= 1e-9 * np.ptp(ora)
+    # the beam through the patches of the oracle's potential
+    n = 200
+    mass = constants.m_p
+    speed = np.sqrt(2.0 * 5.0 * constants.e / mass)
+    position = np.zeros((3, n))
+    position[0] = 1e-6
+    position[1] = np.linspace(0.02e-3, 0.85e-3, n)
+    velocity = np.zeros((3, n))
+    velocity[0] = speed
+    particles = BeamParticles(position, velocity, np.full(n, constants.e), np.full(n, mass),
+                              np.full(n, 1e-6), np.zeros(n, dtype=np.int64))  # fmt: skip
+    maps = PatchedFieldMaps(layout)
+    PatchedElectricField(layout, torch.from_numpy(ora).cuda(), maps=maps)
+    engine = TraceEngine(mesh, planes=(7.5e-3,))
+    engine.set_patches(maps.patch_int, maps.patch_real, maps.n_field_nodes)
+    engine.load(particles)
+    engine.run(maps.fx, maps.fy)
+    charge = torch.zeros(layout.size, dtype=torch.float64, device="cuda")
+    maps.charge_map.apply(engine.charge.reshape(-1), charge)
+    rho_dev = (charge / maps.volumes).cpu().numpy()
+    problem = mesh_problem(mesh, planes=(7.5e-3,))
+    rho_ora, t = oracle_composite.density_of(problem, ora_layout, ora, particles)
+    np.testing.assert_array_equal(engine.status.cpu().numpy(), t.status)
+    assert np.abs(rho_ora).max() > 0.0
+    assert np.abs(rho_dev - rho_ora).max() <= 1e-10 * np.abs(rho_ora).max()
