@@ -351,3 +351,104 @@ def adjoint_design_gradient(design, plane: float = 79e-3, tolerance: float = 1e-
             "moments": {k: float(v.detach()) for k, v in moments.items()}, "solves": 1,
             "adjoint_iterations": problem.adjoint_iterations,
             "converged": problem.converged, "surface_fields": dict(problem.surface_fields)}  # fmt: skip
+
+
+# -- gradients of the candidates of a batch ----------------------------------------------------
+
+
+class _CandidateSolve:
+    """What `SolveAdjoint` and `LensMoments` read of a converged solve, for candidate ``k``
+    of a finished `BatchedVlasov`: its mesh and configuration, the edge fields of its last
+    iteration (kept in the batch's buffers) and its beam traced alone through them (the
+    same trajectories as in the batch, bit for bit)."""
+
+    def __init__(self, batch, k: int) -> None:
+        from types import SimpleNamespace
+
+        from beamtracer_b200.fields import default_extrapolation
+
+        c = batch.candidates[k]
+        if c.planes is None:
+            raise RuntimeError("the candidate has not finished")
+        self.config = c.config
+        self.mesh = c.mesh
+        fx, fy = batch.edge_views(k)
+        engine = c.engine
+        engine.run(fx, fy)
+        self.tracer = SimpleNamespace(engine=lambda: engine)
+        electric = SimpleNamespace(fx_device=fx, fy_device=fy,
+                                   extrapolation=tuple(default_extrapolation(c.mesh)))  # fmt: skip
+        self.state = SimpleNamespace(electric=electric, trace=engine.result())
+        self.stats = {"converged": bool(c.converged)}
+
+    def surface_fields(self) -> dict[str, float]:
+        return {}
+
+    def plane(self, x: float):
+        match = [hits for hits in self.state.trace.planes if np.isclose(hits.position_x, x)]
+        if not match:
+            raise KeyError(f"no diagnostic plane at x = {x}")
+        return match[0]
+
+
+class _BatchLensProblem(LensProblem):
+    """A `LensProblem` whose forward solve is candidate ``k`` of a finished batch (solved
+    there at the design's own parameters)."""
+
+    def __init__(self, batch, k: int, design, plane: float, adjoint_tolerance: float) -> None:
+        super().__init__(design, plane, adjoint_tolerance=adjoint_tolerance)
+        self.batch, self.k = batch, k
+
+    def solve(self, params: np.ndarray):
+        return _CandidateSolve(self.batch, self.k)
+
+
+def batch_design_gradients(batch, designs, plane: float = 79e-3, adjoint_tolerance: float = 1e-8,
+                           concurrency: int = 8) -> list[dict]:  # fmt: skip
+    """The gradients of the rms angle and the current at ``plane`` with respect to the
+    plate voltages and the beam current (`GRADIENT_PARAMETERS`) of every candidate of a
+    finished `BatchedVlasov` of einzel ``designs`` (in its order): the adjoint of each
+    candidate's converged solve, as `adjoint_design_gradient` takes it of a solve of its
+    own (the batch's candidates should be converged as tightly, e.g. to 1e-6 V).  With
+    ``concurrency`` > 1 that many host threads take candidates at once, each on its own
+    CUDA stream and library context; the gradients agree with one candidate at a time to
+    rounding (the reverse sweep's scatter adds with atomics)."""
+    import threading
+
+    import torch
+
+    from beamtracer_b200.einzel import design_cost, resolved_voltages
+
+    device = torch.cuda.current_device()
+    torch.cuda.synchronize()  # the batch's fields, read by every thread
+    local = threading.local()
+
+    def gradient(k: int) -> tuple[int, dict]:
+        design = designs[k]
+        torch.cuda.set_device(device)
+        if getattr(local, "stream", None) is None:
+            local.stream = torch.cuda.Stream() if concurrency > 1 else torch.cuda.current_stream()
+        with torch.cuda.stream(local.stream):
+            problem = _BatchLensProblem(batch, k, design, plane, adjoint_tolerance)
+            start = [*resolved_voltages(design), design.current]
+            params = torch.tensor(start, dtype=torch.float64, requires_grad=True)
+            point, velocity, current, direction = LensMoments.apply(params, problem)
+            moments = moments_torch(point, velocity, current, direction, cylindrical=True)
+            (angle,) = torch.autograd.grad(moments["rms_angle"], params, retain_graph=True)
+            (transmitted,) = torch.autograd.grad(moments["current"], params)
+        local.stream.synchronize()
+        return k, {"rms_angle": angle.numpy().copy(), "current": transmitted.numpy().copy(),
+                   "moments": {name: float(v.detach()) for name, v in moments.items()},
+                   "adjoint_iterations": problem.adjoint_iterations,
+                   "converged": problem.converged}  # fmt: skip
+
+    # the costliest first, so the threads finish together
+    order = sorted(range(len(designs)), key=lambda k: -design_cost(designs[k]))
+    if concurrency <= 1:
+        done = dict(gradient(k) for k in order)
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+
+        with ThreadPoolExecutor(max_workers=concurrency) as pool:
+            done = dict(pool.map(gradient, order))
+    return [done[k] for k in range(len(designs))]

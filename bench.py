@@ -458,6 +458,51 @@ def run_refined(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def sweep_with_gradients(designs, stream) -> dict:
+    """The sweep's forward plus adjoint (one GPU): every candidate converged to 1e-6 V and
+    its gradients of the rms angle and the current at 79 mm with respect to the plate
+    voltages and the beam current -- batched (one `BatchedVlasov`, then the adjoint of each
+    candidate's converged solve) and in the plain form (each candidate's own solve and
+    adjoint, one at a time); both timed once with CUDA events, configuration building
+    included, and their gradients compared."""
+    import torch
+
+    from beamtracer_b200.adjoint import adjoint_design_gradient, batch_design_gradients
+    from beamtracer_b200.batch import BatchedVlasov
+    from beamtracer_b200.einzel import einzel_config
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        out = fn()
+        stop.record(stream)
+        torch.cuda.synchronize()
+        return out, start.elapsed_time(stop)
+
+    def batched():
+        batch = BatchedVlasov([einzel_config(d, tolerance=1e-6, iterations=60)
+                               for d in designs]).run()  # fmt: skip
+        grads = batch_design_gradients(batch, designs)
+        batch.close()
+        return grads
+
+    grads, batched_ms = timed(batched)
+    plain, plain_ms = timed(lambda: [adjoint_design_gradient(d) for d in designs])
+    worst = 0.0
+    for mine, alone in zip(grads, plain):
+        for name in ("rms_angle", "current"):
+            scale = float(np.abs(alone[name]).max())
+            if scale > 0.0:
+                worst = max(worst, float(np.abs(mine[name] - alone[name]).max()) / scale)
+    n = len(designs)
+    return {"unit": "candidates/s", "batched": n * 1e3 / batched_ms,
+            "plain_form": n * 1e3 / plain_ms, "speedup_over_plain": plain_ms / batched_ms,
+            "max_rel_gradient_diff": worst, "forward_tolerance_v": 1e-6,
+            "note": "batched forward in one BatchedVlasov, then each candidate's adjoint; "
+                    "plain: each candidate's own solve and adjoint"}
+
+
 def run_design(args, rank: int, world: int, local: int) -> None:
     """Design workloads: ``gradient`` -- the gradient of the rms angle and the current at
     79 mm with respect to the three plate voltages and the beam current of the einzel lens
@@ -591,6 +636,8 @@ def run_design(args, rank: int, world: int, local: int) -> None:
         line["max_rel_moment_diff_vs_plain"] = worst
         line["iteration_mismatches"] = sum(result[k]["iterations"] != plain[k]["iterations"]
                                            for k in plain)  # fmt: skip
+        if args.adjoint and world == 1:
+            line["forward_plus_adjoint"] = sweep_with_gradients(designs, stream)
     if args.workload == "gradient":
         line["gradient"] = {k: [float(v) for v in result[k]] for k in ("rms_angle", "current")}
         line["adjoint_iterations"] = result["adjoint_iterations"]
@@ -630,6 +677,9 @@ def main() -> None:
                              "gradient: einzel design gradients; sweep: the design sweep")
     parser.add_argument("--sweep-count", type=int, default=32,
                         help="with --workload sweep: the candidates of one step")
+    parser.add_argument("--adjoint", action="store_true",
+                        help="with --workload sweep: also time the forward plus adjoint of "
+                             "every candidate, batched and in the plain form")
     parser.add_argument("--concurrency", type=int, default=8,
                         help="with --workload sweep or gradient: solves at once per GPU")
     args = parser.parse_args()
