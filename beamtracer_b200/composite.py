@@ -236,7 +236,7 @@ class CompositePoisson:
         for number, solver in enumerate(self.corrections):
             d_p = self._view(self._phi_p, number)
             self._gather[number].apply(delta, d_p)
-            solver._set_region(held.sides[number], 0.0)
+            solver.hold(held.sides[number])
             _lib.check(lib.bt_poisson_residual(solver._handle, _lib.dptr(d_p), None,
                                                _lib.dptr(self._view(self._res_p, number))))  # fmt: skip
         held.owned.apply(self._res_p, r)
@@ -281,7 +281,7 @@ class CompositePoisson:
                 e = self._view(self._e_p, number)
                 if self.local == "vcycle":
                     self._gather[number].apply(self._r, rhs)
-                    solver._set_region(held.sides[number], 0.0)
+                    solver.hold(held.sides[number])
                     reaction = None
                     if newton:
                         reaction = self._view(self._reaction_p, number)
@@ -296,7 +296,7 @@ class CompositePoisson:
                 self._gather_eps[number].apply(self._r, rhs)
                 e.zero_()
                 if newton:
-                    solver._set_region(held.sides[number], 0.0)
+                    solver.hold(held.sides[number])
                     reaction = self._view(self._reaction_p, number)
                     self._gather[number].apply(self._reaction, reaction)
                     taken = _lib.I32()
@@ -399,21 +399,20 @@ class PatchedFieldMaps:
                 matrix = _selection(patch.index, n)
                 constant = np.zeros(nxf * nyf)
             else:
+                # the margin bilinear, its electrode nodes at their potential, the box's
+                # own nodes from the composite nodes (in that order of precedence)
                 matrix, constant = self._margin(matrices, constants, mesh)
                 solid = np.asarray(mesh.solid).ravel() >= 0
-                keep = sparse.diags((~solid).astype(float))
-                matrix = (keep @ matrix).tocsr()
-                constant = np.where(solid, np.asarray(mesh.fixed_value).ravel(), constant)
                 inner = np.zeros((nxf, nyf), dtype=bool)
                 inner[patch.inner] = True
                 inner = inner.ravel()
-                rows = np.flatnonzero(inner)
-                matrix = sparse.lil_matrix(matrix)
-                for r, k in zip(rows, patch.index.ravel()):
-                    matrix.rows[r] = [int(k)]
-                    matrix.data[r] = [1.0]
-                matrix = matrix.tocsr()
-                constant = np.where(inner, 0.0, constant)
+                keep = sparse.diags((~solid & ~inner).astype(float))
+                own = sparse.csr_matrix((np.ones(patch.index.size),
+                                         (np.flatnonzero(inner), patch.index.ravel())),
+                                        shape=(nxf * nyf, n))  # fmt: skip
+                matrix = (keep @ matrix + own).tocsr()
+                constant = np.where(inner, 0.0, np.where(
+                    solid, np.asarray(mesh.fixed_value).ravel(), constant))
             matrix.eliminate_zeros()
             matrices.append(matrix)
             constants.append(constant)

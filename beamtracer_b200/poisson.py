@@ -195,6 +195,13 @@ class IonOpticsPoisson:
 
     # -- the device path --------------------------------------------------------------
 
+    def hold(self, region: Any, potential: float = 0.0) -> None:
+        """Hold the nodes of ``region`` (an (nx, ny) mask, a function of the nodes'
+        ``(x, y)``, or None for none) that the mesh does not fix at ``potential`` in later
+        solves (the initial plasma region; a refined box's sides in its corrections); a
+        region equal to the one held already changes nothing."""
+        self._set_region(region, potential)
+
     def _set_region(self, region: Any, potential: float) -> None:
         if region is None:
             key: object = None
