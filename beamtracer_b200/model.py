@@ -262,7 +262,11 @@ class BeamOptics:
         electrode (`surface_field`), 0 for an electrode with no free neighbour."""
         from beamtracer_b200.fields import surface_field_device
 
-        _, _, largest = surface_field_device(self.mesh, self.state.electric)
+        electric = self.state.electric
+        # with refined boxes, the base mesh's field (the patches' own fields cover their
+        # boxes only)
+        base = electric.fields[0] if hasattr(electric, "fields") else electric
+        _, _, largest = surface_field_device(self.mesh, base)
         values = largest.cpu().numpy()
         return {name: float(values[k]) for k, name in enumerate(self.config.objects)}
 

@@ -165,3 +165,37 @@ def test_the_setting_is_checked_and_round_trips() -> None:
     assert again.refinement[0].upper == pytest.approx((3e-3, 1.5e-3))
     with pytest.raises(ValueError, match="2D grid"):
         BeamOpticsConfig(grid=grid, refinement=[RefinementParams(1, (0, 0, 0), (1, 1, 1))])
+
+
+def test_the_oracle_newton_and_held_region_solve_their_equations() -> None:
+    """The oracle's composite Newton iteration and held region: the Boltzmann residual
+    vanishes at its solution, the held nodes keep their potential, and without refinement
+    Newton's composite solution is the mesh's (``oracle/poisson.py``)."""
+    from scipy.constants import epsilon_0 as eps0
+
+    from oracle import poisson as oracle_poisson
+
+    plate = lambda x, y: (x >= 8e-3) & (x <= 10e-3) & (y >= 4e-3)  # noqa: E731
+    faces = {"x_min": FaceCondition("dirichlet", 5.0), "x_max": FaceCondition("dirichlet", -50.0)}
+    mesh = IonOpticsMesh((21, 11), (0.0, 0.0), 1e-3, "cylindrical", faces=faces,
+                         electrodes=[Electrode(plate, -20.0)], classify_on_device=False)  # fmt: skip
+    region = lambda x, y: x < 3e-3  # noqa: E731
+    rho = np.full(layout_of_mesh(mesh).size, 1e-8)
+    for boxes in ([], [Refinement(1, (0.0, 0.0), (6e-3, 4e-3))]):
+        layout = layout_of_mesh(mesh, boxes)
+        rho = np.full(layout.size, 1e-8)
+        held = composite.solve_region(layout, rho, region, 5.0)
+        mask = composite.held_region(layout, region)
+        np.testing.assert_array_equal(held[mask], 5.0)
+        phi, steps = composite.solve_newton(layout, rho, 1e-3 / eps0, 5.0, 5.0, -1, initial=held)
+        assert steps >= 2
+        K, b = composite.assemble(layout, rho)
+        own = (layout.owner >= 0) & ~layout.fixed
+        e = 1e-3 / eps0 * np.exp(np.minimum((phi - 5.0) / 5.0, 50.0))
+        residual = b - np.where(own, e, 0.0) - K @ phi
+        assert np.abs(residual).max() <= 1e-7 * np.abs(b).max()
+        if not boxes:
+            op = oracle_poisson.operator_of_mesh(mesh)
+            direct, _ = oracle_poisson.solve_newton(op, layout.on_base(rho), 1e-3 / eps0, 5.0,
+                                                    5.0, -1, tol=1e-11)  # fmt: skip
+            np.testing.assert_allclose(layout.on_base(phi), direct, rtol=0, atol=1e-9)

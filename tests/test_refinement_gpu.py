@@ -175,6 +175,9 @@ def test_the_refined_vlasov_iteration_equals_the_oracle() -> None:
     state = model.state
     assert state.layout.refined and state.composite_potential.size > state.potential.size
     assert state.potential.shape == model.mesh.shape
+    fields = model.surface_fields()
+    assert set(fields) == set(config.objects) and all(np.isfinite(list(fields.values())))
+    assert model.beam_moments(0.115).current > 0.0
     problem, particles, _, layout = refined_problem(config)
     ora = []
     oracle_composite.vlasov(problem, layout, particles, iterations=3,
@@ -303,3 +306,24 @@ def test_refined_boxes_on_a_graded_axis_equal_the_oracle(geometry) -> None:
     np.testing.assert_array_equal(engine.status.cpu().numpy(), t.status)
     assert np.abs(rho_ora).max() > 0.0
     assert np.abs(rho_dev - rho_ora).max() <= 1e-10 * np.abs(rho_ora).max()
+
+
+def test_a_refined_box_brings_the_beam_to_that_of_the_fine_mesh() -> None:
+    """The reference's behavioural case (``test_refinement.py:168-181``): a box around the
+    extraction aperture moves the beam's divergence towards that of a mesh of half the
+    cells everywhere."""
+    from beamtracer_b200 import BeamOptics, GridParams, RefinementParams
+    from tests.vlasov_cases import extraction
+
+    def divergence(config) -> float:
+        model = BeamOptics(config.replace(iterations=60, tolerance=1e-5)).run()
+        return model.beam_moments(7.5e-3).rms_angle
+
+    coarse = extraction(1.0)
+    grid = coarse.grid
+    fine = coarse.replace(grid=GridParams(num_gridpoints=(161, 61), lower_bound=grid.lower_bound,
+                                          upper_bound=grid.upper_bound,
+                                          coordinates=grid.coordinates))  # fmt: skip
+    box = coarse.replace(refinement=[RefinementParams(1, (0.0, 0.0), (4.5e-3, 2.0e-3))])
+    reference = divergence(fine)
+    assert abs(divergence(box) - reference) < 0.5 * abs(divergence(coarse) - reference)
