@@ -458,7 +458,7 @@ def run_refined(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def sweep_with_gradients(designs, stream) -> dict:
+def sweep_with_gradients(designs, stream, concurrency: int = 8) -> dict:
     """The sweep's forward plus adjoint (one GPU): every candidate converged to 1e-6 V and
     its gradients of the rms angle and the current at 79 mm with respect to the plate
     voltages and the beam current -- batched (one `BatchedVlasov`, then the adjoint of each
@@ -483,7 +483,7 @@ def sweep_with_gradients(designs, stream) -> dict:
     def batched():
         batch = BatchedVlasov([einzel_config(d, tolerance=1e-6, iterations=60)
                                for d in designs]).run()  # fmt: skip
-        grads = batch_design_gradients(batch, designs)
+        grads = batch_design_gradients(batch, designs, concurrency=concurrency)
         batch.close()
         return grads
 
@@ -499,6 +499,7 @@ def sweep_with_gradients(designs, stream) -> dict:
     return {"unit": "candidates/s", "batched": n * 1e3 / batched_ms,
             "plain_form": n * 1e3 / plain_ms, "speedup_over_plain": plain_ms / batched_ms,
             "max_rel_gradient_diff": worst, "forward_tolerance_v": 1e-6,
+            "concurrency": concurrency,
             "note": "batched forward in one BatchedVlasov, then each candidate's adjoint; "
                     "plain: each candidate's own solve and adjoint"}
 
@@ -637,7 +638,8 @@ def run_design(args, rank: int, world: int, local: int) -> None:
         line["iteration_mismatches"] = sum(result[k]["iterations"] != plain[k]["iterations"]
                                            for k in plain)  # fmt: skip
         if args.adjoint and world == 1:
-            line["forward_plus_adjoint"] = sweep_with_gradients(designs, stream)
+            line["forward_plus_adjoint"] = sweep_with_gradients(designs, stream,
+                                                                args.concurrency)
     if args.workload == "gradient":
         line["gradient"] = {k: [float(v) for v in result[k]] for k in ("rms_angle", "current")}
         line["adjoint_iterations"] = result["adjoint_iterations"]

@@ -222,15 +222,19 @@ def density_of(p, layout, potential, particles):
 
 
 def vlasov(p, layout, particles, *, iterations: int, tolerance: float = 0.0,
-           relaxation: float = 1.0, plasma=None, j_over_v: float = 0.0,
-           callback=None) -> dict:  # fmt: skip
-    """The Vlasov iteration on refined boxes (``vlasov.py:327-427``, linear mixing): the
-    first iteration with a plasma holds the nodes below its initial x at the plasma
-    potential, the later ones solve with its Boltzmann species by Newton's method from the
-    last potential; the composite potential and density of the last iteration and the
+           relaxation: float = 1.0, plasma=None, j_over_v: float = 0.0, mixing: str = "linear",
+           anderson_depth: int = 5, callback=None) -> dict:  # fmt: skip
+    """The Vlasov iteration on refined boxes (``vlasov.py:327-427``, linear or Anderson
+    mixing as the mesh's loop mixes): the first iteration with a plasma holds the nodes
+    below its initial x at the plasma potential, the later ones solve with its Boltzmann
+    species by Newton's method from the last potential; the composite potential and
+    density of the last iteration and the
     history."""
     from scipy import constants
 
+    from oracle import vlasov as oracle_vlasov
+
+    mixer = oracle_vlasov.Anderson(anderson_depth, relaxation) if mixing == "anderson" else None
     rho = np.zeros(layout.size)
     potential = None
     history = []
@@ -248,7 +252,12 @@ def vlasov(p, layout, particles, *, iterations: int, tolerance: float = 0.0,
         change = float("inf") if potential is None else float(np.max(np.abs(new - potential)))
         potential = new
         deposit, t = density_of(p, layout, potential, particles)
-        rho = deposit if iteration == 0 else (1.0 - relaxation) * rho + relaxation * deposit
+        if iteration == 0:
+            rho = deposit
+        elif mixer is not None:
+            rho = mixer.update(rho, deposit)
+        else:
+            rho = (1.0 - relaxation) * rho + relaxation * deposit
         history.append({"iteration": iteration, "max_potential_change": change})
         out = {"potential": potential, "charge_density": rho, "deposit": deposit, "trace": t,
                "history": history}  # fmt: skip

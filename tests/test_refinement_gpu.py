@@ -308,6 +308,30 @@ def test_refined_boxes_on_a_graded_axis_equal_the_oracle(geometry) -> None:
     assert np.abs(rho_dev - rho_ora).max() <= 1e-10 * np.abs(rho_ora).max()
 
 
+def test_refined_anderson_mixing_equals_the_oracle() -> None:
+    """Anderson mixing on the composite nodes (``vlasov.py:127-173``): the refined slit
+    lens per iteration against the oracle's NumPy mixer."""
+    from beamtracer_b200 import BeamOptics, RefinementParams
+    from tests.vlasov_cases import refined_problem, slit_lens
+
+    config = slit_lens(iterations=5, mixing="anderson", anderson_depth=3, relaxation=0.7,
+                       refinement=[RefinementParams(1, (0.0, 0.0), (0.04, 0.02))])  # fmt: skip
+    gpu = []
+    BeamOptics(config).run(lambda it, s: gpu.append((s.composite_potential.copy(),
+                                                     s.composite_charge_density.copy())))  # fmt: skip
+    problem, particles, _, layout = refined_problem(config)
+    ora = []
+    oracle_composite.vlasov(problem, layout, particles, iterations=5, relaxation=0.7,
+                            mixing="anderson", anderson_depth=3,
+                            callback=lambda it, o: ora.append((o["potential"].copy(),
+                                                               o["charge_density"].copy())))  # fmt: skip
+    assert len(gpu) == len(ora) == 5
+    span = np.ptp(ora[0][0])
+    for k, ((phi_g, rho_g), (phi_o, rho_o)) in enumerate(zip(gpu, ora)):
+        assert np.abs(phi_g - phi_o).max() <= 1e-8 * span, k
+        assert np.abs(rho_g - rho_o).max() <= 1e-6 * np.abs(rho_o).max(), k
+
+
 def test_a_refined_box_brings_the_beam_to_that_of_the_fine_mesh() -> None:
     """The reference's behavioural case (``test_refinement.py:168-181``): a box around the
     extraction aperture moves the beam's divergence towards that of a mesh of half the
