@@ -318,3 +318,23 @@ def mesh3d_case() -> dict:
         "faces": {"x_max": ("dirichlet", 800.0), "y_min": ("neumann", 0.0)},
         "symmetry_planes": ("y_min",),
     }  # fmt: skip
+
+
+# -- refined boxes ------------------------------------------------------------------------
+
+
+def refinement_cases() -> dict[str, list[tuple[int, tuple[float, float], tuple[float, float]]]]:
+    """Nested boxes ``(level, lower, upper)`` on the meshes of `mesh_cases`: around the
+    plates' ring electrode, along the lens's axis with a finer box off the axis, and over
+    the graded mesh's disc."""
+    return {
+        "planar_plates": [(1, (8e-3, 3e-3), (18e-3, 12e-3)), (2, (10e-3, 5e-3), (14e-3, 9e-3))],
+        "cylindrical_lens": [(1, (15e-3, 0.0), (45e-3, 10e-3)), (2, (36e-3, 2e-3), (44e-3, 8e-3))],
+        "graded_disc": [(1, (12e-3, -5e-3), (28e-3, 5e-3))],
+    }
+
+
+def refinement_potential(x, y):
+    """A smooth potential [V] to take the patches' fields of."""
+    x, y = np.asarray(x, dtype=float), np.asarray(y, dtype=float)
+    return 300.0 * np.sin(170.0 * x + 0.3) * np.cos(110.0 * y) + 2.0e4 * x * y

@@ -330,14 +330,82 @@ def _save(name: str, args: list, result: list, extra: dict | None = None) -> Non
     np.savez_compressed(HERE / f"{name}.npz", **arrays)
 
 
+def refinement_goldens(root: Path) -> None:
+    """The reference's refined patches (``solver/refinement.py:83-152``) and their fields
+    (``PatchedElectricField``, ``:319-365``, its edge fields by the reference's
+    ``_edge_field``) on the meshes of `mesh_cases` with the boxes of `refinement_cases`, for
+    the potential `refinement_potential` at every patch's nodes."""
+    from collections.abc import Sequence
+    from dataclasses import dataclass
+    from typing import Any
+
+    from tests.golden.cases import mesh_cases, refinement_cases, refinement_potential
+
+    mesh_module = reference_mesh_module(root)
+    edge_field = reference_edge_field(root)
+
+    class StaggeredElectricField:
+        """The reference's edge fields of a potential (``fields.py:116-152``)."""
+
+        def __init__(self, mesh, values, extrapolation) -> None:
+            solid, near = mesh.solid >= 0, mesh.near_solid
+            self.values = np.array(values, dtype=float)
+            self.fx = edge_field(self.values, solid, near, mesh.distance[0], mesh.distance[1],
+                                 mesh.dx, extrapolation[0:2])  # fmt: skip
+            self.fy = np.ascontiguousarray(edge_field(
+                self.values.T, solid.T, near.T, mesh.distance[2].T, mesh.distance[3].T, mesh.h,
+                extrapolation[2:4]).T)  # fmt: skip
+
+    namespace = {"np": np, "IonOpticsMesh": mesh_module.IonOpticsMesh, "Any": Any,
+                 "StaggeredElectricField": StaggeredElectricField, "dataclass": dataclass,
+                 "Sequence": Sequence}  # fmt: skip
+    reference_definitions(root, "refinement", (
+        "Refinement", "Patch", "_on_plane", "_part", "patches_of", "_extrapolation_of",
+        "_bilinear", "PatchedElectricField"), namespace)  # fmt: skip
+    for name, settings in mesh_cases().items():
+        settings = dict(settings)
+        electrodes = [mesh_module.Electrode(f, v) for f, v in settings.pop("electrodes")]
+        faces = {k: mesh_module.FaceCondition(*v) for k, v in settings.pop("faces").items()}
+        mesh = mesh_module.IonOpticsMesh(electrodes=electrodes, faces=faces, **settings)
+        boxes = [namespace["Refinement"](*b) for b in refinement_cases()[name]]
+        patches = namespace["patches_of"](mesh, boxes)
+        values, start = [], 0
+        for patch in patches:
+            xn, yn = patch.mesh.nodes()
+            patch.index = start + np.arange(xn.size).reshape(xn.shape)
+            start += xn.size
+            values.append(refinement_potential(xn, yn).ravel())
+        layout = types.SimpleNamespace(patches=patches, base=patches[0])
+        field = namespace["PatchedElectricField"](layout, np.concatenate(values))
+        out = {}
+        for q, (patch, f) in enumerate(zip(patches, field.fields)):
+            fm = patch.field_mesh if patch.field_mesh is not None else patch.mesh
+            out[f"p{q}_level"] = np.array(patch.level)
+            out[f"p{q}_box"] = np.array(patch.box, dtype=np.int64)
+            out[f"p{q}_shape"] = np.array(patch.mesh.shape)
+            out[f"p{q}_origin"] = np.array(patch.mesh.origin)
+            out[f"p{q}_x"] = np.asarray(patch.mesh.x, dtype=float)
+            out[f"p{q}_field_shape"] = np.array(fm.shape)
+            out[f"p{q}_field_origin"] = np.array(fm.origin)
+            out[f"p{q}_inner"] = np.array([[s.start or 0, s.stop if s.stop is not None else -1]
+                                           for s in patch.inner])  # fmt: skip
+            out[f"p{q}_values"] = f.values
+            out[f"p{q}_fx"] = f.fx
+            out[f"p{q}_fy"] = f.fy
+        out["patches"] = np.array(len(patches))
+        np.savez_compressed(HERE / f"refinement_{name}.npz", **out)
+        print("refinement", name, [p.box for p in patches])
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument(
         "--reference", default=os.environ.get("BEAMTRACER_REFERENCE"),
         help="the reference checkout (default: $BEAMTRACER_REFERENCE)",
     )  # fmt: skip
-    parser.add_argument("--only", choices=["trace3d"], default=None,
-                        help="generate only the 3D fixtures (tracer, mesh, edge fields)")
+    parser.add_argument("--only", choices=["trace3d", "refinement"], default=None,
+                        help="generate only the 3D fixtures (tracer, mesh, edge fields) or "
+                             "the refined patches' fixtures")
     args = parser.parse_args()
     given = args.reference
     if not given:
@@ -345,10 +413,14 @@ def main() -> None:
     root = Path(given)
     if not (root / "src" / "beamtracer").is_dir():
         parser.error(f"{root} holds no src/beamtracer package")
+    if args.only == "refinement":
+        refinement_goldens(root)
+        return
     trace3d_goldens(root)
     mesh3d_goldens(root)
     if args.only == "trace3d":
         return
+    refinement_goldens(root)
     host_goldens(root)
     record_goldens(root)
     ref = reference_kernels(root)

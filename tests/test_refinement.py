@@ -199,3 +199,47 @@ def test_the_oracle_newton_and_held_region_solve_their_equations() -> None:
             direct, _ = oracle_poisson.solve_newton(op, layout.on_base(rho), 1e-3 / eps0, 5.0,
                                                     5.0, -1, tol=1e-11)  # fmt: skip
             np.testing.assert_allclose(layout.on_base(phi), direct, rtol=0, atol=1e-9)
+
+
+REFINED = ("planar_plates", "cylindrical_lens", "graded_disc")
+
+
+@pytest.mark.parametrize("name", REFINED)
+def test_patches_and_their_fields_match_the_reference(name) -> None:
+    """The refined patches and the potential and edge fields of every patch's field mesh
+    against the reference's own ``patches_of`` and ``PatchedElectricField`` run on the same
+    meshes, boxes and potential (``tests/golden/refinement_*.npz``, made by
+    ``tests/golden/make_golden.py``): the boxes and shapes exactly, the positions and the
+    fields to rounding."""
+    from tests.golden.cases import refinement_cases, refinement_potential
+    from tests.gpu_util import GOLDEN
+    from tests.test_mesh import build_mesh
+
+    golden = np.load(GOLDEN / f"refinement_{name}.npz")
+    mesh = build_mesh(name)
+    mesh = IonOpticsMesh(shape=mesh.shape, origin=mesh.origin, h=mesh.h, geometry=mesh.geometry,
+                         electrodes=mesh.electrodes, faces=dict(mesh.faces),
+                         x_nodes=mesh.x_nodes, classify_on_device=False)  # fmt: skip
+    boxes = [Refinement(*b) for b in refinement_cases()[name]]
+    layout = layout_of_mesh(mesh, boxes)
+    assert len(layout.patches) == int(golden["patches"])
+    phi = refinement_potential(layout.x, layout.y)
+    values = composite.field_values(layout, phi)
+    fields, _ = composite.edge_fields(layout, phi)
+    for q, patch in enumerate(layout.patches):
+        fm = patch.field_mesh if patch.field_mesh is not None else patch.mesh
+        assert patch.level == int(golden[f"p{q}_level"])
+        np.testing.assert_array_equal(np.array(patch.box), golden[f"p{q}_box"])
+        assert tuple(patch.mesh.shape) == tuple(golden[f"p{q}_shape"])
+        assert tuple(fm.shape) == tuple(golden[f"p{q}_field_shape"])
+        np.testing.assert_allclose(patch.mesh.origin, golden[f"p{q}_origin"], rtol=0, atol=1e-15)
+        np.testing.assert_allclose(fm.origin, golden[f"p{q}_field_origin"], rtol=0, atol=1e-15)
+        np.testing.assert_allclose(patch.mesh.x, golden[f"p{q}_x"], rtol=0, atol=1e-15)
+        inner = [[s.start or 0, s.stop if s.stop is not None else -1] for s in patch.inner]
+        np.testing.assert_array_equal(np.array(inner), golden[f"p{q}_inner"])
+        scale = np.abs(golden[f"p{q}_values"]).max()
+        np.testing.assert_allclose(values[q], golden[f"p{q}_values"], rtol=0, atol=1e-12 * scale)
+        fx, fy = fields[q]
+        fscale = max(np.abs(golden[f"p{q}_fx"]).max(), np.abs(golden[f"p{q}_fy"]).max())
+        np.testing.assert_allclose(fx, golden[f"p{q}_fx"], rtol=0, atol=1e-10 * fscale)
+        np.testing.assert_allclose(fy, golden[f"p{q}_fy"], rtol=0, atol=1e-10 * fscale)
