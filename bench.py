@@ -489,16 +489,31 @@ def sweep_with_gradients(designs, stream, concurrency: int = 8) -> dict:
 
     grads, batched_ms = timed(batched)
     plain, plain_ms = timed(lambda: [adjoint_design_gradient(d) for d in designs])
-    worst = 0.0
-    for mine, alone in zip(grads, plain):
+    worst, worst_k, diffs = 0.0, -1, []
+    for k, (mine, alone) in enumerate(zip(grads, plain)):
+        diff = 0.0
         for name in ("rms_angle", "current"):
             scale = float(np.abs(alone[name]).max())
             if scale > 0.0:
-                worst = max(worst, float(np.abs(mine[name] - alone[name]).max()) / scale)
+                diff = max(diff, float(np.abs(mine[name] - alone[name]).max()) / scale)
+        diffs.append(diff)
+        if diff > worst:
+            worst, worst_k = diff, k
     n = len(designs)
+    worst_case = None
+    if worst_k >= 0:
+        d = designs[worst_k]
+        worst_case = {"candidate": worst_k, "mesh": list(d.shape), "trajectories": d.trajectories,
+                      "converged_batched": bool(grads[worst_k]["converged"]),
+                      "converged_plain": bool(plain[worst_k]["converged"]),
+                      "adjoint_iterations": [grads[worst_k]["adjoint_iterations"],
+                                             plain[worst_k]["adjoint_iterations"]]}  # fmt: skip
     return {"unit": "candidates/s", "batched": n * 1e3 / batched_ms,
             "plain_form": n * 1e3 / plain_ms, "speedup_over_plain": plain_ms / batched_ms,
-            "max_rel_gradient_diff": worst, "forward_tolerance_v": 1e-6,
+            "max_rel_gradient_diff": worst, "worst_candidate": worst_case,
+            "median_rel_gradient_diff": float(np.median(diffs)) if diffs else 0.0,
+            "candidates_within_1e-4": int(sum(v <= 1e-4 for v in diffs)),
+            "forward_tolerance_v": 1e-6,
             "concurrency": concurrency,
             "note": "batched forward in one BatchedVlasov, then each candidate's adjoint; "
                     "plain: each candidate's own solve and adjoint"}
