@@ -243,3 +243,20 @@ def test_patches_and_their_fields_match_the_reference(name) -> None:
         fscale = max(np.abs(golden[f"p{q}_fx"]).max(), np.abs(golden[f"p{q}_fy"]).max())
         np.testing.assert_allclose(fx, golden[f"p{q}_fx"], rtol=0, atol=1e-10 * fscale)
         np.testing.assert_allclose(fy, golden[f"p{q}_fy"], rtol=0, atol=1e-10 * fscale)
+
+
+@pytest.mark.parametrize("geometry", ["planar", "cylindrical"])
+def test_the_composite_scheme_keeps_the_plates_linear_field(geometry) -> None:
+    """The reference's linear plates (``test_ion_optics.py:67-72``, atol 1e-9) on refined
+    boxes: with no charge the potential between two plates is linear in x, which every
+    patch's rows and the hanging nodes' interpolation reproduce exactly, on and off the axis
+    and on a graded axis."""
+    faces = {"x_min": FaceCondition("dirichlet", 0.0), "x_max": FaceCondition("dirichlet", 100.0)}
+    for x_nodes in (None, graded_nodes(21, 0.0, 20e-3)):
+        mesh = IonOpticsMesh((21, 11), (0.0, 0.0), 1e-3, geometry, faces=faces, x_nodes=x_nodes,
+                             classify_on_device=False)  # fmt: skip
+        layout = layout_of_mesh(mesh, [Refinement(1, (4e-3, 0.0), (14e-3, 6e-3)),
+                                       Refinement(2, (6e-3, 2e-3), (10e-3, 4e-3))])  # fmt: skip
+        assert layout.hanging.size > 0
+        phi = composite.solve(layout)
+        np.testing.assert_allclose(phi, 100.0 * layout.x / 20e-3, rtol=0, atol=1e-9)
