@@ -156,6 +156,13 @@ class IonOpticsPoisson:
             self._layout = layout_of_mesh(self.mesh)
         return self._layout
 
+    @property
+    def coordinates(self) -> np.ndarray:
+        """The positions of the composite nodes, ``(2, nodes)`` [m]: ``(x, y)``, or
+        ``(x, r)`` in cylindrical geometry (``poisson.py:617-625``)."""
+        layout = self.layout
+        return np.ascontiguousarray(np.stack([layout.x, layout.y]))
+
     def fixed_adjoint(self, z, phi_bar, out) -> None:
         """``out`` (device, (nx, ny)) <- the sensitivity to the held nodes' potentials of a
         quantity whose sensitivity to the potential is ``phi_bar``, given
