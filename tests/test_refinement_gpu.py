@@ -69,6 +69,7 @@ def test_the_composite_solve_equals_the_oracle(geometry, boxes) -> None:
     solver = IonOpticsPoisson(mesh, refinement=BOXES[boxes])
     layout = solver.layout
     assert layout.refined and layout.hanging.size > 0
+    np.testing.assert_array_equal(solver.coordinates, np.stack([layout.x, layout.y]))
     rho = 1e-4 * np.exp(-((layout.x - 2e-3) ** 2 + layout.y**2) / (1e-3) ** 2)
     phi = solver.solve(rho)
     ora = oracle_composite.solve(oracle_layout(mesh, BOXES[boxes]), rho)
