@@ -50,12 +50,16 @@ class DeviceCSR:
                     else torch.from_numpy(np.asarray(out_rows, dtype=np.int64)).to(dev))  # fmt: skip
         self.constant = (None if constant is None
                          else torch.from_numpy(np.asarray(constant, dtype=np.float64)).to(dev))  # fmt: skip
-
-    def apply(self, x, y, accumulate: bool = False) -> None:
+        # the map's own arrays live as long as it does: their addresses, once
         d = _lib.dptr
-        _lib.check(_lib.lib().bt_csr_apply(
-            _lib.context().handle, self.rows, d(self.out), d(self.ptr), d(self.col),
-            d(self.val), d(self.constant), int(accumulate), d(x), d(y)))  # fmt: skip
+        self._args = (d(self.out), d(self.ptr), d(self.col), d(self.val), d(self.constant))
+
+    def apply(self, x, y, accumulate: bool = False, handle=None) -> None:
+        """``handle``: the library context to queue on (default: the calling thread's)."""
+        d = _lib.dptr
+        handle = _lib.context().handle if handle is None else handle
+        _lib.check(_lib.lib().bt_csr_apply(handle, self.rows, *self._args, int(accumulate),
+                                           d(x), d(y)))  # fmt: skip
 
 
 def _selection(index: np.ndarray, size: int, value: float = 1.0) -> sparse.csr_matrix:
@@ -183,6 +187,11 @@ class CompositePoisson:
         self._hang = (DeviceCSR(layout.interpolation, out_rows=layout.hanging)
                       if layout.hanging.size else None)  # fmt: skip
         self._plain = _Held(layout, layout.fixed, layout.fixed_value, self.offsets)
+        self._views: dict = {}
+        #: the library context of the solve in progress (the calling thread's)
+        self._h = None
+        #: the sides each correction solver holds now (the object last given to it)
+        self._held_sides: list = [None] * len(patches)
         self._region_key: object = None
         self._region: _Held | None = None
         #: FAC sweeps of the last solve, and their corrections' V-cycles; Newton steps
@@ -191,12 +200,24 @@ class CompositePoisson:
         self.newton_iterations = 0
 
     def _view(self, buffer, number: int):
-        lo, hi = self.offsets[number], self.offsets[number + 1]
-        return buffer[lo:hi].view(self.layout.patches[number].mesh.shape)
+        """Patch ``number``'s part of a buffer over every patch's nodes (made once)."""
+        key = (id(buffer), number)
+        view = self._views.get(key)
+        if view is None:
+            lo, hi = self.offsets[number], self.offsets[number + 1]
+            view = buffer[lo:hi].view(self.layout.patches[number].mesh.shape)
+            self._views[key] = view
+        return view
+
+    def _hold(self, number: int, sides) -> None:
+        """Hold a correction solver's ``sides`` (skipped when they are the ones it holds)."""
+        if self._held_sides[number] is not sides:
+            self.corrections[number].hold(sides)
+            self._held_sides[number] = sides
 
     def fill_hanging(self, phi) -> None:
         if self._hang is not None:
-            self._hang.apply(phi, phi)
+            self._hang.apply(phi, phi, handle=self._h)
 
     def _held(self, region, potential: float) -> _Held:
         if region is None:
@@ -222,11 +243,11 @@ class CompositePoisson:
         lib = _lib.lib()
         for number, solver in enumerate(self.rows):
             phi_p = self._view(self._phi_p, number)
-            self._gather[number].apply(phi, phi_p)
+            self._gather[number].apply(phi, phi_p, handle=self._h)
             _lib.check(lib.bt_poisson_residual(solver._handle, _lib.dptr(phi_p),
                                                _lib.dptr(self._view(self._rho_p, number)),
                                                _lib.dptr(self._view(self._res_p, number))))  # fmt: skip
-        held.owned.apply(self._res_p, r)
+        held.owned.apply(self._res_p, r, handle=self._h)
 
     def _step_residual(self, delta, r, held: _Held) -> None:
         """``r`` <- the residual of a Newton step's correction ``delta``: the step's own
@@ -235,18 +256,18 @@ class CompositePoisson:
         lib = _lib.lib()
         for number, solver in enumerate(self.corrections):
             d_p = self._view(self._phi_p, number)
-            self._gather[number].apply(delta, d_p)
-            solver.hold(held.sides[number])
+            self._gather[number].apply(delta, d_p, handle=self._h)
+            self._hold(number, held.sides[number])
             _lib.check(lib.bt_poisson_residual(solver._handle, _lib.dptr(d_p), None,
                                                _lib.dptr(self._view(self._res_p, number))))  # fmt: skip
-        held.owned.apply(self._res_p, r)
+        held.owned.apply(self._res_p, r, handle=self._h)
         d = _lib.dptr
-        _lib.check(lib.bt_newton_residual(_lib.context().handle, self.layout.size, d(held.own),
+        _lib.check(lib.bt_newton_residual(self._h, self.layout.size, d(held.own),
                                           d(self._r0), d(self._reaction), d(delta), d(r)))  # fmt: skip
 
     def _max(self, a, b=None) -> float:
         n = self.layout.size
-        _lib.check(_lib.lib().bt_max_abs_diff(_lib.context().handle, _lib.dptr(a),
+        _lib.check(_lib.lib().bt_max_abs_diff(self._h, _lib.dptr(a),
                                               _lib.dptr(self._zero if b is None else b), n,
                                               _lib.dptr(self._scalars)))  # fmt: skip
         return float(self._scalars[0])
@@ -254,7 +275,7 @@ class CompositePoisson:
     def _max_pair(self, x, previous) -> tuple[float, float]:
         """max |x - previous| and max |x| in one read."""
         n = self.layout.size
-        ctx = _lib.context().handle
+        ctx = self._h
         d = _lib.dptr
         _lib.check(_lib.lib().bt_max_abs_diff(ctx, d(x), d(previous), n, d(self._scalars)))
         _lib.check(_lib.lib().bt_max_abs_diff(ctx, d(x), d(self._zero), n,
@@ -280,25 +301,25 @@ class CompositePoisson:
                 rhs = self._view(self._rhs_p, number)
                 e = self._view(self._e_p, number)
                 if self.local == "vcycle":
-                    self._gather[number].apply(self._r, rhs)
-                    solver.hold(held.sides[number])
+                    self._gather[number].apply(self._r, rhs, handle=self._h)
+                    self._hold(number, held.sides[number])
                     reaction = None
                     if newton:
                         reaction = self._view(self._reaction_p, number)
-                        self._gather[number].apply(self._reaction, reaction)
+                        self._gather[number].apply(self._reaction, reaction, handle=self._h)
                     _lib.check(lib.bt_poisson_vcycle(solver._handle, _lib.dptr(rhs),
                                                      _lib.dptr(reaction),
                                                      int(newton and sweep == 1),
                                                      _lib.dptr(e)))  # fmt: skip
                     cycles += 1
-                    held.prolong[number].apply(e.reshape(-1), x, accumulate=True)
+                    held.prolong[number].apply(e.reshape(-1), x, True, self._h)
                     continue
-                self._gather_eps[number].apply(self._r, rhs)
+                self._gather_eps[number].apply(self._r, rhs, handle=self._h)
                 e.zero_()
                 if newton:
-                    solver.hold(held.sides[number])
+                    self._hold(number, held.sides[number])
                     reaction = self._view(self._reaction_p, number)
-                    self._gather[number].apply(self._reaction, reaction)
+                    self._gather[number].apply(self._reaction, reaction, handle=self._h)
                     taken = _lib.I32()
                     _lib.check(lib.bt_poisson_solve_reaction(
                         solver._handle, _lib.dptr(e), _lib.dptr(rhs), _lib.dptr(reaction),
@@ -308,7 +329,7 @@ class CompositePoisson:
                     solver.solve_device(e, rhs, fixed_region=held.sides[number],
                                         linear_tolerance=self.correction_tolerance)
                     cycles += solver.krylov_steps
-                held.prolong[number].apply(e.reshape(-1), x, accumulate=True)
+                held.prolong[number].apply(e.reshape(-1), x, True, self._h)
             self.fill_hanging(x)
             change, largest = self._max_pair(x, self._prev)
             scale = max(largest, floor, 1e-300)
@@ -326,13 +347,15 @@ class CompositePoisson:
         n = self.layout.size
         if tuple(phi.shape) != (n,) or (rho is not None and tuple(rho.shape) != (n,)):
             raise ValueError(f"the composite solve takes ({n},) composite vectors")
+        self._h = _lib.context().handle
         held = self._held(fixed_region, fixed_potential)
         if rho is None:
             self._rho_p.zero_()
         else:
             for number in range(len(self.rows)):
-                self._gather[number].apply(rho, self._view(self._rho_p, number))
-        held.setter.apply(phi, phi)
+                self._gather[number].apply(rho, self._view(self._rho_p, number),
+                                           handle=self._h)
+        held.setter.apply(phi, phi, handle=self._h)
         self.fill_hanging(phi)
         self.newton_iterations = 0
         if plasma is None:
@@ -344,7 +367,7 @@ class CompositePoisson:
         d = _lib.dptr
         for step in range(1, int(max_newton) + 1):
             self.residual(phi, self._r0, held)
-            _lib.check(lib.bt_boltzmann_terms(_lib.context().handle, n, d(held.own), d(phi),
+            _lib.check(lib.bt_boltzmann_terms(self._h, n, d(held.own), d(phi),
                                               float(amplitude), float(temperature), float(up),
                                               int(sign), d(self._r0), d(self._reaction)))  # fmt: skip
             self._delta.zero_()
