@@ -10,9 +10,11 @@ patch holding it (``solver/refinement.py:299-387``, ``tracer.py:1141-1183``).  H
 - the composite solve is a fast adaptive composite (FAC) iteration: per sweep, coarse to
   fine, the composite residual is taken on a patch's nodes, the patch's homogeneous
   problem (its held nodes and, for a box, its sides inside the domain at zero) is solved
-  by its multigrid, and the correction is added to the composite nodes in the patch's box
-  (bilinear between the patch's nodes at the finer nodes); sweeps stop when the largest
-  change falls below 1e-12 of the potential's scale;
+  inexactly by one V-cycle of its multigrid, and the correction is added to the composite
+  nodes in the patch's box (bilinear between the patch's nodes at the finer nodes); sweeps
+  stop when the largest change falls below 1e-12 of the potential's scale; with a
+  Boltzmann species every Newton step's correction is found by the same sweeps, each
+  patch's multigrid rebuilt with the step's reaction;
 - the maps between composite nodes and patch arrays are row-compressed matrices applied
   by one kernel (``bt_csr_apply``) in a fixed order: the patches' potentials and the wider
   meshes of their fields (the margin bilinear from the coarser patches, finest wins, as
