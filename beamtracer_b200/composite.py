@@ -190,6 +190,10 @@ class CompositePoisson:
                       if layout.hanging.size else None)  # fmt: skip
         self._plain = _Held(layout, layout.fixed, layout.fixed_value, self.offsets)
         self._views: dict = {}
+        #: per patch, the patches whose rows its correction reads: it and the finer ones
+        #: (every patch for the base)
+        self._finer = [[p for p in range(len(patches)) if patches[p].level >= patches[q].level]
+                       for q in range(len(patches))]  # fmt: skip
         #: the library context of the solve in progress (the calling thread's)
         self._h = None
         #: the sides each correction solver holds now (the object last given to it)
@@ -237,13 +241,16 @@ class CompositePoisson:
             self._region_key = key
         return self._region
 
-    def residual(self, phi, r, held: _Held | None = None) -> None:
+    def residual(self, phi, r, held: _Held | None = None, patches=None) -> None:
         """``r`` <- the composite residual of ``phi`` (zero on held and hanging nodes), with
-        the charge density last given to `solve_device`."""
+        the charge density last given to `solve_device`.  ``patches``: only these patches'
+        rows are evaluated again (the others keep their last values): a patch's correction
+        reads the residual at its inside nodes alone, which it and the finer patches own."""
         held = held or self._plain
         self.fill_hanging(phi)
         lib = _lib.lib()
-        for number, solver in enumerate(self.rows):
+        for number in range(len(self.rows)) if patches is None else patches:
+            solver = self.rows[number]
             phi_p = self._view(self._phi_p, number)
             self._gather[number].apply(phi, phi_p, handle=self._h)
             _lib.check(lib.bt_poisson_residual(solver._handle, _lib.dptr(phi_p),
@@ -251,12 +258,14 @@ class CompositePoisson:
                                                _lib.dptr(self._view(self._res_p, number))))  # fmt: skip
         held.owned.apply(self._res_p, r, handle=self._h)
 
-    def _step_residual(self, delta, r, held: _Held) -> None:
+    def _step_residual(self, delta, r, held: _Held, patches=None) -> None:
         """``r`` <- the residual of a Newton step's correction ``delta``: the step's own
-        residual less (K + diag(reaction)) delta, at the nodes with an equation."""
+        residual less (K + diag(reaction)) delta, at the nodes with an equation
+        (``patches`` as in `residual`)."""
         self.fill_hanging(delta)
         lib = _lib.lib()
-        for number, solver in enumerate(self.corrections):
+        for number in range(len(self.corrections)) if patches is None else patches:
+            solver = self.corrections[number]
             d_p = self._view(self._phi_p, number)
             self._gather[number].apply(delta, d_p, handle=self._h)
             self._hold(number, held.sides[number])
@@ -296,10 +305,11 @@ class CompositePoisson:
         for sweep in range(1, self.max_sweeps + 1):
             self._prev.copy_(x)
             for number, solver in enumerate(self.corrections):
+                rows = self._finer[number]
                 if newton:
-                    self._step_residual(x, self._r, held)
+                    self._step_residual(x, self._r, held, rows)
                 else:
-                    self.residual(x, self._r, held)
+                    self.residual(x, self._r, held, rows)
                 rhs = self._view(self._rhs_p, number)
                 e = self._view(self._e_p, number)
                 if self.local == "vcycle":
