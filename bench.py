@@ -18,7 +18,7 @@ converged solve from a zero charge density.
   host core, and SciPy's sparse LU for the field) on one converged solve of the same lens,
   its problem built on the host alone;
 - ``parity``: the device solve's potential and plane moments against that oracle solve's
-  (relative differences; north-star bound 1e-6).
+  (relative differences; the bound is 1e-6 of the moments).
 
 ``--impl reference`` times that CPU path alone (the reference's Pyccel build cannot be
 made here) and prints its moments.  Under torchrun every rank solves its own lens (weak
