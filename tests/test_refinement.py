@@ -260,3 +260,41 @@ def test_the_composite_scheme_keeps_the_plates_linear_field(geometry) -> None:
         assert layout.hanging.size > 0
         phi = composite.solve(layout)
         np.testing.assert_allclose(phi, 100.0 * layout.x / 20e-3, rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_nested_boxes_keep_the_layout_invariants(seed) -> None:
+    """Seeded nested boxes of levels 1-3, touching faces or not: the volumes fill the
+    domain, every patch node is a composite node, the hanging nodes read only nodes that do
+    not hang and interpolate planes exactly, and the composite scheme keeps the plates'
+    linear field."""
+    rng = np.random.default_rng(seed)
+    geometry = ("planar", "cylindrical")[seed % 2]
+    faces = {"x_min": FaceCondition("dirichlet", 0.0), "x_max": FaceCondition("dirichlet", 10.0)}
+    mesh = IonOpticsMesh((17, 9), (0.0, 0.0), 1e-3, geometry, faces=faces,
+                         classify_on_device=False)  # fmt: skip
+    boxes, lower, upper = [], np.array([0.0, 0.0]), np.array([16e-3, 8e-3])
+    for level in (1, 2, 3):
+        span = upper - lower
+        lo = lower + rng.uniform(0.0, 0.3, 2) * span * rng.integers(0, 2, 2)
+        hi = upper - rng.uniform(0.0, 0.3, 2) * span * rng.integers(0, 2, 2)
+        boxes.append(Refinement(level, tuple(lo), tuple(hi)))
+        # the next level inside this one's snapped extent
+        patch = patches_of(mesh, boxes)[-1]
+        x0, y0, x1, y1 = patch.bounds
+        lower, upper = np.array([x0, y0]), np.array([x1, y1])
+    layout = layout_of_mesh(mesh, boxes)
+    total = 16e-3 * 8e-3 if geometry == "planar" else np.pi * 8e-3**2 * 16e-3
+    assert layout.volumes.sum() == pytest.approx(total, rel=1e-12)
+    assert np.all(layout.volumes > 0.0)
+    for patch in layout.patches:
+        np.testing.assert_allclose(layout.x[patch.index], patch.mesh.nodes()[0], atol=1e-15)
+        np.testing.assert_allclose(layout.y[patch.index], patch.mesh.nodes()[1], atol=1e-15)
+    assert not set(layout.interpolation.indices.tolist()) & set(layout.hanging.tolist())
+    plane = 2.0 * layout.x + 5.0 * layout.y
+    filled = plane.copy()
+    filled[layout.hanging] = 0.0
+    layout.fill_hanging(filled)
+    np.testing.assert_allclose(filled, plane, rtol=0, atol=1e-15)
+    phi = composite.solve(layout)
+    np.testing.assert_allclose(phi, 10.0 * layout.x / 16e-3, rtol=0, atol=1e-9)
