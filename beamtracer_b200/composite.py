@@ -28,7 +28,6 @@ import ctypes
 
 import numpy as np
 from scipy import sparse
-from scipy.constants import epsilon_0
 
 from beamtracer_b200 import _lib
 from beamtracer_b200.refinement import Layout, _inside
@@ -140,26 +139,21 @@ class CompositePoisson:
     patch's solver, until its largest update is below ``newton_tolerance``.
     """
 
-    def __init__(self, layout: Layout, *, tolerance: float = 1e-12, max_sweeps: int = 200,
-                 correction_tolerance: float = 1e-6, newton_sweep_tolerance: float = 1e-10,
-                 local: str = "vcycle") -> None:  # fmt: skip
+    def __init__(self, layout: Layout, *, tolerance: float = 1e-13, restart: int = 30,
+                 max_restarts: int = 20, newton_sweep_tolerance: float = 1e-10) -> None:  # fmt: skip
         import torch
 
         from beamtracer_b200.poisson import IonOpticsPoisson
 
         self.layout = layout
+        #: the linear solves' relative residual (of the first residual)
         self.tolerance = float(tolerance)
-        self.max_sweeps = int(max_sweeps)
-        self.correction_tolerance = float(correction_tolerance)
-        #: the sweeps' tolerance for a Newton step's correction (an inexact Newton step:
-        #: the steps continue until their own update is below Newton's tolerance)
+        #: GMRES's restart length and restarts
+        self.restart = int(restart)
+        self.max_restarts = int(max_restarts)
+        #: a Newton step's relative residual (an inexact Newton step: the steps continue
+        #: until their own update is below Newton's tolerance)
         self.newton_sweep_tolerance = float(newton_sweep_tolerance)
-        if local not in ("vcycle", "solve"):
-            raise ValueError(f"local must be 'vcycle' or 'solve', got {local!r}")
-        #: a patch's correction per sweep: one multigrid V-cycle of its operator
-        #: (``bt_poisson_vcycle``, no host round trip) or a GMRES solve to
-        #: ``correction_tolerance``
-        self.local = local
         patches = layout.patches
         n = layout.size
         #: every patch's own operator (its rows: the equations of the nodes it owns)
@@ -181,11 +175,13 @@ class CompositePoisson:
         self._r0 = torch.zeros(n, dtype=f64, device=dev)
         self._reaction = torch.zeros(n, dtype=f64, device=dev)
         self._delta = torch.zeros(n, dtype=f64, device=dev)
-        self._prev = torch.zeros(n, dtype=f64, device=dev)
+        self._w = torch.zeros(n, dtype=f64, device=dev)
+        #: the Krylov basis and its preconditioned images
+        self._basis = torch.zeros((self.restart + 1, n), dtype=f64, device=dev)
+        self._images = torch.zeros((self.restart, n), dtype=f64, device=dev)
         self._zero = torch.zeros(max(n, 1), dtype=f64, device=dev)
         self._scalars = torch.zeros(2, dtype=f64, device=dev)
         self._gather = [DeviceCSR(_selection(p.index, n)) for p in patches]
-        self._gather_eps = [DeviceCSR(_selection(p.index, n, epsilon_0)) for p in patches]
         self._hang = (DeviceCSR(layout.interpolation, out_rows=layout.hanging)
                       if layout.hanging.size else None)  # fmt: skip
         self._plain = _Held(layout, layout.fixed, layout.fixed_value, self.offsets)
@@ -283,75 +279,113 @@ class CompositePoisson:
                                               _lib.dptr(self._scalars)))  # fmt: skip
         return float(self._scalars[0])
 
-    def _max_pair(self, x, previous) -> tuple[float, float]:
-        """max |x - previous| and max |x| in one read."""
-        n = self.layout.size
-        ctx = self._h
-        d = _lib.dptr
-        _lib.check(_lib.lib().bt_max_abs_diff(ctx, d(x), d(previous), n, d(self._scalars)))
-        _lib.check(_lib.lib().bt_max_abs_diff(ctx, d(x), d(self._zero), n,
-                                              d(self._scalars) + 8))  # fmt: skip
-        change, largest = self._scalars.cpu().tolist()
-        return change, largest
-
-    def _sweeps(self, x, held: _Held, newton: bool, floor: float = 0.0) -> int:
-        """FAC sweeps on ``x`` until the largest change is below the tolerance (the linear
-        one, or a Newton step's) of the larger of max |x| and ``floor``; returns the
-        corrections' V-cycles.  Each correction is solved to ``correction_tolerance`` of its
-        right-hand side: the sweeps themselves converge the composite system."""
-        tolerance = self.newton_sweep_tolerance if newton else self.tolerance
+    def _sweep(self, x, held: _Held, reaction: bool, rebuild: bool) -> None:
+        """One FAC sweep on ``x`` for ``J x = r0`` (J the composite operator, plus the
+        reaction when ``reaction``): coarse to fine, the residual at each patch's nodes,
+        one V-cycle of its homogeneous problem, the correction spread over its box."""
         lib = _lib.lib()
-        cycles = 0
-        for sweep in range(1, self.max_sweeps + 1):
-            self._prev.copy_(x)
-            for number, solver in enumerate(self.corrections):
-                rows = self._finer[number]
-                if newton:
-                    self._step_residual(x, self._r, held, rows)
-                else:
-                    self.residual(x, self._r, held, rows)
-                rhs = self._view(self._rhs_p, number)
-                e = self._view(self._e_p, number)
-                if self.local == "vcycle":
-                    self._gather[number].apply(self._r, rhs, handle=self._h)
-                    self._hold(number, held.sides[number])
-                    reaction = None
-                    if newton:
-                        reaction = self._view(self._reaction_p, number)
-                        self._gather[number].apply(self._reaction, reaction, handle=self._h)
-                    _lib.check(lib.bt_poisson_vcycle(solver._handle, _lib.dptr(rhs),
-                                                     _lib.dptr(reaction),
-                                                     int(newton and sweep == 1),
-                                                     _lib.dptr(e)))  # fmt: skip
-                    cycles += 1
-                    held.prolong[number].apply(e.reshape(-1), x, True, self._h)
-                    continue
-                self._gather_eps[number].apply(self._r, rhs, handle=self._h)
-                e.zero_()
-                if newton:
-                    self._hold(number, held.sides[number])
-                    reaction = self._view(self._reaction_p, number)
-                    self._gather[number].apply(self._reaction, reaction, handle=self._h)
-                    taken = _lib.I32()
-                    _lib.check(lib.bt_poisson_solve_reaction(
-                        solver._handle, _lib.dptr(e), _lib.dptr(rhs), _lib.dptr(reaction),
-                        self.correction_tolerance, ctypes.byref(taken)))  # fmt: skip
-                    cycles += taken.value
-                else:
-                    solver.solve_device(e, rhs, fixed_region=held.sides[number],
-                                        linear_tolerance=self.correction_tolerance)
-                    cycles += solver.krylov_steps
-                held.prolong[number].apply(e.reshape(-1), x, True, self._h)
+        for number, solver in enumerate(self.corrections):
+            self._step_residual(x, self._r, held, self._finer[number])
+            rhs = self._view(self._rhs_p, number)
+            e = self._view(self._e_p, number)
+            self._gather[number].apply(self._r, rhs, handle=self._h)
+            self._hold(number, held.sides[number])
+            react = None
+            if reaction:
+                react = self._view(self._reaction_p, number)
+                self._gather[number].apply(self._reaction, react, handle=self._h)
+            _lib.check(lib.bt_poisson_vcycle(solver._handle, _lib.dptr(rhs), _lib.dptr(react),
+                                             int(rebuild), _lib.dptr(e)))  # fmt: skip
+            held.prolong[number].apply(e.reshape(-1), x, True, self._h)
+        self.fill_hanging(x)
+
+    def _krylov(self, x, held: _Held, reaction: bool, tolerance: float, floor: float) -> int:
+        """``x`` (zero on entry) <- the solution of ``J x = r0`` (``self._r0`` on the nodes
+        with an equation) by restarted GMRES, right-preconditioned by one FAC sweep from
+        zero: the sweeps alone diverge on some nestings of three levels, the Krylov method
+        converges whenever the preconditioned operator is regular.  Stops at a residual of
+        ``tolerance`` of the first (at least ``floor``), or where it stalls within 1e4 of
+        that (its rounding floor); returns the sweeps taken."""
+        import torch
+
+        n = self.layout.size
+        m = self.restart
+        basis = self._basis
+        images = self._images
+        r0 = self._r0
+        goal = None
+        sweeps = 0
+        rebuild = reaction
+        rhs = r0.clone()
+        for _cycle in range(self.max_restarts):
+            # r = rhs - J x
+            self._r0.copy_(rhs)
+            self._step_residual(x, self._w, held)
+            beta = float(torch.linalg.vector_norm(self._w))
+            if goal is None:
+                goal = max(tolerance * beta, floor)
+                if not goal > 0.0:
+                    goal = 1e-300
+            if not np.isfinite(beta):
+                raise RuntimeError("the composite field solve diverged (a non-finite residual)")
+            if beta <= goal:
+                break
+            basis[0].copy_(self._w / beta)
+            hess = np.zeros((m + 1, m))
+            g = np.zeros(m + 1)
+            g[0] = beta
+            rot = []
+            k = 0
+            for j in range(m):
+                # z_j = M v_j: one sweep from zero on the right-hand side v_j
+                self._r0.copy_(basis[j])
+                images[j].zero_()
+                self._sweep(images[j], held, reaction, rebuild)
+                rebuild = False
+                sweeps += 1
+                # w = J z_j (the residual of z_j against a zero right-hand side, negated)
+                self._r0.zero_()
+                self._step_residual(images[j], self._w, held)
+                self._w.neg_()
+                # classical Gram-Schmidt, twice
+                h = torch.mv(basis[: j + 1], self._w)
+                self._w.sub_(torch.mv(basis[: j + 1].T, h))
+                h2 = torch.mv(basis[: j + 1], self._w)
+                self._w.sub_(torch.mv(basis[: j + 1].T, h2))
+                col = (h + h2).cpu().numpy()
+                norm = float(torch.linalg.vector_norm(self._w))
+                hess[: j + 1, j] = col
+                hess[j + 1, j] = norm
+                for i, (c, sn) in enumerate(rot):
+                    a, b = hess[i, j], hess[i + 1, j]
+                    hess[i, j], hess[i + 1, j] = c * a + sn * b, -sn * a + c * b
+                a, b = hess[j, j], hess[j + 1, j]
+                radius = float(np.hypot(a, b))
+                c, sn = (a / radius, b / radius) if radius > 0.0 else (1.0, 0.0)
+                rot.append((c, sn))
+                hess[j, j], hess[j + 1, j] = radius, 0.0
+                g[j], g[j + 1] = c * g[j], -sn * g[j]
+                k = j + 1
+                if abs(g[j + 1]) <= goal or norm == 0.0:
+                    break
+                basis[j + 1].copy_(self._w / norm)
+            y = np.linalg.solve(np.triu(hess[:k, :k]), g[:k]) if k else np.zeros(0)
+            update = torch.from_numpy(y).to(images.device)
+            x.add_(torch.mv(images[:k].T, update))
             self.fill_hanging(x)
-            change, largest = self._max_pair(x, self._prev)
-            scale = max(largest, floor, 1e-300)
-            if not np.isfinite(change):
-                raise RuntimeError("the composite field solve diverged (a non-finite update)")
-            if change <= tolerance * scale:
-                self.sweeps = sweep
-                return cycles
-        raise RuntimeError(f"the composite field solve did not converge in {self.max_sweeps} "
-                           "sweeps")  # fmt: skip
+            if abs(g[k]) <= goal:
+                continue  # confirmed by the true residual at the top of the next cycle
+            if abs(g[k]) > 0.5 * beta and abs(g[k]) <= 1e4 * goal:
+                break  # stalled at the rounding floor
+        else:
+            self._r0.copy_(rhs)
+            self._step_residual(x, self._w, held)
+            left = float(torch.linalg.vector_norm(self._w))
+            if not left <= 1e4 * goal:
+                raise RuntimeError("the composite field solve did not converge")
+        self._r0.copy_(rhs)
+        self.sweeps = sweeps
+        return sweeps
 
     def solve_device(self, phi, rho=None, *, fixed_region=None, fixed_potential: float = 0.0,
                      plasma: tuple[float, float, float, int] | None = None,
@@ -370,8 +404,22 @@ class CompositePoisson:
         held.setter.apply(phi, phi, handle=self._h)
         self.fill_hanging(phi)
         self.newton_iterations = 0
+        # the scale of the right-hand side: the residual of the held values alone, whose
+        # 1e-13 is the rounding floor the solves stop at
+        import torch
+
+        self._w.zero_()
+        held.setter.apply(self._w, self._w, handle=self._h)
+        self.residual(self._w, self._r, held)
+        floor = 1e-13 * float(torch.linalg.vector_norm(self._r))
         if plasma is None:
-            self.krylov_steps = self._sweeps(phi, held, newton=False, floor=1.0)
+            # phi += J^-1 (b - K phi), J = K on the nodes with an equation
+            self.residual(phi, self._r0, held)
+            self._reaction.zero_()
+            self._delta.zero_()
+            self.krylov_steps = self._krylov(self._delta, held, False, self.tolerance, floor)
+            phi.add_(self._delta)
+            self.fill_hanging(phi)
             return
         amplitude, temperature, up, sign = plasma
         lib = _lib.lib()
@@ -383,8 +431,7 @@ class CompositePoisson:
                                               float(amplitude), float(temperature), float(up),
                                               int(sign), d(self._r0), d(self._reaction)))  # fmt: skip
             self._delta.zero_()
-            cycles += self._sweeps(self._delta, held, newton=True,
-                                   floor=1e-3 * float(newton_tolerance))
+            cycles += self._krylov(self._delta, held, True, self.newton_sweep_tolerance, floor)
             phi.add_(self._delta)
             self.fill_hanging(phi)
             update = self._max(self._delta)

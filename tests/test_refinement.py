@@ -262,17 +262,15 @@ def test_the_composite_scheme_keeps_the_plates_linear_field(geometry) -> None:
         np.testing.assert_allclose(phi, 100.0 * layout.x / 20e-3, rtol=0, atol=1e-9)
 
 
-@pytest.mark.parametrize("seed", range(6))
-def test_random_nested_boxes_keep_the_layout_invariants(seed) -> None:
-    """Seeded nested boxes of levels 1-3, touching faces or not: the volumes fill the
-    domain, every patch node is a composite node, the hanging nodes read only nodes that do
-    not hang and interpolate planes exactly, and the composite scheme keeps the plates'
-    linear field."""
+def random_boxes(seed: int, classify_on_device: bool | None = False):
+    """A 17 x 9 mesh (planar for even seeds, cylindrical for odd ones, Dirichlet x faces
+    at 0 and 10 V) and seeded nested boxes of levels 1-3, each side inset or on the face
+    of the box (or mesh) below."""
     rng = np.random.default_rng(seed)
     geometry = ("planar", "cylindrical")[seed % 2]
     faces = {"x_min": FaceCondition("dirichlet", 0.0), "x_max": FaceCondition("dirichlet", 10.0)}
     mesh = IonOpticsMesh((17, 9), (0.0, 0.0), 1e-3, geometry, faces=faces,
-                         classify_on_device=False)  # fmt: skip
+                         classify_on_device=classify_on_device)  # fmt: skip
     boxes, lower, upper = [], np.array([0.0, 0.0]), np.array([16e-3, 8e-3])
     for level in (1, 2, 3):
         span = upper - lower
@@ -283,6 +281,17 @@ def test_random_nested_boxes_keep_the_layout_invariants(seed) -> None:
         patch = patches_of(mesh, boxes)[-1]
         x0, y0, x1, y1 = patch.bounds
         lower, upper = np.array([x0, y0]), np.array([x1, y1])
+    return mesh, boxes
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_nested_boxes_keep_the_layout_invariants(seed) -> None:
+    """Seeded nested boxes of levels 1-3, touching faces or not: the volumes fill the
+    domain, every patch node is a composite node, the hanging nodes read only nodes that do
+    not hang and interpolate planes exactly, and the composite scheme keeps the plates'
+    linear field."""
+    mesh, boxes = random_boxes(seed)
+    geometry = mesh.geometry
     layout = layout_of_mesh(mesh, boxes)
     total = 16e-3 * 8e-3 if geometry == "planar" else np.pi * 8e-3**2 * 16e-3
     assert layout.volumes.sum() == pytest.approx(total, rel=1e-12)

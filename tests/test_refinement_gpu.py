@@ -352,3 +352,19 @@ def test_a_refined_box_brings_the_beam_to_that_of_the_fine_mesh() -> None:
     box = coarse.replace(refinement=[RefinementParams(1, (0.0, 0.0), (4.5e-3, 2.0e-3))])
     reference = divergence(fine)
     assert abs(divergence(box) - reference) < 0.5 * abs(divergence(coarse) - reference)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_nested_boxes_solve_as_the_oracle(seed) -> None:
+    """Seeded nested boxes of levels 1-3 (on and off the faces and the axis): the device's
+    composite solve of a charge against the oracle's LU."""
+    from beamtracer_b200.poisson import IonOpticsPoisson
+    from tests.test_refinement import random_boxes
+
+    mesh, boxes = random_boxes(seed, classify_on_device=None)
+    solver = IonOpticsPoisson(mesh, refinement=boxes)
+    layout = solver.layout
+    rho = 1e-7 * np.exp(-((layout.x - 8e-3) ** 2 + (layout.y - 3e-3) ** 2) / (3e-3) ** 2)
+    phi = solver.solve(rho)
+    ora = oracle_composite.solve(oracle_layout(mesh, boxes), rho)
+    assert np.abs(phi - ora).max() <= 1e-9 * np.ptp(ora)
