@@ -7,14 +7,14 @@ patch holding it (``solver/refinement.py:299-387``, ``tracer.py:1141-1183``).  H
 - every patch keeps its own device field solver (`IonOpticsPoisson` of its mesh): its rows
   are the equations of the composite nodes it owns (`beamtracer_b200.refinement`), and its
   multigrid solves the corrections;
-- the composite solve is a fast adaptive composite (FAC) iteration: per sweep, coarse to
-  fine, the composite residual is taken on a patch's nodes, the patch's homogeneous
-  problem (its held nodes and, for a box, its sides inside the domain at zero) is solved
-  inexactly by one V-cycle of its multigrid, and the correction is added to the composite
-  nodes in the patch's box (bilinear between the patch's nodes at the finer nodes); sweeps
-  stop when the largest change falls below 1e-12 of the potential's scale; with a
-  Boltzmann species every Newton step's correction is found by the same sweeps, each
-  patch's multigrid rebuilt with the step's reaction;
+- the composite system is solved by restarted GMRES right-preconditioned with one fast
+  adaptive composite (FAC) sweep: coarse to fine, the composite residual is taken on a
+  patch's nodes, the patch's homogeneous problem (its held nodes and, for a box, its sides
+  inside the domain at zero) is solved inexactly by one V-cycle of its multigrid, and the
+  correction is added to the composite nodes in the patch's box (bilinear between the
+  patch's nodes at the finer nodes); with a Boltzmann species every Newton step's
+  correction is solved the same way, each patch's multigrid rebuilt with the step's
+  reaction;
 - the maps between composite nodes and patch arrays are row-compressed matrices applied
   by one kernel (``bt_csr_apply``) in a fixed order: the patches' potentials and the wider
   meshes of their fields (the margin bilinear from the coarser patches, finest wins, as
@@ -135,8 +135,8 @@ class CompositePoisson:
     ``fixed_region`` (a mask of the composite nodes, or a function of their ``(x, y)``) those
     nodes are held at ``fixed_potential`` as well; with ``plasma`` (a Boltzmann species:
     ``amplitude`` rho_0 / eps0, ``temperature``, ``up``, ``sign``) Newton's method from
-    ``phi``, each step's correction by the same sweeps with the Jacobian's reaction in every
-    patch's solver, until its largest update is below ``newton_tolerance``.
+    ``phi``, each step's correction by the same Krylov solve with the Jacobian's reaction
+    in every patch's solver, until its largest update is below ``newton_tolerance``.
     """
 
     def __init__(self, layout: Layout, *, tolerance: float = 1e-13, restart: int = 30,
