@@ -34,9 +34,30 @@ def _patch_rows(patch):
 
 def assemble(layout, rho=None):
     """The composite matrix and right-hand side for the charge density ``rho`` (composite
-    nodes, C/m^3, or None)."""
+    nodes, C/m^3, or None).  The matrix, the held values and the face sources depend on
+    the layout alone and are assembled once per layout."""
     n = layout.size
     rho = np.zeros(n) if rho is None else np.asarray(rho, dtype=float)
+    cached = _ASSEMBLED.get(id(layout))
+    if cached is None or cached[0] is not layout:
+        cached = (layout, *_assemble_fixed(layout))
+        _ASSEMBLED.clear()  # one layout at a time: no stale entries under a reused id
+        _ASSEMBLED[id(layout)] = cached
+    _, K, b0, charged = cached
+    b = b0.copy()
+    b[charged] += rho[charged] / epsilon_0
+    return K, b
+
+
+#: the last layout's assembled matrix, fixed right-hand side and charged rows
+_ASSEMBLED: dict = {}
+
+
+def _assemble_fixed(layout):
+    """The composite matrix, the right-hand side without charge and the rows that take
+    ``rho / eps0`` (the nodes with an equation of their own)."""
+    n = layout.size
+    rho = np.zeros(n)
     hang_row = {int(k): r for r, k in enumerate(layout.hanging)}
     interp = layout.interpolation.tocsr()
 
@@ -85,7 +106,8 @@ def assemble(layout, rho=None):
                 vals.append(-value * w)
         b[k] = rho[k] / epsilon_0 + src[a, c]
     K = sparse.csr_matrix((vals, (rows, cols)), shape=(n, n))
-    return K, b
+    charged = (layout.owner >= 0) & ~np.asarray(layout.fixed, dtype=bool)
+    return K, b, charged
 
 
 def solve(layout, rho=None) -> np.ndarray:
